@@ -1,0 +1,892 @@
+/* Test infrastructure only -- the checker the CUDA kernels are compared with.
+ * Never linked into, loaded by, or called from the product library.
+ *
+ * Plain-C restatement of the reference algorithms on the RkNN hot path of
+ * Yujian-Fu/anqi-implementation.  Every function names the reference file:line
+ * it restates.  Pinned against the reference's own outputs by the golden
+ * fixtures in tests/golden/ (see tests/test_oracle_golden.py).
+ *
+ * Compiled with -ffp-contract=off so no multiply-add is fused except where the
+ * reference uses an explicit FMA (the AVX-512 _mm512_fmadd_ps lanes).
+ */
+#include "anqi_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define AO_EMPTY 0xFFFFFFFFu
+static const float AO_EPS = 1e-6f; /* distance.h:14 */
+
+/* _mm512_reduce_add_ps as GCC 13 defines it (avx512fintrin.h): fold the upper
+ * 256-bit half onto the lower, then the upper 128-bit half, then lanes {2,3}
+ * onto {0,1}, then lane 1 onto lane 0. */
+static float reduce16(const float* A) {
+    float t3[8], t6[4];
+    for (int i = 0; i < 8; i++) t3[i] = A[i + 8] + A[i];
+    for (int j = 0; j < 4; j++) t6[j] = t3[j + 4] + t3[j];
+    float t80 = t6[0] + t6[2];
+    float t81 = t6[1] + t6[3];
+    return t80 + t81;
+}
+
+/* distance.h:58-86 */
+float ao_l2sqr(const float* a, const float* b, uint32_t dim) {
+    float acc[16] = {0};
+    uint32_t q16 = dim / 16, rem = dim % 16;
+    for (uint32_t c = 0; c < q16; c++)
+        for (int l = 0; l < 16; l++) {
+            float df = a[16 * c + l] - b[16 * c + l];
+            acc[l] = fmaf(df, df, acc[l]);
+        }
+    float res = reduce16(acc);
+    if (rem) {
+        float t[16] = {0};
+        for (uint32_t l = 0; l < rem; l++) {
+            float df = a[16 * q16 + l] - b[16 * q16 + l];
+            t[l] = df * df;
+        }
+        res += reduce16(t);
+    }
+    return res;
+}
+
+/* distance.h:89-116 (and the free function at distance.h:22-51, identical arithmetic) */
+float ao_ip(const float* a, const float* b, uint32_t dim) {
+    float acc[16] = {0};
+    uint32_t q16 = dim / 16, rem = dim % 16;
+    for (uint32_t c = 0; c < q16; c++)
+        for (int l = 0; l < 16; l++) acc[l] = fmaf(a[16 * c + l], b[16 * c + l], acc[l]);
+    float res = reduce16(acc);
+    if (rem) {
+        float t[16] = {0};
+        for (uint32_t l = 0; l < rem; l++) t[l] = a[16 * q16 + l] * b[16 * q16 + l];
+        res += reduce16(t);
+    }
+    return res;
+}
+
+/* distance.h:143-161 -- identical arithmetic to ao_ip(a, a) */
+float ao_norm(const float* a, uint32_t dim) { return ao_ip(a, a, dim); }
+
+/* index.h:172-176 */
+float ao_d2(const float* a, const float* b, float na, float nb, uint32_t dim) {
+    float s = na + nb;
+    float t = 2.0f * ao_ip(a, b, dim);
+    return s - t;
+}
+
+void ao_norms(const float* x, uint64_t n, uint32_t dim, float* out) {
+    for (uint64_t i = 0; i < n; i++) out[i] = ao_norm(x + i * dim, dim);
+}
+
+/* ------------------------------------------------------------------ LRQ */
+
+/* rknn_query.cpp:482-513, floor policy: last centre <= value, else the first. */
+static uint32_t floor_code(double value, const float* c, uint32_t cs) {
+    float v = (float)value;
+    uint32_t lo = 0, hi = cs; /* upper_bound: first element > v */
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) / 2;
+        if (v < c[mid]) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo == 0 ? 0 : lo - 1;
+}
+
+/* rknn_query.cpp:679-720 */
+void ao_lrq_encode(const float* keys, uint64_t n, uint32_t nk, uint32_t rankm,
+                   const float* mu, const float* basis, const float* codebook,
+                   uint32_t code_size, float* coeff, uint8_t* codes) {
+    for (uint64_t i = 0; i < n; i++) {
+        const float* rk = keys + i * nk;
+        float* ci = coeff + i * rankm;
+        for (uint32_t m = 0; m < rankm; m++) {
+            const float* gm = basis + (uint64_t)m * nk;
+            double c = 0.0;
+            for (uint32_t k = 0; k < nk; k++) c += ((double)rk[k] - (double)mu[k]) * (double)gm[k];
+            ci[m] = (float)c;
+        }
+        for (uint32_t k = 0; k < nk; k++) {
+            double recon = (double)mu[k];
+            for (uint32_t m = 0; m < rankm; m++) recon += (double)ci[m] * (double)basis[(uint64_t)m * nk + k];
+            double residual = (double)rk[k] - recon;
+            codes[i * nk + k] = (uint8_t)floor_code(residual, codebook + (uint64_t)k * code_size, code_size);
+        }
+    }
+}
+
+/* rknn_query.cpp:722-753 (L2: clamp at zero) */
+void ao_lrq_materialize(const float* coeff, const uint8_t* codes, uint64_t n, uint32_t nk,
+                        uint32_t rankm, const float* mu, const float* basis,
+                        const float* codebook, uint32_t code_size, uint32_t k_one_based,
+                        double radius_scale, float* thr) {
+    uint32_t k = k_one_based - 1;
+    for (uint64_t i = 0; i < n; i++) {
+        const float* ci = coeff + i * rankm;
+        double value = (double)mu[k];
+        for (uint32_t m = 0; m < rankm; m++) value += (double)ci[m] * (double)basis[(uint64_t)m * nk + k];
+        value += (double)codebook[(uint64_t)k * code_size + codes[i * nk + k]];
+        double scaled = radius_scale * value;
+        thr[i] = (float)(0.0 < scaled ? scaled : 0.0);
+    }
+}
+
+/* ----------------------------------------------------------------- lift */
+
+/* rknn_query.cpp:2203-2235: anyk_lift, L2, graph radius = the AKNN rank-K cutoff.
+ * The sum of squared norms is accumulated row by row in index order (the
+ * reference's OpenMP reduction at one thread). */
+void ao_lift(const float* base, uint64_t n, uint32_t d, const float* radius,
+             float* lifted, double* mstar2, double* scale) {
+    double sum_n2 = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        const float* o = base + i * d;
+        double s = 0;
+        for (uint32_t j = 0; j < d; j++) s += (double)o[j] * o[j];
+        sum_n2 += s;
+    }
+    double s_scale = 1.0 / sqrt(sum_n2 / (double)n + 1e-12), sc2 = s_scale * s_scale;
+    uint32_t dl = d + 1, dout = d + 2;
+    double maxn2 = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        const float* o = base + i * d;
+        float* h = lifted + i * dout;
+        double nr2 = 0;
+        for (uint32_t j = 0; j < d; j++) {
+            double v = (double)o[j] * s_scale;
+            h[j] = (float)v;
+            nr2 += v * v;
+        }
+        h[d] = (float)(0.5 * ((double)radius[i] * sc2 - nr2));
+        double hn2 = nr2 + (double)h[d] * h[d];
+        if (hn2 > maxn2) maxn2 = hn2;
+    }
+    double M2 = maxn2 * 1.0001;
+    for (uint64_t i = 0; i < n; i++) {
+        float* h = lifted + i * dout;
+        double hn2 = 0;
+        for (uint32_t j = 0; j < dl; j++) hn2 += (double)h[j] * h[j];
+        double pad = M2 - hn2;
+        if (pad < 0) pad = 0;
+        h[dl] = (float)sqrt(pad);
+    }
+    *mstar2 = M2;
+    *scale = s_scale;
+}
+
+/* rknn_query.cpp:2724-2729 */
+void ao_lift_query(const float* q, uint32_t d, double scale, float* out) {
+    for (uint32_t j = 0; j < d; j++) out[j] = (float)((double)q[j] * scale);
+    out[d] = 1.0f;
+    out[d + 1] = 0.0f;
+}
+
+/* ------------------------------------------------------------ tree entry */
+
+/* rptrees.h:108-124.  Root = last node (post-order) -- callers pass arrays in
+ * the reference's post-order.  |margin| <= EPS takes the left child (the
+ * reference draws a thread-local random bit there). */
+uint32_t ao_tree_entry(uint32_t n_nodes, uint32_t dim, const uint32_t* left,
+                       const uint32_t* right, const float* offset, const float* hyperplane,
+                       const uint32_t* leaf_first, const float* q) {
+    uint32_t v = n_nodes - 1;
+    while (left[v] != AO_EMPTY) {
+        float margin = ao_ip(hyperplane + (uint64_t)v * dim, q, dim) - offset[v];
+        if (margin < -AO_EPS) v = left[v];
+        else if (margin > AO_EPS) v = right[v];
+        else v = left[v];
+    }
+    return leaf_first[v] == AO_EMPTY ? 0 : leaf_first[v];
+}
+
+/* ---------------------------------------------------- ordered beam queue */
+
+/* neighbor.h:10-27,43-141: (dist, id) total order, bit 31 = expanded. */
+typedef struct {
+    float d;
+    uint32_t id;
+} nb_t;
+typedef struct {
+    nb_t* data;
+    uint32_t size, cap, cur;
+} queue_t;
+
+static int nb_less(nb_t a, nb_t b) {
+    uint32_t ia = a.id & 0x7FFFFFFFu, ib = b.id & 0x7FFFFFFFu;
+    return a.d < b.d || (a.d == b.d && ia < ib);
+}
+
+static void q_init(queue_t* q, uint32_t cap) {
+    q->data = (nb_t*)malloc(sizeof(nb_t) * (cap + 1));
+    q->size = 0;
+    q->cap = cap;
+    q->cur = 0;
+}
+
+/* neighbor.h:61-102 */
+static void q_insert(queue_t* q, float d, uint32_t id) {
+    nb_t x = {d, id};
+    if (q->cap == 0 || (q->size == q->cap && nb_less(q->data[q->size - 1], x))) return;
+    uint32_t lo = 0, hi = q->size;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (nb_less(x, q->data[mid])) hi = mid;
+        else if ((q->data[mid].id & 0x7FFFFFFFu) == id) return;
+        else lo = mid + 1;
+    }
+    if (lo < q->cap) memmove(&q->data[lo + 1], &q->data[lo], (q->size - lo) * sizeof(nb_t));
+    q->data[lo] = x;
+    if (q->size < q->cap) q->size++;
+    if (lo < q->cur) q->cur = lo;
+}
+
+/* neighbor.h:105-111 */
+static uint32_t q_pop(queue_t* q) {
+    q->data[q->cur].id |= 0x80000000u;
+    uint32_t pre = q->cur;
+    while (q->cur < q->size && (q->data[q->cur].id & 0x80000000u)) q->cur++;
+    return q->data[pre].id & 0x7FFFFFFFu;
+}
+
+/* --------------------------------------------------------- range search */
+
+/* index.h:1535-1640 with the pinned configuration: eps = 0, radj = null,
+ * center beam key, collect threshold = flood threshold = R2.  Followed by the
+ * postfilter at rknn_query.cpp:2555-2561,2762-2765. */
+int ao_range_search(const ao_index* ix, const float* q, uint32_t L, const float* thr,
+                    uint32_t* cand, uint32_t cand_cap, uint32_t* n_cand,
+                    uint32_t* pred, uint32_t pred_cap, uint32_t* n_pred, uint32_t* n_dist) {
+    const uint32_t dim = ix->dim, d = ix->d;
+    float* qb = (float*)malloc(sizeof(float) * dim);
+    ao_lift_query(q, d, ix->scale, qb);
+    double R2 = ix->mstar2 + 1.0;
+    uint8_t* vis = (uint8_t*)calloc(ix->n, 1);
+    uint32_t* flood = (uint32_t*)malloc(sizeof(uint32_t) * (ix->n + 1));
+    uint64_t nf = 0, head = 0;
+    uint32_t nc = 0, nd = 0;
+    int rc = 0;
+    queue_t beam;
+    q_init(&beam, L);
+    uint32_t ep = ao_tree_entry(ix->tree_nodes, dim, ix->tree_left, ix->tree_right, ix->tree_offset,
+                                ix->tree_hyperplane, ix->tree_leaf_first, qb);
+    float dep = ao_l2sqr(ix->lifted + (uint64_t)ep * dim, qb, dim);
+    nd++;
+    vis[ep] = 1;
+    q_insert(&beam, dep, ep);
+    if ((double)dep <= R2) {
+        flood[nf++] = ep;
+        if (nc < cand_cap) cand[nc] = ep;
+        nc++;
+    }
+    while (beam.cur < beam.size) {
+        uint32_t cur = q_pop(&beam);
+        const uint32_t* lk = ix->links + (uint64_t)cur * ix->degree;
+        for (uint32_t j = 0; j < ix->deg[cur]; j++) {
+            uint32_t nb = lk[j];
+            if (vis[nb]) continue;
+            vis[nb] = 1;
+            float dd = ao_l2sqr(ix->lifted + (uint64_t)nb * dim, qb, dim);
+            nd++;
+            q_insert(&beam, dd, nb);
+            if ((double)dd <= R2) {
+                flood[nf++] = nb;
+                if (nc < cand_cap) cand[nc] = nb;
+                nc++;
+            }
+        }
+    }
+    while (head < nf) {
+        uint32_t cur = flood[head++];
+        const uint32_t* lk = ix->links + (uint64_t)cur * ix->degree;
+        for (uint32_t j = 0; j < ix->deg[cur]; j++) {
+            uint32_t nb = lk[j];
+            if (vis[nb]) continue;
+            vis[nb] = 1;
+            float dd = ao_l2sqr(ix->lifted + (uint64_t)nb * dim, qb, dim);
+            nd++;
+            if ((double)dd <= R2) {
+                if (nc < cand_cap) cand[nc] = nb;
+                nc++;
+                flood[nf++] = nb;
+            }
+        }
+    }
+    uint32_t np = 0;
+    if (nc > cand_cap) rc = -1;
+    float qn = ao_ip(q, q, d);
+    for (uint32_t c = 0; c < nc && c < cand_cap; c++) {
+        const float* o = ix->base + (uint64_t)cand[c] * d;
+        float ip = ao_ip(o, q, d);
+        float on = ao_ip(o, o, d);
+        float key = (on + qn) - 2.0f * ip;
+        if ((double)key <= (double)thr[cand[c]]) {
+            if (np < pred_cap) pred[np] = cand[c];
+            else rc = -1;
+            np++;
+        }
+    }
+    *n_cand = nc;
+    *n_pred = np;
+    *n_dist = nd;
+    free(beam.data);
+    free(flood);
+    free(vis);
+    free(qb);
+    return rc;
+}
+
+/* ------------------------------------------------------- gather / prune */
+
+static float gd2(const ao_knn_graph* g, uint64_t a, uint64_t b) {
+    return ao_d2(g->x + a * g->dim, g->x + b * g->dim, g->norms[a], g->norms[b], g->dim);
+}
+
+/* index.h:1491-1525 */
+int64_t ao_gather(const ao_knn_graph* g, uint64_t i, uint32_t ef, uint32_t cap,
+                  float* pool_d, uint32_t* pool_id, uint64_t pool_cap) {
+    uint8_t* vis = (uint8_t*)calloc(g->n, 1);
+    queue_t cand;
+    q_init(&cand, ef);
+    uint64_t np = 0;
+    int over = 0;
+#define AO_PUSH(ID, D)                     \
+    do {                                   \
+        if (np < pool_cap) {               \
+            pool_d[np] = (D);              \
+            pool_id[np] = (ID);            \
+        } else                             \
+            over = 1;                      \
+        np++;                              \
+    } while (0)
+    for (uint32_t j = 0; j < g->K; j++) {
+        uint32_t id = g->g_ids[i * g->K + j];
+        if (id == AO_EMPTY || id >= g->n) continue;
+        if (vis[id]) continue;
+        vis[id] = 1;
+        float d = g->g_vals[i * g->K + j];
+        q_insert(&cand, d, id);
+        AO_PUSH(id, d);
+    }
+    while (cand.cur < cand.size) {
+        uint32_t cur = q_pop(&cand);
+        for (uint32_t j = 0; j < g->K; j++) {
+            uint32_t nb = g->g_ids[(uint64_t)cur * g->K + j];
+            if (nb == AO_EMPTY || nb >= g->n || vis[nb]) continue;
+            vis[nb] = 1;
+            float d = gd2(g, i, nb);
+            q_insert(&cand, d, nb);
+            AO_PUSH(nb, d);
+        }
+        for (uint64_t p = g->rev_off[cur]; p < g->rev_off[cur + 1]; p++) {
+            uint32_t nb = g->rev_ids[p];
+            if (nb == AO_EMPTY || nb >= g->n || vis[nb]) continue;
+            vis[nb] = 1;
+            float d = gd2(g, i, nb);
+            q_insert(&cand, d, nb);
+            AO_PUSH(nb, d);
+        }
+        if (np >= cap) break;
+    }
+#undef AO_PUSH
+    free(cand.data);
+    free(vis);
+    return over ? -1 : (int64_t)np;
+}
+
+typedef struct {
+    float d;
+    uint32_t id;
+} pair_t;
+
+static int cmp_dist_id(const void* a, const void* b) {
+    const pair_t* x = (const pair_t*)a;
+    const pair_t* y = (const pair_t*)b;
+    if (x->d < y->d) return -1;
+    if (x->d > y->d) return 1;
+    return (x->id > y->id) - (x->id < y->id);
+}
+
+static int cmp_id_dist(const void* a, const void* b) {
+    const pair_t* x = (const pair_t*)a;
+    const pair_t* y = (const pair_t*)b;
+    if (x->id != y->id) return (x->id > y->id) - (x->id < y->id);
+    return (x->d > y->d) - (x->d < y->d);
+}
+
+/* index.h:1347-1366 */
+void ao_aknn_rows(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t K,
+                  uint32_t* out_ids, float* out_d) {
+    uint64_t pool_cap = (uint64_t)cap + (uint64_t)g->K + (g->rev_off[g->n] - g->rev_off[0]) + 1;
+    float* pd = (float*)malloc(sizeof(float) * pool_cap);
+    uint32_t* pi = (uint32_t*)malloc(sizeof(uint32_t) * pool_cap);
+    pair_t* pr = (pair_t*)malloc(sizeof(pair_t) * pool_cap);
+    for (uint64_t i = 0; i < g->n; i++) {
+        int64_t np = ao_gather(g, i, ef, cap, pd, pi, pool_cap);
+        for (int64_t p = 0; p < np; p++) {
+            pr[p].d = pd[p];
+            pr[p].id = pi[p];
+        }
+        qsort(pr, (size_t)np, sizeof(pair_t), cmp_dist_id);
+        uint32_t c = 0;
+        for (int64_t p = 0; p < np && c < K; p++) {
+            if (pr[p].id == (uint32_t)i) continue;
+            out_ids[i * K + c] = pr[p].id;
+            out_d[i * K + c] = pr[p].d;
+            c++;
+        }
+        for (; c < K; c++) {
+            out_ids[i * K + c] = AO_EMPTY;
+            out_d[i * K + c] = FLT_MAX;
+        }
+    }
+    free(pd);
+    free(pi);
+    free(pr);
+}
+
+/* sort_unique_candidates (index.h:225-248) + rng_extend (index.h:267-281) as
+ * prune_pool_to_ids runs them with the default edge policy (index.h:823-828). */
+uint32_t ao_prune(const float* x, const float* norms, uint32_t dim, uint64_t n, uint64_t i,
+                  float* pool_d, uint32_t* pool_id, uint64_t pool_n, uint32_t M, float alpha,
+                  uint32_t* out) {
+    pair_t* c = (pair_t*)malloc(sizeof(pair_t) * (pool_n + 1));
+    uint64_t m = 0;
+    for (uint64_t p = 0; p < pool_n; p++) {
+        uint32_t id = pool_id[p];
+        if (id == AO_EMPTY || id >= n || id == (uint32_t)i) continue;
+        c[m].d = pool_d[p];
+        c[m].id = id;
+        m++;
+    }
+    qsort(c, (size_t)m, sizeof(pair_t), cmp_id_dist);
+    uint64_t w = 0;
+    for (uint64_t r = 0; r < m;) {
+        uint32_t id = c[r].id;
+        float best = c[r].d;
+        uint64_t e = r + 1;
+        while (e < m && c[e].id == id) {
+            if (c[e].d < best) best = c[e].d;
+            e++;
+        }
+        c[w].d = best;
+        c[w].id = id;
+        w++;
+        r = e;
+    }
+    qsort(c, (size_t)w, sizeof(pair_t), cmp_dist_id);
+    uint32_t sel = 0;
+    for (uint64_t p = 0; p < w; p++) {
+        if (sel >= M) break;
+        uint32_t cid = c[p].id;
+        int occluded = 0;
+        for (uint32_t s = 0; s < sel; s++) {
+            float dsc = ao_d2(x + (uint64_t)out[s] * dim, x + (uint64_t)cid * dim, norms[out[s]], norms[cid], dim);
+            if (alpha * dsc < c[p].d) {
+                occluded = 1;
+                break;
+            }
+        }
+        if (!occluded) out[sel++] = cid;
+    }
+    free(c);
+    return sel;
+}
+
+/* build_index gather + prune loop, index.h:1248-1257 */
+void ao_graph_select(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t M, float alpha,
+                     uint32_t* O, uint32_t* O_deg) {
+    uint64_t pool_cap = (uint64_t)cap + (uint64_t)g->K + (g->rev_off[g->n] - g->rev_off[0]) + 1;
+    float* pd = (float*)malloc(sizeof(float) * pool_cap);
+    uint32_t* pi = (uint32_t*)malloc(sizeof(uint32_t) * pool_cap);
+    for (uint64_t i = 0; i < g->n; i++) {
+        int64_t np = ao_gather(g, i, ef, cap, pd, pi, pool_cap);
+        uint32_t* row = O + i * M;
+        for (uint32_t j = 0; j < M; j++) row[j] = AO_EMPTY;
+        O_deg[i] = ao_prune(g->x, g->norms, g->dim, g->n, i, pd, pi, (uint64_t)np, M, alpha, row);
+    }
+    free(pd);
+    free(pi);
+}
+
+/* commit_edges, index.h:907-930 */
+void ao_graph_commit(const float* x, const float* norms, uint32_t dim, uint64_t n,
+                     const uint32_t* O, const uint32_t* O_deg, uint32_t M, float alpha,
+                     uint32_t* links, uint32_t* deg) {
+    uint64_t* roff = (uint64_t*)calloc(n + 1, sizeof(uint64_t));
+    for (uint64_t i = 0; i < n; i++)
+        for (uint32_t j = 0; j < O_deg[i]; j++) roff[O[i * M + j] + 1]++;
+    for (uint64_t i = 0; i < n; i++) roff[i + 1] += roff[i];
+    uint32_t* rids = (uint32_t*)malloc(sizeof(uint32_t) * (roff[n] + 1));
+    uint64_t* fill = (uint64_t*)calloc(n, sizeof(uint64_t));
+    for (uint64_t i = 0; i < n; i++)
+        for (uint32_t j = 0; j < O_deg[i]; j++) {
+            uint32_t t = O[i * M + j];
+            rids[roff[t] + fill[t]++] = (uint32_t)i;
+        }
+    uint64_t maxc = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t c = O_deg[i] + (roff[i + 1] - roff[i]);
+        if (c > maxc) maxc = c;
+    }
+    float* pd = (float*)malloc(sizeof(float) * (maxc + 1));
+    uint32_t* pi = (uint32_t*)malloc(sizeof(uint32_t) * (maxc + 1));
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t c = 0;
+        for (uint32_t j = 0; j < O_deg[i]; j++) {
+            uint32_t t = O[i * M + j];
+            pd[c] = ao_d2(x + i * dim, x + (uint64_t)t * dim, norms[i], norms[t], dim);
+            pi[c++] = t;
+        }
+        for (uint64_t p = roff[i]; p < roff[i + 1]; p++) {
+            uint32_t t = rids[p];
+            pd[c] = ao_d2(x + i * dim, x + (uint64_t)t * dim, norms[i], norms[t], dim);
+            pi[c++] = t;
+        }
+        uint32_t* row = links + i * M;
+        for (uint32_t j = 0; j < M; j++) row[j] = AO_EMPTY;
+        deg[i] = ao_prune(x, norms, dim, n, i, pd, pi, c, M, alpha, row);
+    }
+    free(pd);
+    free(pi);
+    free(roff);
+    free(rids);
+    free(fill);
+}
+
+/* -------------------------------------------------------------- heaps */
+
+/* heap.h:162-186 (push_nolock; check_push without reverse edges is identical) */
+int ao_heap_push(uint32_t* ids, float* vals, uint32_t K, uint32_t node, float value) {
+    if (value > vals[0]) return 0;
+    for (uint32_t i = 0; i < K; i++)
+        if (ids[i] == node) return 0;
+    uint32_t cur = 0, sw;
+    for (;;) {
+        uint32_t l = 2 * cur + 1, r = l + 1;
+        if (l >= K) break;
+        else if (r >= K) {
+            if (vals[l] > value) sw = l;
+            else break;
+        } else if (vals[l] >= vals[r]) {
+            if (vals[l] > value) sw = l;
+            else break;
+        } else {
+            if (vals[r] > value) sw = r;
+            else break;
+        }
+        ids[cur] = ids[sw];
+        vals[cur] = vals[sw];
+        cur = sw;
+    }
+    ids[cur] = node;
+    vals[cur] = value;
+    return 1;
+}
+
+/* index.h:1210-1217 */
+void ao_warm_start(const float* x, const float* norms, uint32_t dim, uint64_t n,
+                   const uint32_t* cand, uint32_t stride, uint32_t width, uint32_t K,
+                   uint32_t* ids, float* vals) {
+    for (uint64_t i = 0; i < n; i++) {
+        uint32_t* hi = ids + i * K;
+        float* hv = vals + i * K;
+        for (uint32_t s = 0; s < K; s++) {
+            hi[s] = AO_EMPTY;
+            hv[s] = FLT_MAX;
+        }
+        for (uint32_t k = 0; k < width; k++) {
+            uint32_t j = cand[i * stride + k];
+            if (j != (uint32_t)i && j < n)
+                ao_heap_push(hi, hv, K, j, ao_d2(x + i * dim, x + (uint64_t)j * dim, norms[i], norms[j], dim));
+        }
+    }
+}
+
+/* index.h:1468-1487, snapshot form (see the header). */
+uint64_t ao_localjoin_round(const float* x, const float* norms, uint32_t dim, uint64_t n,
+                            uint32_t K, uint32_t sample, uint32_t* ids, float* vals) {
+    uint32_t* loc = (uint32_t*)malloc(sizeof(uint32_t) * n * sample);
+    uint32_t* cnt = (uint32_t*)calloc(n, sizeof(uint32_t));
+    for (uint64_t u = 0; u < n; u++)
+        for (uint32_t s = 0; s < K && cnt[u] < sample; s++) {
+            uint32_t v = ids[u * K + s];
+            if (v != AO_EMPTY) loc[u * sample + cnt[u]++] = v;
+        }
+    /* incoming (source, position) lists per target, sources ascending */
+    uint64_t* off = (uint64_t*)calloc(n + 1, sizeof(uint64_t));
+    for (uint64_t u = 0; u < n; u++)
+        for (uint32_t a = 0; a < cnt[u]; a++) off[loc[u * sample + a] + 1]++;
+    for (uint64_t i = 0; i < n; i++) off[i + 1] += off[i];
+    uint64_t* fill = (uint64_t*)calloc(n, sizeof(uint64_t));
+    uint64_t* inc = (uint64_t*)malloc(sizeof(uint64_t) * (off[n] + 1));
+    for (uint64_t u = 0; u < n; u++)
+        for (uint32_t a = 0; a < cnt[u]; a++) {
+            uint32_t t = loc[u * sample + a];
+            inc[off[t] + fill[t]++] = (u << 8) | a;
+        }
+    uint64_t upd = 0;
+    for (uint64_t t = 0; t < n; t++) {
+        for (uint64_t p = off[t]; p < off[t + 1]; p++) {
+            uint64_t u = inc[p] >> 8;
+            uint32_t a = (uint32_t)(inc[p] & 0xFF);
+            for (uint32_t b = 0; b < cnt[u]; b++) {
+                if (b == a) continue;
+                uint32_t w = loc[u * sample + b];
+                float dd = ao_d2(x + t * dim, x + (uint64_t)w * dim, norms[t], norms[w], dim);
+                upd += (uint64_t)ao_heap_push(ids + t * K, vals + t * K, K, w, dd);
+            }
+        }
+    }
+    free(loc);
+    free(cnt);
+    free(off);
+    free(fill);
+    free(inc);
+    return upd;
+}
+
+/* heap.h:190-207 */
+void ao_reverse(const uint32_t* ids, uint64_t n, uint32_t K, uint64_t* rev_off, uint32_t* rev_ids) {
+    memset(rev_off, 0, sizeof(uint64_t) * (n + 1));
+    for (uint64_t i = 0; i < n; i++)
+        for (uint32_t j = 0; j < K; j++) {
+            uint32_t v = ids[i * K + j];
+            if (v != AO_EMPTY && v < n) rev_off[v + 1]++;
+        }
+    for (uint64_t i = 0; i < n; i++) rev_off[i + 1] += rev_off[i];
+    uint64_t* fill = (uint64_t*)calloc(n, sizeof(uint64_t));
+    for (uint64_t i = 0; i < n; i++)
+        for (uint32_t j = 0; j < K; j++) {
+            uint32_t v = ids[i * K + j];
+            if (v != AO_EMPTY && v < n) rev_ids[rev_off[v] + fill[v]++] = (uint32_t)i;
+        }
+    free(fill);
+}
+
+/* ------------------------------------------------------------ init_knn */
+
+void ao_init_knn(const float* x, const float* norms, uint32_t dim, uint64_t n, uint32_t K,
+                 const uint64_t* leaf_off, const uint32_t* leaf_ids, uint64_t n_leaves,
+                 uint32_t* out_ids, float* out_d) {
+    /* per row: collect (d, id) of all leaf-mates, dedupe, keep K smallest */
+    uint64_t* cnt = (uint64_t*)calloc(n + 1, sizeof(uint64_t));
+    for (uint64_t l = 0; l < n_leaves; l++) {
+        uint64_t sz = leaf_off[l + 1] - leaf_off[l];
+        for (uint64_t a = leaf_off[l]; a < leaf_off[l + 1]; a++) cnt[leaf_ids[a] + 1] += sz - 1;
+    }
+    for (uint64_t i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+    pair_t* all = (pair_t*)malloc(sizeof(pair_t) * (cnt[n] + 1));
+    uint64_t* fill = (uint64_t*)calloc(n, sizeof(uint64_t));
+    for (uint64_t l = 0; l < n_leaves; l++)
+        for (uint64_t a = leaf_off[l]; a < leaf_off[l + 1]; a++)
+            for (uint64_t b = leaf_off[l]; b < leaf_off[l + 1]; b++) {
+                if (a == b) continue;
+                uint32_t p = leaf_ids[a], q = leaf_ids[b];
+                pair_t* e = &all[cnt[p] + fill[p]++];
+                e->id = q;
+                e->d = ao_d2(x + (uint64_t)p * dim, x + (uint64_t)q * dim, norms[p], norms[q], dim);
+            }
+    for (uint64_t i = 0; i < n; i++) {
+        pair_t* r = all + cnt[i];
+        uint64_t m = cnt[i + 1] - cnt[i];
+        qsort(r, (size_t)m, sizeof(pair_t), cmp_dist_id);
+        uint32_t c = 0;
+        for (uint64_t p = 0; p < m && c < K; p++) {
+            if (p > 0 && r[p].id == r[p - 1].id) continue; /* same pair, same distance */
+            int dup = 0;
+            for (uint32_t s = 0; s < c; s++)
+                if (out_ids[i * K + s] == r[p].id) {
+                    dup = 1;
+                    break;
+                }
+            if (dup) continue;
+            out_ids[i * K + c] = r[p].id;
+            out_d[i * K + c] = r[p].d;
+            c++;
+        }
+        for (; c < K; c++) {
+            out_ids[i * K + c] = AO_EMPTY;
+            out_d[i * K + c] = FLT_MAX;
+        }
+    }
+    free(cnt);
+    free(all);
+    free(fill);
+}
+
+/* --------------------------------------------------------------- forest */
+
+uint64_t ao_hash64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+static uint64_t node_key(uint64_t seed, uint32_t tree, uint32_t node) {
+    return ao_hash64(ao_hash64(seed ^ ((uint64_t)tree << 32)) ^ (uint64_t)node);
+}
+
+/* rptrees.h:28-84,127-163 in deterministic breadth-first form. */
+int64_t ao_rp_tree(const float* x, uint64_t n, uint32_t dim, uint32_t leaf_size,
+                   uint32_t max_depth, uint64_t seed, uint32_t tree, ao_tree_out* out) {
+    uint32_t* start = (uint32_t*)malloc(sizeof(uint32_t) * out->cap_nodes);
+    uint32_t* count = (uint32_t*)malloc(sizeof(uint32_t) * out->cap_nodes);
+    uint32_t* depth = (uint32_t*)malloc(sizeof(uint32_t) * out->cap_nodes);
+    uint32_t* tmp = (uint32_t*)malloc(sizeof(uint32_t) * (n + 1));
+    uint8_t* side = (uint8_t*)malloc(n + 1);
+    float* mid = (float*)malloc(sizeof(float) * dim);
+    for (uint64_t i = 0; i < n; i++) out->perm[i] = (uint32_t)i;
+    start[0] = 0;
+    count[0] = (uint32_t)n;
+    depth[0] = 0;
+    uint32_t n_nodes = 1;
+    int64_t rc = 0;
+    for (uint32_t v = 0; v < n_nodes; v++) {
+        uint32_t s = start[v], c = count[v];
+        float* hp = out->hyperplane + (uint64_t)v * dim;
+        if (c <= leaf_size || depth[v] >= max_depth) {
+            out->left[v] = out->right[v] = AO_EMPTY;
+            out->offset[v] = FLT_MAX;
+            out->leaf_off[v] = s;
+            out->leaf_cnt[v] = c <= leaf_size ? c : leaf_size;
+            continue;
+        }
+        if (n_nodes + 2 > out->cap_nodes) {
+            rc = -1;
+            break;
+        }
+        uint64_t key = node_key(seed, tree, v);
+        uint32_t r0 = (uint32_t)(ao_hash64(key ^ 1) % c);
+        uint32_t r1 = (uint32_t)(ao_hash64(key ^ 2) % c);
+        if (r0 == r1) r0 = (r1 + 1) % c;
+        const float* x0 = x + (uint64_t)out->perm[s + r0] * dim;
+        const float* x1 = x + (uint64_t)out->perm[s + r1] * dim;
+        for (uint32_t j = 0; j < dim; j++) {
+            mid[j] = (x0[j] + x1[j]) / 2;
+            hp[j] = x0[j] - x1[j];
+        }
+        float off = ao_ip(hp, mid, dim);
+        uint32_t nl = 0;
+        for (uint32_t p = 0; p < c; p++) {
+            uint32_t id = out->perm[s + p];
+            float m = ao_ip(hp, x + (uint64_t)id * dim, dim) - off;
+            uint8_t sd;
+            if (m < -AO_EPS) sd = 0;
+            else if (m > AO_EPS) sd = 1;
+            else sd = (uint8_t)(ao_hash64(key ^ ((uint64_t)id << 2 | 3)) & 1);
+            side[p] = sd;
+            nl += (sd == 0);
+        }
+        if (nl == 0 || nl == c) {
+            nl = 0;
+            for (uint32_t p = 0; p < c; p++) {
+                uint32_t id = out->perm[s + p];
+                side[p] = (uint8_t)(ao_hash64(key ^ ((uint64_t)id << 2 | 2)) & 1);
+                nl += (side[p] == 0);
+            }
+        }
+        uint32_t a = 0, b = nl;
+        for (uint32_t p = 0; p < c; p++) tmp[side[p] ? b++ : a++] = out->perm[s + p];
+        memcpy(out->perm + s, tmp, sizeof(uint32_t) * c);
+        uint32_t L = n_nodes, R = n_nodes + 1;
+        n_nodes += 2;
+        out->left[v] = L;
+        out->right[v] = R;
+        out->offset[v] = off;
+        out->leaf_off[v] = AO_EMPTY;
+        out->leaf_cnt[v] = 0;
+        start[L] = s;
+        count[L] = nl;
+        depth[L] = depth[v] + 1;
+        start[R] = s + nl;
+        count[R] = c - nl;
+        depth[R] = depth[v] + 1;
+    }
+    free(start);
+    free(count);
+    free(depth);
+    free(tmp);
+    free(side);
+    free(mid);
+    return rc < 0 ? rc : (int64_t)n_nodes;
+}
+
+/* ---------------------------------------------------------- ground truth */
+
+typedef struct {
+    float key;
+    uint32_t id;
+} kv_t;
+
+static int cmp_kv(const void* a, const void* b) {
+    const kv_t* x = (const kv_t*)a;
+    const kv_t* y = (const kv_t*)b;
+    if (x->key < y->key) return -1;
+    if (x->key > y->key) return 1;
+    return (x->id > y->id) - (x->id < y->id);
+}
+
+/* dataset_gt.cpp:206-248: K smallest (key, id) with the diagonal skipped. */
+void ao_exact_topk(const float* base, uint64_t n, uint32_t d, uint32_t K, uint32_t* ids, float* keys) {
+    float* bn = (float*)malloc(sizeof(float) * n);
+    kv_t* row = (kv_t*)malloc(sizeof(kv_t) * n);
+    for (uint64_t i = 0; i < n; i++) bn[i] = ao_ip(base + i * d, base + i * d, d);
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t m = 0;
+        for (uint64_t j = 0; j < n; j++) {
+            if (j == i) continue;
+            float ip = ao_ip(base + i * d, base + j * d, d);
+            row[m].key = (bn[i] + bn[j]) - 2.0f * ip;
+            row[m].id = (uint32_t)j;
+            m++;
+        }
+        qsort(row, (size_t)m, sizeof(kv_t), cmp_kv);
+        for (uint32_t r = 0; r < K; r++) {
+            ids[i * K + r] = r < m ? row[r].id : AO_EMPTY;
+            keys[i * K + r] = r < m ? row[r].key : FLT_MAX;
+        }
+    }
+    free(bn);
+    free(row);
+}
+
+/* dataset_gt.cpp:270-299 */
+int64_t ao_rknn_gt(const float* base, uint64_t n, const float* query, uint64_t nq, uint32_t d,
+                   const float* rk2, uint32_t* off, uint32_t* ids, float* keys, uint64_t cap) {
+    float* bn = (float*)malloc(sizeof(float) * n);
+    kv_t* hits = (kv_t*)malloc(sizeof(kv_t) * (n + 1));
+    for (uint64_t i = 0; i < n; i++) bn[i] = ao_ip(base + i * d, base + i * d, d);
+    uint64_t total = 0;
+    int over = 0;
+    off[0] = 0;
+    for (uint64_t q = 0; q < nq; q++) {
+        const float* qv = query + q * d;
+        float qn = ao_ip(qv, qv, d);
+        uint64_t m = 0;
+        for (uint64_t j = 0; j < n; j++) {
+            float ip = ao_ip(qv, base + j * d, d);
+            float key = (qn + bn[j]) - 2.0f * ip;
+            if (key <= rk2[j]) {
+                hits[m].key = key;
+                hits[m].id = (uint32_t)j;
+                m++;
+            }
+        }
+        qsort(hits, (size_t)m, sizeof(kv_t), cmp_kv);
+        for (uint64_t h = 0; h < m; h++) {
+            if (total + h < cap) {
+                ids[total + h] = hits[h].id;
+                keys[total + h] = hits[h].key;
+            } else
+                over = 1;
+        }
+        total += m;
+        off[q + 1] = (uint32_t)total;
+    }
+    free(bn);
+    free(hits);
+    return over ? -1 : (int64_t)total;
+}

@@ -1,0 +1,264 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures from the reference implementation itself.
+
+Runs only where the reference tree and the binaries built by ``make -C oracle ref``
+exist.  Every number stored in the fixtures comes from the reference's own code:
+its CLIs (build_aknn_source, dataset_gt, rknn_query), its NumPy trainer, and
+oracle/ref_harness (the reference's functions driven stage by stage, one thread).
+
+Fixtures:
+  dist.npz        distance kernels of include/distance.h on random pairs
+  sample_d8.npz   the reference's own sample (scripts/make_sample_dataset.py:24-26,
+                  256 x 8 base, 32 queries, N(0,1), seed 20260819)
+  sample_d32.npz  the same recipe at d = 32 (the small configuration of the build plan)
+
+Usage: python tests/golden/make_golden.py [--ref /root/reference]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import re
+import shutil
+import struct
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent.parent
+REFBIN = REPO / "oracle" / "_ref"
+
+
+def write_fbin(path: Path, x: np.ndarray) -> None:
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    with path.open("wb") as f:
+        f.write(struct.pack("<II", x.shape[0], x.shape[1]))
+        x.tofile(f)
+
+
+def read_fbin(path: Path) -> np.ndarray:
+    raw = path.read_bytes()
+    n, d = struct.unpack("<II", raw[:8])
+    return np.frombuffer(raw[8:], dtype=np.float32).reshape(n, d).copy()
+
+
+def read_csr64(path: Path):
+    raw = path.read_bytes()
+    n = struct.unpack("<Q", raw[:8])[0]
+    off = np.frombuffer(raw[8 : 8 + 8 * (n + 1)], dtype=np.uint64).copy()
+    ids = np.frombuffer(raw[8 + 8 * (n + 1) :], dtype=np.uint32).copy()
+    return off, ids
+
+
+def read_heaps(path: Path, n: int, k: int):
+    raw = np.fromfile(path, dtype=np.uint32)
+    ids = raw[: n * k].reshape(n, k).copy()
+    vals = raw[n * k :].view(np.float32).reshape(n, k).copy()
+    return ids, vals
+
+
+def run(cmd, env=None, cwd=None) -> str:
+    full_env = dict(os.environ)
+    if env:
+        full_env.update(env)
+    p = subprocess.run([str(c) for c in cmd], env=full_env, cwd=cwd, capture_output=True, text=True)
+    if p.returncode != 0:
+        sys.stderr.write(p.stdout[-4000:] + p.stderr[-4000:])
+        raise SystemExit(f"command failed ({p.returncode}): {' '.join(map(str, cmd))}")
+    return p.stdout
+
+
+def dist_fixture(out: Path) -> None:
+    rng = np.random.default_rng(7)
+    data = {}
+    for dim, m in [(8, 32), (10, 32), (16, 32), (32, 32), (34, 32), (128, 32), (130, 32), (962, 8)]:
+        a = rng.normal(size=(m, dim)).astype(np.float32)
+        b = rng.normal(size=(m, dim)).astype(np.float32)
+        if dim in (128, 130):  # integer-valued rows as in the 1M x 128 mixture
+            a[: m // 2] = np.round(rng.uniform(0, 255, size=(m // 2, dim))).astype(np.float32)
+            b[: m // 2] = np.round(rng.uniform(0, 255, size=(m // 2, dim))).astype(np.float32)
+        with tempfile.TemporaryDirectory() as td:
+            inp = Path(td) / "in.bin"
+            with inp.open("wb") as f:
+                f.write(struct.pack("<II", m, dim))
+                for i in range(m):
+                    a[i].tofile(f)
+                    b[i].tofile(f)
+            run([REFBIN / "ref_harness", "dist", inp, Path(td) / "out.bin"])
+            res = np.fromfile(Path(td) / "out.bin", dtype=np.float32).reshape(m, 4)
+        data[f"a_{dim}"] = a
+        data[f"b_{dim}"] = b
+        data[f"l2_{dim}"] = res[:, 0]
+        data[f"ip_{dim}"] = res[:, 1]
+        data[f"norm_{dim}"] = res[:, 2]
+        data[f"d2_{dim}"] = res[:, 3]
+    np.savez_compressed(out, **data)
+
+
+RESULT_RE = re.compile(
+    r"\[rknn\] L_descent=(\d+)\s*\| recall=([\d.]+) precision=([\d.]+) F1=([\d.]+) \| "
+    r"avg cand=(\d+) pred=(\d+) #dist=(\d+)"
+)
+
+
+def sample_fixture(ref: Path, d: int, out: Path) -> None:
+    work = Path(tempfile.mkdtemp(prefix=f"anqi_golden_d{d}_"))
+    pfx = work / "sample"
+    try:
+        rng = np.random.default_rng(20260819)
+        base = rng.normal(0.0, 1.0, size=(256, d)).astype(np.float32)
+        query = rng.normal(0.0, 1.0, size=(32, d)).astype(np.float32)
+        write_fbin(Path(f"{pfx}_base.bin"), base)
+        write_fbin(Path(f"{pfx}_query.bin"), query)
+        Path(f"{pfx}_lifted.meta").write_text(f"0 {d} 100 l2 1.0\n")
+        one = {"OMP_NUM_THREADS": "1"}
+        # AKNN source: run_sample.sh:16-17 parameters, one thread for a reproducible file.
+        run([REFBIN / "build_aknn_source", f"{pfx}_base.bin", pfx, 100, 64, 8, 64, 1, 10, "l2"], env=one)
+        thr = work / "thr"
+        run([REFBIN / "dataset_gt", "--base", f"{pfx}_base.bin", "--K", 100, "--rk_k", 100, "--threads", 1,
+             "--tile", 64, "--mode", "thresholds", "--out_prefix", thr], env=one)
+        for k in (10, 50, 100):
+            t = work / f"gt{k}"
+            run([REFBIN / "dataset_gt", "--base", f"{pfx}_base.bin", "--query", f"{pfx}_query.bin", "--K", 100,
+                 "--rk_k", k, "--threads", 1, "--tile", 64, "--mode", "ground-truth",
+                 "--threshold-table", f"{thr}_baseknn_gt.bin", "--out_prefix", t], env=one)
+            shutil.copy(f"{t}_rknn_gt.bin", f"{pfx}_rknn_gt_k{k}.bin")
+        run([sys.executable, ref / "tools" / "train_final_m8_u8.py", "--pfx", pfx, "--threshold-source",
+             f"{pfx}_baseknn_aknn.rec"], env=one)
+        # rknn_query with the pinned environment of scripts/run_final.sh:55-95.
+        env = {
+            "OMP_NUM_THREADS": "1", "ANQI_GRAPH_GEOMETRY": "anyk_lift",
+            "ANQI_RADIUS_MODE": "rankm_resid_u8_lrq_floor", "ANQI_VERIFIER_PLACEMENT": "postfilter",
+            "ANQI_RANKM": "8", "ANQI_NK": "100", "ANQI_GRAPH_NK": "100", "ANQI_RANKM_SLACK": "0",
+            "ANQI_RECHECK": "0", "ANQI_RQ_OBJECTIVE": "radius_reconstruction", "ANQI_ALPHA": "1.2",
+            "ANQI_LIFTNNK": "50", "ANQI_GRAPHNND": "6", "ANQI_BUILD_BREAKDOWN": "1",
+            "ANQI_PREBUILT_TOPK_REC": f"{pfx}_baseknn_aknn.rec", "ANQI_PREBUILT_TOPK_K": "100",
+            "ANQI_GRAPH_CACHE_DIR": str(work / "cache" / "graph"),
+            "ANQI_VERIFIER_CACHE_DIR": str(work / "cache" / "verifier"),
+            "ANQI_BENCH_CALIBRATED_TIMING": "0", "ANQI_AKNN_BUILD_SECONDS": "0",
+            "ANQI_VERIFIER_TRAIN_SECONDS": "0",
+        }
+        for key in list(os.environ):
+            if key.startswith("ANQI_") and key not in env:
+                env[key] = ""
+        (work / "cache" / "graph").mkdir(parents=True)
+        (work / "cache" / "verifier").mkdir(parents=True)
+        ref_lines = {}
+        for k in (10, 50, 100):
+            stdout = run([REFBIN / "rknn_query", "16,32,64,128", pfx, 48, 500, 64, 600, k], env=env)
+            for m in RESULT_RE.finditer(stdout):
+                ref_lines[(k, int(m.group(1)))] = [float(m.group(i)) for i in range(2, 8)]
+        lifted_files = sorted((work / "cache" / "graph").glob("_approxlift_graph_*.bin"))
+        meta_files = sorted((work / "cache" / "graph").glob("_anqi_meta_graph_*.txt"))
+        assert len(lifted_files) == 1 and len(meta_files) == 1
+        lifted = read_fbin(lifted_files[0])
+        mstar2, scale = (float(v) for v in meta_files[0].read_text().split())
+
+        h = work / "h"
+        run([REFBIN / "ref_harness", "verifier", pfx, h])
+        run([REFBIN / "ref_harness", "graph", lifted_files[0], f"{pfx}_baseknn_aknn.rec", 50, 48, h])
+        thr_all = np.fromfile(f"{h}_thresholds.bin", dtype=np.float32).reshape(4, 256)
+        query_out = {}
+        meta_path = work / "meta.txt"
+        meta_path.write_text(f"{mstar2!r} {scale!r}\n")
+        for ki, k in enumerate((1, 10, 50, 100)):
+            if k == 1:
+                continue
+            tp = work / f"thr{k}.bin"
+            thr_all[ki].tofile(tp)
+            for L in (16, 32, 64, 128):
+                q = work / f"q{k}_{L}"
+                run([REFBIN / "ref_harness", "query", lifted_files[0], f"{h}_graph.bin", f"{pfx}_base.bin",
+                     f"{pfx}_query.bin", meta_path, tp, L, q])
+                off, ids = read_csr64(Path(f"{q}_cand.bin"))
+                poff, pids = read_csr64(Path(f"{q}_pred.bin"))
+                query_out[f"q_cand_off_{k}_{L}"] = off
+                query_out[f"q_cand_{k}_{L}"] = ids
+                query_out[f"q_pred_off_{k}_{L}"] = poff
+                query_out[f"q_pred_{k}_{L}"] = pids
+                query_out[f"q_ndist_{k}_{L}"] = np.fromfile(f"{q}_ndist.bin", dtype=np.uint32)
+        a = work / "a"
+        run([REFBIN / "ref_harness", "aknn", f"{pfx}_base.bin", a, 100, 64, 8, 64, 10])
+
+        rec = np.fromfile(f"{pfx}_baseknn_aknn.rec", dtype=np.uint32).reshape(256, 100, 2)
+        data = dict(query_out)
+        data["base"] = base
+        data["query"] = query
+        data["rec_ids"] = rec[:, :, 0].copy()
+        data["rec_keys"] = rec[:, :, 1].view(np.float32).copy()
+        for k in (10, 50, 100):
+            raw = Path(f"{pfx}_rknn_gt_k{k}.bin").read_bytes()
+            nq = struct.unpack("<I", raw[:4])[0]
+            off = np.frombuffer(raw[4 : 4 + 4 * (nq + 1)], dtype=np.uint32)
+            tot = int(off[-1])
+            body = raw[4 + 4 * (nq + 1) :]
+            data[f"gt_off_{k}"] = off.copy()
+            data[f"gt_ids_{k}"] = np.frombuffer(body[: 4 * tot], dtype=np.uint32).copy()
+            data[f"gt_keys_{k}"] = np.frombuffer(body[4 * tot :], dtype=np.float32).copy()
+        raw = Path(f"{thr}_baseknn_gt.bin").read_bytes()
+        data["exact_ids"] = np.frombuffer(raw[8 : 8 + 256 * 100 * 4], dtype=np.uint32).reshape(256, 100).copy()
+        data["exact_keys"] = np.frombuffer(raw[8 + 256 * 100 * 4 :], dtype=np.float32).reshape(256, 100).copy()
+        braw = Path(f"{pfx}_radbasis_M8.bin").read_bytes()
+        data["mu"] = np.frombuffer(braw[8 : 8 + 400], dtype=np.float32).copy()
+        data["basis"] = np.frombuffer(braw[408:], dtype=np.float32).reshape(8, 100).copy()
+        craw = Path(f"{pfx}_learned_rq_codebook_M8_u8.bin").read_bytes()
+        data["codebook"] = np.frombuffer(craw[24:], dtype=np.float32).reshape(100, 256).copy()
+        vraw = Path(f"{h}_verifier.bin").read_bytes()
+        data["verifier_bytes"] = np.frombuffer(vraw, dtype=np.uint8).copy()
+        data["coeff"] = np.frombuffer(vraw[36 : 36 + 256 * 8 * 4], dtype=np.float32).reshape(256, 8).copy()
+        data["codes"] = np.frombuffer(vraw[36 + 256 * 8 * 4 :], dtype=np.uint8).reshape(256, 100).copy()
+        data["thresholds"] = thr_all  # k = 1, 10, 50, 100
+        data["lifted"] = lifted
+        data["mstar2"] = np.float64(mstar2)
+        data["scale"] = np.float64(scale)
+        for stage in ("warm", "join"):
+            ids, vals = read_heaps(Path(f"{h}_g0_{stage}.bin"), 256, 50)
+            data[f"g_{stage}_ids"] = ids
+            data[f"g_{stage}_vals"] = vals
+        for name in ("g0_rev", "O", "adj"):
+            off, ids = read_csr64(Path(f"{h}_{name}.bin"))
+            data[f"g_{name}_off"] = off
+            data[f"g_{name}"] = ids
+        data["g_pool_sizes"] = np.fromfile(f"{h}_pool_sizes.bin", dtype=np.uint32)
+        data["graph_file"] = np.frombuffer(Path(f"{h}_graph.bin").read_bytes(), dtype=np.uint8).copy()
+        off, ids = read_csr64(Path(f"{a}_leaves.bin"))
+        data["a_leaf_off"] = off
+        data["a_leaves"] = ids
+        ids, vals = read_heaps(Path(f"{a}_g0_init.bin"), 256, 100)
+        data["a_init_ids"] = ids
+        data["a_init_vals"] = vals
+        off, ids = read_csr64(Path(f"{a}_g0_rev.bin"))
+        data["a_rev_off"] = off
+        data["a_rev"] = ids
+        fin = np.fromfile(f"{a}_final.bin", dtype=np.uint32)
+        data["a_final_ids"] = fin[: 256 * 100].reshape(256, 100).copy()
+        data["a_final_d"] = fin[256 * 100 :].view(np.float32).reshape(256, 100).copy()
+        data["a_pool_sizes"] = np.fromfile(f"{a}_pool_sizes.bin", dtype=np.uint32)
+        keys = sorted(ref_lines)
+        data["ref_lines_k_L"] = np.array(keys, dtype=np.int32)
+        data["ref_lines"] = np.array([ref_lines[x] for x in keys], dtype=np.float64)
+        np.savez_compressed(out, **data)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", type=Path, default=Path("/root/reference"))
+    args = ap.parse_args()
+    if not (REFBIN / "ref_harness").exists():
+        raise SystemExit("build the reference first: make -C oracle ref")
+    dist_fixture(HERE / "dist.npz")
+    sample_fixture(args.ref, 8, HERE / "sample_d8.npz")
+    sample_fixture(args.ref, 32, HERE / "sample_d32.npz")
+    for p in sorted(HERE.glob("*.npz")):
+        print(f"{p.name}: {p.stat().st_size} bytes")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
