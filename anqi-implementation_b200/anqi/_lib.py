@@ -1,0 +1,365 @@
+"""ctypes bindings of libanqi.so (include/anqi.h).
+
+The shared library is the product: every call here goes to CUDA kernels built
+for sm_100a.  There is no CPU fallback -- if the library or a GPU is missing,
+``Context()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent.parent
+LIB_PATH = Path(os.environ.get("ANQI_LIBRARY", PKG / "lib" / "libanqi.so"))
+EMPTY = 0xFFFFFFFF
+
+ANQI_OK = 0
+ANQI_ERR_ARGS = 2
+ANQI_ERR_FORMAT = 3
+ANQI_ERR_INVARIANT = 5
+ANQI_ERR_DEVICE = 7
+ANQI_ERR_TIMEOUT = 8
+ANQI_ERR_CAPACITY = 9
+
+
+class AnqiError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[anqi status {status}] {msg}")
+        self.status = status
+
+
+_f32 = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64 = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_u32 = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_u64 = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+_u8 = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+
+
+class IndexDesc(C.Structure):
+    _fields_ = [
+        ("n", C.c_uint64), ("d", C.c_uint32), ("degree", C.c_uint32), ("base", _vp), ("lifted", _vp),
+        ("deg", _vp), ("links", _vp), ("tree_nodes", C.c_uint32), ("tree_left", _vp), ("tree_right", _vp),
+        ("tree_offset", _vp), ("tree_hyperplane", _vp), ("tree_leaf_first", _vp), ("scale", C.c_double),
+        ("mstar2", C.c_double),
+    ]
+
+
+class QueryStats(C.Structure):
+    _fields_ = [
+        ("n_dist", C.c_uint64), ("n_expand", C.c_uint64), ("n_cand", C.c_uint64), ("n_pred", C.c_uint64),
+        ("n_flood", C.c_uint64), ("search_ms", C.c_float), ("total_ms", C.c_float), ("h2d_bytes", C.c_uint64),
+        ("d2h_bytes", C.c_uint64),
+    ]
+
+
+class AknnParams(C.Structure):
+    _fields_ = [("k", C.c_uint32), ("leaf", C.c_uint32), ("trees", C.c_uint32), ("ef", C.c_uint32),
+                ("ef_alpha", C.c_uint32), ("seed", C.c_uint64), ("nn_iters", C.c_uint32), ("nn_sample", C.c_uint32)]
+
+
+class GraphParams(C.Structure):
+    _fields_ = [("degree", C.c_uint32), ("nn_k", C.c_uint32), ("explore", C.c_uint32), ("ef_alpha", C.c_uint32),
+                ("join_iters", C.c_uint32), ("join_sample", C.c_uint32), ("leaf", C.c_uint32),
+                ("max_depth", C.c_uint32), ("seed", C.c_uint64), ("alpha", C.c_float), ("warm_width", C.c_uint32)]
+
+
+class BuildStats(C.Structure):
+    _fields_ = [("total_ms", C.c_double), ("forest_ms", C.c_double), ("init_ms", C.c_double),
+                ("join_ms", C.c_double), ("reverse_ms", C.c_double), ("gather_ms", C.c_double),
+                ("join_updates", C.c_uint64), ("pool_total", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_SIGS = {
+    "anqi_ctx_create": [C.c_int, C.POINTER(_vp)],
+    "anqi_ctx_destroy": [_vp],
+    "anqi_last_error": [_vp],
+    "anqi_version": [],
+    "anqi_device_bytes": [_vp],
+    "anqi_pair_distances": [_vp, _f32, _f32, C.c_uint64, C.c_uint32, _f32, _f32],
+    "anqi_lrq_encode": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _f32, C.c_uint32, _f32, _u8],
+    "anqi_lrq_materialize": [_vp, _f32, _u8, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _f32, C.c_uint32,
+                             C.c_uint32, C.c_double, _f32],
+    "anqi_lift": [_vp, _f32, C.c_uint64, C.c_uint32, _f32, _f32, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+    "anqi_rp_forest": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                       C.c_uint32, _u32, _u32, _u32, _f32, _f32, _u32, _u32, _u32],
+    "anqi_aknn_build": [_vp, _f32, C.c_uint64, C.c_uint32, C.POINTER(AknnParams), _u32, _f32,
+                        C.POINTER(BuildStats)],
+    "anqi_aknn_init": [_vp, _f32, C.c_uint64, C.c_uint32, _u64, _u32, C.c_uint64, C.c_uint32, _u32, _f32],
+    "anqi_aknn_gather": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _f32, C.c_uint32, C.c_uint32, C.c_uint32,
+                         C.c_uint32, _u32, _f32],
+    "anqi_graph_build": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, C.c_uint32, C.POINTER(GraphParams), _u32, _u32,
+                         C.POINTER(BuildStats)],
+    "anqi_graph_tree_size": [_vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)],
+    "anqi_graph_tree_copy": [_vp, _u32, _u32, _f32, _f32, _u32, _u32, _u32],
+    "anqi_graph_warm_start": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, C.c_uint32, C.c_uint32, C.c_uint32, _u32,
+                              _f32],
+    "anqi_graph_localjoin": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _u32, _f32,
+                             _u64, C.POINTER(C.c_uint32)],
+    "anqi_graph_select": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _f32, C.c_uint32, C.c_uint32, C.c_uint32,
+                          C.c_uint32, C.c_float, _u32, _u32],
+    "anqi_graph_commit": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _u32, C.c_uint32, C.c_float, _u32, _u32],
+    "anqi_index_load": [_vp, C.POINTER(IndexDesc)],
+    "anqi_verifier_load": [_vp, _f32, _u8, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _f32, C.c_uint32],
+    "anqi_verifier_materialize": [_vp, C.c_uint32, C.c_double],
+    "anqi_set_thresholds": [_vp, C.c_uint32, _f32],
+    "anqi_rknn_query": [_vp, _f32, C.c_uint32, _vp, C.c_uint32, _vp, C.c_uint32, _u32, _u32, C.c_uint64, _vp, _vp,
+                        C.c_uint64, _vp, C.POINTER(QueryStats)],
+    "anqi_query_upload": [_vp, _f32, C.c_uint32, _vp, C.c_uint32, _vp, C.c_uint32],
+    "anqi_query_run": [_vp, C.c_int, C.POINTER(QueryStats)],
+    "anqi_query_download": [_vp, _u32, _vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp],
+    "anqi_query_evaluate": [_vp, _u32, _u32, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                            C.POINTER(C.c_double), C.POINTER(C.c_uint32)],
+    "anqi_exact_topk": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _u32, _f32],
+    "anqi_rknn_ground_truth": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32, _u32, _u32, _f32,
+                               C.c_uint64, C.POINTER(C.c_uint64)],
+}
+
+#: every symbol include/anqi.h declares (checked by the CPU tests)
+EXPORTED = tuple(_SIGS)
+
+_lib = None
+
+
+def load_library() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise AnqiError(ANQI_ERR_DEVICE, f"libanqi.so not built ({LIB_PATH}); run anqi-implementation_b200/build.py")
+    lib = C.CDLL(str(LIB_PATH))
+    missing = [name for name in _SIGS if not hasattr(lib, name)]
+    if missing:
+        raise AnqiError(ANQI_ERR_DEVICE, f"{LIB_PATH} lacks exported symbols: {missing}")
+    for name, args in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    lib.anqi_ctx_destroy.restype = None
+    lib.anqi_last_error.restype = C.c_char_p
+    lib.anqi_device_bytes.restype = C.c_uint64
+    _lib = lib
+    return lib
+
+
+def _c(a, dtype) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class QueryResult:
+    pred_off: np.ndarray
+    pred_ids: np.ndarray
+    cand_off: np.ndarray | None
+    cand_ids: np.ndarray | None
+    n_dist: np.ndarray | None
+    stats: dict
+
+    def pred(self, i: int) -> np.ndarray:
+        return self.pred_ids[self.pred_off[i]:self.pred_off[i + 1]]
+
+    def cand(self, i: int) -> np.ndarray:
+        return self.cand_ids[self.cand_off[i]:self.cand_off[i + 1]]
+
+
+class Context:
+    """One CUDA context: device memory, one stream, an optional resident index."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        rc = self.lib.anqi_ctx_create(device, C.byref(h))
+        if rc != ANQI_OK:
+            raise AnqiError(rc, f"cannot create a context on CUDA device {device}")
+        self.h = h
+        self._keep = []
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.anqi_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != ANQI_OK:
+            msg = self.lib.anqi_last_error(self.h)
+            raise AnqiError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self.lib.anqi_device_bytes(self.h))
+
+    # ------------------------------------------------------------ kernels
+
+    def pair_distances(self, a, b):
+        a = _c(a, np.float32)
+        b = _c(b, np.float32)
+        m, dim = a.shape
+        l2 = np.empty(m, np.float32)
+        ip = np.empty(m, np.float32)
+        self._check(self.lib.anqi_pair_distances(self.h, a, b, m, dim, l2, ip), "pair_distances")
+        return l2, ip
+
+    def lrq_encode(self, keys, mu, basis, codebook):
+        keys = _c(keys, np.float32)
+        n, nk = keys.shape
+        rankm = basis.shape[0]
+        coeff = np.empty((n, rankm), np.float32)
+        codes = np.empty((n, nk), np.uint8)
+        self._check(self.lib.anqi_lrq_encode(self.h, keys, n, nk, rankm, _c(mu, np.float32), _c(basis, np.float32),
+                                             _c(codebook, np.float32), codebook.shape[1], coeff, codes), "lrq_encode")
+        return coeff, codes
+
+    def lrq_materialize(self, coeff, codes, mu, basis, codebook, k, radius_scale=1.0):
+        codes = _c(codes, np.uint8)
+        n, nk = codes.shape
+        thr = np.empty(n, np.float32)
+        self._check(self.lib.anqi_lrq_materialize(self.h, _c(coeff, np.float32), codes, n, nk, basis.shape[0],
+                                                  _c(mu, np.float32), _c(basis, np.float32),
+                                                  _c(codebook, np.float32), codebook.shape[1], k, radius_scale, thr),
+                    "lrq_materialize")
+        return thr
+
+    def lift(self, base, radius):
+        base = _c(base, np.float32)
+        n, d = base.shape
+        out = np.empty((n, d + 2), np.float32)
+        m2, sc = C.c_double(), C.c_double()
+        self._check(self.lib.anqi_lift(self.h, base, n, d, _c(radius, np.float32), out, C.byref(m2), C.byref(sc)),
+                    "lift")
+        return out, m2.value, sc.value
+
+    # ------------------------------------------------------------- index
+
+    def index_load(self, base, lifted, deg, links, tree, scale: float, mstar2: float) -> None:
+        """tree: post-order arrays with attributes left/right/offset/hyperplane and leaf_first()."""
+        base = _c(base, np.float32)
+        lifted = _c(lifted, np.float32)
+        deg = _c(deg, np.uint32)
+        links = _c(links, np.uint32)
+        tl = _c(tree.left, np.uint32)
+        tr = _c(tree.right, np.uint32)
+        to = _c(tree.offset, np.float32)
+        th = _c(tree.hyperplane, np.float32)
+        tf = _c(tree.leaf_first(), np.uint32)
+        n, d = base.shape
+        desc = IndexDesc(n, d, links.shape[1], _ptr(base), _ptr(lifted), _ptr(deg), _ptr(links), len(tl), _ptr(tl),
+                         _ptr(tr), _ptr(to), _ptr(th), _ptr(tf), float(scale), float(mstar2))
+        self._check(self.lib.anqi_index_load(self.h, C.byref(desc)), "index_load")
+        self.n = n
+        self.d = d
+
+    def verifier_load(self, coeff, codes, mu, basis, codebook) -> None:
+        codes = _c(codes, np.uint8)
+        n, nk = codes.shape
+        self._check(self.lib.anqi_verifier_load(self.h, _c(coeff, np.float32), codes, n, nk, basis.shape[0],
+                                                _c(mu, np.float32), _c(basis, np.float32), _c(codebook, np.float32),
+                                                codebook.shape[1]), "verifier_load")
+
+    def verifier_materialize(self, k: int, radius_scale: float = 1.0) -> None:
+        self._check(self.lib.anqi_verifier_materialize(self.h, k, radius_scale), "verifier_materialize")
+
+    def set_thresholds(self, k: int, thr) -> None:
+        self._check(self.lib.anqi_set_thresholds(self.h, k, _c(thr, np.float32)), "set_thresholds")
+
+    # ----------------------------------------------------------- queries
+
+    @staticmethod
+    def _per_query(v, nq):
+        if v is None or np.isscalar(v):
+            return None, int(v or 0)
+        a = _c(v, np.uint32)
+        assert a.shape == (nq,)
+        return a, 0
+
+    def rknn_query(self, queries, k, L, keep_candidates=False, pred_cap=None) -> QueryResult:
+        """Host-buffer end-to-end call (queries H2D, results D2H inside)."""
+        queries = _c(queries, np.float32)
+        nq = queries.shape[0]
+        ka, kall = self._per_query(k, nq)
+        La, Lall = self._per_query(L, nq)
+        st = QueryStats()
+        cap = pred_cap or max(1024, nq * 256)
+        while True:
+            pred_off = np.empty(nq + 1, np.uint32)
+            pred_ids = np.empty(cap, np.uint32)
+            cand_off = np.empty(nq + 1, np.uint32) if keep_candidates else None
+            ccap = cap * 4 if keep_candidates else 0
+            cand_ids = np.empty(ccap, np.uint32) if keep_candidates else None
+            nd = np.empty(nq, np.uint32)
+            rc = self.lib.anqi_rknn_query(self.h, queries, nq, _ptr(ka), kall, _ptr(La), Lall, pred_off, pred_ids, cap,
+                                          _ptr(cand_off), _ptr(cand_ids), ccap, _ptr(nd), C.byref(st))
+            if rc == ANQI_ERR_CAPACITY:
+                cap *= 4
+                continue
+            self._check(rc, "rknn_query")
+            break
+        stats = {k2: getattr(st, k2) for k2, _ in QueryStats._fields_}
+        return QueryResult(pred_off, pred_ids[:pred_off[-1]].copy(), cand_off,
+                           None if cand_ids is None else cand_ids[:cand_off[-1]].copy(), nd, stats)
+
+    def query_upload(self, queries, k, L) -> None:
+        queries = _c(queries, np.float32)
+        nq = queries.shape[0]
+        ka, kall = self._per_query(k, nq)
+        La, Lall = self._per_query(L, nq)
+        self._keep = [ka, La]
+        self.nq = nq
+        self._check(self.lib.anqi_query_upload(self.h, queries, nq, _ptr(ka), kall, _ptr(La), Lall), "query_upload")
+
+    def query_run(self, keep_candidates=False) -> dict:
+        st = QueryStats()
+        self._check(self.lib.anqi_query_run(self.h, int(keep_candidates), C.byref(st)), "query_run")
+        return {k2: getattr(st, k2) for k2, _ in QueryStats._fields_}
+
+    def query_download(self, with_candidates=False) -> QueryResult:
+        nq = self.nq
+        pred_off = np.empty(nq + 1, np.uint32)
+        self._check(self.lib.anqi_query_download(self.h, pred_off, None, 0, None, None, 0, None), "query_download")
+        pred_ids = np.empty(max(1, int(pred_off[-1])), np.uint32)
+        cand_off = np.empty(nq + 1, np.uint32) if with_candidates else None
+        nd = np.empty(nq, np.uint32)
+        if with_candidates:
+            self._check(self.lib.anqi_query_download(self.h, pred_off, _ptr(pred_ids), len(pred_ids),
+                                                     _ptr(cand_off), None, 0, None), "query_download")
+            cand_ids = np.empty(max(1, int(cand_off[-1])), np.uint32)
+        else:
+            cand_ids = None
+        self._check(self.lib.anqi_query_download(self.h, pred_off, _ptr(pred_ids), len(pred_ids), _ptr(cand_off),
+                                                 _ptr(cand_ids), 0 if cand_ids is None else len(cand_ids),
+                                                 _ptr(nd)), "query_download")
+        return QueryResult(pred_off, pred_ids[:pred_off[-1]], cand_off,
+                           None if cand_ids is None else cand_ids[:cand_off[-1]], nd, {})
+
+    def query_evaluate(self, gt_off, gt_ids) -> dict:
+        gt_off = _c(gt_off, np.uint32)
+        gt_ids = _c(gt_ids, np.uint32) if len(gt_ids) else np.zeros(1, np.uint32)
+        r, p, cr = C.c_double(), C.c_double(), C.c_double()
+        ne = C.c_uint32()
+        self._check(self.lib.anqi_query_evaluate(self.h, gt_off, gt_ids, int(gt_off[-1]), C.byref(r), C.byref(p),
+                                                 C.byref(cr), C.byref(ne)), "query_evaluate")
+        d = max(1, ne.value)
+        return {"recall": r.value / d, "precision": p.value / d, "candidate_recall": cr.value / d,
+                "nonempty": ne.value}

@@ -1,0 +1,224 @@
+// Shared device building blocks for the ANQI RkNN kernels (sm_100a).
+//
+// Bit-exact FP32 distances.  The reference computes every distance with
+// AVX-512 intrinsics (include/distance.h:22-161): 16 lane accumulators, lane l
+// accumulating elements j = l (mod 16) with a fused multiply-add in increasing
+// j; the 16 lanes are folded by _mm512_reduce_add_ps (upper 256 bits onto the
+// lower, upper 128 onto the lower, lanes {2,3} onto {0,1}, lane 1 onto lane 0);
+// a masked tail (dim mod 16 elements) is multiplied without FMA, folded by the
+// same tree and added last.  Here a group of four consecutive threads owns one
+// vector pair: thread t of the group holds AVX lanes 4t..4t+3, loaded as one
+// float4 per 16-element chunk, so rows are read with 16-byte coalesced loads.
+// Every operation uses the _rn intrinsics so nvcc cannot contract or reorder.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace anqi {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr uint32_t kExpanded = 0x80000000u;
+constexpr uint32_t kIdMask = 0x7FFFFFFFu;
+constexpr float kSplitEps = 1e-6f;  // distance.h:14
+
+// Device-side error word codes (first error wins; the host maps them to status codes).
+enum DeviceError : uint32_t {
+    kDevOk = 0,
+    kDevCandOverflow = 1,   // per-query candidate list capacity
+    kDevOutOverflow = 2,    // batch output buffer capacity
+    kDevPoolOverflow = 3,   // gather pool capacity
+    kDevBadId = 4,          // an id read from a graph or list is out of range
+    kDevWaitTimeout = 5,    // a bounded wait ran out
+    kDevSortOverflow = 6,
+};
+
+__device__ __forceinline__ void set_error(uint32_t* err, uint32_t code) {
+    if (err) atomicCAS(err, 0u, code);
+}
+
+// ------------------------------------------------------------ AVX order
+
+// _mm512_reduce_add_ps on a 16-lane value spread over a 4-thread group: thread
+// t holds lanes a[0..3] = A[4t..4t+3].  The result is valid in all 4 threads.
+__device__ __forceinline__ float group_reduce16(float a0, float a1, float a2, float a3, unsigned mask) {
+    // T3[i] = A[i+8] + A[i]: threads 0,1 take the lanes of threads 2,3.
+    float u0 = __shfl_down_sync(mask, a0, 2, 4);
+    float u1 = __shfl_down_sync(mask, a1, 2, 4);
+    float u2 = __shfl_down_sync(mask, a2, 2, 4);
+    float u3 = __shfl_down_sync(mask, a3, 2, 4);
+    float t0 = __fadd_rn(u0, a0), t1 = __fadd_rn(u1, a1), t2 = __fadd_rn(u2, a2), t3 = __fadd_rn(u3, a3);
+    // T6[j] = T3[j+4] + T3[j]: thread 0 takes thread 1's T3[4..7].
+    float v0 = __shfl_down_sync(mask, t0, 1, 4);
+    float v1 = __shfl_down_sync(mask, t1, 1, 4);
+    float v2 = __shfl_down_sync(mask, t2, 1, 4);
+    float v3 = __shfl_down_sync(mask, t3, 1, 4);
+    float s0 = __fadd_rn(v0, t0), s1 = __fadd_rn(v1, t1), s2 = __fadd_rn(v2, t2), s3 = __fadd_rn(v3, t3);
+    // T8 = T6 + shuffle(T6, {2,3,0,1}); result = T8[0] + T8[1]
+    float r = __fadd_rn(__fadd_rn(s0, s2), __fadd_rn(s1, s3));
+    return __shfl_sync(mask, r, 0, 4);
+}
+
+// Squared L2 (distance.h:58-86).  a, b: 16-byte aligned rows whose allocation
+// extends to a multiple of 4 floats past dim.  gt = thread index in the group.
+__device__ __forceinline__ float group_l2sqr(const float* __restrict__ a, const float* __restrict__ b,
+                                             uint32_t dim, uint32_t gt, unsigned mask) {
+    const uint32_t q16 = dim >> 4, rem = dim & 15u;
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+#pragma unroll 4
+    for (uint32_t c = 0; c < q16; c++) {
+        float4 x = *reinterpret_cast<const float4*>(a + 16 * c + 4 * gt);
+        float4 y = *reinterpret_cast<const float4*>(b + 16 * c + 4 * gt);
+        float d0 = __fsub_rn(x.x, y.x), d1 = __fsub_rn(x.y, y.y), d2 = __fsub_rn(x.z, y.z), d3 = __fsub_rn(x.w, y.w);
+        c0 = __fmaf_rn(d0, d0, c0);
+        c1 = __fmaf_rn(d1, d1, c1);
+        c2 = __fmaf_rn(d2, d2, c2);
+        c3 = __fmaf_rn(d3, d3, c3);
+    }
+    float res = group_reduce16(c0, c1, c2, c3, mask);
+    if (rem) {
+        float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+        const uint32_t base = 16 * q16 + 4 * gt;
+        if (4 * gt < rem) {
+            float4 x = *reinterpret_cast<const float4*>(a + base);
+            float4 y = *reinterpret_cast<const float4*>(b + base);
+            float d0 = __fsub_rn(x.x, y.x), d1 = __fsub_rn(x.y, y.y), d2 = __fsub_rn(x.z, y.z), d3 = __fsub_rn(x.w, y.w);
+            p0 = __fmul_rn(d0, d0);
+            p1 = (4 * gt + 1 < rem) ? __fmul_rn(d1, d1) : 0.f;
+            p2 = (4 * gt + 2 < rem) ? __fmul_rn(d2, d2) : 0.f;
+            p3 = (4 * gt + 3 < rem) ? __fmul_rn(d3, d3) : 0.f;
+        }
+        res = __fadd_rn(res, group_reduce16(p0, p1, p2, p3, mask));
+    }
+    return res;
+}
+
+// Inner product (distance.h:89-116; NormSIMD16ExtAVX512__ is ip(a, a)).
+__device__ __forceinline__ float group_ip(const float* __restrict__ a, const float* __restrict__ b,
+                                          uint32_t dim, uint32_t gt, unsigned mask) {
+    const uint32_t q16 = dim >> 4, rem = dim & 15u;
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+#pragma unroll 4
+    for (uint32_t c = 0; c < q16; c++) {
+        float4 x = *reinterpret_cast<const float4*>(a + 16 * c + 4 * gt);
+        float4 y = *reinterpret_cast<const float4*>(b + 16 * c + 4 * gt);
+        c0 = __fmaf_rn(x.x, y.x, c0);
+        c1 = __fmaf_rn(x.y, y.y, c1);
+        c2 = __fmaf_rn(x.z, y.z, c2);
+        c3 = __fmaf_rn(x.w, y.w, c3);
+    }
+    float res = group_reduce16(c0, c1, c2, c3, mask);
+    if (rem) {
+        float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+        const uint32_t base = 16 * q16 + 4 * gt;
+        if (4 * gt < rem) {
+            float4 x = *reinterpret_cast<const float4*>(a + base);
+            float4 y = *reinterpret_cast<const float4*>(b + base);
+            p0 = __fmul_rn(x.x, y.x);
+            p1 = (4 * gt + 1 < rem) ? __fmul_rn(x.y, y.y) : 0.f;
+            p2 = (4 * gt + 2 < rem) ? __fmul_rn(x.z, y.z) : 0.f;
+            p3 = (4 * gt + 3 < rem) ? __fmul_rn(x.w, y.w) : 0.f;
+        }
+        res = __fadd_rn(res, group_reduce16(p0, p1, p2, p3, mask));
+    }
+    return res;
+}
+
+// nndindex::d2 (index.h:172-176): (na + nb) - 2 * ip(a, b)
+__device__ __forceinline__ float norm_d2(float na, float nb, float ip) {
+    return __fsub_rn(__fadd_rn(na, nb), __fmul_rn(2.0f, ip));
+}
+
+// --------------------------------------------------------- ordering
+
+// (dist, id) total order of neighbor.h:22-24 (id without the expanded bit).
+__device__ __forceinline__ bool nb_less(float da, uint32_t ia, float db, uint32_t ib) {
+    return da < db || (da == db && (ia & kIdMask) < (ib & kIdMask));
+}
+
+// Plain (key, id) lexicographic order on full 32-bit ids (std::pair order).
+__device__ __forceinline__ bool kv_less(float da, uint32_t ia, float db, uint32_t ib) {
+    return da < db || (da == db && ia < ib);
+}
+
+// Bitonic sort of 64 (d, id) pairs held two per lane (index lane and lane+32),
+// ascending in nb_less order.  Pads must be (+inf, kEmpty).
+__device__ __forceinline__ void warp_sort64(float& d0, uint32_t& i0, float& d1, uint32_t& i1) {
+    const uint32_t lane = threadIdx.x & 31u;
+    // element e = lane (slot 0) and e = lane + 32 (slot 1)
+#pragma unroll
+    for (uint32_t k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j == 32) {
+                // partner of slot 0 is slot 1 of the same lane
+                bool up = ((lane & k) == 0);  // k == 64 here -> always ascending
+                bool sw = up ? nb_less(d1, i1, d0, i0) : nb_less(d0, i0, d1, i1);
+                if (sw) {
+                    float td = d0; d0 = d1; d1 = td;
+                    uint32_t ti = i0; i0 = i1; i1 = ti;
+                }
+            } else {
+#pragma unroll
+                for (int s = 0; s < 2; s++) {
+                    float& d = s ? d1 : d0;
+                    uint32_t& id = s ? i1 : i0;
+                    const uint32_t e = lane + 32u * s;
+                    float od = __shfl_xor_sync(0xFFFFFFFFu, d, j);
+                    uint32_t oi = __shfl_xor_sync(0xFFFFFFFFu, id, j);
+                    const bool lower = (e & j) == 0;
+                    const bool up = (e & k) == 0;
+                    // keep the smaller if (lower == up)
+                    bool other_less = nb_less(od, oi, d, id);
+                    bool take = (lower == up) ? other_less : !other_less;
+                    // ties cannot occur between distinct entries (total order)
+                    if (take) {
+                        d = od;
+                        id = oi;
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Number of entries in sorted a[0..n) strictly less than (d, id).
+__device__ __forceinline__ uint32_t lower_rank(const float* ad, const uint32_t* ai, uint32_t n, float d, uint32_t id) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (nb_less(ad[mid], ai[mid], d, id)) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// ----------------------------------------------------- visited bitmap
+
+// A per-slot bitmap over all n objects plus a log of set bits, so the slot can
+// be cleared in O(visited) at the end of a query/row (or wholesale on overflow).
+struct VisitSlot {
+    uint32_t* bits;      // ceil(n/32) words
+    uint32_t* log;       // log_cap entries
+    uint32_t log_cap;
+    uint32_t words;
+};
+
+// Returns true when id was not yet visited (and marks it).
+__device__ __forceinline__ bool visit_first(uint32_t* bits, uint32_t id) {
+    const uint32_t m = 1u << (id & 31u);
+    return (atomicOr(bits + (id >> 5), m) & m) == 0u;
+}
+
+// Warp-cooperative clear at the end of a query: either replay the log or wipe.
+__device__ __forceinline__ void visit_clear(const VisitSlot& s, uint32_t logged) {
+    const uint32_t lane = threadIdx.x & 31u;
+    if (logged <= s.log_cap) {
+        for (uint32_t i = lane; i < logged; i += 32) s.bits[s.log[i] >> 5] = 0u;
+    } else {
+        for (uint32_t w = lane; w < s.words; w += 32) s.bits[w] = 0u;
+    }
+    __syncwarp();
+}
+
+}  // namespace anqi

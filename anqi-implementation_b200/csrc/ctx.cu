@@ -1,0 +1,236 @@
+// Context lifetime, device memory, error reporting, and small shared kernels.
+#include <cstdarg>
+#include <cstdio>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace anqi {
+
+int fail(Ctx* c, int status, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->last_error = buf;
+    return status;
+}
+
+int cuda_check(Ctx* c, cudaError_t e, const char* what) {
+    return fail(c, ANQI_ERR_DEVICE, "CUDA error in %s: %s", what, cudaGetErrorString(e));
+}
+
+int ensure(Ctx* c, DevBuf& b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.bytes >= bytes) return ANQI_OK;
+    if (b.p) {
+        cudaFree(b.p);
+        c->device_bytes -= b.bytes;
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return fail(c, ANQI_ERR_DEVICE, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    b.bytes = bytes;
+    c->device_bytes += bytes;
+    return ANQI_OK;
+}
+
+void release(Ctx* c, DevBuf& b) {
+    if (b.p) {
+        cudaFree(b.p);
+        c->device_bytes -= b.bytes;
+    }
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+int h2d(Ctx* c, DevBuf& b, const void* src, size_t bytes) {
+    int rc = ensure(c, b, bytes);
+    if (rc) return rc;
+    if (bytes) ANQI_CUDA(c, cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    return ANQI_OK;
+}
+
+int d2h(Ctx* c, void* dst, const DevBuf& b, size_t bytes) {
+    if (bytes) ANQI_CUDA(c, cudaMemcpyAsync(dst, b.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return ANQI_OK;
+}
+
+int sync(Ctx* c) {
+    ANQI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ANQI_OK;
+}
+
+int check_device_error(Ctx* c, const char* stage) {
+    uint32_t e = 0;
+    ANQI_CUDA(c, cudaMemcpyAsync(&e, c->err.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    ANQI_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (e == kDevOk) return ANQI_OK;
+    ANQI_CUDA(c, cudaMemsetAsync(c->err.p, 0, 4, c->stream));
+    switch (e) {
+        case kDevCandOverflow: return fail(c, ANQI_ERR_CAPACITY, "%s: per-query candidate capacity exceeded", stage);
+        case kDevOutOverflow: return fail(c, ANQI_ERR_CAPACITY, "%s: output capacity exceeded", stage);
+        case kDevPoolOverflow: return fail(c, ANQI_ERR_CAPACITY, "%s: gather pool capacity exceeded", stage);
+        case kDevSortOverflow: return fail(c, ANQI_ERR_CAPACITY, "%s: sort capacity exceeded", stage);
+        case kDevBadId: return fail(c, ANQI_ERR_FORMAT, "%s: an id out of range was read", stage);
+        case kDevWaitTimeout: return fail(c, ANQI_ERR_TIMEOUT, "%s: a bounded device wait timed out", stage);
+        default: return fail(c, ANQI_ERR_DEVICE, "%s: device error word %u", stage, e);
+    }
+}
+
+__global__ void pad_rows_kernel(const float* __restrict__ src, float* __restrict__ dst, uint64_t n, uint32_t d,
+                                uint32_t stride) {
+    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t total = n * stride;
+    for (; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t r = t / stride;
+        uint32_t j = (uint32_t)(t % stride);
+        dst[t] = j < d ? src[r * d + j] : 0.0f;
+    }
+}
+
+int upload_padded(Ctx* c, DevBuf& b, const float* src, uint64_t n, uint32_t d, uint32_t stride) {
+    int rc = ensure(c, b, (size_t)n * stride * 4 + 64);
+    if (rc) return rc;
+    if (stride == d) {
+        ANQI_CUDA(c, cudaMemcpyAsync(b.p, src, (size_t)n * d * 4, cudaMemcpyHostToDevice, c->stream));
+        return ANQI_OK;
+    }
+    TmpBuf tmp(c);
+    rc = ensure(c, tmp, (size_t)n * d * 4);
+    if (rc) return rc;
+    ANQI_CUDA(c, cudaMemcpyAsync(tmp.p, src, (size_t)n * d * 4, cudaMemcpyHostToDevice, c->stream));
+    pad_rows_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(tmp.as<float>(), b.as<float>(), n, d, stride);
+    ANQI_CUDA(c, cudaGetLastError());
+    ANQI_CUDA(c, cudaStreamSynchronize(c->stream));
+    return ANQI_OK;
+}
+
+// IP(x, x) per row in the AVX lane order (NormSIMD16ExtAVX512__ / the
+// verifier's IP(o, o)); one 4-thread group per row.
+__global__ void norms_kernel(const float* __restrict__ x, uint64_t n, uint32_t dim, uint32_t stride,
+                             float* __restrict__ out) {
+    const uint32_t lane = threadIdx.x & 31u, gt = lane & 3u, gw = lane >> 2;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t base = warp * 8; base < n; base += nwarps * 8) {
+        const uint64_t row = base + gw;
+        const bool ok = row < n;
+        const float* r = x + (ok ? row : base) * stride;
+        float v = group_ip(r, r, dim, gt, 0xFFFFFFFFu);
+        if (ok && gt == 0) out[row] = v;
+    }
+}
+
+int compute_norms_device(Ctx* c, const float* d_x, uint64_t n, uint32_t dim, uint32_t stride, float* d_out) {
+    const int threads = 256;
+    uint64_t groups = n;
+    int blocks = (int)std::min<uint64_t>((groups * 4 + threads - 1) / threads, (uint64_t)c->sm_count * 16);
+    if (blocks < 1) blocks = 1;
+    norms_kernel<<<blocks, threads, 0, c->stream>>>(d_x, n, dim, stride, d_out);
+    ANQI_CUDA(c, cudaGetLastError());
+    return ANQI_OK;
+}
+
+__global__ void pair_dist_kernel(const float* __restrict__ a, const float* __restrict__ b, uint64_t m,
+                                 uint32_t dim, uint32_t stride, float* __restrict__ l2, float* __restrict__ ip) {
+    const uint32_t lane = threadIdx.x & 31u, gt = lane & 3u, gw = lane >> 2;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t base = warp * 8; base < m; base += nwarps * 8) {
+        const uint64_t row = base + gw;
+        const bool ok = row < m;
+        const uint64_t r = ok ? row : base;
+        float v1 = group_l2sqr(a + r * stride, b + r * stride, dim, gt, 0xFFFFFFFFu);
+        float v2 = group_ip(a + r * stride, b + r * stride, dim, gt, 0xFFFFFFFFu);
+        if (ok && gt == 0) {
+            l2[row] = v1;
+            ip[row] = v2;
+        }
+    }
+}
+
+}  // namespace anqi
+
+using namespace anqi;
+
+extern "C" {
+
+int anqi_version(void) { return 1; }
+
+int anqi_ctx_create(int device, anqi_ctx** out) {
+    if (!out) return ANQI_ERR_ARGS;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return ANQI_ERR_DEVICE;
+    if (device < 0 || device >= count) return ANQI_ERR_ARGS;
+    if (cudaSetDevice(device) != cudaSuccess) return ANQI_ERR_DEVICE;
+    anqi_ctx* h = new anqi_ctx();
+    Ctx* c = &h->c;
+    c->device = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        delete h;
+        return ANQI_ERR_DEVICE;
+    }
+    c->sm_count = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaEventCreate(&c->ev2) != cudaSuccess || cudaEventCreate(&c->ev3) != cudaSuccess) {
+        delete h;
+        return ANQI_ERR_DEVICE;
+    }
+    if (ensure(c, c->err, 64) || ensure(c, c->counters, 4096)) {
+        delete h;
+        return ANQI_ERR_DEVICE;
+    }
+    cudaMemsetAsync(c->err.p, 0, 64, c->stream);
+    cudaStreamSynchronize(c->stream);
+    *out = h;
+    return ANQI_OK;
+}
+
+void anqi_ctx_destroy(anqi_ctx* h) {
+    if (!h) return;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (DevBuf* b : c->member_bufs()) release(c, *b);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->ev2) cudaEventDestroy(c->ev2);
+    if (c->ev3) cudaEventDestroy(c->ev3);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete h;
+}
+
+const char* anqi_last_error(const anqi_ctx* h) { return h ? h->c.last_error.c_str() : "null context"; }
+
+uint64_t anqi_device_bytes(const anqi_ctx* h) { return h ? h->c.device_bytes : 0; }
+
+int anqi_pair_distances(anqi_ctx* h, const float* a, const float* b, uint64_t m, uint32_t dim, float* l2sqr,
+                        float* ip) {
+    if (!h || !a || !b || !l2sqr || !ip || dim == 0) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    if (m == 0) return ANQI_OK;
+    const uint32_t stride = round_up(dim, 8);
+    TmpBuf da(c), db(c), dl(c), di(c);
+    int rc;
+    if ((rc = upload_padded(c, da, a, m, dim, stride)) || (rc = upload_padded(c, db, b, m, dim, stride)) ||
+        (rc = ensure(c, dl, m * 4)) || (rc = ensure(c, di, m * 4)))
+        return rc;
+    int blocks = (int)std::min<uint64_t>((m * 4 + 255) / 256, (uint64_t)c->sm_count * 16);
+    pair_dist_kernel<<<blocks, 256, 0, c->stream>>>(da.as<float>(), db.as<float>(), m, dim, stride, dl.as<float>(),
+                                                   di.as<float>());
+    ANQI_CUDA(c, cudaGetLastError());
+    if ((rc = d2h(c, l2sqr, dl, m * 4)) || (rc = d2h(c, ip, di, m * 4)) || (rc = sync(c))) return rc;
+    return ANQI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,134 @@
+// Host-side internals shared by the .cu translation units of libanqi.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/anqi.h"
+
+namespace anqi {
+
+// A growable device allocation owned by the context.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+struct Ctx;
+
+// Throws nothing: every helper records the error in ctx and returns a status.
+int fail(Ctx* c, int status, const char* fmt, ...);
+int cuda_check(Ctx* c, cudaError_t e, const char* what);
+#define ANQI_CUDA(ctx, call)                                      \
+    do {                                                          \
+        cudaError_t _e = (call);                                  \
+        if (_e != cudaSuccess) return ::anqi::cuda_check((ctx), _e, #call); \
+    } while (0)
+
+struct QueryIndex {
+    bool loaded = false;
+    uint64_t n = 0;
+    uint32_t d = 0, dim = 0, degree = 0;
+    uint32_t bstride = 0, lstride = 0;  // padded row strides (floats, multiple of 8)
+    uint32_t tree_nodes = 0, troot = 0;
+    double scale = 0, mstar2 = 0;
+    DevBuf base, lifted, onorm, deg, links;
+    DevBuf tleft, tright, toffset, thyper, tleaf;
+};
+
+struct Verifier {
+    bool loaded = false;
+    uint64_t n = 0;
+    uint32_t nk = 0, rankm = 0, code_size = 0;
+    DevBuf coeff, codes_t /* nk x n, k-major */, mu, basis, codebook;
+};
+
+struct Batch {
+    uint32_t nq = 0;
+    uint32_t L_max = 0;
+    bool has_k = false, has_L = false;
+    uint32_t k_all = 0, L_all = 0;
+    std::vector<uint32_t> k_host;        // distinct k values used (slots)
+    DevBuf q, qL, qslot;                 // queries (nq x bstride), per-query L and threshold slot
+    DevBuf npred, ncand, ndist, nexp, nflood, pred_at, cand_at;
+    DevBuf pred_buf, cand_buf;           // atomic-fill output buffers
+    DevBuf pred_off, cand_off;           // CSR offsets (device)
+    DevBuf pred_csr, cand_csr;
+    uint64_t pred_cap = 0, cand_cap = 0;
+    bool have_results = false;
+    bool have_cands = false;
+};
+
+struct Ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+    std::string last_error;
+    QueryIndex ix;
+    Verifier vf;
+    Batch batch;
+    // scratch
+    DevBuf err, counters;
+    DevBuf vis_bits, vis_log, cand_scratch;
+    uint32_t vis_slots = 0, vis_words = 0, log_cap = 0, cand_cap = 0;
+    // last entry tree from anqi_graph_build
+    std::vector<uint32_t> t_left, t_right, t_leaf_off, t_leaf_cnt, t_perm;
+    std::vector<float> t_offset, t_hyper;
+    uint32_t t_nodes = 0;
+    uint64_t device_bytes = 0;
+    std::vector<DevBuf*> member_bufs() {
+        return {&ix.base, &ix.lifted, &ix.onorm, &ix.deg, &ix.links, &ix.tleft, &ix.tright, &ix.toffset,
+                &ix.thyper, &ix.tleaf, &vf.coeff, &vf.codes_t, &vf.mu, &vf.basis, &vf.codebook, &batch.q,
+                &batch.qL, &batch.qslot, &batch.npred, &batch.ncand, &batch.ndist, &batch.nexp, &batch.nflood,
+                &batch.pred_at, &batch.cand_at, &batch.pred_buf, &batch.cand_buf, &batch.pred_off,
+                &batch.cand_off, &batch.pred_csr, &batch.cand_csr, &err, &counters, &vis_bits, &vis_log,
+                &cand_scratch, &thr_table};
+    }
+    // Per-object thresholds for up to kThrSlots values of k: slot s holds
+    // thr_k[s] (0 = unused) in thr_table[s * n .. (s+1) * n).
+    static constexpr int kThrSlots = 8;
+    DevBuf thr_table;
+    uint32_t thr_k[kThrSlots] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t thr_n = 0;
+};
+
+// Grow buf to at least bytes (contents not preserved).
+int ensure(Ctx* c, DevBuf& b, size_t bytes);
+void release(Ctx* c, DevBuf& b);
+
+// A temporary device allocation released when it goes out of scope.
+struct TmpBuf : DevBuf {
+    Ctx* c;
+    explicit TmpBuf(Ctx* ctx) : c(ctx) {}
+    ~TmpBuf() { release(c, *this); }
+    TmpBuf(const TmpBuf&) = delete;
+    TmpBuf& operator=(const TmpBuf&) = delete;
+};
+int h2d(Ctx* c, DevBuf& b, const void* src, size_t bytes);
+int d2h(Ctx* c, void* dst, const DevBuf& b, size_t bytes);
+int sync(Ctx* c);
+// Reads the device error word, maps it to a status (and clears it).
+int check_device_error(Ctx* c, const char* stage);
+
+inline uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
+
+// Pad rows of a host matrix into a device buffer with stride (floats), zero fill.
+int upload_padded(Ctx* c, DevBuf& b, const float* src, uint64_t n, uint32_t d, uint32_t stride);
+
+// Launch helpers implemented in the .cu files.
+int lrq_materialize_device(Ctx* c, const Verifier& v, uint32_t k, double scale, float* d_out);
+int compute_norms_device(Ctx* c, const float* d_x, uint64_t n, uint32_t dim, uint32_t stride, float* d_out);
+
+}  // namespace anqi
+
+struct anqi_ctx {
+    anqi::Ctx c;
+};

@@ -1,0 +1,847 @@
+// Reverse-kNN query path: query lift, RP-tree entry, greedy beam + bounded
+// flood over the lifted G48 graph, FP32 postfilter against the LRQ thresholds.
+//
+// Reference: src/rknn_query.cpp:2714-2765 (per-query work of the timed loop),
+// include/index.h:1535-1640 (range_search), include/neighbor.h:43-141 (the
+// ordered beam queue), include/rptrees.h:108-124 (entry descent).
+//
+// Design.  One warp owns one query at a time and pulls queries from a global
+// counter (persistent grid, one resident warp per slot).  The beam lives in
+// shared memory as two sorted (dist, id) arrays that are merged into each
+// other: inserting one expansion's neighbours as a batch leaves exactly the
+// top-L set and first-unexpanded cursor that the reference's one-at-a-time
+// binary insertion leaves, because the queue order is a total order on
+// (dist, id) and no id is inserted twice.  The flood's visited set is a
+// closure, so its result does not depend on visit order either.  Distances are
+// computed by 4-thread groups in the AVX-512 lane order (common.cuh), so every
+// comparison against R2 and every beam decision matches the reference's FP32
+// arithmetic bit for bit.  The visited set is a per-slot bitmap over all
+// objects (L2-resident words, atomicOr test-and-set) cleared by replaying a
+// log of set bits.
+#include <algorithm>
+#include <cfloat>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace anqi {
+
+struct SearchParams {
+    const float* lifted;
+    const float* base;
+    const float* onorm;
+    const uint32_t* links;
+    const uint32_t* deg;
+    const uint32_t* tleft;
+    const uint32_t* tright;
+    const float* toffset;
+    const float* thyper;
+    const uint32_t* tleaf;
+    uint64_t n;
+    uint32_t dim, d, lstride, bstride, degree, troot;
+    double scale, R2;
+    const float* thr;  // slot-major thresholds
+    const float* queries;
+    const uint32_t* qL;
+    const uint8_t* qslot;
+    uint32_t L_all, slot_all, nq, L_max;
+    uint32_t* vis_bits;
+    uint32_t vis_words;
+    uint32_t* vis_log;
+    uint32_t log_cap;
+    uint32_t* cand_scratch;
+    uint32_t cand_cap;
+    uint32_t* work;
+    unsigned long long* fill;  // [0] predicted ids, [1] candidate ids
+    uint32_t* pred_buf;
+    uint64_t pred_cap;
+    uint32_t* cand_buf;
+    uint64_t cand_out_cap;
+    int keep_cand;
+    uint32_t* npred;
+    uint32_t* ncand;
+    uint32_t* ndist;
+    uint32_t* nexp;
+    uint32_t* nflood;
+    unsigned long long* pred_at;
+    unsigned long long* cand_at;
+    uint32_t* err;
+};
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Visits the links of node: collects the ids seen for the first time into
+// ni[0..m) in link-slot order and logs them.  Returns m.
+__device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t node, uint32_t* bits,
+                                                 uint32_t* vlog, uint32_t& nlog, uint32_t* ni, uint32_t lane) {
+    const uint32_t* lk = p.links + (size_t)node * p.degree;
+    const uint32_t dg = min(p.deg[node], p.degree);
+    uint32_t id0 = kEmpty, id1 = kEmpty;
+    bool f0 = false, f1 = false, bad = false;
+    if (lane < dg) {
+        id0 = lk[lane];
+        if (id0 < p.n) f0 = visit_first(bits, id0);
+        else bad = true;
+    }
+    if (lane + 32 < dg) {
+        id1 = lk[lane + 32];
+        if (id1 < p.n) f1 = visit_first(bits, id1);
+        else bad = true;
+    }
+    if (bad) set_error(p.err, kDevBadId);
+    const unsigned b0 = __ballot_sync(kFull, f0), b1 = __ballot_sync(kFull, f1);
+    const uint32_t c0 = __popc(b0), lt = lanemask_lt();
+    const uint32_t p0 = __popc(b0 & lt), p1 = c0 + __popc(b1 & lt);
+    if (f0) {
+        ni[p0] = id0;
+        if (nlog + p0 < p.log_cap) vlog[nlog + p0] = id0;
+    }
+    if (f1) {
+        ni[p1] = id1;
+        if (nlog + p1 < p.log_cap) vlog[nlog + p1] = id1;
+    }
+    const uint32_t m = c0 + __popc(b1);
+    nlog += m;
+    __syncwarp();
+    return m;
+}
+
+// Distances of the m fresh neighbours to the lifted query: 8 groups of 4 lanes.
+__device__ __forceinline__ void fresh_distances(const SearchParams& p, const float* qhat, const uint32_t* ni,
+                                                float* nd, uint32_t m, uint32_t gw, uint32_t gt) {
+    for (uint32_t r0 = 0; r0 < m; r0 += 16) {
+        const uint32_t ia = r0 + gw, ib = r0 + 8 + gw;
+        const bool oka = ia < m, okb = ib < m;
+        const uint32_t ida = ni[oka ? ia : r0];
+        const uint32_t idb = ni[okb ? ib : r0];
+        float da = group_l2sqr(p.lifted + (size_t)ida * p.lstride, qhat, p.dim, gt, kFull);
+        float db = 0.f;
+        if (r0 + 8 < m) db = group_l2sqr(p.lifted + (size_t)idb * p.lstride, qhat, p.dim, gt, kFull);
+        if (gt == 0) {
+            if (oka) nd[ia] = da;
+            if (okb) nd[ib] = db;
+        }
+    }
+    __syncwarp();
+}
+
+// Appends fresh neighbours within R2 to the candidate / flood list (visit order).
+__device__ __forceinline__ void append_in_range(const SearchParams& p, const float* nd, const uint32_t* ni,
+                                                uint32_t m, uint32_t* cl, uint32_t& ncand, bool& overflow,
+                                                uint32_t lane) {
+    const bool in0 = lane < m && (double)nd[lane] <= p.R2;
+    const bool in1 = lane + 32 < m && (double)nd[lane + 32] <= p.R2;
+    const unsigned b0 = __ballot_sync(kFull, in0), b1 = __ballot_sync(kFull, in1);
+    const uint32_t c0 = __popc(b0), lt = lanemask_lt();
+    const uint32_t pos0 = ncand + __popc(b0 & lt), pos1 = ncand + c0 + __popc(b1 & lt);
+    if (in0) {
+        if (pos0 < p.cand_cap) cl[pos0] = ni[lane];
+        else overflow = true;
+    }
+    if (in1) {
+        if (pos1 < p.cand_cap) cl[pos1] = ni[lane + 32];
+        else overflow = true;
+    }
+    ncand += c0 + __popc(b1);
+    if (ncand > p.cand_cap) ncand = p.cand_cap;
+    overflow = __any_sync(kFull, overflow);
+    __syncwarp();
+}
+
+extern __shared__ __align__(16) unsigned char g_smem[];
+
+__global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
+    const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
+    const size_t per_warp = (size_t)(4 * p.L_max + 128 + p.lstride + p.bstride) * 4;
+    unsigned char* my = g_smem + wib * per_warp;
+    float* qhat = reinterpret_cast<float*>(my);
+    float* qraw = qhat + p.lstride;
+    float* bdA = qraw + p.bstride;
+    uint32_t* biA = reinterpret_cast<uint32_t*>(bdA + p.L_max);
+    float* bdB = reinterpret_cast<float*>(biA + p.L_max);
+    uint32_t* biB = reinterpret_cast<uint32_t*>(bdB + p.L_max);
+    float* nd = reinterpret_cast<float*>(biB + p.L_max);
+    uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 64);
+    uint32_t* bits = p.vis_bits + (size_t)slot * p.vis_words;
+    uint32_t* vlog = p.vis_log + (size_t)slot * p.log_cap;
+    uint32_t* cl = p.cand_scratch + (size_t)slot * p.cand_cap;
+    VisitSlot vs{bits, vlog, p.log_cap, p.vis_words};
+
+    for (;;) {
+        uint32_t qi = 0;
+        if (lane == 0) qi = atomicAdd(p.work, 1u);
+        qi = __shfl_sync(kFull, qi, 0);
+        if (qi >= p.nq) break;
+        const uint32_t L = min(p.qL ? p.qL[qi] : p.L_all, p.L_max);
+        const uint32_t tslot = p.qslot ? p.qslot[qi] : p.slot_all;
+        const float* q = p.queries + (size_t)qi * p.bstride;
+        // query lift, rknn_query.cpp:2724-2729
+        for (uint32_t j = lane; j < p.bstride; j += 32) qraw[j] = q[j];
+        for (uint32_t j = lane; j < p.lstride; j += 32) {
+            float v = 0.0f;
+            if (j < p.d) v = __double2float_rn(__dmul_rn((double)q[j], p.scale));
+            else if (j == p.d) v = 1.0f;
+            qhat[j] = v;
+        }
+        __syncwarp();
+        // RP-tree entry, rptrees.h:108-124 (|margin| <= EPS goes left)
+        uint32_t v = p.troot;
+        for (uint32_t depth = 0; p.tleft[v] != kEmpty && depth < 4096; depth++) {
+            const float ip = group_ip(p.thyper + (size_t)v * p.lstride, qhat, p.dim, gt, kFull);
+            const float margin = __fsub_rn(ip, p.toffset[v]);
+            v = (margin < -kSplitEps) ? p.tleft[v] : (margin > kSplitEps ? p.tright[v] : p.tleft[v]);
+        }
+        uint32_t ep = p.tleaf[v];
+        if (ep == kEmpty || ep >= p.n) ep = 0;
+
+        const float dep = group_l2sqr(p.lifted + (size_t)ep * p.lstride, qhat, p.dim, gt, kFull);
+        if (lane == 0) {
+            visit_first(bits, ep);
+            if (p.log_cap) vlog[0] = ep;
+            bdA[0] = dep;
+            biA[0] = ep;
+        }
+        uint32_t nlog = 1, ncand = 0, nexp = 0, nfl = 0;
+        bool overflow = false;
+        if ((double)dep <= p.R2) {
+            if (lane == 0) cl[0] = ep;
+            ncand = 1;
+        }
+        __syncwarp();
+        float* bd = bdA;
+        uint32_t* bi = biA;
+        float* od = bdB;
+        uint32_t* oi = biB;
+        uint32_t size = 1, cur = 0;
+
+        // ---- greedy beam, index.h:1613-1624
+        while (cur < size && !overflow) {
+            const uint32_t node = bi[cur] & kIdMask;
+            __syncwarp();
+            if (lane == 0) bi[cur] = node | kExpanded;
+            __syncwarp();
+            nexp++;
+            uint32_t nxt = size;
+            for (uint32_t s0 = cur + 1; s0 < size; s0 += 32) {
+                const uint32_t idx = s0 + lane;
+                const bool un = idx < size && !(bi[idx] & kExpanded);
+                const unsigned b = __ballot_sync(kFull, un);
+                if (b) {
+                    nxt = s0 + __ffs(b) - 1;
+                    break;
+                }
+            }
+            const uint32_t m = expand_links(p, node, bits, vlog, nlog, ni, lane);
+            if (m == 0) {
+                cur = nxt;
+                continue;
+            }
+            fresh_distances(p, qhat, ni, nd, m, gw, gt);
+            append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
+            // batch insert = merge of the sorted batch into the sorted beam
+            float d0 = lane < m ? nd[lane] : FLT_MAX;
+            uint32_t i0 = lane < m ? ni[lane] : kEmpty;
+            float d1 = lane + 32 < m ? nd[lane + 32] : FLT_MAX;
+            uint32_t i1 = lane + 32 < m ? ni[lane + 32] : kEmpty;
+            if (lane >= m) d0 = __int_as_float(0x7f800000);
+            if (lane + 32 >= m) d1 = __int_as_float(0x7f800000);
+            warp_sort64(d0, i0, d1, i1);
+            __syncwarp();
+            nd[lane] = d0;
+            ni[lane] = i0;
+            nd[lane + 32] = d1;
+            ni[lane + 32] = i1;
+            __syncwarp();
+            const uint32_t ns = min(L, size + m);
+            for (uint32_t p0 = lane; p0 < size; p0 += 32) {
+                const float dv = bd[p0];
+                const uint32_t iv = bi[p0];
+                const uint32_t pos = p0 + lower_rank(nd, ni, m, dv, iv);
+                if (pos < ns) {
+                    od[pos] = dv;
+                    oi[pos] = iv;
+                }
+            }
+            for (uint32_t r = lane; r < m; r += 32) {
+                const uint32_t pos = r + lower_rank(bd, bi, size, nd[r], ni[r]);
+                if (pos < ns) {
+                    od[pos] = nd[r];
+                    oi[pos] = ni[r];
+                }
+            }
+            uint32_t cb = 0xFFFFFFFFu;
+            if (nxt < size) cb = nxt + lower_rank(nd, ni, m, bd[nxt], bi[nxt]);
+            const uint32_t cn = lower_rank(bd, bi, size, nd[0], ni[0]);
+            uint32_t nc = min(cb, cn);
+            if (nc > ns) nc = ns;
+            __syncwarp();
+            float* td = bd;
+            bd = od;
+            od = td;
+            uint32_t* ti = bi;
+            bi = oi;
+            oi = ti;
+            size = ns;
+            cur = nc;
+        }
+
+        // ---- bounded flood, index.h:1626-1638
+        uint32_t head = 0;
+        while (head < ncand && !overflow) {
+            const uint32_t node = cl[head++];
+            nfl++;
+            const uint32_t m = expand_links(p, node, bits, vlog, nlog, ni, lane);
+            if (m == 0) continue;
+            fresh_distances(p, qhat, ni, nd, m, gw, gt);
+            append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
+        }
+        if (overflow && lane == 0) set_error(p.err, kDevCandOverflow);
+
+        // ---- candidates out (optional), then the postfilter
+        unsigned long long cat = 0;
+        if (p.keep_cand) {
+            if (lane == 0) {
+                cat = atomicAdd(&p.fill[1], (unsigned long long)ncand);
+                if (cat + ncand > p.cand_out_cap) set_error(p.err, kDevOutOverflow);
+            }
+            cat = __shfl_sync(kFull, cat, 0);
+            if (cat + ncand <= p.cand_out_cap)
+                for (uint32_t i = lane; i < ncand; i += 32) p.cand_buf[cat + i] = cl[i];
+            __syncwarp();
+        }
+        // rknn_query.cpp:2555-2561: key = IP(o,o) + IP(q,q) - 2 IP(o,q) <= (double) thr[o]
+        const float qn = group_ip(qraw, qraw, p.d, gt, kFull);
+        const float* thr = p.thr + (size_t)tslot * p.n;
+        uint32_t npred = 0;
+        for (uint32_t r0 = 0; r0 < ncand; r0 += 8) {
+            const uint32_t idx = r0 + gw;
+            const bool ok = idx < ncand;
+            const uint32_t o = cl[ok ? idx : r0];
+            const float ip = group_ip(p.base + (size_t)o * p.bstride, qraw, p.d, gt, kFull);
+            const float key = __fsub_rn(__fadd_rn(p.onorm[o], qn), __fmul_rn(2.0f, ip));
+            const bool pass = ok && (double)key <= (double)thr[o];
+            const unsigned b = __ballot_sync(kFull, pass && gt == 0);
+            __syncwarp();
+            if (pass && gt == 0) cl[npred + __popc(b & lanemask_lt())] = o;
+            npred += __popc(b);
+            __syncwarp();
+        }
+        unsigned long long at = 0;
+        if (lane == 0) {
+            at = atomicAdd(&p.fill[0], (unsigned long long)npred);
+            if (at + npred > p.pred_cap) set_error(p.err, kDevOutOverflow);
+            p.npred[qi] = npred;
+            p.ncand[qi] = ncand;
+            p.ndist[qi] = nlog;
+            p.nexp[qi] = nexp;
+            p.nflood[qi] = nfl;
+            p.pred_at[qi] = at;
+            p.cand_at[qi] = cat;
+        }
+        at = __shfl_sync(kFull, at, 0);
+        if (at + npred <= p.pred_cap)
+            for (uint32_t i = lane; i < npred; i += 32) p.pred_buf[at + i] = cl[i];
+        visit_clear(vs, nlog);
+    }
+}
+
+// Exclusive scan of counts (nq) into off (nq + 1), one block, fixed order.
+__global__ void scan_counts_kernel(const uint32_t* __restrict__ cnt, uint32_t nq, uint32_t* __restrict__ off) {
+    __shared__ unsigned long long part[1024];
+    const uint32_t t = threadIdx.x, T = blockDim.x;
+    const uint32_t chunk = (nq + T - 1) / T;
+    const uint32_t b = min(nq, t * chunk), e = min(nq, b + chunk);
+    unsigned long long s = 0;
+    for (uint32_t i = b; i < e; i++) s += cnt[i];
+    part[t] = s;
+    __syncthreads();
+    if (t == 0) {
+        unsigned long long run = 0;
+        for (uint32_t i = 0; i < T; i++) {
+            unsigned long long v = part[i];
+            part[i] = run;
+            run += v;
+        }
+        off[nq] = (uint32_t)run;
+    }
+    __syncthreads();
+    unsigned long long run = part[t];
+    for (uint32_t i = b; i < e; i++) {
+        off[i] = (uint32_t)run;
+        run += cnt[i];
+    }
+}
+
+__global__ void gather_csr_kernel(const uint32_t* __restrict__ src, const unsigned long long* __restrict__ at,
+                                  const uint32_t* __restrict__ off, uint32_t nq, uint32_t* __restrict__ dst) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t q = w; q < nq; q += nw) {
+        const uint32_t c = off[q + 1] - off[q];
+        const unsigned long long s = at[q];
+        for (uint32_t i = lane; i < c; i += 32) dst[off[q] + i] = src[s + i];
+    }
+}
+
+// Per query recall / precision / candidate recall (rknn_query.cpp:2784-2799);
+// gt ids are sorted ascending per query for binary search.
+__global__ void evaluate_kernel(const uint32_t* __restrict__ pred_off, const uint32_t* __restrict__ pred,
+                                const uint32_t* __restrict__ cand_off, const uint32_t* __restrict__ cand,
+                                const uint32_t* __restrict__ gt_off, const uint32_t* __restrict__ gt_sorted,
+                                uint32_t nq, double* __restrict__ out /* nq x 3, NaN for empty truth */) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t q = w; q < nq; q += nw) {
+        const uint32_t* g = gt_sorted + gt_off[q];
+        const uint32_t ng = gt_off[q + 1] - gt_off[q];
+        auto member = [&](uint32_t id) {
+            uint32_t lo = 0, hi = ng;
+            while (lo < hi) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (g[mid] < id) lo = mid + 1;
+                else hi = mid;
+            }
+            return lo < ng && g[lo] == id;
+        };
+        uint32_t hit = 0, chit = 0;
+        const uint32_t np = pred_off[q + 1] - pred_off[q];
+        for (uint32_t i = lane; i < np; i += 32) hit += member(pred[pred_off[q] + i]);
+        uint32_t nc = 0;
+        if (cand) {
+            nc = cand_off[q + 1] - cand_off[q];
+            for (uint32_t i = lane; i < nc; i += 32) chit += member(cand[cand_off[q] + i]);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            hit += __shfl_xor_sync(kFull, hit, o);
+            chit += __shfl_xor_sync(kFull, chit, o);
+        }
+        if (lane == 0) {
+            double nan = __longlong_as_double(0x7ff8000000000000ull);
+            if (ng == 0) {
+                out[3 * (size_t)q] = nan;
+                out[3 * (size_t)q + 1] = nan;
+                out[3 * (size_t)q + 2] = nan;
+            } else {
+                out[3 * (size_t)q] = (double)hit / ng;
+                out[3 * (size_t)q + 1] = np == 0 ? 1.0 : (double)hit / np;
+                out[3 * (size_t)q + 2] = (double)chit / ng;
+            }
+        }
+    }
+}
+
+static int slot_for_k(Ctx* c, uint32_t k) {
+    for (int s = 0; s < Ctx::kThrSlots; s++)
+        if (c->thr_k[s] == k) return s;
+    return -1;
+}
+
+static int claim_slot(Ctx* c, uint32_t k) {
+    int s = slot_for_k(c, k);
+    if (s >= 0) return s;
+    for (s = 0; s < Ctx::kThrSlots; s++)
+        if (c->thr_k[s] == 0) return s;
+    return 0;  // evict slot 0
+}
+
+static int ensure_thr_table(Ctx* c, uint64_t n) {
+    if (c->thr_n != n) {
+        for (int s = 0; s < Ctx::kThrSlots; s++) c->thr_k[s] = 0;
+        c->thr_n = n;
+    }
+    return ensure(c, c->thr_table, (size_t)Ctx::kThrSlots * n * 4);
+}
+
+static size_t search_smem_per_warp(const Ctx* c, uint32_t L_max) {
+    return (size_t)(4 * L_max + 128 + c->ix.lstride + c->ix.bstride) * 4;
+}
+
+}  // namespace anqi
+
+using namespace anqi;
+
+extern "C" {
+
+int anqi_index_load(anqi_ctx* h, const anqi_index_desc* x) {
+    if (!h || !x || !x->base || !x->lifted || !x->deg || !x->links || !x->tree_left || !x->tree_right ||
+        !x->tree_offset || !x->tree_hyperplane || !x->tree_leaf_first || x->n == 0 || x->d == 0 ||
+        x->degree == 0 || x->tree_nodes == 0)
+        return h ? fail(&h->c, ANQI_ERR_ARGS, "anqi_index_load: missing or empty argument") : ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    if (x->degree > 64) return fail(c, ANQI_ERR_ARGS, "graph degree %u > 64 is not supported", x->degree);
+    if (x->n >= 0x7FFFFFFFull) return fail(c, ANQI_ERR_ARGS, "n must be < 2^31");
+    // index.h:1840-1861 validation: degrees and neighbour ids in range
+    for (uint64_t i = 0; i < x->n; i++) {
+        if (x->deg[i] > x->degree) return fail(c, ANQI_ERR_FORMAT, "invalid adjacency data: deg[%llu]", (unsigned long long)i);
+        const uint32_t* lk = x->links + i * x->degree;
+        for (uint32_t j = 0; j < x->deg[i]; j++)
+            if (lk[j] >= x->n) return fail(c, ANQI_ERR_FORMAT, "invalid neighbor id in graph row %llu", (unsigned long long)i);
+    }
+    for (uint32_t v = 0; v < x->tree_nodes; v++) {
+        const bool leaf = x->tree_left[v] == ANQI_EMPTY;
+        if (!leaf && (x->tree_left[v] >= x->tree_nodes || x->tree_right[v] >= x->tree_nodes))
+            return fail(c, ANQI_ERR_FORMAT, "invalid RP tree node %u", v);
+    }
+    QueryIndex& ix = c->ix;
+    ix.loaded = false;
+    ix.n = x->n;
+    ix.d = x->d;
+    ix.dim = x->d + 2;
+    ix.degree = x->degree;
+    ix.bstride = round_up(x->d, 8);
+    ix.lstride = round_up(x->d + 2, 8);
+    ix.tree_nodes = x->tree_nodes;
+    ix.troot = x->tree_nodes - 1;
+    ix.scale = x->scale;
+    ix.mstar2 = x->mstar2;
+    int rc;
+    if ((rc = upload_padded(c, ix.base, x->base, x->n, x->d, ix.bstride)) ||
+        (rc = upload_padded(c, ix.lifted, x->lifted, x->n, ix.dim, ix.lstride)) ||
+        (rc = ensure(c, ix.onorm, x->n * 4)) || (rc = h2d(c, ix.deg, x->deg, x->n * 4)) ||
+        (rc = h2d(c, ix.links, x->links, x->n * (size_t)x->degree * 4)) ||
+        (rc = h2d(c, ix.tleft, x->tree_left, x->tree_nodes * 4)) ||
+        (rc = h2d(c, ix.tright, x->tree_right, x->tree_nodes * 4)) ||
+        (rc = h2d(c, ix.toffset, x->tree_offset, x->tree_nodes * 4)) ||
+        (rc = upload_padded(c, ix.thyper, x->tree_hyperplane, x->tree_nodes, ix.dim, ix.lstride)) ||
+        (rc = h2d(c, ix.tleaf, x->tree_leaf_first, x->tree_nodes * 4)))
+        return rc;
+    if ((rc = compute_norms_device(c, ix.base.as<float>(), x->n, x->d, ix.bstride, ix.onorm.as<float>()))) return rc;
+    if ((rc = sync(c))) return rc;
+    for (int s = 0; s < Ctx::kThrSlots; s++) c->thr_k[s] = 0;
+    ix.loaded = true;
+    return ANQI_OK;
+}
+
+int anqi_set_thresholds(anqi_ctx* h, uint32_t k, const float* thr) {
+    if (!h || !thr || k == 0) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    if (!c->ix.loaded) return fail(c, ANQI_ERR_ARGS, "anqi_set_thresholds: no index loaded");
+    int rc = ensure_thr_table(c, c->ix.n);
+    if (rc) return rc;
+    const int s = claim_slot(c, k);
+    ANQI_CUDA(c, cudaMemcpyAsync(c->thr_table.as<float>() + (size_t)s * c->ix.n, thr, c->ix.n * 4,
+                                 cudaMemcpyHostToDevice, c->stream));
+    if ((rc = sync(c))) return rc;
+    c->thr_k[s] = k;
+    return ANQI_OK;
+}
+
+int anqi_verifier_materialize(anqi_ctx* h, uint32_t k, double radius_scale) {
+    if (!h || k == 0) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    if (!c->vf.loaded) return fail(c, ANQI_ERR_ARGS, "anqi_verifier_materialize: no verifier loaded");
+    if (k > c->vf.nk) return fail(c, ANQI_ERR_ARGS, "LRQ verifier is not ready for k=%u", k);
+    if (!c->ix.loaded || c->ix.n != c->vf.n)
+        return fail(c, ANQI_ERR_ARGS, "anqi_verifier_materialize: verifier and index sizes differ");
+    int rc = ensure_thr_table(c, c->ix.n);
+    if (rc) return rc;
+    const int s = claim_slot(c, k);
+    c->thr_k[s] = 0;
+    if ((rc = lrq_materialize_device(c, c->vf, k, radius_scale, c->thr_table.as<float>() + (size_t)s * c->ix.n)))
+        return rc;
+    if ((rc = sync(c))) return rc;
+    c->thr_k[s] = k;
+    return ANQI_OK;
+}
+
+int anqi_query_upload(anqi_ctx* h, const float* queries, uint32_t nq, const uint32_t* k_per_query, uint32_t k_all,
+                      const uint32_t* L_per_query, uint32_t L_all) {
+    if (!h || !queries || nq == 0) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    if (!c->ix.loaded) return fail(c, ANQI_ERR_ARGS, "anqi_query_upload: no index loaded");
+    Batch& b = c->batch;
+    b.nq = nq;
+    b.have_results = false;
+    std::vector<uint8_t> slots;
+    uint32_t slot_all = 0;
+    if (k_per_query) {
+        slots.resize(nq);
+        for (uint32_t i = 0; i < nq; i++) {
+            int s = slot_for_k(c, k_per_query[i]);
+            if (s < 0) return fail(c, ANQI_ERR_ARGS, "no thresholds materialized for k=%u", k_per_query[i]);
+            slots[i] = (uint8_t)s;
+        }
+    } else {
+        int s = slot_for_k(c, k_all);
+        if (s < 0) return fail(c, ANQI_ERR_ARGS, "no thresholds materialized for k=%u", k_all);
+        slot_all = (uint32_t)s;
+    }
+    uint32_t L_max = L_all;
+    if (L_per_query) {
+        L_max = 0;
+        for (uint32_t i = 0; i < nq; i++) L_max = std::max(L_max, L_per_query[i]);
+    }
+    if (L_max == 0 || L_max > 4096) return fail(c, ANQI_ERR_ARGS, "beam width must be in [1, 4096]");
+    if (L_per_query)
+        for (uint32_t i = 0; i < nq; i++)
+            if (L_per_query[i] == 0) return fail(c, ANQI_ERR_ARGS, "beam width must be positive");
+    b.L_max = round_up(L_max, 4);
+    b.has_k = k_per_query != nullptr;
+    b.has_L = L_per_query != nullptr;
+    b.k_all = slot_all;
+    b.L_all = L_all;
+    int rc;
+    if ((rc = upload_padded(c, b.q, queries, nq, c->ix.d, c->ix.bstride))) return rc;
+    if (b.has_k && (rc = h2d(c, b.qslot, slots.data(), nq))) return rc;
+    if (b.has_L && (rc = h2d(c, b.qL, L_per_query, nq * 4ull))) return rc;
+    const size_t q4 = (size_t)nq * 4, q8 = (size_t)nq * 8;
+    if ((rc = ensure(c, b.npred, q4)) || (rc = ensure(c, b.ncand, q4)) || (rc = ensure(c, b.ndist, q4)) ||
+        (rc = ensure(c, b.nexp, q4)) || (rc = ensure(c, b.nflood, q4)) || (rc = ensure(c, b.pred_at, q8)) ||
+        (rc = ensure(c, b.cand_at, q8)) || (rc = ensure(c, b.pred_off, q4 + 4)) ||
+        (rc = ensure(c, b.cand_off, q4 + 4)))
+        return rc;
+    return sync(c);
+}
+
+int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
+    if (!h) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    Batch& b = c->batch;
+    if (!c->ix.loaded || b.nq == 0) return fail(c, ANQI_ERR_ARGS, "anqi_query_run: no index or batch");
+    const QueryIndex& ix = c->ix;
+    const size_t smem_warp = search_smem_per_warp(c, b.L_max);
+    const int warps_per_block = 4;
+    const size_t smem = smem_warp * warps_per_block;
+    if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "beam width %u needs too much shared memory", b.L_max);
+    ANQI_CUDA(c, cudaFuncSetAttribute(rknn_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rknn_search_kernel, 32 * warps_per_block, smem));
+    if (per_sm < 1) return fail(c, ANQI_ERR_DEVICE, "search kernel does not fit on an SM");
+    uint32_t blocks = (uint32_t)per_sm * c->sm_count;
+    blocks = std::min<uint32_t>(blocks, (b.nq + warps_per_block - 1) / warps_per_block);
+    const uint32_t slots = blocks * warps_per_block;
+    int rc;
+    // per-slot scratch
+    const uint32_t words = (uint32_t)((ix.n + 31) / 32);
+    const uint32_t log_cap = (uint32_t)std::min<uint64_t>(ix.n, 16384);
+    const uint32_t cand_cap = (uint32_t)std::min<uint64_t>(ix.n, 65536);
+    if (c->vis_slots < slots || c->vis_words != words || c->log_cap != log_cap || c->cand_cap != cand_cap) {
+        if ((rc = ensure(c, c->vis_bits, (size_t)slots * words * 4)) ||
+            (rc = ensure(c, c->vis_log, (size_t)slots * log_cap * 4)) ||
+            (rc = ensure(c, c->cand_scratch, (size_t)slots * cand_cap * 4)))
+            return rc;
+        ANQI_CUDA(c, cudaMemsetAsync(c->vis_bits.p, 0, (size_t)slots * words * 4, c->stream));
+        c->vis_slots = slots;
+        c->vis_words = words;
+        c->log_cap = log_cap;
+        c->cand_cap = cand_cap;
+    }
+    if (b.pred_cap == 0) b.pred_cap = std::max<uint64_t>(1024, (uint64_t)b.nq * 128);
+    if (keep_candidates && b.cand_cap == 0) b.cand_cap = std::max<uint64_t>(1024, (uint64_t)b.nq * 256);
+    for (int attempt = 0; attempt < 3; attempt++) {
+        if ((rc = ensure(c, b.pred_buf, b.pred_cap * 4))) return rc;
+        if (keep_candidates && (rc = ensure(c, b.cand_buf, b.cand_cap * 4))) return rc;
+        ANQI_CUDA(c, cudaMemsetAsync(c->counters.p, 0, 64, c->stream));
+        SearchParams p{};
+        p.lifted = ix.lifted.as<float>();
+        p.base = ix.base.as<float>();
+        p.onorm = ix.onorm.as<float>();
+        p.links = ix.links.as<uint32_t>();
+        p.deg = ix.deg.as<uint32_t>();
+        p.tleft = ix.tleft.as<uint32_t>();
+        p.tright = ix.tright.as<uint32_t>();
+        p.toffset = ix.toffset.as<float>();
+        p.thyper = ix.thyper.as<float>();
+        p.tleaf = ix.tleaf.as<uint32_t>();
+        p.n = ix.n;
+        p.dim = ix.dim;
+        p.d = ix.d;
+        p.lstride = ix.lstride;
+        p.bstride = ix.bstride;
+        p.degree = ix.degree;
+        p.troot = ix.troot;
+        p.scale = ix.scale;
+        p.R2 = ix.mstar2 + 1.0;  // rknn_query.cpp:2729, eps = 0
+        p.thr = c->thr_table.as<float>();
+        p.queries = b.q.as<float>();
+        p.qL = b.has_L ? b.qL.as<uint32_t>() : nullptr;
+        p.qslot = b.has_k ? b.qslot.as<uint8_t>() : nullptr;
+        p.L_all = b.L_all;
+        p.slot_all = b.k_all;
+        p.nq = b.nq;
+        p.L_max = b.L_max;
+        p.vis_bits = c->vis_bits.as<uint32_t>();
+        p.vis_words = words;
+        p.vis_log = c->vis_log.as<uint32_t>();
+        p.log_cap = log_cap;
+        p.cand_scratch = c->cand_scratch.as<uint32_t>();
+        p.cand_cap = cand_cap;
+        p.work = c->counters.as<uint32_t>();
+        p.fill = reinterpret_cast<unsigned long long*>(c->counters.as<uint32_t>() + 4);
+        p.pred_buf = b.pred_buf.as<uint32_t>();
+        p.pred_cap = b.pred_cap;
+        p.cand_buf = keep_candidates ? b.cand_buf.as<uint32_t>() : nullptr;
+        p.cand_out_cap = keep_candidates ? b.cand_cap : 0;
+        p.keep_cand = keep_candidates;
+        p.npred = b.npred.as<uint32_t>();
+        p.ncand = b.ncand.as<uint32_t>();
+        p.ndist = b.ndist.as<uint32_t>();
+        p.nexp = b.nexp.as<uint32_t>();
+        p.nflood = b.nflood.as<uint32_t>();
+        p.pred_at = b.pred_at.as<unsigned long long>();
+        p.cand_at = b.cand_at.as<unsigned long long>();
+        p.err = c->err.as<uint32_t>();
+        ANQI_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+        rknn_search_kernel<<<blocks, 32 * warps_per_block, smem, c->stream>>>(p);
+        ANQI_CUDA(c, cudaGetLastError());
+        ANQI_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+        unsigned long long fill[2] = {0, 0};
+        ANQI_CUDA(c, cudaMemcpyAsync(fill, p.fill, 16, cudaMemcpyDeviceToHost, c->stream));
+        uint32_t err = 0;
+        ANQI_CUDA(c, cudaMemcpyAsync(&err, c->err.p, 4, cudaMemcpyDeviceToHost, c->stream));
+        if ((rc = sync(c))) return rc;
+        if (err == kDevOutOverflow) {
+            ANQI_CUDA(c, cudaMemsetAsync(c->err.p, 0, 4, c->stream));
+            b.pred_cap = std::max<uint64_t>(b.pred_cap, fill[0] + 1024);
+            if (keep_candidates) b.cand_cap = std::max<uint64_t>(b.cand_cap, fill[1] + 1024);
+            continue;
+        }
+        if ((rc = check_device_error(c, "rknn search"))) return rc;
+        float ms = 0;
+        ANQI_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        // CSR offsets + compaction
+        scan_counts_kernel<<<1, 1024, 0, c->stream>>>(b.npred.as<uint32_t>(), b.nq, b.pred_off.as<uint32_t>());
+        if ((rc = ensure(c, b.pred_csr, std::max<uint64_t>(fill[0], 1) * 4))) return rc;
+        gather_csr_kernel<<<c->sm_count * 4, 256, 0, c->stream>>>(b.pred_buf.as<uint32_t>(),
+                                                                  b.pred_at.as<unsigned long long>(),
+                                                                  b.pred_off.as<uint32_t>(), b.nq,
+                                                                  b.pred_csr.as<uint32_t>());
+        if (keep_candidates) {
+            scan_counts_kernel<<<1, 1024, 0, c->stream>>>(b.ncand.as<uint32_t>(), b.nq, b.cand_off.as<uint32_t>());
+            if ((rc = ensure(c, b.cand_csr, std::max<uint64_t>(fill[1], 1) * 4))) return rc;
+            gather_csr_kernel<<<c->sm_count * 4, 256, 0, c->stream>>>(b.cand_buf.as<uint32_t>(),
+                                                                      b.cand_at.as<unsigned long long>(),
+                                                                      b.cand_off.as<uint32_t>(), b.nq,
+                                                                      b.cand_csr.as<uint32_t>());
+        }
+        ANQI_CUDA(c, cudaGetLastError());
+        b.have_results = true;
+        b.have_cands = keep_candidates != 0;
+        if (st) {
+            std::vector<uint32_t> v(b.nq);
+            uint64_t sums[5] = {0, 0, 0, 0, 0};
+            DevBuf* arr[5] = {&b.ndist, &b.nexp, &b.ncand, &b.npred, &b.nflood};
+            for (int a = 0; a < 5; a++) {
+                ANQI_CUDA(c, cudaMemcpyAsync(v.data(), arr[a]->p, b.nq * 4ull, cudaMemcpyDeviceToHost, c->stream));
+                if ((rc = sync(c))) return rc;
+                for (uint32_t x : v) sums[a] += x;
+            }
+            st->n_dist = sums[0];
+            st->n_expand = sums[1];
+            st->n_cand = sums[2];
+            st->n_pred = sums[3];
+            st->n_flood = sums[4];
+            st->search_ms = ms;
+        }
+        return sync(c);
+    }
+    return fail(c, ANQI_ERR_CAPACITY, "rknn search: output capacity could not be satisfied");
+}
+
+int anqi_query_download(anqi_ctx* h, uint32_t* pred_off, uint32_t* pred_ids, uint64_t pred_cap, uint32_t* cand_off,
+                        uint32_t* cand_ids, uint64_t cand_cap, uint32_t* n_dist) {
+    if (!h || !pred_off) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    Batch& b = c->batch;
+    if (!b.have_results) return fail(c, ANQI_ERR_ARGS, "anqi_query_download: no results");
+    ANQI_CUDA(c, cudaMemcpyAsync(pred_off, b.pred_off.p, (b.nq + 1ull) * 4, cudaMemcpyDeviceToHost, c->stream));
+    int rc = sync(c);
+    if (rc) return rc;
+    if (pred_ids && pred_off[b.nq] > pred_cap)
+        return fail(c, ANQI_ERR_CAPACITY, "pred_ids needs %u entries", pred_off[b.nq]);
+    if (pred_ids && pred_off[b.nq])
+        ANQI_CUDA(c, cudaMemcpyAsync(pred_ids, b.pred_csr.p, pred_off[b.nq] * 4ull, cudaMemcpyDeviceToHost, c->stream));
+    if (cand_off) {
+        if (!b.have_cands) return fail(c, ANQI_ERR_ARGS, "candidates were not kept");
+        ANQI_CUDA(c, cudaMemcpyAsync(cand_off, b.cand_off.p, (b.nq + 1ull) * 4, cudaMemcpyDeviceToHost, c->stream));
+        if ((rc = sync(c))) return rc;
+        if (cand_ids && cand_off[b.nq] > cand_cap)
+            return fail(c, ANQI_ERR_CAPACITY, "cand_ids needs %u entries", cand_off[b.nq]);
+        if (cand_ids && cand_off[b.nq])
+            ANQI_CUDA(c, cudaMemcpyAsync(cand_ids, b.cand_csr.p, cand_off[b.nq] * 4ull, cudaMemcpyDeviceToHost,
+                                         c->stream));
+    }
+    if (n_dist) ANQI_CUDA(c, cudaMemcpyAsync(n_dist, b.ndist.p, b.nq * 4ull, cudaMemcpyDeviceToHost, c->stream));
+    return sync(c);
+}
+
+int anqi_rknn_query(anqi_ctx* h, const float* queries, uint32_t nq, const uint32_t* k_per_query, uint32_t k_all,
+                    const uint32_t* L_per_query, uint32_t L_all, uint32_t* pred_off, uint32_t* pred_ids,
+                    uint64_t pred_cap, uint32_t* cand_off, uint32_t* cand_ids, uint64_t cand_cap, uint32_t* n_dist,
+                    anqi_query_stats* st) {
+    if (!h) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    ANQI_CUDA(c, cudaEventRecord(c->ev2, c->stream));
+    int rc = anqi_query_upload(h, queries, nq, k_per_query, k_all, L_per_query, L_all);
+    if (rc) return rc;
+    rc = anqi_query_run(h, cand_off != nullptr, st);
+    if (rc) return rc;
+    rc = anqi_query_download(h, pred_off, pred_ids, pred_cap, cand_off, cand_ids, cand_cap, n_dist);
+    if (rc) return rc;
+    ANQI_CUDA(c, cudaEventRecord(c->ev3, c->stream));
+    if ((rc = sync(c))) return rc;
+    if (st) {
+        float ms = 0;
+        ANQI_CUDA(c, cudaEventElapsedTime(&ms, c->ev2, c->ev3));
+        st->total_ms = ms;
+        st->h2d_bytes = (uint64_t)nq * c->ix.d * 4 + (k_per_query ? nq * 4ull : 0) + (L_per_query ? nq * 4ull : 0);
+        st->d2h_bytes = (nq + 1ull) * 4 + (uint64_t)pred_off[nq] * 4 + (n_dist ? nq * 4ull : 0) +
+                        (cand_off ? (nq + 1ull) * 4 + (uint64_t)cand_off[nq] * 4 : 0);
+    }
+    return ANQI_OK;
+}
+
+int anqi_query_evaluate(anqi_ctx* h, const uint32_t* gt_off, const uint32_t* gt_ids, uint64_t gt_total,
+                        double* recall_sum, double* precision_sum, double* cand_recall_sum, uint32_t* nonempty) {
+    if (!h || !gt_off) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    Batch& b = c->batch;
+    if (!b.have_results) return fail(c, ANQI_ERR_ARGS, "anqi_query_evaluate: no results");
+    if (gt_off[b.nq] != gt_total) return fail(c, ANQI_ERR_ARGS, "ground-truth offsets disagree with gt_total");
+    std::vector<uint32_t> sorted(gt_ids, gt_ids + gt_total);
+    for (uint32_t q = 0; q < b.nq; q++) std::sort(sorted.begin() + gt_off[q], sorted.begin() + gt_off[q + 1]);
+    TmpBuf doff(c), dids(c), dout(c);
+    int rc;
+    if ((rc = h2d(c, doff, gt_off, (b.nq + 1ull) * 4)) || (rc = h2d(c, dids, sorted.data(), gt_total * 4 + 4)) ||
+        (rc = ensure(c, dout, b.nq * 24ull)))
+        return rc;
+    evaluate_kernel<<<c->sm_count * 4, 256, 0, c->stream>>>(
+        b.pred_off.as<uint32_t>(), b.pred_csr.as<uint32_t>(), b.have_cands ? b.cand_off.as<uint32_t>() : nullptr,
+        b.have_cands ? b.cand_csr.as<uint32_t>() : nullptr, doff.as<uint32_t>(), dids.as<uint32_t>(), b.nq,
+        dout.as<double>());
+    ANQI_CUDA(c, cudaGetLastError());
+    std::vector<double> out(b.nq * 3ull);
+    ANQI_CUDA(c, cudaMemcpyAsync(out.data(), dout.p, b.nq * 24ull, cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sync(c))) return rc;
+    double r = 0, p = 0, cr = 0;
+    uint32_t ne = 0;
+    for (uint32_t q = 0; q < b.nq; q++) {
+        if (out[3ull * q] != out[3ull * q]) continue;
+        r += out[3ull * q];
+        p += out[3ull * q + 1];
+        cr += out[3ull * q + 2];
+        ne++;
+    }
+    if (recall_sum) *recall_sum = r;
+    if (precision_sum) *precision_sum = p;
+    if (cand_recall_sum) *cand_recall_sum = cr;
+    if (nonempty) *nonempty = ne;
+    return ANQI_OK;
+}
+
+}  // extern "C"

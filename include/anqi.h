@@ -1,0 +1,241 @@
+/* anqi.h -- C ABI of the B200 (sm_100a) implementation of ANQI's reverse-kNN
+ * hot path.  Plain pointers and sizes only; every function returns a status.
+ *
+ * The reference (Yujian-Fu/anqi-implementation) has no FFI: its boundary is
+ * three CLIs plus prefix files.  Each entry point below replaces one stage of
+ * those CLIs; the comment names the reference code it stands in for.  The CLIs
+ * in anqi-implementation_b200/cli/ and the Python host package call only these
+ * functions.
+ *
+ * Ownership: the caller owns every host buffer; a context owns its device
+ * memory and one CUDA stream.  Threading: one host thread per context.
+ * Errors: no function exits the process; anqi_last_error() describes the last
+ * failure of a context.  Unless a function says "device", all array arguments
+ * are host memory and the call returns after the results are in host memory.
+ */
+#ifndef ANQI_H
+#define ANQI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; 2/3/5 match the reference CLIs' exit codes. */
+#define ANQI_OK 0
+#define ANQI_ERR_ARGS 2        /* bad argument (reference: usage / config error, exit 2) */
+#define ANQI_ERR_FORMAT 3      /* bad input contents (reference: exit 3) */
+#define ANQI_ERR_INVARIANT 5   /* an output failed validation (reference: exit 5) */
+#define ANQI_ERR_DEVICE 7      /* CUDA error or no usable device */
+#define ANQI_ERR_TIMEOUT 8     /* a bounded device wait ran out */
+#define ANQI_ERR_CAPACITY 9    /* a scratch or output capacity was exceeded; retry with more */
+
+#define ANQI_EMPTY 0xFFFFFFFFu /* empty slot / no neighbour */
+
+typedef struct anqi_ctx anqi_ctx;
+
+/* ---------------------------------------------------------------- context */
+int anqi_ctx_create(int device, anqi_ctx** out);
+void anqi_ctx_destroy(anqi_ctx* ctx);
+const char* anqi_last_error(const anqi_ctx* ctx);
+int anqi_version(void);
+/* Bytes of device memory the context currently holds. */
+uint64_t anqi_device_bytes(const anqi_ctx* ctx);
+
+/* ------------------------------------------------------- FP32 distances
+ * Batch forms of include/distance.h:58-161 in the AVX-512 lane order:
+ * out[i] = l2sqr(a_i, b_i) / ip(a_i, b_i) for m pairs of dim floats. */
+int anqi_pair_distances(anqi_ctx* ctx, const float* a, const float* b, uint64_t m, uint32_t dim,
+                        float* l2sqr, float* ip);
+
+/* ------------------------------------------------------------------ LRQ
+ * CompactLrqVerifier::build, floor policy, u8 codes (src/rknn_query.cpp:679-720):
+ * keys n x nk (AKNN cutoffs), mu nk, basis rankm x nk, codebook nk x code_size
+ * (rows ascending) -> coeff n x rankm, codes n x nk. */
+int anqi_lrq_encode(anqi_ctx* ctx, const float* keys, uint64_t n, uint32_t nk, uint32_t rankm,
+                    const float* mu, const float* basis, const float* codebook, uint32_t code_size,
+                    float* coeff, uint8_t* codes);
+/* CompactLrqVerifier::materialize_k (src/rknn_query.cpp:722-753), L2 metric. */
+int anqi_lrq_materialize(anqi_ctx* ctx, const float* coeff, const uint8_t* codes, uint64_t n,
+                         uint32_t nk, uint32_t rankm, const float* mu, const float* basis,
+                         const float* codebook, uint32_t code_size, uint32_t k_one_based,
+                         double radius_scale, float* thr);
+
+/* ----------------------------------------------------------------- lift
+ * The anyk_lift of src/rknn_query.cpp:2203-2235 (L2): base n x d and the
+ * graph-horizon radius (AKNN rank-K cutoff) -> lifted n x (d+2), M*^2, scale. */
+int anqi_lift(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d, const float* radius,
+              float* lifted, double* mstar2, double* scale);
+
+/* ------------------------------------------------------ random projection
+ * RP trees (include/rptrees.h:28-84,127-186) in deterministic breadth-first
+ * form: a counter hash of (seed, tree, node) replaces the reference's
+ * thread-local mt19937.  Outputs per node (n_nodes <= cap_nodes per tree):
+ * left/right child (ANQI_EMPTY on leaves), offset, hyperplane (n_nodes x dim),
+ * leaf_off/leaf_cnt into perm (n per tree).  Tree t's arrays start at
+ * t * cap_nodes (nodes) and t * n (perm); n_nodes[t] receives its node count. */
+int anqi_rp_forest(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, uint32_t trees,
+                   uint32_t leaf_size, uint32_t max_depth, uint64_t seed, uint32_t cap_nodes,
+                   uint32_t* n_nodes, uint32_t* left, uint32_t* right, float* offset,
+                   float* hyperplane, uint32_t* leaf_off, uint32_t* leaf_cnt, uint32_t* perm);
+
+/* --------------------------------------------------------- AKNN source
+ * nndindex::build_approx_knn (include/index.h:1300-1367) as driven by
+ * tools/build_aknn_source.cpp: forest -> init_knn -> [LocalJoin x nn_iters]
+ * -> reverse lists -> gather (queue ef, pool cap max(K, ef_alpha*ef)) ->
+ * per row the K nearest ids != row, ascending.  ids/dists: n x K. */
+typedef struct {
+    uint32_t k;          /* K = 100 */
+    uint32_t leaf;       /* leaf size, 500 */
+    uint32_t trees;      /* 64 */
+    uint32_t ef;         /* explore range, 600 */
+    uint32_t ef_alpha;   /* pool cap multiplier, 8 */
+    uint64_t seed;       /* 10 */
+    uint32_t nn_iters;   /* ANQI_NNITERS, default 0 */
+    uint32_t nn_sample;  /* ANQI_NNSAMPLE, default 20 */
+} anqi_aknn_params;
+
+typedef struct {
+    double total_ms, forest_ms, init_ms, join_ms, reverse_ms, gather_ms;
+    uint64_t join_updates;
+    uint64_t pool_total;
+} anqi_build_stats;
+
+int anqi_aknn_build(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d,
+                    const anqi_aknn_params* p, uint32_t* ids, float* dists, anqi_build_stats* st);
+/* Stage entry points (parity tests at stage boundaries). */
+/* init_knn given leaves (index.h:1433-1460): K nearest unique leaf-mates by (dist, id). */
+int anqi_aknn_init(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint64_t* leaf_off,
+                   const uint32_t* leaf_ids, uint64_t n_leaves, uint32_t K, uint32_t* ids, float* dists);
+/* gather + top-K given a kNN graph (index.h:1347-1366, 1491-1525). */
+int anqi_aknn_gather(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids,
+                     const float* g_vals, uint32_t K, uint32_t ef, uint32_t cap, uint32_t out_k,
+                     uint32_t* ids, float* dists);
+
+/* ----------------------------------------------------------- G48 graph
+ * nndindex::build_index with a flat warm start (include/index.h:1071-1295):
+ * entry RP tree (1 tree, leaf p->leaf) -> warm-start heaps (cap nn_k) from the
+ * first warm_width ids of each row -> LocalJoin rounds (snapshot form, early
+ * exit upd < n/200) -> reverse lists -> gather (queue explore, pool cap
+ * max(M, ef_alpha * explore)) -> alpha-RNG prune -> commit_edges.
+ * Outputs deg (n), links (n x degree, ANQI_EMPTY padded).  The entry tree is
+ * kept in the context; read it with anqi_graph_tree_*. */
+typedef struct {
+    uint32_t degree;       /* M = 48 */
+    uint32_t nn_k;         /* ANQI_LIFTNNK = 50 */
+    uint32_t explore;      /* explore_range = 100 */
+    uint32_t ef_alpha;     /* 8 */
+    uint32_t join_iters;   /* ANQI_GRAPHNND = 6 */
+    uint32_t join_sample;  /* ANQI_NNSAMPLE = 20 */
+    uint32_t leaf;         /* 100 */
+    uint32_t max_depth;    /* 100 */
+    uint64_t seed;         /* 10 */
+    float alpha;           /* ANQI_ALPHA = 1.2 */
+    uint32_t warm_width;   /* 100 */
+} anqi_graph_params;
+
+int anqi_graph_build(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* warm_ids,
+                     uint32_t warm_stride, const anqi_graph_params* p, uint32_t* deg, uint32_t* links,
+                     anqi_build_stats* st);
+/* Entry tree of the last anqi_graph_build, breadth-first arrays (see anqi_rp_forest). */
+int anqi_graph_tree_size(anqi_ctx* ctx, uint32_t* n_nodes, uint64_t* n_points);
+int anqi_graph_tree_copy(anqi_ctx* ctx, uint32_t* left, uint32_t* right, float* offset, float* hyperplane,
+                         uint32_t* leaf_off, uint32_t* leaf_cnt, uint32_t* perm);
+/* Stage entry points. */
+int anqi_graph_warm_start(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* cand,
+                          uint32_t stride, uint32_t width, uint32_t K, uint32_t* ids, float* vals);
+int anqi_graph_localjoin(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, uint32_t K,
+                         uint32_t sample, uint32_t max_rounds, uint32_t* ids, float* vals,
+                         uint64_t* updates /* max_rounds entries */, uint32_t* rounds_done);
+int anqi_graph_select(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids,
+                      const float* g_vals, uint32_t K, uint32_t M, uint32_t ef, uint32_t cap, float alpha,
+                      uint32_t* O, uint32_t* O_deg);
+int anqi_graph_commit(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* O,
+                      const uint32_t* O_deg, uint32_t M, float alpha, uint32_t* links, uint32_t* deg);
+
+/* ------------------------------------------------------- query index
+ * A device-resident copy of what rknn_query holds after index load
+ * (src/rknn_query.cpp:2283-2322): original vectors, lifted vectors, the
+ * fixed-degree adjacency, the entry RP tree, M*^2 and the lift scale. */
+typedef struct {
+    uint64_t n;
+    uint32_t d;                 /* original dimension; lifted is d + 2 */
+    uint32_t degree;            /* link slots per node (M) */
+    const float* base;          /* n x d */
+    const float* lifted;        /* n x (d+2) */
+    const uint32_t* deg;        /* n */
+    const uint32_t* links;      /* n x degree */
+    uint32_t tree_nodes;        /* post-order, root last (the persisted order) */
+    const uint32_t* tree_left;  /* ANQI_EMPTY on leaves */
+    const uint32_t* tree_right;
+    const float* tree_offset;
+    const float* tree_hyperplane; /* tree_nodes x (d+2) */
+    const uint32_t* tree_leaf_first; /* indices[0] of each leaf, ANQI_EMPTY if empty */
+    double scale;
+    double mstar2;
+} anqi_index_desc;
+
+int anqi_index_load(anqi_ctx* ctx, const anqi_index_desc* desc);
+/* The postfilter verifier (LRQ artifact) -> device; materialize thresholds per k. */
+int anqi_verifier_load(anqi_ctx* ctx, const float* coeff, const uint8_t* codes, uint64_t n, uint32_t nk,
+                       uint32_t rankm, const float* mu, const float* basis, const float* codebook,
+                       uint32_t code_size);
+int anqi_verifier_materialize(anqi_ctx* ctx, uint32_t k_one_based, double radius_scale);
+/* Explicit per-object thresholds for k (e.g. exact_f32 mode). */
+int anqi_set_thresholds(anqi_ctx* ctx, uint32_t k_one_based, const float* thr);
+
+/* ------------------------------------------------------------ queries
+ * For every query: lift (rknn_query.cpp:2721-2730), entry by RP-tree descent
+ * (rptrees.h:108-124), greedy beam of width L then bounded flood over
+ * ||q^ - o^||^2 <= M*^2 + 1 (index.h:1535-1640), then the FP32 postfilter
+ * against the k-th materialized threshold (rknn_query.cpp:2555-2561,2762-2765).
+ * Results are CSR: pred_off (nq+1) into pred_ids.  Per query k and L may
+ * differ (k_per_query / L_per_query may be NULL to use k_all / L_all).
+ * cand_* (optional, may be NULL) receive the candidate sets in visit order. */
+typedef struct {
+    uint64_t n_dist;      /* graph distance evaluations, all queries */
+    uint64_t n_expand;    /* beam expansions */
+    uint64_t n_cand;      /* candidates passed to the verifier */
+    uint64_t n_pred;      /* verified results */
+    uint64_t n_flood;     /* flood-phase node expansions */
+    float search_ms;      /* device time of the search kernel (CUDA events on its stream) */
+    float total_ms;       /* device time from first copy to last copy of the call */
+    uint64_t h2d_bytes, d2h_bytes;
+} anqi_query_stats;
+
+int anqi_rknn_query(anqi_ctx* ctx, const float* queries, uint32_t nq, const uint32_t* k_per_query,
+                    uint32_t k_all, const uint32_t* L_per_query, uint32_t L_all, uint32_t* pred_off,
+                    uint32_t* pred_ids, uint64_t pred_cap, uint32_t* cand_off, uint32_t* cand_ids,
+                    uint64_t cand_cap, uint32_t* n_dist, anqi_query_stats* st);
+
+/* Resident-batch form for callers that keep queries and results in HBM:
+ * upload once, run many times (results stay on the device), then download. */
+int anqi_query_upload(anqi_ctx* ctx, const float* queries, uint32_t nq, const uint32_t* k_per_query,
+                      uint32_t k_all, const uint32_t* L_per_query, uint32_t L_all);
+int anqi_query_run(anqi_ctx* ctx, int keep_candidates, anqi_query_stats* st);
+int anqi_query_download(anqi_ctx* ctx, uint32_t* pred_off, uint32_t* pred_ids, uint64_t pred_cap,
+                        uint32_t* cand_off, uint32_t* cand_ids, uint64_t cand_cap, uint32_t* n_dist);
+/* Recall / precision of the resident batch's last results against a
+ * ground-truth CSR (rknn_query.cpp:2784-2799), computed on the device. */
+int anqi_query_evaluate(anqi_ctx* ctx, const uint32_t* gt_off, const uint32_t* gt_ids, uint64_t gt_total,
+                        double* recall_sum, double* precision_sum, double* cand_recall_sum,
+                        uint32_t* nonempty);
+
+/* ---------------------------------------------------- exact ground truth
+ * tools/dataset_gt.cpp:206-313 in FP32 with the reference's summation order:
+ * per base row the K nearest other rows by (key, id), key = |a|^2+|b|^2-2ab. */
+int anqi_exact_topk(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d, uint32_t K,
+                    uint32_t* ids, float* keys);
+/* Reverse-kNN membership: for each query, all j with key(q, j) <= rk2[j],
+ * ascending (key, id).  off: nq+1.  Returns ANQI_ERR_CAPACITY (and the needed
+ * total in *total) when cap is too small. */
+int anqi_rknn_ground_truth(anqi_ctx* ctx, const float* base, uint64_t n, const float* query, uint64_t nq,
+                           uint32_t d, const float* rk2, uint32_t* off, uint32_t* ids, float* keys,
+                           uint64_t cap, uint64_t* total);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ANQI_H */

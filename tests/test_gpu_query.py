@@ -1,0 +1,194 @@
+"""GPU parity of the query path, LRQ codec, lift and distances (sm_100a kernels
+through the C ABI) against the reference's golden outputs and the C oracle.
+Bit-exact: every compared integer is equal and every float has the same bits."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from anqi import formats
+from anqi._lib import Context
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    with Context(0) as c:
+        yield c
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def csr_rows(off, ids):
+    return [ids[int(off[i]):int(off[i + 1])] for i in range(len(off) - 1)]
+
+
+def test_pair_distances_bit_exact(ctx):
+    z = np.load(GOLDEN / "dist.npz")
+    for dim in (8, 10, 16, 32, 34, 128, 130, 962):
+        l2, ip = ctx.pair_distances(z[f"a_{dim}"], z[f"b_{dim}"])
+        assert np.array_equal(bits(l2), bits(z[f"l2_{dim}"])), dim
+        assert np.array_equal(bits(ip), bits(z[f"ip_{dim}"])), dim
+
+
+def test_lrq_bit_exact(ctx, sample):
+    coeff, codes = ctx.lrq_encode(sample["rec_keys"], sample["mu"], sample["basis"], sample["codebook"])
+    assert np.array_equal(bits(coeff), bits(sample["coeff"]))
+    assert np.array_equal(codes, sample["codes"])
+    for i, k in enumerate((1, 10, 50, 100)):
+        thr = ctx.lrq_materialize(coeff, codes, sample["mu"], sample["basis"], sample["codebook"], k)
+        assert np.array_equal(bits(thr), bits(sample["thresholds"][i])), k
+
+
+def test_lrq_random_vs_oracle(ctx):
+    rng = np.random.default_rng(3)
+    n, nk, m = 5003, 100, 8
+    keys = np.sort(rng.gamma(2.0, 10.0, size=(n, nk)).astype(np.float32), axis=1)
+    mu = keys.mean(0).astype(np.float32)
+    basis = np.linalg.qr(rng.normal(size=(nk, m)))[0].T.astype(np.float32)
+    cb = np.sort(rng.normal(scale=3.0, size=(nk, 256)).astype(np.float32), axis=1)
+    c_gpu, k_gpu = ctx.lrq_encode(keys, mu, basis, cb)
+    c_or, k_or = ol.lrq_encode(keys, mu, basis, cb)
+    assert np.array_equal(bits(c_gpu), bits(c_or))
+    assert np.array_equal(k_gpu, k_or)
+    for k in (1, 10, 50, 100):
+        for scale in (1.0, 1.05):
+            a = ctx.lrq_materialize(c_gpu, k_gpu, mu, basis, cb, k, scale)
+            b = ol.lrq_materialize(c_or, k_or, mu, basis, cb, k, scale)
+            assert np.array_equal(bits(a), bits(b))
+
+
+def test_lift_bit_exact(ctx, sample):
+    lifted, m2, sc = ctx.lift(sample["base"], sample["rec_keys"][:, 99])
+    assert sc == float(sample["scale"]) and m2 == float(sample["mstar2"])
+    assert np.array_equal(bits(lifted), bits(sample["lifted"]))
+
+
+def test_lift_random_vs_oracle(ctx):
+    rng = np.random.default_rng(5)
+    base = np.round(rng.uniform(0, 255, size=(20011, 128))).astype(np.float32)
+    radius = rng.gamma(3.0, 1000.0, size=20011).astype(np.float32)
+    a = ctx.lift(base, radius)
+    b = ol.lift(base, radius)
+    assert a[1] == b[1] and a[2] == b[2]
+    assert np.array_equal(bits(a[0]), bits(b[0]))
+
+
+def _load_sample_index(ctx, sample, tmp_path):
+    p = tmp_path / "g.bin"
+    p.write_bytes(sample["graph_file"].tobytes())
+    g = formats.read_graph(p)
+    ctx.index_load(sample["base"], sample["lifted"], g.deg, g.links, g.tree, float(sample["scale"]),
+                   float(sample["mstar2"]))
+    return g
+
+
+def test_query_bit_exact_vs_reference(ctx, sample, tmp_path):
+    """Candidate lists (visit order), #graph_dist and verified lists equal the
+    reference's range_search + postfilter on the reference's own graph."""
+    _load_sample_index(ctx, sample, tmp_path)
+    for ki, k in enumerate((1, 10, 50, 100)):
+        if k == 1:
+            continue
+        ctx.set_thresholds(k, sample["thresholds"][ki])
+        for L in (16, 32, 64, 128):
+            r = ctx.rknn_query(sample["query"], k, L, keep_candidates=True)
+            ref_c = csr_rows(sample[f"q_cand_off_{k}_{L}"], sample[f"q_cand_{k}_{L}"])
+            ref_p = csr_rows(sample[f"q_pred_off_{k}_{L}"], sample[f"q_pred_{k}_{L}"])
+            assert np.array_equal(r.n_dist, sample[f"q_ndist_{k}_{L}"]), (k, L)
+            for i in range(len(ref_c)):
+                assert list(r.cand(i)) == list(ref_c[i]), (k, L, i)
+                assert list(r.pred(i)) == list(ref_p[i]), (k, L, i)
+
+
+def test_query_verifier_materialized_on_device(ctx, sample, tmp_path):
+    _load_sample_index(ctx, sample, tmp_path)
+    ctx.verifier_load(sample["coeff"], sample["codes"], sample["mu"], sample["basis"], sample["codebook"])
+    for k in (10, 50, 100):
+        ctx.verifier_materialize(k)
+    ks = np.array([10, 50, 100] * 11, np.uint32)[:32]
+    Ls = np.array([16, 32, 64, 128] * 8, np.uint32)
+    r = ctx.rknn_query(sample["query"], ks, Ls, keep_candidates=True)
+    for i in range(32):
+        k, L = int(ks[i]), int(Ls[i])
+        ref_p = csr_rows(sample[f"q_pred_off_{k}_{L}"], sample[f"q_pred_{k}_{L}"])
+        assert list(r.pred(i)) == list(ref_p[i]), (i, k, L)
+
+
+def _random_index(n=6000, d=32, nq=300, seed=11):
+    """A G48 index built by the C oracle from an exact-kNN warm start."""
+    rng = np.random.default_rng(seed)
+    centers = rng.normal(scale=4.0, size=(40, d))
+    lab = rng.integers(0, 40, size=n + nq)
+    x = (centers[lab] + rng.normal(size=(n + nq, d))).astype(np.float32)
+    base, query = x[:n], x[n:]
+    nrm = ol.norms(base)
+    d2 = nrm[:, None] + nrm[None, :] - 2.0 * (base.astype(np.float64) @ base.T)
+    np.fill_diagonal(d2, np.inf)
+    knn = np.argsort(d2, axis=1)[:, :100].astype(np.uint32)
+    radius = np.take_along_axis(d2, knn[:, 99:100].astype(np.int64), 1)[:, 0].astype(np.float32)
+    lifted, m2, sc = ol.lift(base, radius)
+    ln = ol.norms(lifted)
+    ids, vals = ol.warm_start(lifted, ln, knn, 100, 50)
+    ids, vals, _ = ol.localjoin(lifted, ln, ids, vals)
+    O, Od = ol.graph_select(lifted, ln, ids, vals)
+    links, deg = ol.graph_commit(lifted, ln, O, Od)
+    t = ol.rp_tree(lifted, 100)
+    tree = formats.bfs_tree_to_postorder(t["left"], t["right"], t["offset"], t["hyperplane"], t["leaf_off"],
+                                        t["leaf_cnt"], t["perm"], 100, d + 2)
+    thr = {k: np.take_along_axis(d2, np.argsort(d2, axis=1)[:, k - 1:k], 1)[:, 0].astype(np.float32)
+           for k in (10, 50, 100)}
+    return base, query, lifted, links, deg, tree, sc, m2, thr
+
+
+@pytest.fixture(scope="module")
+def random_index():
+    return _random_index()
+
+
+def test_query_bit_exact_vs_oracle_random(ctx, random_index):
+    base, query, lifted, links, deg, tree, sc, m2, thr = random_index
+    ctx.index_load(base, lifted, deg, links, tree, sc, m2)
+    ta = ol.TreeArrays(tree.left, tree.right, tree.offset, tree.hyperplane, tree.leaf_first())
+    for k in (10, 100):
+        ctx.set_thresholds(k, thr[k])
+        for L in (8, 48, 200, 1000):
+            r = ctx.rknn_query(query, k, L, keep_candidates=True)
+            cands, preds, nds = ol.range_search_all(lifted, links, deg, base, ta, sc, m2, query, thr[k], L)
+            assert np.array_equal(r.n_dist, nds), (k, L)
+            for i in range(len(query)):
+                assert np.array_equal(r.cand(i), cands[i]), (k, L, i)
+                assert np.array_equal(r.pred(i), preds[i]), (k, L, i)
+
+
+def test_resident_batch_and_evaluate(ctx, random_index):
+    base, query, lifted, links, deg, tree, sc, m2, thr = random_index
+    ctx.index_load(base, lifted, deg, links, tree, sc, m2)
+    ctx.set_thresholds(10, thr[10])
+    ctx.query_upload(query, 10, 64)
+    st1 = ctx.query_run(keep_candidates=True)
+    r1 = ctx.query_download(with_candidates=True)
+    st2 = ctx.query_run(keep_candidates=True)
+    r2 = ctx.query_download(with_candidates=True)
+    assert st1["n_dist"] == st2["n_dist"] and np.array_equal(r1.pred_ids, r2.pred_ids)
+    off, ids, _ = ol.rknn_gt(base, query, thr[10])
+    ev = ctx.query_evaluate(off, ids)
+    # host recomputation
+    rec, prec, ne = 0.0, 0.0, 0
+    for i in range(len(query)):
+        truth = set(ids[off[i]:off[i + 1]].tolist())
+        if not truth:
+            continue
+        pred = set(r1.pred(i).tolist())
+        hit = len(pred & truth)
+        rec += hit / len(truth)
+        prec += 1.0 if not pred else hit / len(pred)
+        ne += 1
+    assert ev["nonempty"] == ne
+    assert abs(ev["recall"] - rec / ne) < 1e-12 and abs(ev["precision"] - prec / ne) < 1e-12
+    assert ev["recall"] > 0.3
