@@ -1,0 +1,1350 @@
+// Index construction: AKNN source (init_knn + gather) and the lifted G48 graph
+// (warm start, LocalJoin, gather + alpha-RNG prune, commit_edges).
+//
+// Reference: include/index.h:1071-1295 (build_index), 1300-1367
+// (build_approx_knn), 1372-1461 (init_knn), 1468-1487 (nndescent_refine),
+// 1491-1525 (gather_candidates), 225-281 + 772-829 (sort_unique_candidates,
+// rng_extend, prune_pool_to_ids), 907-930 (commit_edges); include/heap.h
+// (push_nolock / check_push / push_reverse).
+//
+// Per-row work is one warp; distances are exact FP32 in the AVX lane order
+// (common.cuh), so a stage given the same inputs produces the reference's
+// outputs bit for bit:
+//  * gather: the beam (queue cap ef) is merged batch-wise like the query beam;
+//    the pool is either kept whole (graph: the prune scans it in (dist, id)
+//    order) or reduced to its best K+1 (AKNN: the answer is the K best ids
+//    other than the row).
+//  * init_knn: every row keeps the K smallest unique leaf-mates by (dist, id)
+//    in a sorted list; one launch per tree so each row has one writer.
+//  * LocalJoin: "snapshot" form -- every row samples the first <= S live slots
+//    of its heap at round start; each target heap then receives, in ascending
+//    source order, the other sampled ids of each source that sampled it, and
+//    pushes them with the reference's max-heap semantics.  The reference's
+//    in-place form mutates heaps while other rows sample them, so it is racy
+//    across threads; its outputs are matched statistically.
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+
+#include "internal.h"
+#include "util.cuh"
+
+namespace anqi {
+
+using Clock = std::chrono::steady_clock;
+static double ms_since(Clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+}
+
+// ------------------------------------------------------------ gather
+
+enum GatherMode : int { kModeAknn = 0, kModeSelect = 1, kModeCommit = 2 };
+
+struct GatherParams {
+    const float* x;
+    const float* norms;
+    uint64_t n;
+    uint32_t stride, dim;
+    // forward lists: n x K ids (kEmpty = empty slot) and their stored distances
+    const uint32_t* g_ids;
+    const float* g_vals;
+    uint32_t K;
+    const uint64_t* rev_off;
+    const uint32_t* rev_ids;
+    uint32_t ef, cap;
+    int mode;
+    uint32_t out_k;
+    uint32_t* out_ids;
+    float* out_d;
+    uint32_t M;
+    float alpha;
+    uint32_t* O;       // select output / commit input (n x M)
+    uint32_t* O_deg;
+    uint32_t* links;   // commit output
+    uint32_t* deg;
+    // per-slot scratch
+    uint32_t* vis_bits;
+    uint32_t vis_words;
+    uint32_t* vis_log;
+    uint32_t log_cap;
+    float* pool_d;
+    uint32_t* pool_i;
+    uint32_t pool_cap;  // power of two
+    uint32_t sort_words;  // 2 * kSortSmem in select / commit mode, 0 for AKNN
+    uint32_t* next_row;
+    unsigned long long* pool_total;
+    uint32_t* err;
+};
+
+constexpr uint32_t kSortSmem = 1024;  // pool entries sorted in shared memory per warp
+
+// Distances of batch ids to row i: (n_i + n_j) - 2 ip(x_i, x_j).
+__device__ __forceinline__ void batch_d2(const GatherParams& p, uint64_t i, const uint32_t* ni, float* nd, uint32_t m,
+                                         uint32_t gw, uint32_t gt) {
+    const float* xi = p.x + i * p.stride;
+    const float ni_norm = p.norms[i];
+    for (uint32_t r0 = 0; r0 < m; r0 += 8) {
+        const uint32_t idx = r0 + gw;
+        const bool ok = idx < m;
+        const uint32_t j = ni[ok ? idx : r0];
+        const float ip = group_ip(xi, p.x + (uint64_t)j * p.stride, p.dim, gt, kAll);
+        if (ok && gt == 0) nd[idx] = norm_d2(ni_norm, p.norms[j], ip);
+    }
+    __syncwarp();
+}
+
+// alpha-RNG prune of the sorted candidates (sd/si, m entries, duplicates adjacent)
+// of row i into sel (<= M).  index.h:267-281.
+__device__ uint32_t rng_prune(const GatherParams& p, uint64_t i, const float* sd, const uint32_t* si, uint32_t m,
+                              uint32_t* sel, uint32_t gw, uint32_t gt) {
+    uint32_t nsel = 0;
+    uint32_t prev = kEmpty;
+    for (uint32_t q = 0; q < m && nsel < p.M; q++) {
+        const uint32_t cid = si[q];
+        const float dc = sd[q];
+        if (cid == prev) continue;  // duplicate id (same distance) after sort-unique
+        prev = cid;
+        if (cid == (uint32_t)i || cid >= p.n) continue;
+        bool occluded = false;
+        const float nc = p.norms[cid];
+        const float* xc = p.x + (uint64_t)cid * p.stride;
+        for (uint32_t s0 = 0; s0 < nsel && !occluded; s0 += 8) {
+            const uint32_t j = s0 + gw;
+            const bool ok = j < nsel;
+            const uint32_t sid = sel[ok ? j : s0];
+            const float ip = group_ip(p.x + (uint64_t)sid * p.stride, xc, p.dim, gt, kAll);
+            const float dsc = norm_d2(p.norms[sid], nc, ip);
+            occluded = __any_sync(kAll, ok && __fmul_rn(p.alpha, dsc) < dc);
+        }
+        if (!occluded) {
+            if ((threadIdx.x & 31u) == 0) sel[nsel] = cid;
+            __syncwarp();
+            nsel++;
+        }
+    }
+    __syncwarp();
+    return nsel;
+}
+
+// Sort m pool entries by (dist, id): in shared memory when small, else in the
+// slot's global scratch (pool_cap is a power of two).
+__device__ void sort_pool(float* d, uint32_t* id, uint32_t m, float* sm_d, uint32_t* sm_i, uint32_t cap,
+                          const float** out_d, const uint32_t** out_i) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t np2 = next_pow2(max(m, 2u));
+    const float inf = __int_as_float(0x7f800000);
+    if (np2 <= kSortSmem) {
+        for (uint32_t t = lane; t < np2; t += 32) {
+            sm_d[t] = t < m ? d[t] : inf;
+            sm_i[t] = t < m ? id[t] : kEmpty;
+        }
+        __syncwarp();
+        warp_sort_pairs(sm_d, sm_i, np2);
+        *out_d = sm_d;
+        *out_i = sm_i;
+    } else {
+        for (uint32_t t = m + lane; t < np2 && t < cap; t += 32) {
+            d[t] = inf;
+            id[t] = kEmpty;
+        }
+        __syncwarp();
+        warp_sort_pairs(d, id, min(np2, cap));
+        *out_d = d;
+        *out_i = id;
+    }
+}
+
+extern __shared__ __align__(16) unsigned char g_build_smem[];
+
+__global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
+    const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
+    const uint32_t topk_cap = (p.mode == kModeAknn && p.ef < p.out_k + 1) ? p.out_k + 1 : 0;
+    const size_t per_warp = (size_t)(4 * p.ef + 4 * topk_cap + 128 + 64 + p.sort_words) * 4;
+    unsigned char* my = g_build_smem + wib * per_warp;
+    float* bdA = reinterpret_cast<float*>(my);
+    uint32_t* biA = reinterpret_cast<uint32_t*>(bdA + p.ef);
+    float* bdB = reinterpret_cast<float*>(biA + p.ef);
+    uint32_t* biB = reinterpret_cast<uint32_t*>(bdB + p.ef);
+    float* tdA = reinterpret_cast<float*>(biB + p.ef);
+    uint32_t* tiA = reinterpret_cast<uint32_t*>(tdA + topk_cap);
+    float* tdB = reinterpret_cast<float*>(tiA + topk_cap);
+    uint32_t* tiB = reinterpret_cast<uint32_t*>(tdB + topk_cap);
+    float* nd = reinterpret_cast<float*>(tiB + topk_cap);
+    uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 64);
+    uint32_t* sel = ni + 64;
+    float* sm_d = reinterpret_cast<float*>(sel + 64);
+    uint32_t* sm_i = reinterpret_cast<uint32_t*>(sm_d + kSortSmem);
+    uint32_t* bits = p.vis_bits + (size_t)slot * p.vis_words;
+    uint32_t* vlog = p.vis_log + (size_t)slot * p.log_cap;
+    float* pd = p.pool_d + (size_t)slot * p.pool_cap;
+    uint32_t* pi = p.pool_i + (size_t)slot * p.pool_cap;
+    VisitSlot vs{bits, vlog, p.log_cap, p.vis_words};
+
+    for (;;) {
+        uint32_t row = 0;
+        if (lane == 0) row = atomicAdd(p.next_row, 1u);
+        row = __shfl_sync(kAll, row, 0);
+        if (row >= p.n) break;
+        const uint64_t i = row;
+
+        if (p.mode == kModeCommit) {
+            // cand = O_i + R_i with fresh distances (index.h:921-929)
+            const uint32_t od = p.O_deg[i];
+            const uint64_t r0 = p.rev_off[i], r1 = p.rev_off[i + 1];
+            const uint32_t tot = od + (uint32_t)(r1 - r0);
+            uint32_t np = 0;
+            for (uint32_t c0 = 0; c0 < tot; c0 += 64) {
+                const uint32_t m = min(64u, tot - c0);
+                for (uint32_t t = lane; t < m; t += 32) {
+                    const uint32_t pos = c0 + t;
+                    ni[t] = pos < od ? p.O[i * p.M + pos] : p.rev_ids[r0 + (pos - od)];
+                }
+                __syncwarp();
+                batch_d2(p, i, ni, nd, m, gw, gt);
+                for (uint32_t t = lane; t < m; t += 32) {
+                    if (np + t < p.pool_cap) {
+                        pd[np + t] = nd[t];
+                        pi[np + t] = ni[t];
+                    }
+                }
+                np += m;
+                __syncwarp();
+            }
+            if (np > p.pool_cap) {
+                if (lane == 0) set_error(p.err, kDevPoolOverflow);
+                np = p.pool_cap;
+            }
+            const float* sd;
+            const uint32_t* si;
+            sort_pool(pd, pi, np, sm_d, sm_i, p.pool_cap, &sd, &si);
+            const uint32_t nsel = rng_prune(p, i, sd, si, np, sel, gw, gt);
+            for (uint32_t t = lane; t < p.M; t += 32) p.links[i * p.M + t] = t < nsel ? sel[t] : kEmpty;
+            if (lane == 0) p.deg[i] = nsel;
+            __syncwarp();
+            continue;
+        }
+
+        // ---- gather_candidates, index.h:1491-1525
+        float* bd = bdA;
+        uint32_t* bi = biA;
+        float* od = bdB;
+        uint32_t* oi = biB;
+        float* td = tdA;
+        uint32_t* ti = tiA;
+        float* tod = tdB;
+        uint32_t* toi = tiB;
+        uint32_t size = 0, tsize = 0, nlog = 0;
+        uint64_t npool = 0;
+        // seeds: the row's own list with its stored distances
+        for (uint32_t c0 = 0; c0 < p.K; c0 += 64) {
+            const uint32_t m0 = min(64u, p.K - c0);
+            uint32_t id0 = kEmpty, id1 = kEmpty;
+            bool f0 = false, f1 = false;
+            float v0 = 0.f, v1 = 0.f;
+            if (lane < m0) {
+                id0 = p.g_ids[i * p.K + c0 + lane];
+                v0 = p.g_vals[i * p.K + c0 + lane];
+                f0 = id0 < p.n && visit_first(bits, id0);
+            }
+            if (lane + 32 < m0) {
+                id1 = p.g_ids[i * p.K + c0 + lane + 32];
+                v1 = p.g_vals[i * p.K + c0 + lane + 32];
+                f1 = id1 < p.n && visit_first(bits, id1);
+            }
+            const unsigned b0 = __ballot_sync(kAll, f0), b1 = __ballot_sync(kAll, f1);
+            const uint32_t cnt0 = __popc(b0), lt = lane_lt_mask();
+            const uint32_t q0 = __popc(b0 & lt), q1 = cnt0 + __popc(b1 & lt);
+            if (f0) {
+                ni[q0] = id0;
+                nd[q0] = v0;
+                if (nlog + q0 < p.log_cap) vlog[nlog + q0] = id0;
+            }
+            if (f1) {
+                ni[q1] = id1;
+                nd[q1] = v1;
+                if (nlog + q1 < p.log_cap) vlog[nlog + q1] = id1;
+            }
+            const uint32_t m = cnt0 + __popc(b1);
+            nlog += m;
+            __syncwarp();
+            if (m == 0) continue;
+            if (p.mode == kModeSelect) {
+                for (uint32_t t = lane; t < m; t += 32)
+                    if (npool + t < p.pool_cap) {
+                        pd[npool + t] = nd[t];
+                        pi[npool + t] = ni[t];
+                    }
+            }
+            npool += m;
+            warp_sort_batch64(nd, ni, m);
+            size = warp_merge(bd, bi, size, nd, ni, m, p.ef, od, oi, false);
+            { float* t1 = bd; bd = od; od = t1; uint32_t* t2 = bi; bi = oi; oi = t2; }
+            if (topk_cap) {
+                tsize = warp_merge(td, ti, tsize, nd, ni, m, topk_cap, tod, toi, false);
+                float* t1 = td; td = tod; tod = t1; uint32_t* t2 = ti; ti = toi; toi = t2;
+            }
+        }
+        // expansions
+        for (;;) {
+            uint32_t cur = size;
+            for (uint32_t s0 = 0; s0 < size; s0 += 32) {
+                const uint32_t idx = s0 + lane;
+                const bool un = idx < size && !(bi[idx] & kExpanded);
+                const unsigned b = __ballot_sync(kAll, un);
+                if (b) {
+                    cur = s0 + __ffs(b) - 1;
+                    break;
+                }
+            }
+            if (cur >= size) break;
+            const uint32_t node = bi[cur] & kIdMask;
+            __syncwarp();
+            if (lane == 0) bi[cur] = node | kExpanded;
+            __syncwarp();
+            const uint64_t r0 = p.rev_off[node], r1 = p.rev_off[node + 1];
+            const uint32_t tot = p.K + (uint32_t)(r1 - r0);
+            for (uint32_t c0 = 0; c0 < tot; c0 += 64) {
+                uint32_t id0 = kEmpty, id1 = kEmpty;
+                bool f0 = false, f1 = false;
+                const uint32_t pa = c0 + lane, pb = c0 + lane + 32;
+                if (pa < tot) id0 = pa < p.K ? p.g_ids[(uint64_t)node * p.K + pa] : p.rev_ids[r0 + (pa - p.K)];
+                if (pb < tot) id1 = pb < p.K ? p.g_ids[(uint64_t)node * p.K + pb] : p.rev_ids[r0 + (pb - p.K)];
+                if (id0 < p.n) f0 = visit_first(bits, id0);
+                if (id1 < p.n) f1 = visit_first(bits, id1);
+                const unsigned b0 = __ballot_sync(kAll, f0), b1 = __ballot_sync(kAll, f1);
+                const uint32_t cnt0 = __popc(b0), lt = lane_lt_mask();
+                const uint32_t q0 = __popc(b0 & lt), q1 = cnt0 + __popc(b1 & lt);
+                if (f0) {
+                    ni[q0] = id0;
+                    if (nlog + q0 < p.log_cap) vlog[nlog + q0] = id0;
+                }
+                if (f1) {
+                    ni[q1] = id1;
+                    if (nlog + q1 < p.log_cap) vlog[nlog + q1] = id1;
+                }
+                const uint32_t m = cnt0 + __popc(b1);
+                nlog += m;
+                __syncwarp();
+                if (m == 0) continue;
+                batch_d2(p, i, ni, nd, m, gw, gt);
+                if (p.mode == kModeSelect) {
+                    for (uint32_t t = lane; t < m; t += 32)
+                        if (npool + t < p.pool_cap) {
+                            pd[npool + t] = nd[t];
+                            pi[npool + t] = ni[t];
+                        }
+                }
+                npool += m;
+                warp_sort_batch64(nd, ni, m);
+                size = warp_merge(bd, bi, size, nd, ni, m, p.ef, od, oi, false);
+                { float* t1 = bd; bd = od; od = t1; uint32_t* t2 = bi; bi = oi; oi = t2; }
+                if (topk_cap) {
+                    tsize = warp_merge(td, ti, tsize, nd, ni, m, topk_cap, tod, toi, false);
+                    float* t1 = td; td = tod; tod = t1; uint32_t* t2 = ti; ti = toi; toi = t2;
+                }
+            }
+            if (npool >= p.cap) break;
+        }
+        if (lane == 0) atomicAdd(p.pool_total, (unsigned long long)npool);
+
+        if (p.mode == kModeAknn) {
+            // index.h:1355-1361: sorted pool, first K ids != i
+            const float* ld = topk_cap ? td : bd;
+            const uint32_t* li = topk_cap ? ti : bi;
+            const uint32_t ls = topk_cap ? tsize : size;
+            // position of i (if present) among the first out_k + 1 entries
+            uint32_t self_pos = kEmpty;
+            for (uint32_t t = lane; t < min(ls, p.out_k + 1); t += 32)
+                if ((li[t] & kIdMask) == (uint32_t)i) self_pos = t;
+            for (int o = 16; o > 0; o >>= 1) self_pos = min(self_pos, __shfl_xor_sync(kAll, self_pos, o));
+            for (uint32_t t = lane; t < p.out_k; t += 32) {
+                const uint32_t src = (self_pos != kEmpty && t >= self_pos) ? t + 1 : t;
+                const bool ok = src < ls;
+                p.out_ids[i * p.out_k + t] = ok ? (li[src] & kIdMask) : kEmpty;
+                p.out_d[i * p.out_k + t] = ok ? ld[src] : FLT_MAX;
+            }
+        } else {
+            // prune_pool_to_ids: sort_unique_candidates + rng_extend (index.h:772-829)
+            uint32_t np = (uint32_t)(npool < (uint64_t)p.pool_cap ? npool : (uint64_t)p.pool_cap);
+            if (npool > p.pool_cap && lane == 0) set_error(p.err, kDevPoolOverflow);
+            const float* sd;
+            const uint32_t* si;
+            sort_pool(pd, pi, np, sm_d, sm_i, p.pool_cap, &sd, &si);
+            const uint32_t nsel = rng_prune(p, i, sd, si, np, sel, gw, gt);
+            for (uint32_t t = lane; t < p.M; t += 32) p.O[i * p.M + t] = t < nsel ? sel[t] : kEmpty;
+            if (lane == 0) p.O_deg[i] = nsel;
+        }
+        __syncwarp();
+        visit_clear(vs, nlog);
+    }
+}
+
+// ------------------------------------------------------- warm start
+
+// index.h:1210-1217: heap (cap K) of each row from its first `width` warm ids.
+__global__ void warm_start_kernel(const float* __restrict__ x, const float* __restrict__ norms, uint64_t n,
+                                  uint32_t stride, uint32_t dim, const uint32_t* __restrict__ cand, uint32_t cstride,
+                                  uint32_t width, uint32_t K, uint32_t* __restrict__ hid, float* __restrict__ hval) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
+    const size_t per_warp = (size_t)(2 * width + 2 * K) * 4;
+    uint32_t* cid = reinterpret_cast<uint32_t*>(sm + wib * per_warp);
+    float* cd = reinterpret_cast<float*>(cid + width);
+    uint32_t* hi = reinterpret_cast<uint32_t*>(cd + width);
+    float* hv = reinterpret_cast<float*>(hi + K);
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        for (uint32_t t = lane; t < width; t += 32) cid[t] = cand[i * cstride + t];
+        for (uint32_t t = lane; t < K; t += 32) {
+            hi[t] = kEmpty;
+            hv[t] = FLT_MAX;
+        }
+        __syncwarp();
+        const float* xi = x + i * stride;
+        for (uint32_t r0 = 0; r0 < width; r0 += 8) {
+            const uint32_t idx = r0 + gw;
+            const uint32_t j = idx < width ? cid[idx] : kEmpty;
+            const bool ok = j < n && j != (uint32_t)i;
+            const uint32_t jj = ok ? j : (uint32_t)i;
+            const float ip = group_ip(xi, x + (uint64_t)jj * stride, dim, gt, kAll);
+            if (idx < width && gt == 0) cd[idx] = norm_d2(norms[i], norms[jj], ip);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            for (uint32_t t = 0; t < width; t++) {
+                const uint32_t j = cid[t];
+                if (j != (uint32_t)i && j < n) heap_push(hi, hv, K, j, cd[t]);
+            }
+        }
+        __syncwarp();
+        for (uint32_t t = lane; t < K; t += 32) {
+            hid[i * K + t] = hi[t];
+            hval[i * K + t] = hv[t];
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------ LocalJoin
+
+__global__ void join_sample_kernel(const uint32_t* __restrict__ hid, uint64_t n, uint32_t K, uint32_t S,
+                                   uint32_t* __restrict__ samp, uint32_t* __restrict__ scnt,
+                                   uint32_t* __restrict__ incnt) {
+    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n; u += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t c = 0;
+        for (uint32_t s = 0; s < K && c < S; s++) {
+            const uint32_t v = hid[u * K + s];
+            if (v != kEmpty && v < n) {
+                samp[u * S + c++] = v;
+                atomicAdd(incnt + v, 1u);
+            }
+        }
+        scnt[u] = c;
+    }
+}
+
+__global__ void join_fill_kernel(const uint32_t* __restrict__ samp, const uint32_t* __restrict__ scnt, uint64_t n,
+                                 uint32_t S, const uint64_t* __restrict__ off, uint32_t* __restrict__ fill,
+                                 uint64_t* __restrict__ inc) {
+    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n; u += (uint64_t)gridDim.x * blockDim.x) {
+        for (uint32_t a = 0; a < scnt[u]; a++) {
+            const uint32_t x = samp[u * S + a];
+            const uint32_t pos = atomicAdd(fill + x, 1u);
+            inc[off[x] + pos] = (u << 8) | a;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) join_apply_kernel(const float* __restrict__ x, const float* __restrict__ norms,
+                                                         uint64_t n, uint32_t stride, uint32_t dim,
+                                                         const uint32_t* __restrict__ samp,
+                                                         const uint32_t* __restrict__ scnt, uint32_t S,
+                                                         const uint64_t* __restrict__ off, uint64_t* __restrict__ inc,
+                                                         uint32_t* __restrict__ hid, float* __restrict__ hval, uint32_t K,
+                                                         uint64_t* __restrict__ sort_scratch, uint32_t scratch_cap,
+                                                         unsigned long long* __restrict__ upd, uint32_t* err) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    constexpr uint32_t kIncSmem = 512;
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
+    const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
+    constexpr uint32_t kBatch = 128;
+    const size_t per_warp = (size_t)(2 * kIncSmem + 2 * K + 2 * kBatch) * 4;
+    uint64_t* sinc = reinterpret_cast<uint64_t*>(sm + wib * per_warp);
+    uint32_t* hi = reinterpret_cast<uint32_t*>(sinc + kIncSmem);
+    float* hv = reinterpret_cast<float*>(hi + K);
+    uint32_t* bi = reinterpret_cast<uint32_t*>(hv + K);
+    float* bd = reinterpret_cast<float*>(bi + kBatch);
+    uint64_t* gscr = sort_scratch + (size_t)slot * scratch_cap;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long local_upd = 0;
+    for (uint64_t t = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; t < n; t += nw) {
+        const uint64_t o0 = off[t];
+        const uint32_t s = (uint32_t)(off[t + 1] - o0);
+        if (s == 0) continue;
+        const uint32_t np2 = next_pow2(max(s, 2u));
+        uint64_t* buf;
+        if (np2 <= kIncSmem) buf = sinc;
+        else if (np2 <= scratch_cap) buf = gscr;
+        else {
+            if (lane == 0) set_error(err, kDevSortOverflow);
+            continue;
+        }
+        for (uint32_t k = lane; k < np2; k += 32) buf[k] = k < s ? inc[o0 + k] : ~0ull;
+        __syncwarp();
+        warp_sort_u64(buf, np2);
+        for (uint32_t k = lane; k < K; k += 32) {
+            hi[k] = hid[t * K + k];
+            hv[k] = hval[t * K + k];
+        }
+        __syncwarp();
+        const float* xt = x + t * stride;
+        const float nt = norms[t];
+        uint32_t m = 0;
+        auto flush = [&]() {
+            for (uint32_t r0 = 0; r0 < m; r0 += 8) {
+                const uint32_t idx = r0 + gw;
+                const bool ok = idx < m;
+                const uint32_t w = bi[ok ? idx : r0];
+                const float ip = group_ip(xt, x + (uint64_t)w * stride, dim, gt, kAll);
+                if (ok && gt == 0) bd[idx] = norm_d2(nt, norms[w], ip);
+            }
+            __syncwarp();
+            if (lane == 0)
+                for (uint32_t q = 0; q < m; q++) local_upd += heap_push(hi, hv, K, bi[q], bd[q]);
+            __syncwarp();
+            m = 0;
+        };
+        for (uint32_t e = 0; e < s; e++) {
+            const uint64_t key = buf[e];
+            const uint64_t u = key >> 8;
+            const uint32_t a = (uint32_t)(key & 0xFF);
+            const uint32_t cu = scnt[u];
+            // candidates: the other sampled ids of u, in sample order
+            if (m + cu > kBatch + 1) flush();
+            for (uint32_t b = lane; b < cu; b += 32) {
+                if (b == a) continue;
+                const uint32_t pos = m + (b < a ? b : b - 1);
+                bi[pos] = samp[u * S + b];
+            }
+            __syncwarp();
+            m += cu - 1;
+        }
+        flush();
+        for (uint32_t k = lane; k < K; k += 32) {
+            hid[t * K + k] = hi[k];
+            hval[t * K + k] = hv[k];
+        }
+        __syncwarp();
+    }
+    if (lane == 0 && local_upd) atomicAdd(upd, local_upd);
+}
+
+// ------------------------------------------------------------ reverse CSR
+
+__global__ void count_targets_kernel(const uint32_t* __restrict__ ids, uint64_t n, uint32_t K, uint32_t* __restrict__ cnt) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n * K; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = ids[t];
+        if (v < n) atomicAdd(cnt + v, 1u);
+    }
+}
+
+__global__ void fill_reverse_kernel(const uint32_t* __restrict__ ids, uint64_t n, uint32_t K,
+                                    const uint64_t* __restrict__ off, uint32_t* __restrict__ fill,
+                                    uint32_t* __restrict__ rev) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n * K; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = ids[t];
+        if (v < n) rev[off[v] + atomicAdd(fill + v, 1u)] = (uint32_t)(t / K);
+    }
+}
+
+// ------------------------------------------------------------ init_knn
+
+struct LeafRef {
+    uint64_t off;
+    uint32_t cnt, pad;
+};
+
+constexpr uint32_t kLeafRows = 16;
+
+// CTA (leaf, row block): K smallest unique leaf-mates by (dist, id) merged into
+// each row's sorted list (kd/ki, n x K, size ksz).
+__global__ void __launch_bounds__(256) leaf_topk_kernel(const float* __restrict__ x, const float* __restrict__ norms,
+                                                        uint64_t n, uint32_t stride, uint32_t dim,
+                                                        const uint32_t* __restrict__ ids,
+                                                        const LeafRef* __restrict__ leaves, uint32_t K,
+                                                        uint32_t tile_rows, float* __restrict__ kd,
+                                                        uint32_t* __restrict__ ki, uint32_t* __restrict__ ksz) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const LeafRef lf = leaves[blockIdx.x];
+    const uint32_t rb = blockIdx.y * kLeafRows;
+    if (rb >= lf.cnt) return;
+    const uint32_t rows = min(kLeafRows, lf.cnt - rb);
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
+    const uint32_t nwarp = blockDim.x >> 5;
+    float* rv = reinterpret_cast<float*>(sm);                        // kLeafRows x stride
+    float* tv = rv + (size_t)kLeafRows * stride;                     // tile_rows x stride
+    float* ld = tv + (size_t)tile_rows * stride;                     // 2 x kLeafRows x K
+    uint32_t* li = reinterpret_cast<uint32_t*>(ld + 2 * kLeafRows * K);
+    float* bd = reinterpret_cast<float*>(li + 2 * kLeafRows * K);    // nwarp x 64
+    uint32_t* bi = reinterpret_cast<uint32_t*>(bd + nwarp * 64);
+    uint32_t* tid = bi + nwarp * 64;                                 // tile ids
+    uint32_t* rsz = tid + tile_rows;                                 // row sizes
+    uint32_t* rbuf = rsz + kLeafRows;                                // which half holds the list
+    const uint32_t* mem = ids + lf.off;
+    for (uint32_t t = threadIdx.x; t < rows * stride; t += blockDim.x) {
+        const uint32_t r = t / stride, j = t % stride;
+        rv[t] = x[(uint64_t)mem[rb + r] * stride + j];
+    }
+    for (uint32_t t = threadIdx.x; t < rows * K; t += blockDim.x) {
+        const uint32_t r = t / K, k = t % K;
+        const uint64_t row = mem[rb + r];
+        ld[r * K + k] = kd[row * K + k];
+        li[r * K + k] = ki[row * K + k];
+    }
+    for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) {
+        rsz[r] = ksz[mem[rb + r]];
+        rbuf[r] = 0;
+    }
+    __syncthreads();
+    float* wd = bd + wib * 64;
+    uint32_t* wi = bi + wib * 64;
+    for (uint32_t c0 = 0; c0 < lf.cnt; c0 += tile_rows) {
+        const uint32_t tr = min(tile_rows, lf.cnt - c0);
+        for (uint32_t t = threadIdx.x; t < tr * (stride / 4); t += blockDim.x) {
+            const uint32_t r = t / (stride / 4), q = t % (stride / 4);
+            reinterpret_cast<float4*>(tv)[t] = reinterpret_cast<const float4*>(x + (uint64_t)mem[c0 + r] * stride)[q];
+        }
+        for (uint32_t t = threadIdx.x; t < tr; t += blockDim.x) tid[t] = mem[c0 + t];
+        __syncthreads();
+        for (uint32_t r = wib; r < rows; r += nwarp) {
+            const uint32_t rid = mem[rb + r];
+            const float nr = norms[rid];
+            float* cur_d = ld + (rbuf[r] * kLeafRows + r) * K;
+            uint32_t* cur_i = li + (rbuf[r] * kLeafRows + r) * K;
+            float* alt_d = ld + ((1 - rbuf[r]) * kLeafRows + r) * K;
+            uint32_t* alt_i = li + ((1 - rbuf[r]) * kLeafRows + r) * K;
+            uint32_t size = rsz[r];
+            for (uint32_t b0 = 0; b0 < tr; b0 += 64) {
+                const uint32_t bm = min(64u, tr - b0);
+                // distances for the batch
+                for (uint32_t r0 = 0; r0 < bm; r0 += 8) {
+                    const uint32_t idx = r0 + gw;
+                    const bool ok = idx < bm;
+                    const uint32_t q = b0 + (ok ? idx : r0);
+                    const float ip = group_ip(rv + (size_t)r * stride, tv + (size_t)q * stride, dim, gt, kAll);
+                    if (ok && gt == 0) {
+                        wd[idx] = norm_d2(nr, norms[tid[q]], ip);
+                        wi[idx] = tid[q];
+                    }
+                }
+                __syncwarp();
+                // filter: not self, better than the current K-th
+                uint32_t kept = 0;
+                for (uint32_t s0 = 0; s0 < bm; s0 += 32) {
+                    const uint32_t s = s0 + lane;
+                    bool keep = false;
+                    float dv = 0;
+                    uint32_t iv = 0;
+                    if (s < bm) {
+                        dv = wd[s];
+                        iv = wi[s];
+                        keep = iv != rid && (size < K || nb_less(dv, iv, cur_d[K - 1], cur_i[K - 1]));
+                    }
+                    const unsigned b = __ballot_sync(kAll, keep);
+                    __syncwarp();
+                    if (keep) {
+                        const uint32_t w = kept + __popc(b & lane_lt_mask());
+                        wd[w] = dv;
+                        wi[w] = iv;
+                    }
+                    kept += __popc(b);
+                    __syncwarp();
+                }
+                if (kept == 0) continue;
+                warp_sort_batch64(wd, wi, kept);
+                size = warp_merge(cur_d, cur_i, size, wd, wi, kept, K, alt_d, alt_i, true);
+                float* t1 = cur_d; cur_d = alt_d; alt_d = t1;
+                uint32_t* t2 = cur_i; cur_i = alt_i; alt_i = t2;
+                if (lane == 0) rbuf[r] ^= 1u;
+                __syncwarp();
+            }
+            if (lane == 0) rsz[r] = size;
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+    for (uint32_t t = threadIdx.x; t < rows * K; t += blockDim.x) {
+        const uint32_t r = t / K, k = t % K;
+        const uint64_t row = mem[rb + r];
+        const uint32_t h = rbuf[r];
+        kd[row * K + k] = ld[(h * kLeafRows + r) * K + k];
+        ki[row * K + k] = li[(h * kLeafRows + r) * K + k];
+    }
+    for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) ksz[mem[rb + r]] = rsz[r];
+}
+
+__global__ void init_lists_kernel(float* kd, uint32_t* ki, uint32_t* ksz, uint64_t n, uint32_t K) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n * K; t += (uint64_t)gridDim.x * blockDim.x) {
+        kd[t] = FLT_MAX;
+        ki[t] = kEmpty;
+        if (t < n) ksz[t] = 0;
+    }
+}
+
+// index.h:1452-1460: rows with fewer than K entries get random ids (this
+// project's counter hash instead of mt19937; the id may be the row itself).
+__global__ void random_fill_kernel(const float* __restrict__ x, const float* __restrict__ norms, uint64_t n,
+                                   uint32_t stride, uint32_t dim, uint64_t seed, uint32_t K, float* kd, uint32_t* ki,
+                                   uint32_t* ksz) {
+    const uint32_t lane = threadIdx.x & 31u, gt = lane & 3u;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        uint32_t size = ksz[i];
+        if (size >= K) continue;
+        const uint32_t miss = K - size;
+        float* d = kd + i * K;
+        uint32_t* id = ki + i * K;
+        for (uint32_t t = 0; t < miss; t++) {
+            const uint32_t r = (uint32_t)(hash64(hash64(seed + 0x51ED270Bull) ^ (i << 20) ^ t) % n);
+            const float ip = group_ip(x + i * stride, x + (uint64_t)r * stride, dim, gt, kAll);
+            const float v = norm_d2(norms[i], norms[r], ip);
+            bool dup = false;
+            for (uint32_t s = lane; s < size; s += 32) dup |= id[s] == r;
+            dup = __any_sync(kAll, dup);
+            if (!dup && (size < K || nb_less(v, r, d[K - 1], id[K - 1]))) {
+                if (lane == 0) {
+                    uint32_t pos = size < K ? size : K - 1;
+                    while (pos > 0 && nb_less(v, r, d[pos - 1], id[pos - 1])) {
+                        d[pos] = d[pos - 1];
+                        id[pos] = id[pos - 1];
+                        pos--;
+                    }
+                    d[pos] = v;
+                    id[pos] = r;
+                }
+                if (size < K) size++;
+            }
+            __syncwarp();
+        }
+        if (lane == 0) ksz[i] = size;
+    }
+}
+
+// sorted ascending list -> descending array, a valid max-heap (parents >= children)
+__global__ void list_to_heap_kernel(const float* kd, const uint32_t* ki, const uint32_t* ksz, uint64_t n, uint32_t K,
+                                    float* hv, uint32_t* hi) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n * K; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = t / K;
+        const uint32_t k = (uint32_t)(t % K), s = ksz[i];
+        // heap slot k holds the (K-1-k)-th smallest; empty slots first (FLT_MAX)
+        const uint32_t src = K - 1 - k;
+        hv[t] = src < s ? kd[i * K + src] : FLT_MAX;
+        hi[t] = src < s ? ki[i * K + src] : kEmpty;
+    }
+}
+
+// ------------------------------------------------------------ host side
+
+struct Dev {
+    Ctx* c;
+    explicit Dev(Ctx* ctx) : c(ctx) {}
+};
+
+static int upload_rows(Ctx* c, DevBuf& dx, DevBuf& dn, const float* x, uint64_t n, uint32_t dim, uint32_t stride) {
+    int rc = upload_padded(c, dx, x, n, dim, stride);
+    if (rc) return rc;
+    if ((rc = ensure(c, dn, n * 4))) return rc;
+    return compute_norms_device(c, dx.as<float>(), n, dim, stride, dn.as<float>());
+}
+
+static int build_reverse(Ctx* c, const uint32_t* d_ids, uint64_t n, uint32_t K, DevBuf& off, DevBuf& rev) {
+    TmpBuf cnt(c), fill(c);
+    int rc;
+    if ((rc = ensure(c, cnt, n * 4)) || (rc = ensure(c, fill, n * 4)) || (rc = ensure(c, off, (n + 1) * 8))) return rc;
+    ANQI_CUDA(c, cudaMemsetAsync(cnt.p, 0, n * 4, c->stream));
+    ANQI_CUDA(c, cudaMemsetAsync(fill.p, 0, n * 4, c->stream));
+    const int blocks = c->sm_count * 8;
+    count_targets_kernel<<<blocks, 256, 0, c->stream>>>(d_ids, n, K, cnt.as<uint32_t>());
+    ANQI_CUDA(c, cudaGetLastError());
+    if ((rc = device_scan(c, cnt.as<uint32_t>(), off.as<uint64_t>(), n))) return rc;
+    uint64_t total = 0;
+    ANQI_CUDA(c, cudaMemcpy(&total, off.as<uint64_t>() + n, 8, cudaMemcpyDeviceToHost));
+    if ((rc = ensure(c, rev, total * 4 + 4))) return rc;
+    fill_reverse_kernel<<<blocks, 256, 0, c->stream>>>(d_ids, n, K, off.as<uint64_t>(), fill.as<uint32_t>(),
+                                                      rev.as<uint32_t>());
+    ANQI_CUDA(c, cudaGetLastError());
+    return sync(c);
+}
+
+static uint64_t max_reverse(Ctx* c, const DevBuf& off, uint64_t n) {
+    std::vector<uint64_t> h(n + 1);
+    cudaMemcpy(h.data(), off.p, (n + 1) * 8, cudaMemcpyDeviceToHost);
+    uint64_t m = 0;
+    for (uint64_t i = 0; i < n; i++) m = std::max(m, h[i + 1] - h[i]);
+    return m;
+}
+
+// Runs gather_kernel over all rows.
+static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_total) {
+    const int warps_per_block = 4;
+    const uint32_t topk_cap = (p.mode == kModeAknn && p.ef < p.out_k + 1) ? p.out_k + 1 : 0;
+    p.sort_words = p.mode == kModeAknn ? 0 : 2 * kSortSmem;
+    const size_t per_warp = (size_t)(4 * p.ef + 4 * topk_cap + 128 + 64 + p.sort_words) * 4;
+    const size_t smem = per_warp * warps_per_block;
+    if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "explore range %u too large", p.ef);
+    ANQI_CUDA(c, cudaFuncSetAttribute(gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_kernel, 32 * warps_per_block, smem));
+    if (per_sm < 1) return fail(c, ANQI_ERR_DEVICE, "gather kernel does not fit on an SM");
+    uint32_t blocks = std::min<uint64_t>((uint64_t)per_sm * c->sm_count, (p.n + warps_per_block - 1) / warps_per_block);
+    const uint32_t slots = blocks * warps_per_block;
+    const uint32_t words = (uint32_t)((p.n + 31) / 32);
+    const uint32_t log_cap = (uint32_t)std::min<uint64_t>(p.n, 32768);
+    uint64_t need = (uint64_t)p.cap + p.K + max_rev + 64;
+    if (p.mode == kModeCommit) need = p.M + max_rev + 64;
+    const uint32_t pool_cap = p.mode == kModeAknn ? 1u : (uint32_t)std::min<uint64_t>(1ull << 30, 1ull << (64 - __builtin_clzll(need)));
+    TmpBuf bits(c), vlog(c), pd(c), pi(c);
+    int rc;
+    if ((rc = ensure(c, bits, (size_t)slots * words * 4)) || (rc = ensure(c, vlog, (size_t)slots * log_cap * 4)) ||
+        (rc = ensure(c, pd, (size_t)slots * pool_cap * 4)) || (rc = ensure(c, pi, (size_t)slots * pool_cap * 4)))
+        return rc;
+    ANQI_CUDA(c, cudaMemsetAsync(bits.p, 0, (size_t)slots * words * 4, c->stream));
+    ANQI_CUDA(c, cudaMemsetAsync(c->counters.p, 0, 64, c->stream));
+    p.vis_bits = bits.as<uint32_t>();
+    p.vis_words = words;
+    p.vis_log = vlog.as<uint32_t>();
+    p.log_cap = log_cap;
+    p.pool_d = pd.as<float>();
+    p.pool_i = pi.as<uint32_t>();
+    p.pool_cap = pool_cap;
+    p.next_row = c->counters.as<uint32_t>();
+    p.pool_total = reinterpret_cast<unsigned long long*>(c->counters.as<uint32_t>() + 2);
+    p.err = c->err.as<uint32_t>();
+    gather_kernel<<<blocks, 32 * warps_per_block, smem, c->stream>>>(p);
+    ANQI_CUDA(c, cudaGetLastError());
+    if ((rc = check_device_error(c, "gather"))) return rc;
+    if (pool_total) ANQI_CUDA(c, cudaMemcpy(pool_total, p.pool_total, 8, cudaMemcpyDeviceToHost));
+    return ANQI_OK;
+}
+
+static GatherParams base_params(const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim) {
+    GatherParams p{};
+    p.x = dx.as<float>();
+    p.norms = dn.as<float>();
+    p.n = n;
+    p.stride = stride;
+    p.dim = dim;
+    return p;
+}
+
+// LocalJoin rounds on device heaps; returns rounds done and update counts.
+static int run_localjoin(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
+                         DevBuf& hid, DevBuf& hval, uint32_t K, uint32_t S, uint32_t max_rounds,
+                         std::vector<uint64_t>& updates) {
+    if (S > 120) S = 120;  // index.h:1470
+    TmpBuf samp(c), scnt(c), incnt(c), off(c), fill(c), inc(c), scratch(c), upd(c);
+    int rc;
+    if ((rc = ensure(c, samp, n * S * 4)) || (rc = ensure(c, scnt, n * 4)) || (rc = ensure(c, incnt, n * 4)) ||
+        (rc = ensure(c, off, (n + 1) * 8)) || (rc = ensure(c, fill, n * 4)) || (rc = ensure(c, upd, 8)))
+        return rc;
+    const int blocks = c->sm_count * 8;
+    for (uint32_t it = 0; it < max_rounds; it++) {
+        ANQI_CUDA(c, cudaMemsetAsync(incnt.p, 0, n * 4, c->stream));
+        ANQI_CUDA(c, cudaMemsetAsync(fill.p, 0, n * 4, c->stream));
+        ANQI_CUDA(c, cudaMemsetAsync(upd.p, 0, 8, c->stream));
+        join_sample_kernel<<<blocks, 256, 0, c->stream>>>(hid.as<uint32_t>(), n, K, S, samp.as<uint32_t>(),
+                                                         scnt.as<uint32_t>(), incnt.as<uint32_t>());
+        ANQI_CUDA(c, cudaGetLastError());
+        if ((rc = device_scan(c, incnt.as<uint32_t>(), off.as<uint64_t>(), n))) return rc;
+        std::vector<uint64_t> hoff(n + 1);
+        ANQI_CUDA(c, cudaMemcpy(hoff.data(), off.p, (n + 1) * 8, cudaMemcpyDeviceToHost));
+        uint64_t maxin = 0;
+        for (uint64_t i = 0; i < n; i++) maxin = std::max(maxin, hoff[i + 1] - hoff[i]);
+        if ((rc = ensure(c, inc, hoff[n] * 8 + 8))) return rc;
+        join_fill_kernel<<<blocks, 256, 0, c->stream>>>(samp.as<uint32_t>(), scnt.as<uint32_t>(), n, S,
+                                                       off.as<uint64_t>(), fill.as<uint32_t>(), inc.as<uint64_t>());
+        ANQI_CUDA(c, cudaGetLastError());
+        const int wpb = 4;
+        const size_t smem = (size_t)(2 * 512 + 2 * K + 2 * 128) * 4 * wpb;
+        ANQI_CUDA(c, cudaFuncSetAttribute(join_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, join_apply_kernel, 32 * wpb, smem));
+        const uint32_t jb = std::max(1, per_sm) * c->sm_count;
+        const uint32_t scratch_cap = maxin > 512 ? (uint32_t)(1ull << (64 - __builtin_clzll(maxin - 1))) : 1;
+        if ((rc = ensure(c, scratch, (size_t)jb * wpb * scratch_cap * 8))) return rc;
+        join_apply_kernel<<<jb, 32 * wpb, smem, c->stream>>>(dx.as<float>(), dn.as<float>(), n, stride, dim,
+                                                             samp.as<uint32_t>(), scnt.as<uint32_t>(), S,
+                                                             off.as<uint64_t>(), inc.as<uint64_t>(), hid.as<uint32_t>(),
+                                                             hval.as<float>(), K, scratch.as<uint64_t>(), scratch_cap,
+                                                             upd.as<unsigned long long>(), c->err.as<uint32_t>());
+        ANQI_CUDA(c, cudaGetLastError());
+        if ((rc = check_device_error(c, "localjoin"))) return rc;
+        uint64_t u = 0;
+        ANQI_CUDA(c, cudaMemcpy(&u, upd.p, 8, cudaMemcpyDeviceToHost));
+        updates.push_back(u);
+        if (u < n / 200) break;  // index.h:1485
+    }
+    return ANQI_OK;
+}
+
+static int run_warm_start(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
+                          const uint32_t* d_cand, uint32_t cstride, uint32_t width, uint32_t K, DevBuf& hid,
+                          DevBuf& hval) {
+    int rc;
+    if ((rc = ensure(c, hid, n * K * 4)) || (rc = ensure(c, hval, n * K * 4))) return rc;
+    const int wpb = 4;
+    const size_t smem = (size_t)(2 * width + 2 * K) * 4 * wpb;
+    ANQI_CUDA(c, cudaFuncSetAttribute(warm_start_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    warm_start_kernel<<<c->sm_count * 8, 32 * wpb, smem, c->stream>>>(dx.as<float>(), dn.as<float>(), n, stride, dim,
+                                                                      d_cand, cstride, width, K, hid.as<uint32_t>(),
+                                                                      hval.as<float>());
+    ANQI_CUDA(c, cudaGetLastError());
+    return sync(c);
+}
+
+static int run_select_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
+                             const DevBuf& hid, const DevBuf& hval, uint32_t K, uint32_t M, uint32_t ef, uint32_t cap,
+                             float alpha, DevBuf& O, DevBuf& Odeg, DevBuf* links, DevBuf* deg, uint64_t* pool_total) {
+    TmpBuf roff(c), rev(c);
+    int rc = build_reverse(c, hid.as<uint32_t>(), n, K, roff, rev);
+    if (rc) return rc;
+    const uint64_t mr = max_reverse(c, roff, n);
+    if ((rc = ensure(c, O, n * M * 4)) || (rc = ensure(c, Odeg, n * 4))) return rc;
+    GatherParams p = base_params(dx, dn, n, stride, dim);
+    p.g_ids = hid.as<uint32_t>();
+    p.g_vals = hval.as<float>();
+    p.K = K;
+    p.rev_off = roff.as<uint64_t>();
+    p.rev_ids = rev.as<uint32_t>();
+    p.ef = ef;
+    p.cap = cap;
+    p.mode = kModeSelect;
+    p.M = M;
+    p.alpha = alpha;
+    p.O = O.as<uint32_t>();
+    p.O_deg = Odeg.as<uint32_t>();
+    if ((rc = run_gather(c, p, mr, pool_total))) return rc;
+    if (!links) return ANQI_OK;
+    TmpBuf roff2(c), rev2(c);
+    if ((rc = build_reverse(c, O.as<uint32_t>(), n, M, roff2, rev2))) return rc;
+    const uint64_t mr2 = max_reverse(c, roff2, n);
+    if ((rc = ensure(c, *links, n * M * 4)) || (rc = ensure(c, *deg, n * 4))) return rc;
+    GatherParams q = base_params(dx, dn, n, stride, dim);
+    q.mode = kModeCommit;
+    q.K = 1;
+    q.ef = 4;
+    q.M = M;
+    q.alpha = alpha;
+    q.O = O.as<uint32_t>();
+    q.O_deg = Odeg.as<uint32_t>();
+    q.rev_off = roff2.as<uint64_t>();
+    q.rev_ids = rev2.as<uint32_t>();
+    q.links = links->as<uint32_t>();
+    q.deg = deg->as<uint32_t>();
+    return run_gather(c, q, mr2, nullptr);
+}
+
+// init_knn over leaves; lists kd/ki/ksz already initialised.
+static int run_leaf_topk(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
+                         const uint32_t* d_ids, const std::vector<LeafRef>& leaves, uint32_t K, DevBuf& kd, DevBuf& ki,
+                         DevBuf& ksz) {
+    if (leaves.empty()) return ANQI_OK;
+    uint32_t maxcnt = 0;
+    for (const LeafRef& l : leaves) maxcnt = std::max(maxcnt, l.cnt);
+    uint32_t tile_rows = std::min<uint32_t>(64, std::max<uint32_t>(8, (48 * 1024) / (stride * 4)) / 8 * 8);
+    const uint32_t nwarp = 8;
+    const size_t smem = ((size_t)kLeafRows * stride + (size_t)tile_rows * stride + 4 * (size_t)kLeafRows * K +
+                         2 * nwarp * 64 + tile_rows + 2 * kLeafRows) * 4;
+    if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "init_knn tile does not fit (dim %u, K %u)", dim, K);
+    ANQI_CUDA(c, cudaFuncSetAttribute(leaf_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TmpBuf dl(c);
+    int rc = h2d(c, dl, leaves.data(), leaves.size() * sizeof(LeafRef));
+    if (rc) return rc;
+    dim3 grid((unsigned)leaves.size(), (maxcnt + kLeafRows - 1) / kLeafRows);
+    leaf_topk_kernel<<<grid, 32 * nwarp, smem, c->stream>>>(dx.as<float>(), dn.as<float>(), n, stride, dim, d_ids,
+                                                            dl.as<LeafRef>(), K, tile_rows, kd.as<float>(),
+                                                            ki.as<uint32_t>(), ksz.as<uint32_t>());
+    ANQI_CUDA(c, cudaGetLastError());
+    return sync(c);
+}
+
+static int init_lists(Ctx* c, DevBuf& kd, DevBuf& ki, DevBuf& ksz, uint64_t n, uint32_t K) {
+    int rc;
+    if ((rc = ensure(c, kd, n * K * 4)) || (rc = ensure(c, ki, n * K * 4)) || (rc = ensure(c, ksz, n * 4))) return rc;
+    init_lists_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(kd.as<float>(), ki.as<uint32_t>(), ksz.as<uint32_t>(), n, K);
+    ANQI_CUDA(c, cudaGetLastError());
+    return ANQI_OK;
+}
+
+}  // namespace anqi
+
+using namespace anqi;
+
+extern "C" {
+
+int anqi_graph_warm_start(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* cand, uint32_t stride,
+                          uint32_t width, uint32_t K, uint32_t* ids, float* vals) {
+    if (!h || !x || !cand || !ids || !vals || n == 0 || dim == 0 || K == 0 || width > stride || width > 4096)
+        return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    const uint32_t xs = round_up(dim, 8);
+    TmpBuf dx(c), dn(c), dc(c), hid(c), hv(c);
+    int rc;
+    if ((rc = upload_rows(c, dx, dn, x, n, dim, xs)) || (rc = h2d(c, dc, cand, n * stride * 4ull)) ||
+        (rc = run_warm_start(c, dx, dn, n, xs, dim, dc.as<uint32_t>(), stride, width, K, hid, hv)) ||
+        (rc = d2h(c, ids, hid, n * K * 4)) || (rc = d2h(c, vals, hv, n * K * 4)))
+        return rc;
+    return sync(c);
+}
+
+int anqi_graph_localjoin(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, uint32_t K, uint32_t sample,
+                         uint32_t max_rounds, uint32_t* ids, float* vals, uint64_t* updates, uint32_t* rounds_done) {
+    if (!h || !x || !ids || !vals || n == 0 || dim == 0 || K == 0) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    const uint32_t xs = round_up(dim, 8);
+    TmpBuf dx(c), dn(c), hid(c), hv(c);
+    int rc;
+    if ((rc = upload_rows(c, dx, dn, x, n, dim, xs)) || (rc = h2d(c, hid, ids, n * K * 4)) ||
+        (rc = h2d(c, hv, vals, n * K * 4)))
+        return rc;
+    std::vector<uint64_t> up;
+    if ((rc = run_localjoin(c, dx, dn, n, xs, dim, hid, hv, K, sample, max_rounds, up))) return rc;
+    if (updates)
+        for (size_t i = 0; i < up.size(); i++) updates[i] = up[i];
+    if (rounds_done) *rounds_done = (uint32_t)up.size();
+    if ((rc = d2h(c, ids, hid, n * K * 4)) || (rc = d2h(c, vals, hv, n * K * 4))) return rc;
+    return sync(c);
+}
+
+int anqi_graph_select(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids,
+                      const float* g_vals, uint32_t K, uint32_t M, uint32_t ef, uint32_t cap, float alpha, uint32_t* O,
+                      uint32_t* O_deg) {
+    if (!h || !x || !g_ids || !g_vals || !O || !O_deg || n == 0 || M == 0 || M > 64 || ef == 0) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    const uint32_t xs = round_up(dim, 8);
+    TmpBuf dx(c), dn(c), hid(c), hv(c), dO(c), dOd(c);
+    int rc;
+    if ((rc = upload_rows(c, dx, dn, x, n, dim, xs)) || (rc = h2d(c, hid, g_ids, n * K * 4)) ||
+        (rc = h2d(c, hv, g_vals, n * K * 4)) ||
+        (rc = run_select_commit(c, dx, dn, n, xs, dim, hid, hv, K, M, ef, cap, alpha, dO, dOd, nullptr, nullptr,
+                                nullptr)) ||
+        (rc = d2h(c, O, dO, n * M * 4)) || (rc = d2h(c, O_deg, dOd, n * 4)))
+        return rc;
+    return sync(c);
+}
+
+int anqi_graph_commit(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* O, const uint32_t* O_deg,
+                      uint32_t M, float alpha, uint32_t* links, uint32_t* deg) {
+    if (!h || !x || !O || !O_deg || !links || !deg || n == 0 || M == 0 || M > 64) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    const uint32_t xs = round_up(dim, 8);
+    TmpBuf dx(c), dn(c), dO(c), dOd(c), roff(c), rev(c), dl(c), dd(c);
+    int rc;
+    if ((rc = upload_rows(c, dx, dn, x, n, dim, xs)) || (rc = h2d(c, dO, O, n * M * 4)) ||
+        (rc = h2d(c, dOd, O_deg, n * 4)) || (rc = build_reverse(c, dO.as<uint32_t>(), n, M, roff, rev)) ||
+        (rc = ensure(c, dl, n * M * 4)) || (rc = ensure(c, dd, n * 4)))
+        return rc;
+    GatherParams q = base_params(dx, dn, n, xs, dim);
+    q.mode = kModeCommit;
+    q.K = 1;
+    q.ef = 4;
+    q.M = M;
+    q.alpha = alpha;
+    q.O = dO.as<uint32_t>();
+    q.O_deg = dOd.as<uint32_t>();
+    q.rev_off = roff.as<uint64_t>();
+    q.rev_ids = rev.as<uint32_t>();
+    q.links = dl.as<uint32_t>();
+    q.deg = dd.as<uint32_t>();
+    if ((rc = run_gather(c, q, max_reverse(c, roff, n), nullptr))) return rc;
+    if ((rc = d2h(c, links, dl, n * M * 4)) || (rc = d2h(c, deg, dd, n * 4))) return rc;
+    return sync(c);
+}
+
+int anqi_graph_build(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* warm_ids,
+                     uint32_t warm_stride, const anqi_graph_params* gp, uint32_t* deg, uint32_t* links,
+                     anqi_build_stats* st) {
+    if (!h || !x || !warm_ids || !gp || !deg || !links || n < 2 || dim == 0 || gp->degree == 0 || gp->degree > 64 ||
+        gp->nn_k == 0 || gp->nn_k > 256 || gp->warm_width > warm_stride || gp->leaf == 0)
+        return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    const auto t0 = Clock::now();
+    const uint32_t xs = round_up(dim, 8);
+    TmpBuf dx(c), dn(c), dw(c), hid(c), hv(c), dO(c), dOd(c), dl(c), dd(c);
+    int rc;
+    if ((rc = upload_rows(c, dx, dn, x, n, dim, xs)) || (rc = h2d(c, dw, warm_ids, n * warm_stride * 4ull))) return rc;
+    // entry tree: make_forest with one tree (index.h:1111-1120)
+    auto t = Clock::now();
+    ForestOut f;
+    const uint32_t cap_nodes = (uint32_t)std::min<uint64_t>(4 * n + 8, 0xFFFFFFF0ull);
+    rc = build_forest(c, dx.as<float>(), n, dim, xs, 1, gp->leaf, gp->max_depth ? gp->max_depth : 100, gp->seed,
+                      cap_nodes, f);
+    if (rc) {
+        release(c, f.perm);
+        release(c, f.hyper);
+        return rc;
+    }
+    c->t_nodes = f.n_nodes[0];
+    c->t_left.assign(f.left.begin(), f.left.begin() + c->t_nodes);
+    c->t_right.assign(f.right.begin(), f.right.begin() + c->t_nodes);
+    c->t_offset.assign(f.offset.begin(), f.offset.begin() + c->t_nodes);
+    c->t_leaf_off.assign(f.leaf_off.begin(), f.leaf_off.begin() + c->t_nodes);
+    c->t_leaf_cnt.assign(f.leaf_cnt.begin(), f.leaf_cnt.begin() + c->t_nodes);
+    c->t_hyper.resize((size_t)c->t_nodes * dim);
+    c->t_perm.resize(n);
+    c->t_dim = dim;
+    cudaMemcpy2D(c->t_hyper.data(), dim * 4, f.hyper.p, xs * 4, dim * 4, c->t_nodes, cudaMemcpyDeviceToHost);
+    cudaMemcpy(c->t_perm.data(), f.perm.p, n * 4, cudaMemcpyDeviceToHost);
+    for (uint32_t v = 0; v < c->t_nodes; v++)
+        if (c->t_left[v] == kEmpty) std::memset(c->t_hyper.data() + (size_t)v * dim, 0, dim * 4);
+    release(c, f.perm);
+    release(c, f.hyper);
+    const double forest_ms = ms_since(t);
+    t = Clock::now();
+    if ((rc = run_warm_start(c, dx, dn, n, xs, dim, dw.as<uint32_t>(), warm_stride, gp->warm_width, gp->nn_k, hid, hv)))
+        return rc;
+    const double init_ms = ms_since(t);
+    t = Clock::now();
+    std::vector<uint64_t> up;
+    if ((rc = run_localjoin(c, dx, dn, n, xs, dim, hid, hv, gp->nn_k, gp->join_sample ? gp->join_sample : 20,
+                            gp->join_iters, up)))
+        return rc;
+    const double join_ms = ms_since(t);
+    t = Clock::now();
+    uint64_t pool_total = 0;
+    const uint32_t cap = std::max<uint32_t>(gp->degree, gp->ef_alpha * gp->explore);
+    if ((rc = run_select_commit(c, dx, dn, n, xs, dim, hid, hv, gp->nn_k, gp->degree, gp->explore, cap, gp->alpha, dO,
+                                dOd, &dl, &dd, &pool_total)))
+        return rc;
+    const double gather_ms = ms_since(t);
+    if ((rc = d2h(c, links, dl, n * gp->degree * 4ull)) || (rc = d2h(c, deg, dd, n * 4)) || (rc = sync(c))) return rc;
+    if (st) {
+        st->forest_ms = forest_ms;
+        st->init_ms = init_ms;
+        st->join_ms = join_ms;
+        st->reverse_ms = 0;
+        st->gather_ms = gather_ms;
+        st->total_ms = ms_since(t0);
+        uint64_t tot = 0;
+        for (uint64_t u : up) tot += u;
+        st->join_updates = tot;
+        st->pool_total = pool_total;
+    }
+    return ANQI_OK;
+}
+
+int anqi_graph_tree_size(anqi_ctx* h, uint32_t* n_nodes, uint64_t* n_points) {
+    if (!h || !n_nodes || !n_points) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    if (c->t_nodes == 0) return fail(c, ANQI_ERR_ARGS, "no graph built in this context");
+    *n_nodes = c->t_nodes;
+    *n_points = c->t_perm.size();
+    return ANQI_OK;
+}
+
+int anqi_graph_tree_copy(anqi_ctx* h, uint32_t* left, uint32_t* right, float* offset, float* hyperplane,
+                         uint32_t* leaf_off, uint32_t* leaf_cnt, uint32_t* perm) {
+    if (!h || !left || !right || !offset || !hyperplane || !leaf_off || !leaf_cnt || !perm) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    if (c->t_nodes == 0) return fail(c, ANQI_ERR_ARGS, "no graph built in this context");
+    std::memcpy(left, c->t_left.data(), c->t_nodes * 4);
+    std::memcpy(right, c->t_right.data(), c->t_nodes * 4);
+    std::memcpy(offset, c->t_offset.data(), c->t_nodes * 4);
+    std::memcpy(hyperplane, c->t_hyper.data(), c->t_hyper.size() * 4);
+    std::memcpy(leaf_off, c->t_leaf_off.data(), c->t_nodes * 4);
+    std::memcpy(leaf_cnt, c->t_leaf_cnt.data(), c->t_nodes * 4);
+    std::memcpy(perm, c->t_perm.data(), c->t_perm.size() * 4);
+    return ANQI_OK;
+}
+
+int anqi_aknn_init(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint64_t* leaf_off,
+                   const uint32_t* leaf_ids, uint64_t n_leaves, uint32_t K, uint32_t* ids, float* dists) {
+    if (!h || !x || !leaf_off || !leaf_ids || !ids || !dists || n == 0 || dim == 0 || K == 0 || K > 256)
+        return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    const uint32_t xs = round_up(dim, 8);
+    TmpBuf dx(c), dn(c), dids(c), kd(c), ki(c), ksz(c);
+    int rc;
+    const uint64_t tot = leaf_off[n_leaves];
+    if ((rc = upload_rows(c, dx, dn, x, n, dim, xs)) || (rc = h2d(c, dids, leaf_ids, tot * 4 + 4)) ||
+        (rc = init_lists(c, kd, ki, ksz, n, K)))
+        return rc;
+    // leaves are applied in batches in which every row appears at most once
+    std::vector<uint8_t> seen(n, 0);
+    std::vector<LeafRef> batch;
+    std::vector<uint64_t> batch_rows;
+    for (uint64_t l = 0; l <= n_leaves; l++) {
+        bool conflict = false;
+        if (l < n_leaves)
+            for (uint64_t a = leaf_off[l]; a < leaf_off[l + 1] && !conflict; a++) conflict = seen[leaf_ids[a]];
+        if (l == n_leaves || conflict) {
+            if ((rc = run_leaf_topk(c, dx, dn, n, xs, dim, dids.as<uint32_t>(), batch, K, kd, ki, ksz))) return rc;
+            for (uint64_t r : batch_rows) seen[r] = 0;
+            batch.clear();
+            batch_rows.clear();
+            if (l == n_leaves) break;
+        }
+        batch.push_back({leaf_off[l], (uint32_t)(leaf_off[l + 1] - leaf_off[l]), 0});
+        for (uint64_t a = leaf_off[l]; a < leaf_off[l + 1]; a++) {
+            seen[leaf_ids[a]] = 1;
+            batch_rows.push_back(leaf_ids[a]);
+        }
+    }
+    if ((rc = d2h(c, ids, ki, n * K * 4)) || (rc = d2h(c, dists, kd, n * K * 4))) return rc;
+    return sync(c);
+}
+
+int anqi_aknn_gather(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids, const float* g_vals,
+                     uint32_t K, uint32_t ef, uint32_t cap, uint32_t out_k, uint32_t* ids, float* dists) {
+    if (!h || !x || !g_ids || !g_vals || !ids || !dists || n == 0 || K == 0 || ef == 0 || out_k == 0 || out_k > 1024)
+        return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    const uint32_t xs = round_up(dim, 8);
+    TmpBuf dx(c), dn(c), hid(c), hv(c), roff(c), rev(c), oi(c), od(c);
+    int rc;
+    if ((rc = upload_rows(c, dx, dn, x, n, dim, xs)) || (rc = h2d(c, hid, g_ids, n * K * 4)) ||
+        (rc = h2d(c, hv, g_vals, n * K * 4)) || (rc = build_reverse(c, hid.as<uint32_t>(), n, K, roff, rev)) ||
+        (rc = ensure(c, oi, n * out_k * 4)) || (rc = ensure(c, od, n * out_k * 4)))
+        return rc;
+    GatherParams p = base_params(dx, dn, n, xs, dim);
+    p.g_ids = hid.as<uint32_t>();
+    p.g_vals = hv.as<float>();
+    p.K = K;
+    p.rev_off = roff.as<uint64_t>();
+    p.rev_ids = rev.as<uint32_t>();
+    p.ef = ef;
+    p.cap = cap;
+    p.mode = kModeAknn;
+    p.out_k = out_k;
+    p.out_ids = oi.as<uint32_t>();
+    p.out_d = od.as<float>();
+    if ((rc = run_gather(c, p, max_reverse(c, roff, n), nullptr))) return rc;
+    if ((rc = d2h(c, ids, oi, n * out_k * 4)) || (rc = d2h(c, dists, od, n * out_k * 4))) return rc;
+    return sync(c);
+}
+
+int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, const anqi_aknn_params* ap, uint32_t* ids,
+                    float* dists, anqi_build_stats* st) {
+    if (!h || !base || !ap || !ids || !dists || n == 0 || d == 0 || ap->k == 0 || ap->k > 256 || ap->trees == 0 ||
+        ap->leaf == 0 || ap->ef == 0)
+        return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    if (n <= ap->k) return fail(c, ANQI_ERR_FORMAT, "n must exceed K");
+    const auto t0 = Clock::now();
+    const uint32_t xs = round_up(d, 8);
+    const uint32_t K = ap->k;
+    TmpBuf dx(c), dn(c), kd(c), ki(c), ksz(c), roff(c), rev(c), oi(c), od(c), hv(c), hi(c);
+    int rc;
+    if ((rc = upload_rows(c, dx, dn, base, n, d, xs)) || (rc = init_lists(c, kd, ki, ksz, n, K))) return rc;
+    auto t = Clock::now();
+    ForestOut f;
+    const uint32_t cap_nodes = (uint32_t)std::min<uint64_t>(16 * n / ap->leaf + 1024, 4 * n + 8);
+    rc = build_forest(c, dx.as<float>(), n, d, xs, ap->trees, ap->leaf, 100, ap->seed, cap_nodes, f);
+    const double forest_ms = ms_since(t);
+    t = Clock::now();
+    if (!rc) {
+        // init_knn, one tree at a time (index.h:1433-1449)
+        for (uint32_t tr = 0; tr < ap->trees && !rc; tr++) {
+            std::vector<LeafRef> leaves;
+            for (uint32_t v = 0; v < f.n_nodes[tr]; v++) {
+                const size_t g = (size_t)tr * cap_nodes + v;
+                if (f.left[g] == kEmpty && f.leaf_cnt[g] > 1) leaves.push_back({(uint64_t)tr * n + f.leaf_off[g], f.leaf_cnt[g], 0});
+            }
+            rc = run_leaf_topk(c, dx, dn, n, xs, d, f.perm.as<uint32_t>(), leaves, K, kd, ki, ksz);
+        }
+    }
+    release(c, f.perm);
+    release(c, f.hyper);
+    if (rc) return rc;
+    random_fill_kernel<<<c->sm_count * 8, 128, 0, c->stream>>>(dx.as<float>(), dn.as<float>(), n, xs, d, ap->seed, K,
+                                                               kd.as<float>(), ki.as<uint32_t>(), ksz.as<uint32_t>());
+    ANQI_CUDA(c, cudaGetLastError());
+    if ((rc = sync(c))) return rc;
+    const double init_ms = ms_since(t);
+    t = Clock::now();
+    std::vector<uint64_t> up;
+    if (ap->nn_iters > 0) {
+        // optional LocalJoin on the AKNN heaps (index.h:1314-1333)
+        if ((rc = ensure(c, hv, n * K * 4)) || (rc = ensure(c, hi, n * K * 4))) return rc;
+        list_to_heap_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(kd.as<float>(), ki.as<uint32_t>(),
+                                                                    ksz.as<uint32_t>(), n, K, hv.as<float>(),
+                                                                    hi.as<uint32_t>());
+        ANQI_CUDA(c, cudaGetLastError());
+        if ((rc = run_localjoin(c, dx, dn, n, xs, d, hi, hv, K, ap->nn_sample ? ap->nn_sample : 20, ap->nn_iters, up)))
+            return rc;
+    }
+    const double join_ms = ms_since(t);
+    t = Clock::now();
+    const DevBuf& gid = ap->nn_iters > 0 ? static_cast<const DevBuf&>(hi) : static_cast<const DevBuf&>(ki);
+    const DevBuf& gval = ap->nn_iters > 0 ? static_cast<const DevBuf&>(hv) : static_cast<const DevBuf&>(kd);
+    if ((rc = build_reverse(c, gid.as<uint32_t>(), n, K, roff, rev))) return rc;
+    const double reverse_ms = ms_since(t);
+    t = Clock::now();
+    if ((rc = ensure(c, oi, n * K * 4)) || (rc = ensure(c, od, n * K * 4))) return rc;
+    GatherParams p = base_params(dx, dn, n, xs, d);
+    p.g_ids = gid.as<uint32_t>();
+    p.g_vals = gval.as<float>();
+    p.K = K;
+    p.rev_off = roff.as<uint64_t>();
+    p.rev_ids = rev.as<uint32_t>();
+    p.ef = ap->ef;
+    p.cap = std::max<uint32_t>(K, (ap->ef_alpha ? ap->ef_alpha : 8) * ap->ef);
+    p.mode = kModeAknn;
+    p.out_k = K;
+    p.out_ids = oi.as<uint32_t>();
+    p.out_d = od.as<float>();
+    uint64_t pool_total = 0;
+    if ((rc = run_gather(c, p, max_reverse(c, roff, n), &pool_total))) return rc;
+    const double gather_ms = ms_since(t);
+    if ((rc = d2h(c, ids, oi, n * K * 4)) || (rc = d2h(c, dists, od, n * K * 4)) || (rc = sync(c))) return rc;
+    if (st) {
+        st->forest_ms = forest_ms;
+        st->init_ms = init_ms;
+        st->join_ms = join_ms;
+        st->reverse_ms = reverse_ms;
+        st->gather_ms = gather_ms;
+        st->total_ms = ms_since(t0);
+        uint64_t tot = 0;
+        for (uint64_t u : up) tot += u;
+        st->join_updates = tot;
+        st->pool_total = pool_total;
+    }
+    return ANQI_OK;
+}
+
+// tools/dataset_gt.cpp:206-248: the whole base is one candidate set, every row
+// keeps its K smallest (key, id) over all other rows.
+__global__ void iota_kernel(uint32_t* a, uint64_t n) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x)
+        a[t] = (uint32_t)t;
+}
+
+int anqi_exact_topk(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, uint32_t K, uint32_t* ids, float* keys) {
+    if (!h || !base || !ids || !keys || d == 0 || K == 0 || K > 256) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    if (K >= n) return fail(c, ANQI_ERR_ARGS, "require K < base vector count");
+    const uint32_t xs = round_up(d, 8);
+    TmpBuf dx(c), dn(c), dids(c), kd(c), ki(c), ksz(c);
+    int rc;
+    if ((rc = upload_rows(c, dx, dn, base, n, d, xs)) || (rc = ensure(c, dids, n * 4)) ||
+        (rc = init_lists(c, kd, ki, ksz, n, K)))
+        return rc;
+    iota_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(dids.as<uint32_t>(), n);
+    ANQI_CUDA(c, cudaGetLastError());
+    std::vector<LeafRef> all{{0, (uint32_t)n, 0}};
+    if ((rc = run_leaf_topk(c, dx, dn, n, xs, d, dids.as<uint32_t>(), all, K, kd, ki, ksz))) return rc;
+    if ((rc = d2h(c, ids, ki, n * K * 4)) || (rc = d2h(c, keys, kd, n * K * 4))) return rc;
+    return sync(c);
+}
+
+}  // extern "C"

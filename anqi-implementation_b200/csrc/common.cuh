@@ -33,6 +33,8 @@ enum DeviceError : uint32_t {
     kDevSortOverflow = 6,
 };
 
+__host__ __device__ __forceinline__ uint64_t min_u64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
 __device__ __forceinline__ void set_error(uint32_t* err, uint32_t code) {
     if (err) atomicCAS(err, 0u, code);
 }

@@ -155,6 +155,91 @@ __global__ void pair_dist_kernel(const float* __restrict__ a, const float* __res
     }
 }
 
+// three-phase exclusive scan: block sums, one-block scan of the sums, apply
+constexpr uint32_t kScanBlock = 1024;
+
+__global__ void scan_block_sums_kernel(const uint32_t* __restrict__ in, uint64_t n, uint64_t* __restrict__ bsum) {
+    __shared__ uint64_t s[32];
+    const uint64_t i = (uint64_t)blockIdx.x * kScanBlock + threadIdx.x;
+    uint64_t v = i < n ? in[i] : 0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t t = 0;
+        for (int w = 0; w < (int)(kScanBlock / 32); w++) t += s[w];
+        bsum[blockIdx.x] = t;
+    }
+}
+
+__global__ void scan_sums_kernel(uint64_t* __restrict__ bsum, uint64_t nb) {
+    __shared__ uint64_t part[1024];
+    const uint64_t chunk = (nb + blockDim.x - 1) / blockDim.x;
+    const uint64_t b = min(nb, threadIdx.x * chunk), e = min(nb, b + chunk);
+    uint64_t s = 0;
+    for (uint64_t i = b; i < e; i++) s += bsum[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t run = 0;
+        for (uint32_t i = 0; i < blockDim.x; i++) {
+            const uint64_t v = part[i];
+            part[i] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    uint64_t run = part[threadIdx.x];
+    for (uint64_t i = b; i < e; i++) {
+        const uint64_t v = bsum[i];
+        bsum[i] = run;
+        run += v;
+    }
+}
+
+__global__ void scan_apply_kernel(const uint32_t* __restrict__ in, uint64_t n, const uint64_t* __restrict__ bsum,
+                                  uint64_t* __restrict__ out) {
+    __shared__ uint64_t s[32];
+    const uint64_t i = (uint64_t)blockIdx.x * kScanBlock + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    const uint64_t v = i < n ? in[i] : 0;
+    uint64_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) s[w] = x;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint64_t y = threadIdx.x < kScanBlock / 32 ? s[threadIdx.x] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t z = __shfl_up_sync(0xFFFFFFFFu, y, o);
+            if (threadIdx.x >= (uint32_t)o) y += z;
+        }
+        s[threadIdx.x] = y;
+    }
+    __syncthreads();
+    const uint64_t before = (w ? s[w - 1] : 0) + x - v + bsum[blockIdx.x];
+    if (i < n) out[i] = before;
+    if (i == n - 1) out[n] = before + v;
+}
+
+int device_scan(Ctx* c, const uint32_t* d_in, uint64_t* d_out, uint64_t n) {
+    if (n == 0) {
+        ANQI_CUDA(c, cudaMemsetAsync(d_out, 0, 8, c->stream));
+        return ANQI_OK;
+    }
+    const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
+    TmpBuf bs(c);
+    int rc = ensure(c, bs, nb * 8);
+    if (rc) return rc;
+    scan_block_sums_kernel<<<(unsigned)nb, kScanBlock, 0, c->stream>>>(d_in, n, bs.as<uint64_t>());
+    scan_sums_kernel<<<1, 1024, 0, c->stream>>>(bs.as<uint64_t>(), nb);
+    scan_apply_kernel<<<(unsigned)nb, kScanBlock, 0, c->stream>>>(d_in, n, bs.as<uint64_t>(), d_out);
+    ANQI_CUDA(c, cudaGetLastError());
+    return sync(c);
+}
+
 }  // namespace anqi
 
 using namespace anqi;

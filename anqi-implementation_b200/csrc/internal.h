@@ -82,7 +82,7 @@ struct Ctx {
     // last entry tree from anqi_graph_build
     std::vector<uint32_t> t_left, t_right, t_leaf_off, t_leaf_cnt, t_perm;
     std::vector<float> t_offset, t_hyper;
-    uint32_t t_nodes = 0;
+    uint32_t t_nodes = 0, t_dim = 0;
     uint64_t device_bytes = 0;
     std::vector<DevBuf*> member_bufs() {
         return {&ix.base, &ix.lifted, &ix.onorm, &ix.deg, &ix.links, &ix.tleft, &ix.tright, &ix.toffset,
@@ -122,6 +122,20 @@ inline uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
 
 // Pad rows of a host matrix into a device buffer with stride (floats), zero fill.
 int upload_padded(Ctx* c, DevBuf& b, const float* src, uint64_t n, uint32_t d, uint32_t stride);
+
+// A built random-projection forest (breadth-first node numbering per tree; tree
+// t's nodes at [t * cap_nodes, ...), its permutation at [t * n, ...)).
+struct ForestOut {
+    uint32_t trees = 0, cap_nodes = 0, dim = 0, stride = 0;
+    uint64_t n = 0;
+    std::vector<uint32_t> n_nodes, left, right, leaf_off, leaf_cnt;
+    std::vector<float> offset;
+    DevBuf perm, hyper;  // device; released by the caller
+};
+int build_forest(Ctx* c, const float* d_x, uint64_t n, uint32_t dim, uint32_t stride, uint32_t trees, uint32_t leaf,
+                 uint32_t max_depth, uint64_t seed, uint32_t cap_nodes, ForestOut& out);
+// Exclusive scan of n u32 counts into n + 1 u64 offsets (device).
+int device_scan(Ctx* c, const uint32_t* d_in, uint64_t* d_out, uint64_t n);
 
 // Launch helpers implemented in the .cu files.
 int lrq_materialize_device(Ctx* c, const Verifier& v, uint32_t k, double scale, float* d_out);
