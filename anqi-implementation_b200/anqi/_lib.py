@@ -83,6 +83,8 @@ _SIGS = {
     "anqi_last_error": [_vp],
     "anqi_version": [],
     "anqi_device_bytes": [_vp],
+    "anqi_timer_start": [_vp],
+    "anqi_timer_stop": [_vp, C.POINTER(C.c_float)],
     "anqi_pair_distances": [_vp, _f32, _f32, C.c_uint64, C.c_uint32, _f32, _f32],
     "anqi_lrq_encode": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _f32, C.c_uint32, _f32, _u8],
     "anqi_lrq_materialize": [_vp, _f32, _u8, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _f32, C.c_uint32,
@@ -114,6 +116,7 @@ _SIGS = {
                         C.c_uint64, _vp, C.POINTER(QueryStats)],
     "anqi_query_upload": [_vp, _f32, C.c_uint32, _vp, C.c_uint32, _vp, C.c_uint32],
     "anqi_query_run": [_vp, C.c_int, C.POINTER(QueryStats)],
+    "anqi_query_counters": [_vp, C.POINTER(QueryStats)],
     "anqi_query_download": [_vp, _u32, _vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp],
     "anqi_query_evaluate": [_vp, _u32, _u32, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double),
                             C.POINTER(C.c_double), C.POINTER(C.c_uint32)],
@@ -206,6 +209,14 @@ class Context:
         if rc != ANQI_OK:
             msg = self.lib.anqi_last_error(self.h)
             raise AnqiError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def timer_start(self) -> None:
+        self._check(self.lib.anqi_timer_start(self.h), "timer_start")
+
+    def timer_stop(self) -> float:
+        ms = C.c_float()
+        self._check(self.lib.anqi_timer_stop(self.h, C.byref(ms)), "timer_stop")
+        return ms.value
 
     @property
     def device_bytes(self) -> int:
@@ -329,9 +340,11 @@ class Context:
         self.nq = nq
         self._check(self.lib.anqi_query_upload(self.h, queries, nq, _ptr(ka), kall, _ptr(La), Lall), "query_upload")
 
-    def query_run(self, keep_candidates=False) -> dict:
+    def query_run(self, keep_candidates=False, counters=False) -> dict:
         st = QueryStats()
         self._check(self.lib.anqi_query_run(self.h, int(keep_candidates), C.byref(st)), "query_run")
+        if counters:
+            self._check(self.lib.anqi_query_counters(self.h, C.byref(st)), "query_counters")
         return {k2: getattr(st, k2) for k2, _ in QueryStats._fields_}
 
     def query_download(self, with_candidates=False) -> QueryResult:

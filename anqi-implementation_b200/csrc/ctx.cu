@@ -290,6 +290,8 @@ void anqi_ctx_destroy(anqi_ctx* h) {
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->ev2) cudaEventDestroy(c->ev2);
     if (c->ev3) cudaEventDestroy(c->ev3);
+    if (c->tev0) cudaEventDestroy(c->tev0);
+    if (c->tev1) cudaEventDestroy(c->tev1);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete h;
 }
@@ -297,6 +299,29 @@ void anqi_ctx_destroy(anqi_ctx* h) {
 const char* anqi_last_error(const anqi_ctx* h) { return h ? h->c.last_error.c_str() : "null context"; }
 
 uint64_t anqi_device_bytes(const anqi_ctx* h) { return h ? h->c.device_bytes : 0; }
+
+int anqi_timer_start(anqi_ctx* h) {
+    if (!h) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    if (!c->tev0) {
+        ANQI_CUDA(c, cudaEventCreate(&c->tev0));
+        ANQI_CUDA(c, cudaEventCreate(&c->tev1));
+    }
+    ANQI_CUDA(c, cudaEventRecord(c->tev0, c->stream));
+    return ANQI_OK;
+}
+
+int anqi_timer_stop(anqi_ctx* h, float* ms) {
+    if (!h || !ms) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    if (!c->tev0) return fail(c, ANQI_ERR_ARGS, "anqi_timer_stop without anqi_timer_start");
+    ANQI_CUDA(c, cudaEventRecord(c->tev1, c->stream));
+    ANQI_CUDA(c, cudaEventSynchronize(c->tev1));
+    ANQI_CUDA(c, cudaEventElapsedTime(ms, c->tev0, c->tev1));
+    return ANQI_OK;
+}
 
 int anqi_pair_distances(anqi_ctx* h, const float* a, const float* b, uint64_t m, uint32_t dim, float* l2sqr,
                         float* ip) {

@@ -71,6 +71,7 @@ struct Ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+    cudaEvent_t tev0 = nullptr, tev1 = nullptr;  // anqi_timer_*
     std::string last_error;
     QueryIndex ix;
     Verifier vf;

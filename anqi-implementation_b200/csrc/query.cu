@@ -729,25 +729,33 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
         ANQI_CUDA(c, cudaGetLastError());
         b.have_results = true;
         b.have_cands = keep_candidates != 0;
-        if (st) {
-            std::vector<uint32_t> v(b.nq);
-            uint64_t sums[5] = {0, 0, 0, 0, 0};
-            DevBuf* arr[5] = {&b.ndist, &b.nexp, &b.ncand, &b.npred, &b.nflood};
-            for (int a = 0; a < 5; a++) {
-                ANQI_CUDA(c, cudaMemcpyAsync(v.data(), arr[a]->p, b.nq * 4ull, cudaMemcpyDeviceToHost, c->stream));
-                if ((rc = sync(c))) return rc;
-                for (uint32_t x : v) sums[a] += x;
-            }
-            st->n_dist = sums[0];
-            st->n_expand = sums[1];
-            st->n_cand = sums[2];
-            st->n_pred = sums[3];
-            st->n_flood = sums[4];
-            st->search_ms = ms;
-        }
+        if (st) st->search_ms = ms;
         return sync(c);
     }
     return fail(c, ANQI_ERR_CAPACITY, "rknn search: output capacity could not be satisfied");
+}
+
+int anqi_query_counters(anqi_ctx* h, anqi_query_stats* st) {
+    if (!h || !st) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    Batch& b = c->batch;
+    if (!b.have_results) return fail(c, ANQI_ERR_ARGS, "anqi_query_counters: no results");
+    std::vector<uint32_t> v(b.nq);
+    uint64_t sums[5] = {0, 0, 0, 0, 0};
+    DevBuf* arr[5] = {&b.ndist, &b.nexp, &b.ncand, &b.npred, &b.nflood};
+    for (int a = 0; a < 5; a++) {
+        ANQI_CUDA(c, cudaMemcpyAsync(v.data(), arr[a]->p, b.nq * 4ull, cudaMemcpyDeviceToHost, c->stream));
+        int rc = sync(c);
+        if (rc) return rc;
+        for (uint32_t x : v) sums[a] += x;
+    }
+    st->n_dist = sums[0];
+    st->n_expand = sums[1];
+    st->n_cand = sums[2];
+    st->n_pred = sums[3];
+    st->n_flood = sums[4];
+    return ANQI_OK;
 }
 
 int anqi_query_download(anqi_ctx* h, uint32_t* pred_off, uint32_t* pred_ids, uint64_t pred_cap, uint32_t* cand_off,

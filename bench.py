@@ -1,0 +1,386 @@
+#!/usr/bin/env python3
+"""RkNN query throughput of the B200 implementation on the 1M x 128 mixture.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the reference's full-size configuration): 1,000,000 x 128 base
+vectors, integers in [0, 255] from a 1,000-centre Gaussian mixture, 10,000
+queries from the same mixture.  The index (AKNN top-100 source, M8/u8 LRQ
+verifier, d+2 lift, G48 graph) is built on the GPU first (not timed as
+queries); the exact RkNN ground truth is computed on the GPU for recall.
+
+One step = one batch of 30,000 queries: the 10,000 queries once each for
+k = 10, 50 and 100 (per-query k in a single launch), beam width L for all.
+``value`` is queries/s over K steps with the batch resident in HBM (CUDA events
+on the library's stream); ``e2e`` is the same through the host-buffer C ABI
+call (query upload from pinned memory and result download inside the timed
+region).  The timed working set (lifted + base vectors, graph) is ~1.3 GB,
+larger than the 126 MB L2.
+
+``--impl reference`` times the reference's own CPU query code (its
+nndindex::range_search, postfilter and evaluation, built from its sources into
+oracle/_ref) on this host's cores, on the same index files and workload.
+Under torchrun every rank holds an index replica and runs its own batch
+(weak scaling); rank 0 prints the line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "anqi-implementation_b200"))
+
+METRIC = "RkNN queries/s (1M x 128, k in {10,50,100}, FP32 bit-exact path)"
+
+
+def log(*a):
+    print("[bench]", *a, file=sys.stderr, flush=True)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--d", type=int, default=128)
+    ap.add_argument("--nq", type=int, default=10_000)
+    ap.add_argument("--L", type=int, default=128)
+    ap.add_argument("--ks", default="10,50,100")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU seconds of the cpu_baseline sample")
+    ap.add_argument("--keep", type=Path, default=None, help="write the index prefix files here")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """Samples nvidia-smi clocks/throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) > 8 for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def build_workload(ctx, a, rank, log):
+    from anqi import pipeline
+    t0 = time.perf_counter()
+    base, query = pipeline.mixture(a.n, a.d, a.nq, seed=20260819 + rank)
+    log(f"data {base.shape} + {query.shape} in {time.perf_counter() - t0:.1f}s")
+    ix = pipeline.build_index(ctx, base, train_workers=os.cpu_count() or 8, log=log)
+    t0 = time.perf_counter()
+    _, ex_keys = pipeline.exact_thresholds(ctx, base, 100)
+    t_thr = time.perf_counter() - t0
+    ks = [int(k) for k in a.ks.split(",")]
+    gt = {}
+    t0 = time.perf_counter()
+    for k in ks:
+        gt[k] = pipeline.rknn_ground_truth(ctx, base, query, ex_keys[:, k - 1])
+    log(f"exact thresholds {t_thr:.1f}s, RkNN ground truth {time.perf_counter() - t0:.1f}s, "
+        f"mean |R| = {[round(float(np.diff(gt[k][0]).mean()), 2) for k in ks]}")
+    ix.timings["exact_thresholds_s"] = t_thr
+    return base, query, ix, ks, gt
+
+
+def write_index_files(d: Path, base, query, ix, ks, gt, ctx):
+    """Index + workload files the reference harness reads (reference formats)."""
+    from anqi import formats
+    d.mkdir(parents=True, exist_ok=True)
+    formats.write_fbin(d / "lifted.bin", ix.lifted)
+    formats.write_fbin(d / "base.bin", base)
+    formats.write_fbin(d / "query.bin", query)
+    g = formats.Graph(len(base), ix.lifted.shape[1], ix.links.shape[1], ix.deg, ix.links, ix.tree)
+    formats.write_graph(d / "graph.bin", g)
+    formats.write_graph_meta(d / "meta.txt", ix.mstar2, ix.scale)
+    for k in ks:
+        thr = ctx.lrq_materialize(ix.coeff, ix.codes, ix.mu, ix.basis, ix.codebook, k)
+        thr.tofile(d / f"thr{k}.bin")
+        off, ids, keys = gt[k]
+        formats.write_rknn_csr(d / f"gt{k}.bin", off, ids, keys)
+
+
+def reference_qbench(d: Path, ks, L, threads, warmup, steps, nq):
+    exe = REPO / "oracle" / "_ref" / "ref_harness"
+    if not exe.exists():
+        return None, "oracle/_ref/ref_harness is not built (needs the reference sources)"
+    flags = Path("/proc/cpuinfo").read_text() if Path("/proc/cpuinfo").exists() else ""
+    if "avx512f" not in flags:
+        return None, "host CPU lacks AVX-512 (the reference requires it)"
+    cmd = [str(exe), "qbench", str(d / "lifted.bin"), str(d / "graph.bin"), str(d / "base.bin"), str(d / "query.bin"),
+           str(d / "meta.txt"), str(L), str(threads), str(warmup), str(steps), str(nq)]
+    for k in ks:
+        cmd += [str(d / f"thr{k}.bin"), str(d / f"gt{k}.bin")]
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        return None, f"reference harness failed ({p.returncode}): {p.stderr[-300:]}"
+    line = [l for l in p.stdout.splitlines() if l.startswith("{")][-1]
+    return json.loads(line), None
+
+
+def run_ours(a, rank, world, local):
+    from anqi._lib import Context
+    import torch
+    dev = local if world > 1 else 0
+    ctx = Context(dev)
+    base, query, ix, ks, gt = build_workload(ctx, a, rank, lambda *m: log(f"rank{rank}", *m) if rank == 0 else None)
+    from anqi import pipeline
+    pipeline.load_index(ctx, ix, ks)
+    nq = len(query)
+    nb = nq * len(ks)
+    qb = np.ascontiguousarray(np.tile(query, (len(ks), 1)))
+    kb = np.repeat(np.array(ks, np.uint32), nq)
+    Lb = np.full(nb, a.L, np.uint32)
+    # recall of the batch (device evaluation against the exact CSR)
+    ctx.query_upload(qb, kb, Lb)
+    st = ctx.query_run(keep_candidates=True)
+    gt_off = np.zeros(nb + 1, np.uint32)
+    parts = []
+    for j, k in enumerate(ks):
+        off, ids, _ = gt[k]
+        gt_off[j * nq + 1:(j + 1) * nq + 1] = off[1:] + gt_off[j * nq]
+        parts.append(ids)
+    gt_ids = np.concatenate(parts).astype(np.uint32)
+    ev = ctx.query_evaluate(gt_off, gt_ids)
+    per_k = {}
+    for j, k in enumerate(ks):
+        ctx.query_upload(query, k, a.L)
+        ctx.query_run(keep_candidates=True)
+        off, ids, _ = gt[k]
+        e = ctx.query_evaluate(off, ids)
+        per_k[k] = {"recall": round(e["recall"], 6), "precision": round(e["precision"], 6),
+                    "candidate_recall": round(e["candidate_recall"], 6)}
+    # ---- resident batch: warm-up, then K timed steps
+    ctx.query_upload(qb, kb, Lb)
+    for _ in range(a.warmup):
+        ctx.query_run()
+    stats = []
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    with Clocks(dev) as clk:
+        ctx.timer_start()
+        for _ in range(a.steps):
+            stats.append(ctx.query_run())
+        ms = ctx.timer_stop()
+    clocks = clk.summary()
+    # ---- end to end through the host-buffer C ABI from pinned memory
+    pin_q = torch.empty(qb.shape, dtype=torch.float32, pin_memory=True).numpy()
+    pin_q[:] = qb
+    pin_k = torch.empty(kb.shape, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    pin_k[:] = kb
+    pin_L = torch.empty(Lb.shape, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    pin_L[:] = Lb
+    for _ in range(a.warmup):
+        r = ctx.rknn_query(pin_q, pin_k, pin_L)
+    e2e_stats = []
+    ctx.timer_start()
+    for _ in range(a.steps):
+        r = ctx.rknn_query(pin_q, pin_k, pin_L, pred_cap=int(r.pred_off[-1]) + 4096)
+        e2e_stats.append(r.stats)
+    e2e_ms = ctx.timer_stop()
+    from anqi.dist import max_over_ranks
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], device=f"cuda:{dev}" if world > 1 else None)
+    value = world * a.steps * nb / (ms / 1e3)
+    e2e_value = world * a.steps * nb / (e2e_ms / 1e3)
+    # ---- roofline of the search kernel: algorithmic bytes per launch
+    s0 = ctx.query_run(counters=True)
+    D = a.d + 2
+    X = s0["n_expand"] + s0["n_flood"]
+    alg_bytes = s0["n_dist"] * 4 * D + X * 4 * (1 + ix.links.shape[1]) + s0["n_cand"] * (4 * a.d + 4)
+    kernel_ms = statistics.median([s["search_ms"] for s in stats])
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = None
+    tf = REPO / "profiles" / "search_kernel_traffic.json"
+    if tf.exists():
+        try:
+            tj = json.loads(tf.read_text())
+            traffic = tj["bytes_per_query"] * nb
+        except (ValueError, KeyError):
+            traffic = None
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded 1,000-centre mixture, integers in [0,255])",
+        "config": {"workload": f"rknn_query {a.n}x{a.d}, {a.nq} queries x k{{{a.ks}}}, L={a.L}, "
+                               "G48 graph, M8/u8 LRQ postfilter", "n": a.n, "d": a.d, "nq": a.nq,
+                   "queries_per_step": nb, "ks": ks, "L": a.L, "parallelism": f"replicas x{world}",
+                   "l2": "working set > L2 (lifted+base+graph ~1.3 GB)"},
+        "e2e": {"value": round(e2e_value, 1), "unit": "queries/s",
+                "h2d_bytes_per_step": int(e2e_stats[-1]["h2d_bytes"]),
+                "d2h_bytes_per_step": int(e2e_stats[-1]["d2h_bytes"])},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                     "kernel": "rknn_search_kernel", "kernel_ms": round(kernel_ms, 4),
+                     "alg_bytes_per_launch": int(alg_bytes)},
+        "gpu_launches": 3 * a.steps,
+        "clocks": clocks,
+        "recall": round(ev["recall"], 6), "precision": round(ev["precision"], 6), "per_k": per_k,
+        "counters_per_query": {"graph_dist": round(s0["n_dist"] / nb, 1), "expansions": round(X / nb, 1),
+                               "candidates": round(s0["n_cand"] / nb, 1), "verified": round(s0["n_pred"] / nb, 2)},
+        "build_s": {k: round(v, 3) for k, v in ix.timings.items() if isinstance(v, float)},
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        tmp = Path(a.keep) if a.keep else Path(tempfile.mkdtemp(prefix="anqi_bench_"))
+        try:
+            write_index_files(tmp, base, query, ix, ks, gt, ctx)
+            threads = os.cpu_count() or 1
+            # bounded sample: enough queries for about cpu_seconds of CPU work
+            probe, err = reference_qbench(tmp, ks, a.L, threads, 0, 1, 1000)
+            if probe is None:
+                line["cpu_baseline"] = {"unavailable": err}
+            else:
+                per_q = probe["seconds"] / probe["queries_per_step"]
+                nqs = int(min(nq, max(200, a.cpu_seconds / max(per_q, 1e-9) / len(ks))))
+                res, err = reference_qbench(tmp, ks, a.L, threads, 0, 1, nqs)
+                if res is None:
+                    line["cpu_baseline"] = {"unavailable": err}
+                else:
+                    line["cpu_baseline"] = {"value": round(res["qps"], 1), "unit": "queries/s", "cores": threads,
+                                            "kind": "reference",
+                                            "sample": f"first {nqs} queries x k{{{a.ks}}}, L={a.L}, same index; "
+                                                      "reference range_search + postfilter + evaluation",
+                                            "per_k": res["per_k"]}
+        finally:
+            if not a.keep:
+                shutil.rmtree(tmp, ignore_errors=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def run_reference(a, rank, world, local):
+    if rank != 0:
+        return
+    from anqi._lib import Context
+    ctx = Context(local if world > 1 else 0)
+    base, query, ix, ks, gt = build_workload(ctx, a, rank, lambda *m: log("reference-arm", *m))
+    tmp = Path(a.keep) if a.keep else Path(tempfile.mkdtemp(prefix="anqi_ref_"))
+    threads = os.cpu_count() or 1
+    try:
+        write_index_files(tmp, base, query, ix, ks, gt, ctx)
+        ctx.close()
+        # bounded steps: each step is a sample of the batch sized to ~cpu_seconds / steps
+        probe, err = reference_qbench(tmp, ks, a.L, threads, 0, 1, 500)
+        if probe is None:
+            print(json.dumps({"impl": "reference", "unavailable": err}), flush=True)
+            return
+        per_q = probe["seconds"] / probe["queries_per_step"]
+        budget = 120.0 / max(1, a.steps + a.warmup)
+        nqs = int(min(len(query), max(100, budget / max(per_q, 1e-9) / len(ks))))
+        res, err = reference_qbench(tmp, ks, a.L, threads, a.warmup, a.steps, nqs)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": err}), flush=True)
+            return
+        value = res["qps"]
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(1e3 * res["seconds"] / a.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded 1,000-centre mixture, integers in [0,255])",
+            "config": {"workload": f"rknn_query {a.n}x{a.d}, {a.nq} queries x k{{{a.ks}}}, L={a.L}, "
+                                   "G48 graph, M8/u8 LRQ postfilter", "n": a.n, "d": a.d, "nq": a.nq,
+                       "queries_per_step": nqs * len(ks), "ks": ks, "L": a.L, "parallelism": "cpu"},
+            "impl": "reference",
+            "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": threads, "kind": "reference",
+                             "sample": f"first {nqs} queries x k{{{a.ks}}} per step on the GPU-built index "
+                                       "(reference formats); reference range_search + postfilter + evaluation"},
+            "e2e": {"value": round(value, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "per_k": res["per_k"],
+        }
+        print(json.dumps(line), flush=True)
+    finally:
+        if not a.keep:
+            shutil.rmtree(tmp, ignore_errors=True)
+
+
+def main():
+    a = parse()
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=900))
+    try:
+        if a.impl == "reference":
+            run_reference(a, rank, world, local)
+        else:
+            run_ours(a, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

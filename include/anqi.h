@@ -43,6 +43,10 @@ const char* anqi_last_error(const anqi_ctx* ctx);
 int anqi_version(void);
 /* Bytes of device memory the context currently holds. */
 uint64_t anqi_device_bytes(const anqi_ctx* ctx);
+/* Device timer on the context's stream (CUDA events): start, then stop returns
+ * the elapsed milliseconds of everything the context ran in between. */
+int anqi_timer_start(anqi_ctx* ctx);
+int anqi_timer_stop(anqi_ctx* ctx, float* ms);
 
 /* ------------------------------------------------------- FP32 distances
  * Batch forms of include/distance.h:58-161 in the AVX-512 lane order:
@@ -214,7 +218,10 @@ int anqi_rknn_query(anqi_ctx* ctx, const float* queries, uint32_t nq, const uint
  * upload once, run many times (results stay on the device), then download. */
 int anqi_query_upload(anqi_ctx* ctx, const float* queries, uint32_t nq, const uint32_t* k_per_query,
                       uint32_t k_all, const uint32_t* L_per_query, uint32_t L_all);
+/* st (optional) receives search_ms only; anqi_query_counters sums the
+ * per-query counters of the last run (device -> host copies). */
 int anqi_query_run(anqi_ctx* ctx, int keep_candidates, anqi_query_stats* st);
+int anqi_query_counters(anqi_ctx* ctx, anqi_query_stats* st);
 int anqi_query_download(anqi_ctx* ctx, uint32_t* pred_off, uint32_t* pred_ids, uint64_t pred_cap,
                         uint32_t* cand_off, uint32_t* cand_ids, uint64_t cand_cap, uint32_t* n_dist);
 /* Recall / precision of the resident batch's last results against a

@@ -14,7 +14,7 @@
 //   aknn     BASE OUT K LEAF TREES EF SEED  staged AKNN source build (index.h:1300-1461)
 //   query    LIFTED GRAPH BASE QUERY META THR L OUT
 //                                           range_search + postfilter per query (index.h:1535, rknn_query.cpp:2692-2765)
-//   qbench   LIFTED GRAPH BASE QUERY META THR GT L THREADS SECONDS
+//   qbench   LIFTED GRAPH BASE QUERY META L THREADS WARMUP STEPS NQ THR GT [THR GT ...]
 //                                           the reference's timed query loop body, OpenMP, prints one JSON line
 
 #define main anqi_reference_rknn_query_main
@@ -410,27 +410,38 @@ int cmd_query(int argc, char** argv) {
     return 0;
 }
 
-// qbench LIFTED GRAPH BASE QUERY META THR GT L THREADS SECONDS
+// qbench LIFTED GRAPH BASE QUERY META L THREADS WARMUP STEPS NQ THR1 GT1 [THR2 GT2 ...]
 // Times the reference's own per-query work (rknn_query.cpp:2714-2803): query
 // lift, nndindex::range_search, the FP32 postfilter into an unordered_set, and
-// the recall/precision evaluation against the ground-truth CSR.
+// the recall/precision evaluation against the ground-truth CSR, OpenMP over
+// queries (schedule dynamic, 16).  One step runs the first NQ queries once for
+// every (thresholds, ground truth) pair; prints one JSON line.
 int cmd_qbench(int argc, char** argv) {
-    if (argc != 12) return 2;
+    if (argc < 14 || (argc - 12) % 2 != 0) return 2;
+    const size_t L = std::strtoull(argv[7], nullptr, 10);
+    const int threads = std::atoi(argv[8]);
+    const int warmup = std::atoi(argv[9]);
+    const int steps = std::atoi(argv[10]);
+    const size_t nq_limit = std::strtoull(argv[11], nullptr, 10);
+    const int nk = (argc - 12) / 2;
+    char* env_args[6] = {argv[2], argv[3], argv[4], argv[5], argv[6], argv[12]};
     QueryEnv e;
-    load_query_env(e, argv + 2);
-    const std::string gt_path = argv[8];
-    const size_t L = std::strtoull(argv[9], nullptr, 10);
-    const int threads = std::atoi(argv[10]);
-    const double min_seconds = std::atof(argv[11]);
-    std::vector<uint32_t> goff, gids;
-    {
-        FILE* f = std::fopen(gt_path.c_str(), "rb");
+    load_query_env(e, env_args);
+    const size_t nq = std::min(e.nq, nq_limit ? nq_limit : e.nq);
+    std::vector<std::vector<float>> thr(nk);
+    std::vector<std::vector<uint32_t>> goff(nk), gids(nk);
+    for (int k = 0; k < nk; k++) {
+        thr[k].resize(e.n);
+        FILE* f = std::fopen(argv[12 + 2 * k], "rb");
+        if (!f || std::fread(thr[k].data(), 4, e.n, f) != e.n) die("bad threshold file");
+        std::fclose(f);
+        f = std::fopen(argv[13 + 2 * k], "rb");
         uint32_t gnq = 0;
         if (!f || std::fread(&gnq, 4, 1, f) != 1 || gnq != e.nq) die("bad GT header");
-        goff.resize(gnq + 1);
-        if (std::fread(goff.data(), 4, goff.size(), f) != goff.size()) die("short GT offsets");
-        gids.resize(goff.back());
-        if (std::fread(gids.data(), 4, gids.size(), f) != gids.size()) die("short GT ids");
+        goff[k].resize(gnq + 1);
+        if (std::fread(goff[k].data(), 4, goff[k].size(), f) != goff[k].size()) die("short GT offsets");
+        gids[k].resize(goff[k].back());
+        if (std::fread(gids[k].data(), 4, gids[k].size(), f) != gids[k].size()) die("short GT ids");
         std::fclose(f);
     }
     Parms par = lifted_parms(e.n, e.dim, 50, 48, "/tmp/anqi_harness_work/");
@@ -438,53 +449,72 @@ int cmd_qbench(int argc, char** argv) {
     nndindex index(argv[2], par);
     load_graph_file(index, argv[3]);
     omp_set_num_threads(threads);
-    double sum_rec = 0, sum_prec = 0, sum_cand = 0, sum_nd = 0;
-    size_t nonempty = 0, tasks = 0;
-    double secs = 0;
-    size_t batches = 0;
-    auto t0 = std::chrono::steady_clock::now();
-    while (secs < min_seconds || batches == 0) {
-        #pragma omp parallel reduction(+ : sum_rec, sum_prec, sum_cand, sum_nd, nonempty)
-        {
-            std::vector<uint16_t> mark(e.n, 0);
-            uint16_t ver = 0;
-            std::vector<float> qb(e.dim);
-            #pragma omp for schedule(dynamic, 16)
-            for (size_t i = 0; i < e.nq; i++) {
-                const float* q = e.queries.data() + i * e.d;
-                double R2 = 0;
-                lift_query(e, q, qb, R2);
-                if (++ver == 0) {
-                    std::fill(mark.begin(), mark.end(), 0);
-                    ver = 1;
+    std::vector<double> step_s;
+    std::vector<double> rec(nk, 0), prec(nk, 0), cand(nk, 0), dist(nk, 0);
+    std::vector<size_t> nonempty(nk, 0);
+    for (int st = 0; st < warmup + steps; st++) {
+        const bool timed = st >= warmup;
+        auto t0 = std::chrono::steady_clock::now();
+        for (int k = 0; k < nk; k++) {
+            double s_rec = 0, s_prec = 0, s_cand = 0, s_nd = 0;
+            size_t s_ne = 0;
+            #pragma omp parallel reduction(+ : s_rec, s_prec, s_cand, s_nd, s_ne)
+            {
+                std::vector<uint16_t> mark(e.n, 0);
+                uint16_t ver = 0;
+                std::vector<float> qb(e.dim);
+                #pragma omp for schedule(dynamic, 16)
+                for (size_t i = 0; i < nq; i++) {
+                    const float* q = e.queries.data() + i * e.d;
+                    double R2 = 0;
+                    lift_query(e, q, qb, R2);
+                    if (++ver == 0) {
+                        std::fill(mark.begin(), mark.end(), 0);
+                        ver = 1;
+                    }
+                    std::vector<uint32_t> cd;
+                    size_t nd = 0;
+                    index.range_search(qb.data(), R2, 0.0f, L, cd, nd, mark.data(), ver, nullptr, 0.5f, false);
+                    std::unordered_set<uint32_t> pred;
+                    for (uint32_t id : cd)
+                        if (recheck_key(e, id, q) <= (double)thr[k][id]) pred.insert(id);
+                    nd += cd.size();
+                    std::unordered_set<uint32_t> truth(gids[k].begin() + goff[k][i], gids[k].begin() + goff[k][i + 1]);
+                    if (truth.empty()) continue;
+                    s_ne++;
+                    size_t hit = 0;
+                    for (uint32_t id : pred) hit += truth.count(id);
+                    s_rec += (double)hit / truth.size();
+                    s_prec += pred.empty() ? 1.0 : (double)hit / pred.size();
+                    s_cand += cd.size();
+                    s_nd += nd;
                 }
-                std::vector<uint32_t> cand;
-                size_t nd = 0;
-                index.range_search(qb.data(), R2, 0.0f, L, cand, nd, mark.data(), ver, nullptr, 0.5f, false);
-                std::unordered_set<uint32_t> pred;
-                for (uint32_t id : cand)
-                    if (recheck_key(e, id, q) <= (double)e.thr[id]) pred.insert(id);
-                nd += cand.size();
-                std::unordered_set<uint32_t> truth(gids.begin() + goff[i], gids.begin() + goff[i + 1]);
-                if (truth.empty()) continue;
-                nonempty++;
-                size_t hit = 0;
-                for (uint32_t id : pred) hit += truth.count(id);
-                sum_rec += (double)hit / truth.size();
-                sum_prec += pred.empty() ? 1.0 : (double)hit / pred.size();
-                sum_cand += cand.size();
-                sum_nd += nd;
+            }
+            if (timed) {
+                rec[k] += s_rec;
+                prec[k] += s_prec;
+                cand[k] += s_cand;
+                dist[k] += s_nd;
+                nonempty[k] += s_ne;
             }
         }
-        tasks += e.nq;
-        batches++;
-        secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (timed) step_s.push_back(secs);
     }
-    const double denom = nonempty ? (double)nonempty : 1.0;
-    std::printf("{\"qps\": %.3f, \"tasks\": %zu, \"seconds\": %.6f, \"threads\": %d, \"recall\": %.6f, "
-                "\"precision\": %.6f, \"avg_cand\": %.3f, \"avg_dist\": %.3f, \"L\": %zu}\n",
-                tasks / secs, tasks, secs, threads, sum_rec / denom, sum_prec / denom,
-                sum_cand / denom, sum_nd / denom, L);
+    double tot = 0;
+    for (double x : step_s) tot += x;
+    std::printf("{\"threads\": %d, \"L\": %zu, \"queries_per_step\": %zu, \"steps\": %d, \"seconds\": %.6f, "
+                "\"qps\": %.3f, \"step_seconds\": [",
+                threads, L, nq * (size_t)nk, steps, tot, steps ? (double)nq * nk * steps / tot : 0.0);
+    for (size_t i = 0; i < step_s.size(); i++) std::printf("%s%.6f", i ? ", " : "", step_s[i]);
+    std::printf("], \"per_k\": [");
+    for (int k = 0; k < nk; k++) {
+        const double dn = nonempty[k] ? (double)nonempty[k] : 1.0;
+        std::printf("%s{\"recall\": %.6f, \"precision\": %.6f, \"avg_cand\": %.3f, \"avg_dist\": %.3f, "
+                    "\"nonempty\": %zu}",
+                    k ? ", " : "", rec[k] / dn, prec[k] / dn, cand[k] / dn, dist[k] / dn, nonempty[k]);
+    }
+    std::printf("]}\n");
     return 0;
 }
 
