@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--L", type=int, default=128)
     ap.add_argument("--ks", default="10,50,100")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gt", action="store_true", help="skip the exact ground truth (profiling runs; no recall)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU seconds of the cpu_baseline sample")
     ap.add_argument("--keep", type=Path, default=None, help="write the index prefix files here")
     return ap.parse_args()
@@ -133,10 +134,12 @@ def build_workload(ctx, a, rank, log):
     base, query = pipeline.mixture(a.n, a.d, a.nq, seed=20260819 + rank)
     log(f"data {base.shape} + {query.shape} in {time.perf_counter() - t0:.1f}s")
     ix = pipeline.build_index(ctx, base, train_workers=os.cpu_count() or 8, log=log)
+    ks = [int(k) for k in a.ks.split(",")]
+    if a.no_gt:
+        return base, query, ix, ks, None
     t0 = time.perf_counter()
     _, ex_keys = pipeline.exact_thresholds(ctx, base, 100)
     t_thr = time.perf_counter() - t0
-    ks = [int(k) for k in a.ks.split(",")]
     gt = {}
     t0 = time.perf_counter()
     for k in ks:
@@ -196,24 +199,26 @@ def run_ours(a, rank, world, local):
     kb = np.repeat(np.array(ks, np.uint32), nq)
     Lb = np.full(nb, a.L, np.uint32)
     # recall of the batch (device evaluation against the exact CSR)
-    ctx.query_upload(qb, kb, Lb)
-    st = ctx.query_run(keep_candidates=True)
-    gt_off = np.zeros(nb + 1, np.uint32)
-    parts = []
-    for j, k in enumerate(ks):
-        off, ids, _ = gt[k]
-        gt_off[j * nq + 1:(j + 1) * nq + 1] = off[1:] + gt_off[j * nq]
-        parts.append(ids)
-    gt_ids = np.concatenate(parts).astype(np.uint32)
-    ev = ctx.query_evaluate(gt_off, gt_ids)
+    ev = {"recall": None, "precision": None}
     per_k = {}
-    for j, k in enumerate(ks):
-        ctx.query_upload(query, k, a.L)
+    if gt is not None:
+        ctx.query_upload(qb, kb, Lb)
         ctx.query_run(keep_candidates=True)
-        off, ids, _ = gt[k]
-        e = ctx.query_evaluate(off, ids)
-        per_k[k] = {"recall": round(e["recall"], 6), "precision": round(e["precision"], 6),
-                    "candidate_recall": round(e["candidate_recall"], 6)}
+        gt_off = np.zeros(nb + 1, np.uint32)
+        parts = []
+        for j, k in enumerate(ks):
+            off, ids, _ = gt[k]
+            gt_off[j * nq + 1:(j + 1) * nq + 1] = off[1:] + gt_off[j * nq]
+            parts.append(ids)
+        gt_ids = np.concatenate(parts).astype(np.uint32)
+        ev = ctx.query_evaluate(gt_off, gt_ids)
+        for j, k in enumerate(ks):
+            ctx.query_upload(query, k, a.L)
+            ctx.query_run(keep_candidates=True)
+            off, ids, _ = gt[k]
+            e = ctx.query_evaluate(off, ids)
+            per_k[k] = {"recall": round(e["recall"], 6), "precision": round(e["precision"], 6),
+                        "candidate_recall": round(e["candidate_recall"], 6)}
     # ---- resident batch: warm-up, then K timed steps
     ctx.query_upload(qb, kb, Lb)
     for _ in range(a.warmup):
@@ -260,7 +265,7 @@ def run_ours(a, rank, world, local):
     if tf.exists():
         try:
             tj = json.loads(tf.read_text())
-            traffic = tj["bytes_per_query"] * nb
+            traffic = int(tj["bytes_per_graph_dist"] * s0["n_dist"])
         except (ValueError, KeyError):
             traffic = None
     line = {
@@ -280,12 +285,13 @@ def run_ours(a, rank, world, local):
                      "alg_bytes_per_launch": int(alg_bytes)},
         "gpu_launches": 3 * a.steps,
         "clocks": clocks,
-        "recall": round(ev["recall"], 6), "precision": round(ev["precision"], 6), "per_k": per_k,
+        "recall": None if ev["recall"] is None else round(ev["recall"], 6),
+        "precision": None if ev["precision"] is None else round(ev["precision"], 6), "per_k": per_k,
         "counters_per_query": {"graph_dist": round(s0["n_dist"] / nb, 1), "expansions": round(X / nb, 1),
                                "candidates": round(s0["n_cand"] / nb, 1), "verified": round(s0["n_pred"] / nb, 2)},
         "build_s": {k: round(v, 3) for k, v in ix.timings.items() if isinstance(v, float)},
     }
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+    if rank == 0 and world == 1 and not a.no_cpu_baseline and gt is not None:
         tmp = Path(a.keep) if a.keep else Path(tempfile.mkdtemp(prefix="anqi_bench_"))
         try:
             write_index_files(tmp, base, query, ix, ks, gt, ctx)
