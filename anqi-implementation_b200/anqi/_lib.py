@@ -120,6 +120,7 @@ _SIGS = {
     "anqi_query_download": [_vp, _u32, _vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp],
     "anqi_query_evaluate": [_vp, _u32, _u32, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double),
                             C.POINTER(C.c_double), C.POINTER(C.c_uint32)],
+    "anqi_rknn_query_noalloc": [_vp, _vp, C.c_uint32, _vp, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp],
     "anqi_exact_topk": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _u32, _f32],
     "anqi_rknn_ground_truth": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32, _u32, _u32, _f32,
                                C.c_uint64, C.POINTER(C.c_uint64)],

@@ -230,6 +230,47 @@ int anqi_query_evaluate(anqi_ctx* ctx, const uint32_t* gt_off, const uint32_t* g
                         double* recall_sum, double* precision_sum, double* cand_recall_sum,
                         uint32_t* nonempty);
 
+/* ------------------------------------------------ allocation-free query
+ * No counterpart in the reference: an extra entry point of this library for
+ * callers that cannot allocate device memory -- e.g. code inside a host
+ * framework whose device memory all comes from its own pool, or a process
+ * whose memory budget is fixed up front -- and so cannot use a context (which
+ * allocates).  Same search and postfilter as anqi_rknn_query for one k and one
+ * L, on index arrays the caller already holds in device memory; it allocates
+ * nothing.  Its working memory is a fixed file-scope device array of
+ * ANQI_NOALLOC_SCRATCH_BYTES that every GPU loading this library reserves
+ * until the process exits; n is limited by what fits in it (one visited
+ * bitmap of n/8 bytes per concurrent query: n up to about 130 million).  All calls on a device share that array: calls that overlap on
+ * the GPU race -- serialize them.  The first call on each device looks up the
+ * array (cudaGetSymbolAddress); make it before any stream capture.
+ * Arrays are device pointers; rows 16-byte aligned, strides multiples of 4
+ * floats; queries nq x base_stride.  pred_ids receives up to max_pred ids per
+ * query (row q at q * max_pred), pred_count the full count; returns
+ * ANQI_ERR_CAPACITY if any count exceeded max_pred or a query's candidate list
+ * exceeded 8192 entries, ANQI_ERR_ARGS for bad sizes or alignment. */
+#define ANQI_NOALLOC_SCRATCH_BYTES (16u << 20)
+typedef struct {
+    uint64_t n;
+    uint32_t d, degree;
+    const float* base;            /* n x base_stride */
+    uint32_t base_stride;
+    const float* lifted;          /* n x lifted_stride (>= d + 2) */
+    uint32_t lifted_stride;
+    const uint32_t* deg;          /* n */
+    const uint32_t* links;        /* n x degree */
+    uint32_t tree_nodes;          /* post-order, root last */
+    const uint32_t* tree_left;
+    const uint32_t* tree_right;
+    const float* tree_offset;
+    const float* tree_hyperplane; /* tree_nodes x lifted_stride */
+    const uint32_t* tree_leaf_first;
+    double scale, mstar2;
+} anqi_device_index;
+
+int anqi_rknn_query_noalloc(const anqi_device_index* ix, const float* queries, uint32_t nq,
+                            const float* thresholds, uint32_t L, uint32_t max_pred, uint32_t* pred_count,
+                            uint32_t* pred_ids, uint32_t* n_dist, void* stream);
+
 /* ---------------------------------------------------- exact ground truth
  * tools/dataset_gt.cpp:206-313 in FP32 with the reference's summation order:
  * per base row the K nearest other rows by (key, id), key = |a|^2+|b|^2-2ab. */
