@@ -53,7 +53,7 @@ class QueryStats(C.Structure):
     _fields_ = [
         ("n_dist", C.c_uint64), ("n_expand", C.c_uint64), ("n_cand", C.c_uint64), ("n_pred", C.c_uint64),
         ("n_flood", C.c_uint64), ("search_ms", C.c_float), ("total_ms", C.c_float), ("h2d_bytes", C.c_uint64),
-        ("d2h_bytes", C.c_uint64),
+        ("d2h_bytes", C.c_uint64), ("visited_table", C.c_uint32),
     ]
 
 

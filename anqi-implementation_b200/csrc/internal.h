@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -80,10 +81,16 @@ struct Ctx {
     DevBuf err, counters;
     DevBuf vis_bits, vis_log, cand_scratch;
     uint32_t vis_slots = 0, vis_words = 0, log_cap = 0, cand_cap = 0;
+    // resident ground truth (anqi_gt_load) and evaluation scratch
+    DevBuf gt_off, gt_ids, eval_rows, eval_sums;
+    uint32_t gt_nq = 0;
     // last entry tree from anqi_graph_build
     std::vector<uint32_t> t_left, t_right, t_leaf_off, t_leaf_cnt, t_perm;
     std::vector<float> t_offset, t_hyper;
     uint32_t t_nodes = 0, t_dim = 0;
+    // search-kernel autotuning: configuration key -> shared-memory visited table size
+    std::unordered_map<uint64_t, uint32_t> tuned;
+    uint32_t last_hash_cap = 0;
     uint64_t device_bytes = 0;
     std::vector<DevBuf*> member_bufs() {
         return {&ix.base, &ix.lifted, &ix.onorm, &ix.deg, &ix.links, &ix.tleft, &ix.tright, &ix.toffset,
@@ -91,7 +98,7 @@ struct Ctx {
                 &batch.qL, &batch.qslot, &batch.npred, &batch.ncand, &batch.ndist, &batch.nexp, &batch.nflood,
                 &batch.pred_at, &batch.cand_at, &batch.pred_buf, &batch.cand_buf, &batch.pred_off,
                 &batch.cand_off, &batch.pred_csr, &batch.cand_csr, &err, &counters, &vis_bits, &vis_log,
-                &cand_scratch, &thr_table};
+                &cand_scratch, &thr_table, &gt_off, &gt_ids, &eval_rows, &eval_sums};
     }
     // Per-object thresholds for up to kThrSlots values of k: slot s holds
     // thr_k[s] (0 = unused) in thr_table[s * n .. (s+1) * n).

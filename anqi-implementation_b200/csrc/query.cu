@@ -20,6 +20,7 @@
 // log of set bits.
 #include <algorithm>
 #include <cfloat>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "internal.h"
@@ -66,6 +67,8 @@ struct SearchParams {
     unsigned long long* pred_at;
     unsigned long long* cand_at;
     uint32_t* err;
+    uint32_t hash_cap;    // shared-memory visited table entries per warp (power of two, 0 = bitmap only)
+    uint32_t hash_shift;  // 32 - log2(hash_cap)
 };
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
@@ -76,22 +79,63 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
-// Visits the links of node: collects the ids seen for the first time into
-// ni[0..m) in link-slot order and logs them.  Returns m.
-__device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t node, uint32_t* bits,
-                                                 uint32_t* vlog, uint32_t& nlog, uint32_t* ni, uint32_t lane) {
-    const uint32_t* lk = p.links + (size_t)node * p.degree;
-    const uint32_t dg = min(p.deg[node], p.degree);
-    uint32_t id0 = kEmpty, id1 = kEmpty;
+// The visited set of one query.  While small it is an open-addressing table
+// in the warp's shared memory (atomicCAS, linear probing, kept below 5/8
+// load); before an expansion could push it past that, its ids move into the
+// slot's global bitmap and the query continues there ("global" mode).  The
+// bitmap is cleared afterwards by replaying the log of ids it received.
+struct Visited {
+    uint32_t* tab;
+    uint32_t cap, shift;
+    uint32_t* bits;
+    uint32_t* vlog;
+    uint32_t log_cap;
+    bool global;
+};
+
+__device__ __forceinline__ bool vis_first(Visited& v, uint32_t id, uint32_t* err) {
+    if (v.global) return visit_first(v.bits, id);
+    uint32_t h = (id * 0x9E3779B1u) >> v.shift;
+    for (uint32_t probe = 0; probe < v.cap; probe++) {
+        const uint32_t old = atomicCAS(v.tab + h, kEmpty, id);
+        if (old == kEmpty) return true;
+        if (old == id) return false;
+        h = (h + 1) & (v.cap - 1);
+    }
+    set_error(err, kDevWaitTimeout);  // unreachable below 5/8 load
+    return false;
+}
+
+// Moves every id of the table into the bitmap and the log (warp-collective).
+__device__ void vis_migrate(Visited& v, uint32_t lane) {
+    uint32_t pos0 = 0;
+    for (uint32_t t0 = 0; t0 < v.cap; t0 += 32) {
+        const uint32_t id = v.tab[t0 + lane];
+        const bool has = id != kEmpty;
+        if (has) atomicOr(v.bits + (id >> 5), 1u << (id & 31u));
+        const unsigned b = __ballot_sync(kFull, has);
+        if (has) {
+            const uint32_t pos = pos0 + __popc(b & lanemask_lt());
+            if (pos < v.log_cap) v.vlog[pos] = id;
+        }
+        pos0 += __popc(b);
+    }
+    __syncwarp();
+    v.global = true;
+}
+
+// Visits the links of node (slots l0 = link[lane], l1 = link[lane + 32], dg =
+// degree): collects the ids seen for the first time into ni[0..m) in link-slot
+// order, logging them when the bitmap is in use.  Returns m.
+__device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t l0, uint32_t l1, uint32_t dg,
+                                                 Visited& vis, uint32_t& nlog, uint32_t* ni, uint32_t lane) {
     bool f0 = false, f1 = false, bad = false;
     if (lane < dg) {
-        id0 = lk[lane];
-        if (id0 < p.n) f0 = visit_first(bits, id0);
+        if (l0 < p.n) f0 = vis_first(vis, l0, p.err);
         else bad = true;
     }
     if (lane + 32 < dg) {
-        id1 = lk[lane + 32];
-        if (id1 < p.n) f1 = visit_first(bits, id1);
+        if (l1 < p.n) f1 = vis_first(vis, l1, p.err);
         else bad = true;
     }
     if (bad) set_error(p.err, kDevBadId);
@@ -99,17 +143,60 @@ __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t
     const uint32_t c0 = __popc(b0), lt = lanemask_lt();
     const uint32_t p0 = __popc(b0 & lt), p1 = c0 + __popc(b1 & lt);
     if (f0) {
-        ni[p0] = id0;
-        if (nlog + p0 < p.log_cap) vlog[nlog + p0] = id0;
+        ni[p0] = l0;
+        if (vis.global && nlog + p0 < p.log_cap) vis.vlog[nlog + p0] = l0;
     }
     if (f1) {
-        ni[p1] = id1;
-        if (nlog + p1 < p.log_cap) vlog[nlog + p1] = id1;
+        ni[p1] = l1;
+        if (vis.global && nlog + p1 < p.log_cap) vis.vlog[nlog + p1] = l1;
     }
     const uint32_t m = c0 + __popc(b1);
     nlog += m;
     __syncwarp();
     return m;
+}
+
+__device__ __forceinline__ void load_links(const SearchParams& p, uint32_t node, uint32_t lane, uint32_t& l0,
+                                           uint32_t& l1, uint32_t& dg) {
+    const uint32_t* lk = p.links + (size_t)node * p.degree;
+    dg = min(p.deg[node], p.degree);
+    l0 = lane < p.degree ? lk[lane] : kEmpty;
+    l1 = lane + 32 < p.degree ? lk[lane + 32] : kEmpty;
+}
+
+// Sorts the m (<= 64) fresh (dist, id) entries in nd/ni ascending.  Small
+// batches (the common case after the first expansions) are ranked by counting;
+// larger ones use the register bitonic network.
+__device__ __forceinline__ void sort_fresh(float* nd, uint32_t* ni, uint32_t m, uint32_t lane) {
+    if (m <= 32) {
+        const float dv = lane < m ? nd[lane] : 0.f;
+        const uint32_t iv = lane < m ? ni[lane] : kEmpty;
+        uint32_t rank = 0;
+        for (uint32_t s = 0; s < m; s++) {
+            const float ds = __shfl_sync(kFull, dv, s);
+            const uint32_t is = __shfl_sync(kFull, iv, s);
+            rank += nb_less(ds, is, dv, iv) ? 1u : 0u;
+        }
+        __syncwarp();
+        if (lane < m) {
+            nd[rank] = dv;
+            ni[rank] = iv;
+        }
+        __syncwarp();
+        return;
+    }
+    const float inf = __int_as_float(0x7f800000);
+    float d0 = lane < m ? nd[lane] : inf;
+    uint32_t i0 = lane < m ? ni[lane] : kEmpty;
+    float d1 = lane + 32 < m ? nd[lane + 32] : inf;
+    uint32_t i1 = lane + 32 < m ? ni[lane + 32] : kEmpty;
+    warp_sort64(d0, i0, d1, i1);
+    __syncwarp();
+    nd[lane] = d0;
+    ni[lane] = i0;
+    nd[lane + 32] = d1;
+    ni[lane + 32] = i1;
+    __syncwarp();
 }
 
 // Distances of the m fresh neighbours to the lifted query: 8 groups of 4 lanes.
@@ -156,10 +243,14 @@ __device__ __forceinline__ void append_in_range(const SearchParams& p, const flo
 
 extern __shared__ __align__(16) unsigned char g_smem[];
 
+__device__ __forceinline__ size_t search_smem_words(uint32_t L_max, uint32_t lstride, uint32_t bstride, uint32_t hash_cap) {
+    return (size_t)4 * L_max + 128 + lstride + bstride + hash_cap;
+}
+
 __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
-    const size_t per_warp = (size_t)(4 * p.L_max + 128 + p.lstride + p.bstride) * 4;
+    const size_t per_warp = search_smem_words(p.L_max, p.lstride, p.bstride, p.hash_cap) * 4;
     unsigned char* my = g_smem + wib * per_warp;
     float* qhat = reinterpret_cast<float*>(my);
     float* qraw = qhat + p.lstride;
@@ -169,10 +260,15 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
     uint32_t* biB = reinterpret_cast<uint32_t*>(bdB + p.L_max);
     float* nd = reinterpret_cast<float*>(biB + p.L_max);
     uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 64);
+    uint32_t* tab = ni + 64;
     uint32_t* bits = p.vis_bits + (size_t)slot * p.vis_words;
     uint32_t* vlog = p.vis_log + (size_t)slot * p.log_cap;
     uint32_t* cl = p.cand_scratch + (size_t)slot * p.cand_cap;
     VisitSlot vs{bits, vlog, p.log_cap, p.vis_words};
+    for (uint32_t t = lane; t < p.hash_cap; t += 32) tab[t] = kEmpty;
+    __syncwarp();
+    // migrate before an expansion could take the table past 5/8 load
+    const uint32_t hash_limit = p.hash_cap ? p.hash_cap / 8 * 5 : 0;
 
     for (;;) {
         uint32_t qi = 0;
@@ -201,10 +297,11 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
         uint32_t ep = p.tleaf[v];
         if (ep == kEmpty || ep >= p.n) ep = 0;
 
+        Visited vis{tab, p.hash_cap, p.hash_shift, bits, vlog, p.log_cap, p.hash_cap == 0};
         const float dep = group_l2sqr(p.lifted + (size_t)ep * p.lstride, qhat, p.dim, gt, kFull);
         if (lane == 0) {
-            visit_first(bits, ep);
-            if (p.log_cap) vlog[0] = ep;
+            vis_first(vis, ep, p.err);
+            if (vis.global && p.log_cap) vlog[0] = ep;
             bdA[0] = dep;
             biA[0] = ep;
         }
@@ -220,6 +317,8 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
         float* od = bdB;
         uint32_t* oi = biB;
         uint32_t size = 1, cur = 0;
+        // links of the node expected next, loaded one expansion ahead
+        uint32_t pre_node = kEmpty, pl0 = kEmpty, pl1 = kEmpty, pdg = 0;
 
         // ---- greedy beam, index.h:1613-1624
         while (cur < size && !overflow) {
@@ -238,7 +337,18 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
                     break;
                 }
             }
-            const uint32_t m = expand_links(p, node, bits, vlog, nlog, ni, lane);
+            uint32_t l0, l1, dg;
+            if (node == pre_node) {
+                l0 = pl0;
+                l1 = pl1;
+                dg = pdg;
+            } else {
+                load_links(p, node, lane, l0, l1, dg);
+            }
+            pre_node = nxt < size ? (bi[nxt] & kIdMask) : kEmpty;
+            if (pre_node != kEmpty) load_links(p, pre_node, lane, pl0, pl1, pdg);
+            if (!vis.global && nlog + p.degree > hash_limit) vis_migrate(vis, lane);
+            const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane);
             if (m == 0) {
                 cur = nxt;
                 continue;
@@ -246,19 +356,7 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
             fresh_distances(p, qhat, ni, nd, m, gw, gt);
             append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
             // batch insert = merge of the sorted batch into the sorted beam
-            float d0 = lane < m ? nd[lane] : FLT_MAX;
-            uint32_t i0 = lane < m ? ni[lane] : kEmpty;
-            float d1 = lane + 32 < m ? nd[lane + 32] : FLT_MAX;
-            uint32_t i1 = lane + 32 < m ? ni[lane + 32] : kEmpty;
-            if (lane >= m) d0 = __int_as_float(0x7f800000);
-            if (lane + 32 >= m) d1 = __int_as_float(0x7f800000);
-            warp_sort64(d0, i0, d1, i1);
-            __syncwarp();
-            nd[lane] = d0;
-            ni[lane] = i0;
-            nd[lane + 32] = d1;
-            ni[lane + 32] = i1;
-            __syncwarp();
+            sort_fresh(nd, ni, m, lane);
             const uint32_t ns = min(L, size + m);
             for (uint32_t p0 = lane; p0 < size; p0 += 32) {
                 const float dv = bd[p0];
@@ -294,10 +392,27 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
 
         // ---- bounded flood, index.h:1626-1638
         uint32_t head = 0;
+        if (head < ncand && !overflow) {
+            pre_node = cl[0];
+            load_links(p, pre_node, lane, pl0, pl1, pdg);
+        }
         while (head < ncand && !overflow) {
             const uint32_t node = cl[head++];
             nfl++;
-            const uint32_t m = expand_links(p, node, bits, vlog, nlog, ni, lane);
+            uint32_t l0, l1, dg;
+            if (node == pre_node) {
+                l0 = pl0;
+                l1 = pl1;
+                dg = pdg;
+            } else {
+                load_links(p, node, lane, l0, l1, dg);
+            }
+            if (head < ncand) {
+                pre_node = cl[head];
+                load_links(p, pre_node, lane, pl0, pl1, pdg);
+            }
+            if (!vis.global && nlog + p.degree > hash_limit) vis_migrate(vis, lane);
+            const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane);
             if (m == 0) continue;
             fresh_distances(p, qhat, ni, nd, m, gw, gt);
             append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
@@ -348,7 +463,9 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
         at = __shfl_sync(kFull, at, 0);
         if (at + npred <= p.pred_cap)
             for (uint32_t i = lane; i < npred; i += 32) p.pred_buf[at + i] = cl[i];
-        visit_clear(vs, nlog);
+        if (vis.global) visit_clear(vs, nlog);
+        for (uint32_t t = lane; t < p.hash_cap; t += 32) tab[t] = kEmpty;
+        __syncwarp();
     }
 }
 
@@ -437,6 +554,40 @@ __global__ void evaluate_kernel(const uint32_t* __restrict__ pred_off, const uin
     }
 }
 
+// Sums of the per-query metrics over queries with non-empty truth, in a fixed
+// order (thread t owns a contiguous range; thread 0 adds the partials in t
+// order), so the result does not depend on scheduling.  out: recall,
+// precision, F1, candidate recall, |C|, |P|, graph distances, count.
+__global__ void eval_sums_kernel(const double* __restrict__ rows, const uint32_t* __restrict__ npred,
+                                 const uint32_t* __restrict__ ncand, const uint32_t* __restrict__ ndist,
+                                 uint32_t nq, double* __restrict__ out) {
+    __shared__ double part[256][8];
+    const uint32_t t = threadIdx.x, T = blockDim.x;
+    const uint32_t chunk = (nq + T - 1) / T;
+    const uint32_t b = min(nq, t * chunk), e = min(nq, b + chunk);
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t q = b; q < e; q++) {
+        const double r = rows[3 * (size_t)q], p = rows[3 * (size_t)q + 1];
+        if (r != r) continue;
+        acc[0] += r;
+        acc[1] += p;
+        acc[2] += (r + p > 0.0) ? 2.0 * r * p / (r + p) : 0.0;
+        acc[3] += rows[3 * (size_t)q + 2];
+        acc[4] += (double)ncand[q];
+        acc[5] += (double)npred[q];
+        acc[6] += (double)ndist[q];
+        acc[7] += 1.0;
+    }
+    for (int j = 0; j < 8; j++) part[t][j] = acc[j];
+    __syncthreads();
+    if (t == 0) {
+        double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (uint32_t i = 0; i < T; i++)
+            for (int j = 0; j < 8; j++) s[j] += part[i][j];
+        for (int j = 0; j < 8; j++) out[j] = s[j];
+    }
+}
+
 static int slot_for_k(Ctx* c, uint32_t k) {
     for (int s = 0; s < Ctx::kThrSlots; s++)
         if (c->thr_k[s] == k) return s;
@@ -459,8 +610,28 @@ static int ensure_thr_table(Ctx* c, uint64_t n) {
     return ensure(c, c->thr_table, (size_t)Ctx::kThrSlots * n * 4);
 }
 
-static size_t search_smem_per_warp(const Ctx* c, uint32_t L_max) {
-    return (size_t)(4 * L_max + 128 + c->ix.lstride + c->ix.bstride) * 4;
+static size_t search_smem_per_warp(const Ctx* c, uint32_t L_max, uint32_t hash_cap) {
+    return (size_t)(4 * L_max + 128 + c->ix.lstride + c->ix.bstride + hash_cap) * 4;
+}
+
+struct SearchCfg {
+    uint32_t hash_cap = 0;
+    uint32_t blocks = 0;
+    size_t smem = 0;
+};
+
+static int search_cfg(Ctx* c, uint32_t hash_cap, SearchCfg& cfg) {
+    const Batch& b = c->batch;
+    const int wpb = 4;
+    cfg.hash_cap = hash_cap;
+    cfg.smem = search_smem_per_warp(c, b.L_max, hash_cap) * wpb;
+    if (cfg.smem > 227 * 1024) return ANQI_ERR_ARGS;
+    ANQI_CUDA(c, cudaFuncSetAttribute(rknn_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+    int per_sm = 0;
+    ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rknn_search_kernel, 32 * wpb, cfg.smem));
+    if (per_sm < 1) return ANQI_ERR_ARGS;
+    cfg.blocks = std::min<uint32_t>((uint32_t)per_sm * c->sm_count, (b.nq + wpb - 1) / wpb);
+    return ANQI_OK;
 }
 
 }  // namespace anqi
@@ -563,6 +734,7 @@ int anqi_query_upload(anqi_ctx* h, const float* queries, uint32_t nq, const uint
     Batch& b = c->batch;
     b.nq = nq;
     b.have_results = false;
+    c->gt_nq = 0;  // a resident ground truth belongs to the previous batch
     std::vector<uint8_t> slots;
     uint32_t slot_all = 0;
     if (k_per_query) {
@@ -604,6 +776,84 @@ int anqi_query_upload(anqi_ctx* h, const float* queries, uint32_t nq, const uint
     return sync(c);
 }
 
+// One search launch with configuration cfg; ms = its device time.  Returns
+// ANQI_ERR_CAPACITY (and the needed fill) when an output buffer was too small.
+static int launch_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, float* ms, unsigned long long* fill) {
+    Batch& b = c->batch;
+    const QueryIndex& ix = c->ix;
+    int rc;
+    if ((rc = ensure(c, b.pred_buf, b.pred_cap * 4))) return rc;
+    if (keep_candidates && (rc = ensure(c, b.cand_buf, b.cand_cap * 4))) return rc;
+    ANQI_CUDA(c, cudaMemsetAsync(c->counters.p, 0, 64, c->stream));
+    SearchParams p{};
+    p.lifted = ix.lifted.as<float>();
+    p.base = ix.base.as<float>();
+    p.onorm = ix.onorm.as<float>();
+    p.links = ix.links.as<uint32_t>();
+    p.deg = ix.deg.as<uint32_t>();
+    p.tleft = ix.tleft.as<uint32_t>();
+    p.tright = ix.tright.as<uint32_t>();
+    p.toffset = ix.toffset.as<float>();
+    p.thyper = ix.thyper.as<float>();
+    p.tleaf = ix.tleaf.as<uint32_t>();
+    p.n = ix.n;
+    p.dim = ix.dim;
+    p.d = ix.d;
+    p.lstride = ix.lstride;
+    p.bstride = ix.bstride;
+    p.degree = ix.degree;
+    p.troot = ix.troot;
+    p.scale = ix.scale;
+    p.R2 = ix.mstar2 + 1.0;  // rknn_query.cpp:2729, eps = 0
+    p.thr = c->thr_table.as<float>();
+    p.queries = b.q.as<float>();
+    p.qL = b.has_L ? b.qL.as<uint32_t>() : nullptr;
+    p.qslot = b.has_k ? b.qslot.as<uint8_t>() : nullptr;
+    p.L_all = b.L_all;
+    p.slot_all = b.k_all;
+    p.nq = b.nq;
+    p.L_max = b.L_max;
+    p.vis_bits = c->vis_bits.as<uint32_t>();
+    p.vis_words = c->vis_words;
+    p.vis_log = c->vis_log.as<uint32_t>();
+    p.log_cap = c->log_cap;
+    p.cand_scratch = c->cand_scratch.as<uint32_t>();
+    p.cand_cap = c->cand_cap;
+    p.work = c->counters.as<uint32_t>();
+    p.fill = reinterpret_cast<unsigned long long*>(c->counters.as<uint32_t>() + 4);
+    p.pred_buf = b.pred_buf.as<uint32_t>();
+    p.pred_cap = b.pred_cap;
+    p.cand_buf = keep_candidates ? b.cand_buf.as<uint32_t>() : nullptr;
+    p.cand_out_cap = keep_candidates ? b.cand_cap : 0;
+    p.keep_cand = keep_candidates;
+    p.npred = b.npred.as<uint32_t>();
+    p.ncand = b.ncand.as<uint32_t>();
+    p.ndist = b.ndist.as<uint32_t>();
+    p.nexp = b.nexp.as<uint32_t>();
+    p.nflood = b.nflood.as<uint32_t>();
+    p.pred_at = b.pred_at.as<unsigned long long>();
+    p.cand_at = b.cand_at.as<unsigned long long>();
+    p.err = c->err.as<uint32_t>();
+    p.hash_cap = cfg.hash_cap;
+    p.hash_shift = cfg.hash_cap ? 32u - (uint32_t)__builtin_ctz(cfg.hash_cap) : 0u;
+    ANQI_CUDA(c, cudaFuncSetAttribute(rknn_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+    ANQI_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    rknn_search_kernel<<<cfg.blocks, 128, cfg.smem, c->stream>>>(p);
+    ANQI_CUDA(c, cudaGetLastError());
+    ANQI_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    ANQI_CUDA(c, cudaMemcpyAsync(fill, p.fill, 16, cudaMemcpyDeviceToHost, c->stream));
+    uint32_t err = 0;
+    ANQI_CUDA(c, cudaMemcpyAsync(&err, c->err.p, 4, cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = sync(c))) return rc;
+    if (err == kDevOutOverflow) {
+        ANQI_CUDA(c, cudaMemsetAsync(c->err.p, 0, 4, c->stream));
+        return ANQI_ERR_CAPACITY;
+    }
+    if ((rc = check_device_error(c, "rknn search"))) return rc;
+    ANQI_CUDA(c, cudaEventElapsedTime(ms, c->ev0, c->ev1));
+    return ANQI_OK;
+}
+
 int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
     if (!h) return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
@@ -611,19 +861,19 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
     Batch& b = c->batch;
     if (!c->ix.loaded || b.nq == 0) return fail(c, ANQI_ERR_ARGS, "anqi_query_run: no index or batch");
     const QueryIndex& ix = c->ix;
-    const size_t smem_warp = search_smem_per_warp(c, b.L_max);
-    const int warps_per_block = 4;
-    const size_t smem = smem_warp * warps_per_block;
-    if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "beam width %u needs too much shared memory", b.L_max);
-    ANQI_CUDA(c, cudaFuncSetAttribute(rknn_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rknn_search_kernel, 32 * warps_per_block, smem));
-    if (per_sm < 1) return fail(c, ANQI_ERR_DEVICE, "search kernel does not fit on an SM");
-    uint32_t blocks = (uint32_t)per_sm * c->sm_count;
-    blocks = std::min<uint32_t>(blocks, (b.nq + warps_per_block - 1) / warps_per_block);
-    const uint32_t slots = blocks * warps_per_block;
     int rc;
-    // per-slot scratch
+    // candidate configurations: shared-memory visited table of 0 (bitmap only) .. 4096 entries
+    const char* forced = std::getenv("ANQI_B200_HASH");
+    std::vector<SearchCfg> cfgs;
+    for (uint32_t hc : {0u, 1024u, 2048u, 4096u}) {
+        if (forced && std::strtoul(forced, nullptr, 10) != hc) continue;
+        SearchCfg g;
+        if (search_cfg(c, hc, g) == ANQI_OK) cfgs.push_back(g);
+    }
+    if (cfgs.empty()) return fail(c, ANQI_ERR_ARGS, "beam width %u needs too much shared memory", b.L_max);
+    uint32_t slots = 0;
+    for (const SearchCfg& g : cfgs) slots = std::max(slots, g.blocks * 4);
+    // per-slot scratch (bitmap, log, candidate list) for the largest configuration
     const uint32_t words = (uint32_t)((ix.n + 31) / 32);
     const uint32_t log_cap = (uint32_t)std::min<uint64_t>(ix.n, 16384);
     const uint32_t cand_cap = (uint32_t)std::min<uint64_t>(ix.n, 65536);
@@ -640,77 +890,42 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
     }
     if (b.pred_cap == 0) b.pred_cap = std::max<uint64_t>(1024, (uint64_t)b.nq * 128);
     if (keep_candidates && b.cand_cap == 0) b.cand_cap = std::max<uint64_t>(1024, (uint64_t)b.nq * 256);
+    // autotune once per (n, L_max, nq): time every configuration, keep the fastest
+    const uint64_t key = ix.n * 1000003ull ^ ((uint64_t)b.L_max << 40) ^ ((uint64_t)b.nq << 20);
+    SearchCfg best = cfgs[0];
+    auto it = c->tuned.find(key);
+    if (it != c->tuned.end()) {
+        for (const SearchCfg& g : cfgs)
+            if (g.hash_cap == it->second) best = g;
+    } else if (cfgs.size() > 1) {
+        float best_ms = 1e30f;
+        for (const SearchCfg& g : cfgs) {
+            float ms = 0;
+            unsigned long long fill[2];
+            rc = launch_search(c, g, 0, &ms, fill);
+            if (rc == ANQI_ERR_CAPACITY) {
+                b.pred_cap = std::max<uint64_t>(b.pred_cap, fill[0] + 1024);
+                rc = launch_search(c, g, 0, &ms, fill);
+            }
+            if (rc) return rc;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = g;
+            }
+        }
+        c->tuned[key] = best.hash_cap;
+    }
+    c->last_hash_cap = best.hash_cap;
     for (int attempt = 0; attempt < 3; attempt++) {
-        if ((rc = ensure(c, b.pred_buf, b.pred_cap * 4))) return rc;
-        if (keep_candidates && (rc = ensure(c, b.cand_buf, b.cand_cap * 4))) return rc;
-        ANQI_CUDA(c, cudaMemsetAsync(c->counters.p, 0, 64, c->stream));
-        SearchParams p{};
-        p.lifted = ix.lifted.as<float>();
-        p.base = ix.base.as<float>();
-        p.onorm = ix.onorm.as<float>();
-        p.links = ix.links.as<uint32_t>();
-        p.deg = ix.deg.as<uint32_t>();
-        p.tleft = ix.tleft.as<uint32_t>();
-        p.tright = ix.tright.as<uint32_t>();
-        p.toffset = ix.toffset.as<float>();
-        p.thyper = ix.thyper.as<float>();
-        p.tleaf = ix.tleaf.as<uint32_t>();
-        p.n = ix.n;
-        p.dim = ix.dim;
-        p.d = ix.d;
-        p.lstride = ix.lstride;
-        p.bstride = ix.bstride;
-        p.degree = ix.degree;
-        p.troot = ix.troot;
-        p.scale = ix.scale;
-        p.R2 = ix.mstar2 + 1.0;  // rknn_query.cpp:2729, eps = 0
-        p.thr = c->thr_table.as<float>();
-        p.queries = b.q.as<float>();
-        p.qL = b.has_L ? b.qL.as<uint32_t>() : nullptr;
-        p.qslot = b.has_k ? b.qslot.as<uint8_t>() : nullptr;
-        p.L_all = b.L_all;
-        p.slot_all = b.k_all;
-        p.nq = b.nq;
-        p.L_max = b.L_max;
-        p.vis_bits = c->vis_bits.as<uint32_t>();
-        p.vis_words = words;
-        p.vis_log = c->vis_log.as<uint32_t>();
-        p.log_cap = log_cap;
-        p.cand_scratch = c->cand_scratch.as<uint32_t>();
-        p.cand_cap = cand_cap;
-        p.work = c->counters.as<uint32_t>();
-        p.fill = reinterpret_cast<unsigned long long*>(c->counters.as<uint32_t>() + 4);
-        p.pred_buf = b.pred_buf.as<uint32_t>();
-        p.pred_cap = b.pred_cap;
-        p.cand_buf = keep_candidates ? b.cand_buf.as<uint32_t>() : nullptr;
-        p.cand_out_cap = keep_candidates ? b.cand_cap : 0;
-        p.keep_cand = keep_candidates;
-        p.npred = b.npred.as<uint32_t>();
-        p.ncand = b.ncand.as<uint32_t>();
-        p.ndist = b.ndist.as<uint32_t>();
-        p.nexp = b.nexp.as<uint32_t>();
-        p.nflood = b.nflood.as<uint32_t>();
-        p.pred_at = b.pred_at.as<unsigned long long>();
-        p.cand_at = b.cand_at.as<unsigned long long>();
-        p.err = c->err.as<uint32_t>();
-        ANQI_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-        rknn_search_kernel<<<blocks, 32 * warps_per_block, smem, c->stream>>>(p);
-        ANQI_CUDA(c, cudaGetLastError());
-        ANQI_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+        float ms = 0;
         unsigned long long fill[2] = {0, 0};
-        ANQI_CUDA(c, cudaMemcpyAsync(fill, p.fill, 16, cudaMemcpyDeviceToHost, c->stream));
-        uint32_t err = 0;
-        ANQI_CUDA(c, cudaMemcpyAsync(&err, c->err.p, 4, cudaMemcpyDeviceToHost, c->stream));
-        if ((rc = sync(c))) return rc;
-        if (err == kDevOutOverflow) {
-            ANQI_CUDA(c, cudaMemsetAsync(c->err.p, 0, 4, c->stream));
+        rc = launch_search(c, best, keep_candidates, &ms, fill);
+        if (rc == ANQI_ERR_CAPACITY) {
             b.pred_cap = std::max<uint64_t>(b.pred_cap, fill[0] + 1024);
             if (keep_candidates) b.cand_cap = std::max<uint64_t>(b.cand_cap, fill[1] + 1024);
             continue;
         }
-        if ((rc = check_device_error(c, "rknn search"))) return rc;
-        float ms = 0;
-        ANQI_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        if (rc) return rc;
         // CSR offsets + compaction
         scan_counts_kernel<<<1, 1024, 0, c->stream>>>(b.npred.as<uint32_t>(), b.nq, b.pred_off.as<uint32_t>());
         if ((rc = ensure(c, b.pred_csr, std::max<uint64_t>(fill[0], 1) * 4))) return rc;
@@ -729,7 +944,10 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
         ANQI_CUDA(c, cudaGetLastError());
         b.have_results = true;
         b.have_cands = keep_candidates != 0;
-        if (st) st->search_ms = ms;
+        if (st) {
+            st->search_ms = ms;
+            st->visited_table = best.hash_cap;
+        }
         return sync(c);
     }
     return fail(c, ANQI_ERR_CAPACITY, "rknn search: output capacity could not be satisfied");
@@ -849,6 +1067,56 @@ int anqi_query_evaluate(anqi_ctx* h, const uint32_t* gt_off, const uint32_t* gt_
     if (precision_sum) *precision_sum = p;
     if (cand_recall_sum) *cand_recall_sum = cr;
     if (nonempty) *nonempty = ne;
+    return ANQI_OK;
+}
+
+int anqi_gt_load(anqi_ctx* h, const uint32_t* gt_off, const uint32_t* gt_ids, uint64_t gt_total) {
+    if (!h || !gt_off || (gt_total && !gt_ids)) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    Batch& b = c->batch;
+    if (b.nq == 0) return fail(c, ANQI_ERR_ARGS, "anqi_gt_load: upload the query batch first");
+    if (gt_off[0] != 0 || gt_off[b.nq] != gt_total) return fail(c, ANQI_ERR_FORMAT, "ground-truth offsets disagree");
+    std::vector<uint32_t> sorted(gt_ids, gt_ids + gt_total);
+    for (uint32_t q = 0; q < b.nq; q++) {
+        if (gt_off[q + 1] < gt_off[q]) return fail(c, ANQI_ERR_FORMAT, "ground-truth offsets not ascending");
+        std::sort(sorted.begin() + gt_off[q], sorted.begin() + gt_off[q + 1]);
+    }
+    int rc;
+    if ((rc = h2d(c, c->gt_off, gt_off, (b.nq + 1ull) * 4)) || (rc = h2d(c, c->gt_ids, sorted.data(), gt_total * 4 + 4)) ||
+        (rc = ensure(c, c->eval_rows, b.nq * 24ull)) || (rc = ensure(c, c->eval_sums, 64)))
+        return rc;
+    c->gt_nq = b.nq;
+    return sync(c);
+}
+
+int anqi_query_evaluate_sums(anqi_ctx* h, anqi_eval_sums* out) {
+    if (!h || !out) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    Batch& b = c->batch;
+    if (!b.have_results) return fail(c, ANQI_ERR_ARGS, "anqi_query_evaluate_sums: no results");
+    if (c->gt_nq != b.nq || !c->gt_off.p) return fail(c, ANQI_ERR_ARGS, "anqi_query_evaluate_sums: no ground truth for this batch");
+    evaluate_kernel<<<c->sm_count * 4, 256, 0, c->stream>>>(
+        b.pred_off.as<uint32_t>(), b.pred_csr.as<uint32_t>(), b.have_cands ? b.cand_off.as<uint32_t>() : nullptr,
+        b.have_cands ? b.cand_csr.as<uint32_t>() : nullptr, c->gt_off.as<uint32_t>(), c->gt_ids.as<uint32_t>(), b.nq,
+        c->eval_rows.as<double>());
+    eval_sums_kernel<<<1, 256, 0, c->stream>>>(c->eval_rows.as<double>(), b.npred.as<uint32_t>(),
+                                               b.ncand.as<uint32_t>(), b.ndist.as<uint32_t>(), b.nq,
+                                               c->eval_sums.as<double>());
+    ANQI_CUDA(c, cudaGetLastError());
+    double s[8];
+    ANQI_CUDA(c, cudaMemcpyAsync(s, c->eval_sums.p, 64, cudaMemcpyDeviceToHost, c->stream));
+    int rc;
+    if ((rc = sync(c))) return rc;
+    out->recall = s[0];
+    out->precision = s[1];
+    out->f1 = s[2];
+    out->cand_recall = s[3];
+    out->cand = s[4];
+    out->pred = s[5];
+    out->graph_dist = s[6];
+    out->nonempty = (uint32_t)s[7];
     return ANQI_OK;
 }
 

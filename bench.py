@@ -282,7 +282,8 @@ def run_ours(a, rank, world, local):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
                      "kernel": "rknn_search_kernel", "kernel_ms": round(kernel_ms, 4),
-                     "alg_bytes_per_launch": int(alg_bytes)},
+                     "alg_bytes_per_launch": int(alg_bytes),
+                     "visited_table": int(stats[-1]["visited_table"])},
         "gpu_launches": 3 * a.steps,
         "clocks": clocks,
         "recall": None if ev["recall"] is None else round(ev["recall"], 6),

@@ -207,6 +207,8 @@ typedef struct {
     float search_ms;      /* device time of the search kernel (CUDA events on its stream) */
     float total_ms;       /* device time from first copy to last copy of the call */
     uint64_t h2d_bytes, d2h_bytes;
+    uint32_t visited_table; /* entries of the per-warp shared-memory visited table the search
+                               ran with (chosen by timing; 0 = global bitmap only) */
 } anqi_query_stats;
 
 int anqi_rknn_query(anqi_ctx* ctx, const float* queries, uint32_t nq, const uint32_t* k_per_query,
@@ -229,6 +231,21 @@ int anqi_query_download(anqi_ctx* ctx, uint32_t* pred_off, uint32_t* pred_ids, u
 int anqi_query_evaluate(anqi_ctx* ctx, const uint32_t* gt_off, const uint32_t* gt_ids, uint64_t gt_total,
                         double* recall_sum, double* precision_sum, double* cand_recall_sum,
                         uint32_t* nonempty);
+
+/* Resident form of the evaluation for timed loops: anqi_gt_load keeps a
+ * ground-truth CSR (_rknn_gt.bin layout: nq+1 offsets, ids in any order) on
+ * the device for the current batch; anqi_query_evaluate_sums then reduces the
+ * last run's per-query metrics on the device, in a fixed order, into sums over
+ * the queries with non-empty truth -- the accumulators of
+ * rknn_query.cpp:2784-2799 (recall, precision, F1, candidate recall, |C|, |P|,
+ * graph distances).  Candidate recall needs a run with keep_candidates. */
+typedef struct {
+    double recall, precision, f1, cand_recall;
+    double cand, pred, graph_dist;
+    uint32_t nonempty;
+} anqi_eval_sums;
+int anqi_gt_load(anqi_ctx* ctx, const uint32_t* gt_off, const uint32_t* gt_ids, uint64_t gt_total);
+int anqi_query_evaluate_sums(anqi_ctx* ctx, anqi_eval_sums* out);
 
 /* ------------------------------------------------ allocation-free query
  * No counterpart in the reference: an extra entry point of this library for

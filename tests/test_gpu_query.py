@@ -151,7 +151,16 @@ def random_index():
     return _random_index()
 
 
-def test_query_bit_exact_vs_oracle_random(ctx, random_index):
+_ORACLE_CACHE = {}
+
+
+@pytest.mark.parametrize("table", [None, "0", "1024", "4096"])
+def test_query_bit_exact_vs_oracle_random(ctx, random_index, table, monkeypatch):
+    """Every visited-set form (autotuned; global bitmap only; shared-memory
+    tables of 1024 and 4096 entries, which L=1000 pushes into migration to
+    the bitmap) returns the oracle's candidates, #dist and verified lists."""
+    if table is not None:
+        monkeypatch.setenv("ANQI_B200_HASH", table)
     base, query, lifted, links, deg, tree, sc, m2, thr = random_index
     ctx.index_load(base, lifted, deg, links, tree, sc, m2)
     ta = ol.TreeArrays(tree.left, tree.right, tree.offset, tree.hyperplane, tree.leaf_first())
@@ -159,7 +168,11 @@ def test_query_bit_exact_vs_oracle_random(ctx, random_index):
         ctx.set_thresholds(k, thr[k])
         for L in (8, 48, 200, 1000):
             r = ctx.rknn_query(query, k, L, keep_candidates=True)
-            cands, preds, nds = ol.range_search_all(lifted, links, deg, base, ta, sc, m2, query, thr[k], L)
+            if table is not None:
+                assert r.stats["visited_table"] == int(table)
+            if (k, L) not in _ORACLE_CACHE:
+                _ORACLE_CACHE[k, L] = ol.range_search_all(lifted, links, deg, base, ta, sc, m2, query, thr[k], L)
+            cands, preds, nds = _ORACLE_CACHE[k, L]
             assert np.array_equal(r.n_dist, nds), (k, L)
             for i in range(len(query)):
                 assert np.array_equal(r.cand(i), cands[i]), (k, L, i)
