@@ -49,11 +49,17 @@ class IndexDesc(C.Structure):
     ]
 
 
+class EvalSums(C.Structure):
+    _fields_ = [("recall", C.c_double), ("precision", C.c_double), ("f1", C.c_double), ("cand_recall", C.c_double),
+                ("cand", C.c_double), ("pred", C.c_double), ("graph_dist", C.c_double), ("nonempty", C.c_uint32)]
+
+
 class QueryStats(C.Structure):
     _fields_ = [
         ("n_dist", C.c_uint64), ("n_expand", C.c_uint64), ("n_cand", C.c_uint64), ("n_pred", C.c_uint64),
         ("n_flood", C.c_uint64), ("search_ms", C.c_float), ("total_ms", C.c_float), ("h2d_bytes", C.c_uint64),
         ("d2h_bytes", C.c_uint64), ("visited_table", C.c_uint32),
+        ("visited_l2_table", C.c_uint32),
     ]
 
 
@@ -120,6 +126,8 @@ _SIGS = {
     "anqi_query_download": [_vp, _u32, _vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp],
     "anqi_query_evaluate": [_vp, _u32, _u32, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double),
                             C.POINTER(C.c_double), C.POINTER(C.c_uint32)],
+    "anqi_gt_load": [_vp, _u32, _u32, C.c_uint64],
+    "anqi_query_evaluate_sums": [_vp, C.POINTER(EvalSums)],
     "anqi_rknn_query_noalloc": [_vp, _vp, C.c_uint32, _vp, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp],
     "anqi_exact_topk": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _u32, _f32],
     "anqi_rknn_ground_truth": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32, _u32, _u32, _f32,
@@ -366,6 +374,18 @@ class Context:
                                                  _ptr(nd)), "query_download")
         return QueryResult(pred_off, pred_ids[:pred_off[-1]], cand_off,
                            None if cand_ids is None else cand_ids[:cand_off[-1]], nd, {})
+
+    def gt_load(self, gt_off, gt_ids) -> None:
+        """Keeps a ground-truth CSR on the device for the current batch."""
+        gt_off = _c(gt_off, np.uint32)
+        gt_ids = _c(gt_ids, np.uint32) if len(gt_ids) else np.zeros(1, np.uint32)
+        self._check(self.lib.anqi_gt_load(self.h, gt_off, gt_ids, int(gt_off[-1])), "gt_load")
+
+    def query_evaluate_sums(self) -> dict:
+        """Sums over queries with non-empty truth of the last run's metrics."""
+        e = EvalSums()
+        self._check(self.lib.anqi_query_evaluate_sums(self.h, C.byref(e)), "query_evaluate_sums")
+        return {k: getattr(e, k) for k, _ in EvalSums._fields_}
 
     def query_evaluate(self, gt_off, gt_ids) -> dict:
         gt_off = _c(gt_off, np.uint32)

@@ -187,6 +187,12 @@ inline bool env_flag(const char* k) {
     return s != "0" && s != "false" && s != "no" && s != "off";
 }
 
+// mkdir -p (the run scripts create the cache directories this way).
+inline void mkdir_p(const std::string& dir) {
+    for (size_t i = 1; i <= dir.size(); i++)
+        if (i == dir.size() || dir[i] == '/') ::mkdir(dir.substr(0, i).c_str(), 0700);
+}
+
 inline bool file_exists(const std::string& p) {
     std::ifstream f(p);
     return f.good();

@@ -19,6 +19,7 @@
 #include "cli_common.h"
 
 #include <chrono>
+#include <memory>
 #include <iostream>
 
 using namespace anqi_cli;
@@ -111,7 +112,11 @@ static int run(int argc, char** argv) {
     if (K >= n || rk_k > K) die(2, "[dgt] require rk_k <= K < base vector count");
     std::cout << "[dgt] mode=" << mode << " n=" << n << " D=" << D << " K=" << K << " rk_k=" << rk_k
               << " tile=" << tile << " threads=" << T << "\n";
-    Device dev("[dgt]");
+    std::unique_ptr<Device> device;  // created when the first device stage runs
+    auto dev = [&]() -> Device& {
+        if (!device) device = std::make_unique<Device>("[dgt]");
+        return *device;
+    };
 
     std::vector<float> rk2(n);
     double threshold_build_s = 0.0;
@@ -119,7 +124,7 @@ static int run(int argc, char** argv) {
         std::vector<uint32_t> ids(n * K);
         std::vector<float> keys(n * K);
         const auto t1 = std::chrono::steady_clock::now();
-        dev.check(anqi_exact_topk(dev.get(), base.x.data(), n, (uint32_t)D, (uint32_t)K, ids.data(), keys.data()),
+        dev().check(anqi_exact_topk(dev().get(), base.x.data(), n, (uint32_t)D, (uint32_t)K, ids.data(), keys.data()),
                   "exact top-K");
         std::cout << "[dgt] base-to-base top-K done in "
                   << std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count() << "s\n";
@@ -164,13 +169,13 @@ static int run(int argc, char** argv) {
         for (int attempt = 0; attempt < 2; attempt++) {
             ids.resize(cap);
             keys.resize(cap);
-            const int rc = anqi_rknn_ground_truth(dev.get(), base.x.data(), n, query.x.data(), nq, (uint32_t)D,
+            const int rc = anqi_rknn_ground_truth(dev().get(), base.x.data(), n, query.x.data(), nq, (uint32_t)D,
                                                   rk2.data(), off.data(), ids.data(), keys.data(), cap, &total);
             if (rc == ANQI_ERR_CAPACITY && attempt == 0) {
                 cap = total;
                 continue;
             }
-            dev.check(rc, "reverse-kNN ground truth");
+            dev().check(rc, "reverse-kNN ground truth");
             break;
         }
         ground_truth_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t2).count();

@@ -24,6 +24,7 @@
 #include <chrono>
 #include <iomanip>
 #include <iostream>
+#include <memory>
 #include <sstream>
 
 using namespace anqi_cli;
@@ -160,11 +161,12 @@ static std::string graph_cache_key(uint64_t M, uint64_t leaf, uint64_t nt, uint6
     return sanitize_tag(k);
 }
 
-// nndindex::generate_config (include/index.h:1703-1769) with ANQI_GRAPH_CACHE_KEY set.
+// nndindex::generate_config (include/index.h:1703-1769) with ANQI_GRAPH_CACHE_KEY set;
+// ef_alpha and prune_alpha are floats there, printed by std::to_string.
 static std::string graph_file_name(uint64_t M, uint64_t nn_k, uint64_t n, uint64_t dim, float alpha,
                                    const std::string& graph_key) {
     std::string cfg = "fd_metric_l2_M_" + std::to_string(M) + "_nnk_" + std::to_string(nn_k) + "_ntrees_64_n_" +
-                      std::to_string(n) + "_dim_" + std::to_string(dim) + "_efa_8_pa_" + std::to_string(alpha) +
+                      std::to_string(n) + "_dim_" + std::to_string(dim) + "_efa_" + std::to_string(8.0f) + "_pa_" + std::to_string(alpha) +
                       "_er_100_graphnnd_" + env_or("ANQI_GRAPHNND", "6") + "_gk_" + hash16(graph_key);
     return sanitize_tag(cfg);
 }
@@ -507,8 +509,8 @@ static int run(int argc, char** argv) {
     if (env_flag("ANQI_REQUIRE_GRAPH_CACHE") && !can_load)
         die(3, "[rknn] required graph cache is incomplete or incompatible: dir=%s key=%s", graph_cache_dir.c_str(),
             graph_key.c_str());
-    ::mkdir(graph_cache_dir.c_str(), 0700);
-    ::mkdir(verifier_cache_dir.c_str(), 0700);
+    mkdir_p(graph_cache_dir);
+    mkdir_p(verifier_cache_dir);
 
     Lrq lrq;
     lrq.n = n;
@@ -520,7 +522,11 @@ static int run(int argc, char** argv) {
     load_codebook(cb_path, NK, RANKM, bits, lrq);
     if (lrq.code_size != 256) die(3, "[rknn] u8 LRQ codebook must have 256 entries per rank, got %u", lrq.code_size);
 
-    Device dev("[rknn]");
+    std::unique_ptr<Device> device;  // created when the first device stage runs
+    auto dev = [&]() -> Device& {
+        if (!device) device = std::make_unique<Device>("[rknn]");
+        return *device;
+    };
     const std::string lrq_file = verifier_cache_dir + "_anqi_verifier_" + hash16(radius_key) + ".bin";
     bool lrq_ready = false;
     double verifier_load_ms = 0, verifier_encode_save_ms = 0;
@@ -539,7 +545,7 @@ static int run(int argc, char** argv) {
         const auto t0 = Clock::now();
         lrq.coeff.resize(n * lrq.rankm);
         lrq.codes.resize(n * NK);
-        dev.check(anqi_lrq_encode(dev.get(), keys.data(), n, lrq.nk, lrq.rankm, lrq.mu.data(), lrq.basis.data(),
+        dev().check(anqi_lrq_encode(dev().get(), keys.data(), n, lrq.nk, lrq.rankm, lrq.mu.data(), lrq.basis.data(),
                                   lrq.codebook.data(), lrq.code_size, lrq.coeff.data(), lrq.codes.data()),
                   "LRQ encode");
         save_verifier(lrq_file, lrq);
@@ -566,6 +572,8 @@ static int run(int argc, char** argv) {
         if (lf.n != n || lf.d != dim) die(3, "[rknn] lifted cache %s has shape %ux%u", approxlift.c_str(), lf.n, lf.d);
         lifted = std::move(lf.x);
         printf("[rknn] graph degree M=%" PRIu64 "\n", Marg);
+        std::cout << "Index config: " << graph_path.substr(graph_cache_dir.size()) << "\n";
+        std::cout << "Loading index from: " << graph_path << "\n" << std::flush;
         const auto t0 = Clock::now();
         float ctime = 0;
         std::string why;
@@ -602,7 +610,7 @@ static int run(int argc, char** argv) {
             ap.nn_sample = (uint32_t)std::min(std::max(0, std::atoi(env_or("ANQI_NNSAMPLE", "20").c_str())), 120);
             warm.resize(n * width);
             std::vector<float> wd(n * width);
-            dev.check(anqi_aknn_build(dev.get(), base.x.data(), n, (uint32_t)d, &ap, warm.data(), wd.data(), nullptr),
+            dev().check(anqi_aknn_build(dev().get(), base.x.data(), n, (uint32_t)d, &ap, warm.data(), wd.data(), nullptr),
                       "original-space AKNN");
         }
         source_prepare_s = since(t_src);
@@ -614,7 +622,7 @@ static int run(int argc, char** argv) {
         printf("[rknn] RADIUS_MODE=%s:postfilter conceptual_radius_store=%.3fGB\n", radius_key.c_str(),
                lrq.persistent_bytes() / 1e9);
         lifted.resize(n * dim);
-        dev.check(anqi_lift(dev.get(), base.x.data(), n, (uint32_t)d, radius.data(), lifted.data(), &Mstar2, &scale),
+        dev().check(anqi_lift(dev().get(), base.x.data(), n, (uint32_t)d, radius.data(), lifted.data(), &Mstar2, &scale),
                   "lift");
         {
             const uint32_t hdr[2] = {(uint32_t)n, (uint32_t)dim};
@@ -633,6 +641,7 @@ static int run(int argc, char** argv) {
         lift_verifier_prepare_s = since(t_prep);
 
         printf("[rknn] graph degree M=%" PRIu64 "\n", Marg);
+        std::cout << "Index config: " << graph_path.substr(graph_cache_dir.size()) << "\n" << std::flush;
         const auto t_graph = Clock::now();
         anqi_graph_params gp{};
         gp.degree = (uint32_t)Marg;
@@ -649,15 +658,15 @@ static int run(int argc, char** argv) {
         deg.resize(n);
         links.resize(n * Marg);
         anqi_build_stats gs{};
-        dev.check(anqi_graph_build(dev.get(), lifted.data(), n, (uint32_t)dim, warm.data(), (uint32_t)width, &gp,
+        dev().check(anqi_graph_build(dev().get(), lifted.data(), n, (uint32_t)dim, warm.data(), (uint32_t)width, &gp,
                                    deg.data(), links.data(), &gs),
                   "graph build");
         uint32_t tn = 0;
         uint64_t tp = 0;
-        dev.check(anqi_graph_tree_size(dev.get(), &tn, &tp), "entry tree size");
+        dev().check(anqi_graph_tree_size(dev().get(), &tn, &tp), "entry tree size");
         std::vector<uint32_t> tl(tn), tr(tn), lo(tn), lc(tn), perm(tp);
         std::vector<float> to(tn), th((size_t)tn * dim);
-        dev.check(anqi_graph_tree_copy(dev.get(), tl.data(), tr.data(), to.data(), th.data(), lo.data(), lc.data(),
+        dev().check(anqi_graph_tree_copy(dev().get(), tl.data(), tr.data(), to.data(), th.data(), lo.data(), lc.data(),
                                        perm.data()),
                   "entry tree copy");
         tree = bfs_to_postorder(tl, tr, to, th, lo, lc, perm, 100, (uint32_t)dim);
@@ -697,8 +706,8 @@ static int run(int argc, char** argv) {
     desc.tree_leaf_first = leaf_first.data();
     desc.scale = scale;
     desc.mstar2 = Mstar2;
-    dev.check(anqi_index_load(dev.get(), &desc), "index load");
-    dev.check(anqi_verifier_load(dev.get(), lrq.coeff.data(), lrq.codes.data(), n, lrq.nk, lrq.rankm, lrq.mu.data(),
+    dev().check(anqi_index_load(dev().get(), &desc), "index load");
+    dev().check(anqi_verifier_load(dev().get(), lrq.coeff.data(), lrq.codes.data(), n, lrq.nk, lrq.rankm, lrq.mu.data(),
                                  lrq.basis.data(), lrq.codebook.data(), lrq.code_size),
               "verifier load");
     const double build_s = since(tb0);
@@ -737,7 +746,7 @@ static int run(int argc, char** argv) {
                    end_to_end_s, verifier_encode_save_ms);
     }
     const auto t_mat = Clock::now();
-    dev.check(anqi_verifier_materialize(dev.get(), (uint32_t)Kq, slack_factor), "verifier materialize");
+    dev().check(anqi_verifier_materialize(dev().get(), (uint32_t)Kq, slack_factor), "verifier materialize");
     const double materialize_ms = since(t_mat) * 1e3;
     printf("[rknn] independent verifier ready: mode=rank-M+LRQ k=%" PRIu64 " slack=%.6g persistent=%.3fGB "
            "temporary_thresholds=%.3fGB materialize_ms=%.3f bits=%d\n",
@@ -793,9 +802,9 @@ static int run(int argc, char** argv) {
         PointStats s;
         const auto t0 = Clock::now();
         for (uint64_t b = 0; b < batches; b++) {
-            dev.check(anqi_query_run(dev.get(), 1, nullptr), "query run");
+            dev().check(anqi_query_run(dev().get(), 1, nullptr), "query run");
             anqi_eval_sums e{};
-            dev.check(anqi_query_evaluate_sums(dev.get(), &e), "evaluation");
+            dev().check(anqi_query_evaluate_sums(dev().get(), &e), "evaluation");
             s.recall += e.recall;
             s.prec += e.precision;
             s.f1 += e.f1;
@@ -825,10 +834,10 @@ static int run(int argc, char** argv) {
     };
 
     for (uint64_t L : Lds) {
-        dev.check(anqi_query_upload(dev.get(), query.x.data(), (uint32_t)nq, nullptr, (uint32_t)Kq, nullptr,
+        dev().check(anqi_query_upload(dev().get(), query.x.data(), (uint32_t)nq, nullptr, (uint32_t)Kq, nullptr,
                                     (uint32_t)L),
                   "query upload");
-        dev.check(anqi_gt_load(dev.get(), goff.data(), gids.data(), gids.size()), "ground-truth load");
+        dev().check(anqi_gt_load(dev().get(), goff.data(), gids.data(), gids.size()), "ground-truth load");
         if (!calibrated) {
             const PointStats s = run_point(L, bench_repeats);
             print_point(L, s, (double)s.tasks / s.secs);

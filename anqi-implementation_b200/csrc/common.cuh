@@ -126,6 +126,29 @@ __device__ __forceinline__ float group_ip(const float* __restrict__ a, const flo
     return res;
 }
 
+// ------------------------------------------------------- row staging
+// Global -> shared copies of whole rows with cp.async (16 bytes per
+// instruction, no registers held while in flight): a row costs one memory
+// round trip however long it is.  Rows are `stride` floats, 16-byte aligned,
+// stride a multiple of 4.
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// Waits for this thread's outstanding cp.async copies.
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// The `nthreads` threads starting at `t0` of a warp copy one row; the caller
+// waits (cp_async_wait_all + __syncwarp) before reading it.
+__device__ __forceinline__ void stage_row_async(float* dst, const float* __restrict__ src, uint32_t stride,
+                                                uint32_t t, uint32_t nthreads) {
+    for (uint32_t c = t; c < stride / 4; c += nthreads) cp_async16(dst + 4 * c, src + 4 * c);
+}
+
 // nndindex::d2 (index.h:172-176): (na + nb) - 2 * ip(a, b)
 __device__ __forceinline__ float norm_d2(float na, float nb, float ip) {
     return __fsub_rn(__fadd_rn(na, nb), __fmul_rn(2.0f, ip));

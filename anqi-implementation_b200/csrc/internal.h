@@ -89,8 +89,9 @@ struct Ctx {
     std::vector<float> t_offset, t_hyper;
     uint32_t t_nodes = 0, t_dim = 0;
     // search-kernel autotuning: configuration key -> shared-memory visited table size
-    std::unordered_map<uint64_t, uint32_t> tuned;
-    uint32_t last_hash_cap = 0;
+    std::unordered_map<uint64_t, uint64_t> tuned;  // value: shared entries | L2 entries << 32
+    DevBuf vis_gtab;                               // per-slot L2-resident visited tables
+    uint32_t gtab_slots = 0, gtab_cap = 0;
     uint64_t device_bytes = 0;
     std::vector<DevBuf*> member_bufs() {
         return {&ix.base, &ix.lifted, &ix.onorm, &ix.deg, &ix.links, &ix.tleft, &ix.tright, &ix.toffset,
@@ -98,7 +99,7 @@ struct Ctx {
                 &batch.qL, &batch.qslot, &batch.npred, &batch.ncand, &batch.ndist, &batch.nexp, &batch.nflood,
                 &batch.pred_at, &batch.cand_at, &batch.pred_buf, &batch.cand_buf, &batch.pred_off,
                 &batch.cand_off, &batch.pred_csr, &batch.cand_csr, &err, &counters, &vis_bits, &vis_log,
-                &cand_scratch, &thr_table, &gt_off, &gt_ids, &eval_rows, &eval_sums};
+                &cand_scratch, &thr_table, &gt_off, &gt_ids, &eval_rows, &eval_sums, &vis_gtab};
     }
     // Per-object thresholds for up to kThrSlots values of k: slot s holds
     // thr_k[s] (0 = unused) in thr_table[s * n .. (s+1) * n).

@@ -67,8 +67,11 @@ struct SearchParams {
     unsigned long long* pred_at;
     unsigned long long* cand_at;
     uint32_t* err;
-    uint32_t hash_cap;    // shared-memory visited table entries per warp (power of two, 0 = bitmap only)
+    uint32_t hash_cap;    // shared-memory visited table entries per warp (power of two, 0 = none)
     uint32_t hash_shift;  // 32 - log2(hash_cap)
+    uint32_t* gtab;       // per-slot global visited tables (gcap entries each, all ANQI_EMPTY between queries)
+    uint32_t gcap;        // entries per slot (power of two, 0 = none)
+    uint32_t gshift;      // 32 - log2(gcap)
 };
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
@@ -79,76 +82,132 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
-// The visited set of one query.  While small it is an open-addressing table
-// in the warp's shared memory (atomicCAS, linear probing, kept below 5/8
-// load); before an expansion could push it past that, its ids move into the
-// slot's global bitmap and the query continues there ("global" mode).  The
-// bitmap is cleared afterwards by replaying the log of ids it received.
+// The visited set of one query, in up to three levels:
+//   0  an open-addressing table in the warp's shared memory (atomicCAS,
+//      linear probing, kept at or below 5/8 load);
+//   1  a per-slot open-addressing table in global memory, small enough that
+//      all slots' tables stay resident in L2 (same rules);
+//   2  the per-slot bitmap over all n ids.
+// Before an expansion could push the current level past its load limit, its
+// ids move one level up.  The log records, per first visit, what the clean-up
+// at the end of the query needs: nothing at level 0, the table position at
+// level 1, the id at level 2.
 struct Visited {
     uint32_t* tab;
     uint32_t cap, shift;
+    uint32_t* gtab;
+    uint32_t gcap, gshift;
     uint32_t* bits;
     uint32_t* vlog;
     uint32_t log_cap;
-    bool global;
+    uint32_t level;
 };
 
-__device__ __forceinline__ bool vis_first(Visited& v, uint32_t id, uint32_t* err) {
-    if (v.global) return visit_first(v.bits, id);
-    uint32_t h = (id * 0x9E3779B1u) >> v.shift;
-    for (uint32_t probe = 0; probe < v.cap; probe++) {
-        const uint32_t old = atomicCAS(v.tab + h, kEmpty, id);
-        if (old == kEmpty) return true;
+// Inserts id into an open-addressing table; returns true on first insertion
+// and the position used in pos.  Probes are bounded by the table size.
+__device__ __forceinline__ bool table_insert(uint32_t* t, uint32_t cap, uint32_t shift, uint32_t id, uint32_t& pos,
+                                             uint32_t* err) {
+    uint32_t h = (id * 0x9E3779B1u) >> shift;
+    for (uint32_t probe = 0; probe < cap; probe++) {
+        const uint32_t old = atomicCAS(t + h, kEmpty, id);
+        if (old == kEmpty) {
+            pos = h;
+            return true;
+        }
         if (old == id) return false;
-        h = (h + 1) & (v.cap - 1);
+        h = (h + 1) & (cap - 1);
     }
-    set_error(err, kDevWaitTimeout);  // unreachable below 5/8 load
+    set_error(err, kDevWaitTimeout);  // unreachable at or below 5/8 load
     return false;
 }
 
-// Moves every id of the table into the bitmap and the log (warp-collective).
-__device__ void vis_migrate(Visited& v, uint32_t lane) {
+__device__ __forceinline__ bool vis_first(Visited& v, uint32_t id, uint32_t& pos, uint32_t* err) {
+    if (v.level == 0) return table_insert(v.tab, v.cap, v.shift, id, pos, err);
+    if (v.level == 1) return table_insert(v.gtab, v.gcap, v.gshift, id, pos, err);
+    pos = id;
+    return visit_first(v.bits, id);
+}
+
+// Level 0 -> 1 (gtab present) or 0 -> 2 (warp-collective); nlog entries move.
+__device__ void vis_up_from_shared(Visited& v, uint32_t lane, uint32_t* err) {
+    const uint32_t to = v.gcap ? 1u : 2u;
     uint32_t pos0 = 0;
     for (uint32_t t0 = 0; t0 < v.cap; t0 += 32) {
         const uint32_t id = v.tab[t0 + lane];
         const bool has = id != kEmpty;
-        if (has) atomicOr(v.bits + (id >> 5), 1u << (id & 31u));
+        uint32_t rec = id;
+        if (has) {
+            if (to == 1) table_insert(v.gtab, v.gcap, v.gshift, id, rec, err);
+            else atomicOr(v.bits + (id >> 5), 1u << (id & 31u));
+        }
         const unsigned b = __ballot_sync(kFull, has);
         if (has) {
-            const uint32_t pos = pos0 + __popc(b & lanemask_lt());
-            if (pos < v.log_cap) v.vlog[pos] = id;
+            const uint32_t at = pos0 + __popc(b & lanemask_lt());
+            if (at < v.log_cap) v.vlog[at] = rec;
         }
         pos0 += __popc(b);
     }
     __syncwarp();
-    v.global = true;
+    v.level = to;
+}
+
+// Level 1 -> 2 (warp-collective): positions in the log become ids.
+__device__ void vis_up_from_global(Visited& v, uint32_t nlog, uint32_t lane) {
+    const uint32_t m = min(nlog, v.log_cap);
+    for (uint32_t i = lane; i < m; i += 32) {
+        const uint32_t pos = v.vlog[i];
+        const uint32_t id = v.gtab[pos];
+        v.gtab[pos] = kEmpty;
+        atomicOr(v.bits + (id >> 5), 1u << (id & 31u));
+        v.vlog[i] = id;
+    }
+    __syncwarp();
+    v.level = 2;
+}
+
+// Makes room for `more` first visits: moves up while the level's limit would be passed.
+__device__ __forceinline__ void vis_room(Visited& v, uint32_t nlog, uint32_t more, uint32_t lane, uint32_t* err) {
+    if (v.level == 0 && nlog + more > v.cap / 8 * 5) vis_up_from_shared(v, lane, err);
+    if (v.level == 1 && nlog + more > v.gcap / 8 * 5) vis_up_from_global(v, nlog, lane);
+}
+
+// End of query: leaves level 1 / 2 storage clean (the shared table is reset by the caller).
+__device__ __forceinline__ void vis_release(Visited& v, const VisitSlot& vs, uint32_t nlog, uint32_t lane) {
+    if (v.level == 1) {
+        for (uint32_t i = lane; i < nlog; i += 32) v.gtab[v.vlog[i]] = kEmpty;
+        __syncwarp();
+    } else if (v.level == 2) {
+        visit_clear(vs, nlog);
+    }
 }
 
 // Visits the links of node (slots l0 = link[lane], l1 = link[lane + 32], dg =
 // degree): collects the ids seen for the first time into ni[0..m) in link-slot
-// order, logging them when the bitmap is in use.  Returns m.
+// order and logs them (levels 1 and 2).  Returns m.
 __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t l0, uint32_t l1, uint32_t dg,
                                                  Visited& vis, uint32_t& nlog, uint32_t* ni, uint32_t lane) {
     bool f0 = false, f1 = false, bad = false;
+    uint32_t r0 = 0, r1 = 0;
     if (lane < dg) {
-        if (l0 < p.n) f0 = vis_first(vis, l0, p.err);
+        if (l0 < p.n) f0 = vis_first(vis, l0, r0, p.err);
         else bad = true;
     }
     if (lane + 32 < dg) {
-        if (l1 < p.n) f1 = vis_first(vis, l1, p.err);
+        if (l1 < p.n) f1 = vis_first(vis, l1, r1, p.err);
         else bad = true;
     }
     if (bad) set_error(p.err, kDevBadId);
     const unsigned b0 = __ballot_sync(kFull, f0), b1 = __ballot_sync(kFull, f1);
     const uint32_t c0 = __popc(b0), lt = lanemask_lt();
     const uint32_t p0 = __popc(b0 & lt), p1 = c0 + __popc(b1 & lt);
+    const bool logs = vis.level != 0;
     if (f0) {
         ni[p0] = l0;
-        if (vis.global && nlog + p0 < p.log_cap) vis.vlog[nlog + p0] = l0;
+        if (logs && nlog + p0 < p.log_cap) vis.vlog[nlog + p0] = r0;
     }
     if (f1) {
         ni[p1] = l1;
-        if (vis.global && nlog + p1 < p.log_cap) vis.vlog[nlog + p1] = l1;
+        if (logs && nlog + p1 < p.log_cap) vis.vlog[nlog + p1] = r1;
     }
     const uint32_t m = c0 + __popc(b1);
     nlog += m;
@@ -199,23 +258,22 @@ __device__ __forceinline__ void sort_fresh(float* nd, uint32_t* ni, uint32_t m, 
     __syncwarp();
 }
 
-// Distances of the m fresh neighbours to the lifted query: 8 groups of 4 lanes.
+// Distances of the m fresh neighbours to the lifted query: 8 groups of 4
+// lanes, each group staging its row into shared memory (one round trip for up
+// to 8 rows) and reducing it in the reference's lane order.
 __device__ __forceinline__ void fresh_distances(const SearchParams& p, const float* qhat, const uint32_t* ni,
-                                                float* nd, uint32_t m, uint32_t gw, uint32_t gt) {
-    for (uint32_t r0 = 0; r0 < m; r0 += 16) {
-        const uint32_t ia = r0 + gw, ib = r0 + 8 + gw;
-        const bool oka = ia < m, okb = ib < m;
-        const uint32_t ida = ni[oka ? ia : r0];
-        const uint32_t idb = ni[okb ? ib : r0];
-        float da = group_l2sqr(p.lifted + (size_t)ida * p.lstride, qhat, p.dim, gt, kFull);
-        float db = 0.f;
-        if (r0 + 8 < m) db = group_l2sqr(p.lifted + (size_t)idb * p.lstride, qhat, p.dim, gt, kFull);
-        if (gt == 0) {
-            if (oka) nd[ia] = da;
-            if (okb) nd[ib] = db;
-        }
+                                                float* nd, uint32_t m, uint32_t gw, uint32_t gt, float* stage) {
+    float* row = stage + (size_t)gw * p.lstride;
+    for (uint32_t r0 = 0; r0 < m; r0 += 8) {
+        const uint32_t ia = r0 + gw;
+        const bool oka = ia < m;
+        if (oka) stage_row_async(row, p.lifted + (size_t)ni[ia] * p.lstride, p.lstride, gt, 4);
+        cp_async_wait_all();
+        __syncwarp();
+        const float da = group_l2sqr(oka ? row : stage, qhat, p.dim, gt, kFull);
+        if (gt == 0 && oka) nd[ia] = da;
+        __syncwarp();
     }
-    __syncwarp();
 }
 
 // Appends fresh neighbours within R2 to the candidate / flood list (visit order).
@@ -243,8 +301,10 @@ __device__ __forceinline__ void append_in_range(const SearchParams& p, const flo
 
 extern __shared__ __align__(16) unsigned char g_smem[];
 
-__device__ __forceinline__ size_t search_smem_words(uint32_t L_max, uint32_t lstride, uint32_t bstride, uint32_t hash_cap) {
-    return (size_t)4 * L_max + 128 + lstride + bstride + hash_cap;
+__device__ __host__ __forceinline__ size_t search_smem_words(uint32_t L_max, uint32_t lstride, uint32_t bstride,
+                                                             uint32_t hash_cap) {
+    return (size_t)4 * L_max + 128 + lstride + bstride + 8 * (size_t)(lstride > bstride ? lstride : bstride) +
+           hash_cap;
 }
 
 __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
@@ -260,15 +320,14 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
     uint32_t* biB = reinterpret_cast<uint32_t*>(bdB + p.L_max);
     float* nd = reinterpret_cast<float*>(biB + p.L_max);
     uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 64);
-    uint32_t* tab = ni + 64;
+    float* stage = reinterpret_cast<float*>(ni + 64);  // 8 staged rows of max(lstride, bstride)
+    uint32_t* tab = reinterpret_cast<uint32_t*>(stage + 8 * (size_t)max(p.lstride, p.bstride));
     uint32_t* bits = p.vis_bits + (size_t)slot * p.vis_words;
     uint32_t* vlog = p.vis_log + (size_t)slot * p.log_cap;
     uint32_t* cl = p.cand_scratch + (size_t)slot * p.cand_cap;
     VisitSlot vs{bits, vlog, p.log_cap, p.vis_words};
     for (uint32_t t = lane; t < p.hash_cap; t += 32) tab[t] = kEmpty;
     __syncwarp();
-    // migrate before an expansion could take the table past 5/8 load
-    const uint32_t hash_limit = p.hash_cap ? p.hash_cap / 8 * 5 : 0;
 
     for (;;) {
         uint32_t qi = 0;
@@ -290,18 +349,28 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
         // RP-tree entry, rptrees.h:108-124 (|margin| <= EPS goes left)
         uint32_t v = p.troot;
         for (uint32_t depth = 0; p.tleft[v] != kEmpty && depth < 4096; depth++) {
-            const float ip = group_ip(p.thyper + (size_t)v * p.lstride, qhat, p.dim, gt, kFull);
+            stage_row_async(stage, p.thyper + (size_t)v * p.lstride, p.lstride, lane, 32);
+            cp_async_wait_all();
+            __syncwarp();
+            const float ip = group_ip(stage, qhat, p.dim, gt, kFull);
+            __syncwarp();
             const float margin = __fsub_rn(ip, p.toffset[v]);
             v = (margin < -kSplitEps) ? p.tleft[v] : (margin > kSplitEps ? p.tright[v] : p.tleft[v]);
         }
         uint32_t ep = p.tleaf[v];
         if (ep == kEmpty || ep >= p.n) ep = 0;
 
-        Visited vis{tab, p.hash_cap, p.hash_shift, bits, vlog, p.log_cap, p.hash_cap == 0};
-        const float dep = group_l2sqr(p.lifted + (size_t)ep * p.lstride, qhat, p.dim, gt, kFull);
+        Visited vis{tab,  p.hash_cap, p.hash_shift, p.gtab ? p.gtab + (size_t)slot * p.gcap : nullptr,
+                    p.gcap, p.gshift, bits, vlog, p.log_cap, p.hash_cap ? 0u : (p.gcap ? 1u : 2u)};
+        stage_row_async(stage, p.lifted + (size_t)ep * p.lstride, p.lstride, lane, 32);
+        cp_async_wait_all();
+        __syncwarp();
+        const float dep = group_l2sqr(stage, qhat, p.dim, gt, kFull);
+        __syncwarp();
         if (lane == 0) {
-            vis_first(vis, ep, p.err);
-            if (vis.global && p.log_cap) vlog[0] = ep;
+            uint32_t rec = ep;
+            vis_first(vis, ep, rec, p.err);
+            if (vis.level != 0 && p.log_cap) vlog[0] = rec;
             bdA[0] = dep;
             biA[0] = ep;
         }
@@ -317,7 +386,7 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
         float* od = bdB;
         uint32_t* oi = biB;
         uint32_t size = 1, cur = 0;
-        // links of the node expected next, loaded one expansion ahead
+        // links of the next node to expand, loaded while the current merge runs
         uint32_t pre_node = kEmpty, pl0 = kEmpty, pl1 = kEmpty, pdg = 0;
 
         // ---- greedy beam, index.h:1613-1624
@@ -345,19 +414,32 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
             } else {
                 load_links(p, node, lane, l0, l1, dg);
             }
-            pre_node = nxt < size ? (bi[nxt] & kIdMask) : kEmpty;
-            if (pre_node != kEmpty) load_links(p, pre_node, lane, pl0, pl1, pdg);
-            if (!vis.global && nlog + p.degree > hash_limit) vis_migrate(vis, lane);
+            vis_room(vis, nlog, p.degree, lane, p.err);
             const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane);
             if (m == 0) {
                 cur = nxt;
+                if (nxt < size) {
+                    pre_node = bi[nxt] & kIdMask;
+                    load_links(p, pre_node, lane, pl0, pl1, pdg);
+                }
                 continue;
             }
-            fresh_distances(p, qhat, ni, nd, m, gw, gt);
+            fresh_distances(p, qhat, ni, nd, m, gw, gt, stage);
             append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
             // batch insert = merge of the sorted batch into the sorted beam
             sort_fresh(nd, ni, m, lane);
             const uint32_t ns = min(L, size + m);
+            // first unexpanded entry of the merged beam: the best fresh entry or
+            // the old beam's next one, whichever ranks first
+            uint32_t cb = 0xFFFFFFFFu;
+            if (nxt < size) cb = nxt + lower_rank(nd, ni, m, bd[nxt], bi[nxt]);
+            const uint32_t cn = lower_rank(bd, bi, size, nd[0], ni[0]);
+            uint32_t nc = min(cb, cn);
+            if (nc > ns) nc = ns;
+            if (nc < ns) {
+                pre_node = cn < cb ? ni[0] : (bi[nxt] & kIdMask);
+                load_links(p, pre_node, lane, pl0, pl1, pdg);
+            }
             for (uint32_t p0 = lane; p0 < size; p0 += 32) {
                 const float dv = bd[p0];
                 const uint32_t iv = bi[p0];
@@ -374,11 +456,6 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
                     oi[pos] = ni[r];
                 }
             }
-            uint32_t cb = 0xFFFFFFFFu;
-            if (nxt < size) cb = nxt + lower_rank(nd, ni, m, bd[nxt], bi[nxt]);
-            const uint32_t cn = lower_rank(bd, bi, size, nd[0], ni[0]);
-            uint32_t nc = min(cb, cn);
-            if (nc > ns) nc = ns;
             __syncwarp();
             float* td = bd;
             bd = od;
@@ -411,10 +488,10 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
                 pre_node = cl[head];
                 load_links(p, pre_node, lane, pl0, pl1, pdg);
             }
-            if (!vis.global && nlog + p.degree > hash_limit) vis_migrate(vis, lane);
+            vis_room(vis, nlog, p.degree, lane, p.err);
             const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane);
             if (m == 0) continue;
-            fresh_distances(p, qhat, ni, nd, m, gw, gt);
+            fresh_distances(p, qhat, ni, nd, m, gw, gt, stage);
             append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
         }
         if (overflow && lane == 0) set_error(p.err, kDevCandOverflow);
@@ -435,11 +512,15 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
         const float qn = group_ip(qraw, qraw, p.d, gt, kFull);
         const float* thr = p.thr + (size_t)tslot * p.n;
         uint32_t npred = 0;
+        float* brow = stage + (size_t)gw * max(p.lstride, p.bstride);
         for (uint32_t r0 = 0; r0 < ncand; r0 += 8) {
             const uint32_t idx = r0 + gw;
             const bool ok = idx < ncand;
             const uint32_t o = cl[ok ? idx : r0];
-            const float ip = group_ip(p.base + (size_t)o * p.bstride, qraw, p.d, gt, kFull);
+            if (ok) stage_row_async(brow, p.base + (size_t)o * p.bstride, p.bstride, gt, 4);
+            cp_async_wait_all();
+            __syncwarp();
+            const float ip = group_ip(ok ? brow : stage, qraw, p.d, gt, kFull);
             const float key = __fsub_rn(__fadd_rn(p.onorm[o], qn), __fmul_rn(2.0f, ip));
             const bool pass = ok && (double)key <= (double)thr[o];
             const unsigned b = __ballot_sync(kFull, pass && gt == 0);
@@ -463,7 +544,7 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
         at = __shfl_sync(kFull, at, 0);
         if (at + npred <= p.pred_cap)
             for (uint32_t i = lane; i < npred; i += 32) p.pred_buf[at + i] = cl[i];
-        if (vis.global) visit_clear(vs, nlog);
+        vis_release(vis, vs, nlog, lane);
         for (uint32_t t = lane; t < p.hash_cap; t += 32) tab[t] = kEmpty;
         __syncwarp();
     }
@@ -611,19 +692,21 @@ static int ensure_thr_table(Ctx* c, uint64_t n) {
 }
 
 static size_t search_smem_per_warp(const Ctx* c, uint32_t L_max, uint32_t hash_cap) {
-    return (size_t)(4 * L_max + 128 + c->ix.lstride + c->ix.bstride + hash_cap) * 4;
+    return search_smem_words(L_max, c->ix.lstride, c->ix.bstride, hash_cap) * 4;
 }
 
 struct SearchCfg {
-    uint32_t hash_cap = 0;
+    uint32_t hash_cap = 0;  // shared-memory table entries per warp
+    uint32_t gcap = 0;      // global (L2-resident) table entries per warp
     uint32_t blocks = 0;
     size_t smem = 0;
 };
 
-static int search_cfg(Ctx* c, uint32_t hash_cap, SearchCfg& cfg) {
+static int search_cfg(Ctx* c, uint32_t hash_cap, uint32_t gcap, SearchCfg& cfg) {
     const Batch& b = c->batch;
     const int wpb = 4;
     cfg.hash_cap = hash_cap;
+    cfg.gcap = gcap;
     cfg.smem = search_smem_per_warp(c, b.L_max, hash_cap) * wpb;
     if (cfg.smem > 227 * 1024) return ANQI_ERR_ARGS;
     ANQI_CUDA(c, cudaFuncSetAttribute(rknn_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
@@ -836,6 +919,9 @@ static int launch_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, floa
     p.err = c->err.as<uint32_t>();
     p.hash_cap = cfg.hash_cap;
     p.hash_shift = cfg.hash_cap ? 32u - (uint32_t)__builtin_ctz(cfg.hash_cap) : 0u;
+    p.gcap = cfg.gcap;
+    p.gshift = cfg.gcap ? 32u - (uint32_t)__builtin_ctz(cfg.gcap) : 0u;
+    p.gtab = cfg.gcap ? c->vis_gtab.as<uint32_t>() : nullptr;
     ANQI_CUDA(c, cudaFuncSetAttribute(rknn_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
     ANQI_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     rknn_search_kernel<<<cfg.blocks, 128, cfg.smem, c->stream>>>(p);
@@ -862,17 +948,40 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
     if (!c->ix.loaded || b.nq == 0) return fail(c, ANQI_ERR_ARGS, "anqi_query_run: no index or batch");
     const QueryIndex& ix = c->ix;
     int rc;
-    // candidate configurations: shared-memory visited table of 0 (bitmap only) .. 4096 entries
+    // candidate visited-set configurations (shared-memory entries, L2 table
+    // entries); ANQI_B200_HASH="S" or "S,G" forces one of them
     const char* forced = std::getenv("ANQI_B200_HASH");
+    uint32_t f_hc = 0, f_gc = 0;
+    if (forced) {
+        char* end = nullptr;
+        f_hc = (uint32_t)std::strtoul(forced, &end, 10);
+        if (end && *end == ',') f_gc = (uint32_t)std::strtoul(end + 1, nullptr, 10);
+    }
+    static const uint32_t kCandidates[][2] = {{0, 0},    {1024, 0},    {2048, 0},
+                                                  {4096, 0}, {0, 4096},    {512, 4096}, {1024, 4096}};
     std::vector<SearchCfg> cfgs;
-    for (uint32_t hc : {0u, 1024u, 2048u, 4096u}) {
-        if (forced && std::strtoul(forced, nullptr, 10) != hc) continue;
+    for (const auto& cand : kCandidates) {
+        if (forced && (cand[0] != f_hc || cand[1] != f_gc)) continue;
+        if (!forced && cand[0] == 4096) continue;  // measured slower everywhere (occupancy); kept forcible
+        if (cand[1] && (uint64_t)cand[1] / 8 * 5 > std::min<uint64_t>(ix.n, 16384)) continue;  // log must cover it
         SearchCfg g;
-        if (search_cfg(c, hc, g) == ANQI_OK) cfgs.push_back(g);
+        if (search_cfg(c, cand[0], cand[1], g) == ANQI_OK) cfgs.push_back(g);
     }
     if (cfgs.empty()) return fail(c, ANQI_ERR_ARGS, "beam width %u needs too much shared memory", b.L_max);
-    uint32_t slots = 0;
-    for (const SearchCfg& g : cfgs) slots = std::max(slots, g.blocks * 4);
+    uint32_t slots = 0, gslots = 0, gcap_max = 0;
+    for (const SearchCfg& g : cfgs) {
+        slots = std::max(slots, g.blocks * 4);
+        if (g.gcap) gslots = std::max(gslots, g.blocks * 4);
+        gcap_max = std::max(gcap_max, g.gcap);
+    }
+    // per-slot L2-resident tables, ANQI_EMPTY between queries
+    if (gcap_max && (c->gtab_slots < gslots || c->gtab_cap < gcap_max)) {
+        const size_t bytes = (size_t)gslots * gcap_max * 4;
+        if ((rc = ensure(c, c->vis_gtab, bytes))) return rc;
+        ANQI_CUDA(c, cudaMemsetAsync(c->vis_gtab.p, 0xFF, bytes, c->stream));
+        c->gtab_slots = gslots;
+        c->gtab_cap = gcap_max;
+    }
     // per-slot scratch (bitmap, log, candidate list) for the largest configuration
     const uint32_t words = (uint32_t)((ix.n + 31) / 32);
     const uint32_t log_cap = (uint32_t)std::min<uint64_t>(ix.n, 16384);
@@ -896,7 +1005,7 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
     auto it = c->tuned.find(key);
     if (it != c->tuned.end()) {
         for (const SearchCfg& g : cfgs)
-            if (g.hash_cap == it->second) best = g;
+            if ((g.hash_cap | (uint64_t)g.gcap << 32) == it->second) best = g;
     } else if (cfgs.size() > 1) {
         float best_ms = 1e30f;
         for (const SearchCfg& g : cfgs) {
@@ -913,9 +1022,8 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
                 best = g;
             }
         }
-        c->tuned[key] = best.hash_cap;
+        c->tuned[key] = best.hash_cap | (uint64_t)best.gcap << 32;
     }
-    c->last_hash_cap = best.hash_cap;
     for (int attempt = 0; attempt < 3; attempt++) {
         float ms = 0;
         unsigned long long fill[2] = {0, 0};
@@ -947,6 +1055,7 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
         if (st) {
             st->search_ms = ms;
             st->visited_table = best.hash_cap;
+            st->visited_l2_table = best.gcap;
         }
         return sync(c);
     }

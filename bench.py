@@ -52,7 +52,7 @@ def log(*a):
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--n", type=int, default=1_000_000)
@@ -93,6 +93,10 @@ class Clocks:
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region starts once the sampler reports
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 10 and self.proc.poll() is None:
+                time.sleep(0.02)
         except OSError:
             self.proc = None
         return self
@@ -109,7 +113,13 @@ class Clocks:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
+    def mark(self):
+        """Samples from here on are the ones taken during the timed region."""
+        self.first = len(self.rows)
+
     def summary(self):
+        rows = self.rows[getattr(self, "first", 0):] or self.rows[-1:]
+        self.rows = rows
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
@@ -228,6 +238,7 @@ def run_ours(a, rank, world, local):
         import torch.distributed as dist
         dist.barrier()
     with Clocks(dev) as clk:
+        clk.mark()
         ctx.timer_start()
         for _ in range(a.steps):
             stats.append(ctx.query_run())
@@ -283,7 +294,8 @@ def run_ours(a, rank, world, local):
                      "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
                      "kernel": "rknn_search_kernel", "kernel_ms": round(kernel_ms, 4),
                      "alg_bytes_per_launch": int(alg_bytes),
-                     "visited_table": int(stats[-1]["visited_table"])},
+                     "visited_table": int(stats[-1]["visited_table"]),
+                     "visited_l2_table": int(stats[-1]["visited_l2_table"])},
         "gpu_launches": 3 * a.steps,
         "clocks": clocks,
         "recall": None if ev["recall"] is None else round(ev["recall"], 6),

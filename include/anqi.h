@@ -207,8 +207,10 @@ typedef struct {
     float search_ms;      /* device time of the search kernel (CUDA events on its stream) */
     float total_ms;       /* device time from first copy to last copy of the call */
     uint64_t h2d_bytes, d2h_bytes;
-    uint32_t visited_table; /* entries of the per-warp shared-memory visited table the search
-                               ran with (chosen by timing; 0 = global bitmap only) */
+    uint32_t visited_table;    /* entries of the per-warp shared-memory visited table the search
+                                  ran with (chosen by timing; 0 = none) */
+    uint32_t visited_l2_table; /* entries of the per-warp L2-resident visited table (0 = none);
+                                  beyond both, a per-warp bitmap over all ids */
 } anqi_query_stats;
 
 int anqi_rknn_query(anqi_ctx* ctx, const float* queries, uint32_t nq, const uint32_t* k_per_query,

@@ -1,0 +1,129 @@
+"""The three command-line drivers end to end on the GPU, on the reference's own
+sample (scripts/run_sample.sh): dataset_gt bit-exact against the reference's
+files, build_aknn_source valid and deterministic, and rknn_query printing the
+reference's own result lines when it runs on the reference's graph (cache
+interoperability both ways)."""
+import os
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from anqi import formats
+
+import test_cli as tc
+
+pytestmark = pytest.mark.gpu
+RESULT_RE = re.compile(r"\[rknn\] L_descent=(\d+)\s+\| recall=([\d.]+) precision=([\d.]+) F1=([\d.]+) \| "
+                       r"avg cand=(\d+) pred=(\d+) #dist=(\d+) \| QPS=(\d+)")
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def lines(stdout):
+    return {int(m.group(1)): [float(m.group(i)) for i in range(2, 8)] for m in RESULT_RE.finditer(stdout)}
+
+
+@pytest.mark.parametrize("d", [8, 32])
+def test_dataset_gt_cli_bit_exact(tmp_path, d):
+    z = dict(np.load(tc.GOLDEN / f"sample_d{d}.npz"))
+    base, query = tmp_path / "b.bin", tmp_path / "q.bin"
+    formats.write_fbin(base, z["base"])
+    formats.write_fbin(query, z["query"])
+    thr = tmp_path / "thr"
+    rc, out, err = tc.run("dataset_gt", "--base", base, "--K", 100, "--rk_k", 100, "--threads", 4, "--tile", 64,
+                          "--mode", "thresholds", "--out_prefix", thr)
+    assert rc == 0, err
+    assert "[dgt] THRESHOLD_BUILD_TIME=" in out
+    raw = Path(f"{thr}_baseknn_gt.bin").read_bytes()
+    assert raw[:8] == np.array([256, 100], np.uint32).tobytes()
+    ids = np.frombuffer(raw[8:8 + 256 * 400], np.uint32).reshape(256, 100)
+    keys = np.frombuffer(raw[8 + 256 * 400:], np.float32).reshape(256, 100)
+    assert np.array_equal(ids, z["exact_ids"]) and np.array_equal(bits(keys), bits(z["exact_keys"]))
+    assert Path(f"{thr}_threshold_build_time.meta").read_text().startswith("ANQI_THRESHOLD_BUILD_V1\n")
+    for k in (10, 50, 100):
+        t = tmp_path / f"gt{k}"
+        rc, out, err = tc.run("dataset_gt", "--base", base, "--query", query, "--K", 100, "--rk_k", k,
+                              "--mode", "ground-truth", "--threshold-table", f"{thr}_baseknn_gt.bin",
+                              "--out_prefix", t)
+        assert rc == 0, err
+        off, gids, gkeys = formats.read_rknn_csr(f"{t}_rknn_gt.bin")
+        assert np.array_equal(off, z[f"gt_off_{k}"]) and np.array_equal(gids, z[f"gt_ids_{k}"])
+        assert np.array_equal(bits(gkeys), bits(z[f"gt_keys_{k}"]))
+
+
+def test_build_aknn_source_cli(tmp_path):
+    z = dict(np.load(tc.GOLDEN / "sample_d32.npz"))
+    base = tmp_path / "b.bin"
+    formats.write_fbin(base, z["base"])
+    outs = []
+    for rep in range(2):
+        pfx = tmp_path / f"p{rep}"
+        rc, out, err = tc.run("build_aknn_source", base, pfx, 100, 64, 8, 64, 4, 10, "l2")
+        assert rc == 0, err
+        assert re.search(r"\[aknn\] DONE n=256 d=32 K=100 leaf=64 trees=8 ef=64 threads=4 seed=10 metric=l2", out)
+        ids, keys = formats.read_rec(f"{pfx}_baseknn_aknn.rec", 256, 100)
+        outs.append((ids, keys))
+        meta = Path(f"{pfx}_aknn_build_time.meta").read_text().splitlines()
+        assert meta[0] == "ANQI_AKNN_BUILD_V1" and meta[1].startswith("seconds ")
+        assert not Path(f"{pfx}_baseknn_aknn.rec.part").exists()
+    ids, keys = outs[0]
+    assert np.array_equal(ids, outs[1][0]) and np.array_equal(bits(keys), bits(outs[1][1]))
+    n = 256
+    assert (ids < n).all() and (ids != np.arange(n)[:, None]).all()
+    assert all(len(set(r.tolist())) == 100 for r in ids)
+    assert (np.diff(keys, axis=1) >= 0).all() and (keys >= 0).all()
+    # recall@100 against the exact table (the reference reaches 0.98+ on such data)
+    hit = np.mean([len(set(ids[i]) & set(z["exact_ids"][i])) / 100 for i in range(n)])
+    assert hit > 0.95, hit
+
+
+@pytest.mark.parametrize("d", [8, 32])
+def test_rknn_query_cli_matches_reference_lines(tmp_path, d):
+    pfx, env, z = tc.sample_prefix(tmp_path, d)
+    ref_lines = {(int(k), int(L)): list(v) for (k, L), v in zip(z["ref_lines_k_L"], z["ref_lines"])}
+    # 1) cold: the graph is built on the device from the reference's AKNN warm start
+    built = {}
+    for k in (10, 50, 100):
+        rc, out, err = tc.run("rknn_query", "16,32,64,128", pfx, 48, 500, 64, 600, k, env=env)
+        assert rc == 0, err
+        assert ("[rknn] BUILD_TIME=" in out) == (k == 10) and ("[rknn] INDEX_LOAD_TIME=" in out) == (k != 10)
+        got = lines(out)
+        assert sorted(got) == [16, 32, 64, 128]
+        for L, v in got.items():
+            built[k, L] = v
+            r = ref_lines[k, L]
+            assert abs(v[0] - r[0]) < 0.02 and v[1] >= 0.99, (k, L, v, r)   # recall, precision
+        for tag in ("DIST_BREAKDOWN", "CANDIDATE_RECALL"):
+            assert out.count(f"[rknn] {tag} L_descent=") == 4
+    # 2) the reference's own graph in the same cache slot: its printed lines exactly
+    gdir = Path(env["ANQI_GRAPH_CACHE_DIR"])
+    gfiles = list(gdir.glob("fd_metric_*"))
+    assert len(gfiles) == 1
+    gfiles[0].write_bytes(z["graph_file"].tobytes())
+    for k in (10, 50, 100):
+        rc, out, err = tc.run("rknn_query", "16,32,64,128", pfx, 48, 500, 64, 600, k, env=env)
+        assert rc == 0, err
+        assert "[rknn] loaded cached index" in out
+        for L, v in lines(out).items():
+            assert v == ref_lines[k, L], (k, L, v, ref_lines[k, L])
+
+
+@pytest.mark.skipif(not tc.REF_BIN.exists(), reason="reference binaries not built")
+def test_reference_loads_the_caches_this_driver_writes(tmp_path):
+    pfx, env, z = tc.sample_prefix(tmp_path, 8)
+    rc, ours, err = tc.run("rknn_query", "16,32,64,128", pfx, 48, 500, 64, 600, 50, env=env)
+    assert rc == 0, err
+    e = {k: v for k, v in os.environ.items() if not k.startswith("ANQI_")}
+    e.update(env)
+    e["OMP_NUM_THREADS"] = "4"
+    ref = subprocess.run([str(tc.REF_BIN), "16,32,64,128", str(pfx), "48", "500", "64", "600", "50"], env=e,
+                         capture_output=True, text=True, timeout=300)
+    assert ref.returncode == 0, ref.stderr
+    assert "[rknn] loaded cached index" in ref.stdout and "Loading index from:" in ref.stdout
+    assert "[rknn] loaded independent compact verifier" in ref.stdout
+    assert lines(ref.stdout) == lines(ours)

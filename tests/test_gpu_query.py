@@ -154,11 +154,12 @@ def random_index():
 _ORACLE_CACHE = {}
 
 
-@pytest.mark.parametrize("table", [None, "0", "1024", "4096"])
+@pytest.mark.parametrize("table", [None, "0", "1024", "4096", "0,4096", "512,4096", "1024,4096"])
 def test_query_bit_exact_vs_oracle_random(ctx, random_index, table, monkeypatch):
-    """Every visited-set form (autotuned; global bitmap only; shared-memory
-    tables of 1024 and 4096 entries, which L=1000 pushes into migration to
-    the bitmap) returns the oracle's candidates, #dist and verified lists."""
+    """Every visited-set form (autotuned; bitmap only; shared-memory tables of
+    1024 / 4096 entries; an L2-resident table alone or behind a shared one --
+    L=1000 pushes each through every migration up to the bitmap) returns the
+    oracle's candidates, #dist and verified lists."""
     if table is not None:
         monkeypatch.setenv("ANQI_B200_HASH", table)
     base, query, lifted, links, deg, tree, sc, m2, thr = random_index
@@ -169,7 +170,9 @@ def test_query_bit_exact_vs_oracle_random(ctx, random_index, table, monkeypatch)
         for L in (8, 48, 200, 1000):
             r = ctx.rknn_query(query, k, L, keep_candidates=True)
             if table is not None:
-                assert r.stats["visited_table"] == int(table)
+                sh, _, l2 = table.partition(",")
+                assert r.stats["visited_table"] == int(sh)
+                assert r.stats["visited_l2_table"] == int(l2 or 0)
             if (k, L) not in _ORACLE_CACHE:
                 _ORACLE_CACHE[k, L] = ol.range_search_all(lifted, links, deg, base, ta, sc, m2, query, thr[k], L)
             cands, preds, nds = _ORACLE_CACHE[k, L]
@@ -205,3 +208,31 @@ def test_resident_batch_and_evaluate(ctx, random_index):
     assert ev["nonempty"] == ne
     assert abs(ev["recall"] - rec / ne) < 1e-12 and abs(ev["precision"] - prec / ne) < 1e-12
     assert ev["recall"] > 0.3
+    # resident ground truth + device sums (the accumulators of rknn_query.cpp:2784-2799)
+    ctx.gt_load(off, ids)
+    ctx.query_run(keep_candidates=True)
+    sums = ctx.query_evaluate_sums()
+    h = dict(recall=0.0, precision=0.0, f1=0.0, cand_recall=0.0, cand=0.0, pred=0.0, graph_dist=0.0)
+    for i in range(len(query)):
+        truth = set(ids[off[i]:off[i + 1]].tolist())
+        if not truth:
+            continue
+        pred = set(r1.pred(i).tolist())
+        cand = r1.cand(i)
+        hit = len(pred & truth)
+        r, p = hit / len(truth), (1.0 if not pred else hit / len(pred))
+        h["recall"] += r
+        h["precision"] += p
+        h["f1"] += 2 * r * p / (r + p) if r + p > 0 else 0.0
+        h["cand_recall"] += len(set(cand.tolist()) & truth) / len(truth)
+        h["cand"] += len(cand)
+        h["pred"] += len(pred)
+        h["graph_dist"] += int(r1.n_dist[i])
+    assert sums["nonempty"] == ne
+    for key, v in h.items():
+        assert abs(sums[key] - v) <= 1e-9 * max(1.0, abs(v)), (key, sums[key], v)
+    # a new batch invalidates the resident ground truth
+    ctx.query_upload(query, 10, 64)
+    ctx.query_run()
+    with pytest.raises(Exception):
+        ctx.query_evaluate_sums()
