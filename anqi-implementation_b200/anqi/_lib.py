@@ -129,6 +129,14 @@ _SIGS = {
     "anqi_gt_load": [_vp, _u32, _u32, C.c_uint64],
     "anqi_query_evaluate_sums": [_vp, C.POINTER(EvalSums)],
     "anqi_rknn_query_noalloc": [_vp, _vp, C.c_uint32, _vp, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp],
+    "anqi_lrq_objective_forward": [_vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp, _vp, _vp, C.c_uint32, _vp, _vp,
+                                   _vp, _vp, _vp, _vp],
+    "anqi_lrq_objective_backward": [_vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp, _vp,
+                                    C.c_uint32, C.c_double, _vp, _vp, _vp, _vp],
+    "anqi_exact_topk_tc": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _vp, C.c_uint32, _u32, _f32],
+    "anqi_rknn_ground_truth_tc": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32, _u32, _u32, _f32,
+                                  C.c_uint64, C.POINTER(C.c_uint64)],
+    "anqi_bf16_gram": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32],
     "anqi_exact_topk": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _u32, _f32],
     "anqi_rknn_ground_truth": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32, _u32, _u32, _f32,
                                C.c_uint64, C.POINTER(C.c_uint64)],
@@ -386,6 +394,46 @@ class Context:
         e = EvalSums()
         self._check(self.lib.anqi_query_evaluate_sums(self.h, C.byref(e)), "query_evaluate_sums")
         return {k: getattr(e, k) for k, _ in EvalSums._fields_}
+
+    def exact_topk_tc(self, base: np.ndarray, K: int, hints: np.ndarray | None = None):
+        """Exact top-K (ids, keys) on the BF16 tensor path; equals anqi_exact_topk."""
+        base = _c(base, np.float32)
+        n, d = base.shape
+        ids = np.empty((n, K), np.uint32)
+        keys = np.empty((n, K), np.float32)
+        h = None if hints is None else _c(hints, np.uint32)
+        self._check(self.lib.anqi_exact_topk_tc(self.h, base, n, d, K, _ptr(h), 0 if h is None else h.shape[1], ids,
+                                                keys), "exact_topk_tc")
+        return ids, keys
+
+    def rknn_ground_truth_tc(self, base: np.ndarray, query: np.ndarray, rk2: np.ndarray):
+        """Reverse-kNN CSR (off, ids, keys) on the BF16 tensor path; equals anqi_rknn_ground_truth."""
+        base = _c(base, np.float32)
+        query = _c(query, np.float32)
+        rk2 = _c(rk2, np.float32)
+        n, d = base.shape
+        nq = query.shape[0]
+        off = np.empty(nq + 1, np.uint32)
+        tot = C.c_uint64()
+        cap = max(1024, 64 * nq)
+        while True:
+            ids = np.empty(cap, np.uint32)
+            keys = np.empty(cap, np.float32)
+            rc = self.lib.anqi_rknn_ground_truth_tc(self.h, base, n, query, nq, d, rk2, off, ids, keys, cap,
+                                                    C.byref(tot))
+            if rc == ANQI_ERR_CAPACITY and tot.value > cap:
+                cap = int(tot.value)
+                continue
+            self._check(rc, "rknn_ground_truth_tc")
+            return off.copy(), ids[:tot.value].copy(), keys[:tot.value].copy()
+
+    def bf16_gram(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+        """<bf16(a_i), bf16(b_j)> accumulated in FP32 on the tensor cores."""
+        a = _c(a, np.float32)
+        b = _c(b, np.float32)
+        out = np.empty((a.shape[0], b.shape[0]), np.float32)
+        self._check(self.lib.anqi_bf16_gram(self.h, a, a.shape[0], b, b.shape[0], a.shape[1], out), "bf16_gram")
+        return out
 
     def query_evaluate(self, gt_off, gt_ids) -> dict:
         gt_off = _c(gt_off, np.uint32)

@@ -102,6 +102,22 @@ __global__ void sort_segments_kernel(const uint64_t* __restrict__ off, uint64_t 
     }
 }
 
+// Sorts every CSR segment [off[i], off[i+1]) of (keys, ids) by (key, id).
+int sort_csr_segments(Ctx* c, const uint64_t* d_off, uint64_t nseg, uint32_t* d_ids, float* d_keys, uint64_t maxm) {
+    const uint32_t scr_cap = maxm > 1024 ? (uint32_t)(1ull << (64 - __builtin_clzll(maxm - 1))) : 1;
+    const uint32_t sblocks = (uint32_t)c->sm_count * 4;
+    TmpBuf sd(c), si(c);
+    int rc;
+    if ((rc = ensure(c, sd, (size_t)sblocks * 4 * scr_cap * 4)) || (rc = ensure(c, si, (size_t)sblocks * 4 * scr_cap * 4)))
+        return rc;
+    const size_t ssm = 4 * 2 * 1024 * 4;
+    ANQI_CUDA(c, cudaFuncSetAttribute(sort_segments_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+    sort_segments_kernel<<<sblocks, 128, ssm, c->stream>>>(d_off, nseg, d_ids, d_keys, sd.as<float>(),
+                                                           si.as<uint32_t>(), scr_cap);
+    ANQI_CUDA(c, cudaGetLastError());
+    return sync(c);
+}
+
 }  // namespace anqi
 
 using namespace anqi;

@@ -149,6 +149,7 @@ int device_scan(Ctx* c, const uint32_t* d_in, uint64_t* d_out, uint64_t n);
 // Launch helpers implemented in the .cu files.
 int lrq_materialize_device(Ctx* c, const Verifier& v, uint32_t k, double scale, float* d_out);
 int compute_norms_device(Ctx* c, const float* d_x, uint64_t n, uint32_t dim, uint32_t stride, float* d_out);
+int sort_csr_segments(Ctx* c, const uint64_t* d_off, uint64_t nseg, uint32_t* d_ids, float* d_keys, uint64_t maxm);
 
 }  // namespace anqi
 

@@ -1,0 +1,679 @@
+// BF16 tensor-core (tcgen05) tiles for the brute-force distance work: the
+// exact ground truth (tools/dataset_gt.cpp:206-313) in the precision form.
+//
+// Rows are converted once to bf16 (padded to a multiple of 16).  A CTA of 4
+// warps owns a 128-row query tile resident in shared memory and streams
+// 128-row base tiles through a two-stage shared-memory ring; one thread
+// issues the K = 16 tcgen05.mma steps into one of two 128-column TMEM
+// accumulators while the four warps run the epilogue of the previous tile
+// (tcgen05.ld: thread = query row, 32 columns per load).
+//
+// Epilogue: key~ = |q|^2 + |x|^2 - 2 <q~, x~> with the reference's FP32
+// norms.  A pair is a candidate when key~ - eps <= threshold, where eps bounds
+// |key~ - key32| (key32 = the reference's FP32 key):
+//   eps = 2 (|dq| |x| + |q| |dx| + |dq| |dx|)      bf16 rounding of the rows
+//       + 4 g (|q~| |x~| + |q| |x|)                 FP32 accumulation, g = 2 d 2^-24
+//       + 4 u (|q|^2 + |x|^2 + 2 |q| |x|)           the key's own roundings, u = 2^-24
+// (|dq| = |q - bf16(q)|).  Candidates are recomputed in the reference's FP32
+// order, so accept decisions and keys equal the FP32 path.  When both rows
+// hold integers of magnitude <= 256 and d <= 128, bf16 and every partial
+// sum are exact and key~ == key32: eps = 0 and no recheck is needed.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "internal.h"
+#include "tc.cuh"
+#include "util.cuh"
+
+namespace anqi {
+namespace {
+
+constexpr uint32_t kTile = 128;     // M = N = 128
+constexpr uint32_t kMaxDp = 256;    // padded dimension limit of the tensor path
+constexpr uint32_t kWaitPolls = 1u << 24;
+
+// ------------------------------------------------------------ row prep
+// Per row: bf16 copy padded to dp (zeros), |x| (rounded up), |x - bf16(x)|
+// (rounded up), and whether the row is exact-int (integers, |v| <= 256).
+__global__ void bf16_rows_kernel(const float* __restrict__ x, uint64_t n, uint32_t xs, uint32_t d, uint32_t dp,
+                                 __nv_bfloat16* __restrict__ xb, float* __restrict__ xnorm,
+                                 float* __restrict__ xerr, uint8_t* __restrict__ exact_int) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t r = w; r < n; r += nw) {
+        double s = 0.0, e = 0.0;
+        bool ok = true;
+        for (uint32_t k = lane; k < dp; k += 32) {
+            const float v = k < d ? x[r * xs + k] : 0.0f;
+            const __nv_bfloat16 b = __float2bfloat16_rn(v);
+            xb[r * dp + k] = b;
+            const double dv = (double)v - (double)__bfloat162float(b);
+            s += (double)v * v;
+            e += dv * dv;
+            ok = ok && v == rintf(v) && fabsf(v) <= 256.0f;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+            e += __shfl_xor_sync(0xFFFFFFFFu, e, o);
+        }
+        ok = __all_sync(0xFFFFFFFFu, ok);
+        if (lane == 0) {
+            xnorm[r] = __double2float_ru(sqrt(s) * (1.0 + 1e-12));
+            xerr[r] = __double2float_ru(sqrt(e) * (1.0 + 1e-12));
+            exact_int[r] = ok ? 1 : 0;
+        }
+    }
+}
+
+// Stages rows [r0, r0 + 128) of a bf16 matrix (dp wide) into the interleaved
+// K-major layout; rows at or past nrows are zero-filled.  All threads of the
+// CTA take part; completion via cp.async.wait.
+__device__ __forceinline__ void stage_tile(unsigned char* dst, const __nv_bfloat16* __restrict__ src, uint64_t r0,
+                                           uint64_t nrows, uint32_t dp) {
+    const uint32_t chunks = dp / 8;
+    for (uint32_t t = threadIdx.x; t < kTile * chunks; t += blockDim.x) {
+        const uint32_t r = t % kTile, c = t / kTile;
+        const uint64_t row = r0 + r;
+        const bool ok = row < nrows;
+        const __nv_bfloat16* s = src + (ok ? row : 0) * dp + 8 * c;
+        tc::cp_async16_zfill(dst + (size_t)c * kTile * 16 + r * 16, s, ok ? 16u : 0u);
+    }
+}
+
+__device__ __forceinline__ void cp_async_wait_all_() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Issues the dp/16 MMA steps of one 128 x 128 tile.
+__device__ __forceinline__ void issue_tile_mma(uint32_t tmem_d, const unsigned char* a, const unsigned char* b,
+                                               uint32_t dp) {
+    constexpr uint32_t idesc = tc::idesc_bf16_f32(kTile, kTile);
+    const uint32_t sa = tc::smem_u32(a), sb = tc::smem_u32(b);
+    for (uint32_t s = 0; s < dp / 16; s++) {
+        const uint64_t ad = tc::smem_desc(sa + 2 * s * kTile * 16, kTile * 16, 128);
+        const uint64_t bd = tc::smem_desc(sb + 2 * s * kTile * 16, kTile * 16, 128);
+        tc::mma_bf16(tmem_d, ad, bd, idesc, s > 0 ? 1u : 0u);
+    }
+}
+
+// ------------------------------------------------------------------ Gram
+// out[i, j] = <bf16(a_i), bf16(b_j)> in FP32 for one 128 x 128 tile per CTA.
+__global__ void __launch_bounds__(128) gram_kernel(const __nv_bfloat16* __restrict__ a, uint64_t na,
+                                                   const __nv_bfloat16* __restrict__ b, uint64_t nb, uint32_t dp,
+                                                   float* __restrict__ out, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    unsigned char* sa = sm;
+    unsigned char* sb = sm + (size_t)kTile * dp * 2;
+    __shared__ uint64_t bar;
+    __shared__ uint32_t tslot;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint64_t i0 = (uint64_t)blockIdx.x * kTile, j0 = (uint64_t)blockIdx.y * kTile;
+    if (warp == 0) tc::tmem_alloc(&tslot, 128);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::fence_mbar_init();
+    }
+    stage_tile(sa, a, i0, na, dp);
+    stage_tile(sb, b, j0, nb, dp);
+    cp_async_wait_all_();
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tslot;
+    if (threadIdx.x == 0) {
+        issue_tile_mma(tmem, sa, sb, dp);
+        tc::mma_commit(&bar);
+    }
+    const bool ok = tc::mbar_wait(&bar, 0, kWaitPolls);
+    if (!ok && lane == 0) atomicExch(err, 8u);
+    tc::fence_after_sync();
+    if (ok) {
+        const uint64_t row = i0 + warp * 32 + lane;
+        for (uint32_t c0 = 0; c0 < kTile; c0 += 32) {
+            float v[32];
+            tc::tmem_ld32(tmem + ((warp * 32u) << 16) + c0, v);
+            if (row < na)
+                for (uint32_t e = 0; e < 32; e++)
+                    if (j0 + c0 + e < nb) out[row * nb + j0 + c0 + e] = v[e];
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_free(tmem, 128);
+}
+
+// --------------------------------------------------------- filter
+// One CTA = 8 warps over a 128-row query tile; warp w reads TMEM lanes
+// 32 (w % 4) .. + 31 (its rows) and columns 64 (w / 4) .. + 63 of each tile.
+struct FilterParams {
+    const __nv_bfloat16* qb;  // query rows, bf16, dp wide
+    const float* q32;         // query rows, FP32, stride xs
+    const float* qn;          // reference FP32 norms
+    const float* qnorm;       // |q| rounded up
+    const float* qerr;        // |q - bf16(q)| rounded up
+    const uint8_t* qint;      // exact-int rows
+    const __nv_bfloat16* xb;
+    const float* x32;
+    const float* xn;
+    const float* xnorm;
+    const float* xerr;
+    const uint8_t* xint;
+    uint64_t n;
+    uint32_t xs, d, dp;
+    const float* thr_row;     // per query row (top-K bound) or null
+    const float* thr_col;     // per base row (rank-k threshold) or null
+    int exclude_self;         // skip j == query row (self top-K)
+    const uint32_t* rows;     // query rows to process (null: 0 .. nrows-1)
+    uint64_t nrows;
+    uint64_t split_len;       // base rows per grid.y slice (multiple of 128)
+    uint32_t* cnt;            // per query row: hits (atomic; may exceed cap)
+    uint32_t cap;
+    uint32_t* out_id;         // row * cap + slot
+    float* out_key;
+    uint32_t* err;
+};
+
+constexpr uint32_t kStages = 3;
+constexpr uint32_t kFilterThreads = 256;
+
+// The reference's FP32 key |q|^2 + |x|^2 - 2 <q, x> (dataset_gt.cpp:225, 294)
+// with <q, x> in the 16-lane AVX-512 order of include/distance.h:89-116,
+// computed by one thread.
+__device__ __forceinline__ float ref_key(const float* __restrict__ q, const float* __restrict__ x, uint32_t d,
+                                         float qn, float xn) {
+    const uint32_t d16 = d & ~15u;
+    float acc[16];
+#pragma unroll
+    for (int l = 0; l < 16; l++) acc[l] = 0.f;
+    for (uint32_t k0 = 0; k0 < d16; k0 += 16)
+#pragma unroll
+        for (int l = 0; l < 16; l++) acc[l] = __fmaf_rn(q[k0 + l], x[k0 + l], acc[l]);
+    auto fold = [](float (&a)[16]) {
+        float t3[8], t6[4];
+#pragma unroll
+        for (int i = 0; i < 8; i++) t3[i] = __fadd_rn(a[i + 8], a[i]);
+#pragma unroll
+        for (int i = 0; i < 4; i++) t6[i] = __fadd_rn(t3[i + 4], t3[i]);
+        return __fadd_rn(__fadd_rn(t6[0], t6[2]), __fadd_rn(t6[1], t6[3]));
+    };
+    float ip = fold(acc);
+    if (d16 < d) {
+        float p[16];
+#pragma unroll
+        for (int l = 0; l < 16; l++) p[l] = (d16 + l < d) ? __fmul_rn(q[d16 + l], x[d16 + l]) : 0.f;
+        ip = __fadd_rn(ip, fold(p));
+    }
+    return __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, ip));
+}
+
+__global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterParams p) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    const uint32_t tile_bytes = kTile * p.dp * 2;
+    unsigned char* sa = sm;
+    unsigned char* sb = sm + tile_bytes;                                         // kStages tiles
+    float* col = reinterpret_cast<float*>(sb + (size_t)kStages * tile_bytes);   // kStages x 4 x 128
+    uint8_t* colint = reinterpret_cast<uint8_t*>(col + kStages * 4 * kTile);    // kStages x 128
+    uint64_t* rowid = reinterpret_cast<uint64_t*>(colint + kStages * kTile);    // 128 (aligned: 2*... bytes)
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t tslot;
+    __shared__ int s_abort;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t r = (warp & 3u) * 32 + lane;  // this thread's tile row / TMEM lane
+    const uint32_t half = warp >> 2;             // column half of each tile
+
+    // query rows of this tile
+    if (threadIdx.x < kTile) {
+        const uint64_t t = (uint64_t)blockIdx.x * kTile + threadIdx.x;
+        rowid[threadIdx.x] = t < p.nrows ? (p.rows ? p.rows[t] : t) : ~0ull;
+    }
+    const uint64_t js = (uint64_t)blockIdx.y * p.split_len;
+    const uint64_t je = min_u64(p.n, js + p.split_len);
+    const uint32_t T = js < je ? (uint32_t)((je - js + kTile - 1) / kTile) : 0u;
+    if (warp == 0) tc::tmem_alloc(&tslot, 256);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar[0], 1);
+        tc::mbar_init(&bar[1], 1);
+        tc::fence_mbar_init();
+        s_abort = 0;
+    }
+    __syncthreads();
+
+    // A: the query tile (gathered rows)
+    const uint32_t chunks = p.dp / 8;
+    for (uint32_t t = threadIdx.x; t < kTile * chunks; t += blockDim.x) {
+        const uint32_t rr = t % kTile, c = t / kTile;
+        const uint64_t row = rowid[rr];
+        const bool ok = row != ~0ull;
+        tc::cp_async16_zfill(sa + (size_t)c * kTile * 16 + rr * 16, p.qb + (ok ? row : 0) * p.dp + 8 * c,
+                             ok ? 16u : 0u);
+    }
+    // base tile t -> stage t % kStages (operand + per-column data)
+    auto prefetch = [&](uint32_t t) {
+        const uint32_t st = t % kStages;
+        const uint64_t j0 = js + (uint64_t)t * kTile;
+        unsigned char* dst = sb + (size_t)st * tile_bytes;
+        for (uint32_t i = threadIdx.x; i < kTile * chunks; i += blockDim.x) {
+            const uint32_t rr = i % kTile, c = i / kTile;
+            const uint64_t row = j0 + rr;
+            const bool ok = row < je;
+            tc::cp_async16_zfill(dst + (size_t)c * kTile * 16 + rr * 16, p.xb + (ok ? row : 0) * p.dp + 8 * c,
+                                 ok ? 16u : 0u);
+        }
+        if (threadIdx.x < kTile) {
+            const uint64_t j = j0 + threadIdx.x;
+            const bool ok = j < je;
+            float* cs = col + (size_t)st * 4 * kTile;
+            cs[threadIdx.x] = ok ? p.xn[j] : __int_as_float(0x7f800000);
+            cs[kTile + threadIdx.x] = ok ? p.xnorm[j] : 0.f;
+            cs[2 * kTile + threadIdx.x] = ok ? p.xerr[j] : 0.f;
+            cs[3 * kTile + threadIdx.x] = ok ? (p.thr_col ? p.thr_col[j] : 0.f) : -__int_as_float(0x7f800000);
+            colint[st * kTile + threadIdx.x] = ok ? p.xint[j] : 0;
+        }
+    };
+    if (T > 0) prefetch(0);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    if (T > 1) prefetch(1);
+
+    // per-row constants of the error bound
+    const uint64_t my_row = rowid[r];
+    const bool row_ok = my_row != ~0ull;
+    const float qn = row_ok ? p.qn[my_row] : 0.f;
+    const float qnm = row_ok ? p.qnorm[my_row] : 0.f;
+    const float qer = row_ok ? p.qerr[my_row] : 0.f;
+    const bool qexact = row_ok && p.qint[my_row] && p.d <= 128;
+    const float thr_r = (row_ok && p.thr_row) ? p.thr_row[my_row] : 0.f;
+    const float u = 5.9604645e-8f;        // 2^-24
+    const float g = 2.0f * p.dp * u;
+    const float ca = 2.f * qer + 4.f * g * (qnm + qer) + 4.f * g * qnm + 8.f * u * qnm;
+    const float cb = 2.f * qnm + 2.f * qer + 4.f * g * (qnm + qer);
+    const float cc = 4.f * u;
+    const float cd = 4.f * u * qn;
+    const float* qrow = p.q32 + (row_ok ? my_row : 0) * p.xs;
+
+    for (uint32_t t = 0; t <= T; t++) {
+        // tile t (prefetched one iteration ahead) and the query tile resident
+        // and visible to the tensor cores; TMEM buffer t & 1 free (its last
+        // reader, the epilogue of tile t - 2, ran before this barrier)
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (s_abort) break;  // uniform: read after the barrier
+        const uint32_t tmem = tslot;
+        if (t < T && threadIdx.x == 0) {
+            issue_tile_mma(tmem + (t & 1u) * kTile, sa, sb + (size_t)(t % kStages) * tile_bytes, p.dp);
+            tc::mma_commit(&bar[t & 1u]);
+        }
+        if (t == 0) continue;
+        // epilogue of tile e = t - 1 while the tensor cores run tile t
+        const uint32_t e = t - 1;
+        const bool ok = tc::mbar_wait(&bar[e & 1u], (e >> 1) & 1u, kWaitPolls);
+        if (!ok) {
+            s_abort = 1;
+            atomicExch(p.err, 8u);
+        }
+        tc::fence_after_sync();
+        // stage (t + 1) % 3 last held tile t - 2: its MMA (before MMA e) and
+        // its epilogue (previous iteration) are done
+        if (t + 1 < T) prefetch(t + 1);
+        if (ok) {
+            const uint32_t st = e % kStages;
+            const float* cs = col + (size_t)st * 4 * kTile;
+            const uint64_t j0 = js + (uint64_t)e * kTile;
+            for (uint32_t c0 = half * 64; c0 < half * 64 + 64; c0 += 32) {
+                float v[32];
+                tc::tmem_ld32(tmem + (((warp & 3u) * 32u) << 16) + (e & 1u) * kTile + c0, v);
+                if (!row_ok) continue;
+#pragma unroll 4
+                for (uint32_t k = 0; k < 32; k++) {
+                    const uint32_t cj = c0 + k;
+                    const uint64_t j = j0 + cj;
+                    const float xn = cs[cj];
+                    const float approx = __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, v[k]));
+                    const float thr = p.thr_row ? thr_r : cs[3 * kTile + cj];
+                    const bool exact = qexact && colint[st * kTile + cj];
+                    const float eps =
+                        exact ? 0.f : fmaf(ca, cs[kTile + cj], fmaf(cb, cs[2 * kTile + cj], fmaf(cc, xn, cd)));
+                    if (!(approx - eps <= thr)) continue;
+                    if (p.exclude_self && j == my_row) continue;
+                    const float key = exact ? approx : ref_key(qrow, p.x32 + j * p.xs, p.d, qn, xn);
+                    if (!(key <= thr)) continue;
+                    const uint32_t pos = atomicAdd(p.cnt + my_row, 1u);
+                    if (pos < p.cap) {
+                        p.out_id[my_row * p.cap + pos] = (uint32_t)j;
+                        p.out_key[my_row * p.cap + pos] = key;
+                    }
+                }
+            }
+        }
+        tc::fence_before_sync();
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_free(tslot, 256);
+}
+
+// Upper bound of each row's K-th smallest key: the largest reference FP32 key
+// to K distinct other rows (the hints, e.g. the AKNN lists).  Warp per row.
+__global__ void hint_bound_kernel(const float* __restrict__ x, const float* __restrict__ xn, uint64_t n,
+                                  uint32_t xs, uint32_t d, const uint32_t* __restrict__ hints, uint32_t hk,
+                                  uint32_t K, float* __restrict__ tau) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = w; i < n; i += nw) {
+        float mx = -__int_as_float(0x7f800000);
+        bool bad = false;
+        for (uint32_t k = lane; k < K; k += 32) {
+            const uint32_t j = hints[i * hk + k];
+            if (j >= n || j == i) {
+                bad = true;
+                continue;
+            }
+            mx = fmaxf(mx, ref_key(x + i * xs, x + (uint64_t)j * xs, d, xn[i], xn[j]));
+        }
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+        bad = __any_sync(0xFFFFFFFFu, bad);
+        if (lane == 0) tau[i] = bad ? __int_as_float(0x7f800000) : mx;
+    }
+}
+
+}  // namespace
+
+// Host helpers shared by the tensor-core entry points.
+int tc_prepare_rows(Ctx* c, const float* dx, uint64_t n, uint32_t xs, uint32_t d, uint32_t dp, DevBuf& xb,
+                    DevBuf& xnorm, DevBuf& xerr, DevBuf& xint) {
+    int rc;
+    if ((rc = ensure(c, xb, n * dp * 2)) || (rc = ensure(c, xnorm, n * 4)) || (rc = ensure(c, xerr, n * 4)) ||
+        (rc = ensure(c, xint, n)))
+        return rc;
+    bf16_rows_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(dx, n, xs, d, dp, xb.as<__nv_bfloat16>(),
+                                                             xnorm.as<float>(), xerr.as<float>(), xint.as<uint8_t>());
+    ANQI_CUDA(c, cudaGetLastError());
+    return ANQI_OK;
+}
+
+namespace {
+
+// Rows resident for the tensor path: FP32 copy, reference norms, bf16 copy,
+// |x|, |x - bf16(x)|, exact-int flags.
+struct TcRows {
+    TmpBuf f32, rn, bf, nrm, err, xint;
+    explicit TcRows(Ctx* c) : f32(c), rn(c), bf(c), nrm(c), err(c), xint(c) {}
+    int load(Ctx* c, const float* host, uint64_t n, uint32_t d, uint32_t xs, uint32_t dp) {
+        int rc;
+        if ((rc = upload_padded(c, f32, host, n, d, xs)) || (rc = ensure(c, rn, n * 4)) ||
+            (rc = compute_norms_device(c, f32.as<float>(), n, d, xs, rn.as<float>())) ||
+            (rc = tc_prepare_rows(c, f32.as<float>(), n, xs, d, dp, bf, nrm, err, xint)))
+            return rc;
+        return ANQI_OK;
+    }
+};
+
+__global__ void compact_rows_kernel(const uint32_t* __restrict__ cnt, uint32_t cap, const uint64_t* __restrict__ off,
+                                    uint64_t nrows, const uint32_t* __restrict__ in_id, const float* __restrict__ in_key,
+                                    uint32_t* __restrict__ out_id, float* __restrict__ out_key) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = w; i < nrows; i += nw) {
+        const uint32_t m = min(cnt[i], cap);
+        for (uint32_t k = lane; k < m; k += 32) {
+            out_id[off[i] + k] = in_id[i * cap + k];
+            out_key[off[i] + k] = in_key[i * cap + k];
+        }
+    }
+}
+
+__global__ void take_first_k_kernel(const uint64_t* __restrict__ off, uint64_t nrows, uint32_t K,
+                                    const uint32_t* __restrict__ in_id, const float* __restrict__ in_key,
+                                    uint32_t* __restrict__ ids, float* __restrict__ keys, uint32_t* __restrict__ err) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nrows * K) return;
+    const uint64_t i = t / K, k = t % K;
+    if (off[i + 1] - off[i] < K) {
+        if (k == 0) atomicExch(err, 5u);
+        ids[t] = kEmpty;
+        keys[t] = __int_as_float(0x7f800000);
+        return;
+    }
+    ids[t] = in_id[off[i] + k];
+    keys[t] = in_key[off[i] + k];
+}
+
+size_t filter_smem(uint32_t dp) {
+    return (size_t)(1 + kStages) * kTile * dp * 2 + (size_t)kStages * 4 * kTile * 4 + kStages * kTile + kTile * 8;
+}
+
+int launch_filter(Ctx* c, FilterParams p, uint64_t nrows) {
+    if (nrows == 0) return ANQI_OK;
+    const size_t smem = filter_smem(p.dp);
+    ANQI_CUDA(c, cudaFuncSetAttribute(tc_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const uint64_t gx = (nrows + kTile - 1) / kTile;
+    const uint64_t tiles = (p.n + kTile - 1) / kTile;
+    uint64_t gy = std::max<uint64_t>(1, ((uint64_t)2 * c->sm_count + gx - 1) / gx);
+    gy = std::min<uint64_t>(gy, tiles);
+    p.split_len = (tiles + gy - 1) / gy * kTile;
+    p.nrows = nrows;
+    dim3 grid((unsigned)gx, (unsigned)gy);
+    tc_filter_kernel<<<grid, kFilterThreads, smem, c->stream>>>(p);
+    ANQI_CUDA(c, cudaGetLastError());
+    return ANQI_OK;
+}
+
+// Runs the filter over all query rows, reruns rows whose hits exceeded the
+// capacity with a capacity that fits them, and returns the hits as a CSR
+// (off: nq + 1, host and device) sorted by (key, id) within each row.
+int filter_to_csr(Ctx* c, FilterParams p, uint64_t nq, uint32_t cap, std::vector<uint64_t>& hoff, TmpBuf& doff,
+                  TmpBuf& ids, TmpBuf& keys) {
+    TmpBuf cnt(c), oid(c), okey(c);
+    int rc;
+    if ((rc = ensure(c, cnt, nq * 4)) || (rc = ensure(c, oid, nq * cap * 4)) || (rc = ensure(c, okey, nq * cap * 4)))
+        return rc;
+    ANQI_CUDA(c, cudaMemsetAsync(cnt.p, 0, nq * 4, c->stream));
+    ANQI_CUDA(c, cudaMemsetAsync(c->err.p, 0, 4, c->stream));
+    p.cnt = cnt.as<uint32_t>();
+    p.cap = cap;
+    p.out_id = oid.as<uint32_t>();
+    p.out_key = okey.as<float>();
+    p.rows = nullptr;
+    p.err = c->err.as<uint32_t>();
+    if ((rc = launch_filter(c, p, nq))) return rc;
+    if ((rc = check_device_error(c, "tensor-core filter"))) return rc;
+    std::vector<uint32_t> hc(nq);
+    if ((rc = d2h(c, hc.data(), cnt, nq * 4)) || (rc = sync(c))) return rc;
+    // rows over capacity: run again with room for all their hits
+    std::vector<uint32_t> over;
+    uint32_t cap2 = 0;
+    for (uint64_t i = 0; i < nq; i++)
+        if (hc[i] > cap) {
+            over.push_back((uint32_t)i);
+            cap2 = std::max(cap2, hc[i]);
+        }
+    TmpBuf orow(c), ocnt(c), oid2(c), okey2(c);
+    if (!over.empty()) {
+        const uint64_t no = over.size();
+        // rerun outputs are indexed by row id, so they take nq x cap2 entries
+        if (nq * (uint64_t)cap2 * 4 > (8ull << 30))
+            return fail(c, ANQI_ERR_CAPACITY, "%zu rows need up to %u candidates each", over.size(), cap2);
+        if ((rc = h2d(c, orow, over.data(), no * 4)) || (rc = ensure(c, ocnt, nq * 4)) ||
+            (rc = ensure(c, oid2, nq * (uint64_t)cap2 * 4)) || (rc = ensure(c, okey2, nq * (uint64_t)cap2 * 4)))
+            return rc;
+        ANQI_CUDA(c, cudaMemsetAsync(ocnt.p, 0, nq * 4, c->stream));
+        FilterParams q = p;
+        q.rows = orow.as<uint32_t>();
+        q.cnt = ocnt.as<uint32_t>();
+        q.cap = cap2;
+        q.out_id = oid2.as<uint32_t>();
+        q.out_key = okey2.as<float>();
+        if ((rc = launch_filter(c, q, no))) return rc;
+        if ((rc = check_device_error(c, "tensor-core filter (capacity rerun)"))) return rc;
+    }
+    hoff.assign(nq + 1, 0);
+    uint64_t maxm = 0;
+    for (uint64_t i = 0; i < nq; i++) {
+        hoff[i + 1] = hoff[i] + hc[i];
+        maxm = std::max<uint64_t>(maxm, hc[i]);
+    }
+    const uint64_t tot = hoff[nq];
+    if ((rc = h2d(c, doff, hoff.data(), (nq + 1) * 8)) || (rc = ensure(c, ids, tot * 4 + 4)) ||
+        (rc = ensure(c, keys, tot * 4 + 4)))
+        return rc;
+    compact_rows_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(cnt.as<uint32_t>(), cap, doff.as<uint64_t>(), nq,
+                                                                oid.as<uint32_t>(), okey.as<float>(),
+                                                                ids.as<uint32_t>(), keys.as<float>());
+    ANQI_CUDA(c, cudaGetLastError());
+    if (!over.empty()) {
+        // the rerun rows' full lists replace their truncated ones (row i's
+        // hits went to i * cap2; rows not rerun have no hits there)
+        compact_rows_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(ocnt.as<uint32_t>(), cap2, doff.as<uint64_t>(),
+                                                                    nq, oid2.as<uint32_t>(), okey2.as<float>(),
+                                                                    ids.as<uint32_t>(), keys.as<float>());
+        ANQI_CUDA(c, cudaGetLastError());
+    }
+    return sort_csr_segments(c, doff.as<uint64_t>(), nq, ids.as<uint32_t>(), keys.as<float>(), maxm);
+}
+
+FilterParams make_params(const TcRows& Q, const TcRows& X, uint64_t n, uint32_t xs, uint32_t d, uint32_t dp) {
+    FilterParams p{};
+    p.qb = Q.bf.as<__nv_bfloat16>();
+    p.q32 = Q.f32.as<float>();
+    p.qn = Q.rn.as<float>();
+    p.qnorm = Q.nrm.as<float>();
+    p.qerr = Q.err.as<float>();
+    p.qint = Q.xint.as<uint8_t>();
+    p.xb = X.bf.as<__nv_bfloat16>();
+    p.x32 = X.f32.as<float>();
+    p.xn = X.rn.as<float>();
+    p.xnorm = X.nrm.as<float>();
+    p.xerr = X.err.as<float>();
+    p.xint = X.xint.as<uint8_t>();
+    p.n = n;
+    p.xs = xs;
+    p.d = d;
+    p.dp = dp;
+    return p;
+}
+
+}  // namespace
+
+}  // namespace anqi
+
+using namespace anqi;
+
+extern "C" {
+
+int anqi_bf16_gram(anqi_ctx* h, const float* a, uint64_t na, const float* b, uint64_t nb, uint32_t d, float* out) {
+    if (!h || !a || !b || !out || na == 0 || nb == 0 || d == 0) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    const uint32_t dp = round_up(d, 16u), xs = round_up(d, 8u);
+    if (dp > kMaxDp) return fail(c, ANQI_ERR_ARGS, "dimension %u exceeds the tensor-core tile limit %u", d, kMaxDp);
+    TmpBuf da(c), db(c), ab(c), bb(c), an(c), ae(c), ai(c), bn(c), be(c), bi(c), dout(c);
+    int rc;
+    if ((rc = upload_padded(c, da, a, na, d, xs)) || (rc = upload_padded(c, db, b, nb, d, xs)) ||
+        (rc = tc_prepare_rows(c, da.as<float>(), na, xs, d, dp, ab, an, ae, ai)) ||
+        (rc = tc_prepare_rows(c, db.as<float>(), nb, xs, d, dp, bb, bn, be, bi)) ||
+        (rc = ensure(c, dout, na * nb * 4)))
+        return rc;
+    ANQI_CUDA(c, cudaMemsetAsync(c->err.p, 0, 4, c->stream));
+    const size_t smem = (size_t)2 * kTile * dp * 2;
+    ANQI_CUDA(c, cudaFuncSetAttribute(gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((unsigned)((na + kTile - 1) / kTile), (unsigned)((nb + kTile - 1) / kTile));
+    gram_kernel<<<grid, 128, smem, c->stream>>>(ab.as<__nv_bfloat16>(), na, bb.as<__nv_bfloat16>(), nb, dp,
+                                                dout.as<float>(), c->err.as<uint32_t>());
+    ANQI_CUDA(c, cudaGetLastError());
+    if ((rc = check_device_error(c, "bf16 gram"))) return rc;
+    if ((rc = d2h(c, out, dout, na * nb * 4))) return rc;
+    return sync(c);
+}
+
+int anqi_rknn_ground_truth_tc(anqi_ctx* h, const float* base, uint64_t n, const float* query, uint64_t nq,
+                              uint32_t d, const float* rk2, uint32_t* off, uint32_t* ids, float* keys, uint64_t cap,
+                              uint64_t* total) {
+    if (!h || !base || !query || !rk2 || !off || n == 0 || nq == 0 || d == 0) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    const uint32_t dp = round_up(d, 16u), xs = round_up(d, 8u);
+    if (filter_smem(dp) > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "dimension %u too large for the tensor path", d);
+    TcRows X(c), Q(c);
+    TmpBuf dr(c), doff(c), did(c), dkey(c);
+    int rc;
+    if ((rc = X.load(c, base, n, d, xs, dp)) || (rc = Q.load(c, query, nq, d, xs, dp)) || (rc = h2d(c, dr, rk2, n * 4)))
+        return rc;
+    FilterParams p = make_params(Q, X, n, xs, d, dp);
+    p.thr_col = dr.as<float>();
+    std::vector<uint64_t> hoff;
+    if ((rc = filter_to_csr(c, p, nq, 256, hoff, doff, did, dkey))) return rc;
+    const uint64_t tot = hoff[nq];
+    if (total) *total = tot;
+    if (tot > cap || tot > 0xFFFFFFFFull)
+        return fail(c, ANQI_ERR_CAPACITY, "reverse-kNN output needs %llu entries", (unsigned long long)tot);
+    for (uint64_t i = 0; i <= nq; i++) off[i] = (uint32_t)hoff[i];
+    if (tot) {
+        if (ids && (rc = d2h(c, ids, did, tot * 4))) return rc;
+        if (keys && (rc = d2h(c, keys, dkey, tot * 4))) return rc;
+    }
+    return sync(c);
+}
+
+int anqi_exact_topk_tc(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, uint32_t K, const uint32_t* hints,
+                       uint32_t hint_k, uint32_t* ids, float* keys) {
+    if (!h || !base || !ids || !keys || d == 0 || K == 0 || K > 256) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    if (K >= n) return fail(c, ANQI_ERR_ARGS, "require K < base vector count");
+    const uint32_t dp = round_up(d, 16u), xs = round_up(d, 8u);
+    if (filter_smem(dp) > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "dimension %u too large for the tensor path", d);
+    // hints: the caller's (e.g. AKNN lists) or an AKNN build here
+    std::vector<uint32_t> own;
+    if (!hints) {
+        anqi_aknn_params ap{};
+        ap.k = std::max<uint32_t>(K, 100);
+        ap.leaf = 500;
+        ap.trees = 64;
+        ap.ef = 600;
+        ap.ef_alpha = 8;
+        ap.seed = 10;
+        ap.nn_sample = 20;
+        if (ap.k >= n) ap.k = (uint32_t)n - 1;
+        own.resize(n * ap.k);
+        std::vector<float> od(n * ap.k);
+        int rc0 = anqi_aknn_build(h, base, n, d, &ap, own.data(), od.data(), nullptr);
+        if (rc0) return rc0;
+        hints = own.data();
+        hint_k = ap.k;
+    }
+    if (hint_k < K) return fail(c, ANQI_ERR_ARGS, "need at least K = %u hints per row, got %u", K, hint_k);
+    TcRows X(c);
+    TmpBuf dh(c), tau(c), doff(c), did(c), dkey(c), ko(c), kk(c);
+    int rc;
+    if ((rc = X.load(c, base, n, d, xs, dp)) || (rc = h2d(c, dh, hints, n * hint_k * 4)) || (rc = ensure(c, tau, n * 4)))
+        return rc;
+    hint_bound_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(X.f32.as<float>(), X.rn.as<float>(), n, xs, d,
+                                                              dh.as<uint32_t>(), hint_k, K, tau.as<float>());
+    ANQI_CUDA(c, cudaGetLastError());
+    FilterParams p = make_params(X, X, n, xs, d, dp);
+    p.thr_row = tau.as<float>();
+    p.exclude_self = 1;
+    std::vector<uint64_t> hoff;
+    if ((rc = filter_to_csr(c, p, n, K + 156, hoff, doff, did, dkey))) return rc;
+    if ((rc = ensure(c, ko, n * K * 4)) || (rc = ensure(c, kk, n * K * 4))) return rc;
+    ANQI_CUDA(c, cudaMemsetAsync(c->err.p, 0, 4, c->stream));
+    const uint64_t tk = n * K;
+    take_first_k_kernel<<<(unsigned)((tk + 255) / 256), 256, 0, c->stream>>>(
+        doff.as<uint64_t>(), n, K, did.as<uint32_t>(), dkey.as<float>(), ko.as<uint32_t>(), kk.as<float>(),
+        c->err.as<uint32_t>());
+    ANQI_CUDA(c, cudaGetLastError());
+    if ((rc = check_device_error(c, "exact top-K (tensor path)"))) return rc;
+    if ((rc = d2h(c, ids, ko, n * K * 4)) || (rc = d2h(c, keys, kk, n * K * 4))) return rc;
+    return sync(c);
+}
+
+}  // extern "C"

@@ -290,6 +290,33 @@ int anqi_rknn_query_noalloc(const anqi_device_index* ix, const float* queries, u
                             const float* thresholds, uint32_t L, uint32_t max_pred, uint32_t* pred_count,
                             uint32_t* pred_ids, uint32_t* n_dist, void* stream);
 
+/* ------------------------------------------- LRQ objective (training)
+ * The radius-reconstruction objective the trainer minimises
+ * (tools/train_final_m8_u8.py:90-157, 206-218), FP64, on DEVICE pointers,
+ * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream); they
+ * allocate nothing.  T: n x nk rows; mu: nk; G: m x nk; B: nk x cs, rows
+ * ascending.  c = (T - mu) G^T, base = mu + c G, a = nearest code of T - base
+ * (decode_nearest, :146-156; or codes_in when given), r = base + B[k,a] - T,
+ * *loss = sum(r^2) (divide by n*nk for the mean).  Outputs r (n x nk), c
+ * (n x m), a (n x nk).  Limits: nk <= 128, m <= 16, cs <= 256.
+ * Backward (codes fixed): g_mu, g_G, g_B = scale * d(sum r^2)/d(mu, G, B)
+ * from the forward's r, c, a; the outputs are overwritten.  The B gradient
+ * is a segment sum by code; its accumulation order is not fixed (FP64
+ * atomics), so repeated calls may differ in the last bits. */
+int anqi_lrq_objective_forward(const double* T, uint64_t n, uint32_t nk, uint32_t m, const double* mu,
+                               const double* G, const double* B, uint32_t cs, const uint8_t* codes_in, double* r,
+                               double* c, uint8_t* a, double* loss, void* stream);
+int anqi_lrq_objective_backward(const double* T, uint64_t n, uint32_t nk, uint32_t m, const double* mu,
+                                const double* G, const double* r, const double* c, const uint8_t* a, uint32_t cs,
+                                double scale, double* g_mu, double* g_G, double* g_B, void* stream);
+
+/* ------------------------------------------ BF16 tensor-core tiles
+ * out[i, j] = <bf16(a_i), bf16(b_j)> accumulated in FP32 on the tcgen05 tensor
+ * cores (the tile primitive of the precision-form distance work); a: na x d,
+ * b: nb x d, out: na x nb.  d <= 256.  No reference counterpart: the
+ * reference computes every distance in FP32 (include/distance.h). */
+int anqi_bf16_gram(anqi_ctx* ctx, const float* a, uint64_t na, const float* b, uint64_t nb, uint32_t d, float* out);
+
 /* ---------------------------------------------------- exact ground truth
  * tools/dataset_gt.cpp:206-313 in FP32 with the reference's summation order:
  * per base row the K nearest other rows by (key, id), key = |a|^2+|b|^2-2ab. */
@@ -301,6 +328,19 @@ int anqi_exact_topk(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d, ui
 int anqi_rknn_ground_truth(anqi_ctx* ctx, const float* base, uint64_t n, const float* query, uint64_t nq,
                            uint32_t d, const float* rk2, uint32_t* off, uint32_t* ids, float* keys,
                            uint64_t cap, uint64_t* total);
+
+/* Precision form of the two entry points above: BF16 tcgen05 tiles with FP32
+ * accumulation filter every pair by a derived bound on |key~ - key32|; the
+ * pairs within it are recomputed in the reference's FP32 order.  Outputs equal
+ * anqi_exact_topk / anqi_rknn_ground_truth bit for bit.  d <= 208.
+ * anqi_exact_topk_tc bounds each row's K-th key by the largest FP32 key to K
+ * distinct other rows: hints (n x hint_k ids, e.g. the AKNN lists, hint_k >= K)
+ * or, when hints is NULL, an AKNN build run here. */
+int anqi_exact_topk_tc(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d, uint32_t K, const uint32_t* hints,
+                       uint32_t hint_k, uint32_t* ids, float* keys);
+int anqi_rknn_ground_truth_tc(anqi_ctx* ctx, const float* base, uint64_t n, const float* query, uint64_t nq,
+                              uint32_t d, const float* rk2, uint32_t* off, uint32_t* ids, float* keys,
+                              uint64_t cap, uint64_t* total);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,97 @@
+"""BF16 tensor-core tiles (tcgen05, csrc/tc.cu): the Gram tile primitive
+against NumPy on bf16-rounded inputs, and the precision-form ground truth
+against the FP32 path (bit-exact outputs)."""
+import numpy as np
+import pytest
+
+from anqi._lib import Context
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    with Context(0) as c:
+        yield c
+
+
+def bf16(x):
+    """Round-to-nearest-even to bfloat16, returned as float64."""
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16 << 16
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+@pytest.mark.parametrize("na,nb,d", [(128, 128, 128), (300, 200, 128), (37, 260, 8), (129, 5, 32), (64, 64, 256)])
+def test_gram_integer_inputs_exact(ctx, na, nb, d):
+    rng = np.random.default_rng(na + nb + d)
+    a = rng.integers(0, 256, size=(na, d)).astype(np.float32)
+    b = rng.integers(0, 256, size=(nb, d)).astype(np.float32)
+    got = ctx.bf16_gram(a, b)
+    ref = a.astype(np.float64) @ b.astype(np.float64).T
+    if d * 255 * 255 < 2 ** 24:
+        assert np.array_equal(got.astype(np.float64), ref)
+    else:
+        assert np.max(np.abs(got - ref) / np.maximum(ref, 1)) < 1e-6
+
+
+def test_gram_float_inputs_within_fp32_accumulation(ctx):
+    rng = np.random.default_rng(5)
+    a = rng.normal(size=(256, 96)).astype(np.float32)
+    b = rng.normal(size=(192, 96)).astype(np.float32)
+    got = ctx.bf16_gram(a, b).astype(np.float64)
+    ref = bf16(a) @ bf16(b).T
+    bound = 2 * 96 * 2.0 ** -24 * (np.abs(bf16(a)) @ np.abs(bf16(b)).T)
+    assert np.all(np.abs(got - ref) <= bound + 1e-30)
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def mixture(n, d, seed, integer=True):
+    rng = np.random.default_rng(seed)
+    cen = rng.uniform(0, 128, size=(40, d))
+    x = cen[rng.integers(0, 40, size=n)] + rng.normal(scale=20, size=(n, d))
+    if integer:
+        return np.clip(np.rint(x), 0, 255).astype(np.float32)
+    return (x / 50.0).astype(np.float32)
+
+
+@pytest.mark.parametrize("integer", [True, False])
+def test_exact_topk_tc_equals_fp32(ctx, integer):
+    from anqi import pipeline
+    base = mixture(3000, 128 if integer else 40, 3 + integer, integer)
+    base[17] = base[5]            # duplicates: exact ties at key 0 and elsewhere
+    base[2999] = base[5]
+    ids32, keys32 = pipeline.exact_thresholds(ctx, base, 100)
+    ids, keys = ctx.exact_topk_tc(base, 100, hints=ids32[:, ::-1].copy())   # perfect hints, any order
+    assert np.array_equal(ids, ids32) and np.array_equal(bits(keys), bits(keys32))
+    ids2, keys2 = ctx.exact_topk_tc(base, 100)                               # hints from an AKNN build
+    assert np.array_equal(ids2, ids32) and np.array_equal(bits(keys2), bits(keys32))
+
+
+def test_exact_topk_tc_reference_sample(ctx, sample):
+    ids, keys = ctx.exact_topk_tc(sample["base"], 100)
+    assert np.array_equal(ids, sample["exact_ids"]) and np.array_equal(bits(keys), bits(sample["exact_keys"]))
+
+
+@pytest.mark.parametrize("integer", [True, False])
+def test_rknn_gt_tc_equals_fp32(ctx, integer):
+    from anqi import pipeline
+    d = 128 if integer else 72
+    both = mixture(5300, d, 11, integer)       # queries from the same centres as the base
+    base, query = both[:5000], both[5000:]
+    _, ex = pipeline.exact_thresholds(ctx, base, 50)
+    for k in (10, 50):
+        off, ids, keys = pipeline.rknn_ground_truth(ctx, base, query, ex[:, k - 1])
+        off2, ids2, keys2 = ctx.rknn_ground_truth_tc(base, query, ex[:, k - 1])
+        assert np.array_equal(off, off2) and np.array_equal(ids, ids2) and np.array_equal(bits(keys), bits(keys2))
+        assert off[-1] > 0
+
+
+def test_rknn_gt_tc_reference_sample(ctx, sample):
+    for ki, k in enumerate((10, 50, 100)):
+        off, ids, keys = ctx.rknn_ground_truth_tc(sample["base"], sample["query"], sample["exact_keys"][:, k - 1])
+        assert np.array_equal(off, sample[f"gt_off_{k}"]) and np.array_equal(ids, sample[f"gt_ids_{k}"])
+        assert np.array_equal(bits(keys), bits(sample[f"gt_keys_{k}"]))
