@@ -140,16 +140,24 @@ def load_index(ctx: Context, ix: Index, ks=(10, 50, 100)) -> None:
         ctx.verifier_materialize(k)
 
 
-def exact_thresholds(ctx: Context, base: np.ndarray, K: int = 100):
+def exact_thresholds(ctx: Context, base: np.ndarray, K: int = 100, method: str = "fp32", hints=None):
+    """Exact top-K (dataset_gt --mode thresholds).  method "tc": BF16 tensor-core
+    tiles with FP32 recheck (bit-identical output); hints = AKNN lists bound each
+    row's K-th key (an AKNN build runs when they are absent)."""
     base = np.ascontiguousarray(base, np.float32)
     n, d = base.shape
+    if method == "tc" and d <= 208:
+        return ctx.exact_topk_tc(base, K, hints)
     ids = np.empty((n, K), np.uint32)
     keys = np.empty((n, K), np.float32)
     ctx._check(ctx.lib.anqi_exact_topk(ctx.h, base, n, d, K, ids, keys), "exact_topk")
     return ids, keys
 
 
-def rknn_ground_truth(ctx: Context, base: np.ndarray, query: np.ndarray, rk2: np.ndarray):
+def rknn_ground_truth(ctx: Context, base: np.ndarray, query: np.ndarray, rk2: np.ndarray, method: str = "fp32"):
+    """Exact RkNN CSR (dataset_gt --mode ground-truth); method "tc" as above."""
+    if method == "tc" and base.shape[1] <= 208:
+        return ctx.rknn_ground_truth_tc(base, query, rk2)
     base = np.ascontiguousarray(base, np.float32)
     query = np.ascontiguousarray(query, np.float32)
     n, d = base.shape
