@@ -62,9 +62,11 @@ struct Batch {
     DevBuf pred_buf, cand_buf;           // atomic-fill output buffers
     DevBuf pred_off, cand_off;           // CSR offsets (device)
     DevBuf pred_csr, cand_csr;
+    DevBuf entry, enode, order, leaf_cnt;  // entry object / leaf node per query, leaf-ordered work list
     uint64_t pred_cap = 0, cand_cap = 0;
     bool have_results = false;
     bool have_cands = false;
+    bool ordered = false;  // work list ordered by entry leaf
 };
 
 struct Ctx {

@@ -43,6 +43,8 @@ struct SearchParams {
     double scale, R2;
     const float* thr;  // slot-major thresholds
     const float* queries;
+    const uint32_t* entry;  // entry object per query (rknn_entry_kernel)
+    const uint32_t* order;  // work item -> query (leaf-ordered), or null for identity
     const uint32_t* qL;
     const uint8_t* qslot;
     uint32_t L_all, slot_all, nq, L_max;
@@ -223,26 +225,34 @@ __device__ __forceinline__ void load_links(const SearchParams& p, uint32_t node,
     l1 = lane + 32 < p.degree ? lk[lane + 32] : kEmpty;
 }
 
-// Sorts the m (<= 64) fresh (dist, id) entries in nd/ni ascending.  Small
-// batches (the common case after the first expansions) are ranked by counting;
-// larger ones use the register bitonic network.
-__device__ __forceinline__ void sort_fresh(float* nd, uint32_t* ni, uint32_t m, uint32_t lane) {
+// Of the m (<= 64) fresh (dist, id) entries in nd/ni, keeps those that can
+// enter the beam -- all of them while the beam is not full, else those ranking
+// before its last entry (td, tid), since any other would land at rank >= L --
+// and sorts them ascending into nd/ni[0..m').  Returns m'.  Small batches (the
+// common case after the first expansions) are ranked by counting over the kept
+// entries only; larger ones use the register bitonic network, after which the
+// kept entries are a prefix.
+__device__ __forceinline__ uint32_t sort_fresh_kept(float* nd, uint32_t* ni, uint32_t m, bool full, float td,
+                                                    uint32_t tid, uint32_t lane) {
     if (m <= 32) {
         const float dv = lane < m ? nd[lane] : 0.f;
         const uint32_t iv = lane < m ? ni[lane] : kEmpty;
+        const bool keep = lane < m && (!full || nb_less(dv, iv, td, tid));
+        const unsigned km = __ballot_sync(kFull, keep);
         uint32_t rank = 0;
-        for (uint32_t s = 0; s < m; s++) {
+        for (unsigned r = km; r; r &= r - 1) {
+            const int s = __ffs(r) - 1;
             const float ds = __shfl_sync(kFull, dv, s);
             const uint32_t is = __shfl_sync(kFull, iv, s);
             rank += nb_less(ds, is, dv, iv) ? 1u : 0u;
         }
         __syncwarp();
-        if (lane < m) {
+        if (keep) {
             nd[rank] = dv;
             ni[rank] = iv;
         }
         __syncwarp();
-        return;
+        return __popc(km);
     }
     const float inf = __int_as_float(0x7f800000);
     float d0 = lane < m ? nd[lane] : inf;
@@ -255,7 +265,11 @@ __device__ __forceinline__ void sort_fresh(float* nd, uint32_t* ni, uint32_t m, 
     ni[lane] = i0;
     nd[lane + 32] = d1;
     ni[lane + 32] = i1;
+    const bool k0 = lane < m && (!full || nb_less(d0, i0, td, tid));
+    const bool k1 = lane + 32 < m && (!full || nb_less(d1, i1, td, tid));
+    const uint32_t kept = __popc(__ballot_sync(kFull, k0)) + __popc(__ballot_sync(kFull, k1));
     __syncwarp();
+    return kept;
 }
 
 // Distances of the m fresh neighbours to the lifted query: 8 groups of 4
@@ -303,22 +317,20 @@ extern __shared__ __align__(16) unsigned char g_smem[];
 
 __device__ __host__ __forceinline__ size_t search_smem_words(uint32_t L_max, uint32_t lstride, uint32_t bstride,
                                                              uint32_t hash_cap) {
-    return (size_t)4 * L_max + 128 + lstride + bstride + 8 * (size_t)(lstride > bstride ? lstride : bstride) +
+    return (size_t)2 * L_max + 128 + lstride + bstride + 8 * (size_t)(lstride > bstride ? lstride : bstride) +
            hash_cap;
 }
 
-__global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
+__global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
     const size_t per_warp = search_smem_words(p.L_max, p.lstride, p.bstride, p.hash_cap) * 4;
     unsigned char* my = g_smem + wib * per_warp;
     float* qhat = reinterpret_cast<float*>(my);
     float* qraw = qhat + p.lstride;
-    float* bdA = qraw + p.bstride;
-    uint32_t* biA = reinterpret_cast<uint32_t*>(bdA + p.L_max);
-    float* bdB = reinterpret_cast<float*>(biA + p.L_max);
-    uint32_t* biB = reinterpret_cast<uint32_t*>(bdB + p.L_max);
-    float* nd = reinterpret_cast<float*>(biB + p.L_max);
+    float* bd = qraw + p.bstride;  // the beam: sorted (dist, id), expanded flag in the id's top bit
+    uint32_t* bi = reinterpret_cast<uint32_t*>(bd + p.L_max);
+    float* nd = reinterpret_cast<float*>(bi + p.L_max);
     uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 64);
     float* stage = reinterpret_cast<float*>(ni + 64);  // 8 staged rows of max(lstride, bstride)
     uint32_t* tab = reinterpret_cast<uint32_t*>(stage + 8 * (size_t)max(p.lstride, p.bstride));
@@ -330,10 +342,11 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
     __syncwarp();
 
     for (;;) {
-        uint32_t qi = 0;
-        if (lane == 0) qi = atomicAdd(p.work, 1u);
-        qi = __shfl_sync(kFull, qi, 0);
-        if (qi >= p.nq) break;
+        uint32_t w = 0;
+        if (lane == 0) w = atomicAdd(p.work, 1u);
+        w = __shfl_sync(kFull, w, 0);
+        if (w >= p.nq) break;
+        const uint32_t qi = p.order ? p.order[w] : w;
         const uint32_t L = min(p.qL ? p.qL[qi] : p.L_all, p.L_max);
         const uint32_t tslot = p.qslot ? p.qslot[qi] : p.slot_all;
         const float* q = p.queries + (size_t)qi * p.bstride;
@@ -346,19 +359,8 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
             qhat[j] = v;
         }
         __syncwarp();
-        // RP-tree entry, rptrees.h:108-124 (|margin| <= EPS goes left)
-        uint32_t v = p.troot;
-        for (uint32_t depth = 0; p.tleft[v] != kEmpty && depth < 4096; depth++) {
-            stage_row_async(stage, p.thyper + (size_t)v * p.lstride, p.lstride, lane, 32);
-            cp_async_wait_all();
-            __syncwarp();
-            const float ip = group_ip(stage, qhat, p.dim, gt, kFull);
-            __syncwarp();
-            const float margin = __fsub_rn(ip, p.toffset[v]);
-            v = (margin < -kSplitEps) ? p.tleft[v] : (margin > kSplitEps ? p.tright[v] : p.tleft[v]);
-        }
-        uint32_t ep = p.tleaf[v];
-        if (ep == kEmpty || ep >= p.n) ep = 0;
+        uint32_t ep = p.entry[qi];
+        if (ep >= p.n) ep = 0;
 
         Visited vis{tab,  p.hash_cap, p.hash_shift, p.gtab ? p.gtab + (size_t)slot * p.gcap : nullptr,
                     p.gcap, p.gshift, bits, vlog, p.log_cap, p.hash_cap ? 0u : (p.gcap ? 1u : 2u)};
@@ -371,8 +373,8 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
             uint32_t rec = ep;
             vis_first(vis, ep, rec, p.err);
             if (vis.level != 0 && p.log_cap) vlog[0] = rec;
-            bdA[0] = dep;
-            biA[0] = ep;
+            bd[0] = dep;
+            bi[0] = ep;
         }
         uint32_t nlog = 1, ncand = 0, nexp = 0, nfl = 0;
         bool overflow = false;
@@ -381,10 +383,6 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
             ncand = 1;
         }
         __syncwarp();
-        float* bd = bdA;
-        uint32_t* bi = biA;
-        float* od = bdB;
-        uint32_t* oi = biB;
         uint32_t size = 1, cur = 0;
         // links of the next node to expand, loaded while the current merge runs
         uint32_t pre_node = kEmpty, pl0 = kEmpty, pl1 = kEmpty, pdg = 0;
@@ -396,6 +394,7 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
             if (lane == 0) bi[cur] = node | kExpanded;
             __syncwarp();
             nexp++;
+            // entries before cur are all expanded; nxt = the next unexpanded one
             uint32_t nxt = size;
             for (uint32_t s0 = cur + 1; s0 < size; s0 += 32) {
                 const uint32_t idx = s0 + lane;
@@ -416,7 +415,15 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
             }
             vis_room(vis, nlog, p.degree, lane, p.err);
             const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane);
-            if (m == 0) {
+            uint32_t mk = 0;
+            if (m != 0) {
+                fresh_distances(p, qhat, ni, nd, m, gw, gt, stage);
+                append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
+                const bool full = size >= L;
+                mk = sort_fresh_kept(nd, ni, m, full, full ? bd[L - 1] : 0.f, full ? bi[L - 1] : 0u, lane);
+            }
+            if (mk == 0) {
+                // no fresh entry enters the beam: only the cursor moves
                 cur = nxt;
                 if (nxt < size) {
                     pre_node = bi[nxt] & kIdMask;
@@ -424,45 +431,50 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
                 }
                 continue;
             }
-            fresh_distances(p, qhat, ni, nd, m, gw, gt, stage);
-            append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
-            // batch insert = merge of the sorted batch into the sorted beam
-            sort_fresh(nd, ni, m, lane);
-            const uint32_t ns = min(L, size + m);
-            // first unexpanded entry of the merged beam: the best fresh entry or
-            // the old beam's next one, whichever ranks first
-            uint32_t cb = 0xFFFFFFFFu;
-            if (nxt < size) cb = nxt + lower_rank(nd, ni, m, bd[nxt], bi[nxt]);
-            const uint32_t cn = lower_rank(bd, bi, size, nd[0], ni[0]);
-            uint32_t nc = min(cb, cn);
-            if (nc > ns) nc = ns;
-            if (nc < ns) {
-                pre_node = cn < cb ? ni[0] : (bi[nxt] & kIdMask);
-                load_links(p, pre_node, lane, pl0, pl1, pdg);
-            }
-            for (uint32_t p0 = lane; p0 < size; p0 += 32) {
-                const float dv = bd[p0];
-                const uint32_t iv = bi[p0];
-                const uint32_t pos = p0 + lower_rank(nd, ni, m, dv, iv);
-                if (pos < ns) {
-                    od[pos] = dv;
-                    oi[pos] = iv;
+            // Batch insert of the mk kept entries (sorted) into the sorted
+            // beam.  Fresh entry r lands at r + (beam entries before it);
+            // beam entry j at j + (fresh entries before it); only entries from
+            // cn (the rank of the best fresh one) on move.
+            uint32_t r0 = 0, r1 = 0;
+            if (lane < mk) r0 = lower_rank(bd, bi, size, nd[lane], ni[lane]);
+            if (lane + 32 < mk) r1 = lower_rank(bd, bi, size, nd[lane + 32], ni[lane + 32]);
+            const uint32_t cn = __shfl_sync(kFull, r0, 0);
+            const uint32_t ns = min(L, size + mk);
+            // first unexpanded entry of the merged beam: the old beam's next
+            // one if it ranks before every fresh entry, else the best fresh one
+            const bool old_next = nxt < cn;
+            const uint32_t nc = old_next ? nxt : cn;
+            pre_node = old_next ? (bi[nxt] & kIdMask) : ni[0];
+            load_links(p, pre_node, lane, pl0, pl1, pdg);
+            __syncwarp();
+            // move beam entries [cn, size) right, highest first, so no entry is
+            // overwritten before it is read
+            for (uint32_t hi = size; hi > cn; hi = hi > cn + 32 ? hi - 32 : cn) {
+                const uint32_t j = hi - 1 - lane;
+                const bool mv = lane < hi - cn;
+                float dv = 0.f;
+                uint32_t iv = 0, pos = ns;
+                if (mv) {
+                    dv = bd[j];
+                    iv = bi[j];
+                    pos = j + lower_rank(nd, ni, mk, dv, iv);
                 }
-            }
-            for (uint32_t r = lane; r < m; r += 32) {
-                const uint32_t pos = r + lower_rank(bd, bi, size, nd[r], ni[r]);
+                __syncwarp();
                 if (pos < ns) {
-                    od[pos] = nd[r];
-                    oi[pos] = ni[r];
+                    bd[pos] = dv;
+                    bi[pos] = iv;
                 }
+                __syncwarp();
+            }
+            if (lane < mk && lane + r0 < ns) {
+                bd[lane + r0] = nd[lane];
+                bi[lane + r0] = ni[lane];
+            }
+            if (lane + 32 < mk && lane + 32 + r1 < ns) {
+                bd[lane + 32 + r1] = nd[lane + 32];
+                bi[lane + 32 + r1] = ni[lane + 32];
             }
             __syncwarp();
-            float* td = bd;
-            bd = od;
-            od = td;
-            uint32_t* ti = bi;
-            bi = oi;
-            oi = ti;
             size = ns;
             cur = nc;
         }
@@ -548,6 +560,57 @@ __global__ void __launch_bounds__(128) rknn_search_kernel(SearchParams p) {
         for (uint32_t t = lane; t < p.hash_cap; t += 32) tab[t] = kEmpty;
         __syncwarp();
     }
+}
+
+// Query lift and RP-tree entry (rknn_query.cpp:2724-2729, rptrees.h:108-124;
+// |margin| <= EPS goes left), one warp per query: writes the entry object and
+// the leaf node reached.  The leaf orders the search's work list.
+__global__ void __launch_bounds__(128) rknn_entry_kernel(SearchParams p, uint32_t* __restrict__ enode,
+                                                         uint32_t* __restrict__ entry) {
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u;
+    float* qhat = reinterpret_cast<float*>(g_smem) + (size_t)wib * 2 * p.lstride;
+    float* stage = qhat + p.lstride;
+    for (uint32_t qi = blockIdx.x * (blockDim.x >> 5) + wib; qi < p.nq; qi += gridDim.x * (blockDim.x >> 5)) {
+        const float* q = p.queries + (size_t)qi * p.bstride;
+        for (uint32_t j = lane; j < p.lstride; j += 32) {
+            float v = 0.0f;
+            if (j < p.d) v = __double2float_rn(__dmul_rn((double)q[j], p.scale));
+            else if (j == p.d) v = 1.0f;
+            qhat[j] = v;
+        }
+        __syncwarp();
+        uint32_t v = p.troot;
+        for (uint32_t depth = 0; p.tleft[v] != kEmpty && depth < 4096; depth++) {
+            stage_row_async(stage, p.thyper + (size_t)v * p.lstride, p.lstride, lane, 32);
+            cp_async_wait_all();
+            __syncwarp();
+            const float ip = group_ip(stage, qhat, p.dim, gt, kFull);
+            __syncwarp();
+            const float margin = __fsub_rn(ip, p.toffset[v]);
+            v = (margin < -kSplitEps) ? p.tleft[v] : (margin > kSplitEps ? p.tright[v] : p.tleft[v]);
+        }
+        if (lane == 0) {
+            uint32_t ep = p.tleaf[v];
+            if (ep == kEmpty || ep >= p.n) ep = 0;
+            entry[qi] = ep;
+            enode[qi] = v;
+        }
+        __syncwarp();
+    }
+}
+
+// Counting sort of the queries by entry leaf: queries that start in the same
+// leaf run at about the same time and share the rows they fetch in L2.  The
+// order inside a leaf is arbitrary; it changes scheduling, not results.
+__global__ void leaf_count_kernel(const uint32_t* __restrict__ enode, uint32_t nq, uint32_t* __restrict__ cnt) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x)
+        atomicAdd(cnt + enode[q], 1u);
+}
+
+__global__ void leaf_scatter_kernel(const uint32_t* __restrict__ enode, uint32_t nq, uint32_t* __restrict__ cursor,
+                                    uint32_t* __restrict__ order) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x)
+        order[atomicAdd(cursor + enode[q], 1u)] = q;
 }
 
 // Exclusive scan of counts (nq) into off (nq + 1), one block, fixed order.
@@ -859,6 +922,51 @@ int anqi_query_upload(anqi_ctx* h, const float* queries, uint32_t nq, const uint
     return sync(c);
 }
 
+// Entry objects of the batch (lift + RP-tree descent) and, unless
+// ANQI_B200_ORDER=0, the work list ordered by entry leaf.
+static int prepare_entries(Ctx* c, bool* ordered) {
+    Batch& b = c->batch;
+    const QueryIndex& ix = c->ix;
+    int rc;
+    const uint32_t nq = b.nq;
+    if ((rc = ensure(c, b.entry, nq * 4ull)) || (rc = ensure(c, b.enode, nq * 4ull)) ||
+        (rc = ensure(c, b.order, nq * 4ull)) || (rc = ensure(c, b.leaf_cnt, 2 * (ix.tree_nodes + 1ull) * 4)))
+        return rc;
+    SearchParams p{};
+    p.queries = b.q.as<float>();
+    p.nq = nq;
+    p.n = ix.n;
+    p.d = ix.d;
+    p.dim = ix.dim;
+    p.bstride = ix.bstride;
+    p.lstride = ix.lstride;
+    p.scale = ix.scale;
+    p.tleft = ix.tleft.as<uint32_t>();
+    p.tright = ix.tright.as<uint32_t>();
+    p.toffset = ix.toffset.as<float>();
+    p.thyper = ix.thyper.as<float>();
+    p.tleaf = ix.tleaf.as<uint32_t>();
+    p.troot = ix.troot;
+    const size_t smem = 4ull * 2 * ix.lstride * 4;
+    if (smem > 48 * 1024)
+        ANQI_CUDA(c, cudaFuncSetAttribute(rknn_entry_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const uint32_t blocks = std::min<uint32_t>(c->sm_count * 8, (nq + 3) / 4);
+    rknn_entry_kernel<<<blocks, 128, smem, c->stream>>>(p, b.enode.as<uint32_t>(), b.entry.as<uint32_t>());
+    const char* env = std::getenv("ANQI_B200_ORDER");
+    *ordered = !(env && env[0] == '0');
+    if (*ordered) {
+        uint32_t* cnt = b.leaf_cnt.as<uint32_t>();
+        uint32_t* cursor = cnt + ix.tree_nodes + 1;
+        const uint32_t tb = std::min<uint32_t>(c->sm_count * 4, (nq + 255) / 256);
+        ANQI_CUDA(c, cudaMemsetAsync(cnt, 0, ix.tree_nodes * 4ull, c->stream));
+        leaf_count_kernel<<<tb, 256, 0, c->stream>>>(b.enode.as<uint32_t>(), nq, cnt);
+        scan_counts_kernel<<<1, 1024, 0, c->stream>>>(cnt, ix.tree_nodes, cursor);
+        leaf_scatter_kernel<<<tb, 256, 0, c->stream>>>(b.enode.as<uint32_t>(), nq, cursor, b.order.as<uint32_t>());
+    }
+    ANQI_CUDA(c, cudaGetLastError());
+    return ANQI_OK;
+}
+
 // One search launch with configuration cfg; ms = its device time.  Returns
 // ANQI_ERR_CAPACITY (and the needed fill) when an output buffer was too small.
 static int launch_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, float* ms, unsigned long long* fill) {
@@ -890,6 +998,8 @@ static int launch_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, floa
     p.R2 = ix.mstar2 + 1.0;  // rknn_query.cpp:2729, eps = 0
     p.thr = c->thr_table.as<float>();
     p.queries = b.q.as<float>();
+    p.entry = b.entry.as<uint32_t>();
+    p.order = b.ordered ? b.order.as<uint32_t>() : nullptr;
     p.qL = b.has_L ? b.qL.as<uint32_t>() : nullptr;
     p.qslot = b.has_k ? b.qslot.as<uint8_t>() : nullptr;
     p.L_all = b.L_all;
@@ -997,6 +1107,7 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
         c->log_cap = log_cap;
         c->cand_cap = cand_cap;
     }
+    if ((rc = prepare_entries(c, &b.ordered))) return rc;
     if (b.pred_cap == 0) b.pred_cap = std::max<uint64_t>(1024, (uint64_t)b.nq * 128);
     if (keep_candidates && b.cand_cap == 0) b.cand_cap = std::max<uint64_t>(1024, (uint64_t)b.nq * 256);
     // autotune once per (n, L_max, nq): time every configuration, keep the fastest
