@@ -1,0 +1,207 @@
+// Per-warp search state shared by the query and index-construction kernels:
+// the three-level visited set and the in-place batch insert into a sorted
+// (dist, id) beam.
+#pragma once
+
+#include "common.cuh"
+#include "util.cuh"
+
+namespace anqi {
+
+// The visited set of one query, in up to three levels:
+//   0  an open-addressing table in the warp's shared memory (atomicCAS,
+//      linear probing, kept at or below 5/8 load);
+//   1  a per-slot open-addressing table in global memory, small enough that
+//      all slots' tables stay resident in L2 (same rules);
+//   2  the per-slot bitmap over all n ids.
+// Before an expansion could push the current level past its load limit, its
+// ids move one level up.  The log records, per first visit, what the clean-up
+// at the end of the query needs: nothing at level 0, the table position at
+// level 1, the id at level 2.
+struct Visited {
+    uint32_t* tab;
+    uint32_t cap, shift;
+    uint32_t* gtab;
+    uint32_t gcap, gshift;
+    uint32_t* bits;
+    uint32_t* vlog;
+    uint32_t log_cap;
+    uint32_t level;
+};
+
+// Inserts id into an open-addressing table; returns true on first insertion
+// and the position used in pos.  Probes are bounded by the table size.
+__device__ __forceinline__ bool table_insert(uint32_t* t, uint32_t cap, uint32_t shift, uint32_t id, uint32_t& pos,
+                                             uint32_t* err) {
+    uint32_t h = (id * 0x9E3779B1u) >> shift;
+    for (uint32_t probe = 0; probe < cap; probe++) {
+        const uint32_t old = atomicCAS(t + h, kEmpty, id);
+        if (old == kEmpty) {
+            pos = h;
+            return true;
+        }
+        if (old == id) return false;
+        h = (h + 1) & (cap - 1);
+    }
+    set_error(err, kDevWaitTimeout);  // unreachable at or below 5/8 load
+    return false;
+}
+
+__device__ __forceinline__ bool vis_first(Visited& v, uint32_t id, uint32_t& pos, uint32_t* err) {
+    if (v.level == 0) return table_insert(v.tab, v.cap, v.shift, id, pos, err);
+    if (v.level == 1) return table_insert(v.gtab, v.gcap, v.gshift, id, pos, err);
+    pos = id;
+    return visit_first(v.bits, id);
+}
+
+// Level 0 -> 1 (gtab present) or 0 -> 2 (warp-collective); nlog entries move.
+static __device__ void vis_up_from_shared(Visited& v, uint32_t lane, uint32_t* err) {
+    const uint32_t to = v.gcap ? 1u : 2u;
+    uint32_t pos0 = 0;
+    for (uint32_t t0 = 0; t0 < v.cap; t0 += 32) {
+        const uint32_t id = v.tab[t0 + lane];
+        const bool has = id != kEmpty;
+        uint32_t rec = id;
+        if (has) {
+            if (to == 1) table_insert(v.gtab, v.gcap, v.gshift, id, rec, err);
+            else atomicOr(v.bits + (id >> 5), 1u << (id & 31u));
+        }
+        const unsigned b = __ballot_sync(kAll, has);
+        if (has) {
+            const uint32_t at = pos0 + __popc(b & lane_lt_mask());
+            if (at < v.log_cap) v.vlog[at] = rec;
+        }
+        pos0 += __popc(b);
+    }
+    __syncwarp();
+    v.level = to;
+}
+
+// Level 1 -> 2 (warp-collective): positions in the log become ids.
+static __device__ void vis_up_from_global(Visited& v, uint32_t nlog, uint32_t lane) {
+    const uint32_t m = min(nlog, v.log_cap);
+    for (uint32_t i = lane; i < m; i += 32) {
+        const uint32_t pos = v.vlog[i];
+        const uint32_t id = v.gtab[pos];
+        v.gtab[pos] = kEmpty;
+        atomicOr(v.bits + (id >> 5), 1u << (id & 31u));
+        v.vlog[i] = id;
+    }
+    __syncwarp();
+    v.level = 2;
+}
+
+// Makes room for `more` first visits: moves up while the level's limit would be passed.
+__device__ __forceinline__ void vis_room(Visited& v, uint32_t nlog, uint32_t more, uint32_t lane, uint32_t* err) {
+    if (v.level == 0 && nlog + more > v.cap / 8 * 5) vis_up_from_shared(v, lane, err);
+    if (v.level == 1 && nlog + more > v.gcap / 8 * 5) vis_up_from_global(v, nlog, lane);
+}
+
+// End of query: leaves level 1 / 2 storage clean (the shared table is reset by the caller).
+__device__ __forceinline__ void vis_release(Visited& v, const VisitSlot& vs, uint32_t nlog, uint32_t lane) {
+    if (v.level == 1) {
+        for (uint32_t i = lane; i < nlog; i += 32) v.gtab[v.vlog[i]] = kEmpty;
+        __syncwarp();
+    } else if (v.level == 2) {
+        visit_clear(vs, nlog);
+    }
+}
+
+// Of the m (<= 64) fresh (dist, id) entries in nd/ni, keeps those that can
+// enter the beam -- all of them while the beam is not full, else those ranking
+// before its last entry (td, tid), since any other would land at rank >= L --
+// and sorts them ascending into nd/ni[0..m').  Returns m'.  Small batches (the
+// common case after the first expansions) are ranked by counting over the kept
+// entries only; larger ones use the register bitonic network, after which the
+// kept entries are a prefix.
+__device__ __forceinline__ uint32_t sort_fresh_kept(float* nd, uint32_t* ni, uint32_t m, bool full, float td,
+                                                    uint32_t tid, uint32_t lane) {
+    if (m <= 32) {
+        const float dv = lane < m ? nd[lane] : 0.f;
+        const uint32_t iv = lane < m ? ni[lane] : kEmpty;
+        const bool keep = lane < m && (!full || nb_less(dv, iv, td, tid));
+        const unsigned km = __ballot_sync(kAll, keep);
+        uint32_t rank = 0;
+        for (unsigned r = km; r; r &= r - 1) {
+            const int s = __ffs(r) - 1;
+            const float ds = __shfl_sync(kAll, dv, s);
+            const uint32_t is = __shfl_sync(kAll, iv, s);
+            rank += nb_less(ds, is, dv, iv) ? 1u : 0u;
+        }
+        __syncwarp();
+        if (keep) {
+            nd[rank] = dv;
+            ni[rank] = iv;
+        }
+        __syncwarp();
+        return __popc(km);
+    }
+    const float inf = __int_as_float(0x7f800000);
+    float d0 = lane < m ? nd[lane] : inf;
+    uint32_t i0 = lane < m ? ni[lane] : kEmpty;
+    float d1 = lane + 32 < m ? nd[lane + 32] : inf;
+    uint32_t i1 = lane + 32 < m ? ni[lane + 32] : kEmpty;
+    warp_sort64(d0, i0, d1, i1);
+    __syncwarp();
+    nd[lane] = d0;
+    ni[lane] = i0;
+    nd[lane + 32] = d1;
+    ni[lane + 32] = i1;
+    const bool k0 = lane < m && (!full || nb_less(d0, i0, td, tid));
+    const bool k1 = lane + 32 < m && (!full || nb_less(d1, i1, td, tid));
+    const uint32_t kept = __popc(__ballot_sync(kAll, k0)) + __popc(__ballot_sync(kAll, k1));
+    __syncwarp();
+    return kept;
+}
+
+// Inserts the m (<= 64) fresh entries of nd/ni (any order; their ids are not
+// in the beam) into the sorted beam bd/bi of `size` entries and capacity cap,
+// in place: the beam becomes the cap best of the union in (dist, id) order,
+// which is what inserting them one at a time by binary search
+// (neighbor.h:61-111) leaves.  Fresh entry r lands at r + (beam entries before
+// it), beam entry j at j + (fresh entries before it); entries before cn, the
+// rank of the best kept fresh entry, do not move.  Returns cn (size when no
+// fresh entry enters).  Warp-collective; nd/ni are reordered.
+__device__ __forceinline__ uint32_t beam_insert(float* bd, uint32_t* bi, uint32_t& size, uint32_t cap, float* nd,
+                                                uint32_t* ni, uint32_t m, uint32_t lane) {
+    if (m == 0) return size;
+    const bool full = size >= cap;
+    const uint32_t mk = sort_fresh_kept(nd, ni, m, full, full ? bd[cap - 1] : 0.f, full ? bi[cap - 1] : 0u, lane);
+    if (mk == 0) return size;
+    uint32_t r0 = 0, r1 = 0;
+    if (lane < mk) r0 = lower_rank(bd, bi, size, nd[lane], ni[lane]);
+    if (lane + 32 < mk) r1 = lower_rank(bd, bi, size, nd[lane + 32], ni[lane + 32]);
+    const uint32_t cn = __shfl_sync(kAll, r0, 0);
+    const uint32_t ns = min(cap, size + mk);
+    __syncwarp();
+    for (uint32_t hi = size; hi > cn; hi = hi > cn + 32 ? hi - 32 : cn) {
+        const uint32_t j = hi - 1 - lane;
+        const bool mv = lane < hi - cn;
+        float dv = 0.f;
+        uint32_t iv = 0, pos = ns;
+        if (mv) {
+            dv = bd[j];
+            iv = bi[j];
+            pos = j + lower_rank(nd, ni, mk, dv, iv);
+        }
+        __syncwarp();
+        if (pos < ns) {
+            bd[pos] = dv;
+            bi[pos] = iv;
+        }
+        __syncwarp();
+    }
+    if (lane < mk && lane + r0 < ns) {
+        bd[lane + r0] = nd[lane];
+        bi[lane + r0] = ni[lane];
+    }
+    if (lane + 32 < mk && lane + 32 + r1 < ns) {
+        bd[lane + 32 + r1] = nd[lane + 32];
+        bi[lane + 32 + r1] = ni[lane + 32];
+    }
+    __syncwarp();
+    size = ns;
+    return cn;
+}
+
+}  // namespace anqi

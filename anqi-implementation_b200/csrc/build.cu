@@ -25,7 +25,9 @@
 #include <algorithm>
 #include <cfloat>
 #include <chrono>
+#include <cstdlib>
 
+#include "beam.cuh"
 #include "internal.h"
 #include "util.cuh"
 
@@ -71,6 +73,9 @@ struct GatherParams {
     uint32_t* pool_i;
     uint32_t pool_cap;  // power of two
     uint32_t sort_words;  // 2 * kSortSmem in select / commit mode, 0 for AKNN
+    uint32_t hash_cap, hash_shift;  // shared-memory visited table per warp (power of two, 0 = none)
+    uint32_t* gtab;                 // per-slot L2-resident visited tables (all kEmpty between rows)
+    uint32_t gcap, gshift;          // entries per slot (power of two, 0 = none)
     uint32_t* next_row;
     unsigned long long* pool_total;
     uint32_t* err;
@@ -156,30 +161,66 @@ __device__ void sort_pool(float* d, uint32_t* id, uint32_t m, float* sm_d, uint3
 
 extern __shared__ __align__(16) unsigned char g_build_smem[];
 
+__host__ __device__ __forceinline__ size_t gather_smem_words(uint32_t ef, uint32_t topk_cap, uint32_t sort_words,
+                                                             uint32_t hash_cap) {
+    return 2 * (size_t)ef + 2 * (size_t)topk_cap + (topk_cap ? 128 : 0) + 128 + 64 + sort_words + hash_cap;
+}
+
+// Visits one chunk of up to 64 list ids (slots lane and lane + 32): ids seen
+// for the first time go to ni (with their seed distances v0/v1 in nd when
+// `vals`) in slot order and are logged.  Returns their count.
+__device__ __forceinline__ uint32_t gather_visit(const GatherParams& p, Visited& vis, uint32_t& nlog, uint32_t id0,
+                                                 uint32_t id1, float v0, float v1, bool vals, uint32_t* ni, float* nd,
+                                                 uint32_t lane) {
+    vis_room(vis, nlog, 64, lane, p.err);
+    uint32_t r0 = 0, r1 = 0;
+    const bool f0 = id0 < p.n && vis_first(vis, id0, r0, p.err);
+    const bool f1 = id1 < p.n && vis_first(vis, id1, r1, p.err);
+    const unsigned b0 = __ballot_sync(kAll, f0), b1 = __ballot_sync(kAll, f1);
+    const uint32_t cnt0 = __popc(b0), lt = lane_lt_mask();
+    const uint32_t q0 = __popc(b0 & lt), q1 = cnt0 + __popc(b1 & lt);
+    const bool logs = vis.level != 0;
+    if (f0) {
+        ni[q0] = id0;
+        if (vals) nd[q0] = v0;
+        if (logs && nlog + q0 < p.log_cap) vis.vlog[nlog + q0] = r0;
+    }
+    if (f1) {
+        ni[q1] = id1;
+        if (vals) nd[q1] = v1;
+        if (logs && nlog + q1 < p.log_cap) vis.vlog[nlog + q1] = r1;
+    }
+    const uint32_t m = cnt0 + __popc(b1);
+    nlog += m;
+    __syncwarp();
+    return m;
+}
+
 __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
     const uint32_t topk_cap = (p.mode == kModeAknn && p.ef < p.out_k + 1) ? p.out_k + 1 : 0;
-    const size_t per_warp = (size_t)(4 * p.ef + 4 * topk_cap + 128 + 64 + p.sort_words) * 4;
+    const size_t per_warp = gather_smem_words(p.ef, topk_cap, p.sort_words, p.hash_cap) * 4;
     unsigned char* my = g_build_smem + wib * per_warp;
-    float* bdA = reinterpret_cast<float*>(my);
-    uint32_t* biA = reinterpret_cast<uint32_t*>(bdA + p.ef);
-    float* bdB = reinterpret_cast<float*>(biA + p.ef);
-    uint32_t* biB = reinterpret_cast<uint32_t*>(bdB + p.ef);
-    float* tdA = reinterpret_cast<float*>(biB + p.ef);
-    uint32_t* tiA = reinterpret_cast<uint32_t*>(tdA + topk_cap);
-    float* tdB = reinterpret_cast<float*>(tiA + topk_cap);
-    uint32_t* tiB = reinterpret_cast<uint32_t*>(tdB + topk_cap);
-    float* nd = reinterpret_cast<float*>(tiB + topk_cap);
+    float* bd = reinterpret_cast<float*>(my);  // the beam (queue cap ef), sorted, expanded flag in the id's top bit
+    uint32_t* bi = reinterpret_cast<uint32_t*>(bd + p.ef);
+    float* td = reinterpret_cast<float*>(bi + p.ef);  // best out_k + 1 of the pool when ef is smaller
+    uint32_t* ti = reinterpret_cast<uint32_t*>(td + topk_cap);
+    float* nd = reinterpret_cast<float*>(ti + topk_cap);
     uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 64);
-    uint32_t* sel = ni + 64;
+    float* nd2 = reinterpret_cast<float*>(ni + 64);  // a copy of the batch for the top-K list
+    uint32_t* ni2 = reinterpret_cast<uint32_t*>(nd2 + (topk_cap ? 64 : 0));
+    uint32_t* sel = ni2 + (topk_cap ? 64 : 0);
     float* sm_d = reinterpret_cast<float*>(sel + 64);
-    uint32_t* sm_i = reinterpret_cast<uint32_t*>(sm_d + kSortSmem);
+    uint32_t* sm_i = reinterpret_cast<uint32_t*>(sm_d + p.sort_words / 2);
+    uint32_t* tab = sm_i + p.sort_words / 2;
     uint32_t* bits = p.vis_bits + (size_t)slot * p.vis_words;
     uint32_t* vlog = p.vis_log + (size_t)slot * p.log_cap;
     float* pd = p.pool_d + (size_t)slot * p.pool_cap;
     uint32_t* pi = p.pool_i + (size_t)slot * p.pool_cap;
     VisitSlot vs{bits, vlog, p.log_cap, p.vis_words};
+    for (uint32_t t = lane; t < p.hash_cap; t += 32) tab[t] = kEmpty;
+    __syncwarp();
 
     for (;;) {
         uint32_t row = 0;
@@ -226,49 +267,13 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
         }
 
         // ---- gather_candidates, index.h:1491-1525
-        float* bd = bdA;
-        uint32_t* bi = biA;
-        float* od = bdB;
-        uint32_t* oi = biB;
-        float* td = tdA;
-        uint32_t* ti = tiA;
-        float* tod = tdB;
-        uint32_t* toi = tiB;
+        Visited vis{tab,  p.hash_cap, p.hash_shift, p.gtab ? p.gtab + (size_t)slot * p.gcap : nullptr,
+                    p.gcap, p.gshift, bits, vlog, p.log_cap, p.hash_cap ? 0u : (p.gcap ? 1u : 2u)};
         uint32_t size = 0, tsize = 0, nlog = 0;
+        uint32_t lo = 0;  // beam entries before lo are expanded
         uint64_t npool = 0;
-        // seeds: the row's own list with its stored distances
-        for (uint32_t c0 = 0; c0 < p.K; c0 += 64) {
-            const uint32_t m0 = min(64u, p.K - c0);
-            uint32_t id0 = kEmpty, id1 = kEmpty;
-            bool f0 = false, f1 = false;
-            float v0 = 0.f, v1 = 0.f;
-            if (lane < m0) {
-                id0 = p.g_ids[i * p.K + c0 + lane];
-                v0 = p.g_vals[i * p.K + c0 + lane];
-                f0 = id0 < p.n && visit_first(bits, id0);
-            }
-            if (lane + 32 < m0) {
-                id1 = p.g_ids[i * p.K + c0 + lane + 32];
-                v1 = p.g_vals[i * p.K + c0 + lane + 32];
-                f1 = id1 < p.n && visit_first(bits, id1);
-            }
-            const unsigned b0 = __ballot_sync(kAll, f0), b1 = __ballot_sync(kAll, f1);
-            const uint32_t cnt0 = __popc(b0), lt = lane_lt_mask();
-            const uint32_t q0 = __popc(b0 & lt), q1 = cnt0 + __popc(b1 & lt);
-            if (f0) {
-                ni[q0] = id0;
-                nd[q0] = v0;
-                if (nlog + q0 < p.log_cap) vlog[nlog + q0] = id0;
-            }
-            if (f1) {
-                ni[q1] = id1;
-                nd[q1] = v1;
-                if (nlog + q1 < p.log_cap) vlog[nlog + q1] = id1;
-            }
-            const uint32_t m = cnt0 + __popc(b1);
-            nlog += m;
-            __syncwarp();
-            if (m == 0) continue;
+        // one visited batch: pool (select mode), beam and top-K list
+        auto take = [&](uint32_t m) {
             if (p.mode == kModeSelect) {
                 for (uint32_t t = lane; t < m; t += 32)
                     if (npool + t < p.pool_cap) {
@@ -277,18 +282,36 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
                     }
             }
             npool += m;
-            warp_sort_batch64(nd, ni, m);
-            size = warp_merge(bd, bi, size, nd, ni, m, p.ef, od, oi, false);
-            { float* t1 = bd; bd = od; od = t1; uint32_t* t2 = bi; bi = oi; oi = t2; }
             if (topk_cap) {
-                tsize = warp_merge(td, ti, tsize, nd, ni, m, topk_cap, tod, toi, false);
-                float* t1 = td; td = tod; tod = t1; uint32_t* t2 = ti; ti = toi; toi = t2;
+                for (uint32_t t = lane; t < m; t += 32) {
+                    nd2[t] = nd[t];
+                    ni2[t] = ni[t];
+                }
+                __syncwarp();
+                beam_insert(td, ti, tsize, topk_cap, nd2, ni2, m, lane);
             }
+            lo = min(lo, beam_insert(bd, bi, size, p.ef, nd, ni, m, lane));
+        };
+        // seeds: the row's own list with its stored distances
+        for (uint32_t c0 = 0; c0 < p.K; c0 += 64) {
+            const uint32_t m0 = min(64u, p.K - c0);
+            uint32_t id0 = kEmpty, id1 = kEmpty;
+            float v0 = 0.f, v1 = 0.f;
+            if (lane < m0) {
+                id0 = p.g_ids[i * p.K + c0 + lane];
+                v0 = p.g_vals[i * p.K + c0 + lane];
+            }
+            if (lane + 32 < m0) {
+                id1 = p.g_ids[i * p.K + c0 + lane + 32];
+                v1 = p.g_vals[i * p.K + c0 + lane + 32];
+            }
+            const uint32_t m = gather_visit(p, vis, nlog, id0, id1, v0, v1, true, ni, nd, lane);
+            if (m) take(m);
         }
-        // expansions
+        // expansions: the closest unexpanded entry, its forward then reverse list
         for (;;) {
             uint32_t cur = size;
-            for (uint32_t s0 = 0; s0 < size; s0 += 32) {
+            for (uint32_t s0 = lo; s0 < size; s0 += 32) {
                 const uint32_t idx = s0 + lane;
                 const bool un = idx < size && !(bi[idx] & kExpanded);
                 const unsigned b = __ballot_sync(kAll, un);
@@ -302,47 +325,18 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
             __syncwarp();
             if (lane == 0) bi[cur] = node | kExpanded;
             __syncwarp();
+            lo = cur + 1;
             const uint64_t r0 = p.rev_off[node], r1 = p.rev_off[node + 1];
             const uint32_t tot = p.K + (uint32_t)(r1 - r0);
             for (uint32_t c0 = 0; c0 < tot; c0 += 64) {
                 uint32_t id0 = kEmpty, id1 = kEmpty;
-                bool f0 = false, f1 = false;
                 const uint32_t pa = c0 + lane, pb = c0 + lane + 32;
                 if (pa < tot) id0 = pa < p.K ? p.g_ids[(uint64_t)node * p.K + pa] : p.rev_ids[r0 + (pa - p.K)];
                 if (pb < tot) id1 = pb < p.K ? p.g_ids[(uint64_t)node * p.K + pb] : p.rev_ids[r0 + (pb - p.K)];
-                if (id0 < p.n) f0 = visit_first(bits, id0);
-                if (id1 < p.n) f1 = visit_first(bits, id1);
-                const unsigned b0 = __ballot_sync(kAll, f0), b1 = __ballot_sync(kAll, f1);
-                const uint32_t cnt0 = __popc(b0), lt = lane_lt_mask();
-                const uint32_t q0 = __popc(b0 & lt), q1 = cnt0 + __popc(b1 & lt);
-                if (f0) {
-                    ni[q0] = id0;
-                    if (nlog + q0 < p.log_cap) vlog[nlog + q0] = id0;
-                }
-                if (f1) {
-                    ni[q1] = id1;
-                    if (nlog + q1 < p.log_cap) vlog[nlog + q1] = id1;
-                }
-                const uint32_t m = cnt0 + __popc(b1);
-                nlog += m;
-                __syncwarp();
+                const uint32_t m = gather_visit(p, vis, nlog, id0, id1, 0.f, 0.f, false, ni, nd, lane);
                 if (m == 0) continue;
                 batch_d2(p, i, ni, nd, m, gw, gt);
-                if (p.mode == kModeSelect) {
-                    for (uint32_t t = lane; t < m; t += 32)
-                        if (npool + t < p.pool_cap) {
-                            pd[npool + t] = nd[t];
-                            pi[npool + t] = ni[t];
-                        }
-                }
-                npool += m;
-                warp_sort_batch64(nd, ni, m);
-                size = warp_merge(bd, bi, size, nd, ni, m, p.ef, od, oi, false);
-                { float* t1 = bd; bd = od; od = t1; uint32_t* t2 = bi; bi = oi; oi = t2; }
-                if (topk_cap) {
-                    tsize = warp_merge(td, ti, tsize, nd, ni, m, topk_cap, tod, toi, false);
-                    float* t1 = td; td = tod; tod = t1; uint32_t* t2 = ti; ti = toi; toi = t2;
-                }
+                take(m);
             }
             if (npool >= p.cap) break;
         }
@@ -376,7 +370,9 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
             if (lane == 0) p.O_deg[i] = nsel;
         }
         __syncwarp();
-        visit_clear(vs, nlog);
+        vis_release(vis, vs, nlog, lane);
+        for (uint32_t t = lane; t < p.hash_cap; t += 32) tab[t] = kEmpty;
+        __syncwarp();
     }
 }
 
@@ -790,7 +786,22 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     const int warps_per_block = 4;
     const uint32_t topk_cap = (p.mode == kModeAknn && p.ef < p.out_k + 1) ? p.out_k + 1 : 0;
     p.sort_words = p.mode == kModeAknn ? 0 : 2 * kSortSmem;
-    const size_t per_warp = (size_t)(4 * p.ef + 4 * topk_cap + 128 + 64 + p.sort_words) * 4;
+    const uint32_t log_cap = (uint32_t)std::min<uint64_t>(p.n, 32768);
+    // visited set: a shared-memory table per warp, then an L2-resident table
+    // per slot, then the bitmap (ANQI_B200_GATHER_HASH="S,G" overrides)
+    uint32_t hash_cap = p.mode == kModeCommit ? 0 : 2048, gcap = p.mode == kModeCommit ? 0 : 8192;
+    if (const char* e = std::getenv("ANQI_B200_GATHER_HASH")) {
+        char* end = nullptr;
+        hash_cap = (uint32_t)std::strtoul(e, &end, 10);
+        gcap = (end && *end == ',') ? (uint32_t)std::strtoul(end + 1, nullptr, 10) : 0;
+    }
+    if (hash_cap & (hash_cap - 1)) hash_cap = 0;
+    if ((gcap & (gcap - 1)) || (uint64_t)gcap / 8 * 5 > log_cap) gcap = 0;  // the log must cover level 1
+    p.hash_cap = hash_cap;
+    p.hash_shift = hash_cap ? 32u - (uint32_t)__builtin_ctz(hash_cap) : 0u;
+    p.gcap = gcap;
+    p.gshift = gcap ? 32u - (uint32_t)__builtin_ctz(gcap) : 0u;
+    const size_t per_warp = gather_smem_words(p.ef, topk_cap, p.sort_words, hash_cap) * 4;
     const size_t smem = per_warp * warps_per_block;
     if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "explore range %u too large", p.ef);
     ANQI_CUDA(c, cudaFuncSetAttribute(gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -800,16 +811,18 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     uint32_t blocks = std::min<uint64_t>((uint64_t)per_sm * c->sm_count, (p.n + warps_per_block - 1) / warps_per_block);
     const uint32_t slots = blocks * warps_per_block;
     const uint32_t words = (uint32_t)((p.n + 31) / 32);
-    const uint32_t log_cap = (uint32_t)std::min<uint64_t>(p.n, 32768);
     uint64_t need = (uint64_t)p.cap + p.K + max_rev + 64;
     if (p.mode == kModeCommit) need = p.M + max_rev + 64;
     const uint32_t pool_cap = p.mode == kModeAknn ? 1u : (uint32_t)std::min<uint64_t>(1ull << 30, 1ull << (64 - __builtin_clzll(need)));
-    TmpBuf bits(c), vlog(c), pd(c), pi(c);
+    TmpBuf bits(c), vlog(c), pd(c), pi(c), gtab(c);
     int rc;
     if ((rc = ensure(c, bits, (size_t)slots * words * 4)) || (rc = ensure(c, vlog, (size_t)slots * log_cap * 4)) ||
-        (rc = ensure(c, pd, (size_t)slots * pool_cap * 4)) || (rc = ensure(c, pi, (size_t)slots * pool_cap * 4)))
+        (rc = ensure(c, pd, (size_t)slots * pool_cap * 4)) || (rc = ensure(c, pi, (size_t)slots * pool_cap * 4)) ||
+        (gcap && (rc = ensure(c, gtab, (size_t)slots * gcap * 4))))
         return rc;
     ANQI_CUDA(c, cudaMemsetAsync(bits.p, 0, (size_t)slots * words * 4, c->stream));
+    if (gcap) ANQI_CUDA(c, cudaMemsetAsync(gtab.p, 0xFF, (size_t)slots * gcap * 4, c->stream));
+    p.gtab = gcap ? gtab.as<uint32_t>() : nullptr;
     ANQI_CUDA(c, cudaMemsetAsync(c->counters.p, 0, 64, c->stream));
     p.vis_bits = bits.as<uint32_t>();
     p.vis_words = words;
