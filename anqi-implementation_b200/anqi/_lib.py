@@ -65,7 +65,8 @@ class QueryStats(C.Structure):
 
 class AknnParams(C.Structure):
     _fields_ = [("k", C.c_uint32), ("leaf", C.c_uint32), ("trees", C.c_uint32), ("ef", C.c_uint32),
-                ("ef_alpha", C.c_uint32), ("seed", C.c_uint64), ("nn_iters", C.c_uint32), ("nn_sample", C.c_uint32)]
+                ("ef_alpha", C.c_uint32), ("seed", C.c_uint64), ("nn_iters", C.c_uint32), ("nn_sample", C.c_uint32),
+                ("precision", C.c_uint32)]
 
 
 class GraphParams(C.Structure):

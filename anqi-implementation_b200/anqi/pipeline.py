@@ -65,11 +65,14 @@ class Index:
     timings: dict = field(default_factory=dict)
 
 
-def aknn_build(ctx: Context, base: np.ndarray, k=100, leaf=500, trees=64, ef=600, seed=10, nn_iters=0, nn_sample=20):
-    """build_aknn_source: returns ids (n x k) and keys = max(0, d) (build_aknn_source.cpp:125-126)."""
+def aknn_build(ctx: Context, base: np.ndarray, k=100, leaf=500, trees=64, ef=600, seed=10, nn_iters=0, nn_sample=20,
+               precision="bf16"):
+    """build_aknn_source: returns ids (n x k) and keys = max(0, d) (build_aknn_source.cpp:125-126).
+    precision "bf16": init_knn leaf distances on BF16 tensor-core tiles with FP32
+    recheck; "fp32": CUDA cores.  Both give identical output."""
     base = np.ascontiguousarray(base, np.float32)
     n, d = base.shape
-    p = AknnParams(k, leaf, trees, ef, 8, seed, nn_iters, nn_sample)
+    p = AknnParams(k, leaf, trees, ef, 8, seed, nn_iters, nn_sample, {"fp32": 0, "bf16": 1}[precision])
     ids = np.empty((n, k), np.uint32)
     dist = np.empty((n, k), np.float32)
     st = BuildStats()

@@ -61,6 +61,9 @@ static int run(int argc, char** argv) {
     p.seed = seed;
     p.nn_iters = (uint32_t)std::max(0, std::atoi(env_or("ANQI_NNITERS", "0").c_str()));
     p.nn_sample = (uint32_t)std::min(std::max(0, std::atoi(env_or("ANQI_NNSAMPLE", "20").c_str())), 120);
+    // init_knn distances: BF16 tensor-core tiles with FP32 recheck (default) or
+    // FP32 CUDA cores; the lists are identical either way
+    p.precision = env_or("ANQI_B200_PRECISION", "bf16") == "fp32" ? 0u : 1u;
     std::vector<uint32_t> ids(n * k);
     std::vector<float> dists(n * k);
     anqi_build_stats st{};

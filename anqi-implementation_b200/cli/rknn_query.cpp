@@ -608,6 +608,7 @@ static int run(int argc, char** argv) {
             ap.seed = 10;
             ap.nn_iters = (uint32_t)std::max(0, std::atoi(env_or("ANQI_NNITERS", "0").c_str()));
             ap.nn_sample = (uint32_t)std::min(std::max(0, std::atoi(env_or("ANQI_NNSAMPLE", "20").c_str())), 120);
+            ap.precision = env_or("ANQI_B200_PRECISION", "bf16") == "fp32" ? 0u : 1u;
             warm.resize(n * width);
             std::vector<float> wd(n * width);
             dev().check(anqi_aknn_build(dev().get(), base.x.data(), n, (uint32_t)d, &ap, warm.data(), wd.data(), nullptr),

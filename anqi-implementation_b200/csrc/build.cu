@@ -77,6 +77,7 @@ struct GatherParams {
     uint32_t* gtab;                 // per-slot L2-resident visited tables (all kEmpty between rows)
     uint32_t gcap, gshift;          // entries per slot (power of two, 0 = none)
     uint32_t* next_row;
+    const uint32_t* row_order;  // work item -> row (rows of one RP-tree leaf together), or null for identity
     unsigned long long* pool_total;
     uint32_t* err;
 };
@@ -163,7 +164,7 @@ extern __shared__ __align__(16) unsigned char g_build_smem[];
 
 __host__ __device__ __forceinline__ size_t gather_smem_words(uint32_t ef, uint32_t topk_cap, uint32_t sort_words,
                                                              uint32_t hash_cap) {
-    return 2 * (size_t)ef + 2 * (size_t)topk_cap + (topk_cap ? 128 : 0) + 128 + 64 + sort_words + hash_cap;
+    return 2 * (size_t)ef + 2 * (size_t)topk_cap + (topk_cap ? 128 : 0) + 128 + 64 + sort_words + hash_cap + 256;
 }
 
 // Visits one chunk of up to 64 list ids (slots lane and lane + 32): ids seen
@@ -214,6 +215,7 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
     float* sm_d = reinterpret_cast<float*>(sel + 64);
     uint32_t* sm_i = reinterpret_cast<uint32_t*>(sm_d + p.sort_words / 2);
     uint32_t* tab = sm_i + p.sort_words / 2;
+    uint32_t* lst = tab + p.hash_cap;  // 256 list ids of the expansion being visited
     uint32_t* bits = p.vis_bits + (size_t)slot * p.vis_words;
     uint32_t* vlog = p.vis_log + (size_t)slot * p.log_cap;
     float* pd = p.pool_d + (size_t)slot * p.pool_cap;
@@ -227,7 +229,11 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
         if (lane == 0) row = atomicAdd(p.next_row, 1u);
         row = __shfl_sync(kAll, row, 0);
         if (row >= p.n) break;
-        const uint64_t i = row;
+        const uint64_t i = p.row_order ? p.row_order[row] : row;
+        if (i >= p.n) {
+            if (lane == 0) set_error(p.err, kDevBadId);
+            continue;
+        }
 
         if (p.mode == kModeCommit) {
             // cand = O_i + R_i with fresh distances (index.h:921-929)
@@ -328,15 +334,27 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
             lo = cur + 1;
             const uint64_t r0 = p.rev_off[node], r1 = p.rev_off[node + 1];
             const uint32_t tot = p.K + (uint32_t)(r1 - r0);
-            for (uint32_t c0 = 0; c0 < tot; c0 += 64) {
-                uint32_t id0 = kEmpty, id1 = kEmpty;
-                const uint32_t pa = c0 + lane, pb = c0 + lane + 32;
-                if (pa < tot) id0 = pa < p.K ? p.g_ids[(uint64_t)node * p.K + pa] : p.rev_ids[r0 + (pa - p.K)];
-                if (pb < tot) id1 = pb < p.K ? p.g_ids[(uint64_t)node * p.K + pb] : p.rev_ids[r0 + (pb - p.K)];
-                const uint32_t m = gather_visit(p, vis, nlog, id0, id1, 0.f, 0.f, false, ni, nd, lane);
-                if (m == 0) continue;
-                batch_d2(p, i, ni, nd, m, gw, gt);
-                take(m);
+            // list slots in chunks of 64 (slot c0 + lane, c0 + lane + 32); the
+            // ids of four chunks are loaded together, one memory round trip
+            for (uint32_t c0 = 0; c0 < tot; c0 += 256) {
+                uint32_t ids[8];
+#pragma unroll
+                for (uint32_t u = 0; u < 8; u++) {
+                    const uint32_t pa = c0 + lane + 32 * u;
+                    ids[u] = pa < tot ? (pa < p.K ? p.g_ids[(uint64_t)node * p.K + pa] : p.rev_ids[r0 + (pa - p.K)])
+                                      : kEmpty;
+                }
+#pragma unroll
+                for (uint32_t u = 0; u < 8; u++) lst[32 * u + lane] = ids[u];
+                __syncwarp();
+                for (uint32_t u = 0; u < 8 && c0 + 32 * u < tot; u += 2) {
+                    const uint32_t m =
+                        gather_visit(p, vis, nlog, lst[32 * u + lane], lst[32 * u + 32 + lane], 0.f, 0.f, false, ni, nd, lane);
+                    if (m == 0) continue;
+                    batch_d2(p, i, ni, nd, m, gw, gt);
+                    take(m);
+                }
+                __syncwarp();
             }
             if (npool >= p.cap) break;
         }
@@ -556,11 +574,6 @@ __global__ void fill_reverse_kernel(const uint32_t* __restrict__ ids, uint64_t n
 
 // ------------------------------------------------------------ init_knn
 
-struct LeafRef {
-    uint64_t off;
-    uint32_t cnt, pad;
-};
-
 constexpr uint32_t kLeafRows = 16;
 
 // CTA (leaf, row block): K smallest unique leaf-mates by (dist, id) merged into
@@ -678,6 +691,105 @@ __global__ void __launch_bounds__(256) leaf_topk_kernel(const float* __restrict_
         ki[row * K + k] = li[(h * kLeafRows + r) * K + k];
     }
     for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) ksz[mem[rb + r]] = rsz[r];
+}
+
+// Merges one tree's tensor-core init_knn candidates (tc_leaf_candidates) into
+// every row's list: flagged keys are recomputed in FP32 in the AVX lane order
+// (the leaf_topk_kernel arithmetic), candidates that cannot enter are dropped,
+// the rest sorted and merged with duplicates of list entries removed.  The
+// list stays the K smallest unique (key, id) of all candidates seen, whatever
+// their order.  Resets cnt.  One warp per row.
+__global__ void __launch_bounds__(128) leaf_merge_kernel(const float* __restrict__ x, const float* __restrict__ norms,
+                                                         uint64_t n, uint32_t stride, uint32_t dim,
+                                                         uint32_t* __restrict__ cnt, uint32_t cap,
+                                                         const uint32_t* __restrict__ cid,
+                                                         const float* __restrict__ ckey, uint32_t K,
+                                                         float* __restrict__ kd, uint32_t* __restrict__ ki,
+                                                         uint32_t* __restrict__ ksz, uint32_t* __restrict__ err) {
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
+    float* ld = reinterpret_cast<float*>(g_build_smem) + (size_t)wib * (4 * K + 128);
+    uint32_t* li = reinterpret_cast<uint32_t*>(ld + 2 * K);
+    float* wd = reinterpret_cast<float*>(li + 2 * K);
+    uint32_t* wi = reinterpret_cast<uint32_t*>(wd + 64);
+    const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t row = w0; row < n; row += nw) {
+        uint32_t m = cnt[row];
+        if (m == 0) continue;
+        if (m > cap) {
+            if (lane == 0) set_error(err, kDevPoolOverflow);
+            m = cap;
+        }
+        uint32_t size = ksz[row];
+        for (uint32_t t = lane; t < size; t += 32) {
+            ld[t] = kd[row * K + t];
+            li[t] = ki[row * K + t];
+        }
+        uint32_t h = 0;  // which half holds the list
+        __syncwarp();
+        const float nr = norms[row];
+        const float* xi = x + row * stride;
+        for (uint32_t c0 = 0; c0 < m; c0 += 64) {
+            const uint32_t bm = min(64u, m - c0);
+            bool flag = false;
+            for (uint32_t t = lane; t < bm; t += 32) {
+                const uint32_t id = cid[row * cap + c0 + t];
+                wi[t] = id & ~kRecheck;
+                wd[t] = ckey[row * cap + c0 + t];
+                flag |= (id & kRecheck) != 0;
+            }
+            __syncwarp();
+            if (__any_sync(kAll, flag)) {
+                for (uint32_t r0 = 0; r0 < bm; r0 += 8) {
+                    const uint32_t idx = r0 + gw;
+                    const bool ok = idx < bm;
+                    const uint32_t j = wi[ok ? idx : r0];
+                    const bool re = ok && (cid[row * cap + c0 + idx] & kRecheck);
+                    if (__any_sync(kAll, re)) {
+                        const float ip = group_ip(xi, x + (uint64_t)j * stride, dim, gt, kAll);
+                        if (re && gt == 0) wd[idx] = norm_d2(nr, norms[j], ip);
+                    }
+                }
+                __syncwarp();
+            }
+            float* cd = ld + h * K;
+            uint32_t* ci = li + h * K;
+            uint32_t kept = 0;
+            for (uint32_t s0 = 0; s0 < bm; s0 += 32) {
+                const uint32_t s1 = s0 + lane;
+                bool keep = false;
+                float dv = 0;
+                uint32_t iv = 0;
+                if (s1 < bm) {
+                    dv = wd[s1];
+                    iv = wi[s1];
+                    keep = iv != (uint32_t)row && iv < n && (size < K || nb_less(dv, iv, cd[K - 1], ci[K - 1]));
+                }
+                const unsigned b = __ballot_sync(kAll, keep);
+                __syncwarp();
+                if (keep) {
+                    const uint32_t w = kept + __popc(b & lane_lt_mask());
+                    wd[w] = dv;
+                    wi[w] = iv;
+                }
+                kept += __popc(b);
+                __syncwarp();
+            }
+            if (kept == 0) continue;
+            warp_sort_batch64(wd, wi, kept);
+            size = warp_merge(cd, ci, size, wd, wi, kept, K, ld + (1 - h) * K, li + (1 - h) * K, true);
+            h ^= 1u;
+        }
+        for (uint32_t t = lane; t < size; t += 32) {
+            kd[row * K + t] = ld[h * K + t];
+            ki[row * K + t] = li[h * K + t];
+        }
+        if (lane == 0) {
+            ksz[row] = size;
+            cnt[row] = 0;
+        }
+        __syncwarp();
+    }
 }
 
 __global__ void init_lists_kernel(float* kd, uint32_t* ki, uint32_t* ksz, uint64_t n, uint32_t K) {
@@ -918,7 +1030,8 @@ static int run_warm_start(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n
 
 static int run_select_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
                              const DevBuf& hid, const DevBuf& hval, uint32_t K, uint32_t M, uint32_t ef, uint32_t cap,
-                             float alpha, DevBuf& O, DevBuf& Odeg, DevBuf* links, DevBuf* deg, uint64_t* pool_total) {
+                             float alpha, DevBuf& O, DevBuf& Odeg, DevBuf* links, DevBuf* deg, uint64_t* pool_total,
+                             const uint32_t* row_order = nullptr) {
     TmpBuf roff(c), rev(c);
     int rc = build_reverse(c, hid.as<uint32_t>(), n, K, roff, rev);
     if (rc) return rc;
@@ -937,6 +1050,7 @@ static int run_select_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_
     p.alpha = alpha;
     p.O = O.as<uint32_t>();
     p.O_deg = Odeg.as<uint32_t>();
+    p.row_order = row_order;
     if ((rc = run_gather(c, p, mr, pool_total))) return rc;
     if (!links) return ANQI_OK;
     TmpBuf roff2(c), rev2(c);
@@ -955,6 +1069,7 @@ static int run_select_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_
     q.rev_ids = rev2.as<uint32_t>();
     q.links = links->as<uint32_t>();
     q.deg = deg->as<uint32_t>();
+    q.row_order = row_order;
     return run_gather(c, q, mr2, nullptr);
 }
 
@@ -1116,6 +1231,14 @@ int anqi_graph_build(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, cons
     cudaMemcpy(c->t_perm.data(), f.perm.p, n * 4, cudaMemcpyDeviceToHost);
     for (uint32_t v = 0; v < c->t_nodes; v++)
         if (c->t_left[v] == kEmpty) std::memset(c->t_hyper.data() + (size_t)v * dim, 0, dim * 4);
+    // the entry tree's leaf order groups nearby rows: the gathers run them together
+    TmpBuf order(c);
+    if ((rc = ensure(c, order, n * 4))) {
+        release(c, f.perm);
+        release(c, f.hyper);
+        return rc;
+    }
+    ANQI_CUDA(c, cudaMemcpyAsync(order.p, f.perm.p, n * 4, cudaMemcpyDeviceToDevice, c->stream));
     release(c, f.perm);
     release(c, f.hyper);
     const double forest_ms = ms_since(t);
@@ -1132,8 +1255,10 @@ int anqi_graph_build(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, cons
     t = Clock::now();
     uint64_t pool_total = 0;
     const uint32_t cap = std::max<uint32_t>(gp->degree, gp->ef_alpha * gp->explore);
+    const char* ord_env = std::getenv("ANQI_B200_ORDER");
     if ((rc = run_select_commit(c, dx, dn, n, xs, dim, hid, hv, gp->nn_k, gp->degree, gp->explore, cap, gp->alpha, dO,
-                                dOd, &dl, &dd, &pool_total)))
+                                dOd, &dl, &dd, &pool_total,
+                                ord_env && ord_env[0] == '0' ? nullptr : order.as<uint32_t>())))
         return rc;
     const double gather_ms = ms_since(t);
     if ((rc = d2h(c, links, dl, n * gp->degree * 4ull)) || (rc = d2h(c, deg, dd, n * 4)) || (rc = sync(c))) return rc;
@@ -1266,15 +1391,55 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
     t = Clock::now();
     if (!rc) {
         // init_knn, one tree at a time (index.h:1433-1449)
-        for (uint32_t tr = 0; tr < ap->trees && !rc; tr++) {
-            std::vector<LeafRef> leaves;
+        std::vector<std::vector<LeafRef>> tree_leaves(ap->trees);
+        uint32_t maxcnt = 0;
+        for (uint32_t tr = 0; tr < ap->trees; tr++)
             for (uint32_t v = 0; v < f.n_nodes[tr]; v++) {
                 const size_t g = (size_t)tr * cap_nodes + v;
-                if (f.left[g] == kEmpty && f.leaf_cnt[g] > 1) leaves.push_back({(uint64_t)tr * n + f.leaf_off[g], f.leaf_cnt[g], 0});
+                if (f.left[g] == kEmpty && f.leaf_cnt[g] > 1) {
+                    tree_leaves[tr].push_back({(uint64_t)tr * n + f.leaf_off[g], f.leaf_cnt[g], 0});
+                    maxcnt = std::max(maxcnt, f.leaf_cnt[g]);
+                }
             }
-            rc = run_leaf_topk(c, dx, dn, n, xs, d, f.perm.as<uint32_t>(), leaves, K, kd, ki, ksz);
+        if (ap->precision == 1) {
+            // BF16 tensor-core leaf tiles: candidates per tree, then the merge
+            TcPrep tp;
+            TmpBuf ccnt(c), cid(c), ckey(c);
+            const uint32_t cap = round_up(std::max(maxcnt, 2u), 32u);
+            if (!(rc = tc_prep(c, dx.as<float>(), n, xs, d, tp)) && !(rc = ensure(c, ccnt, n * 4)) &&
+                !(rc = ensure(c, cid, n * (size_t)cap * 4)) && !(rc = ensure(c, ckey, n * (size_t)cap * 4))) {
+                auto cu = [&](cudaError_t e, const char* what) { return e == cudaSuccess ? ANQI_OK : cuda_check(c, e, what); };
+                rc = cu(cudaMemsetAsync(ccnt.p, 0, n * 4, c->stream), "cudaMemsetAsync");
+                const int wpb = 4;
+                const size_t msmem = (size_t)(4 * K + 128) * 4 * wpb;
+                if (!rc && msmem > 48 * 1024)
+                    rc = cu(cudaFuncSetAttribute(leaf_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem),
+                            "cudaFuncSetAttribute");
+                for (uint32_t tr = 0; tr < ap->trees && !rc; tr++) {
+                    rc = tc_leaf_candidates(c, tp, dx.as<float>(), dn.as<float>(), n, xs, d, f.perm.as<uint32_t>(),
+                                            tree_leaves[tr], kd.as<float>(), ksz.as<uint32_t>(), K,
+                                            ccnt.as<uint32_t>(), cap, cid.as<uint32_t>(), ckey.as<float>());
+                    if (rc) break;
+                    leaf_merge_kernel<<<c->sm_count * 8, 32 * wpb, msmem, c->stream>>>(
+                        dx.as<float>(), dn.as<float>(), n, xs, d, ccnt.as<uint32_t>(), cap, cid.as<uint32_t>(),
+                        ckey.as<float>(), K, kd.as<float>(), ki.as<uint32_t>(), ksz.as<uint32_t>(),
+                        c->err.as<uint32_t>());
+                    rc = cu(cudaGetLastError(), "leaf_merge_kernel");
+                }
+                if (!rc) rc = check_device_error(c, "init_knn merge");
+            }
+            tc_release(c, tp);
+        } else {
+            for (uint32_t tr = 0; tr < ap->trees && !rc; tr++)
+                rc = run_leaf_topk(c, dx, dn, n, xs, d, f.perm.as<uint32_t>(), tree_leaves[tr], K, kd, ki, ksz);
         }
     }
+    // tree 0's leaf order groups the rows of one leaf: the gather runs them together
+    TmpBuf order(c);
+    if (!rc && !(rc = ensure(c, order, n * 4)))
+        rc = cudaMemcpyAsync(order.p, f.perm.p, n * 4, cudaMemcpyDeviceToDevice, c->stream) == cudaSuccess
+                 ? ANQI_OK
+                 : fail(c, ANQI_ERR_DEVICE, "row order copy failed");
     release(c, f.perm);
     release(c, f.hyper);
     if (rc) return rc;
@@ -1315,6 +1480,8 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
     p.out_k = K;
     p.out_ids = oi.as<uint32_t>();
     p.out_d = od.as<float>();
+    p.row_order = std::getenv("ANQI_B200_ORDER") && std::getenv("ANQI_B200_ORDER")[0] == '0' ? nullptr
+                                                                                            : order.as<uint32_t>();
     uint64_t pool_total = 0;
     if ((rc = run_gather(c, p, max_reverse(c, roff, n), &pool_total))) return rc;
     const double gather_ms = ms_since(t);

@@ -148,6 +148,37 @@ int build_forest(Ctx* c, const float* d_x, uint64_t n, uint32_t dim, uint32_t st
 // Exclusive scan of n u32 counts into n + 1 u64 offsets (device).
 int device_scan(Ctx* c, const uint32_t* d_in, uint64_t* d_out, uint64_t n);
 
+// One RP-tree leaf of a forest permutation: members perm[off .. off + cnt).
+struct LeafRef {
+    uint64_t off;
+    uint32_t cnt, pad;
+};
+// Row block rb (128 rows) of a leaf: one CTA of the tensor-core init_knn filter.
+struct LeafTile {
+    uint64_t off;
+    uint32_t cnt, rb;
+};
+// Candidate id flag of the tensor-core init_knn filter: the key is the bf16
+// approximation and must be recomputed in FP32.
+constexpr uint32_t kRecheck = 0x80000000u;
+
+// Rows of a device matrix in the BF16 tensor-core form (tc.cu): bf16 copy
+// padded to dp, |x| and |x - bf16(x)| rounded up, exact-integer flags.
+struct TcPrep {
+    DevBuf bf, nrm, err, xint;
+    uint32_t dp = 0;
+};
+int tc_prep(Ctx* c, const float* d_x, uint64_t n, uint32_t xs, uint32_t d, TcPrep& tp);
+void tc_release(Ctx* c, TcPrep& tp);
+// init_knn candidates of one tree's leaves on the tensor cores: for every
+// member row, the leaf-mates j != row whose key may be <= the row's current
+// K-th list key (any while the list is short), appended to out_id / out_key
+// [row * cap ..] with cnt[row] (kRecheck marks keys to recompute in FP32).
+int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs,
+                       uint32_t d, const uint32_t* d_members, const std::vector<LeafRef>& leaves,
+                       const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
+                       uint32_t* out_id, float* out_key);
+
 // Launch helpers implemented in the .cu files.
 int lrq_materialize_device(Ctx* c, const Verifier& v, uint32_t k, double scale, float* d_out);
 int compute_norms_device(Ctx* c, const float* d_x, uint64_t n, uint32_t dim, uint32_t stride, float* d_out);

@@ -175,6 +175,15 @@ struct FilterParams {
     uint32_t* out_id;         // row * cap + slot
     float* out_key;
     uint32_t* err;
+    // leaf mode (init_knn): CTA x = leaf_tiles[x]; rows members[off + 128 rb ..],
+    // columns members[off .. off + cnt); the row threshold is its current
+    // list's K-th key (+inf while the list holds fewer than list_k); keys are
+    // written unchecked, inexact ones flagged by kRecheck in the id
+    const LeafTile* leaf_tiles;
+    const uint32_t* members;
+    const float* list_kd;
+    const uint32_t* list_sz;
+    uint32_t list_k;
 };
 
 constexpr uint32_t kStages = 3;
@@ -218,6 +227,7 @@ __global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterPara
     float* col = reinterpret_cast<float*>(sb + (size_t)kStages * tile_bytes);   // kStages x 4 x 128
     uint8_t* colint = reinterpret_cast<uint8_t*>(col + kStages * 4 * kTile);    // kStages x 128
     uint64_t* rowid = reinterpret_cast<uint64_t*>(colint + kStages * kTile);    // 128 (aligned: 2*... bytes)
+    uint32_t* colid = reinterpret_cast<uint32_t*>(rowid + kTile);                // kStages x 128 (leaf mode)
     __shared__ uint64_t bar[2];
     __shared__ uint32_t tslot;
     __shared__ int s_abort;
@@ -225,13 +235,22 @@ __global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterPara
     const uint32_t r = (warp & 3u) * 32 + lane;  // this thread's tile row / TMEM lane
     const uint32_t half = warp >> 2;             // column half of each tile
 
+    const bool leaf = p.leaf_tiles != nullptr;
+    const LeafTile lt = leaf ? p.leaf_tiles[blockIdx.x] : LeafTile{0, 0, 0};
+    const uint32_t* mem = leaf ? p.members + lt.off : nullptr;
     // query rows of this tile
     if (threadIdx.x < kTile) {
-        const uint64_t t = (uint64_t)blockIdx.x * kTile + threadIdx.x;
-        rowid[threadIdx.x] = t < p.nrows ? (p.rows ? p.rows[t] : t) : ~0ull;
+        if (leaf) {
+            const uint32_t t = lt.rb * kTile + threadIdx.x;
+            rowid[threadIdx.x] = t < lt.cnt ? (uint64_t)mem[t] : ~0ull;
+        } else {
+            const uint64_t t = (uint64_t)blockIdx.x * kTile + threadIdx.x;
+            rowid[threadIdx.x] = t < p.nrows ? (p.rows ? p.rows[t] : t) : ~0ull;
+        }
     }
-    const uint64_t js = (uint64_t)blockIdx.y * p.split_len;
-    const uint64_t je = min_u64(p.n, js + p.split_len);
+    // base columns: positions [js, je) of the base rows, or of the leaf's members
+    const uint64_t js = leaf ? 0 : (uint64_t)blockIdx.y * p.split_len;
+    const uint64_t je = leaf ? (uint64_t)lt.cnt : min_u64(p.n, js + p.split_len);
     const uint32_t T = js < je ? (uint32_t)((je - js + kTile - 1) / kTile) : 0u;
     if (warp == 0) tc::tmem_alloc(&tslot, 256);
     if (threadIdx.x == 0) {
@@ -258,14 +277,16 @@ __global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterPara
         unsigned char* dst = sb + (size_t)st * tile_bytes;
         for (uint32_t i = threadIdx.x; i < kTile * chunks; i += blockDim.x) {
             const uint32_t rr = i % kTile, c = i / kTile;
-            const uint64_t row = j0 + rr;
-            const bool ok = row < je;
-            tc::cp_async16_zfill(dst + (size_t)c * kTile * 16 + rr * 16, p.xb + (ok ? row : 0) * p.dp + 8 * c,
-                                 ok ? 16u : 0u);
+            const uint64_t pos = j0 + rr;
+            const bool ok = pos < je;
+            const uint64_t row = ok ? (leaf ? (uint64_t)mem[pos] : pos) : 0;
+            tc::cp_async16_zfill(dst + (size_t)c * kTile * 16 + rr * 16, p.xb + row * p.dp + 8 * c, ok ? 16u : 0u);
         }
         if (threadIdx.x < kTile) {
-            const uint64_t j = j0 + threadIdx.x;
-            const bool ok = j < je;
+            const uint64_t pos = j0 + threadIdx.x;
+            const bool ok = pos < je;
+            const uint64_t j = ok ? (leaf ? (uint64_t)mem[pos] : pos) : 0;
+            if (leaf) colid[st * kTile + threadIdx.x] = (uint32_t)j;
             float* cs = col + (size_t)st * 4 * kTile;
             cs[threadIdx.x] = ok ? p.xn[j] : __int_as_float(0x7f800000);
             cs[kTile + threadIdx.x] = ok ? p.xnorm[j] : 0.f;
@@ -285,7 +306,10 @@ __global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterPara
     const float qnm = row_ok ? p.qnorm[my_row] : 0.f;
     const float qer = row_ok ? p.qerr[my_row] : 0.f;
     const bool qexact = row_ok && p.qint[my_row] && p.d <= 128;
-    const float thr_r = (row_ok && p.thr_row) ? p.thr_row[my_row] : 0.f;
+    float thr_r = (row_ok && p.thr_row) ? p.thr_row[my_row] : 0.f;
+    if (leaf && row_ok)
+        thr_r = p.list_sz[my_row] >= p.list_k ? p.list_kd[my_row * p.list_k + p.list_k - 1]
+                                                : __int_as_float(0x7f800000);
     const float u = 5.9604645e-8f;        // 2^-24
     const float g = 2.0f * p.dp * u;
     const float ca = 2.f * qer + 4.f * g * (qnm + qer) + 4.f * g * qnm + 8.f * u * qnm;
@@ -332,15 +356,24 @@ __global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterPara
 #pragma unroll 4
                 for (uint32_t k = 0; k < 32; k++) {
                     const uint32_t cj = c0 + k;
-                    const uint64_t j = j0 + cj;
+                    const uint64_t j = leaf ? (uint64_t)colid[st * kTile + cj] : j0 + cj;
                     const float xn = cs[cj];
                     const float approx = __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, v[k]));
-                    const float thr = p.thr_row ? thr_r : cs[3 * kTile + cj];
+                    const float thr = (p.thr_row || leaf) ? thr_r : cs[3 * kTile + cj];
                     const bool exact = qexact && colint[st * kTile + cj];
                     const float eps =
                         exact ? 0.f : fmaf(ca, cs[kTile + cj], fmaf(cb, cs[2 * kTile + cj], fmaf(cc, xn, cd)));
                     if (!(approx - eps <= thr)) continue;
                     if (p.exclude_self && j == my_row) continue;
+                    if (leaf) {
+                        // the merge recomputes flagged keys in FP32 and keeps <= its K-th
+                        const uint32_t pos = atomicAdd(p.cnt + my_row, 1u);
+                        if (pos < p.cap) {
+                            p.out_id[my_row * p.cap + pos] = (uint32_t)j | (exact ? 0u : kRecheck);
+                            p.out_key[my_row * p.cap + pos] = approx;
+                        }
+                        continue;
+                    }
                     const float key = exact ? approx : ref_key(qrow, p.x32 + j * p.xs, p.d, qn, xn);
                     if (!(key <= thr)) continue;
                     const uint32_t pos = atomicAdd(p.cnt + my_row, 1u);
@@ -448,7 +481,8 @@ __global__ void take_first_k_kernel(const uint64_t* __restrict__ off, uint64_t n
 }
 
 size_t filter_smem(uint32_t dp) {
-    return (size_t)(1 + kStages) * kTile * dp * 2 + (size_t)kStages * 4 * kTile * 4 + kStages * kTile + kTile * 8;
+    return (size_t)(1 + kStages) * kTile * dp * 2 + (size_t)kStages * 4 * kTile * 4 + kStages * kTile + kTile * 8 +
+           (size_t)kStages * kTile * 4;
 }
 
 int launch_filter(Ctx* c, FilterParams p, uint64_t nrows) {
@@ -539,6 +573,67 @@ int filter_to_csr(Ctx* c, FilterParams p, uint64_t nq, uint32_t cap, std::vector
     }
     return sort_csr_segments(c, doff.as<uint64_t>(), nq, ids.as<uint32_t>(), keys.as<float>(), maxm);
 }
+
+}  // namespace
+
+int tc_prep(Ctx* c, const float* d_x, uint64_t n, uint32_t xs, uint32_t d, TcPrep& tp) {
+    tp.dp = round_up(d, 16u);
+    if (filter_smem(tp.dp) > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "dimension %u too large for the tensor path", d);
+    return tc_prepare_rows(c, d_x, n, xs, d, tp.dp, tp.bf, tp.nrm, tp.err, tp.xint);
+}
+
+void tc_release(Ctx* c, TcPrep& tp) {
+    release(c, tp.bf);
+    release(c, tp.nrm);
+    release(c, tp.err);
+    release(c, tp.xint);
+}
+
+int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs,
+                       uint32_t d, const uint32_t* d_members, const std::vector<LeafRef>& leaves,
+                       const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
+                       uint32_t* out_id, float* out_key) {
+    std::vector<LeafTile> tiles;
+    for (const LeafRef& l : leaves) {
+        if (l.cnt > cap + 1) return fail(c, ANQI_ERR_ARGS, "leaf of %u rows exceeds the candidate capacity", l.cnt);
+        for (uint32_t rb = 0; rb * kTile < l.cnt; rb++) tiles.push_back({l.off, l.cnt, rb});
+    }
+    if (tiles.empty()) return ANQI_OK;
+    TmpBuf dt(c);
+    int rc;
+    if ((rc = h2d(c, dt, tiles.data(), tiles.size() * sizeof(LeafTile)))) return rc;
+    FilterParams p{};
+    p.qb = p.xb = tp.bf.as<__nv_bfloat16>();
+    p.q32 = p.x32 = d_x;
+    p.qn = p.xn = d_norms;
+    p.qnorm = p.xnorm = tp.nrm.as<float>();
+    p.qerr = p.xerr = tp.err.as<float>();
+    p.qint = p.xint = tp.xint.as<uint8_t>();
+    p.n = n;
+    p.xs = xs;
+    p.d = d;
+    p.dp = tp.dp;
+    p.exclude_self = 1;
+    p.cnt = cnt;
+    p.cap = cap;
+    p.out_id = out_id;
+    p.out_key = out_key;
+    p.err = c->err.as<uint32_t>();
+    p.leaf_tiles = dt.as<LeafTile>();
+    p.members = d_members;
+    p.list_kd = list_kd;
+    p.list_sz = list_sz;
+    p.list_k = K;
+    p.nrows = tiles.size() * kTile;
+    p.split_len = 0;
+    const size_t smem = filter_smem(p.dp);
+    ANQI_CUDA(c, cudaFuncSetAttribute(tc_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    tc_filter_kernel<<<(unsigned)tiles.size(), kFilterThreads, smem, c->stream>>>(p);
+    ANQI_CUDA(c, cudaGetLastError());
+    return check_device_error(c, "tensor-core init_knn filter");
+}
+
+namespace {
 
 FilterParams make_params(const TcRows& Q, const TcRows& X, uint64_t n, uint32_t xs, uint32_t d, uint32_t dp) {
     FilterParams p{};
@@ -642,6 +737,7 @@ int anqi_exact_topk_tc(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, u
         ap.ef_alpha = 8;
         ap.seed = 10;
         ap.nn_sample = 20;
+        ap.precision = 1;
         if (ap.k >= n) ap.k = (uint32_t)n - 1;
         own.resize(n * ap.k);
         std::vector<float> od(n * ap.k);

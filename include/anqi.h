@@ -99,6 +99,8 @@ typedef struct {
     uint64_t seed;       /* 10 */
     uint32_t nn_iters;   /* ANQI_NNITERS, default 0 */
     uint32_t nn_sample;  /* ANQI_NNSAMPLE, default 20 */
+    uint32_t precision;  /* init_knn leaf distances: 0 = FP32 CUDA cores, 1 = BF16 tensor-core
+                            tiles with FP32 recheck (identical output) */
 } anqi_aknn_params;
 
 typedef struct {

@@ -330,3 +330,33 @@ def test_graph_build_query_recall(ctx, sample):
             ref_rec, ref_prec = sample["ref_lines"][sel][:2]
             assert rec / ne >= ref_rec - 0.002, (k, L, rec / ne, ref_rec)
             assert prec / ne >= ref_prec - 0.002, (k, L, prec / ne, ref_prec)
+
+
+def _aknn(ctx, x, precision, K=50, leaf=300, trees=8, ef=150):
+    n, d = x.shape
+    p = AknnParams(K, leaf, trees, ef, 8, 10, 0, 20, precision)
+    ids = np.empty((n, K), np.uint32)
+    dist = np.empty((n, K), np.float32)
+    st = BuildStats()
+    ctx._check(ctx.lib.anqi_aknn_build(ctx.h, f32(x), n, d, C.byref(p), ids, dist, C.byref(st)), "aknn_build")
+    return ids, dist
+
+
+@pytest.mark.parametrize("kind", ["integer", "float", "duplicates"])
+def test_aknn_build_tensor_init_identical(ctx, kind):
+    """init_knn on BF16 tensor-core leaf tiles (exact keys on integer rows, FP32
+    recheck otherwise) gives the FP32 path's AKNN lists bit for bit; leaves of
+    up to 300 rows span several 128-row tiles."""
+    rng = np.random.default_rng(17)
+    if kind == "integer":
+        from anqi import pipeline
+        x, _ = pipeline.mixture(12000, 64, 1, centers=40, seed=5)
+    elif kind == "float":
+        x = clustered(12000, 48, 9, nc=60)
+    else:
+        x = clustered(6000, 40, 4, nc=30)
+        x = np.concatenate([x, x[:3000]])  # exact duplicate rows: ties at distance 0
+    a_ids, a_d = _aknn(ctx, x, 0)
+    b_ids, b_d = _aknn(ctx, x, 1)
+    assert np.array_equal(a_ids, b_ids)
+    assert np.array_equal(bits(a_d), bits(b_d))
