@@ -78,7 +78,7 @@ class GraphParams(C.Structure):
 class BuildStats(C.Structure):
     _fields_ = [("total_ms", C.c_double), ("forest_ms", C.c_double), ("init_ms", C.c_double),
                 ("join_ms", C.c_double), ("reverse_ms", C.c_double), ("gather_ms", C.c_double),
-                ("join_updates", C.c_uint64), ("pool_total", C.c_uint64)]
+                ("join_updates", C.c_uint64), ("pool_total", C.c_uint64), ("gather_kernel_ms", C.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

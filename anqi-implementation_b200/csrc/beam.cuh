@@ -29,27 +29,70 @@ struct Visited {
     uint32_t level;
 };
 
-// Inserts id into an open-addressing table; returns true on first insertion
-// and the position used in pos.  Probes are bounded by the table size.
+// 16-byte bucket loads (shared: the warp's own table; global: bypassing L1,
+// since the table is updated by atomics at L2) and the shared-memory CAS.
+__device__ __forceinline__ uint4 ld_bucket_shared(const uint32_t* p) {
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "r"((uint32_t)__cvta_generic_to_shared(p))
+                 : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint4 ld_bucket_global(const uint32_t* p) {
+    uint4 v;
+    asm volatile("ld.global.cg.v4.u32 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p)
+                 : "memory");
+    return v;
+}
+
+__device__ __forceinline__ uint32_t cas_shared(uint32_t* p, uint32_t cmp, uint32_t val) {
+    uint32_t old;
+    asm volatile("atom.shared.cas.b32 %0, [%1], %2, %3;\n"
+                 : "=r"(old)
+                 : "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(cmp), "r"(val)
+                 : "memory");
+    return old;
+}
+
+// Inserts id into an open-addressing table of 4-slot buckets (bucketed linear
+// probing); returns true on first insertion and the slot used in pos.  A
+// bucket's occupied slots are always a prefix and no entry is removed while
+// the table is in use, so a bucket with a free slot ends the search: a lookup
+// is one 16-byte load in the common case, and only an insertion takes an
+// atomic.  A failed CAS (another lane of the warp took the slot) reads the
+// bucket again.  cap is a power of two >= 8; iterations are bounded.
+template <bool kShared>
 __device__ __forceinline__ bool table_insert(uint32_t* t, uint32_t cap, uint32_t shift, uint32_t id, uint32_t& pos,
                                              uint32_t* err) {
-    uint32_t h = (id * 0x9E3779B1u) >> shift;
-    for (uint32_t probe = 0; probe < cap; probe++) {
-        const uint32_t old = atomicCAS(t + h, kEmpty, id);
+    const uint32_t nb = cap >> 2;
+    uint32_t b = (id * 0x9E3779B1u) >> (shift + 2);
+    for (uint32_t it = 0; it < 2 * nb + 64; it++) {
+        const uint4 v = kShared ? ld_bucket_shared(t + 4 * b) : ld_bucket_global(t + 4 * b);
+        if (v.x == id || v.y == id || v.z == id || v.w == id) return false;
+        const uint32_t e = v.x == kEmpty ? 0u : v.y == kEmpty ? 1u : v.z == kEmpty ? 2u : v.w == kEmpty ? 3u : 4u;
+        if (e == 4u) {
+            b = (b + 1) & (nb - 1);
+            continue;
+        }
+        const uint32_t slot = 4 * b + e;
+        const uint32_t old = kShared ? cas_shared(t + slot, kEmpty, id) : atomicCAS(t + slot, kEmpty, id);
         if (old == kEmpty) {
-            pos = h;
+            pos = slot;
             return true;
         }
         if (old == id) return false;
-        h = (h + 1) & (cap - 1);
     }
     set_error(err, kDevWaitTimeout);  // unreachable at or below 5/8 load
     return false;
 }
 
 __device__ __forceinline__ bool vis_first(Visited& v, uint32_t id, uint32_t& pos, uint32_t* err) {
-    if (v.level == 0) return table_insert(v.tab, v.cap, v.shift, id, pos, err);
-    if (v.level == 1) return table_insert(v.gtab, v.gcap, v.gshift, id, pos, err);
+    if (v.level == 0) return table_insert<true>(v.tab, v.cap, v.shift, id, pos, err);
+    if (v.level == 1) return table_insert<false>(v.gtab, v.gcap, v.gshift, id, pos, err);
     pos = id;
     return visit_first(v.bits, id);
 }
@@ -63,7 +106,7 @@ static __device__ void vis_up_from_shared(Visited& v, uint32_t lane, uint32_t* e
         const bool has = id != kEmpty;
         uint32_t rec = id;
         if (has) {
-            if (to == 1) table_insert(v.gtab, v.gcap, v.gshift, id, rec, err);
+            if (to == 1) table_insert<false>(v.gtab, v.gcap, v.gshift, id, rec, err);
             else atomicOr(v.bits + (id >> 5), 1u << (id & 31u));
         }
         const unsigned b = __ballot_sync(kAll, has);

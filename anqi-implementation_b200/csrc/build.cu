@@ -162,9 +162,16 @@ __device__ void sort_pool(float* d, uint32_t* id, uint32_t m, float* sm_d, uint3
 
 extern __shared__ __align__(16) unsigned char g_build_smem[];
 
+// Per-warp shared words before the visited table (a multiple of 4 words: its
+// 16-byte buckets) and in total (a multiple of 4 words, so every warp's region
+// keeps that alignment).
+__host__ __device__ __forceinline__ size_t gather_smem_pre(uint32_t ef, uint32_t topk_cap, uint32_t sort_words) {
+    return (2 * (size_t)ef + 2 * (size_t)topk_cap + (topk_cap ? 128 : 0) + 128 + 64 + sort_words + 3) & ~(size_t)3;
+}
+
 __host__ __device__ __forceinline__ size_t gather_smem_words(uint32_t ef, uint32_t topk_cap, uint32_t sort_words,
                                                              uint32_t hash_cap) {
-    return 2 * (size_t)ef + 2 * (size_t)topk_cap + (topk_cap ? 128 : 0) + 128 + 64 + sort_words + hash_cap + 256;
+    return gather_smem_pre(ef, topk_cap, sort_words) + hash_cap + 256;
 }
 
 // Visits one chunk of up to 64 list ids (slots lane and lane + 32): ids seen
@@ -214,7 +221,7 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
     uint32_t* sel = ni2 + (topk_cap ? 64 : 0);
     float* sm_d = reinterpret_cast<float*>(sel + 64);
     uint32_t* sm_i = reinterpret_cast<uint32_t*>(sm_d + p.sort_words / 2);
-    uint32_t* tab = sm_i + p.sort_words / 2;
+    uint32_t* tab = reinterpret_cast<uint32_t*>(my) + gather_smem_pre(p.ef, topk_cap, p.sort_words);
     uint32_t* lst = tab + p.hash_cap;  // 256 list ids of the expansion being visited
     uint32_t* bits = p.vis_bits + (size_t)slot * p.vis_words;
     uint32_t* vlog = p.vis_log + (size_t)slot * p.log_cap;
@@ -894,14 +901,16 @@ static uint64_t max_reverse(Ctx* c, const DevBuf& off, uint64_t n) {
 }
 
 // Runs gather_kernel over all rows.
-static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_total) {
+static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_total, double* kernel_ms = nullptr) {
     const int warps_per_block = 4;
     const uint32_t topk_cap = (p.mode == kModeAknn && p.ef < p.out_k + 1) ? p.out_k + 1 : 0;
     p.sort_words = p.mode == kModeAknn ? 0 : 2 * kSortSmem;
     const uint32_t log_cap = (uint32_t)std::min<uint64_t>(p.n, 32768);
-    // visited set: a shared-memory table per warp, then an L2-resident table
-    // per slot, then the bitmap (ANQI_B200_GATHER_HASH="S,G" overrides)
-    uint32_t hash_cap = p.mode == kModeCommit ? 0 : 2048, gcap = p.mode == kModeCommit ? 0 : 8192;
+    // visited set: an L2-resident table per slot (bucketed probing: a lookup
+    // is one 16-byte L2 load), then the bitmap; measured at 1M x 128 this beats
+    // any shared-memory table in front of it, which costs occupancy
+    // (ANQI_B200_GATHER_HASH="S,G" sets the shared and L2 table sizes)
+    uint32_t hash_cap = 0, gcap = p.mode == kModeCommit ? 0 : 4096;
     if (const char* e = std::getenv("ANQI_B200_GATHER_HASH")) {
         char* end = nullptr;
         hash_cap = (uint32_t)std::strtoul(e, &end, 10);
@@ -946,9 +955,16 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     p.next_row = c->counters.as<uint32_t>();
     p.pool_total = reinterpret_cast<unsigned long long*>(c->counters.as<uint32_t>() + 2);
     p.err = c->err.as<uint32_t>();
+    ANQI_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     gather_kernel<<<blocks, 32 * warps_per_block, smem, c->stream>>>(p);
     ANQI_CUDA(c, cudaGetLastError());
+    ANQI_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     if ((rc = check_device_error(c, "gather"))) return rc;
+    if (kernel_ms) {
+        float ms = 0;
+        ANQI_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        *kernel_ms += ms;
+    }
     if (pool_total) ANQI_CUDA(c, cudaMemcpy(pool_total, p.pool_total, 8, cudaMemcpyDeviceToHost));
     return ANQI_OK;
 }
@@ -1031,7 +1047,7 @@ static int run_warm_start(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n
 static int run_select_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
                              const DevBuf& hid, const DevBuf& hval, uint32_t K, uint32_t M, uint32_t ef, uint32_t cap,
                              float alpha, DevBuf& O, DevBuf& Odeg, DevBuf* links, DevBuf* deg, uint64_t* pool_total,
-                             const uint32_t* row_order = nullptr) {
+                             const uint32_t* row_order = nullptr, double* kernel_ms = nullptr) {
     TmpBuf roff(c), rev(c);
     int rc = build_reverse(c, hid.as<uint32_t>(), n, K, roff, rev);
     if (rc) return rc;
@@ -1051,7 +1067,7 @@ static int run_select_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_
     p.O = O.as<uint32_t>();
     p.O_deg = Odeg.as<uint32_t>();
     p.row_order = row_order;
-    if ((rc = run_gather(c, p, mr, pool_total))) return rc;
+    if ((rc = run_gather(c, p, mr, pool_total, kernel_ms))) return rc;
     if (!links) return ANQI_OK;
     TmpBuf roff2(c), rev2(c);
     if ((rc = build_reverse(c, O.as<uint32_t>(), n, M, roff2, rev2))) return rc;
@@ -1070,7 +1086,7 @@ static int run_select_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_
     q.links = links->as<uint32_t>();
     q.deg = deg->as<uint32_t>();
     q.row_order = row_order;
-    return run_gather(c, q, mr2, nullptr);
+    return run_gather(c, q, mr2, nullptr, kernel_ms);
 }
 
 // init_knn over leaves; lists kd/ki/ksz already initialised.
@@ -1254,11 +1270,12 @@ int anqi_graph_build(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, cons
     const double join_ms = ms_since(t);
     t = Clock::now();
     uint64_t pool_total = 0;
+    double gather_kernel_ms = 0;
     const uint32_t cap = std::max<uint32_t>(gp->degree, gp->ef_alpha * gp->explore);
     const char* ord_env = std::getenv("ANQI_B200_ORDER");
     if ((rc = run_select_commit(c, dx, dn, n, xs, dim, hid, hv, gp->nn_k, gp->degree, gp->explore, cap, gp->alpha, dO,
                                 dOd, &dl, &dd, &pool_total,
-                                ord_env && ord_env[0] == '0' ? nullptr : order.as<uint32_t>())))
+                                ord_env && ord_env[0] == '0' ? nullptr : order.as<uint32_t>(), &gather_kernel_ms)))
         return rc;
     const double gather_ms = ms_since(t);
     if ((rc = d2h(c, links, dl, n * gp->degree * 4ull)) || (rc = d2h(c, deg, dd, n * 4)) || (rc = sync(c))) return rc;
@@ -1268,6 +1285,7 @@ int anqi_graph_build(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, cons
         st->join_ms = join_ms;
         st->reverse_ms = 0;
         st->gather_ms = gather_ms;
+        st->gather_kernel_ms = gather_kernel_ms;
         st->total_ms = ms_since(t0);
         uint64_t tot = 0;
         for (uint64_t u : up) tot += u;
@@ -1483,7 +1501,8 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
     p.row_order = std::getenv("ANQI_B200_ORDER") && std::getenv("ANQI_B200_ORDER")[0] == '0' ? nullptr
                                                                                             : order.as<uint32_t>();
     uint64_t pool_total = 0;
-    if ((rc = run_gather(c, p, max_reverse(c, roff, n), &pool_total))) return rc;
+    double gather_kernel_ms = 0;
+    if ((rc = run_gather(c, p, max_reverse(c, roff, n), &pool_total, &gather_kernel_ms))) return rc;
     const double gather_ms = ms_since(t);
     if ((rc = d2h(c, ids, oi, n * K * 4)) || (rc = d2h(c, dists, od, n * K * 4)) || (rc = sync(c))) return rc;
     if (st) {
@@ -1492,6 +1511,7 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
         st->join_ms = join_ms;
         st->reverse_ms = reverse_ms;
         st->gather_ms = gather_ms;
+        st->gather_kernel_ms = gather_kernel_ms;
         st->total_ms = ms_since(t0);
         uint64_t tot = 0;
         for (uint64_t u : up) tot += u;

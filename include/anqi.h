@@ -104,9 +104,10 @@ typedef struct {
 } anqi_aknn_params;
 
 typedef struct {
-    double total_ms, forest_ms, init_ms, join_ms, reverse_ms, gather_ms;
+    double total_ms, forest_ms, init_ms, join_ms, reverse_ms, gather_ms;  /* host clock per stage */
     uint64_t join_updates;
     uint64_t pool_total;
+    double gather_kernel_ms;  /* device time of the gather kernel launches (CUDA events) */
 } anqi_build_stats;
 
 int anqi_aknn_build(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d,
