@@ -144,6 +144,17 @@ def build_workload(ctx, a, rank, log):
     base, query = pipeline.mixture(a.n, a.d, a.nq, seed=20260819 + rank)
     log(f"data {base.shape} + {query.shape} in {time.perf_counter() - t0:.1f}s")
     ix = pipeline.build_index(ctx, base, train_workers=os.cpu_count() or 8, log=log)
+    # the same AKNN source build with init_knn on FP32 CUDA cores (the plain
+    # path): its lists must equal the tensor-core build's
+    t0 = time.perf_counter()
+    ids32, keys32, st32 = pipeline.aknn_build(ctx, base, precision="fp32")
+    ix.timings["aknn_build_fp32_s"] = time.perf_counter() - t0
+    ix.timings["aknn_fp32_identical"] = bool(np.array_equal(ids32, ix.aknn_ids) and
+                                             np.array_equal(keys32.view(np.uint32), ix.aknn_keys.view(np.uint32)))
+    st = ix.timings["aknn_stats"]
+    ix.timings["aknn_init_ms"] = {"bf16": round(st["init_ms"], 1), "fp32": round(st32["init_ms"], 1)}
+    ix.timings["aknn_gather_kernel_ms"] = round(st["gather_kernel_ms"], 1)
+    log(f"AKNN fp32 build {ix.timings['aknn_build_fp32_s']:.2f}s identical={ix.timings['aknn_fp32_identical']}")
     ks = [int(k) for k in a.ks.split(",")]
     if a.no_gt:
         return base, query, ix, ks, None
@@ -306,6 +317,10 @@ def run_ours(a, rank, world, local):
         "counters_per_query": {"graph_dist": round(s0["n_dist"] / nb, 1), "expansions": round(X / nb, 1),
                                "candidates": round(s0["n_cand"] / nb, 1), "verified": round(s0["n_pred"] / nb, 2)},
         "build_s": {k: round(v, 3) for k, v in ix.timings.items() if isinstance(v, float)},
+        "aknn_build": {"bf16_tensor_init_s": round(ix.timings["aknn_build_s"], 3),
+                       "fp32_init_s": round(ix.timings["aknn_build_fp32_s"], 3),
+                       "identical": ix.timings["aknn_fp32_identical"], "init_ms": ix.timings["aknn_init_ms"],
+                       "gather_kernel_ms": ix.timings["aknn_gather_kernel_ms"]},
     }
     if rank == 0 and world == 1 and not a.no_cpu_baseline and gt is not None:
         tmp = Path(a.keep) if a.keep else Path(tempfile.mkdtemp(prefix="anqi_bench_"))
