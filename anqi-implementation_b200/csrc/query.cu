@@ -129,8 +129,10 @@ __device__ __forceinline__ void load_links(const SearchParams& p, uint32_t node,
 // Distances of the m fresh neighbours to the lifted query: 8 groups of 4
 // lanes, each group staging its row into shared memory (one round trip for up
 // to 8 rows) and reducing it in the reference's lane order.
+template <uint32_t kDim>
 __device__ __forceinline__ void fresh_distances(const SearchParams& p, const float* qhat, const uint32_t* ni,
                                                 float* nd, uint32_t m, uint32_t gw, uint32_t gt, float* stage) {
+    const uint32_t dim = kDim ? kDim : p.dim;
     float* row = stage + (size_t)gw * p.lstride;
     for (uint32_t r0 = 0; r0 < m; r0 += 8) {
         const uint32_t ia = r0 + gw;
@@ -138,7 +140,7 @@ __device__ __forceinline__ void fresh_distances(const SearchParams& p, const flo
         if (oka) stage_row_async(row, p.lifted + (size_t)ni[ia] * p.lstride, p.lstride, gt, 4);
         cp_async_wait_all();
         __syncwarp();
-        const float da = group_l2sqr(oka ? row : stage, qhat, p.dim, gt, kFull);
+        const float da = group_l2sqr(oka ? row : stage, qhat, dim, gt, kFull);
         if (gt == 0 && oka) nd[ia] = da;
         __syncwarp();
     }
@@ -175,6 +177,7 @@ __device__ __host__ __forceinline__ size_t search_smem_words(uint32_t L_max, uin
            hash_cap;
 }
 
+template <uint32_t kDim>
 __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -267,22 +270,26 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
             } else {
                 load_links(p, node, lane, l0, l1, dg);
             }
+            // the old beam's next unexpanded entry is the next node unless a
+            // fresh neighbour ranks before it: load its links now, a whole
+            // expansion ahead of their use
+            if (nxt < size) {
+                pre_node = bi[nxt] & kIdMask;
+                load_links(p, pre_node, lane, pl0, pl1, pdg);
+            }
             vis_room(vis, nlog, p.degree, lane, p.err);
             const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane);
             uint32_t mk = 0;
             if (m != 0) {
-                fresh_distances(p, qhat, ni, nd, m, gw, gt, stage);
+                fresh_distances<kDim>(p, qhat, ni, nd, m, gw, gt, stage);
                 append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
                 const bool full = size >= L;
                 mk = sort_fresh_kept(nd, ni, m, full, full ? bd[L - 1] : 0.f, full ? bi[L - 1] : 0u, lane);
             }
             if (mk == 0) {
-                // no fresh entry enters the beam: only the cursor moves
+                // no fresh entry enters the beam: only the cursor moves (to
+                // nxt, whose links are on their way)
                 cur = nxt;
-                if (nxt < size) {
-                    pre_node = bi[nxt] & kIdMask;
-                    load_links(p, pre_node, lane, pl0, pl1, pdg);
-                }
                 continue;
             }
             // Batch insert of the mk kept entries (sorted) into the sorted
@@ -298,8 +305,10 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
             // one if it ranks before every fresh entry, else the best fresh one
             const bool old_next = nxt < cn;
             const uint32_t nc = old_next ? nxt : cn;
-            pre_node = old_next ? (bi[nxt] & kIdMask) : ni[0];
-            load_links(p, pre_node, lane, pl0, pl1, pdg);
+            if (!old_next) {
+                pre_node = ni[0];
+                load_links(p, pre_node, lane, pl0, pl1, pdg);
+            }
             __syncwarp();
             // move beam entries [cn, size) right, highest first, so no entry is
             // overwritten before it is read
@@ -357,7 +366,7 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
             vis_room(vis, nlog, p.degree, lane, p.err);
             const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane);
             if (m == 0) continue;
-            fresh_distances(p, qhat, ni, nd, m, gw, gt, stage);
+            fresh_distances<kDim>(p, qhat, ni, nd, m, gw, gt, stage);
             append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
         }
         if (overflow && lane == 0) set_error(p.err, kDevCandOverflow);
@@ -612,6 +621,12 @@ static size_t search_smem_per_warp(const Ctx* c, uint32_t L_max, uint32_t hash_c
     return search_smem_words(L_max, c->ix.lstride, c->ix.bstride, hash_cap) * 4;
 }
 
+// The search kernel for lifted dimension dim: 130 (d = 128) has its distance
+// loops unrolled at compile time.
+static void (*search_kernel_for(uint32_t dim))(SearchParams) {
+    return dim == 130 ? rknn_search_kernel<130> : rknn_search_kernel<0>;
+}
+
 struct SearchCfg {
     uint32_t hash_cap = 0;  // shared-memory table entries per warp
     uint32_t gcap = 0;      // global (L2-resident) table entries per warp
@@ -626,9 +641,10 @@ static int search_cfg(Ctx* c, uint32_t hash_cap, uint32_t gcap, SearchCfg& cfg) 
     cfg.gcap = gcap;
     cfg.smem = search_smem_per_warp(c, b.L_max, hash_cap) * wpb;
     if (cfg.smem > 227 * 1024) return ANQI_ERR_ARGS;
-    ANQI_CUDA(c, cudaFuncSetAttribute(rknn_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+    auto kern = search_kernel_for(c->ix.dim);
+    ANQI_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
     int per_sm = 0;
-    ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rknn_search_kernel, 32 * wpb, cfg.smem));
+    ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, cfg.smem));
     if (per_sm < 1) return ANQI_ERR_ARGS;
     cfg.blocks = std::min<uint32_t>((uint32_t)per_sm * c->sm_count, (b.nq + wpb - 1) / wpb);
     return ANQI_OK;
@@ -886,9 +902,10 @@ static int launch_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, floa
     p.gcap = cfg.gcap;
     p.gshift = cfg.gcap ? 32u - (uint32_t)__builtin_ctz(cfg.gcap) : 0u;
     p.gtab = cfg.gcap ? c->vis_gtab.as<uint32_t>() : nullptr;
-    ANQI_CUDA(c, cudaFuncSetAttribute(rknn_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
+    auto kern = search_kernel_for(ix.dim);
+    ANQI_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
     ANQI_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-    rknn_search_kernel<<<cfg.blocks, 128, cfg.smem, c->stream>>>(p);
+    kern<<<cfg.blocks, 128, cfg.smem, c->stream>>>(p);
     ANQI_CUDA(c, cudaGetLastError());
     ANQI_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     ANQI_CUDA(c, cudaMemcpyAsync(fill, p.fill, 16, cudaMemcpyDeviceToHost, c->stream));
