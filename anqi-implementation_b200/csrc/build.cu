@@ -955,11 +955,19 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     p.next_row = c->counters.as<uint32_t>();
     p.pool_total = reinterpret_cast<unsigned long long*>(c->counters.as<uint32_t>() + 2);
     p.err = c->err.as<uint32_t>();
+    // the L2 tables persist in L2 for this launch (the query tables' window is
+    // set again by the next search)
+    if (gcap) {
+        set_l2_window(c, gtab.p, (size_t)slots * gcap * 4);
+        c->l2_window = false;
+    }
     ANQI_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     gather_kernel<<<blocks, 32 * warps_per_block, smem, c->stream>>>(p);
     ANQI_CUDA(c, cudaGetLastError());
     ANQI_CUDA(c, cudaEventRecord(c->ev1, c->stream));
-    if ((rc = check_device_error(c, "gather"))) return rc;
+    rc = check_device_error(c, "gather");  // synchronizes
+    if (gcap) clear_l2_window(c);
+    if (rc) return rc;
     if (kernel_ms) {
         float ms = 0;
         ANQI_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));

@@ -1,3 +1,4 @@
+#include <algorithm>
 // Context lifetime, device memory, error reporting, and small shared kernels.
 #include <cstdarg>
 #include <cstdio>
@@ -64,6 +65,42 @@ int d2h(Ctx* c, void* dst, const DevBuf& b, size_t bytes) {
 int sync(Ctx* c) {
     ANQI_CUDA(c, cudaStreamSynchronize(c->stream));
     return ANQI_OK;
+}
+
+// L2 set-aside for one hot device range accessed on the context's stream (the
+// per-warp visited tables): accesses inside the window persist in L2, others
+// are unaffected.  The set-aside is a limit of this process's CUDA context;
+// clear_l2_window (and context teardown) returns it.
+void set_l2_window(Ctx* c, const void* p, size_t bytes) {
+    int maxwin = 0, maxpers = 0;
+    cudaDeviceGetAttribute(&maxwin, cudaDevAttrMaxAccessPolicyWindowSize, c->device);
+    cudaDeviceGetAttribute(&maxpers, cudaDevAttrMaxPersistingL2CacheSize, c->device);
+    if (maxwin <= 0 || maxpers <= 0 || !p || bytes == 0) return;
+    const size_t win = std::min<size_t>(bytes, (size_t)maxwin);
+    const size_t keep = std::min<size_t>(win, (size_t)maxpers);
+    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, keep) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    cudaStreamAttrValue av{};
+    av.accessPolicyWindow.base_ptr = const_cast<void*>(p);
+    av.accessPolicyWindow.num_bytes = win;
+    av.accessPolicyWindow.hitRatio = (float)keep / (float)win;
+    av.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    av.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    if (cudaStreamSetAttribute(c->stream, cudaStreamAttributeAccessPolicyWindow, &av) != cudaSuccess) cudaGetLastError();
+}
+
+void clear_l2_window(Ctx* c) {
+    cudaStreamAttrValue av{};
+    av.accessPolicyWindow.base_ptr = nullptr;
+    av.accessPolicyWindow.num_bytes = 0;
+    av.accessPolicyWindow.hitRatio = 0.f;
+    av.accessPolicyWindow.hitProp = cudaAccessPropertyNormal;
+    av.accessPolicyWindow.missProp = cudaAccessPropertyNormal;
+    if (cudaStreamSetAttribute(c->stream, cudaStreamAttributeAccessPolicyWindow, &av) != cudaSuccess) cudaGetLastError();
+    if (cudaCtxResetPersistingL2Cache() != cudaSuccess) cudaGetLastError();
+    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0) != cudaSuccess) cudaGetLastError();
 }
 
 int check_device_error(Ctx* c, const char* stage) {
@@ -285,6 +322,7 @@ void anqi_ctx_destroy(anqi_ctx* h) {
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->l2_window) clear_l2_window(c);
     for (DevBuf* b : c->member_bufs()) release(c, *b);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);

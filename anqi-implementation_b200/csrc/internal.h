@@ -94,6 +94,7 @@ struct Ctx {
     std::unordered_map<uint64_t, uint64_t> tuned;  // value: shared entries | L2 entries << 32
     DevBuf vis_gtab;                               // per-slot L2-resident visited tables
     uint32_t gtab_slots = 0, gtab_cap = 0;
+    bool l2_window = false;                        // an L2 persisting window is set on the stream
     uint64_t device_bytes = 0;
     std::vector<DevBuf*> member_bufs() {
         return {&ix.base, &ix.lifted, &ix.onorm, &ix.deg, &ix.links, &ix.tleft, &ix.tright, &ix.toffset,
@@ -178,6 +179,10 @@ int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* 
                        uint32_t d, const uint32_t* d_members, const std::vector<LeafRef>& leaves,
                        const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
                        uint32_t* out_id, float* out_key);
+
+// L2 persisting window over [p, p + bytes) for kernels on the context's stream.
+void set_l2_window(Ctx* c, const void* p, size_t bytes);
+void clear_l2_window(Ctx* c);
 
 // Launch helpers implemented in the .cu files.
 int lrq_materialize_device(Ctx* c, const Verifier& v, uint32_t k, double scale, float* d_out);

@@ -938,8 +938,8 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
         f_hc = (uint32_t)std::strtoul(forced, &end, 10);
         if (end && *end == ',') f_gc = (uint32_t)std::strtoul(end + 1, nullptr, 10);
     }
-    static const uint32_t kCandidates[][2] = {{0, 0},    {1024, 0},    {2048, 0},
-                                                  {4096, 0}, {0, 4096},    {512, 4096}, {1024, 4096}};
+    static const uint32_t kCandidates[][2] = {{0, 0},       {1024, 0},    {2048, 0},   {4096, 0}, {0, 2048},
+                                                  {0, 4096},    {512, 4096},  {1024, 4096}};
     std::vector<SearchCfg> cfgs;
     for (const auto& cand : kCandidates) {
         if (forced && (cand[0] != f_hc || cand[1] != f_gc)) continue;
@@ -962,6 +962,12 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
         ANQI_CUDA(c, cudaMemsetAsync(c->vis_gtab.p, 0xFF, bytes, c->stream));
         c->gtab_slots = gslots;
         c->gtab_cap = gcap_max;
+        c->l2_window = false;  // the tables moved: the window is set again below
+    }
+    // the visited tables stay in L2 while the search streams rows past them
+    if (gcap_max && !c->l2_window) {
+        set_l2_window(c, c->vis_gtab.p, (size_t)c->gtab_slots * c->gtab_cap * 4);
+        c->l2_window = true;
     }
     // per-slot scratch (bitmap, log, candidate list) for the largest configuration
     const uint32_t words = (uint32_t)((ix.n + 31) / 32);
