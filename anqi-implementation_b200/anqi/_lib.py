@@ -123,6 +123,7 @@ _SIGS = {
                         C.c_uint64, _vp, C.POINTER(QueryStats)],
     "anqi_query_upload": [_vp, _f32, C.c_uint32, _vp, C.c_uint32, _vp, C.c_uint32],
     "anqi_query_run": [_vp, C.c_int, C.POINTER(QueryStats)],
+    "anqi_query_run_graph": [_vp, C.c_int, C.POINTER(QueryStats)],
     "anqi_query_counters": [_vp, C.POINTER(QueryStats)],
     "anqi_query_download": [_vp, _u32, _vp, C.c_uint64, _vp, _vp, C.c_uint64, _vp],
     "anqi_query_evaluate": [_vp, _u32, _u32, C.c_uint64, C.POINTER(C.c_double), C.POINTER(C.c_double),
@@ -363,6 +364,12 @@ class Context:
         self._check(self.lib.anqi_query_run(self.h, int(keep_candidates), C.byref(st)), "query_run")
         if counters:
             self._check(self.lib.anqi_query_counters(self.h, C.byref(st)), "query_counters")
+        return {k2: getattr(st, k2) for k2, _ in QueryStats._fields_}
+
+    def query_run_graph(self, keep_candidates=False) -> dict:
+        """anqi_query_run through a captured CUDA graph (same results)."""
+        st = QueryStats()
+        self._check(self.lib.anqi_query_run_graph(self.h, int(keep_candidates), C.byref(st)), "query_run_graph")
         return {k2: getattr(st, k2) for k2, _ in QueryStats._fields_}
 
     def query_download(self, with_candidates=False) -> QueryResult:

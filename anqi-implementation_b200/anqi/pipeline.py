@@ -36,6 +36,16 @@ def mixture(n: int, d: int = 128, nq: int = 10_000, centers: int = 1000, sigma: 
     return out[:n], out[n:]
 
 
+def mixture_queries(nq: int, d: int = 128, centers: int = 1000, sigma: float = 20.0, seed: int = 20260819,
+                    qseed: int = 1):
+    """More queries from the mixture of `mixture(..., seed)` (same centres),
+    drawn from their own stream so the base rows stay as they are."""
+    c = np.random.default_rng(seed).uniform(0.0, 128.0, size=(centers, d))
+    rng = np.random.default_rng([seed, qseed])
+    lab = rng.integers(0, centers, size=nq)
+    return np.rint(np.clip(c[lab] + rng.normal(0.0, sigma, size=(nq, d)), 0.0, 255.0)).astype(np.float32)
+
+
 def gaussian(n: int, d: int, nq: int, seed: int = 20260819, normalize: bool = False):
     rng = np.random.default_rng(seed)
     b = rng.normal(0.0, 1.0, size=(n, d)).astype(np.float32)

@@ -323,6 +323,7 @@ void anqi_ctx_destroy(anqi_ctx* h) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->l2_window) clear_l2_window(c);
+    if (c->qgraph) cudaGraphExecDestroy(c->qgraph);
     for (DevBuf* b : c->member_bufs()) release(c, *b);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);

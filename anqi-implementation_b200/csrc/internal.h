@@ -95,6 +95,11 @@ struct Ctx {
     DevBuf vis_gtab;                               // per-slot L2-resident visited tables
     uint32_t gtab_slots = 0, gtab_cap = 0;
     bool l2_window = false;                        // an L2 persisting window is set on the stream
+    // configuration of the last anqi_query_run and the captured graph of it
+    uint32_t last_cfg_hash = 0, last_cfg_gcap = 0, last_cfg_blocks = 0;
+    size_t last_cfg_smem = 0;
+    cudaGraphExec_t qgraph = nullptr;
+    std::vector<uint64_t> qgraph_key;
     uint64_t device_bytes = 0;
     std::vector<DevBuf*> member_bufs() {
         return {&ix.base, &ix.lifted, &ix.onorm, &ix.deg, &ix.links, &ix.tleft, &ix.tright, &ix.toffset,

@@ -837,9 +837,10 @@ static int prepare_entries(Ctx* c, bool* ordered) {
     return ANQI_OK;
 }
 
-// One search launch with configuration cfg; ms = its device time.  Returns
-// ANQI_ERR_CAPACITY (and the needed fill) when an output buffer was too small.
-static int launch_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, float* ms, unsigned long long* fill) {
+// Enqueues one search launch with configuration cfg (counters cleared, CUDA
+// events around the kernel) on the context's stream; no host synchronization,
+// so it can be captured into a graph.
+static int enqueue_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, bool capturing = false) {
     Batch& b = c->batch;
     const QueryIndex& ix = c->ix;
     int rc;
@@ -904,11 +905,22 @@ static int launch_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, floa
     p.gtab = cfg.gcap ? c->vis_gtab.as<uint32_t>() : nullptr;
     auto kern = search_kernel_for(ix.dim);
     ANQI_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
-    ANQI_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    // in a captured graph the events become event-record nodes (so the replay
+    // is timed like a plain launch)
+    const unsigned ef = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    ANQI_CUDA(c, cudaEventRecordWithFlags(c->ev0, c->stream, ef));
     kern<<<cfg.blocks, 128, cfg.smem, c->stream>>>(p);
     ANQI_CUDA(c, cudaGetLastError());
-    ANQI_CUDA(c, cudaEventRecord(c->ev1, c->stream));
-    ANQI_CUDA(c, cudaMemcpyAsync(fill, p.fill, 16, cudaMemcpyDeviceToHost, c->stream));
+    ANQI_CUDA(c, cudaEventRecordWithFlags(c->ev1, c->stream, ef));
+    return ANQI_OK;
+}
+
+// Reads back the output fill and the error word of the last search (one
+// synchronization); ms = the search kernel's device time.  Returns
+// ANQI_ERR_CAPACITY (and the needed fill) when an output buffer was too small.
+static int check_search(Ctx* c, float* ms, unsigned long long* fill) {
+    int rc;
+    ANQI_CUDA(c, cudaMemcpyAsync(fill, c->counters.as<uint32_t>() + 4, 16, cudaMemcpyDeviceToHost, c->stream));
     uint32_t err = 0;
     ANQI_CUDA(c, cudaMemcpyAsync(&err, c->err.p, 4, cudaMemcpyDeviceToHost, c->stream));
     if ((rc = sync(c))) return rc;
@@ -918,6 +930,30 @@ static int launch_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, floa
     }
     if ((rc = check_device_error(c, "rknn search"))) return rc;
     ANQI_CUDA(c, cudaEventElapsedTime(ms, c->ev0, c->ev1));
+    return ANQI_OK;
+}
+
+static int launch_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, float* ms, unsigned long long* fill) {
+    int rc = enqueue_search(c, cfg, keep_candidates);
+    return rc ? rc : check_search(c, ms, fill);
+}
+
+// Enqueues the CSR offsets and the compaction of the last search's output.
+static int enqueue_compaction(Ctx* c, int keep_candidates) {
+    Batch& b = c->batch;
+    scan_counts_kernel<<<1, 1024, 0, c->stream>>>(b.npred.as<uint32_t>(), b.nq, b.pred_off.as<uint32_t>());
+    gather_csr_kernel<<<c->sm_count * 4, 256, 0, c->stream>>>(b.pred_buf.as<uint32_t>(),
+                                                              b.pred_at.as<unsigned long long>(),
+                                                              b.pred_off.as<uint32_t>(), b.nq,
+                                                              b.pred_csr.as<uint32_t>());
+    if (keep_candidates) {
+        scan_counts_kernel<<<1, 1024, 0, c->stream>>>(b.ncand.as<uint32_t>(), b.nq, b.cand_off.as<uint32_t>());
+        gather_csr_kernel<<<c->sm_count * 4, 256, 0, c->stream>>>(b.cand_buf.as<uint32_t>(),
+                                                                  b.cand_at.as<unsigned long long>(),
+                                                                  b.cand_off.as<uint32_t>(), b.nq,
+                                                                  b.cand_csr.as<uint32_t>());
+    }
+    ANQI_CUDA(c, cudaGetLastError());
     return ANQI_OK;
 }
 
@@ -1022,22 +1058,15 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
             continue;
         }
         if (rc) return rc;
-        // CSR offsets + compaction
-        scan_counts_kernel<<<1, 1024, 0, c->stream>>>(b.npred.as<uint32_t>(), b.nq, b.pred_off.as<uint32_t>());
-        if ((rc = ensure(c, b.pred_csr, std::max<uint64_t>(fill[0], 1) * 4))) return rc;
-        gather_csr_kernel<<<c->sm_count * 4, 256, 0, c->stream>>>(b.pred_buf.as<uint32_t>(),
-                                                                  b.pred_at.as<unsigned long long>(),
-                                                                  b.pred_off.as<uint32_t>(), b.nq,
-                                                                  b.pred_csr.as<uint32_t>());
-        if (keep_candidates) {
-            scan_counts_kernel<<<1, 1024, 0, c->stream>>>(b.ncand.as<uint32_t>(), b.nq, b.cand_off.as<uint32_t>());
-            if ((rc = ensure(c, b.cand_csr, std::max<uint64_t>(fill[1], 1) * 4))) return rc;
-            gather_csr_kernel<<<c->sm_count * 4, 256, 0, c->stream>>>(b.cand_buf.as<uint32_t>(),
-                                                                      b.cand_at.as<unsigned long long>(),
-                                                                      b.cand_off.as<uint32_t>(), b.nq,
-                                                                      b.cand_csr.as<uint32_t>());
-        }
-        ANQI_CUDA(c, cudaGetLastError());
+        // CSR offsets + compaction (the CSR buffers hold the whole output
+        // capacity, so a replayed graph never outgrows them)
+        if ((rc = ensure(c, b.pred_csr, std::max<uint64_t>(b.pred_cap, 1) * 4))) return rc;
+        if (keep_candidates && (rc = ensure(c, b.cand_csr, std::max<uint64_t>(b.cand_cap, 1) * 4))) return rc;
+        if ((rc = enqueue_compaction(c, keep_candidates))) return rc;
+        c->last_cfg_hash = best.hash_cap;
+        c->last_cfg_gcap = best.gcap;
+        c->last_cfg_blocks = best.blocks;
+        c->last_cfg_smem = best.smem;
         b.have_results = true;
         b.have_cands = keep_candidates != 0;
         if (st) {
@@ -1048,6 +1077,28 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
         return sync(c);
     }
     return fail(c, ANQI_ERR_CAPACITY, "rknn search: output capacity could not be satisfied");
+}
+
+// Everything a captured query graph depends on: batch shape and mode, search
+// configuration, output capacities and every device buffer it touches.
+static std::vector<uint64_t> query_graph_key(Ctx* c, int keep_candidates) {
+    const Batch& b = c->batch;
+    const QueryIndex& ix = c->ix;
+    auto u = [](const void* q) { return (uint64_t)(uintptr_t)q; };
+    return {b.nq, b.L_max, (uint64_t)b.has_k, (uint64_t)b.has_L, b.k_all, b.L_all, (uint64_t)keep_candidates,
+            (uint64_t)b.ordered, c->last_cfg_hash, c->last_cfg_gcap, c->last_cfg_blocks, c->last_cfg_smem,
+            b.pred_cap, b.cand_cap, u(b.q.p), u(b.qslot.p), u(b.qL.p), u(b.pred_buf.p), u(b.cand_buf.p),
+            u(b.pred_csr.p), u(b.cand_csr.p), u(b.pred_off.p), u(b.cand_off.p), u(b.entry.p), u(b.enode.p),
+            u(b.order.p), u(b.leaf_cnt.p), u(b.npred.p), u(b.ncand.p), u(b.ndist.p), u(b.nexp.p), u(b.nflood.p),
+            u(b.pred_at.p), u(b.cand_at.p), u(c->vis_bits.p), u(c->vis_log.p), u(c->cand_scratch.p),
+            u(c->vis_gtab.p), u(c->thr_table.p), u(c->counters.p), u(c->err.p), u(ix.lifted.p), u(ix.base.p),
+            u(ix.links.p), u(ix.thyper.p), ix.n, c->vis_words, c->log_cap, c->cand_cap};
+}
+
+static void drop_query_graph(Ctx* c) {
+    if (c->qgraph) cudaGraphExecDestroy(c->qgraph);
+    c->qgraph = nullptr;
+    c->qgraph_key.clear();
 }
 
 int anqi_query_counters(anqi_ctx* h, anqi_query_stats* st) {
@@ -1070,6 +1121,61 @@ int anqi_query_counters(anqi_ctx* h, anqi_query_stats* st) {
     st->n_cand = sums[2];
     st->n_pred = sums[3];
     st->n_flood = sums[4];
+    return ANQI_OK;
+}
+
+int anqi_query_run_graph(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
+    if (!h) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    Batch& b = c->batch;
+    if (!c->ix.loaded || b.nq == 0) return fail(c, ANQI_ERR_ARGS, "anqi_query_run_graph: no index or batch");
+    int rc;
+    if (c->qgraph && c->qgraph_key == query_graph_key(c, keep_candidates)) {
+        ANQI_CUDA(c, cudaGraphLaunch(c->qgraph, c->stream));
+        float ms = 0;
+        unsigned long long fill[2] = {0, 0};
+        rc = check_search(c, &ms, fill);
+        if (rc == ANQI_OK) {
+            b.have_results = true;
+            b.have_cands = keep_candidates != 0;
+            if (st) {
+                st->search_ms = ms;
+                st->visited_table = c->last_cfg_hash;
+                st->visited_l2_table = c->last_cfg_gcap;
+            }
+            return ANQI_OK;
+        }
+        if (rc != ANQI_ERR_CAPACITY) return rc;
+        drop_query_graph(c);  // outgrew the captured capacity: run the sized path, capture again
+    }
+    // the plain path sizes buffers, autotunes and produces this batch's results
+    if ((rc = anqi_query_run(h, keep_candidates, st))) return rc;
+    drop_query_graph(c);
+    SearchCfg cfg;
+    cfg.hash_cap = c->last_cfg_hash;
+    cfg.gcap = c->last_cfg_gcap;
+    cfg.blocks = c->last_cfg_blocks;
+    cfg.smem = c->last_cfg_smem;
+    bool ordered = false;
+    cudaGraph_t g = nullptr;
+    ANQI_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    rc = prepare_entries(c, &ordered);
+    if (!rc) rc = enqueue_search(c, cfg, keep_candidates, true);
+    if (!rc) rc = enqueue_compaction(c, keep_candidates);
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ce != cudaSuccess) return cuda_check(c, ce, "cudaStreamEndCapture");
+    const cudaError_t ie = cudaGraphInstantiate(&c->qgraph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+        c->qgraph = nullptr;
+        return cuda_check(c, ie, "cudaGraphInstantiate");
+    }
+    c->qgraph_key = query_graph_key(c, keep_candidates);
     return ANQI_OK;
 }
 

@@ -64,6 +64,10 @@ def parse():
     ap.add_argument("--no-gt", action="store_true", help="skip the exact ground truth (profiling runs; no recall)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU seconds of the cpu_baseline sample")
     ap.add_argument("--keep", type=Path, default=None, help="write the index prefix files here")
+    ap.add_argument("--batched-queries", type=int, default=100_000,
+                    help="queries of the batching form (per-query k and L, CUDA graph); 0 skips it")
+    ap.add_argument("--batch", type=int, default=10_000)
+    ap.add_argument("--batched-reps", type=int, default=2, help="timed passes over the batching-form queries")
     return ap.parse_args()
 
 
@@ -163,6 +167,7 @@ def build_workload(ctx, a, rank, log):
     t0 = time.perf_counter()
     _, ex_keys = pipeline.exact_thresholds(ctx, base, 100, method="tc", hints=ix.aknn_ids)
     t_thr = time.perf_counter() - t0
+    ix.exact_keys = ex_keys
     gt = {}
     t0 = time.perf_counter()
     for k in ks:
@@ -207,6 +212,62 @@ def reference_qbench(d: Path, ks, L, threads, warmup, steps, nq):
         return None, f"reference harness failed ({p.returncode}): {p.stderr[-300:]}"
     line = [l for l in p.stdout.splitlines() if l.startswith("{")][-1]
     return json.loads(line), None
+
+
+def run_batched(ctx, a, base, ix, rank):
+    """Batching form: batched_queries more queries from the mixture, per-query
+    k uniform in {10, 50, 100} and beam width uniform in [64, 600], run as
+    batches of `batch` queries, each one replay of the captured CUDA graph
+    (lift + entry, leaf ordering, search with the LRQ postfilter, CSR
+    compaction).  Per-batch device latency (CUDA events) p50 / p99 and QPS over
+    the whole run; recall against the exact RkNN of every query's own k."""
+    from anqi import pipeline
+    nqb, bs = a.batched_queries, a.batch
+    q = pipeline.mixture_queries(nqb, a.d, qseed=7 + rank)
+    rng = np.random.default_rng(11 + rank)
+    ks = rng.choice(np.array([10, 50, 100], np.uint32), nqb).astype(np.uint32)
+    Ls = rng.integers(64, 601, nqb).astype(np.uint32)
+    nb = nqb // bs
+    lat, preds = [], []
+    for rep in range(1 + a.batched_reps):
+        for i in range(nb):
+            sl = slice(i * bs, (i + 1) * bs)
+            Lb = Ls[sl].copy()
+            Lb[0] = 600  # one beam-width bound for every batch: one captured graph
+            ctx.query_upload(q[sl], ks[sl], Lb)
+            if rep == 0 and i == 0:
+                ctx.query_run_graph()  # plain run + capture
+            ctx.timer_start()
+            st = ctx.query_run_graph()
+            lat.append(ctx.timer_stop())
+            if rep == 0:
+                preds.append(ctx.query_download())
+    lat = np.array(lat[nb:] if a.batched_reps else lat)
+    out = {"queries": nqb, "batch": bs, "k": "uniform {10,50,100}", "L": "uniform [64,600] (bound 600)",
+           "qps": round(bs * len(lat) / (lat.sum() / 1e3), 1), "p50_ms": round(float(np.percentile(lat, 50)), 3),
+           "p99_ms": round(float(np.percentile(lat, 99)), 3), "batches_timed": int(len(lat)), "cuda_graph": True,
+           "visited_table": [st["visited_table"], st["visited_l2_table"]]}
+    ex_keys = getattr(ix, "exact_keys", None)
+    if ex_keys is not None:
+        # exact RkNN of each query at its own k (tensor path), recall / precision
+        rec = prec = 0.0
+        ne = 0
+        for k in (10, 50, 100):
+            sel = np.nonzero(ks[:nb * bs] == k)[0]
+            off, ids, _ = pipeline.rknn_ground_truth(ctx, base, q[sel], ex_keys[:, k - 1], method="tc")
+            for j, qi in enumerate(sel):
+                truth = ids[off[j]:off[j + 1]]
+                if len(truth) == 0:
+                    continue
+                r = preds[qi // bs]
+                p = r.pred(qi % bs)
+                hit = len(np.intersect1d(p, truth))
+                rec += hit / len(truth)
+                prec += 1.0 if len(p) == 0 else hit / len(p)
+                ne += 1
+        out["recall"] = round(rec / max(ne, 1), 6)
+        out["precision"] = round(prec / max(ne, 1), 6)
+    return out
 
 
 def run_ours(a, rank, world, local):
@@ -293,6 +354,7 @@ def run_ours(a, rank, world, local):
             traffic = int(tj["bytes_per_graph_dist"] * s0["n_dist"])
         except (ValueError, KeyError):
             traffic = None
+    batched = run_batched(ctx, a, base, ix, rank) if a.batched_queries else None
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True, "scaling": "weak",
@@ -316,6 +378,7 @@ def run_ours(a, rank, world, local):
         "precision": None if ev["precision"] is None else round(ev["precision"], 6), "per_k": per_k,
         "counters_per_query": {"graph_dist": round(s0["n_dist"] / nb, 1), "expansions": round(X / nb, 1),
                                "candidates": round(s0["n_cand"] / nb, 1), "verified": round(s0["n_pred"] / nb, 2)},
+        "batched_form": batched,
         "build_s": {k: round(v, 3) for k, v in ix.timings.items() if isinstance(v, float)},
         "aknn_build": {"bf16_tensor_init_s": round(ix.timings["aknn_build_s"], 3),
                        "fp32_init_s": round(ix.timings["aknn_build_fp32_s"], 3),

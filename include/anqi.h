@@ -228,6 +228,16 @@ int anqi_query_upload(anqi_ctx* ctx, const float* queries, uint32_t nq, const ui
 /* st (optional) receives search_ms only; anqi_query_counters sums the
  * per-query counters of the last run (device -> host copies). */
 int anqi_query_run(anqi_ctx* ctx, int keep_candidates, anqi_query_stats* st);
+/* CUDA-graph form of anqi_query_run for a stream of batches of one shape (same
+ * nq, beam-width bound, k/L mode and candidate option; no counterpart in the
+ * reference, whose query loop is a host loop).  The first call runs
+ * anqi_query_run (autotuning, sizing the outputs) and captures the batch's
+ * launch sequence -- lift + tree entry, leaf ordering, search, CSR compaction
+ * -- into a graph; later calls replay it on whatever batch anqi_query_upload
+ * left resident, with one small copy back of the output fill.  Results equal
+ * anqi_query_run's.  A batch whose output outgrows the captured capacity runs
+ * the plain path and is captured again. */
+int anqi_query_run_graph(anqi_ctx* ctx, int keep_candidates, anqi_query_stats* st);
 int anqi_query_counters(anqi_ctx* ctx, anqi_query_stats* st);
 int anqi_query_download(anqi_ctx* ctx, uint32_t* pred_off, uint32_t* pred_ids, uint64_t pred_cap,
                         uint32_t* cand_off, uint32_t* cand_ids, uint64_t cand_cap, uint32_t* n_dist);

@@ -182,6 +182,61 @@ def test_query_bit_exact_vs_oracle_random(ctx, random_index, table, monkeypatch)
                 assert np.array_equal(r.pred(i), preds[i]), (k, L, i)
 
 
+@pytest.fixture(scope="module")
+def random_index_128():
+    return _random_index(n=4000, d=128, nq=200, seed=23)
+
+
+def test_query_bit_exact_vs_oracle_d128(ctx, random_index_128):
+    """d = 128 (lifted dimension 130) runs the search kernel instance whose
+    distance loops are unrolled at compile time: same candidates, #dist and
+    verified lists as the oracle."""
+    base, query, lifted, links, deg, tree, sc, m2, thr = random_index_128
+    ctx.index_load(base, lifted, deg, links, tree, sc, m2)
+    ta = ol.TreeArrays(tree.left, tree.right, tree.offset, tree.hyperplane, tree.leaf_first())
+    for k in (10, 100):
+        ctx.set_thresholds(k, thr[k])
+        for L in (32, 128, 400):
+            r = ctx.rknn_query(query, k, L, keep_candidates=True)
+            cands, preds, nds = ol.range_search_all(lifted, links, deg, base, ta, sc, m2, query, thr[k], L)
+            assert np.array_equal(r.n_dist, nds), (k, L)
+            for i in range(len(query)):
+                assert np.array_equal(r.cand(i), cands[i]), (k, L, i)
+                assert np.array_equal(r.pred(i), preds[i]), (k, L, i)
+
+
+def test_query_graph_replay_equals_plain(ctx, random_index):
+    """anqi_query_run_graph: the first call runs the plain path and captures
+    the launch sequence; replays on newly uploaded batches of the same shape
+    return exactly what anqi_query_run returns for them."""
+    base, query, lifted, links, deg, tree, sc, m2, thr = random_index
+    ctx.index_load(base, lifted, deg, links, tree, sc, m2)
+    for k in (10, 50, 100):
+        ctx.set_thresholds(k, thr[k])
+    rng = np.random.default_rng(7)
+    nq = len(query)
+
+    def batch(seed):
+        r = np.random.default_rng(seed)
+        q = query[r.permutation(nq)]
+        return q, r.choice([10, 50, 100], nq).astype(np.uint32), r.integers(16, 400, nq).astype(np.uint32)
+
+    for seed in (1, 2, 3):
+        q, ks, Ls = batch(seed)
+        Ls[0] = 400  # same beam-width bound in every batch
+        ctx.query_upload(q, ks, Ls)
+        ctx.query_run(keep_candidates=True)
+        want = ctx.query_download(with_candidates=True)
+        ctx.query_upload(q, ks, Ls)
+        for _ in range(2):
+            st = ctx.query_run_graph(keep_candidates=True)
+            got = ctx.query_download(with_candidates=True)
+            assert np.array_equal(got.pred_off, want.pred_off) and np.array_equal(got.pred_ids, want.pred_ids)
+            assert np.array_equal(got.cand_off, want.cand_off) and np.array_equal(got.cand_ids, want.cand_ids)
+            assert np.array_equal(got.n_dist, want.n_dist)
+            assert st["search_ms"] > 0
+
+
 def test_resident_batch_and_evaluate(ctx, random_index):
     base, query, lifted, links, deg, tree, sc, m2, thr = random_index
     ctx.index_load(base, lifted, deg, links, tree, sc, m2)
