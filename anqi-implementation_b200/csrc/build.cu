@@ -1427,7 +1427,8 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
                     maxcnt = std::max(maxcnt, f.leaf_cnt[g]);
                 }
             }
-        if (ap->precision == 1) {
+        // the tensor-core tiles hold rows of up to 256 (padded) dimensions
+        if (ap->precision == 1 && round_up(d, 16u) <= 256) {
             // BF16 tensor-core leaf tiles: candidates per tree, then the merge
             TcPrep tp;
             TmpBuf ccnt(c), cid(c), ckey(c);

@@ -24,6 +24,7 @@
 
 #include "beam.cuh"
 #include "internal.h"
+#include "tc.cuh"
 
 namespace anqi {
 
@@ -84,11 +85,30 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+// Bulk (TMA) copy of one row into shared memory, completing on the warp's
+// mbarrier; and the arrive that sets the bytes a phase waits for.
+__device__ __forceinline__ void bulk_row(float* dst, const float* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("fence.proxy.async.shared::cta;\n"
+                 "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+                 ::"r"(tc::smem_u32(dst)), "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void bar_expect(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(tc::smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+constexpr uint32_t kRowWaitPolls = 1u << 24;
+
 // Visits the links of node (slots l0 = link[lane], l1 = link[lane + 32], dg =
 // degree): collects the ids seen for the first time into ni[0..m) in link-slot
-// order and logs them (levels 1 and 2).  Returns m.
+// order and logs them (levels 1 and 2).  The lifted rows of the first 8 of
+// them are requested at once, one bulk copy per row into stage[slot],
+// completing on bar.  Returns m.
 __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t l0, uint32_t l1, uint32_t dg,
-                                                 Visited& vis, uint32_t& nlog, uint32_t* ni, uint32_t lane) {
+                                                 Visited& vis, uint32_t& nlog, uint32_t* ni, uint32_t lane,
+                                                 float* stage, uint64_t* bar) {
     bool f0 = false, f1 = false, bad = false;
     uint32_t r0 = 0, r1 = 0;
     if (lane < dg) {
@@ -103,6 +123,13 @@ __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t
     const unsigned b0 = __ballot_sync(kFull, f0), b1 = __ballot_sync(kFull, f1);
     const uint32_t c0 = __popc(b0), lt = lanemask_lt();
     const uint32_t p0 = __popc(b0 & lt), p1 = c0 + __popc(b1 & lt);
+    const uint32_t m = c0 + __popc(b1);
+    const uint32_t rb = p.lstride * 4;
+    if (m) {
+        if (lane == 0) bar_expect(bar, min(m, 8u) * rb);
+        if (f0 && p0 < 8) bulk_row(stage + (size_t)p0 * p.lstride, p.lifted + (size_t)l0 * p.lstride, rb, bar);
+        if (f1 && p1 < 8) bulk_row(stage + (size_t)p1 * p.lstride, p.lifted + (size_t)l1 * p.lstride, rb, bar);
+    }
     const bool logs = vis.level != 0;
     if (f0) {
         ni[p0] = l0;
@@ -112,7 +139,6 @@ __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t
         ni[p1] = l1;
         if (logs && nlog + p1 < p.log_cap) vis.vlog[nlog + p1] = r1;
     }
-    const uint32_t m = c0 + __popc(b1);
     nlog += m;
     __syncwarp();
     return m;
@@ -127,23 +153,34 @@ __device__ __forceinline__ void load_links(const SearchParams& p, uint32_t node,
 }
 
 // Distances of the m fresh neighbours to the lifted query: 8 groups of 4
-// lanes, each group staging its row into shared memory (one round trip for up
-// to 8 rows) and reducing it in the reference's lane order.
+// lanes, each reducing its row in the reference's lane order.  Rows arrive by
+// bulk copy, 8 per round (the first round was requested by expand_links);
+// each round is one phase of bar (parity ph).  Returns false when a wait ran
+// out (the error word is set).
 template <uint32_t kDim>
-__device__ __forceinline__ void fresh_distances(const SearchParams& p, const float* qhat, const uint32_t* ni,
-                                                float* nd, uint32_t m, uint32_t gw, uint32_t gt, float* stage) {
+__device__ __forceinline__ bool fresh_distances(const SearchParams& p, const float* qhat, const uint32_t* ni,
+                                                float* nd, uint32_t m, uint32_t gw, uint32_t gt, float* stage,
+                                                uint64_t* bar, uint32_t& ph, uint32_t lane) {
     const uint32_t dim = kDim ? kDim : p.dim;
+    const uint32_t rb = p.lstride * 4;
     float* row = stage + (size_t)gw * p.lstride;
     for (uint32_t r0 = 0; r0 < m; r0 += 8) {
-        const uint32_t ia = r0 + gw;
-        const bool oka = ia < m;
-        if (oka) stage_row_async(row, p.lifted + (size_t)ni[ia] * p.lstride, p.lstride, gt, 4);
-        cp_async_wait_all();
-        __syncwarp();
+        const uint32_t nr = min(m - r0, 8u);
+        if (r0 > 0) {
+            if (lane == 0) bar_expect(bar, nr * rb);
+            if (lane < nr) bulk_row(stage + (size_t)lane * p.lstride, p.lifted + (size_t)ni[r0 + lane] * p.lstride, rb, bar);
+        }
+        if (!tc::mbar_wait(bar, ph, kRowWaitPolls)) {
+            set_error(p.err, kDevWaitTimeout);
+            return false;
+        }
+        ph ^= 1u;
+        const bool oka = gw < nr;
         const float da = group_l2sqr(oka ? row : stage, qhat, dim, gt, kFull);
-        if (gt == 0 && oka) nd[ia] = da;
+        if (gt == 0 && oka) nd[r0 + gw] = da;
         __syncwarp();
     }
+    return true;
 }
 
 // Appends fresh neighbours within R2 to the candidate / flood list (visit order).
@@ -174,7 +211,7 @@ extern __shared__ __align__(16) unsigned char g_smem[];
 __device__ __host__ __forceinline__ size_t search_smem_words(uint32_t L_max, uint32_t lstride, uint32_t bstride,
                                                              uint32_t hash_cap) {
     return (size_t)2 * L_max + 128 + lstride + bstride + 8 * (size_t)(lstride > bstride ? lstride : bstride) +
-           hash_cap;
+           hash_cap + 8;
 }
 
 template <uint32_t kDim>
@@ -191,6 +228,13 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
     uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 64);
     float* stage = reinterpret_cast<float*>(ni + 64);  // 8 staged rows of max(lstride, bstride)
     uint32_t* tab = reinterpret_cast<uint32_t*>(stage + 8 * (size_t)max(p.lstride, p.bstride));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tab + p.hash_cap);  // row-copy mbarrier of this warp
+    uint32_t ph = 0;
+    if (lane == 0) {
+        tc::mbar_init(bar, 1);
+        tc::fence_mbar_init();
+    }
+    __syncwarp();
     uint32_t* bits = p.vis_bits + (size_t)slot * p.vis_words;
     uint32_t* vlog = p.vis_log + (size_t)slot * p.log_cap;
     uint32_t* cl = p.cand_scratch + (size_t)slot * p.cand_cap;
@@ -278,10 +322,10 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
                 load_links(p, pre_node, lane, pl0, pl1, pdg);
             }
             vis_room(vis, nlog, p.degree, lane, p.err);
-            const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane);
+            const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane, stage, bar);
             uint32_t mk = 0;
             if (m != 0) {
-                fresh_distances<kDim>(p, qhat, ni, nd, m, gw, gt, stage);
+                if (!fresh_distances<kDim>(p, qhat, ni, nd, m, gw, gt, stage, bar, ph, lane)) return;
                 append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
                 const bool full = size >= L;
                 mk = sort_fresh_kept(nd, ni, m, full, full ? bd[L - 1] : 0.f, full ? bi[L - 1] : 0u, lane);
@@ -364,9 +408,9 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
                 load_links(p, pre_node, lane, pl0, pl1, pdg);
             }
             vis_room(vis, nlog, p.degree, lane, p.err);
-            const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane);
+            const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane, stage, bar);
             if (m == 0) continue;
-            fresh_distances<kDim>(p, qhat, ni, nd, m, gw, gt, stage);
+            if (!fresh_distances<kDim>(p, qhat, ni, nd, m, gw, gt, stage, bar, ph, lane)) return;
             append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
         }
         if (overflow && lane == 0) set_error(p.err, kDevCandOverflow);

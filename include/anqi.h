@@ -100,7 +100,8 @@ typedef struct {
     uint32_t nn_iters;   /* ANQI_NNITERS, default 0 */
     uint32_t nn_sample;  /* ANQI_NNSAMPLE, default 20 */
     uint32_t precision;  /* init_knn leaf distances: 0 = FP32 CUDA cores, 1 = BF16 tensor-core
-                            tiles with FP32 recheck (identical output) */
+                            tiles with FP32 recheck (identical output; d <= 256, larger d
+                            runs on the CUDA cores) */
 } anqi_aknn_params;
 
 typedef struct {
