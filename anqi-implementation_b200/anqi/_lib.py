@@ -93,6 +93,7 @@ _SIGS = {
     "anqi_timer_start": [_vp],
     "anqi_timer_stop": [_vp, C.POINTER(C.c_float)],
     "anqi_pair_distances": [_vp, _f32, _f32, C.c_uint64, C.c_uint32, _f32, _f32],
+    "anqi_pair_distances_group": [_vp, _f32, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32],
     "anqi_lrq_encode": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _f32, C.c_uint32, _f32, _u8],
     "anqi_lrq_materialize": [_vp, _f32, _u8, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _f32, C.c_uint32,
                              C.c_uint32, C.c_double, _f32],
@@ -243,13 +244,13 @@ class Context:
 
     # ------------------------------------------------------------ kernels
 
-    def pair_distances(self, a, b):
+    def pair_distances(self, a, b, group=4):
         a = _c(a, np.float32)
         b = _c(b, np.float32)
         m, dim = a.shape
         l2 = np.empty(m, np.float32)
         ip = np.empty(m, np.float32)
-        self._check(self.lib.anqi_pair_distances(self.h, a, b, m, dim, l2, ip), "pair_distances")
+        self._check(self.lib.anqi_pair_distances_group(self.h, a, b, m, dim, group, l2, ip), "pair_distances")
         return l2, ip
 
     def lrq_encode(self, keys, mu, basis, codebook):

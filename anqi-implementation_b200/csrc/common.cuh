@@ -126,6 +126,102 @@ __device__ __forceinline__ float group_ip(const float* __restrict__ a, const flo
     return res;
 }
 
+// ------------------------------------------- wider groups (same arithmetic)
+// A group of G = 8 or 16 threads per vector pair: thread t holds AVX lanes
+// (16 / G) t .. (16 / G) t + 16 / G - 1.  Every lane accumulates the same
+// FMAs in the same order as in the 4-thread form and the fold is the same
+// tree, so the result has the same bits; fewer rows per round, fewer
+// instructions per row.  Used when a batch has few rows, and for long rows
+// (large dimensions), where fewer rows fit the staging buffer.
+
+// _mm512_reduce_add_ps over a G-thread group (G = 8: a0, a1 = lanes 2t, 2t+1;
+// G = 16: a0 = lane t).  The result is valid in all G threads.
+template <int G>
+__device__ __forceinline__ float group_reduce16_w(float a0, float a1, unsigned mask) {
+    if constexpr (G == 8) {
+        // T3[i] = A[i+8] + A[i]: threads 0..3 take threads 4..7
+        const float t0 = __fadd_rn(__shfl_down_sync(mask, a0, 4, 8), a0);
+        const float t1 = __fadd_rn(__shfl_down_sync(mask, a1, 4, 8), a1);
+        // T6[i] = T3[i+4] + T3[i]: threads 0, 1 take threads 2, 3
+        const float s0 = __fadd_rn(__shfl_down_sync(mask, t0, 2, 8), t0);
+        const float s1 = __fadd_rn(__shfl_down_sync(mask, t1, 2, 8), t1);
+        // (T6[0] + T6[2]) + (T6[1] + T6[3]): thread 0 holds T6[0..1], thread 1 T6[2..3]
+        const float w0 = __shfl_down_sync(mask, s0, 1, 8), w1 = __shfl_down_sync(mask, s1, 1, 8);
+        return __shfl_sync(mask, __fadd_rn(__fadd_rn(s0, w0), __fadd_rn(s1, w1)), 0, 8);
+    } else {
+        const float t0 = __fadd_rn(__shfl_down_sync(mask, a0, 8, 16), a0);
+        const float s0 = __fadd_rn(__shfl_down_sync(mask, t0, 4, 16), t0);
+        const float x = __fadd_rn(s0, __shfl_down_sync(mask, s0, 2, 16));  // T6[0]+T6[2] | T6[1]+T6[3]
+        return __shfl_sync(mask, __fadd_rn(x, __shfl_down_sync(mask, x, 1, 16)), 0, 16);
+    }
+}
+
+// Squared L2 (distance.h:58-86) by a group of G = 8 or 16 threads.
+template <int G>
+__device__ __forceinline__ float group_l2sqr_w(const float* __restrict__ a, const float* __restrict__ b,
+                                               uint32_t dim, uint32_t gt, unsigned mask) {
+    const uint32_t q16 = dim >> 4, rem = dim & 15u;
+    constexpr uint32_t NL = 16 / G;
+    float c0 = 0.f, c1 = 0.f;
+#pragma unroll 4
+    for (uint32_t c = 0; c < q16; c++) {
+        if constexpr (NL == 2) {
+            const float2 x = *reinterpret_cast<const float2*>(a + 16 * c + 2 * gt);
+            const float2 y = *reinterpret_cast<const float2*>(b + 16 * c + 2 * gt);
+            const float d0 = __fsub_rn(x.x, y.x), d1 = __fsub_rn(x.y, y.y);
+            c0 = __fmaf_rn(d0, d0, c0);
+            c1 = __fmaf_rn(d1, d1, c1);
+        } else {
+            const float d0 = __fsub_rn(a[16 * c + gt], b[16 * c + gt]);
+            c0 = __fmaf_rn(d0, d0, c0);
+        }
+    }
+    float res = group_reduce16_w<G>(c0, c1, mask);
+    if (rem) {
+        const uint32_t base = 16 * q16 + NL * gt;
+        float p0 = 0.f, p1 = 0.f;
+        if (NL * gt < rem) {
+            const float d0 = __fsub_rn(a[base], b[base]);
+            p0 = __fmul_rn(d0, d0);
+        }
+        if (NL == 2 && NL * gt + 1 < rem) {
+            const float d1 = __fsub_rn(a[base + 1], b[base + 1]);
+            p1 = __fmul_rn(d1, d1);
+        }
+        res = __fadd_rn(res, group_reduce16_w<G>(p0, p1, mask));
+    }
+    return res;
+}
+
+// Inner product (distance.h:89-116) by a group of G = 8 or 16 threads.
+template <int G>
+__device__ __forceinline__ float group_ip_w(const float* __restrict__ a, const float* __restrict__ b, uint32_t dim,
+                                            uint32_t gt, unsigned mask) {
+    const uint32_t q16 = dim >> 4, rem = dim & 15u;
+    constexpr uint32_t NL = 16 / G;
+    float c0 = 0.f, c1 = 0.f;
+#pragma unroll 4
+    for (uint32_t c = 0; c < q16; c++) {
+        if constexpr (NL == 2) {
+            const float2 x = *reinterpret_cast<const float2*>(a + 16 * c + 2 * gt);
+            const float2 y = *reinterpret_cast<const float2*>(b + 16 * c + 2 * gt);
+            c0 = __fmaf_rn(x.x, y.x, c0);
+            c1 = __fmaf_rn(x.y, y.y, c1);
+        } else {
+            c0 = __fmaf_rn(a[16 * c + gt], b[16 * c + gt], c0);
+        }
+    }
+    float res = group_reduce16_w<G>(c0, c1, mask);
+    if (rem) {
+        const uint32_t base = 16 * q16 + NL * gt;
+        float p0 = 0.f, p1 = 0.f;
+        if (NL * gt < rem) p0 = __fmul_rn(a[base], b[base]);
+        if (NL == 2 && NL * gt + 1 < rem) p1 = __fmul_rn(a[base + 1], b[base + 1]);
+        res = __fadd_rn(res, group_reduce16_w<G>(p0, p1, mask));
+    }
+    return res;
+}
+
 // ------------------------------------------------------- row staging
 // Global -> shared copies of whole rows with cp.async (16 bytes per
 // instruction, no registers held while in flight): a row costs one memory

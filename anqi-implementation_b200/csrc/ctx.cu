@@ -174,17 +174,26 @@ int compute_norms_device(Ctx* c, const float* d_x, uint64_t n, uint32_t dim, uin
     return ANQI_OK;
 }
 
+// G threads per pair (4, 8 or 16): the same results bit for bit.
+template <int G>
 __global__ void pair_dist_kernel(const float* __restrict__ a, const float* __restrict__ b, uint64_t m,
                                  uint32_t dim, uint32_t stride, float* __restrict__ l2, float* __restrict__ ip) {
-    const uint32_t lane = threadIdx.x & 31u, gt = lane & 3u, gw = lane >> 2;
+    constexpr uint32_t R = 32 / G;
+    const uint32_t lane = threadIdx.x & 31u, gt = lane % G, gw = lane / G;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t base = warp * 8; base < m; base += nwarps * 8) {
+    for (uint64_t base = warp * R; base < m; base += nwarps * R) {
         const uint64_t row = base + gw;
         const bool ok = row < m;
         const uint64_t r = ok ? row : base;
-        float v1 = group_l2sqr(a + r * stride, b + r * stride, dim, gt, 0xFFFFFFFFu);
-        float v2 = group_ip(a + r * stride, b + r * stride, dim, gt, 0xFFFFFFFFu);
+        float v1, v2;
+        if constexpr (G == 4) {
+            v1 = group_l2sqr(a + r * stride, b + r * stride, dim, gt, 0xFFFFFFFFu);
+            v2 = group_ip(a + r * stride, b + r * stride, dim, gt, 0xFFFFFFFFu);
+        } else {
+            v1 = group_l2sqr_w<G>(a + r * stride, b + r * stride, dim, gt, 0xFFFFFFFFu);
+            v2 = group_ip_w<G>(a + r * stride, b + r * stride, dim, gt, 0xFFFFFFFFu);
+        }
         if (ok && gt == 0) {
             l2[row] = v1;
             ip[row] = v2;
@@ -364,7 +373,12 @@ int anqi_timer_stop(anqi_ctx* h, float* ms) {
 
 int anqi_pair_distances(anqi_ctx* h, const float* a, const float* b, uint64_t m, uint32_t dim, float* l2sqr,
                         float* ip) {
-    if (!h || !a || !b || !l2sqr || !ip || dim == 0) return ANQI_ERR_ARGS;
+    return anqi_pair_distances_group(h, a, b, m, dim, 4, l2sqr, ip);
+}
+
+int anqi_pair_distances_group(anqi_ctx* h, const float* a, const float* b, uint64_t m, uint32_t dim,
+                              uint32_t group, float* l2sqr, float* ip) {
+    if (!h || !a || !b || !l2sqr || !ip || dim == 0 || (group != 4 && group != 8 && group != 16)) return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     if (m == 0) return ANQI_OK;
@@ -375,8 +389,9 @@ int anqi_pair_distances(anqi_ctx* h, const float* a, const float* b, uint64_t m,
         (rc = ensure(c, dl, m * 4)) || (rc = ensure(c, di, m * 4)))
         return rc;
     int blocks = (int)std::min<uint64_t>((m * 4 + 255) / 256, (uint64_t)c->sm_count * 16);
-    pair_dist_kernel<<<blocks, 256, 0, c->stream>>>(da.as<float>(), db.as<float>(), m, dim, stride, dl.as<float>(),
-                                                   di.as<float>());
+    auto kern = group == 4 ? pair_dist_kernel<4> : group == 8 ? pair_dist_kernel<8> : pair_dist_kernel<16>;
+    kern<<<blocks, 256, 0, c->stream>>>(da.as<float>(), db.as<float>(), m, dim, stride, dl.as<float>(),
+                                        di.as<float>());
     ANQI_CUDA(c, cudaGetLastError());
     if ((rc = d2h(c, l2sqr, dl, m * 4)) || (rc = d2h(c, ip, di, m * 4)) || (rc = sync(c))) return rc;
     return ANQI_OK;

@@ -41,6 +41,7 @@ struct SearchParams {
     const uint32_t* tleaf;
     uint64_t n;
     uint32_t dim, d, lstride, bstride, degree, troot;
+    uint32_t stage_rows;  // rows per staging round: 8, 4 or 2 (long rows)
     double scale, R2;
     const float* thr;  // slot-major thresholds
     const float* queries;
@@ -85,6 +86,11 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+// Rows per staging round fixed at compile time for the d = 128 instance (8
+// rows, 4-thread groups); 0 = from the launch parameters.
+template <uint32_t kDim>
+constexpr uint32_t kSearchRows = kDim == 130 ? 8u : 0u;
+
 // Bulk (TMA) copy of one row into shared memory, completing on the warp's
 // mbarrier; and the arrive that sets the bytes a phase waits for.
 __device__ __forceinline__ void bulk_row(float* dst, const float* src, uint32_t bytes, uint64_t* bar) {
@@ -103,12 +109,14 @@ constexpr uint32_t kRowWaitPolls = 1u << 24;
 
 // Visits the links of node (slots l0 = link[lane], l1 = link[lane + 32], dg =
 // degree): collects the ids seen for the first time into ni[0..m) in link-slot
-// order and logs them (levels 1 and 2).  The lifted rows of the first 8 of
-// them are requested at once, one bulk copy per row into stage[slot],
-// completing on bar.  Returns m.
+// order and logs them (levels 1 and 2).  The lifted rows of the first
+// stage_rows of them are requested at once, one bulk copy per row into
+// stage[slot], completing on bar.  Returns m.
+template <uint32_t kDim>
 __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t l0, uint32_t l1, uint32_t dg,
                                                  Visited& vis, uint32_t& nlog, uint32_t* ni, uint32_t lane,
                                                  float* stage, uint64_t* bar) {
+    const uint32_t srows = kSearchRows<kDim> ? kSearchRows<kDim> : p.stage_rows;
     bool f0 = false, f1 = false, bad = false;
     uint32_t r0 = 0, r1 = 0;
     if (lane < dg) {
@@ -126,9 +134,9 @@ __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t
     const uint32_t m = c0 + __popc(b1);
     const uint32_t rb = p.lstride * 4;
     if (m) {
-        if (lane == 0) bar_expect(bar, min(m, 8u) * rb);
-        if (f0 && p0 < 8) bulk_row(stage + (size_t)p0 * p.lstride, p.lifted + (size_t)l0 * p.lstride, rb, bar);
-        if (f1 && p1 < 8) bulk_row(stage + (size_t)p1 * p.lstride, p.lifted + (size_t)l1 * p.lstride, rb, bar);
+        if (lane == 0) bar_expect(bar, min(m, srows) * rb);
+        if (f0 && p0 < srows) bulk_row(stage + (size_t)p0 * p.lstride, p.lifted + (size_t)l0 * p.lstride, rb, bar);
+        if (f1 && p1 < srows) bulk_row(stage + (size_t)p1 * p.lstride, p.lifted + (size_t)l1 * p.lstride, rb, bar);
     }
     const bool logs = vis.level != 0;
     if (f0) {
@@ -152,20 +160,29 @@ __device__ __forceinline__ void load_links(const SearchParams& p, uint32_t node,
     l1 = lane + 32 < p.degree ? lk[lane + 32] : kEmpty;
 }
 
-// Distances of the m fresh neighbours to the lifted query: 8 groups of 4
-// lanes, each reducing its row in the reference's lane order.  Rows arrive by
-// bulk copy, 8 per round (the first round was requested by expand_links);
-// each round is one phase of bar (parity ph).  Returns false when a wait ran
-// out (the error word is set).
+// Distance of staged row `row` to the lifted query by a group of G threads
+// (thread gt of the group): the reference's lane order for G = 4, 8, 16.
+template <int G>
+__device__ __forceinline__ float row_l2sqr(const float* row, const float* qhat, uint32_t dim, uint32_t gt) {
+    if constexpr (G == 4) return group_l2sqr(row, qhat, dim, gt, kFull);
+    else return group_l2sqr_w<G>(row, qhat, dim, gt, kFull);
+}
+
+// Distances of the m fresh neighbours to the lifted query.  Rows arrive by
+// bulk copy, stage_rows per round (the first round was requested by
+// expand_links); each round is one phase of bar (parity ph).  Rows are
+// reduced by groups of 32 / stage_rows threads (4, 8 or 16: long rows are
+// staged 4 or 2 at a time).  Returns false when a wait ran out (the error
+// word is set).
 template <uint32_t kDim>
 __device__ __forceinline__ bool fresh_distances(const SearchParams& p, const float* qhat, const uint32_t* ni,
-                                                float* nd, uint32_t m, uint32_t gw, uint32_t gt, float* stage,
-                                                uint64_t* bar, uint32_t& ph, uint32_t lane) {
+                                                float* nd, uint32_t m, float* stage, uint64_t* bar, uint32_t& ph,
+                                                uint32_t lane) {
     const uint32_t dim = kDim ? kDim : p.dim;
+    const uint32_t srows = kSearchRows<kDim> ? kSearchRows<kDim> : p.stage_rows;
     const uint32_t rb = p.lstride * 4;
-    float* row = stage + (size_t)gw * p.lstride;
-    for (uint32_t r0 = 0; r0 < m; r0 += 8) {
-        const uint32_t nr = min(m - r0, 8u);
+    for (uint32_t r0 = 0; r0 < m; r0 += srows) {
+        const uint32_t nr = min(m - r0, srows);
         if (r0 > 0) {
             if (lane == 0) bar_expect(bar, nr * rb);
             if (lane < nr) bulk_row(stage + (size_t)lane * p.lstride, p.lifted + (size_t)ni[r0 + lane] * p.lstride, rb, bar);
@@ -175,9 +192,20 @@ __device__ __forceinline__ bool fresh_distances(const SearchParams& p, const flo
             return false;
         }
         ph ^= 1u;
-        const bool oka = gw < nr;
-        const float da = group_l2sqr(oka ? row : stage, qhat, dim, gt, kFull);
-        if (gt == 0 && oka) nd[r0 + gw] = da;
+        if (srows == 2) {
+            const uint32_t gw = lane >> 4, gt = lane & 15u;
+            const float da = row_l2sqr<16>(stage + (size_t)gw * p.lstride, qhat, dim, gt);
+            if (gt == 0 && gw < nr) nd[r0 + gw] = da;
+        } else if (srows == 4) {
+            const uint32_t gw = lane >> 3, gt = lane & 7u;
+            const float da = row_l2sqr<8>(stage + (size_t)gw * p.lstride, qhat, dim, gt);
+            if (gt == 0 && gw < nr) nd[r0 + gw] = da;
+        } else {
+            const uint32_t gw = lane >> 2, gt = lane & 3u;
+            const bool oka = gw < nr;
+            const float da = row_l2sqr<4>(oka ? stage + (size_t)gw * p.lstride : stage, qhat, dim, gt);
+            if (gt == 0 && oka) nd[r0 + gw] = da;
+        }
         __syncwarp();
     }
     return true;
@@ -208,10 +236,16 @@ __device__ __forceinline__ void append_in_range(const SearchParams& p, const flo
 
 extern __shared__ __align__(16) unsigned char g_smem[];
 
+// Rows per staging round: 8 rows of up to 1 KB, else 4 of up to 2 KB, else 2.
+__device__ __host__ __forceinline__ uint32_t stage_rows_for(uint32_t lstride, uint32_t bstride) {
+    const uint32_t w = lstride > bstride ? lstride : bstride;
+    return w <= 256 ? 8u : (w <= 512 ? 4u : 2u);
+}
+
 __device__ __host__ __forceinline__ size_t search_smem_words(uint32_t L_max, uint32_t lstride, uint32_t bstride,
                                                              uint32_t hash_cap) {
-    return (size_t)2 * L_max + 128 + lstride + bstride + 8 * (size_t)(lstride > bstride ? lstride : bstride) +
-           hash_cap + 8;
+    return (size_t)2 * L_max + 128 + lstride + bstride +
+           stage_rows_for(lstride, bstride) * (size_t)(lstride > bstride ? lstride : bstride) + hash_cap + 8;
 }
 
 template <uint32_t kDim>
@@ -226,8 +260,9 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
     uint32_t* bi = reinterpret_cast<uint32_t*>(bd + p.L_max);
     float* nd = reinterpret_cast<float*>(bi + p.L_max);
     uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 64);
-    float* stage = reinterpret_cast<float*>(ni + 64);  // 8 staged rows of max(lstride, bstride)
-    uint32_t* tab = reinterpret_cast<uint32_t*>(stage + 8 * (size_t)max(p.lstride, p.bstride));
+    float* stage = reinterpret_cast<float*>(ni + 64);  // stage_rows staged rows of max(lstride, bstride)
+    const uint32_t srows = kSearchRows<kDim> ? kSearchRows<kDim> : p.stage_rows;
+    uint32_t* tab = reinterpret_cast<uint32_t*>(stage + srows * (size_t)max(p.lstride, p.bstride));
     uint64_t* bar = reinterpret_cast<uint64_t*>(tab + p.hash_cap);  // row-copy mbarrier of this warp
     uint32_t ph = 0;
     if (lane == 0) {
@@ -322,10 +357,10 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
                 load_links(p, pre_node, lane, pl0, pl1, pdg);
             }
             vis_room(vis, nlog, p.degree, lane, p.err);
-            const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane, stage, bar);
+            const uint32_t m = expand_links<kDim>(p, l0, l1, dg, vis, nlog, ni, lane, stage, bar);
             uint32_t mk = 0;
             if (m != 0) {
-                if (!fresh_distances<kDim>(p, qhat, ni, nd, m, gw, gt, stage, bar, ph, lane)) return;
+                if (!fresh_distances<kDim>(p, qhat, ni, nd, m, stage, bar, ph, lane)) return;
                 append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
                 const bool full = size >= L;
                 mk = sort_fresh_kept(nd, ni, m, full, full ? bd[L - 1] : 0.f, full ? bi[L - 1] : 0u, lane);
@@ -408,9 +443,9 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
                 load_links(p, pre_node, lane, pl0, pl1, pdg);
             }
             vis_room(vis, nlog, p.degree, lane, p.err);
-            const uint32_t m = expand_links(p, l0, l1, dg, vis, nlog, ni, lane, stage, bar);
+            const uint32_t m = expand_links<kDim>(p, l0, l1, dg, vis, nlog, ni, lane, stage, bar);
             if (m == 0) continue;
-            if (!fresh_distances<kDim>(p, qhat, ni, nd, m, gw, gt, stage, bar, ph, lane)) return;
+            if (!fresh_distances<kDim>(p, qhat, ni, nd, m, stage, bar, ph, lane)) return;
             append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
         }
         if (overflow && lane == 0) set_error(p.err, kDevCandOverflow);
@@ -431,20 +466,26 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
         const float qn = group_ip(qraw, qraw, p.d, gt, kFull);
         const float* thr = p.thr + (size_t)tslot * p.n;
         uint32_t npred = 0;
-        float* brow = stage + (size_t)gw * max(p.lstride, p.bstride);
-        for (uint32_t r0 = 0; r0 < ncand; r0 += 8) {
-            const uint32_t idx = r0 + gw;
+        // base rows in rounds of srows, G = 32 / srows threads per row
+        const uint32_t G = srows == 8 ? 4u : (srows == 4 ? 8u : 16u);
+        const uint32_t pg = srows == 8 ? lane >> 2 : (srows == 4 ? lane >> 3 : lane >> 4), pt = lane & (G - 1);
+        float* brow = stage + (size_t)pg * max(p.lstride, p.bstride);
+        for (uint32_t r0 = 0; r0 < ncand; r0 += srows) {
+            const uint32_t idx = r0 + pg;
             const bool ok = idx < ncand;
             const uint32_t o = cl[ok ? idx : r0];
-            if (ok) stage_row_async(brow, p.base + (size_t)o * p.bstride, p.bstride, gt, 4);
+            if (ok) stage_row_async(brow, p.base + (size_t)o * p.bstride, p.bstride, pt, G);
             cp_async_wait_all();
             __syncwarp();
-            const float ip = group_ip(ok ? brow : stage, qraw, p.d, gt, kFull);
+            const float* rr = ok ? brow : stage;
+            const float ip = G == 4 ? group_ip(rr, qraw, p.d, pt, kFull)
+                                    : (G == 8 ? group_ip_w<8>(rr, qraw, p.d, pt, kFull)
+                                              : group_ip_w<16>(rr, qraw, p.d, pt, kFull));
             const float key = __fsub_rn(__fadd_rn(p.onorm[o], qn), __fmul_rn(2.0f, ip));
             const bool pass = ok && (double)key <= (double)thr[o];
-            const unsigned b = __ballot_sync(kFull, pass && gt == 0);
+            const unsigned b = __ballot_sync(kFull, pass && pt == 0);
             __syncwarp();
-            if (pass && gt == 0) cl[npred + __popc(b & lanemask_lt())] = o;
+            if (pass && pt == 0) cl[npred + __popc(b & lanemask_lt())] = o;
             npred += __popc(b);
             __syncwarp();
         }
@@ -909,6 +950,7 @@ static int enqueue_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, boo
     p.bstride = ix.bstride;
     p.degree = ix.degree;
     p.troot = ix.troot;
+    p.stage_rows = stage_rows_for(ix.lstride, ix.bstride);
     p.scale = ix.scale;
     p.R2 = ix.mstar2 + 1.0;  // rknn_query.cpp:2729, eps = 0
     p.thr = c->thr_table.as<float>();

@@ -53,6 +53,10 @@ int anqi_timer_stop(anqi_ctx* ctx, float* ms);
  * out[i] = l2sqr(a_i, b_i) / ip(a_i, b_i) for m pairs of dim floats. */
 int anqi_pair_distances(anqi_ctx* ctx, const float* a, const float* b, uint64_t m, uint32_t dim,
                         float* l2sqr, float* ip);
+/* The same with `group` = 4, 8 or 16 threads per pair: the forms the kernels
+ * use for many short rows, few rows and long rows; identical results. */
+int anqi_pair_distances_group(anqi_ctx* ctx, const float* a, const float* b, uint64_t m, uint32_t dim,
+                              uint32_t group, float* l2sqr, float* ip);
 
 /* ------------------------------------------------------------------ LRQ
  * CompactLrqVerifier::build, floor policy, u8 codes (src/rknn_query.cpp:679-720):

@@ -28,10 +28,12 @@ def csr_rows(off, ids):
     return [ids[int(off[i]):int(off[i + 1])] for i in range(len(off) - 1)]
 
 
-def test_pair_distances_bit_exact(ctx):
+@pytest.mark.parametrize("group", [4, 8, 16])
+def test_pair_distances_bit_exact(ctx, group):
+    """The reference's AVX-512 order with 4, 8 or 16 threads per pair."""
     z = np.load(GOLDEN / "dist.npz")
     for dim in (8, 10, 16, 32, 34, 128, 130, 962):
-        l2, ip = ctx.pair_distances(z[f"a_{dim}"], z[f"b_{dim}"])
+        l2, ip = ctx.pair_distances(z[f"a_{dim}"], z[f"b_{dim}"], group)
         assert np.array_equal(bits(l2), bits(z[f"l2_{dim}"])), dim
         assert np.array_equal(bits(ip), bits(z[f"ip_{dim}"])), dim
 
@@ -182,16 +184,41 @@ def test_query_bit_exact_vs_oracle_random(ctx, random_index, table, monkeypatch)
                 assert np.array_equal(r.pred(i), preds[i]), (k, L, i)
 
 
-@pytest.fixture(scope="module")
-def random_index_128():
-    return _random_index(n=4000, d=128, nq=200, seed=23)
+def _gpu_built_index(ctx, n, d, nq, seed):
+    """L2-normalised N(0,1) rows (the 960-d shape); the G48 graph and entry tree
+    built by the GPU builders (their parity is tested on their own); the
+    query stage is then compared with the oracle on that index."""
+    from anqi import pipeline
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(n + nq, d)).astype(np.float32)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    base, query = np.ascontiguousarray(x[:n]), np.ascontiguousarray(x[n:])
+    nrm = ol.norms(base)
+    d2 = nrm[:, None] + nrm[None, :] - 2.0 * (base.astype(np.float64) @ base.T)
+    np.fill_diagonal(d2, np.inf)
+    knn = np.argsort(d2, axis=1)[:, :100].astype(np.uint32)
+    radius = np.take_along_axis(d2, knn[:, 99:100].astype(np.int64), 1)[:, 0].astype(np.float32)
+    lifted, m2, sc = ctx.lift(base, radius)
+    deg, links, tree, _ = pipeline.graph_build(ctx, lifted, knn)
+    thr = {k: np.take_along_axis(d2, np.argsort(d2, axis=1)[:, k - 1:k], 1)[:, 0].astype(np.float32)
+           for k in (10, 50, 100)}
+    return base, query, lifted, links, deg, tree, sc, m2, thr
 
 
-def test_query_bit_exact_vs_oracle_d128(ctx, random_index_128):
+@pytest.fixture(scope="module", params=[128, 960])
+def random_index_wide(request, ctx):
+    d = request.param
+    if d == 128:
+        return _random_index(n=4000, d=d, nq=200, seed=23)
+    return _gpu_built_index(ctx, 3000, d, 100, seed=29)
+
+
+def test_query_bit_exact_vs_oracle_wide(ctx, random_index_wide):
     """d = 128 (lifted dimension 130) runs the search kernel instance whose
-    distance loops are unrolled at compile time: same candidates, #dist and
+    distance loops are unrolled at compile time; d = 960 stages two long rows
+    per round, reduced by 16-thread groups: same candidates, #dist and
     verified lists as the oracle."""
-    base, query, lifted, links, deg, tree, sc, m2, thr = random_index_128
+    base, query, lifted, links, deg, tree, sc, m2, thr = random_index_wide
     ctx.index_load(base, lifted, deg, links, tree, sc, m2)
     ta = ol.TreeArrays(tree.left, tree.right, tree.offset, tree.hyperplane, tree.leaf_first())
     for k in (10, 100):
