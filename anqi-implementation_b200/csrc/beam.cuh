@@ -157,19 +157,20 @@ __device__ __forceinline__ void vis_release(Visited& v, const VisitSlot& vs, uin
 // common case after the first expansions) are ranked by counting over the kept
 // entries only; larger ones use the register bitonic network, after which the
 // kept entries are a prefix.
+template <class Ord = IdOrder>
 __device__ __forceinline__ uint32_t sort_fresh_kept(float* nd, uint32_t* ni, uint32_t m, bool full, float td,
-                                                    uint32_t tid, uint32_t lane) {
+                                                    uint32_t tid, uint32_t lane, Ord ord = Ord()) {
     if (m <= 32) {
         const float dv = lane < m ? nd[lane] : 0.f;
         const uint32_t iv = lane < m ? ni[lane] : kEmpty;
-        const bool keep = lane < m && (!full || nb_less(dv, iv, td, tid));
+        const bool keep = lane < m && (!full || ord(dv, iv, td, tid));
         const unsigned km = __ballot_sync(kAll, keep);
         uint32_t rank = 0;
         for (unsigned r = km; r; r &= r - 1) {
             const int s = __ffs(r) - 1;
             const float ds = __shfl_sync(kAll, dv, s);
             const uint32_t is = __shfl_sync(kAll, iv, s);
-            rank += nb_less(ds, is, dv, iv) ? 1u : 0u;
+            rank += ord(ds, is, dv, iv) ? 1u : 0u;
         }
         __syncwarp();
         if (keep) {
@@ -184,14 +185,14 @@ __device__ __forceinline__ uint32_t sort_fresh_kept(float* nd, uint32_t* ni, uin
     uint32_t i0 = lane < m ? ni[lane] : kEmpty;
     float d1 = lane + 32 < m ? nd[lane + 32] : inf;
     uint32_t i1 = lane + 32 < m ? ni[lane + 32] : kEmpty;
-    warp_sort64(d0, i0, d1, i1);
+    warp_sort64(d0, i0, d1, i1, ord);
     __syncwarp();
     nd[lane] = d0;
     ni[lane] = i0;
     nd[lane + 32] = d1;
     ni[lane + 32] = i1;
-    const bool k0 = lane < m && (!full || nb_less(d0, i0, td, tid));
-    const bool k1 = lane + 32 < m && (!full || nb_less(d1, i1, td, tid));
+    const bool k0 = lane < m && (!full || ord(d0, i0, td, tid));
+    const bool k1 = lane + 32 < m && (!full || ord(d1, i1, td, tid));
     const uint32_t kept = __popc(__ballot_sync(kAll, k0)) + __popc(__ballot_sync(kAll, k1));
     __syncwarp();
     return kept;

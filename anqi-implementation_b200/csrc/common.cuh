@@ -257,14 +257,35 @@ __device__ __forceinline__ bool nb_less(float da, uint32_t ia, float db, uint32_
     return da < db || (da == db && (ia & kIdMask) < (ib & kIdMask));
 }
 
+// The (dist, id) order as a functor: ids compared directly ...
+struct IdOrder {
+    __device__ __forceinline__ bool operator()(float da, uint32_t ia, float db, uint32_t ib) const {
+        return nb_less(da, ia, db, ib);
+    }
+};
+
+// ... or, for objects renumbered for locality, through their original ids
+// (perm: new id -> original id), so ties break exactly as in the original
+// numbering.  The lookup happens only on equal distances.
+struct PermOrder {
+    const uint32_t* perm;
+    __device__ __forceinline__ bool operator()(float da, uint32_t ia, float db, uint32_t ib) const {
+        if (da != db) return da < db;
+        const uint32_t a = ia & kIdMask, b = ib & kIdMask;
+        if (a == b) return false;  // also two pads (+inf, kEmpty)
+        return perm[a] < perm[b];
+    }
+};
+
 // Plain (key, id) lexicographic order on full 32-bit ids (std::pair order).
 __device__ __forceinline__ bool kv_less(float da, uint32_t ia, float db, uint32_t ib) {
     return da < db || (da == db && ia < ib);
 }
 
 // Bitonic sort of 64 (d, id) pairs held two per lane (index lane and lane+32),
-// ascending in nb_less order.  Pads must be (+inf, kEmpty).
-__device__ __forceinline__ void warp_sort64(float& d0, uint32_t& i0, float& d1, uint32_t& i1) {
+// ascending in the order ord (nb_less by default).  Pads must be (+inf, kEmpty).
+template <class Ord = IdOrder>
+__device__ __forceinline__ void warp_sort64(float& d0, uint32_t& i0, float& d1, uint32_t& i1, Ord ord = Ord()) {
     const uint32_t lane = threadIdx.x & 31u;
     // element e = lane (slot 0) and e = lane + 32 (slot 1)
 #pragma unroll
@@ -274,7 +295,7 @@ __device__ __forceinline__ void warp_sort64(float& d0, uint32_t& i0, float& d1, 
             if (j == 32) {
                 // partner of slot 0 is slot 1 of the same lane
                 bool up = ((lane & k) == 0);  // k == 64 here -> always ascending
-                bool sw = up ? nb_less(d1, i1, d0, i0) : nb_less(d0, i0, d1, i1);
+                bool sw = up ? ord(d1, i1, d0, i0) : ord(d0, i0, d1, i1);
                 if (sw) {
                     float td = d0; d0 = d1; d1 = td;
                     uint32_t ti = i0; i0 = i1; i1 = ti;
@@ -290,7 +311,7 @@ __device__ __forceinline__ void warp_sort64(float& d0, uint32_t& i0, float& d1, 
                     const bool lower = (e & j) == 0;
                     const bool up = (e & k) == 0;
                     // keep the smaller if (lower == up)
-                    bool other_less = nb_less(od, oi, d, id);
+                    bool other_less = ord(od, oi, d, id);
                     bool take = (lower == up) ? other_less : !other_less;
                     // ties cannot occur between distinct entries (total order)
                     if (take) {
@@ -304,11 +325,13 @@ __device__ __forceinline__ void warp_sort64(float& d0, uint32_t& i0, float& d1, 
 }
 
 // Number of entries in sorted a[0..n) strictly less than (d, id).
-__device__ __forceinline__ uint32_t lower_rank(const float* ad, const uint32_t* ai, uint32_t n, float d, uint32_t id) {
+template <class Ord = IdOrder>
+__device__ __forceinline__ uint32_t lower_rank(const float* ad, const uint32_t* ai, uint32_t n, float d, uint32_t id,
+                                               Ord ord = Ord()) {
     uint32_t lo = 0, hi = n;
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
-        if (nb_less(ad[mid], ai[mid], d, id)) lo = mid + 1;
+        if (ord(ad[mid], ai[mid], d, id)) lo = mid + 1;
         else hi = mid;
     }
     return lo;

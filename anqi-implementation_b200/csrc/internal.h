@@ -42,6 +42,10 @@ struct QueryIndex {
     double scale = 0, mstar2 = 0;
     DevBuf base, lifted, onorm, deg, links;
     DevBuf tleft, tright, toffset, thyper, tleaf;
+    // objects are held renumbered in breadth-first order of the graph:
+    // perm[new id] = original id (base, lifted, norms, graph, entries and
+    // thresholds are stored by new id; results are returned as original ids)
+    DevBuf perm;
 };
 
 struct Verifier {
@@ -103,7 +107,7 @@ struct Ctx {
     uint64_t device_bytes = 0;
     std::vector<DevBuf*> member_bufs() {
         return {&ix.base, &ix.lifted, &ix.onorm, &ix.deg, &ix.links, &ix.tleft, &ix.tright, &ix.toffset,
-                &ix.thyper, &ix.tleaf, &vf.coeff, &vf.codes_t, &vf.mu, &vf.basis, &vf.codebook, &batch.q,
+                &ix.thyper, &ix.tleaf, &ix.perm, &vf.coeff, &vf.codes_t, &vf.mu, &vf.basis, &vf.codebook, &batch.q,
                 &batch.qL, &batch.qslot, &batch.npred, &batch.ncand, &batch.ndist, &batch.nexp, &batch.nflood,
                 &batch.pred_at, &batch.cand_at, &batch.pred_buf, &batch.cand_buf, &batch.pred_off,
                 &batch.cand_off, &batch.pred_csr, &batch.cand_csr, &err, &counters, &vis_bits, &vis_log,

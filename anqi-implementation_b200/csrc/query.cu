@@ -46,6 +46,7 @@ struct SearchParams {
     const float* thr;  // slot-major thresholds
     const float* queries;
     const uint32_t* entry;  // entry object per query (rknn_entry_kernel)
+    const uint32_t* perm;   // object id -> original id (objects are renumbered for locality)
     const uint32_t* order;  // work item -> query (leaf-ordered), or null for identity
     const uint32_t* qL;
     const uint8_t* qslot;
@@ -107,24 +108,45 @@ __device__ __forceinline__ void bar_expect(uint64_t* bar, uint32_t bytes) {
 
 constexpr uint32_t kRowWaitPolls = 1u << 24;
 
+// Objects are numbered in breadth-first order of the graph (anqi_index_load),
+// so a query's visits fall mostly near its entry object.  A per-warp bitmap
+// in shared memory covers the kWinBits ids around the entry; visits outside
+// it go to the visited tables.
+constexpr uint32_t kWinBits = 4096;
+constexpr uint32_t kWinWords = kWinBits / 32;
+
 // Visits the links of node (slots l0 = link[lane], l1 = link[lane + 32], dg =
 // degree): collects the ids seen for the first time into ni[0..m) in link-slot
-// order and logs them (levels 1 and 2).  The lifted rows of the first
+// order and logs the table visits (levels 1 and 2).  The lifted rows of the first
 // stage_rows of them are requested at once, one bulk copy per row into
 // stage[slot], completing on bar.  Returns m.
+// A first visit of id in the window bitmap (win covers [wbase, wbase +
+// kWinBits)) or else in the visited tables; `logged` tells which.
+__device__ __forceinline__ bool visit_id(Visited& vis, uint32_t* win, uint32_t wbase, uint32_t id, uint32_t& rec,
+                                         bool& logged, uint32_t* err) {
+    const uint32_t w = id - wbase;
+    if (w < kWinBits) {
+        logged = false;
+        const uint32_t bit = 1u << (w & 31u);
+        return (atomicOr(win + (w >> 5), bit) & bit) == 0u;
+    }
+    logged = true;
+    return vis_first(vis, id, rec, err);
+}
+
 template <uint32_t kDim>
 __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t l0, uint32_t l1, uint32_t dg,
                                                  Visited& vis, uint32_t& nlog, uint32_t* ni, uint32_t lane,
-                                                 float* stage, uint64_t* bar) {
+                                                 float* stage, uint64_t* bar, uint32_t* win, uint32_t wbase) {
     const uint32_t srows = kSearchRows<kDim> ? kSearchRows<kDim> : p.stage_rows;
-    bool f0 = false, f1 = false, bad = false;
+    bool f0 = false, f1 = false, bad = false, g0 = false, g1 = false;
     uint32_t r0 = 0, r1 = 0;
     if (lane < dg) {
-        if (l0 < p.n) f0 = vis_first(vis, l0, r0, p.err);
+        if (l0 < p.n) f0 = visit_id(vis, win, wbase, l0, r0, g0, p.err);
         else bad = true;
     }
     if (lane + 32 < dg) {
-        if (l1 < p.n) f1 = vis_first(vis, l1, r1, p.err);
+        if (l1 < p.n) f1 = visit_id(vis, win, wbase, l1, r1, g1, p.err);
         else bad = true;
     }
     if (bad) set_error(p.err, kDevBadId);
@@ -132,6 +154,9 @@ __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t
     const uint32_t c0 = __popc(b0), lt = lanemask_lt();
     const uint32_t p0 = __popc(b0 & lt), p1 = c0 + __popc(b1 & lt);
     const uint32_t m = c0 + __popc(b1);
+    // table visits are logged for the clean-up (window visits are not)
+    const unsigned h0 = __ballot_sync(kFull, f0 && g0), h1 = __ballot_sync(kFull, f1 && g1);
+    const uint32_t q0 = __popc(h0 & lt), q1 = __popc(h0) + __popc(h1 & lt);
     const uint32_t rb = p.lstride * 4;
     if (m) {
         if (lane == 0) bar_expect(bar, min(m, srows) * rb);
@@ -141,13 +166,13 @@ __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t
     const bool logs = vis.level != 0;
     if (f0) {
         ni[p0] = l0;
-        if (logs && nlog + p0 < p.log_cap) vis.vlog[nlog + p0] = r0;
+        if (g0 && logs && nlog + q0 < p.log_cap) vis.vlog[nlog + q0] = r0;
     }
     if (f1) {
         ni[p1] = l1;
-        if (logs && nlog + p1 < p.log_cap) vis.vlog[nlog + p1] = r1;
+        if (g1 && logs && nlog + q1 < p.log_cap) vis.vlog[nlog + q1] = r1;
     }
-    nlog += m;
+    nlog += __popc(h0) + __popc(h1);
     __syncwarp();
     return m;
 }
@@ -244,7 +269,7 @@ __device__ __host__ __forceinline__ uint32_t stage_rows_for(uint32_t lstride, ui
 
 __device__ __host__ __forceinline__ size_t search_smem_words(uint32_t L_max, uint32_t lstride, uint32_t bstride,
                                                              uint32_t hash_cap) {
-    return (size_t)2 * L_max + 128 + lstride + bstride +
+    return (size_t)2 * L_max + 128 + lstride + kWinWords +
            stage_rows_for(lstride, bstride) * (size_t)(lstride > bstride ? lstride : bstride) + hash_cap + 8;
 }
 
@@ -255,8 +280,8 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
     const size_t per_warp = search_smem_words(p.L_max, p.lstride, p.bstride, p.hash_cap) * 4;
     unsigned char* my = g_smem + wib * per_warp;
     float* qhat = reinterpret_cast<float*>(my);
-    float* qraw = qhat + p.lstride;
-    float* bd = qraw + p.bstride;  // the beam: sorted (dist, id), expanded flag in the id's top bit
+    uint32_t* win = reinterpret_cast<uint32_t*>(qhat + p.lstride);  // window bitmap, kWinWords
+    float* bd = reinterpret_cast<float*>(win + kWinWords);  // the beam: sorted (dist, id), expanded flag in the id's top bit
     uint32_t* bi = reinterpret_cast<uint32_t*>(bd + p.L_max);
     float* nd = reinterpret_cast<float*>(bi + p.L_max);
     uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 64);
@@ -275,7 +300,9 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
     uint32_t* cl = p.cand_scratch + (size_t)slot * p.cand_cap;
     VisitSlot vs{bits, vlog, p.log_cap, p.vis_words};
     for (uint32_t t = lane; t < p.hash_cap; t += 32) tab[t] = kEmpty;
+    for (uint32_t t = lane; t < kWinWords; t += 32) win[t] = 0u;
     __syncwarp();
+    const PermOrder ord{p.perm};
 
     for (;;) {
         uint32_t w = 0;
@@ -287,7 +314,6 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
         const uint32_t tslot = p.qslot ? p.qslot[qi] : p.slot_all;
         const float* q = p.queries + (size_t)qi * p.bstride;
         // query lift, rknn_query.cpp:2724-2729
-        for (uint32_t j = lane; j < p.bstride; j += 32) qraw[j] = q[j];
         for (uint32_t j = lane; j < p.lstride; j += 32) {
             float v = 0.0f;
             if (j < p.d) v = __double2float_rn(__dmul_rn((double)q[j], p.scale));
@@ -297,6 +323,10 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
         __syncwarp();
         uint32_t ep = p.entry[qi];
         if (ep >= p.n) ep = 0;
+        // the window of ids around the entry object
+        uint32_t wbase = ep > kWinBits / 2 ? ep - kWinBits / 2 : 0u;
+        if (p.n <= kWinBits) wbase = 0;
+        else if ((uint64_t)wbase > p.n - kWinBits) wbase = (uint32_t)(p.n - kWinBits);
 
         Visited vis{tab,  p.hash_cap, p.hash_shift, p.gtab ? p.gtab + (size_t)slot * p.gcap : nullptr,
                     p.gcap, p.gshift, bits, vlog, p.log_cap, p.hash_cap ? 0u : (p.gcap ? 1u : 2u)};
@@ -306,13 +336,11 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
         const float dep = group_l2sqr(stage, qhat, p.dim, gt, kFull);
         __syncwarp();
         if (lane == 0) {
-            uint32_t rec = ep;
-            vis_first(vis, ep, rec, p.err);
-            if (vis.level != 0 && p.log_cap) vlog[0] = rec;
+            win[(ep - wbase) >> 5] |= 1u << ((ep - wbase) & 31u);  // the entry lies in the window
             bd[0] = dep;
             bi[0] = ep;
         }
-        uint32_t nlog = 1, ncand = 0, nexp = 0, nfl = 0;
+        uint32_t nlog = 0, nvis = 1, ncand = 0, nexp = 0, nfl = 0;
         bool overflow = false;
         if ((double)dep <= p.R2) {
             if (lane == 0) cl[0] = ep;
@@ -357,13 +385,14 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
                 load_links(p, pre_node, lane, pl0, pl1, pdg);
             }
             vis_room(vis, nlog, p.degree, lane, p.err);
-            const uint32_t m = expand_links<kDim>(p, l0, l1, dg, vis, nlog, ni, lane, stage, bar);
+            const uint32_t m = expand_links<kDim>(p, l0, l1, dg, vis, nlog, ni, lane, stage, bar, win, wbase);
+            nvis += m;
             uint32_t mk = 0;
             if (m != 0) {
                 if (!fresh_distances<kDim>(p, qhat, ni, nd, m, stage, bar, ph, lane)) return;
                 append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
                 const bool full = size >= L;
-                mk = sort_fresh_kept(nd, ni, m, full, full ? bd[L - 1] : 0.f, full ? bi[L - 1] : 0u, lane);
+                mk = sort_fresh_kept(nd, ni, m, full, full ? bd[L - 1] : 0.f, full ? bi[L - 1] : 0u, lane, ord);
             }
             if (mk == 0) {
                 // no fresh entry enters the beam: only the cursor moves (to
@@ -376,8 +405,8 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
             // beam entry j at j + (fresh entries before it); only entries from
             // cn (the rank of the best fresh one) on move.
             uint32_t r0 = 0, r1 = 0;
-            if (lane < mk) r0 = lower_rank(bd, bi, size, nd[lane], ni[lane]);
-            if (lane + 32 < mk) r1 = lower_rank(bd, bi, size, nd[lane + 32], ni[lane + 32]);
+            if (lane < mk) r0 = lower_rank(bd, bi, size, nd[lane], ni[lane], ord);
+            if (lane + 32 < mk) r1 = lower_rank(bd, bi, size, nd[lane + 32], ni[lane + 32], ord);
             const uint32_t cn = __shfl_sync(kFull, r0, 0);
             const uint32_t ns = min(L, size + mk);
             // first unexpanded entry of the merged beam: the old beam's next
@@ -399,7 +428,7 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
                 if (mv) {
                     dv = bd[j];
                     iv = bi[j];
-                    pos = j + lower_rank(nd, ni, mk, dv, iv);
+                    pos = j + lower_rank(nd, ni, mk, dv, iv, ord);
                 }
                 __syncwarp();
                 if (pos < ns) {
@@ -443,7 +472,8 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
                 load_links(p, pre_node, lane, pl0, pl1, pdg);
             }
             vis_room(vis, nlog, p.degree, lane, p.err);
-            const uint32_t m = expand_links<kDim>(p, l0, l1, dg, vis, nlog, ni, lane, stage, bar);
+            const uint32_t m = expand_links<kDim>(p, l0, l1, dg, vis, nlog, ni, lane, stage, bar, win, wbase);
+            nvis += m;
             if (m == 0) continue;
             if (!fresh_distances<kDim>(p, qhat, ni, nd, m, stage, bar, ph, lane)) return;
             append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
@@ -459,11 +489,11 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
             }
             cat = __shfl_sync(kFull, cat, 0);
             if (cat + ncand <= p.cand_out_cap)
-                for (uint32_t i = lane; i < ncand; i += 32) p.cand_buf[cat + i] = cl[i];
+                for (uint32_t i = lane; i < ncand; i += 32) p.cand_buf[cat + i] = p.perm[cl[i]];
             __syncwarp();
         }
         // rknn_query.cpp:2555-2561: key = IP(o,o) + IP(q,q) - 2 IP(o,q) <= (double) thr[o]
-        const float qn = group_ip(qraw, qraw, p.d, gt, kFull);
+        const float qn = group_ip(q, q, p.d, gt, kFull);
         const float* thr = p.thr + (size_t)tslot * p.n;
         uint32_t npred = 0;
         // base rows in rounds of srows, G = 32 / srows threads per row
@@ -478,9 +508,9 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
             cp_async_wait_all();
             __syncwarp();
             const float* rr = ok ? brow : stage;
-            const float ip = G == 4 ? group_ip(rr, qraw, p.d, pt, kFull)
-                                    : (G == 8 ? group_ip_w<8>(rr, qraw, p.d, pt, kFull)
-                                              : group_ip_w<16>(rr, qraw, p.d, pt, kFull));
+            const float ip = G == 4 ? group_ip(rr, q, p.d, pt, kFull)
+                                    : (G == 8 ? group_ip_w<8>(rr, q, p.d, pt, kFull)
+                                              : group_ip_w<16>(rr, q, p.d, pt, kFull));
             const float key = __fsub_rn(__fadd_rn(p.onorm[o], qn), __fmul_rn(2.0f, ip));
             const bool pass = ok && (double)key <= (double)thr[o];
             const unsigned b = __ballot_sync(kFull, pass && pt == 0);
@@ -495,7 +525,7 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
             if (at + npred > p.pred_cap) set_error(p.err, kDevOutOverflow);
             p.npred[qi] = npred;
             p.ncand[qi] = ncand;
-            p.ndist[qi] = nlog;
+            p.ndist[qi] = nvis;
             p.nexp[qi] = nexp;
             p.nflood[qi] = nfl;
             p.pred_at[qi] = at;
@@ -503,9 +533,10 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
         }
         at = __shfl_sync(kFull, at, 0);
         if (at + npred <= p.pred_cap)
-            for (uint32_t i = lane; i < npred; i += 32) p.pred_buf[at + i] = cl[i];
+            for (uint32_t i = lane; i < npred; i += 32) p.pred_buf[at + i] = p.perm[cl[i]];
         vis_release(vis, vs, nlog, lane);
         for (uint32_t t = lane; t < p.hash_cap; t += 32) tab[t] = kEmpty;
+        for (uint32_t t = lane; t < kWinWords; t += 32) win[t] = 0u;
         __syncwarp();
     }
 }
@@ -680,6 +711,26 @@ __global__ void eval_sums_kernel(const double* __restrict__ rows, const uint32_t
     }
 }
 
+// dst[i] = src[perm[i]] for rows of `stride` floats (warp per row).
+__global__ void permute_rows_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                                    const uint32_t* __restrict__ perm, uint64_t n, uint32_t stride) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = w0; i < n; i += nw) {
+        const float4* s4 = reinterpret_cast<const float4*>(src + (uint64_t)perm[i] * stride);
+        float4* d4 = reinterpret_cast<float4*>(dst + i * stride);
+        for (uint32_t t = lane; t < stride / 4; t += 32) d4[t] = s4[t];
+    }
+}
+
+// dst[i] = src[perm[i]] for one value per object.
+__global__ void permute_vals_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                                    const uint32_t* __restrict__ perm, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = src[perm[i]];
+}
+
 static int slot_for_k(Ctx* c, uint32_t k) {
     for (int s = 0; s < Ctx::kThrSlots; s++)
         if (c->thr_k[s] == k) return s;
@@ -775,15 +826,66 @@ int anqi_index_load(anqi_ctx* h, const anqi_index_desc* x) {
     ix.scale = x->scale;
     ix.mstar2 = x->mstar2;
     int rc;
-    if ((rc = upload_padded(c, ix.base, x->base, x->n, x->d, ix.bstride)) ||
-        (rc = upload_padded(c, ix.lifted, x->lifted, x->n, ix.dim, ix.lstride)) ||
-        (rc = ensure(c, ix.onorm, x->n * 4)) || (rc = h2d(c, ix.deg, x->deg, x->n * 4)) ||
-        (rc = h2d(c, ix.links, x->links, x->n * (size_t)x->degree * 4)) ||
+    // Renumber the objects in breadth-first order of the graph (from object 0,
+    // then from the smallest object not reached): a search's visits then fall
+    // on nearby numbers, which the search kernel's window bitmap exploits.
+    // ANQI_B200_RENUMBER=0 keeps the given order.
+    const uint64_t n = x->n;
+    std::vector<uint32_t> perm;
+    perm.reserve(n);
+    const char* ren = std::getenv("ANQI_B200_RENUMBER");
+    if (ren && ren[0] == '0') {
+        for (uint64_t i = 0; i < n; i++) perm.push_back((uint32_t)i);
+    } else {
+        std::vector<uint8_t> seen(n, 0);
+        uint64_t head = 0;
+        for (uint64_t s0 = 0; s0 < n; s0++) {
+            if (seen[s0]) continue;
+            seen[s0] = 1;
+            perm.push_back((uint32_t)s0);
+            while (head < perm.size()) {
+                const uint32_t u = perm[head++];
+                const uint32_t* lk = x->links + (uint64_t)u * x->degree;
+                for (uint32_t j = 0; j < x->deg[u]; j++)
+                    if (!seen[lk[j]]) {
+                        seen[lk[j]] = 1;
+                        perm.push_back(lk[j]);
+                    }
+            }
+        }
+    }
+    std::vector<uint32_t> rank(n), deg_r(n), links_r(n * (size_t)x->degree, kEmpty), leaf_r(x->tree_leaf_first,
+                                                                                         x->tree_leaf_first + x->tree_nodes);
+    for (uint64_t i = 0; i < n; i++) rank[perm[i]] = (uint32_t)i;
+    for (uint64_t i = 0; i < n; i++) {
+        const uint32_t o = perm[i];
+        deg_r[i] = x->deg[o];
+        const uint32_t* lk = x->links + (uint64_t)o * x->degree;
+        for (uint32_t j = 0; j < x->deg[o]; j++) links_r[i * x->degree + j] = rank[lk[j]];
+    }
+    for (uint32_t& e : leaf_r)
+        if (e < n) e = rank[e];
+    {
+        TmpBuf tb(c), tl(c);
+        if ((rc = upload_padded(c, tb, x->base, n, x->d, ix.bstride)) ||
+            (rc = upload_padded(c, tl, x->lifted, n, ix.dim, ix.lstride)) || (rc = h2d(c, ix.perm, perm.data(), n * 4)) ||
+            (rc = ensure(c, ix.base, n * (size_t)ix.bstride * 4)) || (rc = ensure(c, ix.lifted, n * (size_t)ix.lstride * 4)))
+            return rc;
+        const uint32_t blocks = c->sm_count * 8;
+        permute_rows_kernel<<<blocks, 256, 0, c->stream>>>(tb.as<float>(), ix.base.as<float>(), ix.perm.as<uint32_t>(),
+                                                           n, ix.bstride);
+        permute_rows_kernel<<<blocks, 256, 0, c->stream>>>(tl.as<float>(), ix.lifted.as<float>(),
+                                                           ix.perm.as<uint32_t>(), n, ix.lstride);
+        ANQI_CUDA(c, cudaGetLastError());
+        if ((rc = sync(c))) return rc;
+    }
+    if ((rc = ensure(c, ix.onorm, n * 4)) || (rc = h2d(c, ix.deg, deg_r.data(), n * 4)) ||
+        (rc = h2d(c, ix.links, links_r.data(), n * (size_t)x->degree * 4)) ||
         (rc = h2d(c, ix.tleft, x->tree_left, x->tree_nodes * 4)) ||
         (rc = h2d(c, ix.tright, x->tree_right, x->tree_nodes * 4)) ||
         (rc = h2d(c, ix.toffset, x->tree_offset, x->tree_nodes * 4)) ||
         (rc = upload_padded(c, ix.thyper, x->tree_hyperplane, x->tree_nodes, ix.dim, ix.lstride)) ||
-        (rc = h2d(c, ix.tleaf, x->tree_leaf_first, x->tree_nodes * 4)))
+        (rc = h2d(c, ix.tleaf, leaf_r.data(), x->tree_nodes * 4)))
         return rc;
     if ((rc = compute_norms_device(c, ix.base.as<float>(), x->n, x->d, ix.bstride, ix.onorm.as<float>()))) return rc;
     if ((rc = sync(c))) return rc;
@@ -800,8 +902,12 @@ int anqi_set_thresholds(anqi_ctx* h, uint32_t k, const float* thr) {
     int rc = ensure_thr_table(c, c->ix.n);
     if (rc) return rc;
     const int s = claim_slot(c, k);
-    ANQI_CUDA(c, cudaMemcpyAsync(c->thr_table.as<float>() + (size_t)s * c->ix.n, thr, c->ix.n * 4,
-                                 cudaMemcpyHostToDevice, c->stream));
+    // stored by object number (objects are renumbered)
+    TmpBuf t(c);
+    if ((rc = h2d(c, t, thr, c->ix.n * 4))) return rc;
+    permute_vals_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(t.as<float>(), c->thr_table.as<float>() + (size_t)s * c->ix.n,
+                                                               c->ix.perm.as<uint32_t>(), c->ix.n);
+    ANQI_CUDA(c, cudaGetLastError());
     if ((rc = sync(c))) return rc;
     c->thr_k[s] = k;
     return ANQI_OK;
@@ -819,8 +925,12 @@ int anqi_verifier_materialize(anqi_ctx* h, uint32_t k, double radius_scale) {
     if (rc) return rc;
     const int s = claim_slot(c, k);
     c->thr_k[s] = 0;
-    if ((rc = lrq_materialize_device(c, c->vf, k, radius_scale, c->thr_table.as<float>() + (size_t)s * c->ix.n)))
+    TmpBuf t(c);
+    if ((rc = ensure(c, t, c->ix.n * 4)) || (rc = lrq_materialize_device(c, c->vf, k, radius_scale, t.as<float>())))
         return rc;
+    permute_vals_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(t.as<float>(), c->thr_table.as<float>() + (size_t)s * c->ix.n,
+                                                               c->ix.perm.as<uint32_t>(), c->ix.n);
+    ANQI_CUDA(c, cudaGetLastError());
     if ((rc = sync(c))) return rc;
     c->thr_k[s] = k;
     return ANQI_OK;
@@ -956,6 +1066,7 @@ static int enqueue_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, boo
     p.thr = c->thr_table.as<float>();
     p.queries = b.q.as<float>();
     p.entry = b.entry.as<uint32_t>();
+    p.perm = ix.perm.as<uint32_t>();
     p.order = b.ordered ? b.order.as<uint32_t>() : nullptr;
     p.qL = b.has_L ? b.qL.as<uint32_t>() : nullptr;
     p.qslot = b.has_k ? b.qslot.as<uint8_t>() : nullptr;
