@@ -150,6 +150,32 @@ __device__ __forceinline__ void vis_release(Visited& v, const VisitSlot& vs, uin
     }
 }
 
+// Window bitmap: when objects are numbered for locality (graph or RP-tree
+// order), one search's visits fall mostly within a few thousand ids of where
+// it starts.  A per-warp bitmap in shared memory covers kWinBits ids from
+// wbase; visits outside it go to the visited tables.
+constexpr uint32_t kWinBits = 4096;
+constexpr uint32_t kWinWords = kWinBits / 32;
+
+// Visits the links of node (slots l0 = link[lane], l1 = link[lane + 32], dg =
+// degree): collects the ids seen for the first time into ni[0..m) in link-slot
+// order and logs the table visits (levels 1 and 2).  The lifted rows of the first
+// stage_rows of them are requested at once, one bulk copy per row into
+// stage[slot], completing on bar.  Returns m.
+// A first visit of id in the window bitmap (win covers [wbase, wbase +
+// kWinBits)) or else in the visited tables; `logged` tells which.
+__device__ __forceinline__ bool visit_id(Visited& vis, uint32_t* win, uint32_t wbase, uint32_t id, uint32_t& rec,
+                                         bool& logged, uint32_t* err) {
+    const uint32_t w = id - wbase;
+    if (w < kWinBits) {
+        logged = false;
+        const uint32_t bit = 1u << (w & 31u);
+        return (atomicOr(win + (w >> 5), bit) & bit) == 0u;
+    }
+    logged = true;
+    return vis_first(vis, id, rec, err);
+}
+
 // Of the m (<= 64) fresh (dist, id) entries in nd/ni, keeps those that can
 // enter the beam -- all of them while the beam is not full, else those ranking
 // before its last entry (td, tid), since any other would land at rank >= L --
@@ -170,7 +196,7 @@ __device__ __forceinline__ uint32_t sort_fresh_kept(float* nd, uint32_t* ni, uin
             const int s = __ffs(r) - 1;
             const float ds = __shfl_sync(kAll, dv, s);
             const uint32_t is = __shfl_sync(kAll, iv, s);
-            rank += ord(ds, is, dv, iv) ? 1u : 0u;
+            rank += (keep && ord(ds, is, dv, iv)) ? 1u : 0u;  // only kept lanes use their rank
         }
         __syncwarp();
         if (keep) {
@@ -206,15 +232,16 @@ __device__ __forceinline__ uint32_t sort_fresh_kept(float* nd, uint32_t* ni, uin
 // it), beam entry j at j + (fresh entries before it); entries before cn, the
 // rank of the best kept fresh entry, do not move.  Returns cn (size when no
 // fresh entry enters).  Warp-collective; nd/ni are reordered.
+template <class Ord = IdOrder>
 __device__ __forceinline__ uint32_t beam_insert(float* bd, uint32_t* bi, uint32_t& size, uint32_t cap, float* nd,
-                                                uint32_t* ni, uint32_t m, uint32_t lane) {
+                                                uint32_t* ni, uint32_t m, uint32_t lane, Ord ord = Ord()) {
     if (m == 0) return size;
     const bool full = size >= cap;
-    const uint32_t mk = sort_fresh_kept(nd, ni, m, full, full ? bd[cap - 1] : 0.f, full ? bi[cap - 1] : 0u, lane);
+    const uint32_t mk = sort_fresh_kept(nd, ni, m, full, full ? bd[cap - 1] : 0.f, full ? bi[cap - 1] : 0u, lane, ord);
     if (mk == 0) return size;
     uint32_t r0 = 0, r1 = 0;
-    if (lane < mk) r0 = lower_rank(bd, bi, size, nd[lane], ni[lane]);
-    if (lane + 32 < mk) r1 = lower_rank(bd, bi, size, nd[lane + 32], ni[lane + 32]);
+    if (lane < mk) r0 = lower_rank(bd, bi, size, nd[lane], ni[lane], ord);
+    if (lane + 32 < mk) r1 = lower_rank(bd, bi, size, nd[lane + 32], ni[lane + 32], ord);
     const uint32_t cn = __shfl_sync(kAll, r0, 0);
     const uint32_t ns = min(cap, size + mk);
     __syncwarp();
@@ -226,7 +253,7 @@ __device__ __forceinline__ uint32_t beam_insert(float* bd, uint32_t* bi, uint32_
         if (mv) {
             dv = bd[j];
             iv = bi[j];
-            pos = j + lower_rank(nd, ni, mk, dv, iv);
+            pos = j + lower_rank(nd, ni, mk, dv, iv, ord);
         }
         __syncwarp();
         if (pos < ns) {

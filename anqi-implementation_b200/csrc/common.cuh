@@ -268,11 +268,13 @@ struct IdOrder {
 // (perm: new id -> original id), so ties break exactly as in the original
 // numbering.  The lookup happens only on equal distances.
 struct PermOrder {
-    const uint32_t* perm;
+    const uint32_t* perm;  // null: the ids are original ids
     __device__ __forceinline__ bool operator()(float da, uint32_t ia, float db, uint32_t ib) const {
         if (da != db) return da < db;
         const uint32_t a = ia & kIdMask, b = ib & kIdMask;
-        if (a == b) return false;  // also two pads (+inf, kEmpty)
+        // equal ids, or a pad / idle-lane value (kEmpty; never an object id):
+        // no lookup
+        if (a == b || !perm || a == kIdMask || b == kIdMask) return a < b;
         return perm[a] < perm[b];
     }
 };

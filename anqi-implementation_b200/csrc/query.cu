@@ -109,30 +109,8 @@ __device__ __forceinline__ void bar_expect(uint64_t* bar, uint32_t bytes) {
 constexpr uint32_t kRowWaitPolls = 1u << 24;
 
 // Objects are numbered in breadth-first order of the graph (anqi_index_load),
-// so a query's visits fall mostly near its entry object.  A per-warp bitmap
-// in shared memory covers the kWinBits ids around the entry; visits outside
-// it go to the visited tables.
-constexpr uint32_t kWinBits = 4096;
-constexpr uint32_t kWinWords = kWinBits / 32;
-
-// Visits the links of node (slots l0 = link[lane], l1 = link[lane + 32], dg =
-// degree): collects the ids seen for the first time into ni[0..m) in link-slot
-// order and logs the table visits (levels 1 and 2).  The lifted rows of the first
-// stage_rows of them are requested at once, one bulk copy per row into
-// stage[slot], completing on bar.  Returns m.
-// A first visit of id in the window bitmap (win covers [wbase, wbase +
-// kWinBits)) or else in the visited tables; `logged` tells which.
-__device__ __forceinline__ bool visit_id(Visited& vis, uint32_t* win, uint32_t wbase, uint32_t id, uint32_t& rec,
-                                         bool& logged, uint32_t* err) {
-    const uint32_t w = id - wbase;
-    if (w < kWinBits) {
-        logged = false;
-        const uint32_t bit = 1u << (w & 31u);
-        return (atomicOr(win + (w >> 5), bit) & bit) == 0u;
-    }
-    logged = true;
-    return vis_first(vis, id, rec, err);
-}
+// so a query's visits fall mostly near its entry object: the window bitmap of
+// beam.cuh covers the kWinBits ids around the entry.
 
 template <uint32_t kDim>
 __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t l0, uint32_t l1, uint32_t dg,

@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--nq", type=int, default=10_000)
     ap.add_argument("--L", type=int, default=128)
     ap.add_argument("--ks", default="10,50,100")
+    ap.add_argument("--data", choices=("mixture", "gaussian"), default="mixture",
+                    help="mixture: the 1,000-centre integer mixture; gaussian: L2-normalised N(0,1) rows "
+                         "(the 1M x 960 shape); exact ground truth needs d <= 256 (tensor path)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gt", action="store_true", help="skip the exact ground truth (profiling runs; no recall)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU seconds of the cpu_baseline sample")
@@ -145,13 +148,18 @@ def measured_peaks():
 def build_workload(ctx, a, rank, log):
     from anqi import pipeline
     t0 = time.perf_counter()
-    base, query = pipeline.mixture(a.n, a.d, a.nq, seed=20260819 + rank)
+    if a.data == "gaussian":
+        base, query = pipeline.gaussian(a.n, a.d, a.nq, seed=20260819 + rank, normalize=True)
+    else:
+        base, query = pipeline.mixture(a.n, a.d, a.nq, seed=20260819 + rank)
     log(f"data {base.shape} + {query.shape} in {time.perf_counter() - t0:.1f}s")
     ix = pipeline.build_index(ctx, base, train_workers=os.cpu_count() or 8, log=log)
     # the same AKNN source build with init_knn on FP32 CUDA cores (the plain
     # path): its lists must equal the tensor-core build's
     t0 = time.perf_counter()
-    ids32, keys32, st32 = pipeline.aknn_build(ctx, base, precision="fp32")
+    # (above 256 dimensions both builds run init_knn on the CUDA cores)
+    ids32, keys32, st32 = (pipeline.aknn_build(ctx, base, precision="fp32") if a.d <= 256
+                           else (ix.aknn_ids, ix.aknn_keys, ix.timings["aknn_stats"]))
     ix.timings["aknn_build_fp32_s"] = time.perf_counter() - t0
     ix.timings["aknn_fp32_identical"] = bool(np.array_equal(ids32, ix.aknn_ids) and
                                              np.array_equal(keys32.view(np.uint32), ix.aknn_keys.view(np.uint32)))
@@ -160,7 +168,7 @@ def build_workload(ctx, a, rank, log):
     ix.timings["aknn_gather_kernel_ms"] = round(st["gather_kernel_ms"], 1)
     log(f"AKNN fp32 build {ix.timings['aknn_build_fp32_s']:.2f}s identical={ix.timings['aknn_fp32_identical']}")
     ks = [int(k) for k in a.ks.split(",")]
-    if a.no_gt:
+    if a.no_gt or a.d > 256:
         return base, query, ix, ks, None
     # exact ground truth on the BF16 tensor path (bit-identical to FP32; the
     # AKNN lists bound each row's 100th key)
@@ -358,7 +366,9 @@ def run_ours(a, rank, world, local):
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded 1,000-centre mixture, integers in [0,255])",
+        "vs_baseline": None, "dtype": "f32",
+        "data": ("synthetic (seeded 1,000-centre mixture, integers in [0,255])" if a.data == "mixture"
+                 else "synthetic (seeded N(0,1), L2-normalised rows)"),
         "config": {"workload": f"rknn_query {a.n}x{a.d}, {a.nq} queries x k{{{a.ks}}}, L={a.L}, "
                                "G48 graph, M8/u8 LRQ postfilter", "n": a.n, "d": a.d, "nq": a.nq,
                    "queries_per_step": nb, "ks": ks, "L": a.L, "parallelism": f"replicas x{world}",

@@ -360,3 +360,4 @@ def test_aknn_build_tensor_init_identical(ctx, kind):
     b_ids, b_d = _aknn(ctx, x, 1)
     assert np.array_equal(a_ids, b_ids)
     assert np.array_equal(bits(a_d), bits(b_d))
+
