@@ -520,33 +520,46 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
 }
 
 // Query lift and RP-tree entry (rknn_query.cpp:2724-2729, rptrees.h:108-124;
-// |margin| <= EPS goes left), one warp per query: writes the entry object and
-// the leaf node reached.  The leaf orders the search's work list.
+// |margin| <= EPS goes left): every 4-lane group of a warp descends for its
+// own query (qpw queries per warp, 8 unless the rows are long), staging each
+// hyperplane with cp.async and reducing in the reference's lane order.
+// Writes the entry object and the leaf node reached; the leaf orders the
+// search's work list.
 __global__ void __launch_bounds__(128) rknn_entry_kernel(SearchParams p, uint32_t* __restrict__ enode,
-                                                         uint32_t* __restrict__ entry) {
-    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u;
-    float* qhat = reinterpret_cast<float*>(g_smem) + (size_t)wib * 2 * p.lstride;
+                                                         uint32_t* __restrict__ entry, uint32_t qpw) {
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
+    float* qhat = reinterpret_cast<float*>(g_smem) + ((size_t)wib * qpw + (gw < qpw ? gw : 0)) * 2 * p.lstride;
     float* stage = qhat + p.lstride;
-    for (uint32_t qi = blockIdx.x * (blockDim.x >> 5) + wib; qi < p.nq; qi += gridDim.x * (blockDim.x >> 5)) {
-        const float* q = p.queries + (size_t)qi * p.bstride;
-        for (uint32_t j = lane; j < p.lstride; j += 32) {
-            float v = 0.0f;
-            if (j < p.d) v = __double2float_rn(__dmul_rn((double)q[j], p.scale));
-            else if (j == p.d) v = 1.0f;
-            qhat[j] = v;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t q0 = (blockIdx.x * (blockDim.x >> 5) + wib) * qpw; q0 < p.nq; q0 += warps * qpw) {
+        const uint32_t qi = q0 + gw;
+        const bool ok = gw < qpw && qi < p.nq;
+        if (ok) {
+            const float* q = p.queries + (size_t)qi * p.bstride;
+            for (uint32_t j = gt; j < p.lstride; j += 4) {
+                float v = 0.0f;
+                if (j < p.d) v = __double2float_rn(__dmul_rn((double)q[j], p.scale));
+                else if (j == p.d) v = 1.0f;
+                qhat[j] = v;
+            }
         }
         __syncwarp();
         uint32_t v = p.troot;
-        for (uint32_t depth = 0; p.tleft[v] != kEmpty && depth < 4096; depth++) {
-            stage_row_async(stage, p.thyper + (size_t)v * p.lstride, p.lstride, lane, 32);
+        bool done = !ok;
+        for (uint32_t depth = 0; depth < 4096; depth++) {
+            if (!done && p.tleft[v] == kEmpty) done = true;
+            if (__all_sync(kFull, done)) break;
+            if (!done) stage_row_async(stage, p.thyper + (size_t)v * p.lstride, p.lstride, gt, 4);
             cp_async_wait_all();
             __syncwarp();
-            const float ip = group_ip(stage, qhat, p.dim, gt, kFull);
+            const float ip = group_ip(done ? qhat : stage, qhat, p.dim, gt, kFull);
             __syncwarp();
-            const float margin = __fsub_rn(ip, p.toffset[v]);
-            v = (margin < -kSplitEps) ? p.tleft[v] : (margin > kSplitEps ? p.tright[v] : p.tleft[v]);
+            if (!done) {
+                const float margin = __fsub_rn(ip, p.toffset[v]);
+                v = (margin < -kSplitEps) ? p.tleft[v] : (margin > kSplitEps ? p.tright[v] : p.tleft[v]);
+            }
         }
-        if (lane == 0) {
+        if (ok && gt == 0) {
             uint32_t ep = p.tleaf[v];
             if (ep == kEmpty || ep >= p.n) ep = 0;
             entry[qi] = ep;
@@ -570,31 +583,50 @@ __global__ void leaf_scatter_kernel(const uint32_t* __restrict__ enode, uint32_t
         order[atomicAdd(cursor + enode[q], 1u)] = q;
 }
 
-// Exclusive scan of counts (nq) into off (nq + 1), one block, fixed order.
-__global__ void scan_counts_kernel(const uint32_t* __restrict__ cnt, uint32_t nq, uint32_t* __restrict__ off) {
-    __shared__ unsigned long long part[1024];
-    const uint32_t t = threadIdx.x, T = blockDim.x;
-    const uint32_t chunk = (nq + T - 1) / T;
-    const uint32_t b = min(nq, t * chunk), e = min(nq, b + chunk);
-    unsigned long long s = 0;
-    for (uint32_t i = b; i < e; i++) s += cnt[i];
-    part[t] = s;
-    __syncthreads();
-    if (t == 0) {
-        unsigned long long run = 0;
-        for (uint32_t i = 0; i < T; i++) {
-            unsigned long long v = part[i];
-            part[i] = run;
-            run += v;
+// Exclusive scan of counts (nq) into off (nq + 1), one block of 1024 threads:
+// tiles of 4,096 counts, 4 consecutive per thread, warp-shuffle scans.
+__global__ void __launch_bounds__(1024) scan_counts_kernel(const uint32_t* __restrict__ cnt, uint32_t nq,
+                                                           uint32_t* __restrict__ off) {
+    __shared__ uint32_t wsum[32];
+    const uint32_t t = threadIdx.x, lane = t & 31u, w = t >> 5;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < nq; base += 4096) {
+        uint32_t v[4], loc[4], s0 = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < 4; k++) {
+            const uint32_t idx = base + 4 * t + k;
+            v[k] = idx < nq ? cnt[idx] : 0u;
+            loc[k] = s0;
+            s0 += v[k];
         }
-        off[nq] = (uint32_t)run;
+        uint32_t x = s0;  // inclusive scan over the warp
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            uint32_t z = wsum[lane];
+#pragma unroll
+            for (uint32_t o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, z, o);
+                if (lane >= o) z += y;
+            }
+            wsum[lane] = z;
+        }
+        __syncthreads();
+        const uint32_t pre = carry + (w ? wsum[w - 1] : 0u) + x - s0;
+#pragma unroll
+        for (uint32_t k = 0; k < 4; k++) {
+            const uint32_t idx = base + 4 * t + k;
+            if (idx < nq) off[idx] = pre + loc[k];
+        }
+        carry += wsum[31];
+        __syncthreads();
     }
-    __syncthreads();
-    unsigned long long run = part[t];
-    for (uint32_t i = b; i < e; i++) {
-        off[i] = (uint32_t)run;
-        run += cnt[i];
-    }
+    if (t == 0) off[nq] = carry;
 }
 
 __global__ void gather_csr_kernel(const uint32_t* __restrict__ src, const unsigned long long* __restrict__ at,
@@ -990,11 +1022,13 @@ static int prepare_entries(Ctx* c, bool* ordered) {
     p.thyper = ix.thyper.as<float>();
     p.tleaf = ix.tleaf.as<uint32_t>();
     p.troot = ix.troot;
-    const size_t smem = 4ull * 2 * ix.lstride * 4;
+    // 8 queries per warp (one per 4-lane group) while their rows fit 48 KB per block
+    const uint32_t qpw = 4ull * 8 * 2 * ix.lstride * 4 <= 48 * 1024 ? 8u : 1u;
+    const size_t smem = 4ull * qpw * 2 * ix.lstride * 4;
     if (smem > 48 * 1024)
         ANQI_CUDA(c, cudaFuncSetAttribute(rknn_entry_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const uint32_t blocks = std::min<uint32_t>(c->sm_count * 8, (nq + 3) / 4);
-    rknn_entry_kernel<<<blocks, 128, smem, c->stream>>>(p, b.enode.as<uint32_t>(), b.entry.as<uint32_t>());
+    const uint32_t blocks = std::min<uint32_t>(c->sm_count * 8, (nq + 4 * qpw - 1) / (4 * qpw));
+    rknn_entry_kernel<<<blocks, 128, smem, c->stream>>>(p, b.enode.as<uint32_t>(), b.entry.as<uint32_t>(), qpw);
     const char* env = std::getenv("ANQI_B200_ORDER");
     *ordered = !(env && env[0] == '0');
     if (*ordered) {
