@@ -1433,7 +1433,7 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
             TcPrep tp;
             TmpBuf ccnt(c), cid(c), ckey(c);
             const uint32_t cap = round_up(std::max(maxcnt, 2u), 32u);
-            if (!(rc = tc_prep(c, dx.as<float>(), n, xs, d, tp)) && !(rc = ensure(c, ccnt, n * 4)) &&
+            if (!(rc = tc_prep(c, dx.as<float>(), dn.as<float>(), n, xs, d, tp)) && !(rc = ensure(c, ccnt, n * 4)) &&
                 !(rc = ensure(c, cid, n * (size_t)cap * 4)) && !(rc = ensure(c, ckey, n * (size_t)cap * 4))) {
                 auto cu = [&](cudaError_t e, const char* what) { return e == cudaSuccess ? ANQI_OK : cuda_check(c, e, what); };
                 rc = cu(cudaMemsetAsync(ccnt.p, 0, n * 4, c->stream), "cudaMemsetAsync");

@@ -177,8 +177,10 @@ constexpr uint32_t kRecheck = 0x80000000u;
 struct TcPrep {
     DevBuf bf, nrm, err, xint;
     uint32_t dp = 0;
+    float bnorm = 0, berr = 0, bn = 0;  // maxima of |x|, |x - bf16(x)|, the FP32 norm
+    int all_exact = 0;                  // every row exact-integer
 };
-int tc_prep(Ctx* c, const float* d_x, uint64_t n, uint32_t xs, uint32_t d, TcPrep& tp);
+int tc_prep(Ctx* c, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs, uint32_t d, TcPrep& tp);
 void tc_release(Ctx* c, TcPrep& tp);
 // init_knn candidates of one tree's leaves on the tensor cores: for every
 // member row, the leaf-mates j != row whose key may be <= the row's current

@@ -184,6 +184,11 @@ struct FilterParams {
     const float* list_kd;
     const uint32_t* list_sz;
     uint32_t list_k;
+    // bounds over the base rows (columns) of |x| (rounded up), |x - bf16(x)|
+    // and the FP32 norm, and whether every base row is exact-integer: they
+    // bound eps for a whole row, so most pairs are rejected by one compare
+    float bx_norm, bx_err, bx_n;
+    int all_exact;
 };
 
 constexpr uint32_t kStages = 3;
@@ -317,6 +322,9 @@ __global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterPara
     const float cc = 4.f * u;
     const float cd = 4.f * u * qn;
     const float* qrow = p.q32 + (row_ok ? my_row : 0) * p.xs;
+    // eps <= epsmax for every column of this row (eps grows with the column's
+    // |x|, |x - bf16(x)| and norm; exact rows against all-exact columns: 0)
+    const float epsmax = (qexact && p.all_exact) ? 0.f : fmaf(ca, p.bx_norm, fmaf(cb, p.bx_err, fmaf(cc, p.bx_n, cd)));
 
     for (uint32_t t = 0; t <= T; t++) {
         // tile t (prefetched one iteration ahead) and the query tile resident
@@ -360,6 +368,7 @@ __global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterPara
                     const float xn = cs[cj];
                     const float approx = __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, v[k]));
                     const float thr = (p.thr_row || leaf) ? thr_r : cs[3 * kTile + cj];
+                    if (approx - epsmax > thr) continue;  // then approx - eps > thr too
                     const bool exact = qexact && colint[st * kTile + cj];
                     const float eps =
                         exact ? 0.f : fmaf(ca, cs[kTile + cj], fmaf(cb, cs[2 * kTile + cj], fmaf(cc, xn, cd)));
@@ -420,6 +429,41 @@ __global__ void hint_bound_kernel(const float* __restrict__ x, const float* __re
 }  // namespace
 
 // Host helpers shared by the tensor-core entry points.
+// Maxima of |x|, |x - bf16(x)| and the FP32 norm over n rows, and whether all
+// rows are exact-integer (out: 3 float bit patterns as u32, then a flag).
+__global__ void row_bounds_kernel(const float* __restrict__ rn, const float* __restrict__ xnorm,
+                                  const float* __restrict__ xerr, const uint8_t* __restrict__ xint, uint64_t n,
+                                  uint32_t* __restrict__ out) {
+    uint32_t a = 0, b = 0, c = 0, e = 1;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        a = max(a, __float_as_uint(fmaxf(xnorm[i], 0.f)));  // non-negative floats order as their bits
+        b = max(b, __float_as_uint(fmaxf(xerr[i], 0.f)));
+        c = max(c, __float_as_uint(fmaxf(rn[i], 0.f)));
+        e &= xint[i] ? 1u : 0u;
+    }
+    atomicMax(out, a);
+    atomicMax(out + 1, b);
+    atomicMax(out + 2, c);
+    atomicAnd(out + 3, e);
+}
+
+int tc_row_bounds(Ctx* c, const float* rn, const float* xnorm, const float* xerr, const uint8_t* xint, uint64_t n,
+                  float* bnorm, float* berr, float* bn, int* all_exact) {
+    TmpBuf t(c);
+    int rc;
+    const uint32_t init[4] = {0, 0, 0, 1};
+    if ((rc = h2d(c, t, init, 16))) return rc;
+    row_bounds_kernel<<<c->sm_count * 4, 256, 0, c->stream>>>(rn, xnorm, xerr, xint, n, t.as<uint32_t>());
+    ANQI_CUDA(c, cudaGetLastError());
+    uint32_t h[4];
+    if ((rc = d2h(c, h, t, 16)) || (rc = sync(c))) return rc;
+    std::memcpy(bnorm, &h[0], 4);
+    std::memcpy(berr, &h[1], 4);
+    std::memcpy(bn, &h[2], 4);
+    *all_exact = (int)h[3];
+    return ANQI_OK;
+}
+
 int tc_prepare_rows(Ctx* c, const float* dx, uint64_t n, uint32_t xs, uint32_t d, uint32_t dp, DevBuf& xb,
                     DevBuf& xnorm, DevBuf& xerr, DevBuf& xint) {
     int rc;
@@ -576,10 +620,13 @@ int filter_to_csr(Ctx* c, FilterParams p, uint64_t nq, uint32_t cap, std::vector
 
 }  // namespace
 
-int tc_prep(Ctx* c, const float* d_x, uint64_t n, uint32_t xs, uint32_t d, TcPrep& tp) {
+int tc_prep(Ctx* c, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs, uint32_t d, TcPrep& tp) {
     tp.dp = round_up(d, 16u);
     if (filter_smem(tp.dp) > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "dimension %u too large for the tensor path", d);
-    return tc_prepare_rows(c, d_x, n, xs, d, tp.dp, tp.bf, tp.nrm, tp.err, tp.xint);
+    int rc = tc_prepare_rows(c, d_x, n, xs, d, tp.dp, tp.bf, tp.nrm, tp.err, tp.xint);
+    if (rc) return rc;
+    return tc_row_bounds(c, d_norms, tp.nrm.as<float>(), tp.err.as<float>(), tp.xint.as<uint8_t>(), n, &tp.bnorm,
+                         &tp.berr, &tp.bn, &tp.all_exact);
 }
 
 void tc_release(Ctx* c, TcPrep& tp) {
@@ -624,6 +671,10 @@ int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* 
     p.list_kd = list_kd;
     p.list_sz = list_sz;
     p.list_k = K;
+    p.bx_norm = tp.bnorm;
+    p.bx_err = tp.berr;
+    p.bx_n = tp.bn;
+    p.all_exact = tp.all_exact;
     p.nrows = tiles.size() * kTile;
     p.split_len = 0;
     const size_t smem = filter_smem(p.dp);
@@ -703,6 +754,9 @@ int anqi_rknn_ground_truth_tc(anqi_ctx* h, const float* base, uint64_t n, const 
     if ((rc = X.load(c, base, n, d, xs, dp)) || (rc = Q.load(c, query, nq, d, xs, dp)) || (rc = h2d(c, dr, rk2, n * 4)))
         return rc;
     FilterParams p = make_params(Q, X, n, xs, d, dp);
+    if ((rc = tc_row_bounds(c, X.rn.as<float>(), X.nrm.as<float>(), X.err.as<float>(), X.xint.as<uint8_t>(), n,
+                            &p.bx_norm, &p.bx_err, &p.bx_n, &p.all_exact)))
+        return rc;
     p.thr_col = dr.as<float>();
     std::vector<uint64_t> hoff;
     if ((rc = filter_to_csr(c, p, nq, 256, hoff, doff, did, dkey))) return rc;
@@ -756,6 +810,9 @@ int anqi_exact_topk_tc(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, u
                                                               dh.as<uint32_t>(), hint_k, K, tau.as<float>());
     ANQI_CUDA(c, cudaGetLastError());
     FilterParams p = make_params(X, X, n, xs, d, dp);
+    if ((rc = tc_row_bounds(c, X.rn.as<float>(), X.nrm.as<float>(), X.err.as<float>(), X.xint.as<uint8_t>(), n,
+                            &p.bx_norm, &p.bx_err, &p.bx_n, &p.all_exact)))
+        return rc;
     p.thr_row = tau.as<float>();
     p.exclude_self = 1;
     std::vector<uint64_t> hoff;
