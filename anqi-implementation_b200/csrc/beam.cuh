@@ -97,6 +97,27 @@ __device__ __forceinline__ bool vis_first(Visited& v, uint32_t id, uint32_t& pos
     return visit_first(v.bits, id);
 }
 
+// Read-only probe of the visited set for id: the id's first bucket (levels 0
+// and 1) or its bitmap word (level 2, in .x).  probe_found tells whether the
+// probe alone shows id visited; nothing leaves the set while it is in use, so
+// "found" is final, and "not found" needs vis_first.  Probes of many ids can
+// be in flight at once.
+__device__ __forceinline__ uint4 probe_visited(const Visited& v, uint32_t id) {
+    if (v.level == 2) {
+        uint32_t w;
+        asm volatile("ld.global.cg.u32 %0, [%1];\n" : "=r"(w) : "l"(v.bits + (id >> 5)) : "memory");
+        return make_uint4(w, 0, 0, 0);
+    }
+    const bool sh = v.level == 0;
+    const uint32_t b = (id * 0x9E3779B1u) >> ((sh ? v.shift : v.gshift) + 2);
+    return sh ? ld_bucket_shared(v.tab + 4 * b) : ld_bucket_global(v.gtab + 4 * b);
+}
+
+__device__ __forceinline__ bool probe_found(const Visited& v, const uint4& q, uint32_t id) {
+    if (v.level == 2) return (q.x >> (id & 31u)) & 1u;
+    return q.x == id || q.y == id || q.z == id || q.w == id;
+}
+
 // Level 0 -> 1 (gtab present) or 0 -> 2 (warp-collective); nlog entries move.
 static __device__ void vis_up_from_shared(Visited& v, uint32_t lane, uint32_t* err) {
     const uint32_t to = v.gcap ? 1u : 2u;

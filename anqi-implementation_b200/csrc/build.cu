@@ -353,10 +353,28 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
                 }
 #pragma unroll
                 for (uint32_t u = 0; u < 8; u++) lst[32 * u + lane] = ids[u];
+                // Visited prefilter: one read-only probe per id, four in flight
+                // at a time; an id found there is visited (late in a row almost
+                // every id is), the rest take the exact path below.  Within one
+                // expansion the order in which chunks are inserted does not
+                // change the beam or the pool after sorting.
+                uint32_t maybe = 0;  // bit u: ids[u] may be a first visit
+#pragma unroll
+                for (uint32_t h = 0; h < 8; h += 4) {
+                    uint4 q[4];
+#pragma unroll
+                    for (uint32_t k = 0; k < 4; k++)
+                        q[k] = ids[h + k] < p.n ? probe_visited(vis, ids[h + k]) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+                    for (uint32_t k = 0; k < 4; k++)
+                        if (ids[h + k] < p.n && !probe_found(vis, q[k], ids[h + k])) maybe |= 1u << (h + k);
+                }
                 __syncwarp();
                 for (uint32_t u = 0; u < 8 && c0 + 32 * u < tot; u += 2) {
-                    const uint32_t m =
-                        gather_visit(p, vis, nlog, lst[32 * u + lane], lst[32 * u + 32 + lane], 0.f, 0.f, false, ni, nd, lane);
+                    const bool a0 = (maybe >> u) & 1u, a1 = (maybe >> (u + 1)) & 1u;
+                    if (!__any_sync(kAll, a0 || a1)) continue;
+                    const uint32_t m = gather_visit(p, vis, nlog, a0 ? lst[32 * u + lane] : kEmpty,
+                                                    a1 ? lst[32 * u + 32 + lane] : kEmpty, 0.f, 0.f, false, ni, nd, lane);
                     if (m == 0) continue;
                     batch_d2(p, i, ni, nd, m, gw, gt);
                     take(m);
@@ -1431,7 +1449,11 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
         if (ap->precision == 1 && round_up(d, 16u) <= 256) {
             // BF16 tensor-core leaf tiles: candidates per tree, then the merge
             TcPrep tp;
-            TmpBuf ccnt(c), cid(c), ckey(c);
+            // candidate buffers (n x cap entries; GBs at 1M) are kept by the
+            // context: allocating them anew for every build cost up to seconds
+            DevBuf& ccnt = c->init_cnt;
+            DevBuf& cid = c->init_cid;
+            DevBuf& ckey = c->init_key;
             const uint32_t cap = round_up(std::max(maxcnt, 2u), 32u);
             if (!(rc = tc_prep(c, dx.as<float>(), dn.as<float>(), n, xs, d, tp)) && !(rc = ensure(c, ccnt, n * 4)) &&
                 !(rc = ensure(c, cid, n * (size_t)cap * 4)) && !(rc = ensure(c, ckey, n * (size_t)cap * 4))) {

@@ -103,6 +103,7 @@ struct Ctx {
     uint32_t last_cfg_hash = 0, last_cfg_gcap = 0, last_cfg_blocks = 0;
     size_t last_cfg_smem = 0;
     cudaGraphExec_t qgraph = nullptr;
+    DevBuf init_cnt, init_cid, init_key;  // tensor-core init_knn candidate buffers
     std::vector<uint64_t> qgraph_key;
     uint64_t device_bytes = 0;
     std::vector<DevBuf*> member_bufs() {
@@ -111,7 +112,8 @@ struct Ctx {
                 &batch.qL, &batch.qslot, &batch.npred, &batch.ncand, &batch.ndist, &batch.nexp, &batch.nflood,
                 &batch.pred_at, &batch.cand_at, &batch.pred_buf, &batch.cand_buf, &batch.pred_off,
                 &batch.cand_off, &batch.pred_csr, &batch.cand_csr, &err, &counters, &vis_bits, &vis_log,
-                &cand_scratch, &thr_table, &gt_off, &gt_ids, &eval_rows, &eval_sums, &vis_gtab};
+                &cand_scratch, &thr_table, &gt_off, &gt_ids, &eval_rows, &eval_sums, &vis_gtab,
+                &init_cnt, &init_cid, &init_key};
     }
     // Per-object thresholds for up to kThrSlots values of k: slot s holds
     // thr_k[s] (0 = unused) in thr_table[s * n .. (s+1) * n).
