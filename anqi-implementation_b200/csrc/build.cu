@@ -726,7 +726,8 @@ __global__ void __launch_bounds__(256) leaf_topk_kernel(const float* __restrict_
 // their order.  Resets cnt.  One warp per row.
 __global__ void __launch_bounds__(128) leaf_merge_kernel(const float* __restrict__ x, const float* __restrict__ norms,
                                                          uint64_t n, uint32_t stride, uint32_t dim,
-                                                         uint32_t* __restrict__ cnt, uint32_t cap,
+                                                         const uint32_t* __restrict__ members, uint64_t pos_base,
+                                                         uint64_t nslots, uint32_t* __restrict__ cnt, uint32_t cap,
                                                          const uint32_t* __restrict__ cid,
                                                          const float* __restrict__ ckey, uint32_t K,
                                                          float* __restrict__ kd, uint32_t* __restrict__ ki,
@@ -738,9 +739,10 @@ __global__ void __launch_bounds__(128) leaf_merge_kernel(const float* __restrict
     uint32_t* wi = reinterpret_cast<uint32_t*>(wd + 64);
     const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t row = w0; row < n; row += nw) {
-        uint32_t m = cnt[row];
+    for (uint64_t sl = w0; sl < nslots; sl += nw) {
+        uint32_t m = cnt[sl];
         if (m == 0) continue;
+        const uint64_t row = members[pos_base + sl];
         if (m > cap) {
             if (lane == 0) set_error(err, kDevPoolOverflow);
             m = cap;
@@ -758,9 +760,9 @@ __global__ void __launch_bounds__(128) leaf_merge_kernel(const float* __restrict
             const uint32_t bm = min(64u, m - c0);
             bool flag = false;
             for (uint32_t t = lane; t < bm; t += 32) {
-                const uint32_t id = cid[row * cap + c0 + t];
+                const uint32_t id = cid[sl * cap + c0 + t];
                 wi[t] = id & ~kRecheck;
-                wd[t] = ckey[row * cap + c0 + t];
+                wd[t] = ckey[sl * cap + c0 + t];
                 flag |= (id & kRecheck) != 0;
             }
             __syncwarp();
@@ -769,7 +771,7 @@ __global__ void __launch_bounds__(128) leaf_merge_kernel(const float* __restrict
                     const uint32_t idx = r0 + gw;
                     const bool ok = idx < bm;
                     const uint32_t j = wi[ok ? idx : r0];
-                    const bool re = ok && (cid[row * cap + c0 + idx] & kRecheck);
+                    const bool re = ok && (cid[sl * cap + c0 + idx] & kRecheck);
                     if (__any_sync(kAll, re)) {
                         const float ip = group_ip(xi, x + (uint64_t)j * stride, dim, gt, kAll);
                         if (re && gt == 0) wd[idx] = norm_d2(nr, norms[j], ip);
@@ -811,7 +813,7 @@ __global__ void __launch_bounds__(128) leaf_merge_kernel(const float* __restrict
         }
         if (lane == 0) {
             ksz[row] = size;
-            cnt[row] = 0;
+            cnt[sl] = 0;
         }
         __syncwarp();
     }
@@ -923,7 +925,10 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     const int warps_per_block = 4;
     const uint32_t topk_cap = (p.mode == kModeAknn && p.ef < p.out_k + 1) ? p.out_k + 1 : 0;
     p.sort_words = p.mode == kModeAknn ? 0 : 2 * kSortSmem;
-    const uint32_t log_cap = (uint32_t)std::min<uint64_t>(p.n, 32768);
+    // the log covers a row's first visits up to the pool cap plus one expansion
+    // (a row past it clears its whole bitmap instead)
+    const uint32_t log_cap = (uint32_t)std::min<uint64_t>(
+        p.n, std::max<uint64_t>(8192, std::min<uint64_t>(32768, (uint64_t)p.cap + p.K + max_rev + 64)));
     // visited set: an L2-resident table per slot (bucketed probing: a lookup
     // is one 16-byte L2 load), then the bitmap; measured at 1M x 128 this beats
     // any shared-memory table in front of it, which costs occupancy
@@ -953,7 +958,13 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     uint64_t need = (uint64_t)p.cap + p.K + max_rev + 64;
     if (p.mode == kModeCommit) need = p.M + max_rev + 64;
     const uint32_t pool_cap = p.mode == kModeAknn ? 1u : (uint32_t)std::min<uint64_t>(1ull << 30, 1ull << (64 - __builtin_clzll(need)));
-    TmpBuf bits(c), vlog(c), pd(c), pi(c), gtab(c);
+    // per-slot scratch, kept by the context between builds (the first build
+    // maps it; later ones reuse it)
+    DevBuf& bits = c->g_bits;
+    DevBuf& vlog = c->g_vlog;
+    DevBuf& pd = c->g_pd;
+    DevBuf& pi = c->g_pi;
+    DevBuf& gtab = c->g_gtab;
     int rc;
     if ((rc = ensure(c, bits, (size_t)slots * words * 4)) || (rc = ensure(c, vlog, (size_t)slots * log_cap * 4)) ||
         (rc = ensure(c, pd, (size_t)slots * pool_cap * 4)) || (rc = ensure(c, pi, (size_t)slots * pool_cap * 4)) ||
@@ -1455,25 +1466,40 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
             DevBuf& cid = c->init_cid;
             DevBuf& ckey = c->init_key;
             const uint32_t cap = round_up(std::max(maxcnt, 2u), 32u);
-            if (!(rc = tc_prep(c, dx.as<float>(), dn.as<float>(), n, xs, d, tp)) && !(rc = ensure(c, ccnt, n * 4)) &&
-                !(rc = ensure(c, cid, n * (size_t)cap * 4)) && !(rc = ensure(c, ckey, n * (size_t)cap * 4))) {
+            // candidate slots for batches of leaves covering up to brows rows (~1 GB)
+            uint64_t want = (512ull << 20) / (cap * 4ull);
+            if (const char* e = std::getenv("ANQI_B200_INIT_BATCH_ROWS")) want = std::strtoull(e, nullptr, 10);
+            const uint64_t brows = std::min<uint64_t>(n, std::max<uint64_t>(maxcnt, want));
+            if (!(rc = tc_prep(c, dx.as<float>(), dn.as<float>(), n, xs, d, tp)) && !(rc = ensure(c, ccnt, brows * 4)) &&
+                !(rc = ensure(c, cid, brows * (size_t)cap * 4)) && !(rc = ensure(c, ckey, brows * (size_t)cap * 4))) {
                 auto cu = [&](cudaError_t e, const char* what) { return e == cudaSuccess ? ANQI_OK : cuda_check(c, e, what); };
-                rc = cu(cudaMemsetAsync(ccnt.p, 0, n * 4, c->stream), "cudaMemsetAsync");
+                rc = cu(cudaMemsetAsync(ccnt.p, 0, brows * 4, c->stream), "cudaMemsetAsync");
                 const int wpb = 4;
                 const size_t msmem = (size_t)(4 * K + 128) * 4 * wpb;
                 if (!rc && msmem > 48 * 1024)
                     rc = cu(cudaFuncSetAttribute(leaf_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem),
                             "cudaFuncSetAttribute");
                 for (uint32_t tr = 0; tr < ap->trees && !rc; tr++) {
-                    rc = tc_leaf_candidates(c, tp, dx.as<float>(), dn.as<float>(), n, xs, d, f.perm.as<uint32_t>(),
-                                            tree_leaves[tr], kd.as<float>(), ksz.as<uint32_t>(), K,
-                                            ccnt.as<uint32_t>(), cap, cid.as<uint32_t>(), ckey.as<float>());
-                    if (rc) break;
-                    leaf_merge_kernel<<<c->sm_count * 8, 32 * wpb, msmem, c->stream>>>(
-                        dx.as<float>(), dn.as<float>(), n, xs, d, ccnt.as<uint32_t>(), cap, cid.as<uint32_t>(),
-                        ckey.as<float>(), K, kd.as<float>(), ki.as<uint32_t>(), ksz.as<uint32_t>(),
-                        c->err.as<uint32_t>());
-                    rc = cu(cudaGetLastError(), "leaf_merge_kernel");
+                    // leaves in permutation order, in batches of contiguous positions
+                    std::vector<LeafRef>& lv = tree_leaves[tr];
+                    std::sort(lv.begin(), lv.end(), [](const LeafRef& a, const LeafRef& b) { return a.off < b.off; });
+                    for (size_t l0 = 0; l0 < lv.size() && !rc;) {
+                        const uint64_t base = lv[l0].off;
+                        size_t l1 = l0;
+                        while (l1 < lv.size() && lv[l1].off + lv[l1].cnt - base <= brows) l1++;
+                        const std::vector<LeafRef> batch(lv.begin() + l0, lv.begin() + l1);
+                        const uint64_t nslots = lv[l1 - 1].off + lv[l1 - 1].cnt - base;
+                        rc = tc_leaf_candidates(c, tp, dx.as<float>(), dn.as<float>(), n, xs, d, f.perm.as<uint32_t>(),
+                                                batch, kd.as<float>(), ksz.as<uint32_t>(), K, ccnt.as<uint32_t>(), cap,
+                                                cid.as<uint32_t>(), ckey.as<float>(), base);
+                        if (rc) break;
+                        leaf_merge_kernel<<<c->sm_count * 8, 32 * wpb, msmem, c->stream>>>(
+                            dx.as<float>(), dn.as<float>(), n, xs, d, f.perm.as<uint32_t>(), base, nslots,
+                            ccnt.as<uint32_t>(), cap, cid.as<uint32_t>(), ckey.as<float>(), K, kd.as<float>(),
+                            ki.as<uint32_t>(), ksz.as<uint32_t>(), c->err.as<uint32_t>());
+                        rc = cu(cudaGetLastError(), "leaf_merge_kernel");
+                        l0 = l1;
+                    }
                 }
                 if (!rc) rc = check_device_error(c, "init_knn merge");
             }

@@ -104,6 +104,7 @@ struct Ctx {
     size_t last_cfg_smem = 0;
     cudaGraphExec_t qgraph = nullptr;
     DevBuf init_cnt, init_cid, init_key;  // tensor-core init_knn candidate buffers
+    DevBuf g_bits, g_vlog, g_pd, g_pi, g_gtab;  // gather kernel per-slot scratch
     std::vector<uint64_t> qgraph_key;
     uint64_t device_bytes = 0;
     std::vector<DevBuf*> member_bufs() {
@@ -113,7 +114,7 @@ struct Ctx {
                 &batch.pred_at, &batch.cand_at, &batch.pred_buf, &batch.cand_buf, &batch.pred_off,
                 &batch.cand_off, &batch.pred_csr, &batch.cand_csr, &err, &counters, &vis_bits, &vis_log,
                 &cand_scratch, &thr_table, &gt_off, &gt_ids, &eval_rows, &eval_sums, &vis_gtab,
-                &init_cnt, &init_cid, &init_key};
+                &init_cnt, &init_cid, &init_key, &g_bits, &g_vlog, &g_pd, &g_pi, &g_gtab};
     }
     // Per-object thresholds for up to kThrSlots values of k: slot s holds
     // thr_k[s] (0 = unused) in thr_table[s * n .. (s+1) * n).
@@ -184,14 +185,15 @@ struct TcPrep {
 };
 int tc_prep(Ctx* c, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs, uint32_t d, TcPrep& tp);
 void tc_release(Ctx* c, TcPrep& tp);
-// init_knn candidates of one tree's leaves on the tensor cores: for every
-// member row, the leaf-mates j != row whose key may be <= the row's current
-// K-th list key (any while the list is short), appended to out_id / out_key
-// [row * cap ..] with cnt[row] (kRecheck marks keys to recompute in FP32).
+// init_knn candidates of a batch of one tree's leaves on the tensor cores:
+// for every member row, the leaf-mates j != row whose key may be <= the
+// row's current K-th list key (any while the list is short), appended to
+// out_id / out_key [slot * cap ..] with cnt[slot], slot = the row's position in
+// the forest permutation - pos_base (kRecheck marks keys to recompute in FP32).
 int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs,
                        uint32_t d, const uint32_t* d_members, const std::vector<LeafRef>& leaves,
                        const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
-                       uint32_t* out_id, float* out_key);
+                       uint32_t* out_id, float* out_key, uint64_t pos_base);
 
 // L2 persisting window over [p, p + bytes) for kernels on the context's stream.
 void set_l2_window(Ctx* c, const void* p, size_t bytes);

@@ -189,6 +189,7 @@ struct FilterParams {
     // bound eps for a whole row, so most pairs are rejected by one compare
     float bx_norm, bx_err, bx_n;
     int all_exact;
+    uint64_t pos_base;  // leaf mode: candidate slot = member position - pos_base (the batch's first)
 };
 
 constexpr uint32_t kStages = 3;
@@ -375,11 +376,13 @@ __global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterPara
                     if (!(approx - eps <= thr)) continue;
                     if (p.exclude_self && j == my_row) continue;
                     if (leaf) {
-                        // the merge recomputes flagged keys in FP32 and keeps <= its K-th
-                        const uint32_t pos = atomicAdd(p.cnt + my_row, 1u);
+                        // the merge recomputes flagged keys in FP32 and keeps <= its K-th;
+                        // slots are indexed by the row's position in the batch of leaves
+                        const uint64_t cs0 = lt.off + (uint64_t)lt.rb * kTile + r - p.pos_base;
+                        const uint32_t pos = atomicAdd(p.cnt + cs0, 1u);
                         if (pos < p.cap) {
-                            p.out_id[my_row * p.cap + pos] = (uint32_t)j | (exact ? 0u : kRecheck);
-                            p.out_key[my_row * p.cap + pos] = approx;
+                            p.out_id[cs0 * p.cap + pos] = (uint32_t)j | (exact ? 0u : kRecheck);
+                            p.out_key[cs0 * p.cap + pos] = approx;
                         }
                         continue;
                     }
@@ -639,7 +642,7 @@ void tc_release(Ctx* c, TcPrep& tp) {
 int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs,
                        uint32_t d, const uint32_t* d_members, const std::vector<LeafRef>& leaves,
                        const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
-                       uint32_t* out_id, float* out_key) {
+                       uint32_t* out_id, float* out_key, uint64_t pos_base) {
     std::vector<LeafTile> tiles;
     for (const LeafRef& l : leaves) {
         if (l.cnt > cap + 1) return fail(c, ANQI_ERR_ARGS, "leaf of %u rows exceeds the candidate capacity", l.cnt);
@@ -671,6 +674,7 @@ int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* 
     p.list_kd = list_kd;
     p.list_sz = list_sz;
     p.list_k = K;
+    p.pos_base = pos_base;
     p.bx_norm = tp.bnorm;
     p.bx_err = tp.berr;
     p.bx_n = tp.bn;

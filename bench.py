@@ -161,12 +161,18 @@ def build_workload(ctx, a, rank, log):
     ids32, keys32, st32 = (pipeline.aknn_build(ctx, base, precision="fp32") if a.d <= 256
                            else (ix.aknn_ids, ix.aknn_keys, ix.timings["aknn_stats"]))
     ix.timings["aknn_build_fp32_s"] = time.perf_counter() - t0
+    # the index's build ran first, in a fresh context (it also mapped the
+    # build scratch); one more tensor-core build compares like with like
+    t0 = time.perf_counter()
+    _, _, st16 = pipeline.aknn_build(ctx, base) if a.d <= 256 else (None, None, ix.timings["aknn_stats"])
+    ix.timings["aknn_build_warm_s"] = time.perf_counter() - t0
     ix.timings["aknn_fp32_identical"] = bool(np.array_equal(ids32, ix.aknn_ids) and
                                              np.array_equal(keys32.view(np.uint32), ix.aknn_keys.view(np.uint32)))
-    st = ix.timings["aknn_stats"]
+    st = st16
     ix.timings["aknn_init_ms"] = {"bf16": round(st["init_ms"], 1), "fp32": round(st32["init_ms"], 1)}
     # the library's own clock around the build (excludes the Python-side host copies)
-    ix.timings["aknn_total_ms"] = {"bf16": round(st["total_ms"], 1), "fp32": round(st32["total_ms"], 1)}
+    ix.timings["aknn_total_ms"] = {"bf16": round(st["total_ms"], 1), "fp32": round(st32["total_ms"], 1),
+                                   "bf16_first_build": round(ix.timings["aknn_stats"]["total_ms"], 1)}
     ix.timings["aknn_gather_kernel_ms"] = round(st["gather_kernel_ms"], 1)
     log(f"AKNN fp32 build {ix.timings['aknn_build_fp32_s']:.2f}s identical={ix.timings['aknn_fp32_identical']}")
     ks = [int(k) for k in a.ks.split(",")]
@@ -393,8 +399,9 @@ def run_ours(a, rank, world, local):
                                "candidates": round(s0["n_cand"] / nb, 1), "verified": round(s0["n_pred"] / nb, 2)},
         "batched_form": batched,
         "build_s": {k: round(v, 3) for k, v in ix.timings.items() if isinstance(v, float)},
-        "aknn_build": {"bf16_tensor_init_s": round(ix.timings["aknn_build_s"], 3),
+        "aknn_build": {"bf16_tensor_init_s": round(ix.timings["aknn_build_warm_s"], 3),
                        "fp32_init_s": round(ix.timings["aknn_build_fp32_s"], 3),
+                       "bf16_first_build_s": round(ix.timings["aknn_build_s"], 3),
                        "identical": ix.timings["aknn_fp32_identical"], "init_ms": ix.timings["aknn_init_ms"],
                        "library_total_ms": ix.timings["aknn_total_ms"],
                        "gather_kernel_ms": ix.timings["aknn_gather_kernel_ms"]},

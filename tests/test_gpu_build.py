@@ -342,15 +342,18 @@ def _aknn(ctx, x, precision, K=50, leaf=300, trees=8, ef=150):
     return ids, dist
 
 
-@pytest.mark.parametrize("kind", ["integer", "float", "duplicates"])
-def test_aknn_build_tensor_init_identical(ctx, kind):
+@pytest.mark.parametrize("kind", ["integer", "float", "duplicates", "batched"])
+def test_aknn_build_tensor_init_identical(ctx, kind, monkeypatch):
     """init_knn on BF16 tensor-core leaf tiles (exact keys on integer rows, FP32
     recheck otherwise) gives the FP32 path's AKNN lists bit for bit; leaves of
-    up to 300 rows span several 128-row tiles."""
+    up to 300 rows span several 128-row tiles; "batched" runs each tree's
+    leaves in batches of candidate slots."""
     rng = np.random.default_rng(17)
-    if kind == "integer":
+    if kind in ("integer", "batched"):
         from anqi import pipeline
         x, _ = pipeline.mixture(12000, 64, 1, centers=40, seed=5)
+        if kind == "batched":  # leaves in batches of about 1,500 rows per tree
+            monkeypatch.setenv("ANQI_B200_INIT_BATCH_ROWS", "1500")
     elif kind == "float":
         x = clustered(12000, 48, 9, nc=60)
     else:
