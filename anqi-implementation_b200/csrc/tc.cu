@@ -362,14 +362,33 @@ __global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterPara
                 float v[32];
                 tc::tmem_ld32(tmem + (((warp & 3u) * 32u) << 16) + (e & 1u) * kTile + c0, v);
                 if (!row_ok) continue;
-#pragma unroll 4
-                for (uint32_t k = 0; k < 32; k++) {
+                // columns that survive the row's eps bound, without branches:
+                // 4 norms (and thresholds) per shared load
+                const bool rowthr = p.thr_row || leaf;
+                uint32_t keep = 0;
+#pragma unroll
+                for (uint32_t k = 0; k < 32; k += 4) {
+                    const float4 xn4 = *reinterpret_cast<const float4*>(cs + c0 + k);
+                    const float4 th4 = rowthr ? make_float4(thr_r, thr_r, thr_r, thr_r)
+                                              : *reinterpret_cast<const float4*>(cs + 3 * kTile + c0 + k);
+                    const float xa[4] = {xn4.x, xn4.y, xn4.z, xn4.w}, ta[4] = {th4.x, th4.y, th4.z, th4.w};
+#pragma unroll
+                    for (uint32_t q = 0; q < 4; q++) {
+                        const float approx = __fsub_rn(__fadd_rn(qn, xa[q]), __fmul_rn(2.0f, v[k + q]));
+                        keep |= (approx - epsmax <= ta[q] ? 1u : 0u) << (k + q);
+                    }
+                }
+                for (; keep; keep &= keep - 1) {
+                    const uint32_t k = __ffs(keep) - 1;
                     const uint32_t cj = c0 + k;
                     const uint64_t j = leaf ? (uint64_t)colid[st * kTile + cj] : j0 + cj;
                     const float xn = cs[cj];
-                    const float approx = __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, v[k]));
-                    const float thr = (p.thr_row || leaf) ? thr_r : cs[3 * kTile + cj];
-                    if (approx - epsmax > thr) continue;  // then approx - eps > thr too
+                    float vk = 0.f;
+#pragma unroll
+                    for (uint32_t q = 0; q < 32; q++)
+                        if (q == k) vk = v[q];
+                    const float approx = __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, vk));
+                    const float thr = rowthr ? thr_r : cs[3 * kTile + cj];
                     const bool exact = qexact && colint[st * kTile + cj];
                     const float eps =
                         exact ? 0.f : fmaf(ca, cs[kTile + cj], fmaf(cb, cs[2 * kTile + cj], fmaf(cc, xn, cd)));
