@@ -192,7 +192,7 @@ struct FilterParams {
     uint64_t pos_base;  // leaf mode: candidate slot = member position - pos_base (the batch's first)
 };
 
-constexpr uint32_t kStages = 3;
+constexpr uint32_t kStages = 2;  // base-tile ring; two CTAs fit an SM (shared memory, TMEM)
 constexpr uint32_t kFilterThreads = 256;
 
 // The reference's FP32 key |q|^2 + |x|^2 - 2 <q, x> (dataset_gt.cpp:225, 294)
@@ -225,7 +225,7 @@ __device__ __forceinline__ float ref_key(const float* __restrict__ q, const floa
     return __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, ip));
 }
 
-__global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterParams p) {
+__global__ void __launch_bounds__(kFilterThreads, 2) tc_filter_kernel(FilterParams p) {
     extern __shared__ __align__(128) unsigned char sm[];
     const uint32_t tile_bytes = kTile * p.dp * 2;
     unsigned char* sa = sm;
@@ -351,9 +351,6 @@ __global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterPara
             atomicExch(p.err, 8u);
         }
         tc::fence_after_sync();
-        // stage (t + 1) % 3 last held tile t - 2: its MMA (before MMA e) and
-        // its epilogue (previous iteration) are done
-        if (t + 1 < T) prefetch(t + 1);
         if (ok) {
             const uint32_t st = e % kStages;
             const float* cs = col + (size_t)st * 4 * kTile;
@@ -414,6 +411,12 @@ __global__ void __launch_bounds__(kFilterThreads, 1) tc_filter_kernel(FilterPara
                     }
                 }
             }
+        }
+        // stage (t + 1) % 2 held tile e: its MMA finished (waited above); once
+        // every warp has left its epilogue the stage is refilled
+        if (t + 1 < T) {
+            __syncthreads();
+            prefetch(t + 1);
         }
         tc::fence_before_sync();
     }
