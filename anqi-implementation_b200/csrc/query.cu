@@ -329,23 +329,42 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
         // links of the next node to expand, loaded while the current merge runs
         uint32_t pre_node = kEmpty, pl0 = kEmpty, pl1 = kEmpty, pdg = 0;
 
-        // ---- greedy beam, index.h:1613-1624
-        while (cur < size && !overflow) {
-            const uint32_t node = bi[cur] & kIdMask;
-            __syncwarp();
-            if (lane == 0) bi[cur] = node | kExpanded;
-            __syncwarp();
-            nexp++;
-            // entries before cur are all expanded; nxt = the next unexpanded one
-            uint32_t nxt = size;
-            for (uint32_t s0 = cur + 1; s0 < size; s0 += 32) {
-                const uint32_t idx = s0 + lane;
-                const bool un = idx < size && !(bi[idx] & kExpanded);
-                const unsigned b = __ballot_sync(kFull, un);
-                if (b) {
-                    nxt = s0 + __ffs(b) - 1;
-                    break;
+        // ---- greedy beam (index.h:1613-1624), then the bounded flood
+        // (index.h:1626-1638), as one loop so the expansion code exists once
+        // in the kernel (instruction fetch)
+        bool flood = false;
+        uint32_t head = 0;
+        for (;;) {
+            uint32_t node, nxt = 0;
+            if (!flood) {
+                if (cur >= size || overflow) {
+                    flood = true;
+                    if (ncand > 0 && !overflow) {
+                        pre_node = cl[0];
+                        load_links(p, pre_node, lane, pl0, pl1, pdg);
+                    }
+                    continue;
                 }
+                node = bi[cur] & kIdMask;
+                __syncwarp();
+                if (lane == 0) bi[cur] = node | kExpanded;
+                __syncwarp();
+                nexp++;
+                // entries before cur are all expanded; nxt = the next unexpanded one
+                nxt = size;
+                for (uint32_t s0 = cur + 1; s0 < size; s0 += 32) {
+                    const uint32_t idx = s0 + lane;
+                    const bool un = idx < size && !(bi[idx] & kExpanded);
+                    const unsigned b = __ballot_sync(kFull, un);
+                    if (b) {
+                        nxt = s0 + __ffs(b) - 1;
+                        break;
+                    }
+                }
+            } else {
+                if (head >= ncand || overflow) break;
+                node = cl[head++];
+                nfl++;
             }
             uint32_t l0, l1, dg;
             if (node == pre_node) {
@@ -355,11 +374,14 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
             } else {
                 load_links(p, node, lane, l0, l1, dg);
             }
-            // the old beam's next unexpanded entry is the next node unless a
-            // fresh neighbour ranks before it: load its links now, a whole
-            // expansion ahead of their use
-            if (nxt < size) {
+            // links of the likely next node, an expansion ahead of their use:
+            // the old beam's next unexpanded entry (unless a fresh neighbour
+            // ranks before it), or the flood's next candidate
+            if (!flood && nxt < size) {
                 pre_node = bi[nxt] & kIdMask;
+                load_links(p, pre_node, lane, pl0, pl1, pdg);
+            } else if (flood && head < ncand) {
+                pre_node = cl[head];
                 load_links(p, pre_node, lane, pl0, pl1, pdg);
             }
             vis_room(vis, nlog, p.degree, lane, p.err);
@@ -369,9 +391,12 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
             if (m != 0) {
                 if (!fresh_distances<kDim>(p, qhat, ni, nd, m, stage, bar, ph, lane)) return;
                 append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
-                const bool full = size >= L;
-                mk = sort_fresh_kept(nd, ni, m, full, full ? bd[L - 1] : 0.f, full ? bi[L - 1] : 0u, lane, ord);
+                if (!flood) {
+                    const bool full = size >= L;
+                    mk = sort_fresh_kept(nd, ni, m, full, full ? bd[L - 1] : 0.f, full ? bi[L - 1] : 0u, lane, ord);
+                }
             }
+            if (flood) continue;
             if (mk == 0) {
                 // no fresh entry enters the beam: only the cursor moves (to
                 // nxt, whose links are on their way)
@@ -428,34 +453,6 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
             cur = nc;
         }
 
-        // ---- bounded flood, index.h:1626-1638
-        uint32_t head = 0;
-        if (head < ncand && !overflow) {
-            pre_node = cl[0];
-            load_links(p, pre_node, lane, pl0, pl1, pdg);
-        }
-        while (head < ncand && !overflow) {
-            const uint32_t node = cl[head++];
-            nfl++;
-            uint32_t l0, l1, dg;
-            if (node == pre_node) {
-                l0 = pl0;
-                l1 = pl1;
-                dg = pdg;
-            } else {
-                load_links(p, node, lane, l0, l1, dg);
-            }
-            if (head < ncand) {
-                pre_node = cl[head];
-                load_links(p, pre_node, lane, pl0, pl1, pdg);
-            }
-            vis_room(vis, nlog, p.degree, lane, p.err);
-            const uint32_t m = expand_links<kDim>(p, l0, l1, dg, vis, nlog, ni, lane, stage, bar, win, wbase);
-            nvis += m;
-            if (m == 0) continue;
-            if (!fresh_distances<kDim>(p, qhat, ni, nd, m, stage, bar, ph, lane)) return;
-            append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
-        }
         if (overflow && lane == 0) set_error(p.err, kDevCandOverflow);
 
         // ---- candidates out (optional), then the postfilter
