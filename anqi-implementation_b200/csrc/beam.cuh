@@ -204,7 +204,7 @@ __device__ __forceinline__ bool visit_id(Visited& vis, uint32_t* win, uint32_t w
 // common case after the first expansions) are ranked by counting over the kept
 // entries only; larger ones use the register bitonic network, after which the
 // kept entries are a prefix.
-template <class Ord = IdOrder>
+template <class Ord = IdOrder, bool kCompact = false>
 __device__ __forceinline__ uint32_t sort_fresh_kept(float* nd, uint32_t* ni, uint32_t m, bool full, float td,
                                                     uint32_t tid, uint32_t lane, Ord ord = Ord()) {
     if (m <= 32) {
@@ -232,7 +232,7 @@ __device__ __forceinline__ uint32_t sort_fresh_kept(float* nd, uint32_t* ni, uin
     uint32_t i0 = lane < m ? ni[lane] : kEmpty;
     float d1 = lane + 32 < m ? nd[lane + 32] : inf;
     uint32_t i1 = lane + 32 < m ? ni[lane + 32] : kEmpty;
-    warp_sort64(d0, i0, d1, i1, ord);
+    warp_sort64<Ord, kCompact>(d0, i0, d1, i1, ord);
     __syncwarp();
     nd[lane] = d0;
     ni[lane] = i0;

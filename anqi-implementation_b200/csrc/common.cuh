@@ -284,45 +284,58 @@ __device__ __forceinline__ bool kv_less(float da, uint32_t ia, float db, uint32_
     return da < db || (da == db && ia < ib);
 }
 
-// Bitonic sort of 64 (d, id) pairs held two per lane (index lane and lane+32),
-// ascending in the order ord (nb_less by default).  Pads must be (+inf, kEmpty).
-template <class Ord = IdOrder>
-__device__ __forceinline__ void warp_sort64(float& d0, uint32_t& i0, float& d1, uint32_t& i1, Ord ord = Ord()) {
+// One compare-exchange step (stage k, distance j) of the 64-entry bitonic
+// network below.
+template <class Ord>
+__device__ __forceinline__ void bitonic64_step(uint32_t k, uint32_t j, float& d0, uint32_t& i0, float& d1,
+                                               uint32_t& i1, Ord ord) {
     const uint32_t lane = threadIdx.x & 31u;
-    // element e = lane (slot 0) and e = lane + 32 (slot 1)
+    if (j == 32) {
+        // partner of slot 0 is slot 1 of the same lane
+        bool up = ((lane & k) == 0);  // k == 64 here -> always ascending
+        bool sw = up ? ord(d1, i1, d0, i0) : ord(d0, i0, d1, i1);
+        if (sw) {
+            float td = d0; d0 = d1; d1 = td;
+            uint32_t ti = i0; i0 = i1; i1 = ti;
+        }
+    } else {
 #pragma unroll
-    for (uint32_t k = 2; k <= 64; k <<= 1) {
-#pragma unroll
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            if (j == 32) {
-                // partner of slot 0 is slot 1 of the same lane
-                bool up = ((lane & k) == 0);  // k == 64 here -> always ascending
-                bool sw = up ? ord(d1, i1, d0, i0) : ord(d0, i0, d1, i1);
-                if (sw) {
-                    float td = d0; d0 = d1; d1 = td;
-                    uint32_t ti = i0; i0 = i1; i1 = ti;
-                }
-            } else {
-#pragma unroll
-                for (int s = 0; s < 2; s++) {
-                    float& d = s ? d1 : d0;
-                    uint32_t& id = s ? i1 : i0;
-                    const uint32_t e = lane + 32u * s;
-                    float od = __shfl_xor_sync(0xFFFFFFFFu, d, j);
-                    uint32_t oi = __shfl_xor_sync(0xFFFFFFFFu, id, j);
-                    const bool lower = (e & j) == 0;
-                    const bool up = (e & k) == 0;
-                    // keep the smaller if (lower == up)
-                    bool other_less = ord(od, oi, d, id);
-                    bool take = (lower == up) ? other_less : !other_less;
-                    // ties cannot occur between distinct entries (total order)
-                    if (take) {
-                        d = od;
-                        id = oi;
-                    }
-                }
+        for (int s = 0; s < 2; s++) {
+            float& d = s ? d1 : d0;
+            uint32_t& id = s ? i1 : i0;
+            const uint32_t e = lane + 32u * s;
+            float od = __shfl_xor_sync(0xFFFFFFFFu, d, j);
+            uint32_t oi = __shfl_xor_sync(0xFFFFFFFFu, id, j);
+            const bool lower = (e & j) == 0;
+            const bool up = (e & k) == 0;
+            // keep the smaller if (lower == up); ties cannot occur between
+            // distinct entries (total order)
+            bool other_less = ord(od, oi, d, id);
+            bool take = (lower == up) ? other_less : !other_less;
+            if (take) {
+                d = od;
+                id = oi;
             }
         }
+    }
+}
+
+// Bitonic sort of 64 (d, id) pairs held two per lane (index lane and lane+32),
+// ascending in the order ord (nb_less by default).  Pads must be (+inf, kEmpty).
+// kCompact keeps the network as loops (small code, for kernels whose speed
+// depends on instruction fetch and that sort 64 entries rarely).
+template <class Ord = IdOrder, bool kCompact = false>
+__device__ __forceinline__ void warp_sort64(float& d0, uint32_t& i0, float& d1, uint32_t& i1, Ord ord = Ord()) {
+    if constexpr (kCompact) {
+#pragma unroll 1
+        for (uint32_t k = 2; k <= 64; k <<= 1)
+#pragma unroll 1
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) bitonic64_step(k, j, d0, i0, d1, i1, ord);
+    } else {
+#pragma unroll
+        for (uint32_t k = 2; k <= 64; k <<= 1)
+#pragma unroll
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) bitonic64_step(k, j, d0, i0, d1, i1, ord);
     }
 }
 

@@ -393,7 +393,8 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
                 append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
                 if (!flood) {
                     const bool full = size >= L;
-                    mk = sort_fresh_kept(nd, ni, m, full, full ? bd[L - 1] : 0.f, full ? bi[L - 1] : 0u, lane, ord);
+                    mk = sort_fresh_kept<PermOrder, true>(nd, ni, m, full, full ? bd[L - 1] : 0.f,
+                                                          full ? bi[L - 1] : 0u, lane, ord);
                 }
             }
             if (flood) continue;
