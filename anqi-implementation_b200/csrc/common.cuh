@@ -222,6 +222,70 @@ __device__ __forceinline__ float group_ip_w(const float* __restrict__ a, const f
     return res;
 }
 
+// ------------------------------------------------ chunk column order
+// A row layout for 4-thread groups: within each full 16-float chunk, position
+// 4t + k holds element t + 4k, so thread t of the group loads AVX lanes t,
+// t + 4, t + 8, t + 12 as one float4 and the first two fold steps (lane i + 8
+// onto i, then i + 4 onto i) stay in its registers.  Elements from `full` on
+// (the tail) keep their places.  The map is its own inverse.
+__host__ __device__ __forceinline__ uint32_t chunk_col_pos(uint32_t j, uint32_t full) {
+    return j < full ? (j & ~15u) | ((j & 3u) << 2) | ((j >> 2) & 3u) : j;
+}
+
+// Squared L2 (distance.h:58-86) of two rows in chunk column order, dimension
+// kDim known at compile time with a tail of at most 4 elements.  The lane
+// accumulators, the fold tree and the tail are those of group_l2sqr, so the
+// bits are the same; the result is valid in all 4 threads.
+template <uint32_t kDim>
+__device__ __forceinline__ float group_l2sqr_cols(const float* __restrict__ a, const float* __restrict__ b,
+                                                  uint32_t gt, unsigned mask) {
+    constexpr uint32_t q16 = kDim / 16, rem = kDim % 16;
+    static_assert(rem <= 4, "the tail must fit one float4");
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;  // AVX lanes gt, gt + 4, gt + 8, gt + 12
+#pragma unroll
+    for (uint32_t c = 0; c < q16; c++) {
+        const float4 x = *reinterpret_cast<const float4*>(a + 16 * c + 4 * gt);
+        const float4 y = *reinterpret_cast<const float4*>(b + 16 * c + 4 * gt);
+        const float d0 = __fsub_rn(x.x, y.x), d1 = __fsub_rn(x.y, y.y), d2 = __fsub_rn(x.z, y.z),
+                    d3 = __fsub_rn(x.w, y.w);
+        c0 = __fmaf_rn(d0, d0, c0);
+        c1 = __fmaf_rn(d1, d1, c1);
+        c2 = __fmaf_rn(d2, d2, c2);
+        c3 = __fmaf_rn(d3, d3, c3);
+    }
+    // T3[i] = A[i + 8] + A[i]; T6[gt] = T3[gt + 4] + T3[gt]
+    const float t6 = __fadd_rn(__fadd_rn(c3, c1), __fadd_rn(c2, c0));
+    // T8[k] = T6[k + 2] + T6[k]; T8[0] + T8[1] (xor partners: every thread
+    // forms the same sums, addition being commutative)
+    const float t8 = __fadd_rn(__shfl_xor_sync(mask, t6, 2, 4), t6);
+    float res = __fadd_rn(__shfl_xor_sync(mask, t8, 1, 4), t8);
+    if constexpr (rem != 0) {
+        // masked tail, lanes 0..rem-1, products without FMA, same fold:
+        // (p0 + p2) + (p1 + p3) with absent lanes zero (x + 0 = x for the
+        // non-negative squares)
+        const float4 x = *reinterpret_cast<const float4*>(a + 16 * q16);
+        const float4 y = *reinterpret_cast<const float4*>(b + 16 * q16);
+        const float e0 = __fsub_rn(x.x, y.x), p0 = __fmul_rn(e0, e0);
+        float tail = p0;
+        if constexpr (rem >= 2) {
+            const float e1 = __fsub_rn(x.y, y.y), p1 = __fmul_rn(e1, e1);
+            float lo = p0;
+            if constexpr (rem >= 3) {
+                const float e2 = __fsub_rn(x.z, y.z);
+                lo = __fadd_rn(p0, __fmul_rn(e2, e2));
+            }
+            float hi = p1;
+            if constexpr (rem == 4) {
+                const float e3 = __fsub_rn(x.w, y.w);
+                hi = __fadd_rn(p1, __fmul_rn(e3, e3));
+            }
+            tail = __fadd_rn(lo, hi);
+        }
+        res = __fadd_rn(res, tail);
+    }
+    return res;
+}
+
 // ------------------------------------------------------- row staging
 // Global -> shared copies of whole rows with cp.async (16 bytes per
 // instruction, no registers held while in flight): a row costs one memory

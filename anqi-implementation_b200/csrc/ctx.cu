@@ -201,6 +201,34 @@ __global__ void pair_dist_kernel(const float* __restrict__ a, const float* __res
     }
 }
 
+// 4 threads per pair on rows in chunk column order (common.cuh), the layout
+// of the d = 128 search's lifted rows: squared L2 only.
+template <uint32_t kDim>
+__global__ void pair_dist_cols_kernel(const float* __restrict__ a, const float* __restrict__ b, uint64_t m,
+                                      uint32_t stride, float* __restrict__ l2) {
+    const uint32_t lane = threadIdx.x & 31u, gt = lane & 3u, gw = lane >> 2;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t base = warp * 8; base < m; base += nwarps * 8) {
+        const uint64_t row = base + gw;
+        const bool ok = row < m;
+        const uint64_t r = ok ? row : base;
+        const float v = group_l2sqr_cols<kDim>(a + r * stride, b + r * stride, gt, 0xFFFFFFFFu);
+        if (ok && gt == 0) l2[row] = v;
+    }
+}
+
+// dst row i = src row i with each full 16-float chunk in chunk column order.
+__global__ void chunk_cols_kernel(const float* __restrict__ src, float* __restrict__ dst, uint64_t n,
+                                  uint32_t stride, uint32_t full) {
+    const uint64_t total = n * stride;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t row = e / stride;
+        const uint32_t j = (uint32_t)(e - row * stride);
+        dst[e] = src[row * stride + chunk_col_pos(j, full)];
+    }
+}
+
 // three-phase exclusive scan: block sums, one-block scan of the sums, apply
 constexpr uint32_t kScanBlock = 1024;
 
@@ -378,7 +406,9 @@ int anqi_pair_distances(anqi_ctx* h, const float* a, const float* b, uint64_t m,
 
 int anqi_pair_distances_group(anqi_ctx* h, const float* a, const float* b, uint64_t m, uint32_t dim,
                               uint32_t group, float* l2sqr, float* ip) {
-    if (!h || !a || !b || !l2sqr || !ip || dim == 0 || (group != 4 && group != 8 && group != 16)) return ANQI_ERR_ARGS;
+    if (!h || !a || !b || !l2sqr || !ip || dim == 0 || (group != 0 && group != 4 && group != 8 && group != 16) ||
+        (group == 0 && dim != 130))
+        return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     if (m == 0) return ANQI_OK;
@@ -389,6 +419,21 @@ int anqi_pair_distances_group(anqi_ctx* h, const float* a, const float* b, uint6
         (rc = ensure(c, dl, m * 4)) || (rc = ensure(c, di, m * 4)))
         return rc;
     int blocks = (int)std::min<uint64_t>((m * 4 + 255) / 256, (uint64_t)c->sm_count * 16);
+    if (group == 0) {
+        // ip through the 4-thread form, then l2 (overwritten) through the
+        // chunk-column one
+        TmpBuf ca(c), cb(c);
+        if ((rc = ensure(c, ca, m * (size_t)stride * 4)) || (rc = ensure(c, cb, m * (size_t)stride * 4))) return rc;
+        pair_dist_kernel<4><<<blocks, 256, 0, c->stream>>>(da.as<float>(), db.as<float>(), m, dim, stride,
+                                                           dl.as<float>(), di.as<float>());
+        chunk_cols_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(da.as<float>(), ca.as<float>(), m, stride, 128);
+        chunk_cols_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(db.as<float>(), cb.as<float>(), m, stride, 128);
+        pair_dist_cols_kernel<130><<<blocks, 256, 0, c->stream>>>(ca.as<float>(), cb.as<float>(), m, stride,
+                                                                  dl.as<float>());
+        ANQI_CUDA(c, cudaGetLastError());
+        if ((rc = d2h(c, l2sqr, dl, m * 4)) || (rc = d2h(c, ip, di, m * 4)) || (rc = sync(c))) return rc;
+        return ANQI_OK;
+    }
     auto kern = group == 4 ? pair_dist_kernel<4> : group == 8 ? pair_dist_kernel<8> : pair_dist_kernel<16>;
     kern<<<blocks, 256, 0, c->stream>>>(da.as<float>(), db.as<float>(), m, dim, stride, dl.as<float>(),
                                         di.as<float>());

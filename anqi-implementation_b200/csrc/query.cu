@@ -6,20 +6,22 @@
 // ordered beam queue), include/rptrees.h:108-124 (entry descent).
 //
 // Design.  One warp owns one query at a time and pulls queries from a global
-// counter (persistent grid, one resident warp per slot).  The beam lives in
-// shared memory as two sorted (dist, id) arrays that are merged into each
-// other: inserting one expansion's neighbours as a batch leaves exactly the
+// counter (persistent grid), in RP-tree leaf order.  The beam is one sorted
+// (dist, id) array in shared memory; an expansion's fresh neighbours are
+// filtered, sorted and inserted in place as a batch, which leaves exactly the
 // top-L set and first-unexpanded cursor that the reference's one-at-a-time
 // binary insertion leaves, because the queue order is a total order on
 // (dist, id) and no id is inserted twice.  The flood's visited set is a
 // closure, so its result does not depend on visit order either.  Distances are
 // computed by 4-thread groups in the AVX-512 lane order (common.cuh), so every
 // comparison against R2 and every beam decision matches the reference's FP32
-// arithmetic bit for bit.  The visited set is a per-slot bitmap over all
-// objects (L2-resident words, atomicOr test-and-set) cleared by replaying a
-// log of set bits.
+// arithmetic bit for bit.  Objects are renumbered in breadth-first graph order
+// at index load; the visited set is a per-warp window bitmap around the entry
+// object in shared memory, backed by visited tables and a per-warp bitmap
+// over all objects (beam.cuh).  Fresh lifted rows arrive by TMA bulk copies.
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
 #include <cstdlib>
 
 #include "beam.cuh"
@@ -43,6 +45,7 @@ struct SearchParams {
     uint32_t dim, d, lstride, bstride, degree, troot;
     uint32_t stage_rows;  // rows per staging round: 8, 4 or 2 (long rows)
     double scale, R2;
+    float R2f;  // the largest float <= R2 (float distances compare the same against either)
     const float* thr;  // slot-major thresholds
     const float* queries;
     const uint32_t* entry;  // entry object per query (rknn_entry_kernel)
@@ -92,11 +95,26 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 template <uint32_t kDim>
 constexpr uint32_t kSearchRows = kDim == 130 ? 8u : 0u;
 
+// The d = 128 instance also has its row stride fixed, and reads the lifted
+// rows and the lifted query in chunk column order (common.cuh), which
+// anqi_index_load gives the lifted rows for that dimension.
+constexpr uint32_t kColsDim = 130;
+template <uint32_t kDim>
+constexpr uint32_t kSearchLStride = kDim ? (kDim + 7) / 8 * 8 : 0u;
+template <uint32_t kDim>
+__device__ __forceinline__ uint32_t search_lstride(const SearchParams& p) {
+    return kSearchLStride<kDim> ? kSearchLStride<kDim> : p.lstride;
+}
+
 // Bulk (TMA) copy of one row into shared memory, completing on the warp's
-// mbarrier; and the arrive that sets the bytes a phase waits for.
+// mbarrier; and the arrive that sets the bytes a phase waits for.  The
+// staging buffer is written by the generic proxy only through cp.async (the
+// entry row and the postfilter's base rows); the kernel orders those writes
+// before later bulk copies with one proxy fence per query, after the entry
+// row.  Reads of staged rows are complete (their values consumed) before the
+// warp issues the next copies into them.
 __device__ __forceinline__ void bulk_row(float* dst, const float* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("fence.proxy.async.shared::cta;\n"
-                 "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
                  ::"r"(tc::smem_u32(dst)), "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
                  : "memory");
 }
@@ -132,35 +150,40 @@ __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t
     const uint32_t c0 = __popc(b0), lt = lanemask_lt();
     const uint32_t p0 = __popc(b0 & lt), p1 = c0 + __popc(b1 & lt);
     const uint32_t m = c0 + __popc(b1);
-    // table visits are logged for the clean-up (window visits are not)
-    const unsigned h0 = __ballot_sync(kFull, f0 && g0), h1 = __ballot_sync(kFull, f1 && g1);
-    const uint32_t q0 = __popc(h0 & lt), q1 = __popc(h0) + __popc(h1 & lt);
-    const uint32_t rb = p.lstride * 4;
+    const uint32_t ls = search_lstride<kDim>(p), rb = ls * 4;
     if (m) {
         if (lane == 0) bar_expect(bar, min(m, srows) * rb);
-        if (f0 && p0 < srows) bulk_row(stage + (size_t)p0 * p.lstride, p.lifted + (size_t)l0 * p.lstride, rb, bar);
-        if (f1 && p1 < srows) bulk_row(stage + (size_t)p1 * p.lstride, p.lifted + (size_t)l1 * p.lstride, rb, bar);
+        if (f0 && p0 < srows) bulk_row(stage + (size_t)p0 * ls, p.lifted + (size_t)l0 * ls, rb, bar);
+        if (f1 && p1 < srows) bulk_row(stage + (size_t)p1 * ls, p.lifted + (size_t)l1 * ls, rb, bar);
     }
-    const bool logs = vis.level != 0;
-    if (f0) {
-        ni[p0] = l0;
-        if (g0 && logs && nlog + q0 < p.log_cap) vis.vlog[nlog + q0] = r0;
+    if (f0) ni[p0] = l0;
+    if (f1) ni[p1] = l1;
+    // table visits are counted (the level's load) and, above level 0, logged
+    // for the clean-up; window visits are neither
+    if (__any_sync(kFull, (f0 && g0) || (f1 && g1))) {
+        const unsigned h0 = __ballot_sync(kFull, f0 && g0), h1 = __ballot_sync(kFull, f1 && g1);
+        const uint32_t q0 = nlog + __popc(h0 & lt), q1 = nlog + __popc(h0) + __popc(h1 & lt);
+        const bool logs = vis.level != 0;
+        if (logs && f0 && g0 && q0 < p.log_cap) vis.vlog[q0] = r0;
+        if (logs && f1 && g1 && q1 < p.log_cap) vis.vlog[q1] = r1;
+        nlog += __popc(h0) + __popc(h1);
     }
-    if (f1) {
-        ni[p1] = l1;
-        if (g1 && logs && nlog + q1 < p.log_cap) vis.vlog[nlog + q1] = r1;
-    }
-    nlog += __popc(h0) + __popc(h1);
     __syncwarp();
     return m;
 }
 
+// Issues the loads of node's degree and link slots lane and lane + 32.  No
+// instruction here uses the loaded values, so the warp does not wait for them
+// until it expands the node (usually one expansion later).  Slots at or past
+// the degree are never used; the links array has 64 padding entries, so the
+// loads past the last row stay in bounds, and degrees were checked against the
+// slot count at index load.
 __device__ __forceinline__ void load_links(const SearchParams& p, uint32_t node, uint32_t lane, uint32_t& l0,
                                            uint32_t& l1, uint32_t& dg) {
     const uint32_t* lk = p.links + (size_t)node * p.degree;
-    dg = min(p.deg[node], p.degree);
-    l0 = lane < p.degree ? lk[lane] : kEmpty;
-    l1 = lane + 32 < p.degree ? lk[lane + 32] : kEmpty;
+    dg = p.deg[node];
+    l0 = lk[lane];
+    l1 = lk[lane + 32];
 }
 
 // Distance of staged row `row` to the lifted query by a group of G threads
@@ -183,12 +206,12 @@ __device__ __forceinline__ bool fresh_distances(const SearchParams& p, const flo
                                                 uint32_t lane) {
     const uint32_t dim = kDim ? kDim : p.dim;
     const uint32_t srows = kSearchRows<kDim> ? kSearchRows<kDim> : p.stage_rows;
-    const uint32_t rb = p.lstride * 4;
+    const uint32_t ls = search_lstride<kDim>(p), rb = ls * 4;
     for (uint32_t r0 = 0; r0 < m; r0 += srows) {
         const uint32_t nr = min(m - r0, srows);
         if (r0 > 0) {
             if (lane == 0) bar_expect(bar, nr * rb);
-            if (lane < nr) bulk_row(stage + (size_t)lane * p.lstride, p.lifted + (size_t)ni[r0 + lane] * p.lstride, rb, bar);
+            if (lane < nr) bulk_row(stage + (size_t)lane * ls, p.lifted + (size_t)ni[r0 + lane] * ls, rb, bar);
         }
         if (!tc::mbar_wait(bar, ph, kRowWaitPolls)) {
             set_error(p.err, kDevWaitTimeout);
@@ -197,16 +220,19 @@ __device__ __forceinline__ bool fresh_distances(const SearchParams& p, const flo
         ph ^= 1u;
         if (srows == 2) {
             const uint32_t gw = lane >> 4, gt = lane & 15u;
-            const float da = row_l2sqr<16>(stage + (size_t)gw * p.lstride, qhat, dim, gt);
+            const float da = row_l2sqr<16>(stage + (size_t)gw * ls, qhat, dim, gt);
             if (gt == 0 && gw < nr) nd[r0 + gw] = da;
         } else if (srows == 4) {
             const uint32_t gw = lane >> 3, gt = lane & 7u;
-            const float da = row_l2sqr<8>(stage + (size_t)gw * p.lstride, qhat, dim, gt);
+            const float da = row_l2sqr<8>(stage + (size_t)gw * ls, qhat, dim, gt);
             if (gt == 0 && gw < nr) nd[r0 + gw] = da;
         } else {
             const uint32_t gw = lane >> 2, gt = lane & 3u;
             const bool oka = gw < nr;
-            const float da = row_l2sqr<4>(oka ? stage + (size_t)gw * p.lstride : stage, qhat, dim, gt);
+            const float* row = oka ? stage + (size_t)gw * ls : stage;
+            float da;
+            if constexpr (kDim == kColsDim) da = group_l2sqr_cols<kColsDim>(row, qhat, gt, kFull);
+            else da = row_l2sqr<4>(row, qhat, dim, gt);
             if (gt == 0 && oka) nd[r0 + gw] = da;
         }
         __syncwarp();
@@ -214,12 +240,14 @@ __device__ __forceinline__ bool fresh_distances(const SearchParams& p, const flo
     return true;
 }
 
-// Appends fresh neighbours within R2 to the candidate / flood list (visit order).
+// Appends fresh neighbours within R2 to the candidate / flood list (visit
+// order).  For a float x, (double)x <= R2 exactly when x <= R2f, the largest
+// float not above R2.
 __device__ __forceinline__ void append_in_range(const SearchParams& p, const float* nd, const uint32_t* ni,
                                                 uint32_t m, uint32_t* cl, uint32_t& ncand, bool& overflow,
                                                 uint32_t lane) {
-    const bool in0 = lane < m && (double)nd[lane] <= p.R2;
-    const bool in1 = lane + 32 < m && (double)nd[lane + 32] <= p.R2;
+    const bool in0 = lane < m && nd[lane] <= p.R2f;
+    const bool in1 = lane + 32 < m && nd[lane + 32] <= p.R2f;
     const unsigned b0 = __ballot_sync(kFull, in0), b1 = __ballot_sync(kFull, in1);
     const uint32_t c0 = __popc(b0), lt = lanemask_lt();
     const uint32_t pos0 = ncand + __popc(b0 & lt), pos1 = ncand + c0 + __popc(b1 & lt);
@@ -255,17 +283,18 @@ template <uint32_t kDim>
 __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
-    const size_t per_warp = search_smem_words(p.L_max, p.lstride, p.bstride, p.hash_cap) * 4;
+    const uint32_t ls = search_lstride<kDim>(p);
+    const size_t per_warp = search_smem_words(p.L_max, ls, p.bstride, p.hash_cap) * 4;
     unsigned char* my = g_smem + wib * per_warp;
     float* qhat = reinterpret_cast<float*>(my);
-    uint32_t* win = reinterpret_cast<uint32_t*>(qhat + p.lstride);  // window bitmap, kWinWords
+    uint32_t* win = reinterpret_cast<uint32_t*>(qhat + ls);  // window bitmap, kWinWords
     float* bd = reinterpret_cast<float*>(win + kWinWords);  // the beam: sorted (dist, id), expanded flag in the id's top bit
     uint32_t* bi = reinterpret_cast<uint32_t*>(bd + p.L_max);
     float* nd = reinterpret_cast<float*>(bi + p.L_max);
     uint32_t* ni = reinterpret_cast<uint32_t*>(nd + 64);
     float* stage = reinterpret_cast<float*>(ni + 64);  // stage_rows staged rows of max(lstride, bstride)
     const uint32_t srows = kSearchRows<kDim> ? kSearchRows<kDim> : p.stage_rows;
-    uint32_t* tab = reinterpret_cast<uint32_t*>(stage + srows * (size_t)max(p.lstride, p.bstride));
+    uint32_t* tab = reinterpret_cast<uint32_t*>(stage + srows * (size_t)max(ls, p.bstride));
     uint64_t* bar = reinterpret_cast<uint64_t*>(tab + p.hash_cap);  // row-copy mbarrier of this warp
     uint32_t ph = 0;
     if (lane == 0) {
@@ -291,12 +320,12 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
         const uint32_t L = min(p.qL ? p.qL[qi] : p.L_all, p.L_max);
         const uint32_t tslot = p.qslot ? p.qslot[qi] : p.slot_all;
         const float* q = p.queries + (size_t)qi * p.bstride;
-        // query lift, rknn_query.cpp:2724-2729
-        for (uint32_t j = lane; j < p.lstride; j += 32) {
+        // query lift, rknn_query.cpp:2724-2729 (in the rows' column order)
+        for (uint32_t j = lane; j < ls; j += 32) {
             float v = 0.0f;
             if (j < p.d) v = __double2float_rn(__dmul_rn((double)q[j], p.scale));
             else if (j == p.d) v = 1.0f;
-            qhat[j] = v;
+            qhat[kDim == kColsDim ? chunk_col_pos(j, kColsDim / 16 * 16) : j] = v;
         }
         __syncwarp();
         uint32_t ep = p.entry[qi];
@@ -308,10 +337,15 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
 
         Visited vis{tab,  p.hash_cap, p.hash_shift, p.gtab ? p.gtab + (size_t)slot * p.gcap : nullptr,
                     p.gcap, p.gshift, bits, vlog, p.log_cap, p.hash_cap ? 0u : (p.gcap ? 1u : 2u)};
-        stage_row_async(stage, p.lifted + (size_t)ep * p.lstride, p.lstride, lane, 32);
+        stage_row_async(stage, p.lifted + (size_t)ep * ls, ls, lane, 32);
         cp_async_wait_all();
+        // generic-proxy writes to the staging buffer (this row, the last
+        // query's base rows) before the bulk copies of this query
+        tc::fence_async_smem();
         __syncwarp();
-        const float dep = group_l2sqr(stage, qhat, p.dim, gt, kFull);
+        float dep;
+        if constexpr (kDim == kColsDim) dep = group_l2sqr_cols<kColsDim>(stage, qhat, gt, kFull);
+        else dep = group_l2sqr(stage, qhat, p.dim, gt, kFull);
         __syncwarp();
         if (lane == 0) {
             win[(ep - wbase) >> 5] |= 1u << ((ep - wbase) & 31u);  // the entry lies in the window
@@ -320,7 +354,7 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
         }
         uint32_t nlog = 0, nvis = 1, ncand = 0, nexp = 0, nfl = 0;
         bool overflow = false;
-        if ((double)dep <= p.R2) {
+        if (dep <= p.R2f) {
             if (lane == 0) cl[0] = ep;
             ncand = 1;
         }
@@ -475,7 +509,7 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
         // base rows in rounds of srows, G = 32 / srows threads per row
         const uint32_t G = srows == 8 ? 4u : (srows == 4 ? 8u : 16u);
         const uint32_t pg = srows == 8 ? lane >> 2 : (srows == 4 ? lane >> 3 : lane >> 4), pt = lane & (G - 1);
-        float* brow = stage + (size_t)pg * max(p.lstride, p.bstride);
+        float* brow = stage + (size_t)pg * max(ls, p.bstride);
         for (uint32_t r0 = 0; r0 < ncand; r0 += srows) {
             const uint32_t idx = r0 + pg;
             const bool ok = idx < ncand;
@@ -488,7 +522,7 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
                                     : (G == 8 ? group_ip_w<8>(rr, q, p.d, pt, kFull)
                                               : group_ip_w<16>(rr, q, p.d, pt, kFull));
             const float key = __fsub_rn(__fadd_rn(p.onorm[o], qn), __fmul_rn(2.0f, ip));
-            const bool pass = ok && (double)key <= (double)thr[o];
+            const bool pass = ok && key <= thr[o];  // (double) of both sides in the reference: same order
             const unsigned b = __ballot_sync(kFull, pass && pt == 0);
             __syncwarp();
             if (pass && pt == 0) cl[npred + __popc(b & lanemask_lt())] = o;
@@ -720,13 +754,21 @@ __global__ void eval_sums_kernel(const double* __restrict__ rows, const uint32_t
 }
 
 // dst[i] = src[perm[i]] for rows of `stride` floats (warp per row).
+// With cols_full > 0, each row's first cols_full elements are stored in chunk
+// column order (common.cuh).
 __global__ void permute_rows_kernel(const float* __restrict__ src, float* __restrict__ dst,
-                                    const uint32_t* __restrict__ perm, uint64_t n, uint32_t stride) {
+                                    const uint32_t* __restrict__ perm, uint64_t n, uint32_t stride,
+                                    uint32_t cols_full) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = w0; i < n; i += nw) {
-        const float4* s4 = reinterpret_cast<const float4*>(src + (uint64_t)perm[i] * stride);
+        const float* s = src + (uint64_t)perm[i] * stride;
+        if (cols_full) {
+            for (uint32_t t = lane; t < stride; t += 32) dst[i * stride + t] = s[chunk_col_pos(t, cols_full)];
+            continue;
+        }
+        const float4* s4 = reinterpret_cast<const float4*>(s);
         float4* d4 = reinterpret_cast<float4*>(dst + i * stride);
         for (uint32_t t = lane; t < stride / 4; t += 32) d4[t] = s4[t];
     }
@@ -768,7 +810,7 @@ static size_t search_smem_per_warp(const Ctx* c, uint32_t L_max, uint32_t hash_c
 // The search kernel for lifted dimension dim: 130 (d = 128) has its distance
 // loops unrolled at compile time.
 static void (*search_kernel_for(uint32_t dim))(SearchParams) {
-    return dim == 130 ? rknn_search_kernel<130> : rknn_search_kernel<0>;
+    return dim == kColsDim ? rknn_search_kernel<kColsDim> : rknn_search_kernel<0>;
 }
 
 struct SearchCfg {
@@ -862,7 +904,8 @@ int anqi_index_load(anqi_ctx* h, const anqi_index_desc* x) {
             }
         }
     }
-    std::vector<uint32_t> rank(n), deg_r(n), links_r(n * (size_t)x->degree, kEmpty), leaf_r(x->tree_leaf_first,
+    // 64 padding entries: the search loads link slots 0..63 of a row whatever its degree
+    std::vector<uint32_t> rank(n), deg_r(n), links_r(n * (size_t)x->degree + 64, kEmpty), leaf_r(x->tree_leaf_first,
                                                                                          x->tree_leaf_first + x->tree_nodes);
     for (uint64_t i = 0; i < n; i++) rank[perm[i]] = (uint32_t)i;
     for (uint64_t i = 0; i < n; i++) {
@@ -881,14 +924,16 @@ int anqi_index_load(anqi_ctx* h, const anqi_index_desc* x) {
             return rc;
         const uint32_t blocks = c->sm_count * 8;
         permute_rows_kernel<<<blocks, 256, 0, c->stream>>>(tb.as<float>(), ix.base.as<float>(), ix.perm.as<uint32_t>(),
-                                                           n, ix.bstride);
+                                                           n, ix.bstride, 0u);
+        // the d = 128 search instance reads its lifted rows in chunk column order
         permute_rows_kernel<<<blocks, 256, 0, c->stream>>>(tl.as<float>(), ix.lifted.as<float>(),
-                                                           ix.perm.as<uint32_t>(), n, ix.lstride);
+                                                           ix.perm.as<uint32_t>(), n, ix.lstride,
+                                                           ix.dim == kColsDim ? kColsDim / 16 * 16 : 0u);
         ANQI_CUDA(c, cudaGetLastError());
         if ((rc = sync(c))) return rc;
     }
     if ((rc = ensure(c, ix.onorm, n * 4)) || (rc = h2d(c, ix.deg, deg_r.data(), n * 4)) ||
-        (rc = h2d(c, ix.links, links_r.data(), n * (size_t)x->degree * 4)) ||
+        (rc = h2d(c, ix.links, links_r.data(), links_r.size() * 4)) ||
         (rc = h2d(c, ix.tleft, x->tree_left, x->tree_nodes * 4)) ||
         (rc = h2d(c, ix.tright, x->tree_right, x->tree_nodes * 4)) ||
         (rc = h2d(c, ix.toffset, x->tree_offset, x->tree_nodes * 4)) ||
@@ -1073,6 +1118,8 @@ static int enqueue_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, boo
     p.stage_rows = stage_rows_for(ix.lstride, ix.bstride);
     p.scale = ix.scale;
     p.R2 = ix.mstar2 + 1.0;  // rknn_query.cpp:2729, eps = 0
+    p.R2f = (float)p.R2;
+    if ((double)p.R2f > p.R2) p.R2f = std::nextafter(p.R2f, -INFINITY);
     p.thr = c->thr_table.as<float>();
     p.queries = b.q.as<float>();
     p.entry = b.entry.as<uint32_t>();

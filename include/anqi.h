@@ -54,7 +54,9 @@ int anqi_timer_stop(anqi_ctx* ctx, float* ms);
 int anqi_pair_distances(anqi_ctx* ctx, const float* a, const float* b, uint64_t m, uint32_t dim,
                         float* l2sqr, float* ip);
 /* The same with `group` = 4, 8 or 16 threads per pair: the forms the kernels
- * use for many short rows, few rows and long rows; identical results. */
+ * use for many short rows, few rows and long rows; identical results.
+ * group = 0 (dim 130 only): l2sqr by the d = 128 search's form, 4 threads per
+ * pair on rows stored with each 16-float chunk transposed as 4 x 4. */
 int anqi_pair_distances_group(anqi_ctx* ctx, const float* a, const float* b, uint64_t m, uint32_t dim,
                               uint32_t group, float* l2sqr, float* ip);
 
