@@ -212,12 +212,24 @@ __device__ __forceinline__ uint32_t sort_fresh_kept(float* nd, uint32_t* ni, uin
         const uint32_t iv = lane < m ? ni[lane] : kEmpty;
         const bool keep = lane < m && (!full || ord(dv, iv, td, tid));
         const unsigned km = __ballot_sync(kAll, keep);
-        uint32_t rank = 0;
+        // rank by distance alone, counting equal distances; only kept lanes
+        // use their rank
+        uint32_t rank = 0, ties = 0;
         for (unsigned r = km; r; r &= r - 1) {
             const int s = __ffs(r) - 1;
             const float ds = __shfl_sync(kAll, dv, s);
-            const uint32_t is = __shfl_sync(kAll, iv, s);
-            rank += (keep && ord(ds, is, dv, iv)) ? 1u : 0u;  // only kept lanes use their rank
+            rank += ds < dv ? 1u : 0u;
+            ties += (ds == dv && s != (int)lane) ? 1u : 0u;
+        }
+        if (__any_sync(kAll, keep && ties != 0)) {
+            // two kept entries at one distance: rank by the full order
+            rank = 0;
+            for (unsigned r = km; r; r &= r - 1) {
+                const int s = __ffs(r) - 1;
+                const float ds = __shfl_sync(kAll, dv, s);
+                const uint32_t is = __shfl_sync(kAll, iv, s);
+                rank += (keep && ord(ds, is, dv, iv)) ? 1u : 0u;
+            }
         }
         __syncwarp();
         if (keep) {
