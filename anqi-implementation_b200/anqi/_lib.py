@@ -325,21 +325,37 @@ class Context:
         assert a.shape == (nq,)
         return a, 0
 
-    def rknn_query(self, queries, k, L, keep_candidates=False, pred_cap=None) -> QueryResult:
-        """Host-buffer end-to-end call (queries H2D, results D2H inside)."""
+    def rknn_query(self, queries, k, L, keep_candidates=False, pred_cap=None, out=None) -> QueryResult:
+        """Host-buffer end-to-end call (queries H2D, results D2H inside).
+
+        out: optional (pred_off, pred_ids, n_dist) uint32 arrays of nq + 1,
+        any capacity and nq entries -- e.g. pinned buffers reused across
+        calls; the results are then copied straight into them (a larger
+        pred_ids is allocated if the results outgrow it)."""
         queries = _c(queries, np.float32)
         nq = queries.shape[0]
         ka, kall = self._per_query(k, nq)
         La, Lall = self._per_query(L, nq)
         st = QueryStats()
         cap = pred_cap or max(1024, nq * 256)
+        if out is not None:
+            o_off, o_ids, o_nd = out
+            if (o_off.dtype != np.uint32 or o_ids.dtype != np.uint32 or o_nd.dtype != np.uint32
+                    or o_off.shape != (nq + 1,) or o_nd.shape != (nq,) or o_ids.ndim != 1
+                    or not (o_off.flags.c_contiguous and o_ids.flags.c_contiguous and o_nd.flags.c_contiguous)):
+                raise ValueError("out: uint32 C-contiguous arrays of nq + 1, any and nq entries")
+            cap = len(o_ids)
         while True:
-            pred_off = np.empty(nq + 1, np.uint32)
-            pred_ids = np.empty(cap, np.uint32)
+            if out is not None and cap == len(out[1]):
+                pred_off, pred_ids, nd = out
+            else:
+                pred_off = np.empty(nq + 1, np.uint32)
+                pred_ids = np.empty(cap, np.uint32)
             cand_off = np.empty(nq + 1, np.uint32) if keep_candidates else None
             ccap = cap * 4 if keep_candidates else 0
             cand_ids = np.empty(ccap, np.uint32) if keep_candidates else None
-            nd = np.empty(nq, np.uint32)
+            if out is None or cap != len(out[1]):
+                nd = np.empty(nq, np.uint32)
             rc = self.lib.anqi_rknn_query(self.h, queries, nq, _ptr(ka), kall, _ptr(La), Lall, pred_off, pred_ids, cap,
                                           _ptr(cand_off), _ptr(cand_ids), ccap, _ptr(nd), C.byref(st))
             if rc == ANQI_ERR_CAPACITY:
@@ -348,6 +364,10 @@ class Context:
             self._check(rc, "rknn_query")
             break
         stats = {k2: getattr(st, k2) for k2, _ in QueryStats._fields_}
+        if out is not None and pred_ids is out[1]:
+            # the caller's buffers hold the results: views, no copies
+            return QueryResult(pred_off, pred_ids[:pred_off[-1]], cand_off,
+                               None if cand_ids is None else cand_ids[:cand_off[-1]].copy(), nd, stats)
         return QueryResult(pred_off, pred_ids[:pred_off[-1]].copy(), cand_off,
                            None if cand_ids is None else cand_ids[:cand_off[-1]].copy(), nd, stats)
 

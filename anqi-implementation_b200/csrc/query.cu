@@ -989,8 +989,13 @@ int anqi_verifier_materialize(anqi_ctx* h, uint32_t k, double radius_scale) {
     return ANQI_OK;
 }
 
-int anqi_query_upload(anqi_ctx* h, const float* queries, uint32_t nq, const uint32_t* k_per_query, uint32_t k_all,
-                      const uint32_t* L_per_query, uint32_t L_all) {
+}  // extern "C"
+
+// The upload; with sync_after false the copies may still be in flight from
+// the caller's buffers on return (anqi_rknn_query, which synchronizes before
+// it returns).
+static int query_upload(anqi_ctx* h, const float* queries, uint32_t nq, const uint32_t* k_per_query, uint32_t k_all,
+                        const uint32_t* L_per_query, uint32_t L_all, bool sync_after) {
     if (!h || !queries || nq == 0) return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
@@ -1037,8 +1042,15 @@ int anqi_query_upload(anqi_ctx* h, const float* queries, uint32_t nq, const uint
         (rc = ensure(c, b.cand_at, q8)) || (rc = ensure(c, b.pred_off, q4 + 4)) ||
         (rc = ensure(c, b.cand_off, q4 + 4)))
         return rc;
-    return sync(c);
+    return sync_after ? sync(c) : ANQI_OK;
 }
+
+extern "C" int anqi_query_upload(anqi_ctx* h, const float* queries, uint32_t nq, const uint32_t* k_per_query,
+                                 uint32_t k_all, const uint32_t* L_per_query, uint32_t L_all) {
+    return query_upload(h, queries, nq, k_per_query, k_all, L_per_query, L_all, true);
+}
+
+extern "C" {
 
 // Entry objects of the batch (lift + RP-tree descent) and, unless
 // ANQI_B200_ORDER=0, the work list ordered by entry leaf.
@@ -1211,7 +1223,11 @@ static int enqueue_compaction(Ctx* c, int keep_candidates) {
     return ANQI_OK;
 }
 
-int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
+}  // extern "C"
+
+// The run; with sync_after false it returns once the last kernel is enqueued
+// (the search itself is always waited for: its output sizes are checked).
+static int query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st, bool sync_after) {
     if (!h) return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
@@ -1328,10 +1344,16 @@ int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
             st->visited_table = best.hash_cap;
             st->visited_l2_table = best.gcap;
         }
-        return sync(c);
+        return sync_after ? sync(c) : ANQI_OK;
     }
     return fail(c, ANQI_ERR_CAPACITY, "rknn search: output capacity could not be satisfied");
 }
+
+extern "C" int anqi_query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st) {
+    return query_run(h, keep_candidates, st, true);
+}
+
+extern "C" {
 
 // Everything a captured query graph depends on: batch shape and mode, search
 // configuration, output capacities and every device buffer it touches.
@@ -1469,10 +1491,15 @@ int anqi_rknn_query(anqi_ctx* h, const float* queries, uint32_t nq, const uint32
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     ANQI_CUDA(c, cudaEventRecord(c->ev2, c->stream));
-    int rc = anqi_query_upload(h, queries, nq, k_per_query, k_all, L_per_query, L_all);
-    if (rc) return rc;
-    rc = anqi_query_run(h, cand_off != nullptr, st);
-    if (rc) return rc;
+    // no host round trip between the upload, the run and the first copy back;
+    // on an error the stream is drained before the caller's buffers are
+    // handed back
+    int rc = query_upload(h, queries, nq, k_per_query, k_all, L_per_query, L_all, false);
+    if (!rc) rc = query_run(h, cand_off != nullptr, st, false);
+    if (rc) {
+        cudaStreamSynchronize(c->stream);
+        return rc;
+    }
     rc = anqi_query_download(h, pred_off, pred_ids, pred_cap, cand_off, cand_ids, cand_cap, n_dist);
     if (rc) return rc;
     ANQI_CUDA(c, cudaEventRecord(c->ev3, c->stream));

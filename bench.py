@@ -14,8 +14,8 @@ k = 10, 50 and 100 (per-query k in a single launch), beam width L for all.
 ``value`` is queries/s over K steps with the batch resident in HBM (CUDA events
 on the library's stream; each step one replay of the batch's CUDA graph);
 ``e2e`` is the same through the host-buffer C ABI
-call (query upload from pinned memory and result download inside the timed
-region).  The timed working set (lifted + base vectors, graph) is ~1.3 GB,
+call (query upload from pinned memory and result download into pinned
+buffers reused across calls, both inside the timed region).  The timed working set (lifted + base vectors, graph) is ~1.3 GB,
 larger than the 126 MB L2.
 
 ``--impl reference`` times the reference's own CPU query code (its
@@ -344,12 +344,17 @@ def run_ours(a, rank, world, local):
     pin_k[:] = kb
     pin_L = torch.empty(Lb.shape, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     pin_L[:] = Lb
+    r = ctx.rknn_query(pin_q, pin_k, pin_L)
+    # results land in pinned buffers reused by every call, as a serving loop does
+    def pinned_u32(n):
+        return torch.empty(n, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    out = (pinned_u32(nb + 1), pinned_u32(int(r.pred_off[-1]) + 4096), pinned_u32(nb))
     for _ in range(a.warmup):
-        r = ctx.rknn_query(pin_q, pin_k, pin_L)
+        r = ctx.rknn_query(pin_q, pin_k, pin_L, out=out)
     e2e_stats = []
     ctx.timer_start()
     for _ in range(a.steps):
-        r = ctx.rknn_query(pin_q, pin_k, pin_L, pred_cap=int(r.pred_off[-1]) + 4096)
+        r = ctx.rknn_query(pin_q, pin_k, pin_L, out=out)
         e2e_stats.append(r.stats)
     e2e_ms = ctx.timer_stop()
     from anqi.dist import max_over_ranks

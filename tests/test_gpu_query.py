@@ -288,6 +288,26 @@ def test_query_graph_replay_equals_plain(ctx, random_index):
             assert st["search_ms"] > 0
 
 
+def test_rknn_query_into_caller_buffers(ctx, random_index):
+    """out=: results copied straight into caller-owned buffers reused across
+    calls (views returned), and a pred buffer too small for the results is
+    replaced by a larger one; same results as the allocating call."""
+    base, query, lifted, links, deg, tree, sc, m2, thr = random_index
+    ctx.index_load(base, lifted, deg, links, tree, sc, m2)
+    ctx.set_thresholds(10, thr[10])
+    want = ctx.rknn_query(query, 10, 64)
+    nq = len(query)
+    out = (np.empty(nq + 1, np.uint32), np.empty(int(want.pred_off[-1]) + 10, np.uint32), np.empty(nq, np.uint32))
+    for _ in range(2):
+        got = ctx.rknn_query(query, 10, 64, out=out)
+        assert np.shares_memory(got.pred_ids, out[1]) and got.pred_off is out[0]
+        assert np.array_equal(got.pred_off, want.pred_off) and np.array_equal(got.pred_ids, want.pred_ids)
+        assert np.array_equal(got.n_dist, want.n_dist)
+    small = (np.empty(nq + 1, np.uint32), np.empty(3, np.uint32), np.empty(nq, np.uint32))
+    got = ctx.rknn_query(query, 10, 64, out=small)
+    assert np.array_equal(got.pred_off, want.pred_off) and np.array_equal(got.pred_ids, want.pred_ids)
+
+
 def test_resident_batch_and_evaluate(ctx, random_index):
     base, query, lifted, links, deg, tree, sc, m2, thr = random_index
     ctx.index_load(base, lifted, deg, links, tree, sc, m2)
