@@ -188,7 +188,7 @@ int cmd_graph(int argc, char** argv) {
     const size_t nnk = std::strtoull(argv[4], nullptr, 10), M = std::strtoull(argv[5], nullptr, 10);
     size_t n = 0, dim = 0;
     read_fbin(lifted, n, dim);
-    Parms par = lifted_parms(n, dim, nnk, M, out + "_work/");
+    Parms par = lifted_parms(n, dim, nnk, M, out + "_scratch/");
     nndindex index(lifted, par);
     // Warm-start IDs: the interleaved {u32 id, f32 key} top-100 records.
     std::vector<uint32_t> ids(n * 100);
@@ -279,7 +279,7 @@ int cmd_aknn(int argc, char** argv) {
     po.prune_alpha = 1.2f;
     po.explore_range = ef;
     po.n_threads = 1;
-    po.folder_path = out + "_work/";
+    po.folder_path = out + "_scratch/";
     nndindex index(base, po);
     float* cvec = static_cast<float*>(_mm_malloc(n * d * sizeof(float), 64));
     for (size_t i = 0; i < n; i++) std::memcpy(cvec + i * d, index.vec(i), d * sizeof(float));
@@ -378,7 +378,7 @@ int cmd_query(int argc, char** argv) {
     load_query_env(e, argv + 2);
     const size_t L = std::strtoull(argv[8], nullptr, 10);
     const std::string out = argv[9];
-    Parms par = lifted_parms(e.n, e.dim, 50, 48, out + "_work/");
+    Parms par = lifted_parms(e.n, e.dim, 50, 48, out + "_scratch/");
     nndindex index(argv[2], par);
     load_graph_file(index, argv[3]);
     std::vector<uint16_t> mark(e.n, 0);

@@ -261,7 +261,7 @@ def test_aknn_gather_beam_path_vs_oracle(ctx):
 
 def test_aknn_build_recall(ctx):
     """End-to-end AKNN source build: recall@K vs exact, as the reference's own
-    build_aknn_source gets on the same data (0.98 at 50k in the survey)."""
+    build_aknn_source gets on such data (0.98 at 50k on the reference recipe)."""
     x = clustered(20000, 32, 51, nc=200)
     n, d = x.shape
     K = 50
