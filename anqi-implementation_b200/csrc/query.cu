@@ -1008,10 +1008,15 @@ static int query_upload(anqi_ctx* h, const float* queries, uint32_t nq, const ui
     uint32_t slot_all = 0;
     if (k_per_query) {
         slots.resize(nq);
+        uint32_t last_k = 0;
+        int last_s = -1;  // slot of last_k (batches hold runs of equal k)
         for (uint32_t i = 0; i < nq; i++) {
-            int s = slot_for_k(c, k_per_query[i]);
-            if (s < 0) return fail(c, ANQI_ERR_ARGS, "no thresholds materialized for k=%u", k_per_query[i]);
-            slots[i] = (uint8_t)s;
+            if (last_s < 0 || k_per_query[i] != last_k) {
+                last_k = k_per_query[i];
+                last_s = slot_for_k(c, last_k);
+                if (last_s < 0) return fail(c, ANQI_ERR_ARGS, "no thresholds materialized for k=%u", last_k);
+            }
+            slots[i] = (uint8_t)last_s;
         }
     } else {
         int s = slot_for_k(c, k_all);
@@ -1019,14 +1024,16 @@ static int query_upload(anqi_ctx* h, const float* queries, uint32_t nq, const ui
         slot_all = (uint32_t)s;
     }
     uint32_t L_max = L_all;
+    bool L_zero = false;
     if (L_per_query) {
         L_max = 0;
-        for (uint32_t i = 0; i < nq; i++) L_max = std::max(L_max, L_per_query[i]);
+        for (uint32_t i = 0; i < nq; i++) {
+            L_max = std::max(L_max, L_per_query[i]);
+            L_zero |= L_per_query[i] == 0;
+        }
     }
     if (L_max == 0 || L_max > 4096) return fail(c, ANQI_ERR_ARGS, "beam width must be in [1, 4096]");
-    if (L_per_query)
-        for (uint32_t i = 0; i < nq; i++)
-            if (L_per_query[i] == 0) return fail(c, ANQI_ERR_ARGS, "beam width must be positive");
+    if (L_zero) return fail(c, ANQI_ERR_ARGS, "beam width must be positive");
     b.L_max = round_up(L_max, 4);
     b.has_k = k_per_query != nullptr;
     b.has_L = L_per_query != nullptr;

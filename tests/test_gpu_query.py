@@ -8,7 +8,7 @@ import pytest
 
 import oracle_lib as ol
 from anqi import formats
-from anqi._lib import Context
+from anqi._lib import AnqiError, Context
 
 pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -305,6 +305,33 @@ def test_rknn_query_into_caller_buffers(ctx, random_index):
         assert np.array_equal(got.n_dist, want.n_dist)
     small = (np.empty(nq + 1, np.uint32), np.empty(3, np.uint32), np.empty(nq, np.uint32))
     got = ctx.rknn_query(query, 10, 64, out=small)
+    assert np.array_equal(got.pred_off, want.pred_off) and np.array_equal(got.pred_ids, want.pred_ids)
+
+
+def test_query_upload_rejects_bad_k_and_L(ctx, random_index):
+    """Per-query k without materialized thresholds, a zero beam width and a
+    beam width above 4,096 are argument errors (status 2) naming the value;
+    the context then runs a valid batch as before."""
+    base, query, lifted, links, deg, tree, sc, m2, thr = random_index
+    ctx.index_load(base, lifted, deg, links, tree, sc, m2)
+    ctx.set_thresholds(10, thr[10])
+    want = ctx.rknn_query(query, 10, 64)
+    nq = len(query)
+    ks = np.full(nq, 10, np.uint32)
+    ks[nq // 2] = 77
+    with pytest.raises(AnqiError, match="k=77") as e:
+        ctx.query_upload(query, ks, 64)
+    assert e.value.status == 2
+    Ls = np.full(nq, 64, np.uint32)
+    Ls[5] = 0
+    with pytest.raises(AnqiError, match="positive") as e:
+        ctx.query_upload(query, 10, Ls)
+    assert e.value.status == 2
+    Ls[5] = 5000
+    with pytest.raises(AnqiError, match="4096") as e:
+        ctx.rknn_query(query, 10, Ls)
+    assert e.value.status == 2
+    got = ctx.rknn_query(query, np.full(nq, 10, np.uint32), 64)
     assert np.array_equal(got.pred_off, want.pred_off) and np.array_equal(got.pred_ids, want.pred_ids)
 
 
