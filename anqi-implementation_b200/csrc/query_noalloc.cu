@@ -18,7 +18,16 @@
 // overlaps on the GPU (different streams, or different host threads) race on
 // it -- serialize them.  The first call on each device looks up the array's
 // device address (cudaGetSymbolAddress, with that device current); make that
-// first call before any stream capture begins.
+// first call before any stream capture begins.  Every call also ends by
+// reading the error word back and synchronizing the caller's stream, so no
+// call can be made while that stream is being captured.
+//
+// Concurrency: each query in flight holds one slot of the array (a visited
+// bitmap of n/8 bytes plus 40 KB of log and candidate list).  A block runs up
+// to four warps, one query each, and fewer when fewer slots fit, down to one
+// slot: n up to about 134 million objects.  At n = 1M a slot is 166 KB, so
+// about 100 queries run at once (25 four-warp blocks on 148 SMs): this entry
+// point trades throughput for owning no memory.
 #include <algorithm>
 #include <cfloat>
 #include <mutex>
@@ -36,7 +45,7 @@ constexpr uint32_t kHeaderWords = 64;  // [0] work counter, [1] error word
 constexpr uint32_t kLogCap = 2048;
 constexpr uint32_t kCandCap = 8192;
 constexpr uint32_t kMaxL = 1024;
-constexpr uint32_t kWarps = 4;
+constexpr uint32_t kWarps = 4;  // most warps per block (fewer when fewer slots fit)
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
 
@@ -127,7 +136,7 @@ extern __shared__ __align__(16) unsigned char na_smem[];
 // coming from a precomputed norm array.  Results: pred_ids[q * max_pred + i].
 __global__ void __launch_bounds__(32 * kWarps) noalloc_search_kernel(NoAllocParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
-    const uint32_t slot = blockIdx.x * kWarps + wib;
+    const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
     const uint32_t ls = p.ix.lifted_stride, bs = p.ix.base_stride, dim = p.ix.d + 2;
     const size_t per_warp = (size_t)(4 * p.L + 128 + ls + bs) * 4;
     float* qhat = reinterpret_cast<float*>(na_smem + wib * per_warp);
@@ -160,13 +169,22 @@ __global__ void __launch_bounds__(32 * kWarps) noalloc_search_kernel(NoAllocPara
             qhat[j] = v;
         }
         __syncwarp();
+        // descent; a child index outside the tree is reported and the search
+        // starts from object 0
         uint32_t v = p.ix.tree_nodes - 1;
+        bool bad_tree = false;
         for (uint32_t depth = 0; p.ix.tree_left[v] != kEmpty && depth < 4096; depth++) {
             const float ip = group_ip(p.ix.tree_hyperplane + (size_t)v * ls, qhat, dim, gt, kAll);
             const float margin = __fsub_rn(ip, p.ix.tree_offset[v]);
-            v = (margin < -kSplitEps) ? p.ix.tree_left[v] : (margin > kSplitEps ? p.ix.tree_right[v] : p.ix.tree_left[v]);
+            const uint32_t c = (margin > kSplitEps) ? p.ix.tree_right[v] : p.ix.tree_left[v];
+            if (c >= p.ix.tree_nodes) {
+                bad_tree = true;
+                break;
+            }
+            v = c;
         }
-        uint32_t ep = p.ix.tree_leaf_first[v];
+        if (bad_tree && lane == 0) set_error(err, kDevBadId);
+        uint32_t ep = bad_tree ? 0u : p.ix.tree_leaf_first[v];
         if (ep == kEmpty || ep >= p.ix.n) ep = 0;
         const float dep = group_l2sqr(p.ix.lifted + (size_t)ep * ls, qhat, dim, gt, kAll);
         if (lane == 0) {
@@ -307,24 +325,26 @@ extern "C" int anqi_rknn_query_noalloc(const anqi_device_index* ix, const float*
     const uint32_t words = (uint32_t)((ix->n + 31) / 32);
     const uint64_t slot_words = (uint64_t)words + kLogCap + kCandCap;
     const uint64_t fit = (kNoAllocWords - kHeaderWords) / slot_words;
-    if (fit == 0) return ANQI_ERR_CAPACITY;  // n too large for the fixed scratch (above about 130M objects)
-    const size_t smem = (size_t)(4 * L + 128 + ix->lifted_stride + ix->base_stride) * 4 * kWarps;
+    if (fit == 0) return ANQI_ERR_CAPACITY;  // n too large for the fixed scratch (above about 134M objects)
+    // one query slot per warp: blocks of up to kWarps warps, fewer when fewer slots fit
+    const uint32_t wpb = (uint32_t)std::min<uint64_t>(kWarps, fit);
+    const size_t smem = (size_t)(4 * L + 128 + ix->lifted_stride + ix->base_stride) * 4 * wpb;
     if (smem > 227 * 1024) return ANQI_ERR_ARGS;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (cudaFuncSetAttribute(noalloc_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return ANQI_ERR_DEVICE;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, noalloc_search_kernel, 32 * kWarps, smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, noalloc_search_kernel, 32 * wpb, smem) !=
             cudaSuccess ||
         per_sm < 1)
         return ANQI_ERR_DEVICE;
-    uint64_t blocks = std::min<uint64_t>((uint64_t)per_sm * sms, fit / kWarps);
-    blocks = std::min<uint64_t>(blocks, (nq + kWarps - 1) / kWarps);
+    uint64_t blocks = std::min<uint64_t>((uint64_t)per_sm * sms, fit / wpb);
+    blocks = std::min<uint64_t>(blocks, (nq + wpb - 1) / wpb);
     if (blocks == 0) blocks = 1;
-    if (blocks * kWarps > fit) return ANQI_ERR_CAPACITY;
+    if (blocks * wpb > fit) return ANQI_ERR_CAPACITY;
     // zero the header and every slot this call uses (the array keeps the last call's contents)
-    const uint64_t used = kHeaderWords + blocks * kWarps * slot_words;
+    const uint64_t used = kHeaderWords + blocks * wpb * slot_words;
     noalloc_clear_kernel<<<sms * 4, 256, 0, st>>>(scratch, used);
     NoAllocParams p;
     p.ix = *ix;
@@ -339,7 +359,7 @@ extern "C" int anqi_rknn_query_noalloc(const anqi_device_index* ix, const float*
     p.scratch = scratch;
     p.words = words;
     p.slot_words = (uint32_t)slot_words;
-    noalloc_search_kernel<<<(unsigned)blocks, 32 * kWarps, smem, st>>>(p);
+    noalloc_search_kernel<<<(unsigned)blocks, 32 * wpb, smem, st>>>(p);
     if (cudaGetLastError() != cudaSuccess) return ANQI_ERR_DEVICE;
     uint32_t err = 0;
     if (cudaMemcpyAsync(&err, scratch + 1, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||

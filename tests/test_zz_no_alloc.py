@@ -6,8 +6,11 @@ they hand in device arrays they already own and the library uses a fixed
 static scratch array instead of cudaMalloc.  This checks, through the C ABI,
 that two calls in a row return exactly what the allocating entry point
 (anqi_rknn_query) returns on the same index and queries, and that an index
-too large for the fixed scratch is rejected.  Collected last on purpose: it
-runs after every other test, and it also passes on its own."""
+too large for the fixed scratch is rejected.  Cases: d = 32 and d = 128 (the
+product's stride), and an index of 34 million objects (the small index held in
+the first rows of larger arrays), where only three query slots fit in the
+scratch and the blocks run three warps.  Collected last on purpose: it runs
+after every other test, and it also passes on its own."""
 import ctypes as C
 
 import numpy as np
@@ -61,32 +64,57 @@ def padded(torch, a, stride):
     return torch.from_numpy(out).cuda()
 
 
-def test_noalloc_matches_allocating_query_twice():
-    torch = pytest.importorskip("torch")
-    base, query, lifted, links, deg, tree, sc, m2, thr = small_index()
-    n, d = base.shape
-    L = 64
+def bind(lib):
+    lib.anqi_rknn_query_noalloc.argtypes = [C.POINTER(DeviceIndex), C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                            C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.anqi_rknn_query_noalloc.restype = C.c_int
+    return lib
+
+
+def device_rows(torch, a, stride, rows=None):
+    """a (m x w) in the first m rows of a device array of `rows` x stride
+    floats (rows beyond m are allocated but never written)."""
+    a = np.ascontiguousarray(a, np.float32)
+    rows = rows or a.shape[0]
+    t = torch.empty((rows, stride), dtype=torch.float32, device="cuda")
+    t[:a.shape[0]] = padded(torch, a, stride)
+    return t
+
+
+def device_u32(torch, a, rows=None):
+    a = np.ascontiguousarray(a).astype(np.uint32)
+    rows = rows or a.shape[0]
+    t = torch.empty((rows,) + a.shape[1:], dtype=torch.int32, device="cuda")
+    t[:a.shape[0]] = torch.from_numpy(a.view(np.int32))
+    return t
+
+
+def check_noalloc(torch, d, n_alloc=None, L=64):
+    """Two calls in a row through the C ABI equal anqi_rknn_query's results.
+    n_alloc: the object count the index arrays (and the call) declare; the
+    index's own objects are the first rows."""
+    base, query, lifted, links, deg, tree, sc, m2, thr = small_index(d=d)
+    n = len(base)
     with Context(0) as ctx:
         ctx.index_load(base, lifted, deg, links, tree, sc, m2)
         ctx.set_thresholds(10, thr)
         ref = ctx.rknn_query(query, 10, L)
-    lib = load_library()
-    lib.anqi_rknn_query_noalloc.argtypes = [C.POINTER(DeviceIndex), C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
-                                            C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
-    lib.anqi_rknn_query_noalloc.restype = C.c_int
-    bs, ls = 32, 40
-    t_base = padded(torch, base, bs)
-    t_lift = padded(torch, lifted, ls)
-    t_deg = torch.from_numpy(deg.astype(np.int32)).cuda()
-    t_links = torch.from_numpy(links.astype(np.int64).astype(np.uint32).view(np.int32)).cuda()
-    t_left = torch.from_numpy(tree.left.view(np.int32).copy()).cuda()
-    t_right = torch.from_numpy(tree.right.view(np.int32).copy()).cuda()
+    lib = bind(load_library())
+    bs = (d + 3) // 4 * 4
+    ls = (d + 2 + 3) // 4 * 4
+    rows = n_alloc or n
+    t_base = device_rows(torch, base, bs, rows)
+    t_lift = device_rows(torch, lifted, ls, rows)
+    t_deg = device_u32(torch, deg, rows)
+    t_links = device_u32(torch, links, rows)
+    t_thr = device_rows(torch, thr[:, None], 1, rows)
+    t_left = device_u32(torch, tree.left)
+    t_right = device_u32(torch, tree.right)
     t_off = torch.from_numpy(tree.offset.copy()).cuda()
     t_hyp = padded(torch, tree.hyperplane, ls)
-    t_leaf = torch.from_numpy(tree.leaf_first().view(np.int32).copy()).cuda()
-    t_thr = torch.from_numpy(thr).cuda()
+    t_leaf = device_u32(torch, tree.leaf_first())
     t_q = padded(torch, query, bs)
-    ix = DeviceIndex(n, d, links.shape[1], t_base.data_ptr(), bs, t_lift.data_ptr(), ls, t_deg.data_ptr(),
+    ix = DeviceIndex(rows, d, links.shape[1], t_base.data_ptr(), bs, t_lift.data_ptr(), ls, t_deg.data_ptr(),
                      t_links.data_ptr(), tree.n_nodes, t_left.data_ptr(), t_right.data_ptr(), t_off.data_ptr(),
                      t_hyp.data_ptr(), t_leaf.data_ptr(), sc, m2)
     nq = len(query)
@@ -106,13 +134,30 @@ def test_noalloc_matches_allocating_query_twice():
         assert np.array_equal(nd.cpu().numpy().astype(np.uint32), ref.n_dist), call
         for q in range(nq):
             assert np.array_equal(ids_h[q, :cnt_h[q]], ref.pred(q)), (call, q)
+        assert int(cnt_h.sum()) > 0
+
+
+@pytest.mark.parametrize("d", [32, 128])
+def test_noalloc_matches_allocating_query_twice(d):
+    torch = pytest.importorskip("torch")
+    check_noalloc(torch, d)
+
+
+def test_noalloc_three_slots_at_34m_objects():
+    """n = 34M: a slot is 1,062,500 bitmap words + 10,240, so three fit in the
+    scratch and each block runs three warps (the largest n with four slots is
+    about 33.5M)."""
+    torch = pytest.importorskip("torch")
+    n_big = 34_000_000
+    slot_words = (n_big + 31) // 32 + 2048 + 8192
+    assert ((16 << 20) // 4 - 64) // slot_words == 3
+    check_noalloc(torch, 32, n_alloc=n_big)
+    torch.cuda.empty_cache()
 
 
 def test_noalloc_rejects_an_index_beyond_its_scratch():
     torch = pytest.importorskip("torch")
-    lib = load_library()
-    lib.anqi_rknn_query_noalloc.argtypes = [C.POINTER(DeviceIndex), C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
-                                            C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib = bind(load_library())
     buf = torch.zeros(4096, dtype=torch.float32, device="cuda")
     p = buf.data_ptr()
     huge = DeviceIndex(1 << 30, 8, 48, p, 8, p, 16, p, p, 1, p, p, p, p, p, 1.0, 1.0)
