@@ -77,6 +77,28 @@ float ao_d2(const float* a, const float* b, float na, float nb, uint32_t dim) {
     return s - t;
 }
 
+/* distance.h:170-174: the "ip" metric's scalar distance 1 - sum a_i b_i, a
+ * sequential sum in index order, as the reference's compiler (GCC 13, -O3,
+ * x86-64-v4 / AVX-512 hosts) emits it: the first 8 floor(dim / 8) products are
+ * formed in 8-wide vectors and added one by one (each rounded), the remaining
+ * dim mod 8 are accumulated by fused multiply-adds.  Pinned against the
+ * compiled reference at dimensions 3, 8, 13, 32 and 130 (tests/golden). */
+float ao_ip_dist(const float* a, const float* b, uint32_t dim) {
+    const uint32_t d8 = dim & ~7u;
+    float product = 0.0f;
+    for (uint32_t i = 0; i < d8; i++) {
+        float t = a[i] * b[i];
+        product = product + t;
+    }
+    for (uint32_t i = d8; i < dim; i++) product = fmaf(a[i], b[i], product);
+    return 1.0f - product;
+}
+
+/* nndindex::d2 (index.h:172-176): L2 by norms, or the ip metric's distance */
+static float metric_d2(const float* a, const float* b, float na, float nb, uint32_t dim, uint32_t ip) {
+    return ip ? ao_ip_dist(a, b, dim) : ao_d2(a, b, na, nb, dim);
+}
+
 void ao_norms(const float* x, uint64_t n, uint32_t dim, float* out) {
     for (uint64_t i = 0; i < n; i++) out[i] = ao_norm(x + i * dim, dim);
 }
@@ -133,6 +155,108 @@ void ao_lrq_materialize(const float* coeff, const uint8_t* codes, uint64_t n, ui
     }
 }
 
+/* rknn_query.cpp:482-513 for every policy (0 nearest, 1 floor, 2 ceil):
+ * searches with the float value, breaks nearest ties in double. */
+static uint32_t policy_code(double value, const float* c, uint32_t cs, uint32_t policy) {
+    if (policy == 1) return floor_code(value, c, cs);
+    float v = (float)value;
+    uint32_t lo = 0, hi = cs; /* lower_bound: first element >= v */
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) / 2;
+        if (c[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    if (policy == 2) return lo == cs ? cs - 1 : lo;
+    if (lo == 0) return 0;
+    if (lo == cs) return cs - 1;
+    double up = (double)c[lo], dn = (double)c[lo - 1];
+    return fabs(up - value) < fabs(value - dn) ? lo : lo - 1;
+}
+
+/* packed_code_array.h:20-61 */
+static void put_code(uint8_t* d, uint64_t idx, uint32_t bits, uint32_t code) {
+    if (bits == 2) {
+        unsigned sh = (unsigned)(idx & 3u) * 2u;
+        d[idx >> 2] = (uint8_t)((d[idx >> 2] & ~(3u << sh)) | ((code & 3u) << sh));
+    } else if (bits == 4) {
+        if (idx & 1u) d[idx >> 1] = (uint8_t)((d[idx >> 1] & 0x0fu) | ((code & 15u) << 4));
+        else d[idx >> 1] = (uint8_t)((d[idx >> 1] & 0xf0u) | (code & 15u));
+    } else if (bits == 8) {
+        d[idx] = (uint8_t)code;
+    } else if (bits == 16) {
+        d[2 * idx] = (uint8_t)(code & 255u);
+        d[2 * idx + 1] = (uint8_t)(code >> 8);
+    }
+}
+
+static uint32_t take_code(const uint8_t* d, uint64_t idx, uint32_t bits) {
+    if (bits == 2) return (d[idx >> 2] >> ((unsigned)(idx & 3u) * 2u)) & 3u;
+    if (bits == 4) return (idx & 1u) ? (uint32_t)(d[idx >> 1] >> 4) : (uint32_t)(d[idx >> 1] & 15u);
+    if (bits == 8) return d[idx];
+    if (bits == 16) return (uint32_t)d[2 * idx] | ((uint32_t)d[2 * idx + 1] << 8);
+    return 0;
+}
+
+/* rknn_query.cpp:679-720 for every form: bits 0 (coefficients only), 2/4/8/16
+ * (packed codes; the caller zeroes `codes`), 32 (float residuals). */
+void ao_lrq_encode_bits(const float* keys, uint64_t n, uint32_t nk, uint32_t rankm, const float* mu,
+                        const float* basis, const float* codebook, uint32_t code_size, uint32_t bits,
+                        uint32_t policy, float* coeff, uint8_t* codes, float* residual) {
+    for (uint64_t i = 0; i < n; i++) {
+        const float* rk = keys + i * nk;
+        float* ci = coeff + i * rankm;
+        for (uint32_t m = 0; m < rankm; m++) {
+            const float* gm = basis + (uint64_t)m * nk;
+            double c = 0.0;
+            for (uint32_t k = 0; k < nk; k++) c += ((double)rk[k] - (double)mu[k]) * (double)gm[k];
+            ci[m] = (float)c;
+        }
+        if (bits == 0) continue;
+        for (uint32_t k = 0; k < nk; k++) {
+            double recon = (double)mu[k];
+            for (uint32_t m = 0; m < rankm; m++) recon += (double)ci[m] * (double)basis[(uint64_t)m * nk + k];
+            double r = (double)rk[k] - recon;
+            if (bits == 32) residual[i * nk + k] = (float)r;
+            else put_code(codes, i * nk + k, bits,
+                          policy_code(r, codebook + (uint64_t)k * code_size, code_size, policy));
+        }
+    }
+}
+
+/* rknn_query.cpp:722-753 for every form; signed_keys (IP) skips the clamp. */
+void ao_lrq_materialize_bits(const float* coeff, const uint8_t* codes, const float* residual, uint64_t n,
+                             uint32_t nk, uint32_t rankm, uint32_t bits, const float* mu, const float* basis,
+                             const float* codebook, uint32_t code_size, uint32_t k_one_based,
+                             double radius_scale, int signed_keys, float* thr) {
+    uint32_t k = k_one_based - 1;
+    for (uint64_t i = 0; i < n; i++) {
+        const float* ci = coeff + i * rankm;
+        double value = (double)mu[k];
+        for (uint32_t m = 0; m < rankm; m++) value += (double)ci[m] * (double)basis[(uint64_t)m * nk + k];
+        if (bits == 32) value += (double)residual[i * nk + k];
+        else if (bits) value += (double)codebook[(uint64_t)k * code_size + take_code(codes, i * nk + k, bits)];
+        double scaled = radius_scale * value;
+        thr[i] = (float)(signed_keys ? scaled : (0.0 < scaled ? scaled : 0.0));
+    }
+}
+
+/* rknn_query.cpp:576-600 (AnalyticRankMVerifier::materialize_k) */
+void ao_analytic_rankm_materialize(const float* coeff, uint64_t n, uint32_t rankm, uint32_t train_kmax,
+                                   uint32_t flags, double b0, uint32_t k_one_based, double radius_scale,
+                                   float* thr) {
+    double ratio = (flags & 4u) ? (double)k_one_based / (double)train_kmax : (double)k_one_based;
+    double logk = log(ratio);
+    double b[16];
+    b[0] = pow(ratio, b0);
+    for (uint32_t m = 1; m < rankm && m < 16; m++) b[m] = b[m - 1] * logk;
+    for (uint64_t i = 0; i < n; i++) {
+        double value = 0.0;
+        for (uint32_t m = 0; m < rankm; m++) value += (double)coeff[i * rankm + m] * b[m];
+        double scaled = radius_scale * value;
+        thr[i] = (float)(0.0 < scaled ? scaled : 0.0);
+    }
+}
+
 /* ----------------------------------------------------------------- lift */
 
 /* rknn_query.cpp:2203-2235: anyk_lift, L2, graph radius = the AKNN rank-K cutoff.
@@ -140,6 +264,12 @@ void ao_lrq_materialize(const float* coeff, const uint8_t* codes, uint64_t n, ui
  * reference's OpenMP reduction at one thread). */
 void ao_lift(const float* base, uint64_t n, uint32_t d, const float* radius,
              float* lifted, double* mstar2, double* scale) {
+    ao_lift_metric(base, n, d, radius, 0, lifted, mstar2, scale);
+}
+
+/* The same for either metric: the ip lift's coordinate is s^2 r (rknn_query.cpp:2227). */
+void ao_lift_metric(const float* base, uint64_t n, uint32_t d, const float* radius, uint32_t ip,
+                    float* lifted, double* mstar2, double* scale) {
     double sum_n2 = 0;
     for (uint64_t i = 0; i < n; i++) {
         const float* o = base + i * d;
@@ -159,7 +289,7 @@ void ao_lift(const float* base, uint64_t n, uint32_t d, const float* radius,
             h[j] = (float)v;
             nr2 += v * v;
         }
-        h[d] = (float)(0.5 * ((double)radius[i] * sc2 - nr2));
+        h[d] = ip ? (float)((double)radius[i] * sc2) : (float)(0.5 * ((double)radius[i] * sc2 - nr2));
         double hn2 = nr2 + (double)h[d] * h[d];
         if (hn2 > maxn2) maxn2 = hn2;
     }
@@ -261,7 +391,13 @@ int ao_range_search(const ao_index* ix, const float* q, uint32_t L, const float*
     const uint32_t dim = ix->dim, d = ix->d;
     float* qb = (float*)malloc(sizeof(float) * dim);
     ao_lift_query(q, d, ix->scale, qb);
-    double R2 = ix->mstar2 + 1.0;
+    /* rknn_query.cpp:2724-2731: ip adds the lifted query's squared norm */
+    double qn2s = 0;
+    for (uint32_t j = 0; j < d; j++) {
+        double v = (double)q[j] * ix->scale;
+        qn2s += v * v;
+    }
+    double R2 = ix->metric ? (qn2s + 1.0 + ix->mstar2) : (ix->mstar2 + 1.0);
     uint8_t* vis = (uint8_t*)calloc(ix->n, 1);
     uint32_t* flood = (uint32_t*)malloc(sizeof(uint32_t) * (ix->n + 1));
     uint64_t nf = 0, head = 0;
@@ -320,7 +456,7 @@ int ao_range_search(const ao_index* ix, const float* q, uint32_t L, const float*
         const float* o = ix->base + (uint64_t)cand[c] * d;
         float ip = ao_ip(o, q, d);
         float on = ao_ip(o, o, d);
-        float key = (on + qn) - 2.0f * ip;
+        float key = ix->metric ? -ip : (on + qn) - 2.0f * ip;  /* rknn_query.cpp:2555-2561 */
         if ((double)key <= (double)thr[cand[c]]) {
             if (np < pred_cap) pred[np] = cand[c];
             else rc = -1;
@@ -340,7 +476,7 @@ int ao_range_search(const ao_index* ix, const float* q, uint32_t L, const float*
 /* ------------------------------------------------------- gather / prune */
 
 static float gd2(const ao_knn_graph* g, uint64_t a, uint64_t b) {
-    return ao_d2(g->x + a * g->dim, g->x + b * g->dim, g->norms[a], g->norms[b], g->dim);
+    return metric_d2(g->x + a * g->dim, g->x + b * g->dim, g->norms[a], g->norms[b], g->dim, g->metric);
 }
 
 /* index.h:1491-1525 */
@@ -670,6 +806,12 @@ void ao_reverse(const uint32_t* ids, uint64_t n, uint32_t K, uint64_t* rev_off, 
 void ao_init_knn(const float* x, const float* norms, uint32_t dim, uint64_t n, uint32_t K,
                  const uint64_t* leaf_off, const uint32_t* leaf_ids, uint64_t n_leaves,
                  uint32_t* out_ids, float* out_d) {
+    ao_init_knn_metric(x, norms, dim, n, K, leaf_off, leaf_ids, n_leaves, 0, out_ids, out_d);
+}
+
+void ao_init_knn_metric(const float* x, const float* norms, uint32_t dim, uint64_t n, uint32_t K,
+                        const uint64_t* leaf_off, const uint32_t* leaf_ids, uint64_t n_leaves, uint32_t ip,
+                        uint32_t* out_ids, float* out_d) {
     /* per row: collect (d, id) of all leaf-mates, dedupe, keep K smallest */
     uint64_t* cnt = (uint64_t*)calloc(n + 1, sizeof(uint64_t));
     for (uint64_t l = 0; l < n_leaves; l++) {
@@ -686,7 +828,7 @@ void ao_init_knn(const float* x, const float* norms, uint32_t dim, uint64_t n, u
                 uint32_t p = leaf_ids[a], q = leaf_ids[b];
                 pair_t* e = &all[cnt[p] + fill[p]++];
                 e->id = q;
-                e->d = ao_d2(x + (uint64_t)p * dim, x + (uint64_t)q * dim, norms[p], norms[q], dim);
+                e->d = metric_d2(x + (uint64_t)p * dim, x + (uint64_t)q * dim, norms[p], norms[q], dim, ip);
             }
     for (uint64_t i = 0; i < n; i++) {
         pair_t* r = all + cnt[i];
@@ -732,6 +874,13 @@ static uint64_t node_key(uint64_t seed, uint32_t tree, uint32_t node) {
 /* rptrees.h:28-84,127-163 in deterministic breadth-first form. */
 int64_t ao_rp_tree(const float* x, uint64_t n, uint32_t dim, uint32_t leaf_size,
                    uint32_t max_depth, uint64_t seed, uint32_t tree, ao_tree_out* out) {
+    return ao_rp_tree_metric(x, n, dim, leaf_size, max_depth, seed, tree, 0, out);
+}
+
+/* angular (the ip metric, rptrees.h:41-52): the hyperplane is the normalized
+ * difference of the two unit-scaled points, offset 0. */
+int64_t ao_rp_tree_metric(const float* x, uint64_t n, uint32_t dim, uint32_t leaf_size, uint32_t max_depth,
+                          uint64_t seed, uint32_t tree, uint32_t angular, ao_tree_out* out) {
     uint32_t* start = (uint32_t*)malloc(sizeof(uint32_t) * out->cap_nodes);
     uint32_t* count = (uint32_t*)malloc(sizeof(uint32_t) * out->cap_nodes);
     uint32_t* depth = (uint32_t*)malloc(sizeof(uint32_t) * out->cap_nodes);
@@ -764,11 +913,23 @@ int64_t ao_rp_tree(const float* x, uint64_t n, uint32_t dim, uint32_t leaf_size,
         if (r0 == r1) r0 = (r1 + 1) % c;
         const float* x0 = x + (uint64_t)out->perm[s + r0] * dim;
         const float* x1 = x + (uint64_t)out->perm[s + r1] * dim;
-        for (uint32_t j = 0; j < dim; j++) {
-            mid[j] = (x0[j] + x1[j]) / 2;
-            hp[j] = x0[j] - x1[j];
+        float off = 0.0f;
+        if (angular) {
+            float n0 = sqrtf(ao_ip(x0, x0, dim));
+            float n1 = sqrtf(ao_ip(x1, x1, dim));
+            if (fabsf(n0) < AO_EPS) n0 = 1.0f;
+            if (fabsf(n1) < AO_EPS) n1 = 1.0f;
+            for (uint32_t j = 0; j < dim; j++) hp[j] = x0[j] / n0 - x1[j] / n1;
+            float hn = sqrtf(ao_ip(hp, hp, dim));
+            if (fabsf(hn) < AO_EPS) hn = 1.0f;
+            for (uint32_t j = 0; j < dim; j++) hp[j] /= hn;
+        } else {
+            for (uint32_t j = 0; j < dim; j++) {
+                mid[j] = (x0[j] + x1[j]) / 2;
+                hp[j] = x0[j] - x1[j];
+            }
+            off = ao_ip(hp, mid, dim);
         }
-        float off = ao_ip(hp, mid, dim);
         uint32_t nl = 0;
         for (uint32_t p = 0; p < c; p++) {
             uint32_t id = out->perm[s + p];
@@ -831,6 +992,12 @@ static int cmp_kv(const void* a, const void* b) {
 
 /* dataset_gt.cpp:206-248: K smallest (key, id) with the diagonal skipped. */
 void ao_exact_topk(const float* base, uint64_t n, uint32_t d, uint32_t K, uint32_t* ids, float* keys) {
+    ao_exact_topk_metric(base, n, d, K, 0, ids, keys);
+}
+
+/* the ip metric's key is -<a, b> (dataset_gt.cpp:224, 288) */
+void ao_exact_topk_metric(const float* base, uint64_t n, uint32_t d, uint32_t K, uint32_t ip, uint32_t* ids,
+                          float* keys) {
     float* bn = (float*)malloc(sizeof(float) * n);
     kv_t* row = (kv_t*)malloc(sizeof(kv_t) * n);
     for (uint64_t i = 0; i < n; i++) bn[i] = ao_ip(base + i * d, base + i * d, d);
@@ -838,8 +1005,8 @@ void ao_exact_topk(const float* base, uint64_t n, uint32_t d, uint32_t K, uint32
         uint64_t m = 0;
         for (uint64_t j = 0; j < n; j++) {
             if (j == i) continue;
-            float ip = ao_ip(base + i * d, base + j * d, d);
-            row[m].key = (bn[i] + bn[j]) - 2.0f * ip;
+            float v = ao_ip(base + i * d, base + j * d, d);
+            row[m].key = ip ? -v : (bn[i] + bn[j]) - 2.0f * v;
             row[m].id = (uint32_t)j;
             m++;
         }
@@ -856,6 +1023,11 @@ void ao_exact_topk(const float* base, uint64_t n, uint32_t d, uint32_t K, uint32
 /* dataset_gt.cpp:270-299 */
 int64_t ao_rknn_gt(const float* base, uint64_t n, const float* query, uint64_t nq, uint32_t d,
                    const float* rk2, uint32_t* off, uint32_t* ids, float* keys, uint64_t cap) {
+    return ao_rknn_gt_metric(base, n, query, nq, d, rk2, 0, off, ids, keys, cap);
+}
+
+int64_t ao_rknn_gt_metric(const float* base, uint64_t n, const float* query, uint64_t nq, uint32_t d,
+                          const float* rk2, uint32_t is_ip, uint32_t* off, uint32_t* ids, float* keys, uint64_t cap) {
     float* bn = (float*)malloc(sizeof(float) * n);
     kv_t* hits = (kv_t*)malloc(sizeof(kv_t) * (n + 1));
     for (uint64_t i = 0; i < n; i++) bn[i] = ao_ip(base + i * d, base + i * d, d);
@@ -868,7 +1040,7 @@ int64_t ao_rknn_gt(const float* base, uint64_t n, const float* query, uint64_t n
         uint64_t m = 0;
         for (uint64_t j = 0; j < n; j++) {
             float ip = ao_ip(qv, base + j * d, d);
-            float key = (qn + bn[j]) - 2.0f * ip;
+            float key = is_ip ? -ip : (qn + bn[j]) - 2.0f * ip;
             if (key <= rk2[j]) {
                 hits[m].key = key;
                 hits[m].id = (uint32_t)j;

@@ -35,10 +35,28 @@ void ao_lrq_materialize(const float* coeff, const uint8_t* codes, uint64_t n, ui
                         const float* codebook, uint32_t code_size, uint32_t k_one_based,
                         double radius_scale, float* thr);
 
+/* every CompactLrqVerifier form: bits 0 / 2 / 4 / 8 / 16 / 32, policy 0 nearest,
+ * 1 floor, 2 ceil; codes packed as include/packed_code_array.h (zeroed by the caller) */
+void ao_lrq_encode_bits(const float* keys, uint64_t n, uint32_t nk, uint32_t rankm, const float* mu,
+                        const float* basis, const float* codebook, uint32_t code_size, uint32_t bits,
+                        uint32_t policy, float* coeff, uint8_t* codes, float* residual);
+void ao_lrq_materialize_bits(const float* coeff, const uint8_t* codes, const float* residual, uint64_t n,
+                             uint32_t nk, uint32_t rankm, uint32_t bits, const float* mu, const float* basis,
+                             const float* codebook, uint32_t code_size, uint32_t k_one_based,
+                             double radius_scale, int signed_keys, float* thr);
+void ao_analytic_rankm_materialize(const float* coeff, uint64_t n, uint32_t rankm, uint32_t train_kmax,
+                                   uint32_t flags, double b0, uint32_t k_one_based, double radius_scale,
+                                   float* thr);
+
 /* ---- lift, src/rknn_query.cpp:2203-2235 (anyk_lift, L2) ---- */
 void ao_lift(const float* base, uint64_t n, uint32_t d, const float* radius,
              float* lifted /* n x (d+2) */, double* mstar2, double* scale);
 void ao_lift_query(const float* q, uint32_t d, double scale, float* out /* d+2 */);
+/* ip = 1: the ip metric's lift coordinate s^2 r (rknn_query.cpp:2227) */
+void ao_lift_metric(const float* base, uint64_t n, uint32_t d, const float* radius, uint32_t ip,
+                    float* lifted, double* mstar2, double* scale);
+/* the ip metric's scalar distance 1 - sum a_i b_i (distance.h:170-174) */
+float ao_ip_dist(const float* a, const float* b, uint32_t dim);
 
 /* ---- RP tree query descent, include/rptrees.h:108-124 ---- */
 uint32_t ao_tree_entry(uint32_t n_nodes, uint32_t dim, const uint32_t* left,
@@ -63,6 +81,7 @@ typedef struct {
     const uint32_t* tree_leaf_first;
     double scale;
     double mstar2;
+    uint32_t metric;         /* 1: ip (per-query R2, key -<o,q>) */
 } ao_index;
 
 /* One query: writes candidate ids (visit order), predicted ids, returns counts.
@@ -83,6 +102,7 @@ typedef struct {
     const float* g_vals;     /* n x K */
     const uint64_t* rev_off; /* n+1 */
     const uint32_t* rev_ids;
+    uint32_t metric;         /* 1: the ip metric's distance */
 } ao_knn_graph;
 
 /* gather_candidates for row i; the pool is written as (dist,id) in visit order.
@@ -124,6 +144,9 @@ void ao_reverse(const uint32_t* ids, uint64_t n, uint32_t K, uint64_t* rev_off, 
 void ao_init_knn(const float* x, const float* norms, uint32_t dim, uint64_t n, uint32_t K,
                  const uint64_t* leaf_off, const uint32_t* leaf_ids, uint64_t n_leaves,
                  uint32_t* out_ids, float* out_d);
+void ao_init_knn_metric(const float* x, const float* norms, uint32_t dim, uint64_t n, uint32_t K,
+                        const uint64_t* leaf_off, const uint32_t* leaf_ids, uint64_t n_leaves, uint32_t ip,
+                        uint32_t* out_ids, float* out_d);
 
 /* ---- random-projection forest (rptrees.h:28-84,127-163) in this project's
  *      deterministic form: a counter-hash RNG replaces the thread-local mt19937,
@@ -140,6 +163,8 @@ typedef struct {
 } ao_tree_out;
 int64_t ao_rp_tree(const float* x, uint64_t n, uint32_t dim, uint32_t leaf_size,
                    uint32_t max_depth, uint64_t seed, uint32_t tree, ao_tree_out* out);
+int64_t ao_rp_tree_metric(const float* x, uint64_t n, uint32_t dim, uint32_t leaf_size, uint32_t max_depth,
+                          uint64_t seed, uint32_t tree, uint32_t angular, ao_tree_out* out);
 uint64_t ao_hash64(uint64_t x);
 
 /* ---- exact ground truth, tools/dataset_gt.cpp:206-313 ---- */
@@ -148,6 +173,11 @@ void ao_exact_topk(const float* base, uint64_t n, uint32_t d, uint32_t K,
 /* returns total hits; off has nq+1 entries; ids/keys sized by cap (-1 if exceeded) */
 int64_t ao_rknn_gt(const float* base, uint64_t n, const float* query, uint64_t nq, uint32_t d,
                    const float* rk2, uint32_t* off, uint32_t* ids, float* keys, uint64_t cap);
+/* the same for either metric (ip = 1: key -<a, b>, dataset_gt.cpp:224, 288) */
+void ao_exact_topk_metric(const float* base, uint64_t n, uint32_t d, uint32_t K, uint32_t ip, uint32_t* ids,
+                          float* keys);
+int64_t ao_rknn_gt_metric(const float* base, uint64_t n, const float* query, uint64_t nq, uint32_t d,
+                          const float* rk2, uint32_t is_ip, uint32_t* off, uint32_t* ids, float* keys, uint64_t cap);
 
 #ifdef __cplusplus
 }

@@ -9,13 +9,19 @@
 //
 // Subcommands (all single-threaded unless stated, so dumps are reproducible):
 //   dist     IN OUT                         distance kernels of include/distance.h
-//   verifier PFX OUT                        CompactLrqVerifier build/materialize (rknn_query.cpp:679-753)
+//   verifier PFX OUT [BITS POLICY SIGNED]   CompactLrqVerifier build/materialize (rknn_query.cpp:679-753)
+//   analytic MODEL N RANKM OUT              AnalyticRankMVerifier load/materialize (rknn_query.cpp:515-601)
 //   graph    LIFTED WARM_REC NNK M OUT      staged lifted-graph build (index.h:1071-1295)
-//   aknn     BASE OUT K LEAF TREES EF SEED  staged AKNN source build (index.h:1300-1461)
+//   aknn     BASE OUT K LEAF TREES EF SEED [METRIC]
+//                                           staged AKNN source build (index.h:1300-1461), l2 or ip
+//   ipdist   IN OUT                         the ip metric's scalar distance (distance.h:170-174)
 //   query    LIFTED GRAPH BASE QUERY META THR L OUT
 //                                           range_search + postfilter per query (index.h:1535, rknn_query.cpp:2692-2765)
 //   qbench   LIFTED GRAPH BASE QUERY META L THREADS WARMUP STEPS NQ THR GT [THR GT ...]
 //                                           the reference's timed query loop body, OpenMP, prints one JSON line
+//   qparity  LIFTED GRAPH BASE QUERY META L ENTRY NQ OUT THR [THR ...]
+//                                           per-query candidates / verified sets / #dist, entry
+//                                           descent as the reference draws it or with ties sent left
 
 #define main anqi_reference_rknn_query_main
 #include "src/rknn_query.cpp"
@@ -147,9 +153,36 @@ int cmd_dist(int argc, char** argv) {
     return 0;
 }
 
-int cmd_verifier(int argc, char** argv) {
+// verifier PFX OUT [BITS POLICY SIGNED]: CompactLrqVerifier build + save +
+// materialize_k for k = 1, 10, 50, 100.  BITS 0 (rankm_only), 2/4/8/16
+// (learned codebook PFX_learned_rq_codebook_M8_u{BITS}.bin), 32 (float
+// residuals); POLICY floor / ceil / nearest; SIGNED 1 = IP keys (no clamp).
+// ipdist IN OUT: the scalar inner-product distance 1 - sum a_i b_i of the
+// "ip" metric (include/distance.h:170-174), per pair.
+int cmd_ipdist(int argc, char** argv) {
     if (argc != 4) return 2;
+    FILE* f = std::fopen(argv[2], "rb");
+    if (!f) die("cannot open ipdist input");
+    uint32_t m = 0, dim = 0;
+    if (std::fread(&m, 4, 1, f) != 1 || std::fread(&dim, 4, 1, f) != 1) die("short ipdist header");
+    std::vector<float> a(dim), b(dim);
+    FILE* o = open_out(argv[3]);
+    for (uint32_t i = 0; i < m; i++) {
+        if (std::fread(a.data(), 4, dim, f) != dim || std::fread(b.data(), 4, dim, f) != dim) die("short ipdist body");
+        const float v = DistCal(dim, "ip").calculate(a.data(), b.data());
+        std::fwrite(&v, 4, 1, o);
+    }
+    std::fclose(o);
+    std::fclose(f);
+    return 0;
+}
+
+int cmd_verifier(int argc, char** argv) {
+    if (argc != 4 && argc != 7) return 2;
     const std::string pfx = argv[2], out = argv[3];
+    const int bits = argc == 7 ? std::atoi(argv[4]) : 8;
+    const std::string policy = argc == 7 ? argv[5] : "floor";
+    const bool is_ip = argc == 7 && std::atoi(argv[6]) != 0;
     size_t n = 0, d = 0;
     read_fbin(pfx + "_base.bin", n, d);
     const size_t NK = 100;
@@ -163,21 +196,41 @@ int cmd_verifier(int argc, char** argv) {
     bf.read((char*)mu.data(), NK * 4);
     bf.read((char*)G.data(), NK * RANKM * 4);
     size_t code_size = 0;
-    std::vector<float> cb = load_learned_rq_codebook(pfx + "_learned_rq_codebook_M8_u8.bin", NK, RANKM, 8, code_size);
+    std::vector<float> cb;
+    if (anqi::supported_packed_code_bits(bits))
+        cb = load_learned_rq_codebook(pfx + "_learned_rq_codebook_M8_u" + std::to_string(bits) + ".bin", NK, RANKM,
+                                      bits, code_size);
     std::vector<float> src(n * NK);
     setenv("ANQI_PREBUILT_TOPK_REC", (pfx + "_baseknn_aknn.rec").c_str(), 1);
     setenv("ANQI_PREBUILT_TOPK_K", "100", 1);
-    load_threshold_table(pfx, n, NK, false, src);
+    load_threshold_table(pfx, n, NK, is_ip, src);
     CompactLrqVerifier v;
-    v.configure(n, NK, RANKM, 8, "floor", mu, G, cb, code_size);
+    v.configure(n, NK, RANKM, bits, policy, mu, G, cb, code_size);
     v.build(src);
     v.save(out + "_verifier.bin");
     FILE* f = open_out(out + "_thresholds.bin");
     for (size_t k : {1, 10, 50, 100}) {
         std::vector<float> thr;
-        v.materialize_k(k, 1.0, false, thr);
+        v.materialize_k(k, 1.0, is_ip, thr);
         write_vec(f, thr);
     }
+    std::fclose(f);
+    return 0;
+}
+
+// analytic MODEL N RANKM OUT: AnalyticRankMVerifier::load + materialize_k for
+// k = 1, 10, 50, 100 at radius scales 1 and 1.25.
+int cmd_analytic(int argc, char** argv) {
+    if (argc != 6) return 2;
+    AnalyticRankMVerifier a;
+    a.load(argv[2], std::strtoull(argv[3], nullptr, 10), std::atoi(argv[4]));
+    FILE* f = open_out(std::string(argv[5]) + "_thresholds.bin");
+    for (double scale : {1.0, 1.25})
+        for (size_t k : {1, 10, 50, 100}) {
+            std::vector<float> thr;
+            a.materialize_k(k, scale, thr);
+            write_vec(f, thr);
+        }
     std::fclose(f);
     return 0;
 }
@@ -258,17 +311,19 @@ int cmd_graph(int argc, char** argv) {
 }
 
 int cmd_aknn(int argc, char** argv) {
-    if (argc != 9) return 2;
+    if (argc != 9 && argc != 10) return 2;
     const std::string base = argv[2], out = argv[3];
     const size_t K = std::strtoull(argv[4], nullptr, 10), leaf = std::strtoull(argv[5], nullptr, 10);
     const size_t trees = std::strtoull(argv[6], nullptr, 10), ef = std::strtoull(argv[7], nullptr, 10);
     const size_t seed = std::strtoull(argv[8], nullptr, 10);
+    const std::string metric = argc == 10 ? argv[9] : "l2";
+    const bool angular = metric == "ip";
     size_t n = 0, d = 0;
     read_fbin(base, n, d);
     Parms po;
     po.n = n;
     po.dim = d;
-    po.meric = "l2";
+    po.meric = metric;
     po.random_seed = seed;
     po.nn_k = K;
     po.M = 32;
@@ -283,7 +338,7 @@ int cmd_aknn(int argc, char** argv) {
     nndindex index(base, po);
     float* cvec = static_cast<float*>(_mm_malloc(n * d * sizeof(float), 64));
     for (size_t i = 0; i < n; i++) std::memcpy(cvec + i * d, index.vec(i), d * sizeof(float));
-    std::vector<rptree> forest = make_forest(cvec, n, d, trees, leaf, false, 100, seed, 1);
+    std::vector<rptree> forest = make_forest(cvec, n, d, trees, leaf, angular, 100, seed, 1);
     _mm_free(cvec);
     {
         std::vector<std::vector<uint32_t>> leaves;
@@ -332,10 +387,13 @@ int cmd_aknn(int argc, char** argv) {
     return 0;
 }
 
+// ANQI_HARNESS_METRIC=ip switches the query modes to the ip metric's lifted
+// query and key (rknn_query.cpp:2724-2731, 2555-2558).
 struct QueryEnv {
     size_t n = 0, dim = 0, d = 0, nq = 0;
     std::vector<float> base, queries, thr;
     double mstar2 = 0, scale = 0;
+    bool is_ip = std::getenv("ANQI_HARNESS_METRIC") && std::string(std::getenv("ANQI_HARNESS_METRIC")) == "ip";
 };
 
 void load_query_env(QueryEnv& e, char** a) {
@@ -357,15 +415,21 @@ void load_query_env(QueryEnv& e, char** a) {
 }
 
 void lift_query(const QueryEnv& e, const float* q, std::vector<float>& qb, double& R2) {
-    for (size_t j = 0; j < e.d; j++) qb[j] = (float)((double)q[j] * e.scale);
+    double qn2s = 0;
+    for (size_t j = 0; j < e.d; j++) {
+        const double v = (double)q[j] * e.scale;
+        qb[j] = (float)v;
+        qn2s += v * v;
+    }
     qb[e.d] = 1.0f;
     qb[e.d + 1] = 0.0f;
-    R2 = e.mstar2 + 1.0;
+    R2 = e.is_ip ? (qn2s + 1.0 + e.mstar2) : (e.mstar2 + 1.0);
 }
 
 float recheck_key(const QueryEnv& e, size_t id, const float* q) {
     const float* o = e.base.data() + id * e.d;
     float ip = DistCal::InnerProductSIMD16ExtAVX512_(o, q, (uint32_t)e.d);
+    if (e.is_ip) return -ip;
     float on = DistCal::InnerProductSIMD16ExtAVX512_(o, o, (uint32_t)e.d);
     float qn = DistCal::InnerProductSIMD16ExtAVX512_(q, q, (uint32_t)e.d);
     return on + qn - 2.0f * ip;
@@ -406,6 +470,93 @@ int cmd_query(int argc, char** argv) {
     dump_csr(preds, out + "_pred.bin");
     FILE* f = open_out(out + "_ndist.bin");
     write_vec(f, ndists);
+    std::fclose(f);
+    return 0;
+}
+
+// The reference's entry descent (rptrees.h:108-124) with ties (|margin| <= EPS)
+// sent left instead of to a random side; *tie reports whether any node on the
+// path had such a margin (where the reference's own descent may go right).
+uint32_t entry_ties_left(nndindex& index, const float* qb, bool* tie) {
+    const rptree& t = index.search_tree;
+    size_t v = t.nodes.size() - 1;
+    *tie = false;
+    while (t.nodes[v].left != UINT32_MAX) {
+        const std::vector<float>& h = t.nodes[v].hyperplane;
+        const float margin = DistCal::InnerProductSIMD16ExtAVX512_(h.data(), qb, h.size()) - t.nodes[v].offset;
+        if (!(margin < -EPS) && !(margin > EPS)) *tie = true;
+        v = margin > EPS ? t.nodes[v].right : t.nodes[v].left;
+    }
+    return t.nodes[v].indices.empty() ? 0u : t.nodes[v].indices[0];
+}
+
+// qparity LIFTED GRAPH BASE QUERY META L ENTRY NQ OUT THR1 [THR2 ...]
+// Per-query outputs of the reference's range_search + FP32 postfilter for the
+// first NQ queries (one thread), for comparison with another implementation
+// query by query.  ENTRY "tree": the reference's own entry descent, which draws
+// a random side at margin ties; ENTRY "left": the same descent with ties sent
+// left (the entry handed to range_search through its single-entry switch).
+// Writes OUT_entry.bin (per query: u32 tie-left entry, u32 1 if the tie-left
+// path met a tie), OUT_cand.bin (CSR, visit order), OUT_ndist.bin (u32), and
+// per threshold file t: OUT_pred{t}.bin (CSR, candidate order).
+int cmd_qparity(int argc, char** argv) {
+    if (argc < 12) return 2;
+    char* env_args[6] = {argv[2], argv[3], argv[4], argv[5], argv[6], argv[11]};
+    QueryEnv e;
+    load_query_env(e, env_args);
+    const size_t L = std::strtoull(argv[7], nullptr, 10);
+    const std::string mode = argv[8];
+    if (mode != "tree" && mode != "left") return 2;
+    const size_t nq = std::min(e.nq, (size_t)std::strtoull(argv[9], nullptr, 10));
+    const std::string out = argv[10];
+    const int nt = argc - 11;
+    std::vector<std::vector<float>> thr(nt);
+    for (int t = 0; t < nt; t++) {
+        thr[t].resize(e.n);
+        FILE* f = std::fopen(argv[11 + t], "rb");
+        if (!f || std::fread(thr[t].data(), 4, e.n, f) != e.n) die("bad threshold file");
+        std::fclose(f);
+    }
+    if (mode == "left") setenv("ANQI_QUERY_SINGLE_ENTRY", "1", 1);
+    else unsetenv("ANQI_QUERY_SINGLE_ENTRY");
+    unsetenv("ANQI_VAMANA_QUERY_ENTRY");
+    Parms par = lifted_parms(e.n, e.dim, 50, 48, out + "_scratch/");
+    nndindex index(argv[2], par);
+    load_graph_file(index, argv[3]);
+    std::vector<uint16_t> mark(e.n, 0);
+    uint16_t ver = 0;
+    std::vector<float> qb(e.dim);
+    std::vector<std::vector<uint32_t>> cands(nq);
+    std::vector<std::vector<std::vector<uint32_t>>> preds(nt, std::vector<std::vector<uint32_t>>(nq));
+    std::vector<uint32_t> ndists(nq), entry(2 * nq);
+    for (size_t i = 0; i < nq; i++) {
+        const float* q = e.queries.data() + i * e.d;
+        double R2 = 0;
+        lift_query(e, q, qb, R2);
+        bool tie = false;
+        entry[2 * i] = entry_ties_left(index, qb.data(), &tie);
+        entry[2 * i + 1] = tie ? 1u : 0u;
+        index.graph_entry_ = entry[2 * i];
+        if (++ver == 0) {
+            std::fill(mark.begin(), mark.end(), 0);
+            ver = 1;
+        }
+        size_t nd = 0;
+        index.range_search(qb.data(), R2, 0.0f, L, cands[i], nd, mark.data(), ver, nullptr, 0.5f, false);
+        ndists[i] = (uint32_t)nd;
+        for (uint32_t id : cands[i]) {
+            const float key = recheck_key(e, id, q);
+            for (int t = 0; t < nt; t++)
+                if (key <= (double)thr[t][id]) preds[t][i].push_back(id);
+        }
+    }
+    dump_csr(cands, out + "_cand.bin");
+    for (int t = 0; t < nt; t++) dump_csr(preds[t], out + "_pred" + std::to_string(t) + ".bin");
+    FILE* f = open_out(out + "_ndist.bin");
+    write_vec(f, ndists);
+    std::fclose(f);
+    f = open_out(out + "_entry.bin");
+    write_vec(f, entry);
     std::fclose(f);
     return 0;
 }
@@ -522,17 +673,20 @@ int cmd_qbench(int argc, char** argv) {
 
 int main(int argc, char** argv) {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: ref_harness dist|verifier|graph|aknn|query|qbench ...\n");
+        std::fprintf(stderr, "usage: ref_harness dist|verifier|analytic|graph|aknn|query|qbench|qparity ...\n");
         return 2;
     }
     const std::string cmd = argv[1];
     int rc = 2;
     if (cmd == "dist") rc = cmd_dist(argc, argv);
     else if (cmd == "verifier") rc = cmd_verifier(argc, argv);
+    else if (cmd == "analytic") rc = cmd_analytic(argc, argv);
+    else if (cmd == "ipdist") rc = cmd_ipdist(argc, argv);
     else if (cmd == "graph") rc = cmd_graph(argc, argv);
     else if (cmd == "aknn") rc = cmd_aknn(argc, argv);
     else if (cmd == "query") rc = cmd_query(argc, argv);
     else if (cmd == "qbench") rc = cmd_qbench(argc, argv);
+    else if (cmd == "qparity") rc = cmd_qparity(argc, argv);
     if (rc == 2) std::fprintf(stderr, "[ref_harness] bad arguments for %s\n", cmd.c_str());
     return rc;
 }

@@ -11,8 +11,12 @@ Fixtures:
   sample_d8.npz   the reference's own sample (scripts/make_sample_dataset.py:24-26,
                   256 x 8 base, 32 queries, N(0,1), seed 20260819)
   sample_d32.npz  the same recipe at d = 32 (the small configuration of the build plan)
+  sample_ip_d32.npz  the d = 32 sample under the ip metric (every stage, as sample_d32.npz)
+  lrq_forms.npz   CompactLrqVerifier in every form (bits 0/2/4/8/16/32, three policies,
+                  signed IP keys) and the analytic Rank-M model, on the d = 32 sample
 
-Usage: python tests/golden/make_golden.py [--ref /root/reference]
+Usage: python tests/golden/make_golden.py --ref REFERENCE_TREE
+       (or set ANQI_REFERENCE to the reference source tree)
 """
 from __future__ import annotations
 
@@ -105,8 +109,10 @@ RESULT_RE = re.compile(
 )
 
 
-def sample_fixture(ref: Path, d: int, out: Path) -> None:
+def sample_fixture(ref: Path, d: int, out: Path, metric: str = "l2") -> None:
     work = Path(tempfile.mkdtemp(prefix=f"anqi_golden_d{d}_"))
+    ip = metric == "ip"
+    henv = {"ANQI_HARNESS_METRIC": metric}
     pfx = work / "sample"
     try:
         rng = np.random.default_rng(20260819)
@@ -114,17 +120,17 @@ def sample_fixture(ref: Path, d: int, out: Path) -> None:
         query = rng.normal(0.0, 1.0, size=(32, d)).astype(np.float32)
         write_fbin(Path(f"{pfx}_base.bin"), base)
         write_fbin(Path(f"{pfx}_query.bin"), query)
-        Path(f"{pfx}_lifted.meta").write_text(f"0 {d} 100 l2 1.0\n")
+        Path(f"{pfx}_lifted.meta").write_text(f"0 {d} 100 {metric} 1.0\n")
         one = {"OMP_NUM_THREADS": "1"}
         # AKNN source: run_sample.sh:16-17 parameters, one thread for a reproducible file.
-        run([REFBIN / "build_aknn_source", f"{pfx}_base.bin", pfx, 100, 64, 8, 64, 1, 10, "l2"], env=one)
+        run([REFBIN / "build_aknn_source", f"{pfx}_base.bin", pfx, 100, 64, 8, 64, 1, 10, metric], env=one)
         thr = work / "thr"
         run([REFBIN / "dataset_gt", "--base", f"{pfx}_base.bin", "--K", 100, "--rk_k", 100, "--threads", 1,
-             "--tile", 64, "--mode", "thresholds", "--out_prefix", thr], env=one)
+             "--tile", 64, "--mode", "thresholds", "--metric", metric, "--out_prefix", thr], env=one)
         for k in (10, 50, 100):
             t = work / f"gt{k}"
             run([REFBIN / "dataset_gt", "--base", f"{pfx}_base.bin", "--query", f"{pfx}_query.bin", "--K", 100,
-                 "--rk_k", k, "--threads", 1, "--tile", 64, "--mode", "ground-truth",
+                 "--rk_k", k, "--threads", 1, "--tile", 64, "--mode", "ground-truth", "--metric", metric,
                  "--threshold-table", f"{thr}_baseknn_gt.bin", "--out_prefix", t], env=one)
             shutil.copy(f"{t}_rknn_gt.bin", f"{pfx}_rknn_gt_k{k}.bin")
         run([sys.executable, ref / "tools" / "train_final_m8_u8.py", "--pfx", pfx, "--threshold-source",
@@ -159,7 +165,7 @@ def sample_fixture(ref: Path, d: int, out: Path) -> None:
         mstar2, scale = (float(v) for v in meta_files[0].read_text().split())
 
         h = work / "h"
-        run([REFBIN / "ref_harness", "verifier", pfx, h])
+        run([REFBIN / "ref_harness", "verifier", pfx, h, 8, "floor", int(ip)])
         run([REFBIN / "ref_harness", "graph", lifted_files[0], f"{pfx}_baseknn_aknn.rec", 50, 48, h])
         thr_all = np.fromfile(f"{h}_thresholds.bin", dtype=np.float32).reshape(4, 256)
         query_out = {}
@@ -173,7 +179,7 @@ def sample_fixture(ref: Path, d: int, out: Path) -> None:
             for L in (16, 32, 64, 128):
                 q = work / f"q{k}_{L}"
                 run([REFBIN / "ref_harness", "query", lifted_files[0], f"{h}_graph.bin", f"{pfx}_base.bin",
-                     f"{pfx}_query.bin", meta_path, tp, L, q])
+                     f"{pfx}_query.bin", meta_path, tp, L, q], env=henv)
                 off, ids = read_csr64(Path(f"{q}_cand.bin"))
                 poff, pids = read_csr64(Path(f"{q}_pred.bin"))
                 query_out[f"q_cand_off_{k}_{L}"] = off
@@ -182,7 +188,7 @@ def sample_fixture(ref: Path, d: int, out: Path) -> None:
                 query_out[f"q_pred_{k}_{L}"] = pids
                 query_out[f"q_ndist_{k}_{L}"] = np.fromfile(f"{q}_ndist.bin", dtype=np.uint32)
         a = work / "a"
-        run([REFBIN / "ref_harness", "aknn", f"{pfx}_base.bin", a, 100, 64, 8, 64, 10])
+        run([REFBIN / "ref_harness", "aknn", f"{pfx}_base.bin", a, 100, 64, 8, 64, 10, metric])
 
         rec = np.fromfile(f"{pfx}_baseknn_aknn.rec", dtype=np.uint32).reshape(256, 100, 2)
         data = dict(query_out)
@@ -241,6 +247,92 @@ def sample_fixture(ref: Path, d: int, out: Path) -> None:
         keys = sorted(ref_lines)
         data["ref_lines_k_L"] = np.array(keys, dtype=np.int32)
         data["ref_lines"] = np.array([ref_lines[x] for x in keys], dtype=np.float64)
+        if ip:
+            # the ip metric's scalar distance on random pairs (include/distance.h:170-174)
+            prng = np.random.default_rng(9)
+            for dim in (3, 8, 13, 32, 130):
+                pa = prng.normal(size=(24, dim)).astype(np.float32)
+                pb = prng.normal(size=(24, dim)).astype(np.float32)
+                inp = work / f"ipd{dim}.bin"
+                with inp.open("wb") as f:
+                    f.write(struct.pack("<II", 24, dim))
+                    for i in range(24):
+                        pa[i].tofile(f)
+                        pb[i].tofile(f)
+                run([REFBIN / "ref_harness", "ipdist", inp, work / f"ipd{dim}.out"])
+                data[f"ipd_a_{dim}"] = pa
+                data[f"ipd_b_{dim}"] = pb
+                data[f"ipd_{dim}"] = np.fromfile(work / f"ipd{dim}.out", dtype=np.float32)
+        np.savez_compressed(out, **data)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+# (bits, policy, signed keys): every CompactLrqVerifier form and both key signs
+LRQ_FORMS = [(0, "floor", 0), (2, "floor", 0), (2, "nearest", 0), (4, "ceil", 0), (8, "nearest", 0),
+             (8, "ceil", 0), (16, "floor", 0), (32, "floor", 0), (8, "floor", 1), (32, "floor", 1)]
+
+
+def form_codebook(lo: np.ndarray, hi: np.ndarray, bits: int) -> np.ndarray:
+    """Sorted codebook rows: 2^bits evenly spaced centres from lo[k] to hi[k]
+    (any sorted codebook exercises the codec; the tests rebuild it from lo/hi)."""
+    cs = 1 << bits
+    t = np.arange(cs, dtype=np.float64) / (cs - 1)
+    return (lo[:, None].astype(np.float64) + t[None, :] * (hi - lo)[:, None].astype(np.float64)).astype(np.float32)
+
+
+def lrq_forms_fixture(sample: Path, out: Path) -> None:
+    """The reference's CompactLrqVerifier (build, save, materialize_k) in every
+    form, on the d = 32 sample's AKNN cutoffs and basis; signed forms shift the
+    keys and mu below zero as IP keys are."""
+    z = dict(np.load(sample))
+    data = {"lo": None, "hi": None}
+    keys, mu, basis = z["rec_keys"].astype(np.float32), z["mu"].astype(np.float32), z["basis"].astype(np.float32)
+    # residual range of the sample, widened a little (the codebook spans it)
+    c = (keys.astype(np.float64) - mu) @ basis.astype(np.float64).T
+    res = keys - (mu + c @ basis)
+    lo = (res.min(0) - 0.25).astype(np.float32)
+    hi = (res.max(0) + 0.25).astype(np.float32)
+    data["lo"], data["hi"] = lo, hi
+    shift = np.float32(keys.max() + 7.0)
+    work = Path(tempfile.mkdtemp(prefix="anqi_golden_lrq_"))
+    try:
+        for bits, policy, signed in LRQ_FORMS:
+            pfx = work / f"f{bits}{policy}{signed}"
+            k_src = keys - shift if signed else keys
+            m_src = mu - shift if signed else mu
+            write_fbin(Path(f"{pfx}_base.bin"), z["base"])
+            rec = np.empty(keys.shape + (2,), np.uint32)
+            rec[:, :, 0] = z["rec_ids"]
+            rec[:, :, 1] = k_src.view(np.uint32)
+            rec.tofile(f"{pfx}_baseknn_aknn.rec")
+            with open(f"{pfx}_radbasis_M8.bin", "wb") as f:
+                f.write(struct.pack("<ii", 100, 8))
+                m_src.astype(np.float32).tofile(f)
+                basis.tofile(f)
+            if bits in (2, 4, 8, 16):
+                with open(f"{pfx}_learned_rq_codebook_M8_u{bits}.bin", "wb") as f:
+                    f.write(b"ANQIRQ1\0" + struct.pack("<iiii", 100, 8, bits, 1 << bits))
+                    form_codebook(lo, hi, bits).tofile(f)
+            run([REFBIN / "ref_harness", "verifier", pfx, pfx, bits, policy, signed])
+            tag = f"{bits}_{policy}_{signed}"
+            data[f"vf_{tag}"] = np.frombuffer(Path(f"{pfx}_verifier.bin").read_bytes(), np.uint8)
+            data[f"thr_{tag}"] = np.fromfile(f"{pfx}_thresholds.bin", np.float32).reshape(4, -1)
+        data["shift"] = np.array([shift], np.float32)
+        # analytic Rank-M models (ANQIPW1), flags 3 and 7 (centred log ratio)
+        rng = np.random.default_rng(23)
+        for flags in (3, 7):
+            coeff = rng.normal(0.0, 1.0, size=(256, 8)).astype(np.float32)
+            coeff[:, 0] = np.abs(coeff[:, 0]) * 5.0
+            b0 = 0.37 if flags == 3 else -0.21
+            path = work / f"pw{flags}.bin"
+            with open(path, "wb") as f:
+                f.write(b"ANQIPW1\0" + struct.pack("<QIIII", 256, 100, 8, 10, flags) + struct.pack("<d", b0))
+                coeff.tofile(f)
+            run([REFBIN / "ref_harness", "analytic", path, 256, 8, work / f"pw{flags}"])
+            data[f"pw_coeff_{flags}"] = coeff
+            data[f"pw_b0_{flags}"] = np.array([b0])
+            data[f"pw_thr_{flags}"] = np.fromfile(work / f"pw{flags}_thresholds.bin", np.float32).reshape(2, 4, -1)
         np.savez_compressed(out, **data)
     finally:
         shutil.rmtree(work, ignore_errors=True)
@@ -248,13 +340,26 @@ def sample_fixture(ref: Path, d: int, out: Path) -> None:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", type=Path, default=Path("/root/reference"))
+    env = os.environ.get("ANQI_REFERENCE")
+    ap.add_argument("--ref", type=Path, default=Path(env) if env else None,
+                    help="reference source tree (default: $ANQI_REFERENCE)")
+    ap.add_argument("--only", choices=("lrq_forms", "sample_ip"), help="regenerate one fixture")
     args = ap.parse_args()
+    if args.ref is None or not (args.ref / "include" / "index.h").exists():
+        raise SystemExit("give the reference source tree with --ref or ANQI_REFERENCE")
     if not (REFBIN / "ref_harness").exists():
         raise SystemExit("build the reference first: make -C oracle ref")
+    if args.only == "lrq_forms":
+        lrq_forms_fixture(HERE / "sample_d32.npz", HERE / "lrq_forms.npz")
+        return 0
+    if args.only == "sample_ip":
+        sample_fixture(args.ref, 32, HERE / "sample_ip_d32.npz", metric="ip")
+        return 0
     dist_fixture(HERE / "dist.npz")
     sample_fixture(args.ref, 8, HERE / "sample_d8.npz")
     sample_fixture(args.ref, 32, HERE / "sample_d32.npz")
+    lrq_forms_fixture(HERE / "sample_d32.npz", HERE / "lrq_forms.npz")
+    sample_fixture(args.ref, 32, HERE / "sample_ip_d32.npz", metric="ip")
     for p in sorted(HERE.glob("*.npz")):
         print(f"{p.name}: {p.stat().st_size} bytes")
     return 0

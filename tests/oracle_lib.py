@@ -33,8 +33,23 @@ def _load() -> C.CDLL:
         "ao_lrq_encode": (None, [f32p, C.c_uint64, C.c_uint32, C.c_uint32, f32p, f32p, f32p, C.c_uint32, f32p, u8p]),
         "ao_lrq_materialize": (None, [f32p, u8p, C.c_uint64, C.c_uint32, C.c_uint32, f32p, f32p, f32p,
                                       C.c_uint32, C.c_uint32, C.c_double, f32p]),
+        "ao_lrq_encode_bits": (None, [f32p, C.c_uint64, C.c_uint32, C.c_uint32, f32p, f32p, C.c_void_p, C.c_uint32,
+                                      C.c_uint32, C.c_uint32, f32p, C.c_void_p, C.c_void_p]),
+        "ao_lrq_materialize_bits": (None, [f32p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32,
+                                           C.c_uint32, f32p, f32p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_double,
+                                           C.c_int, f32p]),
+        "ao_analytic_rankm_materialize": (None, [f32p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double,
+                                                 C.c_uint32, C.c_double, f32p]),
         "ao_lift": (None, [f32p, C.c_uint64, C.c_uint32, f32p, f32p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "ao_lift_query": (None, [f32p, C.c_uint32, C.c_double, f32p]),
+        "ao_lift_metric": (None, [f32p, C.c_uint64, C.c_uint32, f32p, C.c_uint32, f32p, C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double)]),
+        "ao_ip_dist": (C.c_float, [f32p, f32p, C.c_uint32]),
+        "ao_init_knn_metric": (None, [f32p, f32p, C.c_uint32, C.c_uint64, C.c_uint32, u64p, u32p, C.c_uint64,
+                                      C.c_uint32, u32p, f32p]),
+        "ao_exact_topk_metric": (None, [f32p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, u32p, f32p]),
+        "ao_rknn_gt_metric": (C.c_int64, [f32p, C.c_uint64, f32p, C.c_uint64, C.c_uint32, f32p, C.c_uint32, u32p,
+                                          u32p, f32p, C.c_uint64]),
         "ao_heap_push": (C.c_int, [u32p, f32p, C.c_uint32, C.c_uint32, C.c_float]),
         "ao_warm_start": (None, [f32p, f32p, C.c_uint32, C.c_uint64, u32p, C.c_uint32, C.c_uint32, C.c_uint32,
                                  u32p, f32p]),
@@ -62,7 +77,7 @@ class AoIndex(C.Structure):
         ("lifted", C.c_void_p), ("deg", C.c_void_p), ("links", C.c_void_p), ("base", C.c_void_p),
         ("tree_nodes", C.c_uint32), ("tree_left", C.c_void_p), ("tree_right", C.c_void_p),
         ("tree_offset", C.c_void_p), ("tree_hyperplane", C.c_void_p), ("tree_leaf_first", C.c_void_p),
-        ("scale", C.c_double), ("mstar2", C.c_double),
+        ("scale", C.c_double), ("mstar2", C.c_double), ("metric", C.c_uint32),
     ]
 
 
@@ -70,6 +85,7 @@ class AoKnnGraph(C.Structure):
     _fields_ = [
         ("n", C.c_uint64), ("dim", C.c_uint32), ("x", C.c_void_p), ("norms", C.c_void_p), ("K", C.c_uint32),
         ("g_ids", C.c_void_p), ("g_vals", C.c_void_p), ("rev_off", C.c_void_p), ("rev_ids", C.c_void_p),
+        ("metric", C.c_uint32),
     ]
 
 
@@ -92,6 +108,9 @@ LIB.ao_graph_select.argtypes = [C.POINTER(AoKnnGraph), C.c_uint32, C.c_uint32, C
 LIB.ao_rp_tree.restype = C.c_int64
 LIB.ao_rp_tree.argtypes = [f32p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
                            C.POINTER(AoTreeOut)]
+LIB.ao_rp_tree_metric.restype = C.c_int64
+LIB.ao_rp_tree_metric.argtypes = [f32p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
+                                  C.c_uint32, C.POINTER(AoTreeOut)]
 
 
 def _p(a: np.ndarray) -> int:
@@ -130,13 +149,50 @@ def lrq_materialize(coeff, codes, mu, basis, codebook, k, scale=1.0):
     return thr
 
 
-def lift(base, radius):
+def _vp(a):
+    return None if a is None else a.ctypes.data
+
+
+def lrq_encode_bits(keys, mu, basis, codebook, bits, policy):
+    """Every codec form: returns coeff, packed codes (bytes, object-major) or
+    None, float residuals or None."""
+    keys = np.ascontiguousarray(keys, np.float32)
+    n, nk = keys.shape
+    rankm = basis.shape[0]
+    coeff = np.empty((n, rankm), np.float32)
+    codes = np.zeros((n * nk * bits + 7) // 8, np.uint8) if bits in (2, 4, 8, 16) else None
+    resid = np.empty((n, nk), np.float32) if bits == 32 else None
+    cb = None if codebook is None else np.ascontiguousarray(codebook, np.float32)
+    LIB.ao_lrq_encode_bits(keys, n, nk, rankm, np.ascontiguousarray(mu, np.float32),
+                           np.ascontiguousarray(basis, np.float32), _vp(cb), 0 if cb is None else cb.shape[1], bits,
+                           policy, coeff, _vp(codes), _vp(resid))
+    return coeff, codes, resid
+
+
+def lrq_materialize_bits(coeff, codes, resid, n, nk, mu, basis, codebook, bits, k, scale=1.0, signed_keys=False):
+    thr = np.empty(n, np.float32)
+    cb = None if codebook is None else np.ascontiguousarray(codebook, np.float32)
+    LIB.ao_lrq_materialize_bits(np.ascontiguousarray(coeff, np.float32), _vp(codes), _vp(resid), n, nk,
+                                basis.shape[0], bits, np.ascontiguousarray(mu, np.float32),
+                                np.ascontiguousarray(basis, np.float32), _vp(cb), 0 if cb is None else cb.shape[1], k,
+                                scale, int(signed_keys), thr)
+    return thr
+
+
+def analytic_rankm_materialize(coeff, train_kmax, flags, b0, k, scale=1.0):
+    coeff = np.ascontiguousarray(coeff, np.float32)
+    thr = np.empty(coeff.shape[0], np.float32)
+    LIB.ao_analytic_rankm_materialize(coeff, coeff.shape[0], coeff.shape[1], train_kmax, flags, b0, k, scale, thr)
+    return thr
+
+
+def lift(base, radius, metric=0):
     base = np.ascontiguousarray(base, np.float32)
     n, d = base.shape
     out = np.empty((n, d + 2), np.float32)
     m2 = C.c_double()
     sc = C.c_double()
-    LIB.ao_lift(base, n, d, np.ascontiguousarray(radius, np.float32), out, C.byref(m2), C.byref(sc))
+    LIB.ao_lift_metric(base, n, d, np.ascontiguousarray(radius, np.float32), metric, out, C.byref(m2), C.byref(sc))
     return out, m2.value, sc.value
 
 
@@ -173,10 +229,10 @@ def reverse(ids):
     return off, rev[:tot]
 
 
-def knn_graph(x, nrm, ids, vals, rev_off, rev):
+def knn_graph(x, nrm, ids, vals, rev_off, rev, metric=0):
     keep = (x, nrm, ids, vals, rev_off, rev)
     g = AoKnnGraph(x.shape[0], x.shape[1], _p(x), _p(nrm), ids.shape[1], _p(ids), _p(vals), _p(rev_off),
-                   _p(rev) if rev.size else _p(np.zeros(1, np.uint32)))
+                   _p(rev) if rev.size else _p(np.zeros(1, np.uint32)), metric)
     g._keep = keep
     return g
 
@@ -204,13 +260,13 @@ def graph_commit(x, nrm, O, Od, alpha=1.2):
     return links, deg
 
 
-def aknn_rows(x, nrm, ids, vals, K=100, ef=600, ef_alpha=8):
+def aknn_rows(x, nrm, ids, vals, K=100, ef=600, ef_alpha=8, metric=0):
     x = np.ascontiguousarray(x, np.float32)
     ids = np.ascontiguousarray(ids, np.uint32)
     vals = np.ascontiguousarray(vals, np.float32)
     off, rev = reverse(ids)
     rev = rev if rev.size else np.zeros(1, np.uint32)
-    g = knn_graph(x, nrm, ids, vals, off, rev)
+    g = knn_graph(x, nrm, ids, vals, off, rev, metric)
     n = x.shape[0]
     out_i = np.empty((n, K), np.uint32)
     out_d = np.empty((n, K), np.float32)
@@ -218,16 +274,16 @@ def aknn_rows(x, nrm, ids, vals, K=100, ef=600, ef_alpha=8):
     return out_i, out_d
 
 
-def init_knn(x, nrm, leaf_off, leaves, K):
+def init_knn(x, nrm, leaf_off, leaves, K, metric=0):
     n, dim = x.shape
     out_i = np.empty((n, K), np.uint32)
     out_d = np.empty((n, K), np.float32)
-    LIB.ao_init_knn(x, nrm, dim, n, K, np.ascontiguousarray(leaf_off, np.uint64),
-                    np.ascontiguousarray(leaves, np.uint32), len(leaf_off) - 1, out_i, out_d)
+    LIB.ao_init_knn_metric(x, nrm, dim, n, K, np.ascontiguousarray(leaf_off, np.uint64),
+                           np.ascontiguousarray(leaves, np.uint32), len(leaf_off) - 1, metric, out_i, out_d)
     return out_i, out_d
 
 
-def rp_tree(x, leaf_size, max_depth=100, seed=10, tree=0):
+def rp_tree(x, leaf_size, max_depth=100, seed=10, tree=0, angular=0):
     """Deterministic RP tree; returns dict of BFS-ordered node arrays + perm."""
     x = np.ascontiguousarray(x, np.float32)
     n, dim = x.shape
@@ -239,7 +295,7 @@ def rp_tree(x, leaf_size, max_depth=100, seed=10, tree=0):
     }
     t = AoTreeOut(_p(arr["left"]), _p(arr["right"]), _p(arr["offset"]), _p(arr["hyperplane"]), _p(arr["leaf_off"]),
                   _p(arr["leaf_cnt"]), _p(arr["perm"]), cap)
-    nn = LIB.ao_rp_tree(x, n, dim, leaf_size, max_depth, seed, tree, C.byref(t))
+    nn = LIB.ao_rp_tree_metric(x, n, dim, leaf_size, max_depth, seed, tree, angular, C.byref(t))
     assert nn > 0
     for k in ("left", "right", "offset", "hyperplane", "leaf_off", "leaf_cnt"):
         arr[k] = arr[k][:nn].copy()
@@ -247,16 +303,16 @@ def rp_tree(x, leaf_size, max_depth=100, seed=10, tree=0):
     return arr
 
 
-def exact_topk(base, K):
+def exact_topk(base, K, metric=0):
     base = np.ascontiguousarray(base, np.float32)
     n, d = base.shape
     ids = np.empty((n, K), np.uint32)
     keys = np.empty((n, K), np.float32)
-    LIB.ao_exact_topk(base, n, d, K, ids, keys)
+    LIB.ao_exact_topk_metric(base, n, d, K, metric, ids, keys)
     return ids, keys
 
 
-def rknn_gt(base, query, rk2):
+def rknn_gt(base, query, rk2, metric=0):
     base = np.ascontiguousarray(base, np.float32)
     query = np.ascontiguousarray(query, np.float32)
     n, d = base.shape
@@ -265,7 +321,8 @@ def rknn_gt(base, query, rk2):
     off = np.empty(nq + 1, np.uint32)
     ids = np.empty(cap, np.uint32)
     keys = np.empty(cap, np.float32)
-    tot = LIB.ao_rknn_gt(base, n, query, nq, d, np.ascontiguousarray(rk2, np.float32), off, ids, keys, cap)
+    tot = LIB.ao_rknn_gt_metric(base, n, query, nq, d, np.ascontiguousarray(rk2, np.float32), metric, off, ids, keys,
+                                cap)
     assert tot >= 0
     return off, ids[:tot], keys[:tot]
 
@@ -281,7 +338,7 @@ class TreeArrays:
         self.leaf_first = np.ascontiguousarray(leaf_first, np.uint32)
 
 
-def range_search_all(lifted, links, deg, base, tree: TreeArrays, scale, mstar2, queries, thr, L):
+def range_search_all(lifted, links, deg, base, tree: TreeArrays, scale, mstar2, queries, thr, L, metric=0):
     """Runs ao_range_search for each query; returns lists of candidate arrays,
     predicted arrays and distance counts."""
     lifted = np.ascontiguousarray(lifted, np.float32)
@@ -291,7 +348,7 @@ def range_search_all(lifted, links, deg, base, tree: TreeArrays, scale, mstar2, 
     n, dim = lifted.shape
     ix = AoIndex(n, dim, base.shape[1], links.shape[1], _p(lifted), _p(deg), _p(links), _p(base),
                  len(tree.left), _p(tree.left), _p(tree.right), _p(tree.offset), _p(tree.hyperplane),
-                 _p(tree.leaf_first), scale, mstar2)
+                 _p(tree.leaf_first), scale, mstar2, metric)
     cap = n
     cand = np.empty(cap, np.uint32)
     pred = np.empty(cap, np.uint32)

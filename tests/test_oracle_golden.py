@@ -134,6 +134,52 @@ def test_range_search_and_postfilter_bit_exact(sample, tmp_path):
                 assert list(preds[i]) == list(ref_p[i])
 
 
+def test_harness_qparity_both_entry_rules(sample, tmp_path):
+    """The reference harness's per-query mode: with ties sent left its
+    candidates, #dist and verified sets equal the oracle's range_search (whose
+    descent sends ties left, as the CUDA entry kernel does); with the
+    reference's own descent they equal the recorded reference outputs."""
+    import sys
+    sys.path.insert(0, str(GOLDEN.parent.parent / "oracle"))
+    import harness_io as hio
+    if not hio.HARNESS.exists():
+        pytest.skip("oracle/_ref/ref_harness not built")
+    p = tmp_path / "g.bin"
+    p.write_bytes(sample["graph_file"].tobytes())
+    g = formats.read_graph(p)
+    ks = (10, 50, 100)
+    thr = {k: sample["thresholds"][ki] for ki, k in enumerate((1, 10, 50, 100)) if k > 1}
+    hio.write_query_files(tmp_path, sample["base"], sample["query"], sample["lifted"], g.deg, g.links, g.tree,
+                          float(sample["mstar2"]), float(sample["scale"]), thr)
+    nq = len(sample["query"])
+    L = 32
+
+    class Res:
+        def __init__(self, cands, preds, nds):
+            self.c, self.p, self.n_dist = cands, preds, nds
+
+        def cand(self, i):
+            return self.c[i]
+
+        def pred(self, i):
+            return self.p[i]
+
+    oracle = {}
+    for k in ks:
+        cands, preds, nds = ol.range_search_all(sample["lifted"], g.links, g.deg, sample["base"], _tree_arrays(g),
+                                                float(sample["scale"]), float(sample["mstar2"]), sample["query"],
+                                                thr[k], L)
+        oracle[k] = Res(cands, preds, nds)
+    left = hio.run_qparity(tmp_path, L, "left", nq, ks)
+    assert hio.compare(left, oracle, nq)["identical"] == nq
+    recorded = {k: Res(csr_rows(sample[f"q_cand_off_{k}_{L}"], sample[f"q_cand_{k}_{L}"]),
+                       csr_rows(sample[f"q_pred_off_{k}_{L}"], sample[f"q_pred_{k}_{L}"]), sample[f"q_ndist_{k}_{L}"])
+                for k in ks}
+    tree = hio.run_qparity(tmp_path, L, "tree", nq, ks)
+    c = hio.compare(tree, recorded, nq)
+    assert c["identical"] == nq and c["differ_without_tie"] == 0, c
+
+
 def test_aknn_gather_bit_exact(sample):
     """Given the reference's init_knn heaps, the gather + top-K rows match."""
     x = sample["base"]
@@ -178,3 +224,41 @@ def test_reference_result_lines_reproduced(sample, tmp_path):
     for (k, L), v in zip(keys, vals):
         recall, precision = v[0], v[1]
         assert 0.9 <= recall <= 1.0 and 0.9 <= precision <= 1.0
+
+
+def test_lrq_every_form_bit_exact(tmp_path):
+    """Every CompactLrqVerifier form -- rank-M only, u2 / u4 / u8 / u16 codes
+    under each policy, float32 residuals, signed (IP) keys -- and the analytic
+    Rank-M model: the oracle's encode reproduces the reference's artifact byte
+    for byte (written by anqi.formats), its materialize the thresholds."""
+    import lrq_forms as lf
+    z, s = lf.load()
+    for bits, policy, signed in lf.forms(z):
+        keys, mu, basis = lf.inputs(z, s, signed)
+        cb = lf.codebook(z, bits)
+        coeff, codes, resid = ol.lrq_encode_bits(keys, mu, basis, cb, bits, formats.POLICY_CODE[policy])
+        p = tmp_path / f"o_{bits}_{policy}_{signed}.bin"
+        formats.write_verifier(p, coeff, codes, bits, policy, resid, nk=100)
+        assert p.read_bytes() == z[f"vf_{bits}_{policy}_{signed}"].tobytes(), (bits, policy, signed)
+        rc, rcodes, rres = lf.reference_artifact(z, tmp_path, bits, policy, signed)
+        for i, k in enumerate((1, 10, 50, 100)):
+            thr = ol.lrq_materialize_bits(rc, rcodes, rres, 256, 100, mu, basis, cb, bits, k, 1.0, bool(signed))
+            assert np.array_equal(thr.view(np.uint32), z[f"thr_{bits}_{policy}_{signed}"][i].view(np.uint32)), \
+                (bits, policy, signed, k)
+    for flags in (3, 7):
+        for si, scale in enumerate((1.0, 1.25)):
+            for i, k in enumerate((1, 10, 50, 100)):
+                thr = ol.analytic_rankm_materialize(z[f"pw_coeff_{flags}"], 100, flags, float(z[f"pw_b0_{flags}"][0]),
+                                                    k, scale)
+                assert np.array_equal(thr.view(np.uint32), z[f"pw_thr_{flags}"][si, i].view(np.uint32)), (flags, k)
+
+
+def test_analytic_model_file_roundtrip(tmp_path):
+    import lrq_forms as lf
+    z, _ = lf.load()
+    m = formats.AnalyticModel(100, 8, 10, 7, float(z["pw_b0_7"][0]), z["pw_coeff_7"])
+    formats.write_analytic(tmp_path / "pw.bin", m)
+    r = formats.read_analytic(tmp_path / "pw.bin", 256, 8)
+    assert r.flags == 7 and r.b0 == m.b0 and np.array_equal(r.coeff, m.coeff)
+    with pytest.raises(formats.FormatError):
+        formats.read_analytic(tmp_path / "pw.bin", 255, 8)
