@@ -13,6 +13,8 @@ from pathlib import Path
 
 import numpy as np
 
+from . import formats
+
 PKG = Path(__file__).resolve().parent.parent
 LIB_PATH = Path(os.environ.get("ANQI_LIBRARY", PKG / "lib" / "libanqi.so"))
 EMPTY = 0xFFFFFFFF
@@ -59,7 +61,7 @@ class QueryStats(C.Structure):
         ("n_dist", C.c_uint64), ("n_expand", C.c_uint64), ("n_cand", C.c_uint64), ("n_pred", C.c_uint64),
         ("n_flood", C.c_uint64), ("search_ms", C.c_float), ("total_ms", C.c_float), ("h2d_bytes", C.c_uint64),
         ("d2h_bytes", C.c_uint64), ("visited_table", C.c_uint32),
-        ("visited_l2_table", C.c_uint32),
+        ("visited_l2_table", C.c_uint32), ("warps_per_block", C.c_uint32), ("candidate_tile", C.c_uint32),
     ]
 
 
@@ -72,7 +74,8 @@ class AknnParams(C.Structure):
 class GraphParams(C.Structure):
     _fields_ = [("degree", C.c_uint32), ("nn_k", C.c_uint32), ("explore", C.c_uint32), ("ef_alpha", C.c_uint32),
                 ("join_iters", C.c_uint32), ("join_sample", C.c_uint32), ("leaf", C.c_uint32),
-                ("max_depth", C.c_uint32), ("seed", C.c_uint64), ("alpha", C.c_float), ("warm_width", C.c_uint32)]
+                ("max_depth", C.c_uint32), ("seed", C.c_uint64), ("alpha", C.c_float), ("warm_width", C.c_uint32),
+                ("precision", C.c_uint32)]
 
 
 class BuildStats(C.Structure):
@@ -89,6 +92,7 @@ _SIGS = {
     "anqi_ctx_destroy": [_vp],
     "anqi_last_error": [_vp],
     "anqi_version": [],
+    "anqi_inject_fault": [_vp, C.c_uint32],
     "anqi_device_bytes": [_vp],
     "anqi_timer_start": [_vp],
     "anqi_timer_stop": [_vp, C.POINTER(C.c_float)],
@@ -97,6 +101,12 @@ _SIGS = {
     "anqi_lrq_encode": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _f32, C.c_uint32, _f32, _u8],
     "anqi_lrq_materialize": [_vp, _f32, _u8, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _f32, C.c_uint32,
                              C.c_uint32, C.c_double, _f32],
+    "anqi_lrq_encode_bits": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _vp, C.c_uint32,
+                             C.c_uint32, C.c_uint32, _f32, _vp, _vp],
+    "anqi_lrq_materialize_bits": [_vp, _f32, _vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, _f32, _f32,
+                                  _vp, C.c_uint32, C.c_uint32, C.c_double, C.c_int, _f32],
+    "anqi_analytic_rankm_materialize": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                        C.c_double, C.c_uint32, C.c_double, _f32],
     "anqi_lift": [_vp, _f32, C.c_uint64, C.c_uint32, _f32, _f32, C.POINTER(C.c_double), C.POINTER(C.c_double)],
     "anqi_rp_forest": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
                        C.c_uint32, _u32, _u32, _u32, _f32, _f32, _u32, _u32, _u32],
@@ -113,11 +123,17 @@ _SIGS = {
                               _f32],
     "anqi_graph_localjoin": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _u32, _f32,
                              _u64, C.POINTER(C.c_uint32)],
+    "anqi_graph_localjoin_precision": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                       C.c_uint32, _u32, _f32, _u64, C.POINTER(C.c_uint32), C.POINTER(C.c_float)],
     "anqi_graph_select": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _f32, C.c_uint32, C.c_uint32, C.c_uint32,
                           C.c_uint32, C.c_float, _u32, _u32],
     "anqi_graph_commit": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _u32, C.c_uint32, C.c_float, _u32, _u32],
     "anqi_index_load": [_vp, C.POINTER(IndexDesc)],
     "anqi_verifier_load": [_vp, _f32, _u8, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _f32, C.c_uint32],
+    "anqi_verifier_load_bits": [_vp, _f32, _vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, _f32, _f32,
+                                _vp, C.c_uint32, C.c_int],
+    "anqi_verifier_load_analytic": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                    C.c_double],
     "anqi_verifier_materialize": [_vp, C.c_uint32, C.c_double],
     "anqi_set_thresholds": [_vp, C.c_uint32, _f32],
     "anqi_rknn_query": [_vp, _f32, C.c_uint32, _vp, C.c_uint32, _vp, C.c_uint32, _u32, _u32, C.c_uint64, _vp, _vp,
@@ -230,6 +246,11 @@ class Context:
             msg = self.lib.anqi_last_error(self.h)
             raise AnqiError(rc, f"{what}: {msg.decode() if msg else ''}")
 
+    def inject_fault(self, flags: int) -> None:
+        """Test hook (anqi_inject_fault): 1 = the search issues no row copies, so
+        its bounded waits run out and queries fail with ANQI_ERR_TIMEOUT; 0 = off."""
+        self._check(self.lib.anqi_inject_fault(self.h, flags), "inject_fault")
+
     def timer_start(self) -> None:
         self._check(self.lib.anqi_timer_start(self.h), "timer_start")
 
@@ -273,6 +294,45 @@ class Context:
                     "lrq_materialize")
         return thr
 
+    def lrq_encode_bits(self, keys, mu, basis, codebook, bits: int, policy: str = "floor"):
+        """Every CompactLrqVerifier form: returns coeff, packed code bytes (or
+        None), float residuals (bits 32, else None)."""
+        keys = _c(keys, np.float32)
+        n, nk = keys.shape
+        rankm = basis.shape[0]
+        coeff = np.empty((n, rankm), np.float32)
+        codes = np.zeros(formats.packed_code_bytes(n * nk, bits), np.uint8) if bits in formats.PACKED_BITS else None
+        resid = np.empty((n, nk), np.float32) if bits == 32 else None
+        cb = None if codebook is None else _c(codebook, np.float32)
+        self._check(self.lib.anqi_lrq_encode_bits(self.h, keys, n, nk, rankm, _c(mu, np.float32), _c(basis, np.float32),
+                                                  _ptr(cb), 0 if cb is None else cb.shape[1], bits,
+                                                  formats.POLICY_CODE[policy], coeff, _ptr(codes), _ptr(resid)),
+                    "lrq_encode_bits")
+        return coeff, codes, resid
+
+    def lrq_materialize_bits(self, coeff, codes, resid, nk: int, mu, basis, codebook, bits: int, k: int,
+                             radius_scale=1.0, signed_keys=False):
+        coeff = _c(coeff, np.float32)
+        n = coeff.shape[0]
+        thr = np.empty(n, np.float32)
+        cb = None if codebook is None else _c(codebook, np.float32)
+        self._check(self.lib.anqi_lrq_materialize_bits(
+            self.h, coeff, _ptr(None if codes is None else _c(codes, np.uint8)),
+            _ptr(None if resid is None else _c(resid, np.float32)), n, nk, basis.shape[0], bits, _c(mu, np.float32),
+            _c(basis, np.float32), _ptr(cb), 0 if cb is None else cb.shape[1], k, radius_scale, int(signed_keys), thr),
+            "lrq_materialize_bits")
+        return thr
+
+    def analytic_materialize(self, model, k: int, radius_scale=1.0):
+        """AnalyticRankMVerifier::materialize_k for a formats.AnalyticModel."""
+        coeff = _c(model.coeff, np.float32)
+        thr = np.empty(coeff.shape[0], np.float32)
+        self._check(self.lib.anqi_analytic_rankm_materialize(self.h, coeff, coeff.shape[0], coeff.shape[1],
+                                                             model.train_kmax, model.fit_kmin, model.flags,
+                                                             model.b0, k, radius_scale, thr),
+                    "analytic_rankm_materialize")
+        return thr
+
     def lift(self, base, radius):
         base = _c(base, np.float32)
         n, d = base.shape
@@ -308,6 +368,22 @@ class Context:
         self._check(self.lib.anqi_verifier_load(self.h, _c(coeff, np.float32), codes, n, nk, basis.shape[0],
                                                 _c(mu, np.float32), _c(basis, np.float32), _c(codebook, np.float32),
                                                 codebook.shape[1]), "verifier_load")
+
+    def verifier_load_bits(self, coeff, codes, resid, nk: int, mu, basis, codebook, bits: int,
+                           signed_keys=False) -> None:
+        coeff = _c(coeff, np.float32)
+        cb = None if codebook is None else _c(codebook, np.float32)
+        self._check(self.lib.anqi_verifier_load_bits(
+            self.h, coeff, _ptr(None if codes is None else _c(codes, np.uint8)),
+            _ptr(None if resid is None else _c(resid, np.float32)), coeff.shape[0], nk, basis.shape[0], bits,
+            _c(mu, np.float32), _c(basis, np.float32), _ptr(cb), 0 if cb is None else cb.shape[1],
+            int(signed_keys)), "verifier_load_bits")
+
+    def verifier_load_analytic(self, model) -> None:
+        coeff = _c(model.coeff, np.float32)
+        self._check(self.lib.anqi_verifier_load_analytic(self.h, coeff, coeff.shape[0], coeff.shape[1],
+                                                         model.train_kmax, model.fit_kmin, model.flags, model.b0),
+                    "verifier_load_analytic")
 
     def verifier_materialize(self, k: int, radius_scale: float = 1.0) -> None:
         self._check(self.lib.anqi_verifier_materialize(self.h, k, radius_scale), "verifier_materialize")

@@ -230,16 +230,94 @@ def write_knn_table(path, ids: np.ndarray, keys: np.ndarray) -> None:
 VERIFIER_MAGIC = b"ANQIVF2\0"
 
 
-def write_verifier(path, coeff: np.ndarray, codes: np.ndarray, bits: int = 8, policy: str = "floor") -> None:
-    """``"ANQIVF2\\0"[u64 n][u32 nk, rankm, bits, code_size, policy]`` + coeff + codes
-    (src/rknn_query.cpp:755-789; policy 1 = floor)."""
+PACKED_BITS = (2, 4, 8, 16)
+POLICY_CODE = {"nearest": 0, "floor": 1, "ceil": 2}
+
+
+def packed_code_bytes(count: int, bits: int) -> int:
+    """include/packed_code_array.h:14-18."""
+    return (count * bits + 7) // 8 if bits in PACKED_BITS else 0
+
+
+def write_verifier(path, coeff: np.ndarray, codes: np.ndarray | None = None, bits: int = 8, policy: str = "floor",
+                   residual: np.ndarray | None = None, nk: int | None = None) -> None:
+    """``"ANQIVF2\\0"[u64 n][u32 nk, rankm, bits, code_size, policy]`` + coeff +
+    packed codes + float residuals (src/rknn_query.cpp:755-789).  bits 0: no
+    codes; 2/4/8/16: codes as packed bytes (or an n x nk array for u8); 32:
+    residual n x nk.  code_size is 2^bits for packed codes, else 0."""
     n, rankm = coeff.shape
-    nk = codes.shape[1]
-    pol = {"floor": 1, "ceil": 2}.get(policy, 0)
-    hdr = VERIFIER_MAGIC + struct.pack("<QIIIII", n, nk, rankm, bits, 1 << bits, pol)
+    if nk is None:
+        nk = codes.shape[1] if codes is not None and codes.ndim == 2 else residual.shape[1]
+    cs = 1 << bits if bits in PACKED_BITS else 0
+    body = np.asarray(coeff, "<f4").tobytes()
+    if bits in PACKED_BITS:
+        cb = np.asarray(codes, np.uint8).tobytes()
+        if len(cb) != packed_code_bytes(n * nk, bits):
+            raise FormatError("packed code size does not match n x nk x bits")
+        body += cb
+    if bits == 32:
+        body += np.asarray(residual, "<f4").tobytes()
+    hdr = VERIFIER_MAGIC + struct.pack("<QIIIII", n, nk, rankm, bits, cs, POLICY_CODE.get(policy, 0))
     tmp = Path(str(path) + ".tmp")
-    tmp.write_bytes(hdr + np.asarray(coeff, "<f4").tobytes() + np.asarray(codes, np.uint8).tobytes())
+    tmp.write_bytes(hdr + body)
     os.replace(tmp, path)
+
+
+def read_verifier_any(path, n: int, nk: int = 100, rankm: int = 8, bits: int = 8, policy: str = "floor"):
+    """Any ANQIVF2 form (CompactLrqVerifier::load, src/rknn_query.cpp:791-838):
+    returns coeff (n x rankm), packed code bytes or None, residual (n x nk) or None."""
+    raw = Path(path).read_bytes()
+    if len(raw) < 36 or raw[:8] != VERIFIER_MAGIC:
+        raise FormatError(f"LRQ verifier artifact header mismatch {path}")
+    n64, nk32, m32, b32, cs32, pol = struct.unpack("<QIIIII", raw[8:36])
+    cs = 1 << bits if bits in PACKED_BITS else 0
+    if (n64 != n or nk32 != nk or m32 != rankm or b32 != bits or cs32 != cs
+            or pol != POLICY_CODE.get(policy, 0)):
+        raise FormatError(f"LRQ verifier artifact header mismatch {path}")
+    cbytes = packed_code_bytes(n * nk, bits)
+    rbytes = 4 * n * nk if bits == 32 else 0
+    if len(raw) != 36 + 4 * n * rankm + cbytes + rbytes:
+        raise FormatError(f"truncated or oversized LRQ verifier artifact {path}")
+    coeff = np.frombuffer(raw, "<f4", n * rankm, 36).reshape(n, rankm).copy()
+    at = 36 + 4 * n * rankm
+    codes = np.frombuffer(raw, np.uint8, cbytes, at).copy() if cbytes else None
+    resid = np.frombuffer(raw, "<f4", n * nk, at + cbytes).reshape(n, nk).copy() if rbytes else None
+    return coeff, codes, resid
+
+
+ANALYTIC_MAGIC = b"ANQIPW1\0"
+
+
+@dataclass
+class AnalyticModel:
+    """``_analytic_rankm_M{M}.bin``: ``"ANQIPW1\\0"[u64 n][u32 train_kmax, rankm,
+    fit_kmin, flags][f64 b0][f32 n x rankm]`` (src/rknn_query.cpp:528-573)."""
+
+    train_kmax: int
+    rankm: int
+    fit_kmin: int
+    flags: int
+    b0: float
+    coeff: np.ndarray
+
+
+def read_analytic(path, n: int, rankm: int) -> AnalyticModel:
+    raw = Path(path).read_bytes()
+    if len(raw) < 40 or raw[:8] != ANALYTIC_MAGIC:
+        raise FormatError(f"analytic Rank-M header mismatch {path}")
+    n64, tk, m, fk, flags = struct.unpack("<QIIII", raw[8:32])
+    (b0,) = struct.unpack("<d", raw[32:40])
+    if (n64 != n or m != rankm or tk < 1 or fk < 1 or fk > tk or flags not in (3, 7) or not np.isfinite(b0)):
+        raise FormatError(f"analytic Rank-M header mismatch {path}")
+    if len(raw) != 40 + 4 * n * rankm:
+        raise FormatError(f"truncated or oversized analytic Rank-M model {path}")
+    return AnalyticModel(tk, m, fk, flags, b0, np.frombuffer(raw, "<f4", n * m, 40).reshape(n, m).copy())
+
+
+def write_analytic(path, model: AnalyticModel) -> None:
+    n, m = model.coeff.shape
+    Path(path).write_bytes(ANALYTIC_MAGIC + struct.pack("<QIIII", n, model.train_kmax, m, model.fit_kmin, model.flags)
+                           + struct.pack("<d", model.b0) + np.asarray(model.coeff, "<f4").tobytes())
 
 
 def read_verifier(path, n: int, nk: int = 100, rankm: int = 8, bits: int = 8):

@@ -91,12 +91,16 @@ def aknn_build(ctx: Context, base: np.ndarray, k=100, leaf=500, trees=64, ef=600
 
 
 def graph_build(ctx: Context, lifted: np.ndarray, warm_ids: np.ndarray, degree=48, nn_k=50, explore=100,
-                ef_alpha=8, join_iters=6, join_sample=20, leaf=100, seed=10, alpha=1.2, warm_width=100):
-    """build_index with the flat AKNN warm start; returns deg, links, post-order tree, stats."""
+                ef_alpha=8, join_iters=6, join_sample=20, leaf=100, seed=10, alpha=1.2, warm_width=100,
+                precision="bf16"):
+    """build_index with the flat AKNN warm start; returns deg, links, post-order tree, stats.
+    precision "bf16": LocalJoin pairs filtered on BF16 tensor-core tiles, kept
+    pairs recomputed in FP32 (identical graph); "fp32": CUDA cores only."""
     lifted = np.ascontiguousarray(lifted, np.float32)
     warm_ids = np.ascontiguousarray(warm_ids, np.uint32)
     n, dim = lifted.shape
-    gp = GraphParams(degree, nn_k, explore, ef_alpha, join_iters, join_sample, leaf, 100, seed, alpha, warm_width)
+    gp = GraphParams(degree, nn_k, explore, ef_alpha, join_iters, join_sample, leaf, 100, seed, alpha, warm_width,
+                     {"fp32": 0, "bf16": 1}[precision])
     deg = np.empty(n, np.uint32)
     links = np.empty((n, degree), np.uint32)
     st = BuildStats()
@@ -116,6 +120,34 @@ def graph_build(ctx: Context, lifted: np.ndarray, warm_ids: np.ndarray, degree=4
     ctx._check(ctx.lib.anqi_graph_tree_copy(ctx.h, left, right, off, hyp, lo, lc, perm), "tree_copy")
     tree = formats.bfs_tree_to_postorder(left, right, off, hyp, lo, lc, perm, leaf, dim)
     return deg, links, tree, st.as_dict()
+
+
+def graph_warm_start(ctx: Context, lifted: np.ndarray, warm_ids: np.ndarray, width=100, K=50):
+    """Warm-start heaps of the G48 build (index.h:1204-1218): ids, vals (n x K)."""
+    lifted = np.ascontiguousarray(lifted, np.float32)
+    warm_ids = np.ascontiguousarray(warm_ids, np.uint32)
+    n, dim = lifted.shape
+    ids = np.empty((n, K), np.uint32)
+    vals = np.empty((n, K), np.float32)
+    ctx._check(ctx.lib.anqi_graph_warm_start(ctx.h, lifted, n, dim, warm_ids, warm_ids.shape[1], width, K, ids, vals),
+               "graph_warm_start")
+    return ids, vals
+
+
+def graph_localjoin(ctx: Context, lifted: np.ndarray, ids, vals, precision="bf16", sample=20, rounds=6):
+    """LocalJoin rounds on given heaps (index.h:1468-1487, snapshot form):
+    returns ids, vals, per-round updates, device milliseconds of the rounds."""
+    lifted = np.ascontiguousarray(lifted, np.float32)
+    ids = np.ascontiguousarray(ids, np.uint32).copy()
+    vals = np.ascontiguousarray(vals, np.float32).copy()
+    n, dim = lifted.shape
+    up = np.zeros(rounds, np.uint64)
+    done = C.c_uint32()
+    ms = C.c_float()
+    ctx._check(ctx.lib.anqi_graph_localjoin_precision(ctx.h, lifted, n, dim, ids.shape[1], sample, rounds,
+                                                      {"fp32": 0, "bf16": 1}[precision], ids, vals, up,
+                                                      C.byref(done), C.byref(ms)), "graph_localjoin")
+    return ids, vals, [int(u) for u in up[:done.value]], ms.value
 
 
 def build_index(ctx: Context, base: np.ndarray, aknn=None, graph=None, train_workers: int = 8, log=print) -> Index:

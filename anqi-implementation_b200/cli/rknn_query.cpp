@@ -172,14 +172,21 @@ static std::string graph_file_name(uint64_t M, uint64_t nn_k, uint64_t n, uint64
 }
 
 // ------------------------------------------------------------- verifier
+// CompactLrqVerifier state (rknn_query.cpp:604-753): bits 0 (rank-M only),
+// 2 / 4 / 8 / 16 (packed codes, learned codebook), 32 (float residuals).
 struct Lrq {
     uint64_t n = 0;
     uint32_t nk = 0, rankm = 0, bits = 0, code_size = 0;
-    std::vector<float> mu, basis, codebook, coeff;
-    std::vector<uint8_t> codes;
+    std::string policy = "floor";
+    std::vector<float> mu, basis, codebook, coeff, residual;
+    std::vector<uint8_t> codes;  // packed, object-major
+    uint32_t policy_code() const { return policy == "floor" ? 1u : (policy == "ceil" ? 2u : 0u); }
+    uint64_t code_bytes() const {
+        return (bits == 2 || bits == 4 || bits == 8 || bits == 16) ? (n * nk * bits + 7) / 8 : 0;
+    }
     uint64_t persistent_bytes() const {
-        return coeff.size() * 4 + codes.size() + mu.size() * 4 + basis.size() * 4 + codebook.size() * 4 + 36 + 8 +
-               (bits ? 24 : 0);
+        return coeff.size() * 4 + codes.size() + residual.size() * 4 + mu.size() * 4 + basis.size() * 4 +
+               codebook.size() * 4 + 36 + 8 + (bits ? 24 : 0);
     }
 };
 
@@ -230,17 +237,18 @@ static void load_codebook(const std::string& path, uint64_t NK, int RANKM, int b
                 die(3, "[rknn] LRQ codebook row %d is not sorted: %s", k, path.c_str());
 }
 
-// ANQIVF2 artifact, CompactLrqVerifier::save/load (rknn_query.cpp:755-838), floor policy.
+// ANQIVF2 artifact, CompactLrqVerifier::save/load (rknn_query.cpp:755-838).
 static void save_verifier(const std::string& path, const Lrq& v) {
     const std::string tmp = path + ".tmp";
     std::ofstream f(tmp, std::ios::binary | std::ios::trunc);
     if (!f) die(3, "[rknn] cannot write LRQ verifier artifact %s", tmp.c_str());
-    const uint32_t hdr[5] = {v.nk, v.rankm, v.bits, v.code_size, 1u};
+    const uint32_t hdr[5] = {v.nk, v.rankm, v.bits, v.code_size, v.policy_code()};
     f.write("ANQIVF2\0", 8);
     f.write(reinterpret_cast<const char*>(&v.n), 8);
     f.write(reinterpret_cast<const char*>(hdr), sizeof(hdr));
     f.write(reinterpret_cast<const char*>(v.coeff.data()), (std::streamsize)v.coeff.size() * 4);
     f.write(reinterpret_cast<const char*>(v.codes.data()), (std::streamsize)v.codes.size());
+    f.write(reinterpret_cast<const char*>(v.residual.data()), (std::streamsize)v.residual.size() * 4);
     if (!f) die(3, "[rknn] failed while writing LRQ verifier artifact %s", tmp.c_str());
     f.close();
     if (!f || std::rename(tmp.c_str(), path.c_str()) != 0) die(3, "[rknn] cannot publish LRQ verifier artifact %s", path.c_str());
@@ -256,16 +264,56 @@ static void load_verifier(const std::string& path, Lrq& v) {
     f.read(reinterpret_cast<char*>(&n64), 8);
     f.read(reinterpret_cast<char*>(hdr), sizeof(hdr));
     if (!f || std::memcmp(magic, "ANQIVF2\0", 8) != 0 || n64 != v.n || hdr[0] != v.nk || hdr[1] != v.rankm ||
-        hdr[2] != v.bits || hdr[3] != v.code_size || hdr[4] != 1u)
+        hdr[2] != v.bits || hdr[3] != v.code_size || hdr[4] != v.policy_code())
         die(3, "[rknn] LRQ verifier artifact header mismatch %s", path.c_str());
     v.coeff.resize(v.n * v.rankm);
-    v.codes.resize(v.n * v.nk);
+    v.codes.resize(v.code_bytes());
+    v.residual.resize(v.bits == 32 ? v.n * v.nk : 0);
     f.read(reinterpret_cast<char*>(v.coeff.data()), (std::streamsize)v.coeff.size() * 4);
     if (f.gcount() != (std::streamsize)v.coeff.size() * 4) die(3, "[rknn] truncated LRQ verifier coefficients %s", path.c_str());
     f.read(reinterpret_cast<char*>(v.codes.data()), (std::streamsize)v.codes.size());
     if (f.gcount() != (std::streamsize)v.codes.size()) die(3, "[rknn] truncated LRQ verifier codes %s", path.c_str());
+    f.read(reinterpret_cast<char*>(v.residual.data()), (std::streamsize)v.residual.size() * 4);
+    if (f.gcount() != (std::streamsize)v.residual.size() * 4)
+        die(3, "[rknn] truncated float32 residuals %s", path.c_str());
     char extra;
     if (f.read(&extra, 1)) die(3, "[rknn] oversized LRQ verifier artifact %s", path.c_str());
+}
+
+// ANQIPW1 analytic Rank-M model, AnalyticRankMVerifier::load (rknn_query.cpp:528-573).
+struct AnalyticModel {
+    uint32_t train_kmax = 0, fit_kmin = 0, flags = 0;
+    double b0 = 0;
+    std::vector<float> coeff;
+};
+
+static AnalyticModel read_analytic_model(const std::string& path, uint64_t n, int rankm) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) die(3, "[rknn] missing analytic Rank-M model %s", path.c_str());
+    char magic[8] = {};
+    uint64_t n64 = 0;
+    uint32_t h[4] = {0, 0, 0, 0};
+    AnalyticModel m;
+    f.read(magic, 8);
+    f.read(reinterpret_cast<char*>(&n64), 8);
+    f.read(reinterpret_cast<char*>(h), sizeof(h));
+    f.read(reinterpret_cast<char*>(&m.b0), 8);
+    m.train_kmax = h[0];
+    m.fit_kmin = h[2];
+    m.flags = h[3];
+    if (!f || std::memcmp(magic, "ANQIPW1\0", 8) != 0 || n64 != n || h[1] != (uint32_t)rankm || h[0] < 1 ||
+        h[2] < 1 || h[2] > h[0] || (h[3] != 3u && h[3] != 7u) || !std::isfinite(m.b0))
+        die(3,
+            "[rknn] analytic Rank-M header mismatch %s: n=%llu train_kmax=%u rankm=%u fit_kmin=%u flags=%u b0=%.9g "
+            "expected n=%" PRIu64 " rankm=%d",
+            path.c_str(), (unsigned long long)n64, h[0], h[1], h[2], h[3], m.b0, n, rankm);
+    m.coeff.resize(n * (uint64_t)rankm);
+    f.read(reinterpret_cast<char*>(m.coeff.data()), (std::streamsize)m.coeff.size() * 4);
+    if (f.gcount() != (std::streamsize)m.coeff.size() * 4)
+        die(3, "[rknn] truncated analytic Rank-M coefficients %s", path.c_str());
+    char extra;
+    if (f.read(&extra, 1)) die(3, "[rknn] oversized analytic Rank-M model %s", path.c_str());
+    return m;
 }
 
 // ------------------------------------------------------------------ main
@@ -421,17 +469,48 @@ static int run(int argc, char** argv) {
     };
     if (metric != "l2") not_here("metric=" + metric);
     if (geometry != "anyk_lift") not_here("ANQI_GRAPH_GEOMETRY=" + geometry);
-    if (!is_learned_rq_mode(radius_mode) || radius_mode.rfind("rankm_resid_u8_lrq_", 0) != 0 ||
-        radius_mode.size() < 6 || radius_mode.compare(radius_mode.size() - 6, 6, "_floor") != 0)
+    // the independent postfilter verifiers (rknn_query.cpp:1771-1792): learned
+    // LRQ (u2 / u4 / u8 / u16, floor / ceil / nearest), float32 residuals,
+    // rank-M only, exact source thresholds, analytic rank-M
+    enum class VMode { Compact, Exact, Analytic };
+    VMode vmode = VMode::Compact;
+    int bits = 0;
+    std::string lrq_policy = "floor";
+    std::string vmode_label;
+    if (is_learned_rq_mode(radius_mode)) {
+        bits = radius_mode.rfind("rankm_resid_u2_", 0) == 0 ? 2
+               : radius_mode.rfind("rankm_resid_u4_", 0) == 0 ? 4
+               : radius_mode.rfind("rankm_resid_u8_", 0) == 0 ? 8 : 16;
+        const bool fl = radius_mode.size() >= 6 && radius_mode.compare(radius_mode.size() - 6, 6, "_floor") == 0;
+        const bool ce = radius_mode.size() >= 5 && radius_mode.compare(radius_mode.size() - 5, 5, "_ceil") == 0;
+        lrq_policy = fl ? "floor" : (ce ? "ceil" : "nearest");
+        vmode_label = "rank-M+LRQ";
+    } else if (radius_mode == "rankm_resid_f32") {
+        bits = 32;
+        vmode_label = "rank-M+float32-residual";
+    } else if (radius_mode == "rankm_only") {
+        bits = 0;
+        vmode_label = "rank-M-only";
+    } else if (radius_mode == "exact_f32") {
+        vmode = VMode::Exact;
+        vmode_label = "exact_f32";
+    } else if (radius_mode == "analytic_rankm") {
+        vmode = VMode::Analytic;
+        vmode_label = "analytic-rank-M";
+    } else {
         not_here("ANQI_RADIUS_MODE=" + radius_mode);
+    }
     const std::string placement = env_or("ANQI_VERIFIER_PLACEMENT", "postfilter");
     if (placement != "integrated" && placement != "postfilter")
         die(2, "[rknn] unsupported ANQI_VERIFIER_PLACEMENT=%s (expected integrated or postfilter)", placement.c_str());
     if (placement != "postfilter") not_here("ANQI_VERIFIER_PLACEMENT=" + placement);
-    if (RANKM <= 0) die(2, "[rknn] the LRQ verifier requires ANQI_RANKM>0");
+    if (RANKM <= 0 && vmode == VMode::Compact) die(2, "[rknn] the rank-M verifier requires ANQI_RANKM>0");
+    if (RANKM <= 0 && vmode == VMode::Analytic) die(2, "[rknn] analytic_rankm requires ANQI_RANKM>0");
     if (std::getenv("ANQI_SPECIFIC"))
         die(2, "[rknn] independent postfilter verifier requires a shared graph; unset ANQI_SPECIFIC");
-    const std::string envelope = env_or("ANQI_CANDIDATE_ENVELOPE", "graph_horizon");
+    // analytic_rankm defaults to the verifier envelope (rknn_query.cpp:1816-1818)
+    const std::string envelope =
+        env_or("ANQI_CANDIDATE_ENVELOPE", vmode == VMode::Analytic ? "verifier" : "graph_horizon");
     if (envelope != "graph_horizon" && envelope != "verifier")
         die(2, "[rknn] unsupported ANQI_CANDIDATE_ENVELOPE=%s (expected graph_horizon or verifier)", envelope.c_str());
     if (envelope != "graph_horizon") not_here("ANQI_CANDIDATE_ENVELOPE=" + envelope);
@@ -453,26 +532,36 @@ static int run(int argc, char** argv) {
     const double slack_factor = 1.0 + rankm_slack;
     if (slack_factor <= 0.0)
         die(2, "[rknn] ANQI_RANKM_SLACK=%.6g makes non-positive radius scale", rankm_slack);
-    const int bits = 8;
+    if (vmode == VMode::Exact && rankm_slack != 0.0)
+        die(2, "[rknn] exact_f32 postfilter does not accept ANQI_RANKM_SLACK");
 
     // ---- cache identities (rknn_query.cpp:1840-1872, 1217-1241)
     const std::string basis_path = PFX + "_radbasis_M" + std::to_string(RANKM) + ".bin";
     const std::string cb_path = env_or("ANQI_RQ_CODEBOOK", (PFX + "_learned_rq_codebook_M" + std::to_string(RANKM) +
                                                             "_u" + std::to_string(bits) + ".bin").c_str());
-    std::string radius_key = radius_mode + ":M" + env_or("ANQI_RANKM", "0") + ":b" +
-                             (std::getenv("ANQI_RESID_BIAS") ? std::getenv("ANQI_RESID_BIAS") : "0") +
-                             ":obj" + env_or("ANQI_RQ_OBJECTIVE", "radius_reconstruction") + ":basis" +
-                             (std::getenv("ANQI_RQ_BASIS_ID") && *std::getenv("ANQI_RQ_BASIS_ID")
-                                  ? std::string(std::getenv("ANQI_RQ_BASIS_ID"))
-                                  : file_fingerprint(basis_path)) +
-                             ":cb" +
-                             (std::getenv("ANQI_RQ_CODEBOOK_ID") && *std::getenv("ANQI_RQ_CODEBOOK_ID")
-                                  ? std::string(std::getenv("ANQI_RQ_CODEBOOK_ID"))
-                                  : file_fingerprint(cb_path));
-    const std::string radius_source_id = std::getenv("ANQI_RADIUS_SOURCE_ID")
-                                             ? env_or("ANQI_RADIUS_SOURCE_ID", "missing_radius_source_id")
-                                             : threshold_source_identity(PFX);
-    radius_key += ":src" + hash16(radius_source_id) + ":rqpred_v3";
+    const std::string model_path =
+        env_or("ANQI_ANALYTIC_RANKM_MODEL", (PFX + "_analytic_rankm_M" + std::to_string(RANKM) + ".bin").c_str());
+    std::string radius_key;
+    if (vmode == VMode::Compact) {
+        radius_key = radius_mode + ":M" + env_or("ANQI_RANKM", "0") + ":b" +
+                     (std::getenv("ANQI_RESID_BIAS") ? std::getenv("ANQI_RESID_BIAS") : "0") + ":obj" +
+                     env_or("ANQI_RQ_OBJECTIVE", "radius_reconstruction") + ":basis" +
+                     (std::getenv("ANQI_RQ_BASIS_ID") && *std::getenv("ANQI_RQ_BASIS_ID")
+                          ? std::string(std::getenv("ANQI_RQ_BASIS_ID"))
+                          : file_fingerprint(basis_path));
+        if (is_learned_rq_mode(radius_mode))
+            radius_key += ":cb" + (std::getenv("ANQI_RQ_CODEBOOK_ID") && *std::getenv("ANQI_RQ_CODEBOOK_ID")
+                                       ? std::string(std::getenv("ANQI_RQ_CODEBOOK_ID"))
+                                       : file_fingerprint(cb_path));
+        const std::string radius_source_id = std::getenv("ANQI_RADIUS_SOURCE_ID")
+                                                 ? env_or("ANQI_RADIUS_SOURCE_ID", "missing_radius_source_id")
+                                                 : threshold_source_identity(PFX);
+        radius_key += ":src" + hash16(radius_source_id) + ":rqpred_v3";
+    } else if (vmode == VMode::Analytic) {
+        radius_key = radius_mode + ":M" + std::to_string(RANKM) + ":model" + hash16(file_fingerprint(model_path));
+    } else {
+        radius_key = radius_mode;
+    }
     std::string graph_key = graph_cache_key(Marg, leafA, ntA, efA);
     const std::string graph_radius_source = env_or("ANQI_GRAPH_RADIUS_SOURCE_PFX", PFX.c_str());
     const std::string graph_radius_id =
@@ -516,44 +605,72 @@ static int run(int argc, char** argv) {
     lrq.n = n;
     lrq.nk = (uint32_t)NK;
     lrq.rankm = (uint32_t)RANKM;
-    lrq.bits = bits;
-    load_basis(basis_path, NK, RANKM, lrq);
-    printf("[rknn] loaded rank-M basis: M=%d path=%s\n", RANKM, basis_path.c_str());
-    load_codebook(cb_path, NK, RANKM, bits, lrq);
-    if (lrq.code_size != 256) die(3, "[rknn] u8 LRQ codebook must have 256 entries per rank, got %u", lrq.code_size);
-
+    lrq.bits = (uint32_t)bits;
+    lrq.policy = is_learned_rq_mode(radius_mode) ? lrq_policy : (bits == 32 ? "float32" : "rankm");
     std::unique_ptr<Device> device;  // created when the first device stage runs
     auto dev = [&]() -> Device& {
         if (!device) device = std::make_unique<Device>("[rknn]");
         return *device;
     };
-    const std::string lrq_file = verifier_cache_dir + "_anqi_verifier_" + hash16(radius_key) + ".bin";
-    bool lrq_ready = false;
     double verifier_load_ms = 0, verifier_encode_save_ms = 0;
-    if (file_exists(lrq_file)) {
+    AnalyticModel model;
+    if (vmode == VMode::Analytic) {
+        const auto t0 = Clock::now();
+        model = read_analytic_model(model_path, n, RANKM);
+        verifier_load_ms = since(t0) * 1e3;
+        if (model.train_kmax != GRAPH_NK)
+            die(2, "[rknn] analytic Rank-M training horizon=%u must match graph horizon=%" PRIu64
+                   " for the controlled multi-rank experiment", model.train_kmax, GRAPH_NK);
+        printf("[rknn] loaded analytic Rank-M verifier %s (train_kmax=%u fit_kmin=%u M=%d b0=%.9g flags=%u "
+               "persistent=%.3fGB load_ms=%.3f)\n",
+               model_path.c_str(), model.train_kmax, model.fit_kmin, RANKM, model.b0, model.flags,
+               (40.0 + model.coeff.size() * 4.0) / 1e9, verifier_load_ms);
+    }
+    if (vmode == VMode::Compact) {
+        load_basis(basis_path, NK, RANKM, lrq);
+        printf("[rknn] loaded rank-M basis: M=%d path=%s\n", RANKM, basis_path.c_str());
+        if (is_learned_rq_mode(radius_mode)) {
+            load_codebook(cb_path, NK, RANKM, bits, lrq);
+            if (lrq.code_size != (1u << bits)) die(3, "[rknn] invalid CompactLrqVerifier configuration");
+        }
+        if ((bits == 2 && NK % 4 != 0) || (bits == 4 && NK % 2 != 0))
+            die(3, "[rknn] packed u%d verifier requires NK divisible by %d, got %" PRIu64, bits, bits == 2 ? 4 : 2, NK);
+    }
+    const std::string lrq_file = verifier_cache_dir + "_anqi_verifier_" + hash16(radius_key) + ".bin";
+    bool lrq_ready = vmode != VMode::Compact;
+    if (vmode == VMode::Compact && file_exists(lrq_file)) {
         const auto t0 = Clock::now();
         load_verifier(lrq_file, lrq);
         lrq_ready = true;
         verifier_load_ms = since(t0) * 1e3;
-        printf("[rknn] loaded independent compact verifier mode=rank-M+LRQ bits=%d %s (persistent=%.3fGB "
+        printf("[rknn] loaded independent compact verifier mode=%s bits=%d %s (persistent=%.3fGB "
                "load_ms=%.3f)\n",
-               bits, lrq_file.c_str(), lrq.persistent_bytes() / 1e9, verifier_load_ms);
+               vmode_label.c_str(), bits, lrq_file.c_str(), lrq.persistent_bytes() / 1e9, verifier_load_ms);
     }
     auto ensure_lrq = [&]() {
         if (lrq_ready) return;
         const std::vector<float> keys = load_threshold_table(PFX, n, NK);
         const auto t0 = Clock::now();
         lrq.coeff.resize(n * lrq.rankm);
-        lrq.codes.resize(n * NK);
-        dev().check(anqi_lrq_encode(dev().get(), keys.data(), n, lrq.nk, lrq.rankm, lrq.mu.data(), lrq.basis.data(),
-                                  lrq.codebook.data(), lrq.code_size, lrq.coeff.data(), lrq.codes.data()),
-                  "LRQ encode");
+        lrq.codes.assign(lrq.code_bytes(), 0);
+        lrq.residual.resize(bits == 32 ? n * NK : 0);
+        dev().check(anqi_lrq_encode_bits(dev().get(), keys.data(), n, lrq.nk, lrq.rankm, lrq.mu.data(),
+                                         lrq.basis.data(), lrq.codebook.empty() ? nullptr : lrq.codebook.data(),
+                                         lrq.code_size, lrq.bits, lrq.policy_code(), lrq.coeff.data(),
+                                         lrq.codes.empty() ? nullptr : lrq.codes.data(),
+                                         lrq.residual.empty() ? nullptr : lrq.residual.data()),
+                    "LRQ encode");
         save_verifier(lrq_file, lrq);
         verifier_encode_save_ms = since(t0) * 1e3;
         lrq_ready = true;
-        printf("[rknn] built independent compact verifier mode=rank-M+LRQ bits=%d %s (persistent=%.3fGB "
+        printf("[rknn] built independent compact verifier mode=%s bits=%d %s (persistent=%.3fGB "
                "encode_save_ms=%.3f)\n",
-               bits, lrq_file.c_str(), lrq.persistent_bytes() / 1e9, verifier_encode_save_ms);
+               vmode_label.c_str(), bits, lrq_file.c_str(), lrq.persistent_bytes() / 1e9, verifier_encode_save_ms);
+    };
+    // bytes the reference reports for the verification structure (rknn_query.cpp:2015-2020, 1243-1264)
+    auto verification_bytes = [&]() -> uint64_t {
+        return vmode == VMode::Compact ? lrq.persistent_bytes()
+                                       : (vmode == VMode::Analytic ? 40 + n * (uint64_t)RANKM * 4 : n * NK * 4);
     };
 
     std::vector<float> lifted;
@@ -621,7 +738,7 @@ static int run(int argc, char** argv) {
         ensure_lrq();
         const std::vector<float> radius = load_threshold_column(graph_radius_source, n, GRAPH_NK);
         printf("[rknn] RADIUS_MODE=%s:postfilter conceptual_radius_store=%.3fGB\n", radius_key.c_str(),
-               lrq.persistent_bytes() / 1e9);
+               verification_bytes() / 1e9);
         lifted.resize(n * dim);
         dev().check(anqi_lift(dev().get(), base.x.data(), n, (uint32_t)d, radius.data(), lifted.data(), &Mstar2, &scale),
                   "lift");
@@ -656,6 +773,7 @@ static int run(int argc, char** argv) {
         gp.seed = 10;
         gp.alpha = alpha;
         gp.warm_width = (uint32_t)width;
+        gp.precision = env_or("ANQI_B200_PRECISION", "bf16") == "fp32" ? 0u : 1u;
         deg.resize(n);
         links.resize(n * Marg);
         anqi_build_stats gs{};
@@ -708,9 +826,16 @@ static int run(int argc, char** argv) {
     desc.scale = scale;
     desc.mstar2 = Mstar2;
     dev().check(anqi_index_load(dev().get(), &desc), "index load");
-    dev().check(anqi_verifier_load(dev().get(), lrq.coeff.data(), lrq.codes.data(), n, lrq.nk, lrq.rankm, lrq.mu.data(),
-                                 lrq.basis.data(), lrq.codebook.data(), lrq.code_size),
-              "verifier load");
+    if (vmode == VMode::Compact)
+        dev().check(anqi_verifier_load_bits(dev().get(), lrq.coeff.data(), lrq.codes.empty() ? nullptr : lrq.codes.data(),
+                                            lrq.residual.empty() ? nullptr : lrq.residual.data(), n, lrq.nk, lrq.rankm,
+                                            lrq.bits, lrq.mu.data(), lrq.basis.data(),
+                                            lrq.codebook.empty() ? nullptr : lrq.codebook.data(), lrq.code_size, 0),
+                    "verifier load");
+    else if (vmode == VMode::Analytic)
+        dev().check(anqi_verifier_load_analytic(dev().get(), model.coeff.data(), n, (uint32_t)RANKM, model.train_kmax,
+                                                model.fit_kmin, model.flags, model.b0),
+                    "verifier load");
     const double build_s = since(tb0);
     auto external_seconds = [](const char* name) {
         const char* raw = std::getenv(name);
@@ -725,8 +850,8 @@ static int run(int argc, char** argv) {
     const double aknn_build_s = external_seconds("ANQI_AKNN_BUILD_SECONDS");
     const double verifier_train_s = external_seconds("ANQI_VERIFIER_TRAIN_SECONDS");
     const double end_to_end_s = aknn_build_s + verifier_train_s + build_s;
-    const double verification_gb = lrq.persistent_bytes() / 1e9;
-    const double idx_gb = ((double)n * Marg * 4 + (double)n * dim * 4 + (double)lrq.persistent_bytes()) / 1e9;
+    const double verification_gb = verification_bytes() / 1e9;
+    const double idx_gb = ((double)n * Marg * 4 + (double)n * dim * 4 + (double)verification_bytes()) / 1e9;
     if (can_load) {
         printf("[rknn] INDEX_LOAD_TIME=%.1fs INDEX_SIZE=%.2fGB (graph M=%" PRIu64 " + graph dim=%" PRIu64
                " + verification=%.3fGB + envelope=%.3fGB)\n",
@@ -747,11 +872,18 @@ static int run(int argc, char** argv) {
                    end_to_end_s, verifier_encode_save_ms);
     }
     const auto t_mat = Clock::now();
-    dev().check(anqi_verifier_materialize(dev().get(), (uint32_t)Kq, slack_factor), "verifier materialize");
+    if (vmode == VMode::Exact) {
+        // exact_f32: the rank-Kq column of the source thresholds (load_threshold_column)
+        const std::vector<float> col = load_threshold_column(PFX, n, Kq);
+        dev().check(anqi_set_thresholds(dev().get(), (uint32_t)Kq, col.data()), "verifier thresholds");
+    } else {
+        dev().check(anqi_verifier_materialize(dev().get(), (uint32_t)Kq, slack_factor), "verifier materialize");
+    }
     const double materialize_ms = since(t_mat) * 1e3;
-    printf("[rknn] independent verifier ready: mode=rank-M+LRQ k=%" PRIu64 " slack=%.6g persistent=%.3fGB "
+    printf("[rknn] independent verifier ready: mode=%s k=%" PRIu64 " slack=%.6g persistent=%.3fGB "
            "temporary_thresholds=%.3fGB materialize_ms=%.3f bits=%d\n",
-           Kq, rankm_slack, verification_gb, n * 4 / 1e9, materialize_ms, bits);
+           vmode_label.c_str(), Kq, rankm_slack, verification_gb, n * 4 / 1e9, materialize_ms,
+           vmode == VMode::Compact ? bits : 0);
     const float beta = std::getenv("ANQI_BETA") ? (float)std::atof(std::getenv("ANQI_BETA")) : 0.5f;
     printf("[rknn] k-adaptive flood: Kq=%" PRIu64 " radj=off beta=%.2f\n", Kq, beta);
     printf("[rknn] candidate generator: AKNN-k%" PRIu64 " envelope, center graph search; verifier is post-filter only\n",

@@ -502,7 +502,8 @@ __global__ void __launch_bounds__(128) join_apply_kernel(const float* __restrict
                                                          const uint64_t* __restrict__ off, uint64_t* __restrict__ inc,
                                                          uint32_t* __restrict__ hid, float* __restrict__ hval, uint32_t K,
                                                          uint64_t* __restrict__ sort_scratch, uint32_t scratch_cap,
-                                                         unsigned long long* __restrict__ upd, uint32_t* err) {
+                                                         unsigned long long* __restrict__ upd, uint32_t* err,
+                                                         const uint32_t* __restrict__ mask) {
     extern __shared__ __align__(16) unsigned char sm[];
     constexpr uint32_t kIncSmem = 512;
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
@@ -561,6 +562,15 @@ __global__ void __launch_bounds__(128) join_apply_kernel(const float* __restrict
             const uint32_t cu = scnt[u];
             // candidates: the other sampled ids of u, in sample order
             if (m + cu > kBatch + 1) flush();
+            if (mask) {
+                // precision form (S <= 32): only the candidates the tensor-core
+                // filter kept; the others would be rejected by the push
+                const uint32_t mk = mask[u * S + a] & (cu >= 32 ? kAll : ((1u << cu) - 1u));
+                if ((mk >> lane) & 1u) bi[m + __popc(mk & lane_lt_mask())] = samp[u * S + lane];
+                __syncwarp();
+                m += __popc(mk);
+                continue;
+            }
             for (uint32_t b = lane; b < cu; b += 32) {
                 if (b == a) continue;
                 const uint32_t pos = m + (b < a ? b : b - 1);
@@ -1017,15 +1027,30 @@ static GatherParams base_params(const DevBuf& dx, const DevBuf& dn, uint64_t n, 
 }
 
 // LocalJoin rounds on device heaps; returns rounds done and update counts.
+// precision 1: the round's distances filtered on BF16 tensor-core tiles first
+// (tc_join_filter), only the kept pairs recomputed in FP32 and pushed; the
+// heaps equal the FP32 form's.  Needs S <= 32; falls back to FP32 otherwise.
 static int run_localjoin(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
                          DevBuf& hid, DevBuf& hval, uint32_t K, uint32_t S, uint32_t max_rounds,
-                         std::vector<uint64_t>& updates) {
+                         std::vector<uint64_t>& updates, uint32_t precision = 0) {
     if (S > 120) S = 120;  // index.h:1470
-    TmpBuf samp(c), scnt(c), incnt(c), off(c), fill(c), inc(c), scratch(c), upd(c);
+    TmpBuf samp(c), scnt(c), incnt(c), off(c), fill(c), inc(c), scratch(c), upd(c), mask(c);
     int rc;
     if ((rc = ensure(c, samp, n * S * 4)) || (rc = ensure(c, scnt, n * 4)) || (rc = ensure(c, incnt, n * 4)) ||
         (rc = ensure(c, off, (n + 1) * 8)) || (rc = ensure(c, fill, n * 4)) || (rc = ensure(c, upd, 8)))
         return rc;
+    const bool tensor = precision == 1 && S <= 32 && dim <= 256;
+    TcPrep tp;
+    if (tensor && ((rc = tc_prep(c, dx.as<float>(), dn.as<float>(), n, stride, dim, tp)) ||
+                   (rc = ensure(c, mask, n * S * 4)))) {
+        tc_release(c, tp);
+        return rc;
+    }
+    struct Release {
+        Ctx* c;
+        TcPrep& tp;
+        ~Release() { tc_release(c, tp); }
+    } release_tp{c, tp};
     const int blocks = c->sm_count * 8;
     for (uint32_t it = 0; it < max_rounds; it++) {
         ANQI_CUDA(c, cudaMemsetAsync(incnt.p, 0, n * 4, c->stream));
@@ -1034,6 +1059,9 @@ static int run_localjoin(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n,
         join_sample_kernel<<<blocks, 256, 0, c->stream>>>(hid.as<uint32_t>(), n, K, S, samp.as<uint32_t>(),
                                                          scnt.as<uint32_t>(), incnt.as<uint32_t>());
         ANQI_CUDA(c, cudaGetLastError());
+        if (tensor && (rc = tc_join_filter(c, tp, dn.as<float>(), n, samp.as<uint32_t>(), scnt.as<uint32_t>(), S,
+                                           hval.as<float>(), K, mask.as<uint32_t>())))
+            return rc;
         if ((rc = device_scan(c, incnt.as<uint32_t>(), off.as<uint64_t>(), n))) return rc;
         std::vector<uint64_t> hoff(n + 1);
         ANQI_CUDA(c, cudaMemcpy(hoff.data(), off.p, (n + 1) * 8, cudaMemcpyDeviceToHost));
@@ -1055,7 +1083,8 @@ static int run_localjoin(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n,
                                                              samp.as<uint32_t>(), scnt.as<uint32_t>(), S,
                                                              off.as<uint64_t>(), inc.as<uint64_t>(), hid.as<uint32_t>(),
                                                              hval.as<float>(), K, scratch.as<uint64_t>(), scratch_cap,
-                                                             upd.as<unsigned long long>(), c->err.as<uint32_t>());
+                                                             upd.as<unsigned long long>(), c->err.as<uint32_t>(),
+                                                             tensor ? mask.as<uint32_t>() : nullptr);
         ANQI_CUDA(c, cudaGetLastError());
         if ((rc = check_device_error(c, "localjoin"))) return rc;
         uint64_t u = 0;
@@ -1182,7 +1211,14 @@ int anqi_graph_warm_start(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim,
 
 int anqi_graph_localjoin(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, uint32_t K, uint32_t sample,
                          uint32_t max_rounds, uint32_t* ids, float* vals, uint64_t* updates, uint32_t* rounds_done) {
-    if (!h || !x || !ids || !vals || n == 0 || dim == 0 || K == 0) return ANQI_ERR_ARGS;
+    return anqi_graph_localjoin_precision(h, x, n, dim, K, sample, max_rounds, 0, ids, vals, updates, rounds_done,
+                                          nullptr);
+}
+
+int anqi_graph_localjoin_precision(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, uint32_t K, uint32_t sample,
+                                   uint32_t max_rounds, uint32_t precision, uint32_t* ids, float* vals,
+                                   uint64_t* updates, uint32_t* rounds_done, float* join_ms) {
+    if (!h || !x || !ids || !vals || n == 0 || dim == 0 || K == 0 || precision > 1) return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     const uint32_t xs = round_up(dim, 8);
@@ -1192,7 +1228,13 @@ int anqi_graph_localjoin(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, 
         (rc = h2d(c, hv, vals, n * K * 4)))
         return rc;
     std::vector<uint64_t> up;
-    if ((rc = run_localjoin(c, dx, dn, n, xs, dim, hid, hv, K, sample, max_rounds, up))) return rc;
+    ANQI_CUDA(c, cudaEventRecord(c->ev2, c->stream));
+    if ((rc = run_localjoin(c, dx, dn, n, xs, dim, hid, hv, K, sample, max_rounds, up, precision))) return rc;
+    ANQI_CUDA(c, cudaEventRecord(c->ev3, c->stream));
+    if (join_ms) {
+        ANQI_CUDA(c, cudaEventSynchronize(c->ev3));
+        ANQI_CUDA(c, cudaEventElapsedTime(join_ms, c->ev2, c->ev3));
+    }
     if (updates)
         for (size_t i = 0; i < up.size(); i++) updates[i] = up[i];
     if (rounds_done) *rounds_done = (uint32_t)up.size();
@@ -1302,7 +1344,7 @@ int anqi_graph_build(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, cons
     t = Clock::now();
     std::vector<uint64_t> up;
     if ((rc = run_localjoin(c, dx, dn, n, xs, dim, hid, hv, gp->nn_k, gp->join_sample ? gp->join_sample : 20,
-                            gp->join_iters, up)))
+                            gp->join_iters, up, gp->precision)))
         return rc;
     const double join_ms = ms_since(t);
     t = Clock::now();

@@ -322,6 +322,12 @@ extern "C" {
 
 int anqi_version(void) { return 1; }
 
+int anqi_inject_fault(anqi_ctx* h, uint32_t flags) {
+    if (!h || (flags & ~ANQI_FAULT_DROP_ROW_COPIES)) return ANQI_ERR_ARGS;
+    h->c.inject = flags;
+    return ANQI_OK;
+}
+
 int anqi_ctx_create(int device, anqi_ctx** out) {
     if (!out) return ANQI_ERR_ARGS;
     *out = nullptr;

@@ -52,7 +52,13 @@ struct Verifier {
     bool loaded = false;
     uint64_t n = 0;
     uint32_t nk = 0, rankm = 0, code_size = 0;
-    DevBuf coeff, codes_t /* nk x n, k-major */, mu, basis, codebook;
+    uint32_t bits = 8;         // 0 (rank-M only), 2, 4, 8, 16 (codes), 32 (float residuals)
+    bool signed_keys = false;  // IP: thresholds are not clamped at zero
+    // analytic Rank-M model (coeff only): power-law basis in k
+    bool analytic = false;
+    uint32_t train_kmax = 0, flags = 0;
+    double b0 = 0;
+    DevBuf coeff, codes_t /* nk x n4, k-major: u8 / u16 codes or f32 residuals */, mu, basis, codebook;
 };
 
 struct Batch {
@@ -76,6 +82,7 @@ struct Batch {
 struct Ctx {
     int device = 0;
     int sm_count = 0;
+    uint32_t inject = 0;  // ANQI_FAULT_* flags (anqi_inject_fault)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
     cudaEvent_t tev0 = nullptr, tev1 = nullptr;  // anqi_timer_*
@@ -102,6 +109,7 @@ struct Ctx {
     // configuration of the last anqi_query_run and the captured graph of it
     uint32_t last_cfg_hash = 0, last_cfg_gcap = 0, last_cfg_blocks = 0;
     size_t last_cfg_smem = 0;
+    uint32_t last_cfg_wpb = 4, last_cfg_post = 8;  // block shape and candidate tile
     cudaGraphExec_t qgraph = nullptr;
     DevBuf init_cnt, init_cid, init_key;  // tensor-core init_knn candidate buffers
     DevBuf g_bits, g_vlog, g_pd, g_pi, g_gtab;  // gather kernel per-slot scratch
@@ -185,6 +193,11 @@ struct TcPrep {
 };
 int tc_prep(Ctx* c, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs, uint32_t d, TcPrep& tp);
 void tc_release(Ctx* c, TcPrep& tp);
+// LocalJoin precision form: for each source u's samples (samp, scnt; S <= 32)
+// the tensor-core Gram tile keeps, per target sample a, the candidates b whose
+// key may reach the target's heap top (hval[t * K]); mask[u * S + a] bit b.
+int tc_join_filter(Ctx* c, const TcPrep& tp, const float* d_norms, uint64_t n, const uint32_t* samp,
+                   const uint32_t* scnt, uint32_t S, const float* hval, uint32_t K, uint32_t* mask);
 // init_knn candidates of a batch of one tree's leaves on the tensor cores:
 // for every member row, the leaf-mates j != row whose key may be <= the
 // row's current K-th list key (any while the list is short), appended to

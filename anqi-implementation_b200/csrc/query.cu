@@ -80,6 +80,8 @@ struct SearchParams {
     uint32_t* gtab;       // per-slot global visited tables (gcap entries each, all ANQI_EMPTY between queries)
     uint32_t gcap;        // entries per slot (power of two, 0 = none)
     uint32_t gshift;      // 32 - log2(gcap)
+    uint32_t drop_row_copies;  // test fault: issue no row copies, so the bounded row waits run out
+    uint32_t post_rows;        // candidate tile: base rows per postfilter round (<= stage_rows)
 };
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
@@ -124,7 +126,7 @@ __device__ __forceinline__ void bar_expect(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
-constexpr uint32_t kRowWaitPolls = 1u << 24;
+constexpr uint32_t kRowWaitPolls = 1u << 22;
 
 // Objects are numbered in breadth-first order of the graph (anqi_index_load),
 // so a query's visits fall mostly near its entry object: the window bitmap of
@@ -153,8 +155,10 @@ __device__ __forceinline__ uint32_t expand_links(const SearchParams& p, uint32_t
     const uint32_t ls = search_lstride<kDim>(p), rb = ls * 4;
     if (m) {
         if (lane == 0) bar_expect(bar, min(m, srows) * rb);
-        if (f0 && p0 < srows) bulk_row(stage + (size_t)p0 * ls, p.lifted + (size_t)l0 * ls, rb, bar);
-        if (f1 && p1 < srows) bulk_row(stage + (size_t)p1 * ls, p.lifted + (size_t)l1 * ls, rb, bar);
+        if (!p.drop_row_copies) {
+            if (f0 && p0 < srows) bulk_row(stage + (size_t)p0 * ls, p.lifted + (size_t)l0 * ls, rb, bar);
+            if (f1 && p1 < srows) bulk_row(stage + (size_t)p1 * ls, p.lifted + (size_t)l1 * ls, rb, bar);
+        }
     }
     if (f0) ni[p0] = l0;
     if (f1) ni[p1] = l1;
@@ -279,8 +283,10 @@ __device__ __host__ __forceinline__ size_t search_smem_words(uint32_t L_max, uin
            stage_rows_for(lstride, bstride) * (size_t)(lstride > bstride ? lstride : bstride) + hash_cap + 8;
 }
 
-template <uint32_t kDim>
-__global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
+// kWpb warps per block (one query each): 2, 4 or 8, the block shape the
+// autotuner picks; 32 warps per SM at 64 registers in every shape.
+template <uint32_t kDim, uint32_t kWpb>
+__global__ void __launch_bounds__(32 * kWpb, 32 / kWpb) rknn_search_kernel(SearchParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
     const uint32_t ls = search_lstride<kDim>(p);
@@ -506,11 +512,12 @@ __global__ void __launch_bounds__(128, 8) rknn_search_kernel(SearchParams p) {
         const float qn = group_ip(q, q, p.d, gt, kFull);
         const float* thr = p.thr + (size_t)tslot * p.n;
         uint32_t npred = 0;
-        // base rows in rounds of srows, G = 32 / srows threads per row
-        const uint32_t G = srows == 8 ? 4u : (srows == 4 ? 8u : 16u);
-        const uint32_t pg = srows == 8 ? lane >> 2 : (srows == 4 ? lane >> 3 : lane >> 4), pt = lane & (G - 1);
+        // base rows in rounds of prow (the candidate tile), G = 32 / prow threads per row
+        const uint32_t prow = min(p.post_rows, srows);
+        const uint32_t G = prow == 8 ? 4u : (prow == 4 ? 8u : 16u);
+        const uint32_t pg = prow == 8 ? lane >> 2 : (prow == 4 ? lane >> 3 : lane >> 4), pt = lane & (G - 1);
         float* brow = stage + (size_t)pg * max(ls, p.bstride);
-        for (uint32_t r0 = 0; r0 < ncand; r0 += srows) {
+        for (uint32_t r0 = 0; r0 < ncand; r0 += prow) {
             const uint32_t idx = r0 + pg;
             const bool ok = idx < ncand;
             const uint32_t o = cl[ok ? idx : r0];
@@ -807,27 +814,40 @@ static size_t search_smem_per_warp(const Ctx* c, uint32_t L_max, uint32_t hash_c
     return search_smem_words(L_max, c->ix.lstride, c->ix.bstride, hash_cap) * 4;
 }
 
-// The search kernel for lifted dimension dim: 130 (d = 128) has its distance
-// loops unrolled at compile time.
-static void (*search_kernel_for(uint32_t dim))(SearchParams) {
-    return dim == kColsDim ? rknn_search_kernel<kColsDim> : rknn_search_kernel<0>;
+using SearchKernel = void (*)(SearchParams);
+
+// The search kernel for lifted dimension dim (130, d = 128, has its distance
+// loops unrolled at compile time) and block shape wpb.
+template <uint32_t kDim>
+static SearchKernel search_kernel_wpb(uint32_t wpb) {
+    return wpb == 2 ? rknn_search_kernel<kDim, 2> : (wpb == 8 ? rknn_search_kernel<kDim, 8> : rknn_search_kernel<kDim, 4>);
+}
+static SearchKernel search_kernel_for(uint32_t dim, uint32_t wpb) {
+    return dim == kColsDim ? search_kernel_wpb<kColsDim>(wpb) : search_kernel_wpb<0>(wpb);
 }
 
+// One launch configuration of the search: the visited-set sizes, the block
+// shape (warps per block) and the postfilter's candidate tile (base rows per
+// round).  The autotuner times the candidates per batch shape.
 struct SearchCfg {
     uint32_t hash_cap = 0;  // shared-memory table entries per warp
     uint32_t gcap = 0;      // global (L2-resident) table entries per warp
+    uint32_t wpb = 4;       // warps per block
+    uint32_t post_rows = 8; // candidate tile
     uint32_t blocks = 0;
     size_t smem = 0;
+    uint64_t code() const { return hash_cap | (uint64_t)gcap << 24 | (uint64_t)wpb << 48 | (uint64_t)post_rows << 56; }
 };
 
-static int search_cfg(Ctx* c, uint32_t hash_cap, uint32_t gcap, SearchCfg& cfg) {
+static int search_cfg(Ctx* c, uint32_t hash_cap, uint32_t gcap, uint32_t wpb, uint32_t post_rows, SearchCfg& cfg) {
     const Batch& b = c->batch;
-    const int wpb = 4;
     cfg.hash_cap = hash_cap;
     cfg.gcap = gcap;
+    cfg.wpb = wpb;
+    cfg.post_rows = std::min(post_rows, stage_rows_for(c->ix.lstride, c->ix.bstride));
     cfg.smem = search_smem_per_warp(c, b.L_max, hash_cap) * wpb;
     if (cfg.smem > 227 * 1024) return ANQI_ERR_ARGS;
-    auto kern = search_kernel_for(c->ix.dim);
+    auto kern = search_kernel_for(c->ix.dim, wpb);
     ANQI_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
     int per_sm = 0;
     ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, cfg.smem));
@@ -1176,13 +1196,15 @@ static int enqueue_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, boo
     p.gcap = cfg.gcap;
     p.gshift = cfg.gcap ? 32u - (uint32_t)__builtin_ctz(cfg.gcap) : 0u;
     p.gtab = cfg.gcap ? c->vis_gtab.as<uint32_t>() : nullptr;
-    auto kern = search_kernel_for(ix.dim);
+    p.drop_row_copies = (c->inject & ANQI_FAULT_DROP_ROW_COPIES) ? 1u : 0u;
+    p.post_rows = cfg.post_rows;
+    auto kern = search_kernel_for(ix.dim, cfg.wpb);
     ANQI_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cfg.smem));
     // in a captured graph the events become event-record nodes (so the replay
     // is timed like a plain launch)
     const unsigned ef = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     ANQI_CUDA(c, cudaEventRecordWithFlags(c->ev0, c->stream, ef));
-    kern<<<cfg.blocks, 128, cfg.smem, c->stream>>>(p);
+    kern<<<cfg.blocks, 32 * cfg.wpb, cfg.smem, c->stream>>>(p);
     ANQI_CUDA(c, cudaGetLastError());
     ANQI_CUDA(c, cudaEventRecordWithFlags(c->ev1, c->stream, ef));
     return ANQI_OK;
@@ -1253,19 +1275,33 @@ static int query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st, boo
     }
     static const uint32_t kCandidates[][2] = {{0, 0},       {1024, 0},    {2048, 0},   {4096, 0}, {0, 2048},
                                                   {0, 4096},    {512, 4096},  {1024, 4096}};
+    // block shapes (warps per block) and candidate tiles; ANQI_B200_SHAPE="W"
+    // or "W,T" forces one
+    const char* fshape = std::getenv("ANQI_B200_SHAPE");
+    uint32_t f_w = 0, f_t = 0;
+    if (fshape) {
+        char* end = nullptr;
+        f_w = (uint32_t)std::strtoul(fshape, &end, 10);
+        if (end && *end == ',') f_t = (uint32_t)std::strtoul(end + 1, nullptr, 10);
+    }
+    static const uint32_t kShapes[][2] = {{4, 8}, {2, 8}, {8, 8}, {4, 4}, {2, 4}, {8, 4}};
+    // cfgs: every (visited set, shape) candidate; the first shape is the default
     std::vector<SearchCfg> cfgs;
-    for (const auto& cand : kCandidates) {
-        if (forced && (cand[0] != f_hc || cand[1] != f_gc)) continue;
-        if (!forced && cand[0] == 4096) continue;  // measured slower everywhere (occupancy); kept forcible
-        if (cand[1] && (uint64_t)cand[1] / 8 * 5 > std::min<uint64_t>(ix.n, 16384)) continue;  // log must cover it
-        SearchCfg g;
-        if (search_cfg(c, cand[0], cand[1], g) == ANQI_OK) cfgs.push_back(g);
+    for (const auto& shape : kShapes) {
+        if (fshape && (shape[0] != f_w || (f_t && shape[1] != f_t))) continue;
+        for (const auto& cand : kCandidates) {
+            if (forced && (cand[0] != f_hc || cand[1] != f_gc)) continue;
+            if (!forced && cand[0] == 4096) continue;  // measured slower everywhere (occupancy); kept forcible
+            if (cand[1] && (uint64_t)cand[1] / 8 * 5 > std::min<uint64_t>(ix.n, 16384)) continue;  // log must cover it
+            SearchCfg g;
+            if (search_cfg(c, cand[0], cand[1], shape[0], shape[1], g) == ANQI_OK) cfgs.push_back(g);
+        }
     }
     if (cfgs.empty()) return fail(c, ANQI_ERR_ARGS, "beam width %u needs too much shared memory", b.L_max);
     uint32_t slots = 0, gslots = 0, gcap_max = 0;
     for (const SearchCfg& g : cfgs) {
-        slots = std::max(slots, g.blocks * 4);
-        if (g.gcap) gslots = std::max(gslots, g.blocks * 4);
+        slots = std::max(slots, g.blocks * g.wpb);
+        if (g.gcap) gslots = std::max(gslots, g.blocks * g.wpb);
         gcap_max = std::max(gcap_max, g.gcap);
     }
     // per-slot L2-resident tables, ANQI_EMPTY between queries
@@ -1306,24 +1342,34 @@ static int query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st, boo
     auto it = c->tuned.find(key);
     if (it != c->tuned.end()) {
         for (const SearchCfg& g : cfgs)
-            if ((g.hash_cap | (uint64_t)g.gcap << 32) == it->second) best = g;
+            if (g.code() == it->second) best = g;
     } else if (cfgs.size() > 1) {
+        // coordinate descent: the visited sets at the first shape, then every
+        // shape with the fastest visited set
         float best_ms = 1e30f;
-        for (const SearchCfg& g : cfgs) {
+        auto time_cfg = [&](const SearchCfg& g) -> int {
             float ms = 0;
             unsigned long long fill[2];
-            rc = launch_search(c, g, 0, &ms, fill);
-            if (rc == ANQI_ERR_CAPACITY) {
+            int r = launch_search(c, g, 0, &ms, fill);
+            if (r == ANQI_ERR_CAPACITY) {
                 b.pred_cap = std::max<uint64_t>(b.pred_cap, fill[0] + 1024);
-                rc = launch_search(c, g, 0, &ms, fill);
+                r = launch_search(c, g, 0, &ms, fill);
             }
-            if (rc) return rc;
+            if (r) return r;
             if (ms < best_ms) {
                 best_ms = ms;
                 best = g;
             }
-        }
-        c->tuned[key] = best.hash_cap | (uint64_t)best.gcap << 32;
+            return ANQI_OK;
+        };
+        for (const SearchCfg& g : cfgs)
+            if (g.wpb == cfgs[0].wpb && g.post_rows == cfgs[0].post_rows && (rc = time_cfg(g))) return rc;
+        const SearchCfg vis = best;
+        for (const SearchCfg& g : cfgs)
+            if (g.hash_cap == vis.hash_cap && g.gcap == vis.gcap &&
+                (g.wpb != cfgs[0].wpb || g.post_rows != cfgs[0].post_rows) && (rc = time_cfg(g)))
+                return rc;
+        c->tuned[key] = best.code();
     }
     for (int attempt = 0; attempt < 3; attempt++) {
         float ms = 0;
@@ -1344,12 +1390,16 @@ static int query_run(anqi_ctx* h, int keep_candidates, anqi_query_stats* st, boo
         c->last_cfg_gcap = best.gcap;
         c->last_cfg_blocks = best.blocks;
         c->last_cfg_smem = best.smem;
+        c->last_cfg_wpb = best.wpb;
+        c->last_cfg_post = best.post_rows;
         b.have_results = true;
         b.have_cands = keep_candidates != 0;
         if (st) {
             st->search_ms = ms;
             st->visited_table = best.hash_cap;
             st->visited_l2_table = best.gcap;
+            st->warps_per_block = best.wpb;
+            st->candidate_tile = best.post_rows;
         }
         return sync_after ? sync(c) : ANQI_OK;
     }
@@ -1370,6 +1420,7 @@ static std::vector<uint64_t> query_graph_key(Ctx* c, int keep_candidates) {
     auto u = [](const void* q) { return (uint64_t)(uintptr_t)q; };
     return {b.nq, b.L_max, (uint64_t)b.has_k, (uint64_t)b.has_L, b.k_all, b.L_all, (uint64_t)keep_candidates,
             (uint64_t)b.ordered, c->last_cfg_hash, c->last_cfg_gcap, c->last_cfg_blocks, c->last_cfg_smem,
+            c->last_cfg_wpb, c->last_cfg_post,
             b.pred_cap, b.cand_cap, u(b.q.p), u(b.qslot.p), u(b.qL.p), u(b.pred_buf.p), u(b.cand_buf.p),
             u(b.pred_csr.p), u(b.cand_csr.p), u(b.pred_off.p), u(b.cand_off.p), u(b.entry.p), u(b.enode.p),
             u(b.order.p), u(b.leaf_cnt.p), u(b.npred.p), u(b.ncand.p), u(b.ndist.p), u(b.nexp.p), u(b.nflood.p),
@@ -1426,6 +1477,8 @@ int anqi_query_run_graph(anqi_ctx* h, int keep_candidates, anqi_query_stats* st)
                 st->search_ms = ms;
                 st->visited_table = c->last_cfg_hash;
                 st->visited_l2_table = c->last_cfg_gcap;
+                st->warps_per_block = c->last_cfg_wpb;
+                st->candidate_tile = c->last_cfg_post;
             }
             return ANQI_OK;
         }
@@ -1440,6 +1493,8 @@ int anqi_query_run_graph(anqi_ctx* h, int keep_candidates, anqi_query_stats* st)
     cfg.gcap = c->last_cfg_gcap;
     cfg.blocks = c->last_cfg_blocks;
     cfg.smem = c->last_cfg_smem;
+    cfg.wpb = c->last_cfg_wpb;
+    cfg.post_rows = c->last_cfg_post;
     bool ordered = false;
     cudaGraph_t g = nullptr;
     ANQI_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));

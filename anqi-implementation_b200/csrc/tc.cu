@@ -661,6 +661,141 @@ void tc_release(Ctx* c, TcPrep& tp) {
     release(c, tp.xint);
 }
 
+// ------------------------------------------------------ LocalJoin filter
+// Precision form of one LocalJoin round's distances (index.h:1468-1487, in
+// the snapshot form of build.cu's join_apply_kernel).  Every pair the round
+// pushes is (target, candidate) = (sample a, sample b) of one source u, so
+// the Gram matrix of u's samples holds all of them.  A CTA of 4 warps takes 4
+// sources: warp w's 32 TMEM lanes (tile rows 32 w .. 32 w + 31) hold the
+// samples of source 4 x + w, and one 128 x 128 BF16 tile of the gathered rows
+// with themselves on the tensor cores gives each source's pairs in its
+// diagonal 32 x 32 block (thread = target row, one tcgen05.ld of the block).
+// A pair stays when key~ - eps <= the target's heap top at the start of the
+// round (eps as in the filter kernel: bf16 rounding of both rows, FP32
+// accumulation, the key's roundings).  A pair above it is rejected by the
+// heap push whatever is pushed before it, since a heap's top only falls
+// during a round; so pushing only the kept pairs, each with its FP32 key,
+// leaves the heaps bit-identical to the FP32 form.
+// mask[u * S + a] bit b: candidate b of target a of source u stays.
+struct JoinFilterParams {
+    const __nv_bfloat16* xb;
+    const float* xn;     // reference FP32 norms
+    const float* xnorm;  // |x| rounded up
+    const float* xerr;   // |x - bf16(x)| rounded up
+    uint64_t n;
+    uint32_t dp, S, K;
+    const uint32_t* samp;
+    const uint32_t* scnt;
+    const float* hval;   // heaps, top first
+    uint32_t* mask;
+    uint32_t* err;
+};
+
+namespace {
+
+__global__ void __launch_bounds__(128) join_filter_kernel(JoinFilterParams p) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    __shared__ uint32_t rowid[kTile];
+    __shared__ float cn[kTile], cnm[kTile], cer[kTile];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t tslot;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, r = threadIdx.x;
+    const uint64_t u = (uint64_t)blockIdx.x * 4 + warp;
+    const uint32_t su = u < p.n ? min(p.scnt[u], min(p.S, 32u)) : 0u;
+    {
+        const bool ok = lane < su;
+        const uint32_t id = ok ? p.samp[u * p.S + lane] : kEmpty;
+        const bool okid = ok && id < p.n;
+        rowid[r] = okid ? id : kEmpty;
+        cn[r] = okid ? p.xn[id] : 0.f;
+        cnm[r] = okid ? p.xnorm[id] : 0.f;
+        cer[r] = okid ? p.xerr[id] : 0.f;
+    }
+    if (warp == 0) tc::tmem_alloc(&tslot, kTile);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::fence_mbar_init();
+    }
+    __syncthreads();
+    const uint32_t chunks = p.dp / 8;
+    for (uint32_t t = threadIdx.x; t < kTile * chunks; t += blockDim.x) {
+        const uint32_t rr = t % kTile, c = t / kTile;
+        const uint32_t id = rowid[rr];
+        const bool ok = id != kEmpty;
+        tc::cp_async16_zfill(sm + (size_t)c * kTile * 16 + rr * 16, p.xb + (uint64_t)(ok ? id : 0u) * p.dp + 8 * c,
+                             ok ? 16u : 0u);
+    }
+    cp_async_wait_all_();
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tslot;
+    if (threadIdx.x == 0) {
+        issue_tile_mma(tmem, sm, sm, p.dp);  // the tile against itself: A = B
+        tc::mma_commit(&bar);
+    }
+    const bool ok = tc::mbar_wait(&bar, 0, kWaitPolls);
+    if (!ok && lane == 0) atomicExch(p.err, 8u);
+    tc::fence_after_sync();
+    if (ok) {
+        float v[32];
+        tc::tmem_ld32(tmem + ((warp * 32u) << 16) + warp * 32u, v);
+        if (lane < su && rowid[r] != kEmpty) {
+            const uint32_t t = rowid[r];
+            const float top = p.hval[(uint64_t)t * p.K];
+            const float qn = cn[r], qnm = cnm[r], qer = cer[r];
+            const float uu = 5.9604645e-8f;  // 2^-24
+            const float g = 2.0f * p.dp * uu;
+            const float ca = 2.f * qer + 4.f * g * (qnm + qer) + 4.f * g * qnm + 8.f * uu * qnm;
+            const float cb = 2.f * qnm + 2.f * qer + 4.f * g * (qnm + qer);
+            const float cc = 4.f * uu;
+            const float cd = 4.f * uu * qn;
+            uint32_t keep = 0;
+#pragma unroll
+            for (uint32_t b = 0; b < 32; b++) {
+                const uint32_t j = warp * 32 + b;
+                const float approx = __fsub_rn(__fadd_rn(qn, cn[j]), __fmul_rn(2.0f, v[b]));
+                const float eps = fmaf(ca, cnm[j], fmaf(cb, cer[j], fmaf(cc, cn[j], cd)));
+                const bool stay = b < su && b != lane && rowid[j] != kEmpty && approx - eps <= top;
+                keep |= (stay ? 1u : 0u) << b;
+            }
+            p.mask[u * p.S + lane] = keep;
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_free(tmem, kTile);
+}
+
+}  // namespace
+
+int tc_join_filter(Ctx* c, const TcPrep& tp, const float* d_norms, uint64_t n, const uint32_t* samp,
+                   const uint32_t* scnt, uint32_t S, const float* hval, uint32_t K, uint32_t* mask) {
+    if (S > 32) return fail(c, ANQI_ERR_ARGS, "tensor-core LocalJoin needs at most 32 samples per row, got %u", S);
+    JoinFilterParams p;
+    p.xb = tp.bf.as<__nv_bfloat16>();
+    p.xn = d_norms;
+    p.xnorm = tp.nrm.as<float>();
+    p.xerr = tp.err.as<float>();
+    p.n = n;
+    p.dp = tp.dp;
+    p.S = S;
+    p.K = K;
+    p.samp = samp;
+    p.scnt = scnt;
+    p.hval = hval;
+    p.mask = mask;
+    p.err = c->err.as<uint32_t>();
+    const size_t smem = (size_t)kTile * tp.dp * 2;
+    ANQI_CUDA(c, cudaFuncSetAttribute(join_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const uint64_t blocks = (n + 3) / 4;
+    if (blocks > 0x7FFFFFFFull) return fail(c, ANQI_ERR_ARGS, "too many rows for the LocalJoin filter");
+    join_filter_kernel<<<(unsigned)blocks, 128, smem, c->stream>>>(p);
+    ANQI_CUDA(c, cudaGetLastError());
+    return ANQI_OK;
+}
+
 int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs,
                        uint32_t d, const uint32_t* d_members, const std::vector<LeafRef>& leaves,
                        const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,

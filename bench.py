@@ -18,9 +18,15 @@ call (query upload from pinned memory and result download into pinned
 buffers reused across calls, both inside the timed region).  The timed working set (lifted + base vectors, graph) is ~1.3 GB,
 larger than the 126 MB L2.
 
-``--impl reference`` times the reference's own CPU query code (its
-nndindex::range_search, postfilter and evaluation, built from its sources into
-oracle/_ref) on this host's cores, on the same index files and workload.
+Beside the timed steps: recall / precision / QPS over the reference's beam
+width list (``per_L``), and, in the CPU-baseline leg, the reference's query
+code on this index (timed on a bounded sample) and compared with the CUDA
+results query by query (``parity``).
+
+``--impl reference`` runs the reference's own pipeline on this host's cores
+(its build_aknn_source, its trainer's NumPy restatement, CPU ground truth,
+its rknn_query; oracle/reference_pipeline.py) on the same data, no GPU library
+in any of its processes, and times the same steps with rknn_query's own clock.
 Under torchrun every rank holds an index replica and runs its own batch
 (weak scaling); rank 0 prints the line.
 """
@@ -44,6 +50,16 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO / "anqi-implementation_b200"))
 
 METRIC = "RkNN queries/s (1M x 128, k in {10,50,100}, FP32 bit-exact path)"
+# the reference's own beam-width list (scripts/run_final.sh protocol)
+SWEEP_L = [20, 52, 85, 128, 256, 512, 1024]
+
+
+def bench_config(a, ks, world):
+    """The workload both arms measure (identical in both lines)."""
+    return {"workload": f"rknn_query {a.n}x{a.d}, {a.nq} queries x k{{{a.ks}}}, L={a.L}, "
+                        "G48 graph, M8/u8 LRQ postfilter", "n": a.n, "d": a.d, "nq": a.nq,
+            "queries_per_step": a.nq * len(ks), "ks": ks, "L": a.L, "parallelism": f"replicas x{world}",
+            "l2": "working set > L2 (lifted+base+graph ~1.3 GB)"}
 
 
 def log(*a):
@@ -175,6 +191,17 @@ def build_workload(ctx, a, rank, log):
     ix.timings["aknn_total_ms"] = {"bf16": round(st["total_ms"], 1), "fp32": round(st32["total_ms"], 1),
                                    "bf16_first_build": round(ix.timings["aknn_stats"]["total_ms"], 1)}
     ix.timings["aknn_gather_kernel_ms"] = round(st["gather_kernel_ms"], 1)
+    # the G48 build's LocalJoin in both forms from the same warm start: BF16
+    # tensor-core filter + FP32 recheck (the index's) and FP32 CUDA cores
+    wi, wv = pipeline.graph_warm_start(ctx, ix.lifted, ix.aknn_ids)
+    j16 = pipeline.graph_localjoin(ctx, ix.lifted, wi, wv, "bf16")
+    j32 = pipeline.graph_localjoin(ctx, ix.lifted, wi, wv, "fp32")
+    ix.timings["localjoin"] = {
+        "bf16_ms": round(j16[3], 1), "fp32_ms": round(j32[3], 1), "updates_per_round": j32[2],
+        "identical": bool(j16[2] == j32[2] and np.array_equal(j16[0], j32[0])
+                          and np.array_equal(j16[1].view(np.uint32), j32[1].view(np.uint32)))}
+    del wi, wv, j16, j32
+    log(f"LocalJoin {ix.timings['localjoin']}")
     log(f"AKNN fp32 build {ix.timings['aknn_build_fp32_s']:.2f}s identical={ix.timings['aknn_fp32_identical']}")
     ks = [int(k) for k in a.ks.split(",")]
     if a.no_gt or a.d > 256:
@@ -263,7 +290,8 @@ def run_batched(ctx, a, base, ix, rank):
     out = {"queries": nqb, "batch": bs, "k": "uniform {10,50,100}", "L": "uniform [64,600] (bound 600)",
            "qps": round(bs * len(lat) / (lat.sum() / 1e3), 1), "p50_ms": round(float(np.percentile(lat, 50)), 3),
            "p99_ms": round(float(np.percentile(lat, 99)), 3), "batches_timed": int(len(lat)), "cuda_graph": True,
-           "visited_table": [st["visited_table"], st["visited_l2_table"]]}
+           "visited_table": [st["visited_table"], st["visited_l2_table"]],
+           "shape": {"warps_per_block": st["warps_per_block"], "candidate_tile": st["candidate_tile"]}}
     ex_keys = getattr(ix, "exact_keys", None)
     if ex_keys is not None:
         # exact RkNN of each query at its own k (tensor path), recall / precision
@@ -285,6 +313,52 @@ def run_batched(ctx, a, base, ix, rank):
         out["recall"] = round(rec / max(ne, 1), 6)
         out["precision"] = round(prec / max(ne, 1), 6)
     return out
+
+
+class _Env:
+    """Sets environment variables for a block (the library reads its
+    switches at call time) and restores them after."""
+
+    def __init__(self, **kv):
+        self.kv = kv
+
+    def __enter__(self):
+        self.old = {k: os.environ.get(k) for k in self.kv}
+        os.environ.update(self.kv)
+
+    def __exit__(self, *exc):
+        for k, v in self.old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+def run_plain(a, dev, ix, query, ks, steps, warmup):
+    """The plain FP32 GPU path the batched form is compared with: the same
+    bit-exact search kernel on the given object numbering (no breadth-first
+    renumbering), work in query order (no leaf ordering), one plain launch per
+    k (no CUDA graph, no per-query k), fixed launch shape and visited set (no
+    autotuning).  Queries/s over `steps` passes of the three launches, each
+    timed on the device around the launch (entry, search, compaction)."""
+    from anqi import pipeline
+    from anqi._lib import Context
+    with _Env(ANQI_B200_RENUMBER="0", ANQI_B200_ORDER="0", ANQI_B200_HASH="0,4096", ANQI_B200_SHAPE="4,8"):
+        with Context(dev) as c2:
+            pipeline.load_index(c2, ix, ks)
+            ms = 0.0
+            for rep in range(warmup + steps):
+                for k in ks:
+                    c2.query_upload(query, k, a.L)
+                    c2.timer_start()
+                    c2.query_run()
+                    t = c2.timer_stop()
+                    if rep >= warmup:
+                        ms += t
+    nq = len(query)
+    return {"qps": round(steps * nq * len(ks) / (ms / 1e3), 1), "ms_per_pass": round(ms / steps, 4),
+            "launches_per_pass": len(ks), "renumbered": False, "leaf_ordered": False, "cuda_graph": False,
+            "visited_table": [0, 4096], "shape": {"warps_per_block": 4, "candidate_tile": 8}}
 
 
 def run_ours(a, rank, world, local):
@@ -321,6 +395,28 @@ def run_ours(a, rank, world, local):
             e = ctx.query_evaluate(off, ids)
             per_k[k] = {"recall": round(e["recall"], 6), "precision": round(e["precision"], 6),
                         "candidate_recall": round(e["candidate_recall"], 6)}
+    # ---- the reference's beam-width sweep, one launch of nq queries per (k, L):
+    # recall / precision and QPS with the device evaluation inside the timing,
+    # as the reference's query loop has it
+    per_L = []
+    if gt is not None:
+        for k in ks:
+            off, ids, _ = gt[k]
+            for L in SWEEP_L:
+                ctx.query_upload(query, k, L)
+                ctx.gt_load(off, ids)
+                ctx.query_run()
+                ctx.timer_start()
+                ctx.query_run()
+                s = ctx.query_evaluate_sums()
+                ms_L = ctx.timer_stop()
+                ne = max(1, s["nonempty"])
+                per_L.append({"k": k, "L": L, "recall": round(s["recall"] / ne, 6),
+                              "precision": round(s["precision"] / ne, 6), "qps": round(nq / (ms_L / 1e3), 1),
+                              "graph_dist": round(s["graph_dist"] / ne, 1)})
+    # per-query results at the bench's beam width, for the comparison with the
+    # reference's query code in the CPU-baseline leg
+    ours_k = {k: ctx.rknn_query(query, k, a.L, keep_candidates=True) for k in ks} if gt is not None else {}
     # ---- resident batch: warm-up, then K timed steps, each one replay of the
     # batch's captured CUDA graph (entry, leaf order, search, compaction)
     ctx.query_upload(qb, kb, Lb)
@@ -378,16 +474,24 @@ def run_ours(a, rank, world, local):
         except (ValueError, KeyError):
             traffic = None
     batched = run_batched(ctx, a, base, ix, rank) if a.batched_queries else None
+    # error of every distance form against FP64 on 20,000 random pairs: base
+    # rows against queries (the verifier / ground-truth key) and lifted rows
+    # against lifted rows (the graph build's LocalJoin key)
+    from anqi import precision as prec
+    fp64_error = {"base_query": prec.report(ctx, base, query),
+                  "lifted": prec.report(ctx, ix.lifted, ix.lifted, seed=5)}
+    # the plain FP32 GPU path on the same index and queries, for the batched form's speed-up
+    plain = run_plain(a, dev, ix, query, ks, max(3, min(a.steps, 10)), 2) if a.batched_queries else None
+    if batched is not None and plain is not None:
+        batched["plain_fp32"] = plain
+        batched["speedup_vs_plain"] = {"resident_step": round(value / world / plain["qps"], 3)}
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
         "data": ("synthetic (seeded 1,000-centre mixture, integers in [0,255])" if a.data == "mixture"
                  else "synthetic (seeded N(0,1), L2-normalised rows)"),
-        "config": {"workload": f"rknn_query {a.n}x{a.d}, {a.nq} queries x k{{{a.ks}}}, L={a.L}, "
-                               "G48 graph, M8/u8 LRQ postfilter", "n": a.n, "d": a.d, "nq": a.nq,
-                   "queries_per_step": nb, "ks": ks, "L": a.L, "parallelism": f"replicas x{world}",
-                   "l2": "working set > L2 (lifted+base+graph ~1.3 GB)"},
+        "config": bench_config(a, ks, world),
         "e2e": {"value": round(e2e_value, 1), "unit": "queries/s",
                 "h2d_bytes_per_step": int(e2e_stats[-1]["h2d_bytes"]),
                 "d2h_bytes_per_step": int(e2e_stats[-1]["d2h_bytes"])},
@@ -403,10 +507,13 @@ def run_ours(a, rank, world, local):
         "clocks": clocks,
         "recall": None if ev["recall"] is None else round(ev["recall"], 6),
         "precision": None if ev["precision"] is None else round(ev["precision"], 6), "per_k": per_k,
+        "per_L": per_L,
         "counters_per_query": {"graph_dist": round(s0["n_dist"] / nb, 1), "expansions": round(X / nb, 1),
                                "candidates": round(s0["n_cand"] / nb, 1), "verified": round(s0["n_pred"] / nb, 2)},
         "batched_form": batched,
         "build_s": {k: round(v, 3) for k, v in ix.timings.items() if isinstance(v, float)},
+        "localjoin": ix.timings["localjoin"],
+        "fp64_error": fp64_error,
         "aknn_build": {"bf16_tensor_init_s": round(ix.timings["aknn_build_warm_s"], 3),
                        "fp32_init_s": round(ix.timings["aknn_build_fp32_s"], 3),
                        "bf16_first_build_s": round(ix.timings["aknn_build_s"], 3),
@@ -435,6 +542,19 @@ def run_ours(a, rank, world, local):
                                             "sample": f"first {nqs} queries x k{{{a.ks}}}, L={a.L}, same index; "
                                                       "reference range_search + postfilter + evaluation",
                                             "per_k": res["per_k"]}
+            # query-by-query parity on this index: the reference's range_search
+            # + postfilter (one thread) with its entry descent's ties sent
+            # left, and with its own random tie side
+            if probe is not None:
+                sys.path.insert(0, str(REPO / "oracle"))
+                import harness_io as hio
+                par = {"L": a.L}
+                for mode in ("left", "tree"):
+                    t0 = time.perf_counter()
+                    ref = hio.run_qparity(tmp, a.L, mode, nq, ks)
+                    par[f"{mode}_entry"] = hio.compare(ref, ours_k, nq)
+                    log(f"parity ({mode} entry) {par[f'{mode}_entry']} in {time.perf_counter() - t0:.1f}s")
+                line["parity"] = par
         finally:
             if not a.keep:
                 shutil.rmtree(tmp, ignore_errors=True)
@@ -444,45 +564,77 @@ def run_ours(a, rank, world, local):
 
 
 def run_reference(a, rank, world, local):
+    """The reference's own pipeline on this host's CPU cores, no GPU library in
+    any of its processes (oracle/reference_pipeline.py): its build_aknn_source,
+    the NumPy trainer (byte-identical restatement of its trainer), exact ground
+    truth on the CPU, then its rknn_query.  rknn_query runs once per k over an
+    L list holding W + K copies of the bench's beam width (one step each) and
+    then the sweep; a step's time is the sum over k of nq / QPS, the reference's
+    own clock around its query loop (lift, range_search, postfilter,
+    evaluation)."""
     if rank != 0:
         return
-    from anqi._lib import Context
-    ctx = Context(local if world > 1 else 0)
-    base, query, ix, ks, gt = build_workload(ctx, a, rank, lambda *m: log("reference-arm", *m))
-    tmp = Path(a.keep) if a.keep else Path(tempfile.mkdtemp(prefix="anqi_ref_"))
+    sys.path.insert(0, str(REPO / "oracle"))
+    import reference_pipeline as rp
+    from anqi import formats, pipeline
+
+    def unavailable(why):
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+
+    why = rp.unavailable_reason()
+    if why:
+        return unavailable(why)
+    if a.data != "mixture":
+        return unavailable("the reference arm runs the integer mixture (its CPU ground truth needs small integers)")
     threads = os.cpu_count() or 1
+    ks = [int(k) for k in a.ks.split(",")]
+    tmp = Path(a.keep) if a.keep else Path(tempfile.mkdtemp(prefix="anqi_ref_"))
     try:
-        write_index_files(tmp, base, query, ix, ks, gt, ctx)
-        ctx.close()
-        # bounded steps: each step is a sample of the batch sized to ~cpu_seconds / steps
-        probe, err = reference_qbench(tmp, ks, a.L, threads, 0, 1, 500)
-        if probe is None:
-            print(json.dumps({"impl": "reference", "unavailable": err}), flush=True)
-            return
-        per_q = probe["seconds"] / probe["queries_per_step"]
-        budget = 120.0 / max(1, a.steps + a.warmup)
-        nqs = int(min(len(query), max(100, budget / max(per_q, 1e-9) / len(ks))))
-        res, err = reference_qbench(tmp, ks, a.L, threads, a.warmup, a.steps, nqs)
-        if res is None:
-            print(json.dumps({"impl": "reference", "unavailable": err}), flush=True)
-            return
-        value = res["qps"]
+        tmp.mkdir(parents=True, exist_ok=True)
+        t0 = time.perf_counter()
+        base, query = pipeline.mixture(a.n, a.d, a.nq, seed=20260819 + rank)
+        pfx = tmp / "m"
+        formats.write_fbin(f"{pfx}_base.bin", base)
+        formats.write_fbin(f"{pfx}_query.bin", query)
+        Path(f"{pfx}_lifted.meta").write_text(f"0 {a.d} 100 l2 1.0\n")
+        del base
+        log(f"reference-arm data in {time.perf_counter() - t0:.1f}s; {threads} host threads")
+        rlog = lambda m: log("reference-arm", m)  # noqa: E731
+        info = rp.build(pfx, threads, log=rlog)
+        Ls = [a.L] * (a.warmup + a.steps) + SWEEP_L
+        runs = {k: rp.query(pfx, k, Ls, threads, tmp / "cache", info, log=rlog) for k in ks}
+        nq = len(query)
+        step_s = [sum(nq / runs[k]["points"][s]["qps"] for k in ks) for s in range(a.warmup, a.warmup + a.steps)]
+        value = a.steps * nq * len(ks) / sum(step_s)
+        first = runs[ks[0]]
+        per_k = {k: {x: runs[k]["points"][a.warmup][x] for x in ("recall", "precision", "cand", "pred", "dist",
+                                                                  "graph_dist") if x in runs[k]["points"][a.warmup]}
+                 for k in ks}
+        per_L = [{"k": k, **{x: p[x] for x in ("L", "recall", "precision", "qps", "graph_dist") if x in p}}
+                 for k in ks for p in runs[k]["points"][a.warmup + a.steps:]]
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "queries/s", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": round(1e3 * res["seconds"] / a.steps, 4), "higher_is_better": True,
+            "warmup": a.warmup, "ms_per_step": round(1e3 * sum(step_s) / a.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded 1,000-centre mixture, integers in [0,255])",
-            "config": {"workload": f"rknn_query {a.n}x{a.d}, {a.nq} queries x k{{{a.ks}}}, L={a.L}, "
-                                   "G48 graph, M8/u8 LRQ postfilter", "n": a.n, "d": a.d, "nq": a.nq,
-                       "queries_per_step": nqs * len(ks), "ks": ks, "L": a.L, "parallelism": "cpu"},
+            "config": bench_config(a, ks, world),
             "impl": "reference",
             "cpu_baseline": {"value": round(value, 1), "unit": "queries/s", "cores": threads, "kind": "reference",
-                             "sample": f"first {nqs} queries x k{{{a.ks}}} per step on the GPU-built index "
-                                       "(reference formats); reference range_search + postfilter + evaluation"},
+                             "sample": f"the whole step ({nq} queries x k{{{a.ks}}}, L={a.L}) on the reference's "
+                                       "own index; its rknn_query timing (query lift, range_search, postfilter, "
+                                       "evaluation), one L-list entry per step"},
             "e2e": {"value": round(value, 1), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "per_k": res["per_k"],
+            "per_k": per_k,
+            "per_L": per_L,
+            "build_s": {"aknn_source": round(info["aknn_build_s"], 3),
+                        "verifier_train": round(info["verifier_train_s"], 3),
+                        "graph_index": first.get("graph_index_s"), "index_total": first.get("index_s"),
+                        "ground_truth_cpu": round(info["ground_truth_s"], 3)},
+            "ground_truth": json.loads(info["ground_truth_path"]),
         }
         print(json.dumps(line), flush=True)
+    except (RuntimeError, OSError, ValueError, subprocess.TimeoutExpired) as e:
+        unavailable(f"reference pipeline failed: {str(e)[:300]}")
     finally:
         if not a.keep:
             shutil.rmtree(tmp, ignore_errors=True)

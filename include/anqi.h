@@ -43,6 +43,14 @@ const char* anqi_last_error(const anqi_ctx* ctx);
 int anqi_version(void);
 /* Bytes of device memory the context currently holds. */
 uint64_t anqi_device_bytes(const anqi_ctx* ctx);
+/* Test hook, no counterpart in the reference: makes the device waits of this
+ * context run out without any fault.  ANQI_FAULT_DROP_ROW_COPIES: the search
+ * kernel of later anqi_query_run / anqi_rknn_query calls issues no bulk copies
+ * of lifted rows, so its bounded waits for them (a fixed number of polls)
+ * expire with nothing in flight; the call returns ANQI_ERR_TIMEOUT and the context
+ * stays usable.  flags = 0 restores normal operation. */
+#define ANQI_FAULT_DROP_ROW_COPIES 1u
+int anqi_inject_fault(anqi_ctx* ctx, uint32_t flags);
 /* Device timer on the context's stream (CUDA events): start, then stop returns
  * the elapsed milliseconds of everything the context ran in between. */
 int anqi_timer_start(anqi_ctx* ctx);
@@ -72,6 +80,34 @@ int anqi_lrq_materialize(anqi_ctx* ctx, const float* coeff, const uint8_t* codes
                          uint32_t nk, uint32_t rankm, const float* mu, const float* basis,
                          const float* codebook, uint32_t code_size, uint32_t k_one_based,
                          double radius_scale, float* thr);
+
+/* Every CompactLrqVerifier form (src/rknn_query.cpp:144-178, 604-753): bits
+ * 0 = rankm_only (no residual), 2 / 4 / 8 / 16 = rankm_resid_u{bits}_lrq_*
+ * (codebook of 2^bits sorted centres per rank, codes packed object-major as
+ * include/packed_code_array.h:8-63 lays them out: (n * nk * bits + 7) / 8
+ * bytes; u2 needs nk % 4 == 0 and u4 nk % 2 == 0, else ANQI_ERR_FORMAT),
+ * 32 = rankm_resid_f32 (residual n x nk floats).  policy: the artifact's
+ * numbering (encode_learned_residual, :482-513).  codes / residual / codebook
+ * may be NULL where the form has none. */
+#define ANQI_LRQ_NEAREST 0u
+#define ANQI_LRQ_FLOOR 1u
+#define ANQI_LRQ_CEIL 2u
+int anqi_lrq_encode_bits(anqi_ctx* ctx, const float* keys, uint64_t n, uint32_t nk, uint32_t rankm,
+                         const float* mu, const float* basis, const float* codebook, uint32_t code_size,
+                         uint32_t bits, uint32_t policy, float* coeff, uint8_t* codes, float* residual);
+/* materialize_k for any form; signed_keys != 0 (IP metric, -<q,o> keys) keeps
+ * negative thresholds instead of clamping them at zero (:748-751). */
+int anqi_lrq_materialize_bits(anqi_ctx* ctx, const float* coeff, const uint8_t* codes, const float* residual,
+                              uint64_t n, uint32_t nk, uint32_t rankm, uint32_t bits, const float* mu,
+                              const float* basis, const float* codebook, uint32_t code_size,
+                              uint32_t k_one_based, double radius_scale, int signed_keys, float* thr);
+/* AnalyticRankMVerifier::materialize_k (src/rknn_query.cpp:515-601): the
+ * ANQIPW1 model's coefficients (n x rankm) and header fields; thr[i] =
+ * max(0, scale * sum_m c_im * ratio^b0 * log(ratio)^m), ratio = k / train_kmax
+ * when flags & 4, else k. */
+int anqi_analytic_rankm_materialize(anqi_ctx* ctx, const float* coeff, uint64_t n, uint32_t rankm,
+                                    uint32_t train_kmax, uint32_t fit_kmin, uint32_t flags, double b0,
+                                    uint32_t k_one_based, double radius_scale, float* thr);
 
 /* ----------------------------------------------------------------- lift
  * The anyk_lift of src/rknn_query.cpp:2203-2235 (L2): base n x d and the
@@ -148,6 +184,10 @@ typedef struct {
     uint64_t seed;         /* 10 */
     float alpha;           /* ANQI_ALPHA = 1.2 */
     uint32_t warm_width;   /* 100 */
+    uint32_t precision;    /* LocalJoin distances: 0 = FP32 CUDA cores, 1 = BF16 tensor-core tiles
+                              filter each round's pairs against the round-start heap tops and
+                              only kept pairs are recomputed in FP32 (identical heaps; needs
+                              join_sample <= 32 and dim <= 256, else FP32) */
 } anqi_graph_params;
 
 int anqi_graph_build(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* warm_ids,
@@ -163,6 +203,11 @@ int anqi_graph_warm_start(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t di
 int anqi_graph_localjoin(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, uint32_t K,
                          uint32_t sample, uint32_t max_rounds, uint32_t* ids, float* vals,
                          uint64_t* updates /* max_rounds entries */, uint32_t* rounds_done);
+/* The same with the LocalJoin precision form of anqi_graph_params.precision;
+ * join_ms (optional) receives the device time of the rounds. */
+int anqi_graph_localjoin_precision(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, uint32_t K,
+                                   uint32_t sample, uint32_t max_rounds, uint32_t precision, uint32_t* ids,
+                                   float* vals, uint64_t* updates, uint32_t* rounds_done, float* join_ms);
 int anqi_graph_select(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids,
                       const float* g_vals, uint32_t K, uint32_t M, uint32_t ef, uint32_t cap, float alpha,
                       uint32_t* O, uint32_t* O_deg);
@@ -196,6 +241,13 @@ int anqi_index_load(anqi_ctx* ctx, const anqi_index_desc* desc);
 int anqi_verifier_load(anqi_ctx* ctx, const float* coeff, const uint8_t* codes, uint64_t n, uint32_t nk,
                        uint32_t rankm, const float* mu, const float* basis, const float* codebook,
                        uint32_t code_size);
+/* The same for any CompactLrqVerifier form (see anqi_lrq_encode_bits), and
+ * the analytic Rank-M model; anqi_verifier_materialize then uses it. */
+int anqi_verifier_load_bits(anqi_ctx* ctx, const float* coeff, const uint8_t* codes, const float* residual,
+                            uint64_t n, uint32_t nk, uint32_t rankm, uint32_t bits, const float* mu,
+                            const float* basis, const float* codebook, uint32_t code_size, int signed_keys);
+int anqi_verifier_load_analytic(anqi_ctx* ctx, const float* coeff, uint64_t n, uint32_t rankm,
+                                uint32_t train_kmax, uint32_t fit_kmin, uint32_t flags, double b0);
 int anqi_verifier_materialize(anqi_ctx* ctx, uint32_t k_one_based, double radius_scale);
 /* Explicit per-object thresholds for k (e.g. exact_f32 mode). */
 int anqi_set_thresholds(anqi_ctx* ctx, uint32_t k_one_based, const float* thr);
@@ -221,6 +273,9 @@ typedef struct {
                                   ran with (chosen by timing; 0 = none) */
     uint32_t visited_l2_table; /* entries of the per-warp L2-resident visited table (0 = none);
                                   beyond both, a per-warp bitmap over all ids */
+    uint32_t warps_per_block;  /* block shape of the search launch (2, 4 or 8 warps, one query
+                                  each), chosen by timing with the visited-set sizes */
+    uint32_t candidate_tile;   /* base rows per postfilter round (8, 4 or 2), chosen by timing */
 } anqi_query_stats;
 
 int anqi_rknn_query(anqi_ctx* ctx, const float* queries, uint32_t nq, const uint32_t* k_per_query,
@@ -278,15 +333,21 @@ int anqi_query_evaluate_sums(anqi_ctx* ctx, anqi_eval_sums* out);
  * L, on index arrays the caller already holds in device memory; it allocates
  * nothing.  Its working memory is a fixed file-scope device array of
  * ANQI_NOALLOC_SCRATCH_BYTES that every GPU loading this library reserves
- * until the process exits; n is limited by what fits in it (one visited
- * bitmap of n/8 bytes per concurrent query: n up to about 130 million).  All calls on a device share that array: calls that overlap on
- * the GPU race -- serialize them.  The first call on each device looks up the
- * array (cudaGetSymbolAddress); make it before any stream capture.
+ * until the process exits.  Each query in flight holds one slot of it (a
+ * visited bitmap of n/8 bytes plus 40 KB), so n is at most about 134 million
+ * (one slot) and concurrency falls as n grows: at n = 1M about 100 queries run
+ * at once, a fraction of what the context path keeps in flight.  All calls on
+ * a device share that array: calls that overlap on the GPU race -- serialize
+ * them.  The first call on each device looks up the array
+ * (cudaGetSymbolAddress).  Every call synchronizes `stream` before it returns
+ * (it reads back an error word), so it cannot be called while that stream is
+ * being captured.
  * Arrays are device pointers; rows 16-byte aligned, strides multiples of 4
  * floats; queries nq x base_stride.  pred_ids receives up to max_pred ids per
  * query (row q at q * max_pred), pred_count the full count; returns
  * ANQI_ERR_CAPACITY if any count exceeded max_pred or a query's candidate list
- * exceeded 8192 entries, ANQI_ERR_ARGS for bad sizes or alignment. */
+ * exceeded 8192 entries, ANQI_ERR_FORMAT for a link or tree child out of
+ * range, ANQI_ERR_ARGS for bad sizes or alignment. */
 #define ANQI_NOALLOC_SCRATCH_BYTES (16u << 20)
 typedef struct {
     uint64_t n;

@@ -169,7 +169,8 @@ def test_rknn_bad_inputs_exit_3(tmp_path):
 
 
 @pytest.mark.parametrize("var,val", [
-    ("ANQI_GRAPH_GEOMETRY", "original"), ("ANQI_GRAPH_GEOMETRY", "bogus"), ("ANQI_RADIUS_MODE", "exact_f32"),
+    ("ANQI_GRAPH_GEOMETRY", "original"), ("ANQI_GRAPH_GEOMETRY", "bogus"), ("ANQI_RADIUS_MODE", "knots"),
+    ("ANQI_RADIUS_MODE", "rankm_resid_u8_floor"), ("ANQI_RADIUS_MODE", "analytic_rankm"),
     ("ANQI_VERIFIER_PLACEMENT", "integrated"), ("ANQI_VERIFIER_PLACEMENT", "x"), ("ANQI_RECHECK", "1"),
     ("ANQI_SPECIFIC", "1"), ("ANQI_VAMANA", "1"), ("ANQI_EDGE_POLICY", "lsg_rng"),
     ("ANQI_RQ_OBJECTIVE", "predicate_boundary"), ("ANQI_CANDIDATE_ENVELOPE", "verifier"),
@@ -179,6 +180,29 @@ def test_rknn_configurations_outside_the_path_exit_2(tmp_path, var, val):
     pfx, env, _ = sample_prefix(tmp_path)
     rc, out, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10, env={**env, var: val})
     assert rc == 2, (out, err)
+
+
+def test_rknn_exact_f32_rejects_slack(tmp_path):
+    pfx, env, _ = sample_prefix(tmp_path)
+    rc, _, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10,
+                     env={**env, "ANQI_RADIUS_MODE": "exact_f32", "ANQI_RANKM_SLACK": "0.1"})
+    assert rc == 2 and "exact_f32 postfilter does not accept ANQI_RANKM_SLACK" in err
+
+
+def test_rknn_verifier_mode_files_are_validated(tmp_path):
+    """A learned codebook of the wrong width and a malformed analytic model
+    exit 3 before any device work, as the reference does."""
+    pfx, env, _ = sample_prefix(tmp_path)
+    import lrq_forms as lf
+    f, _ = lf.load()
+    formats.write_codebook(f"{pfx}_learned_rq_codebook_M8_u4.bin", lf.codebook(f, 2), 8, 4)
+    rc, _, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10,
+                     env={**env, "ANQI_RADIUS_MODE": "rankm_resid_u4_lrq_floor"})
+    assert rc == 3, err
+    Path(f"{pfx}_analytic_rankm_M8.bin").write_bytes(b"ANQIPW1\0" + b"\0" * 40)
+    rc, _, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10,
+                     env={**env, "ANQI_RADIUS_MODE": "analytic_rankm", "ANQI_CANDIDATE_ENVELOPE": "graph_horizon"})
+    assert rc == 3 and "analytic Rank-M header mismatch" in err
 
 
 def test_rknn_ip_metric_is_named(tmp_path):

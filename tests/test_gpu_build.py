@@ -289,7 +289,7 @@ def test_graph_build_query_recall(ctx, sample):
     within 0.2 points of the reference's own result lines (same L, k)."""
     x = sample["lifted"]
     n, dim = x.shape
-    gp = GraphParams(48, 50, 100, 8, 6, 20, 100, 100, 10, 1.2, 100)
+    gp = GraphParams(48, 50, 100, 8, 6, 20, 100, 100, 10, 1.2, 100, 0)
     deg = np.empty(n, np.uint32)
     links = np.empty((n, 48), np.uint32)
     st = BuildStats()
@@ -364,3 +364,43 @@ def test_aknn_build_tensor_init_identical(ctx, kind, monkeypatch):
     assert np.array_equal(a_ids, b_ids)
     assert np.array_equal(bits(a_d), bits(b_d))
 
+
+
+def localjoin_precision(ctx, x, ids, vals, precision, sample=20, rounds=6):
+    x = f32(x)
+    ids = u32(ids).copy()
+    vals = f32(vals).copy()
+    n, dim = x.shape
+    up = np.zeros(rounds, np.uint64)
+    done = C.c_uint32()
+    ms = C.c_float()
+    ctx._check(ctx.lib.anqi_graph_localjoin_precision(ctx.h, x, n, dim, ids.shape[1], sample, rounds, precision, ids,
+                                                      vals, up, C.byref(done), C.byref(ms)), "localjoin")
+    return ids, vals, [int(u) for u in up[:done.value]], ms.value
+
+
+@pytest.mark.parametrize("kind", ["lifted_mixture", "clustered_float", "duplicates"])
+def test_localjoin_tensor_tiles_identical(ctx, kind):
+    """The LocalJoin precision form (BF16 tcgen05 tiles filter each round's
+    pairs against the round-start heap tops, the kept pairs are recomputed in
+    FP32) leaves the heaps and per-round update counts bit-identical to the FP32
+    form, on lifted (non-integer) vectors as the graph build sees them."""
+    from anqi import pipeline
+    if kind == "lifted_mixture":
+        base, _ = pipeline.mixture(6000, 128, 0, centers=30, seed=5)
+        radius = np.random.default_rng(8).uniform(2000.0, 8000.0, 6000).astype(np.float32)
+        x, _, _ = ol.lift(base, radius)
+    elif kind == "clustered_float":
+        x = clustered(5000, 40, 9)
+    else:
+        x = clustered(4000, 24, 12)
+        x[100:140] = x[7]
+    n = len(x)
+    rng = np.random.default_rng(3)
+    cand = rng.integers(0, n, size=(n, 100)).astype(np.uint32)
+    gi, gv = warm_start(ctx, x, cand, 100, 50)
+    a = localjoin_precision(ctx, x, gi, gv, 0)
+    b = localjoin_precision(ctx, x, gi, gv, 1)
+    assert a[2] == b[2], (a[2], b[2])
+    assert np.array_equal(a[0], b[0]) and np.array_equal(bits(a[1]), bits(b[1]))
+    assert sum(a[2]) > 0

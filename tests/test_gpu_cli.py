@@ -127,3 +127,53 @@ def test_reference_loads_the_caches_this_driver_writes(tmp_path):
     assert "[rknn] loaded cached index" in ref.stdout and "Loading index from:" in ref.stdout
     assert "[rknn] loaded independent compact verifier" in ref.stdout
     assert lines(ref.stdout) == lines(ours)
+
+
+VERIFIER_MODES = ["rankm_resid_u2_lrq_floor", "rankm_resid_u4_lrq_nearest", "rankm_resid_u8_lrq_ceil",
+                  "rankm_resid_u16_lrq_floor", "rankm_resid_f32", "rankm_only", "exact_f32", "analytic_rankm"]
+
+
+@pytest.mark.skipif(not tc.REF_BIN.exists(), reason="reference binaries not built")
+@pytest.mark.parametrize("mode", VERIFIER_MODES)
+def test_rknn_query_verifier_modes_match_reference(tmp_path, mode):
+    """Every independent postfilter verifier of the reference (rknn_query.cpp:
+    1771-1792) through this driver: the verifier artifact it writes equals the
+    one the reference writes byte for byte, and on the reference's graph it
+    prints the reference's result lines exactly."""
+    import lrq_forms as lf
+    pfx, env, z = tc.sample_prefix(tmp_path, 32)
+    f, _ = lf.load()
+    env = dict(env, ANQI_RADIUS_MODE=mode)
+    for b in (2, 4, 8, 16):
+        formats.write_codebook(f"{pfx}_learned_rq_codebook_M8_u{b}.bin", lf.codebook(f, b), 8, b)
+    if mode == "analytic_rankm":
+        formats.write_analytic(f"{pfx}_analytic_rankm_M8.bin",
+                               formats.AnalyticModel(100, 8, 10, 7, float(f["pw_b0_7"][0]), f["pw_coeff_7"]))
+        env["ANQI_CANDIDATE_ENVELOPE"] = "graph_horizon"
+    ref_env = {k: v for k, v in os.environ.items() if not k.startswith("ANQI_")}
+    ref_env.update(env, OMP_NUM_THREADS="1", ANQI_GRAPH_CACHE_DIR=str(tmp_path / "ref" / "graph"),
+                   ANQI_VERIFIER_CACHE_DIR=str(tmp_path / "ref" / "verifier"))
+    for sub in ("graph", "verifier"):
+        (tmp_path / "ref" / sub).mkdir(parents=True)
+    ref = subprocess.run([str(tc.REF_BIN), "16,32,64", str(pfx), "48", "500", "64", "600", "50"], env=ref_env,
+                         capture_output=True, text=True, timeout=300)
+    assert ref.returncode == 0, ref.stderr
+    rc, ours, err = tc.run("rknn_query", "16,32,64", pfx, 48, 500, 64, 600, 50, env=env)
+    assert rc == 0, err
+    ref_vf = sorted((tmp_path / "ref" / "verifier").glob("_anqi_verifier_*.bin"))
+    our_vf = sorted(Path(env["ANQI_VERIFIER_CACHE_DIR"]).glob("_anqi_verifier_*.bin"))
+    assert [p.name for p in our_vf] == [p.name for p in ref_vf]
+    for a, b in zip(our_vf, ref_vf):
+        assert a.read_bytes() == b.read_bytes(), mode
+    # the reference's graph in this driver's cache slot: its printed lines exactly
+    gref = list((tmp_path / "ref" / "graph").glob("fd_metric_*"))
+    gours = list(Path(env["ANQI_GRAPH_CACHE_DIR"]).glob("fd_metric_*"))
+    assert len(gref) == 1 and len(gours) == 1 and gref[0].name == gours[0].name
+    gours[0].write_bytes(gref[0].read_bytes())
+    for suffix in ("_approxlift_graph_", "_anqi_meta_graph_"):
+        for p in (tmp_path / "ref" / "graph").glob(suffix + "*"):
+            (Path(env["ANQI_GRAPH_CACHE_DIR"]) / p.name).write_bytes(p.read_bytes())
+    rc, ours, err = tc.run("rknn_query", "16,32,64", pfx, 48, 500, 64, 600, 50, env=env)
+    assert rc == 0, err
+    assert "[rknn] loaded cached index" in ours
+    assert lines(ours) == lines(ref.stdout), (mode, lines(ours), lines(ref.stdout))

@@ -1,6 +1,7 @@
 """GPU parity of the query path, LRQ codec, lift and distances (sm_100a kernels
 through the C ABI) against the reference's golden outputs and the C oracle.
 Bit-exact: every compared integer is equal and every float has the same bits."""
+import tempfile
 from pathlib import Path
 
 import numpy as np
@@ -389,3 +390,33 @@ def test_resident_batch_and_evaluate(ctx, random_index):
     ctx.query_run()
     with pytest.raises(Exception):
         ctx.query_evaluate_sums()
+
+
+def test_bounded_wait_runs_out_without_a_fault(sample):
+    """Failure detection without a GPU fault: with the search's row copies
+    withheld (anqi_inject_fault), every bounded wait for them expires after
+    a fixed number of polls with nothing in flight; the call returns ANQI_ERR_TIMEOUT,
+    and the same context then answers the same batch exactly as before."""
+    import time
+    from anqi._lib import ANQI_ERR_TIMEOUT, AnqiError
+    z = sample
+    with tempfile.TemporaryDirectory() as td:
+        p = Path(td) / "g.bin"
+        p.write_bytes(z["graph_file"].tobytes())
+        g = formats.read_graph(p)
+    with Context(0) as ctx:
+        ctx.index_load(z["base"], z["lifted"], g.deg, g.links, g.tree, float(z["scale"]), float(z["mstar2"]))
+        ctx.set_thresholds(10, z["thresholds"][1])
+        before = ctx.rknn_query(z["query"], 10, 32)
+        ctx.inject_fault(1)
+        t0 = time.time()
+        with pytest.raises(AnqiError) as e:
+            ctx.rknn_query(z["query"], 10, 32)
+        assert e.value.status == ANQI_ERR_TIMEOUT, e.value
+        waited = time.time() - t0
+        print(f"bounded row waits ran out after {waited:.2f} s")
+        assert waited < 60
+        ctx.inject_fault(0)
+        after = ctx.rknn_query(z["query"], 10, 32)
+        assert np.array_equal(before.pred_off, after.pred_off) and np.array_equal(before.pred_ids, after.pred_ids)
+        assert np.array_equal(before.n_dist, after.n_dist)
