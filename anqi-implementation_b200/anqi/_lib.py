@@ -47,7 +47,7 @@ class IndexDesc(C.Structure):
         ("n", C.c_uint64), ("d", C.c_uint32), ("degree", C.c_uint32), ("base", _vp), ("lifted", _vp),
         ("deg", _vp), ("links", _vp), ("tree_nodes", C.c_uint32), ("tree_left", _vp), ("tree_right", _vp),
         ("tree_offset", _vp), ("tree_hyperplane", _vp), ("tree_leaf_first", _vp), ("scale", C.c_double),
-        ("mstar2", C.c_double),
+        ("mstar2", C.c_double), ("metric", C.c_uint32),
     ]
 
 
@@ -68,7 +68,7 @@ class QueryStats(C.Structure):
 class AknnParams(C.Structure):
     _fields_ = [("k", C.c_uint32), ("leaf", C.c_uint32), ("trees", C.c_uint32), ("ef", C.c_uint32),
                 ("ef_alpha", C.c_uint32), ("seed", C.c_uint64), ("nn_iters", C.c_uint32), ("nn_sample", C.c_uint32),
-                ("precision", C.c_uint32)]
+                ("precision", C.c_uint32), ("metric", C.c_uint32)]
 
 
 class GraphParams(C.Structure):
@@ -108,13 +108,21 @@ _SIGS = {
     "anqi_analytic_rankm_materialize": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                         C.c_double, C.c_uint32, C.c_double, _f32],
     "anqi_lift": [_vp, _f32, C.c_uint64, C.c_uint32, _f32, _f32, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+    "anqi_lift_metric": [_vp, _f32, C.c_uint64, C.c_uint32, _f32, C.c_uint32, _f32, C.POINTER(C.c_double),
+                         C.POINTER(C.c_double)],
     "anqi_rp_forest": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
                        C.c_uint32, _u32, _u32, _u32, _f32, _f32, _u32, _u32, _u32],
+    "anqi_rp_forest_metric": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                              C.c_uint32, C.c_uint32, _u32, _u32, _u32, _f32, _f32, _u32, _u32, _u32],
     "anqi_aknn_build": [_vp, _f32, C.c_uint64, C.c_uint32, C.POINTER(AknnParams), _u32, _f32,
                         C.POINTER(BuildStats)],
     "anqi_aknn_init": [_vp, _f32, C.c_uint64, C.c_uint32, _u64, _u32, C.c_uint64, C.c_uint32, _u32, _f32],
     "anqi_aknn_gather": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _f32, C.c_uint32, C.c_uint32, C.c_uint32,
                          C.c_uint32, _u32, _f32],
+    "anqi_aknn_init_metric": [_vp, _f32, C.c_uint64, C.c_uint32, _u64, _u32, C.c_uint64, C.c_uint32, C.c_uint32, _u32,
+                              _f32],
+    "anqi_aknn_gather_metric": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _f32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                C.c_uint32, C.c_uint32, _u32, _f32],
     "anqi_graph_build": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, C.c_uint32, C.POINTER(GraphParams), _u32, _u32,
                          C.POINTER(BuildStats)],
     "anqi_graph_tree_size": [_vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)],
@@ -159,7 +167,13 @@ _SIGS = {
     "anqi_exact_topk": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _u32, _f32],
     "anqi_rknn_ground_truth": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32, _u32, _u32, _f32,
                                C.c_uint64, C.POINTER(C.c_uint64)],
+    "anqi_exact_topk_metric": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, _u32, _f32],
+    "anqi_rknn_ground_truth_metric": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32, C.c_uint32, _u32,
+                                      _u32, _f32, C.c_uint64, C.POINTER(C.c_uint64)],
 }
+
+#: metric codes of the C ABI (ANQI_METRIC_L2 / ANQI_METRIC_IP)
+METRICS = {"l2": 0, "ip": 1}
 
 #: every symbol include/anqi.h declares (checked by the CPU tests)
 EXPORTED = tuple(_SIGS)
@@ -333,18 +347,18 @@ class Context:
                     "analytic_rankm_materialize")
         return thr
 
-    def lift(self, base, radius):
+    def lift(self, base, radius, metric: str = "l2"):
         base = _c(base, np.float32)
         n, d = base.shape
         out = np.empty((n, d + 2), np.float32)
         m2, sc = C.c_double(), C.c_double()
-        self._check(self.lib.anqi_lift(self.h, base, n, d, _c(radius, np.float32), out, C.byref(m2), C.byref(sc)),
-                    "lift")
+        self._check(self.lib.anqi_lift_metric(self.h, base, n, d, _c(radius, np.float32), METRICS[metric], out,
+                                              C.byref(m2), C.byref(sc)), "lift")
         return out, m2.value, sc.value
 
     # ------------------------------------------------------------- index
 
-    def index_load(self, base, lifted, deg, links, tree, scale: float, mstar2: float) -> None:
+    def index_load(self, base, lifted, deg, links, tree, scale: float, mstar2: float, metric: str = "l2") -> None:
         """tree: post-order arrays with attributes left/right/offset/hyperplane and leaf_first()."""
         base = _c(base, np.float32)
         lifted = _c(lifted, np.float32)
@@ -357,7 +371,7 @@ class Context:
         tf = _c(tree.leaf_first(), np.uint32)
         n, d = base.shape
         desc = IndexDesc(n, d, links.shape[1], _ptr(base), _ptr(lifted), _ptr(deg), _ptr(links), len(tl), _ptr(tl),
-                         _ptr(tr), _ptr(to), _ptr(th), _ptr(tf), float(scale), float(mstar2))
+                         _ptr(tr), _ptr(to), _ptr(th), _ptr(tf), float(scale), float(mstar2), METRICS[metric])
         self._check(self.lib.anqi_index_load(self.h, C.byref(desc)), "index_load")
         self.n = n
         self.d = d

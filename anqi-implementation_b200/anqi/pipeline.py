@@ -15,7 +15,7 @@ from pathlib import Path
 import numpy as np
 
 from . import formats, lrq_train
-from ._lib import AknnParams, BuildStats, Context, GraphParams
+from ._lib import METRICS, AknnParams, BuildStats, Context, GraphParams
 
 EMPTY = 0xFFFFFFFF
 
@@ -76,18 +76,21 @@ class Index:
 
 
 def aknn_build(ctx: Context, base: np.ndarray, k=100, leaf=500, trees=64, ef=600, seed=10, nn_iters=0, nn_sample=20,
-               precision="bf16"):
-    """build_aknn_source: returns ids (n x k) and keys = max(0, d) (build_aknn_source.cpp:125-126).
+               precision="bf16", metric="l2"):
+    """build_aknn_source: returns ids (n x k) and the record keys: max(0, d) for
+    l2, d - 1 = -<a, b> for ip (build_aknn_source.cpp:125-126).
     precision "bf16": init_knn leaf distances on BF16 tensor-core tiles with FP32
-    recheck; "fp32": CUDA cores.  Both give identical output."""
+    recheck; "fp32": CUDA cores.  Both give identical output (ip runs FP32)."""
     base = np.ascontiguousarray(base, np.float32)
     n, d = base.shape
-    p = AknnParams(k, leaf, trees, ef, 8, seed, nn_iters, nn_sample, {"fp32": 0, "bf16": 1}[precision])
+    p = AknnParams(k, leaf, trees, ef, 8, seed, nn_iters, nn_sample, {"fp32": 0, "bf16": 1}[precision],
+                   METRICS[metric])
     ids = np.empty((n, k), np.uint32)
     dist = np.empty((n, k), np.float32)
     st = BuildStats()
     ctx._check(ctx.lib.anqi_aknn_build(ctx.h, base, n, d, C.byref(p), ids, dist, C.byref(st)), "aknn_build")
-    return ids, np.maximum(dist, np.float32(0.0)), st.as_dict()
+    keys = dist - np.float32(1.0) if metric == "ip" else np.maximum(dist, np.float32(0.0))
+    return ids, keys, st.as_dict()
 
 
 def graph_build(ctx: Context, lifted: np.ndarray, warm_ids: np.ndarray, degree=48, nn_k=50, explore=100,
@@ -185,23 +188,26 @@ def load_index(ctx: Context, ix: Index, ks=(10, 50, 100)) -> None:
         ctx.verifier_materialize(k)
 
 
-def exact_thresholds(ctx: Context, base: np.ndarray, K: int = 100, method: str = "fp32", hints=None):
+def exact_thresholds(ctx: Context, base: np.ndarray, K: int = 100, method: str = "fp32", hints=None,
+                     metric: str = "l2"):
     """Exact top-K (dataset_gt --mode thresholds).  method "tc": BF16 tensor-core
     tiles with FP32 recheck (bit-identical output); hints = AKNN lists bound each
-    row's K-th key (an AKNN build runs when they are absent)."""
+    row's K-th key (an AKNN build runs when they are absent).  metric "ip": keys
+    -<a, b> (FP32 CUDA cores)."""
     base = np.ascontiguousarray(base, np.float32)
     n, d = base.shape
-    if method == "tc" and d <= 208:
+    if method == "tc" and d <= 208 and metric == "l2":
         return ctx.exact_topk_tc(base, K, hints)
     ids = np.empty((n, K), np.uint32)
     keys = np.empty((n, K), np.float32)
-    ctx._check(ctx.lib.anqi_exact_topk(ctx.h, base, n, d, K, ids, keys), "exact_topk")
+    ctx._check(ctx.lib.anqi_exact_topk_metric(ctx.h, base, n, d, K, METRICS[metric], ids, keys), "exact_topk")
     return ids, keys
 
 
-def rknn_ground_truth(ctx: Context, base: np.ndarray, query: np.ndarray, rk2: np.ndarray, method: str = "fp32"):
+def rknn_ground_truth(ctx: Context, base: np.ndarray, query: np.ndarray, rk2: np.ndarray, method: str = "fp32",
+                      metric: str = "l2"):
     """Exact RkNN CSR (dataset_gt --mode ground-truth); method "tc" as above."""
-    if method == "tc" and base.shape[1] <= 208:
+    if method == "tc" and base.shape[1] <= 208 and metric == "l2":
         return ctx.rknn_ground_truth_tc(base, query, rk2)
     base = np.ascontiguousarray(base, np.float32)
     query = np.ascontiguousarray(query, np.float32)
@@ -213,8 +219,8 @@ def rknn_ground_truth(ctx: Context, base: np.ndarray, query: np.ndarray, rk2: np
     while True:
         ids = np.empty(cap, np.uint32)
         keys = np.empty(cap, np.float32)
-        rc = ctx.lib.anqi_rknn_ground_truth(ctx.h, base, n, query, nq, d, np.ascontiguousarray(rk2, np.float32), off,
-                                            ids, keys, cap, C.byref(tot))
+        rc = ctx.lib.anqi_rknn_ground_truth_metric(ctx.h, base, n, query, nq, d, np.ascontiguousarray(rk2, np.float32),
+                                                   METRICS[metric], off, ids, keys, cap, C.byref(tot))
         if rc == 9 and tot.value > cap:
             cap = int(tot.value)
             continue

@@ -8,12 +8,12 @@
 //   2  usage / bad argument            3  unreadable base file or n <= K
 //   4  row-count mismatch              5  invalid neighbour row
 //   6  output write failure            7/8/9  device failure (library status)
-// Outputs: PREFIX_baseknn_aknn.rec (n x K x {u32 id, f32 key}, key = max(0, d),
-// written to .part then renamed) and PREFIX_aknn_build_time.meta.  `threads`
-// is recorded in the metadata; the device decides its own parallelism.
-// ANQI_NNITERS / ANQI_NNSAMPLE select NN-Descent rounds as in
-// include/index.h:1312-1316.  Only metric=l2 is implemented on this path; ip
-// exits 2.
+// Outputs: PREFIX_baseknn_aknn.rec (n x K x {u32 id, f32 key}, key = max(0, d)
+// for l2 and d - 1 = -<a, b> for ip, written to .part then renamed) and
+// PREFIX_aknn_build_time.meta.  `threads` is recorded in the metadata; the
+// device decides its own parallelism.  ANQI_NNITERS / ANQI_NNSAMPLE select
+// NN-Descent rounds as in include/index.h:1312-1316 (metric l2 only: with ip
+// and ANQI_NNITERS > 0 the tool exits 2).
 #include "cli_common.h"
 
 #include <algorithm>
@@ -37,7 +37,6 @@ static int run(int argc, char** argv) {
         if (!parse_count(argv[i], *slots[i - 3])) die(2, "[aknn] invalid argument %d: %s", i, argv[i]);
     const std::string metric = argc > 9 ? argv[9] : "l2";
     if (metric != "l2" && metric != "ip") die(2, "[aknn] metric must be l2 or ip");
-    if (metric == "ip") die(2, "[aknn] metric ip is not implemented on the GPU path (l2 only)");
     if (k == 0 || leaf == 0 || trees == 0 || ef == 0) die(2, "[aknn] K, leaf, trees and ef must be positive");
 
     uint32_t hn = 0, hd = 0;
@@ -64,6 +63,9 @@ static int run(int argc, char** argv) {
     // init_knn distances: BF16 tensor-core tiles with FP32 recheck (default) or
     // FP32 CUDA cores; the lists are identical either way
     p.precision = env_or("ANQI_B200_PRECISION", "bf16") == "fp32" ? 0u : 1u;
+    p.metric = metric == "ip" ? ANQI_METRIC_IP : ANQI_METRIC_L2;
+    if (p.metric == ANQI_METRIC_IP && p.nn_iters > 0)
+        die(2, "[aknn] ANQI_NNITERS > 0 is implemented for metric l2 only on this path");
     std::vector<uint32_t> ids(n * k);
     std::vector<float> dists(n * k);
     anqi_build_stats st{};
@@ -94,7 +96,9 @@ static int run(int argc, char** argv) {
     const std::string record_tmp = record_path + ".part";
     {
         std::vector<TopKRecord> recs(n * k);
-        for (uint64_t i = 0; i < n * k; i++) recs[i] = {ids[i], std::max(0.0f, dists[i])};
+        // build_aknn_source.cpp:125-126
+        for (uint64_t i = 0; i < n * k; i++)
+            recs[i] = {ids[i], p.metric == ANQI_METRIC_IP ? dists[i] - 1.0f : std::max(0.0f, dists[i])};
         write_file_or_die(record_tmp, {{recs.data(), recs.size() * sizeof(TopKRecord)}}, 6, "[aknn]");
     }
     if (std::rename(record_tmp.c_str(), record_path.c_str()) != 0) {

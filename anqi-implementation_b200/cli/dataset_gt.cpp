@@ -12,10 +12,9 @@
 //   PREFIX_rknn_gt.bin.rk     [u32 n][u32 rk_k][n f32 rank-k keys]
 //   PREFIX_rknn_gt.bin        [u32 nq][(nq+1) u32 off][ids][f32 keys]
 //   PREFIX_threshold_build_time.meta
-// Keys are the reference's FP32 |a|^2 + |b|^2 - 2<a,b> in its summation order,
-// so the files are bit-identical.  --tile and --threads are accepted and
-// reported; the device tiles on its own.  Only --metric l2 is implemented on
-// this path; ip exits 2.
+// Keys are the reference's FP32 |a|^2 + |b|^2 - 2<a,b> (--metric l2) or
+// -<a,b> (--metric ip) in its summation order, so the files are bit-identical.
+// --tile and --threads are accepted and reported; the device tiles on its own.
 #include "cli_common.h"
 
 #include <chrono>
@@ -102,7 +101,7 @@ static int run(int argc, char** argv) {
         return 2;
     }
     if (metric != "l2" && metric != "ip") die(2, "[dgt] metric must be l2 or ip");
-    if (metric == "ip") die(2, "[dgt] metric ip is not implemented on the GPU path (l2 only)");
+    const uint32_t metric_code = metric == "ip" ? ANQI_METRIC_IP : ANQI_METRIC_L2;
     if (nthreads > (uint64_t)std::numeric_limits<int>::max()) die(2, "[dgt] thread count is too large");
     const int T = nthreads ? (int)nthreads : 1;
     const auto t_all = std::chrono::steady_clock::now();
@@ -124,8 +123,9 @@ static int run(int argc, char** argv) {
         std::vector<uint32_t> ids(n * K);
         std::vector<float> keys(n * K);
         const auto t1 = std::chrono::steady_clock::now();
-        dev().check(anqi_exact_topk(dev().get(), base.x.data(), n, (uint32_t)D, (uint32_t)K, ids.data(), keys.data()),
-                  "exact top-K");
+        dev().check(anqi_exact_topk_metric(dev().get(), base.x.data(), n, (uint32_t)D, (uint32_t)K, metric_code,
+                                           ids.data(), keys.data()),
+                    "exact top-K");
         std::cout << "[dgt] base-to-base top-K done in "
                   << std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count() << "s\n";
         for (uint64_t i = 0; i < n; i++) rk2[i] = keys[i * K + rk_k - 1];
@@ -169,8 +169,9 @@ static int run(int argc, char** argv) {
         for (int attempt = 0; attempt < 2; attempt++) {
             ids.resize(cap);
             keys.resize(cap);
-            const int rc = anqi_rknn_ground_truth(dev().get(), base.x.data(), n, query.x.data(), nq, (uint32_t)D,
-                                                  rk2.data(), off.data(), ids.data(), keys.data(), cap, &total);
+            const int rc = anqi_rknn_ground_truth_metric(dev().get(), base.x.data(), n, query.x.data(), nq,
+                                                         (uint32_t)D, rk2.data(), metric_code, off.data(), ids.data(),
+                                                         keys.data(), cap, &total);
             if (rc == ANQI_ERR_CAPACITY && attempt == 0) {
                 cap = total;
                 continue;

@@ -4,12 +4,14 @@
 //   rknn_query L_DESCENT_LIST PREFIX [GRAPH_DEGREE=48] [LEAF_SIZE=1000]
 //              [TREE_COUNT=64] [BUILD_EF=400] [QUERY_K]
 //
-// Mirrors src/rknn_query.cpp:1547-2956 for the configuration scripts/run_final.sh
-// pins (anyk_lift geometry, postfilter placement, rankm_resid_u*_lrq_* verifier,
-// L2): the same argv, environment, prefix files, caches (file names and
-// identity keys, so a cache written by either program is found by the other),
-// stdout result lines and exit codes.  Configurations outside that path
-// (IP metric, rank-M or original geometry, integrated verifier, Vamana, edge
+// Mirrors src/rknn_query.cpp:1547-2956 for the anyk_lift geometry with the
+// postfilter placement -- the configuration scripts/run_final.sh pins -- under
+// either metric (the prefix's meta file names l2 or ip) and every independent
+// verifier (compact LRQ forms, rank-M only, float32 residuals, exact_f32,
+// analytic rank-M): the same argv, environment, prefix files, caches (file
+// names and identity keys, so a cache written by either program is found by
+// the other), stdout result lines and exit codes.  Configurations outside that
+// path (rank-M or original geometry, integrated verifier, Vamana, edge
 // policies, fixed-k lift, recheck) exit 2 with a message naming the setting.
 //
 // Differences of mechanism, not of result: the graph build, lift, LRQ
@@ -467,7 +469,7 @@ static int run(int argc, char** argv) {
         die(2, "[rknn] %s is not implemented on the GPU path (supported: the scripts/run_final.sh configuration)",
             what.c_str());
     };
-    if (metric != "l2") not_here("metric=" + metric);
+    const bool is_ip = metric == "ip";
     if (geometry != "anyk_lift") not_here("ANQI_GRAPH_GEOMETRY=" + geometry);
     // the independent postfilter verifiers (rknn_query.cpp:1771-1792): learned
     // LRQ (u2 / u4 / u8 / u16, floor / ceil / nearest), float32 residuals,
@@ -534,6 +536,12 @@ static int run(int argc, char** argv) {
         die(2, "[rknn] ANQI_RANKM_SLACK=%.6g makes non-positive radius scale", rankm_slack);
     if (vmode == VMode::Exact && rankm_slack != 0.0)
         die(2, "[rknn] exact_f32 postfilter does not accept ANQI_RANKM_SLACK");
+    // rknn_query.cpp:1812-1816, 2417-2422
+    if (vmode == VMode::Analytic && is_ip)
+        die(2, "[rknn] analytic_rankm uses the L2 LID power law and does not support IP");
+    if (vmode == VMode::Compact && is_ip && rankm_slack != 0.0)
+        die(2, "[rknn] IP compact postfilter currently requires ANQI_RANKM_SLACK=0; multiplicative scaling is not "
+               "monotone for signed -ip thresholds");
 
     // ---- cache identities (rknn_query.cpp:1840-1872, 1217-1241)
     const std::string basis_path = PFX + "_radbasis_M" + std::to_string(RANKM) + ".bin";
@@ -714,8 +722,8 @@ static int run(int argc, char** argv) {
             for (uint64_t i = 0; i < n; i++)
                 for (uint64_t j = 0; j < width; j++) warm[i * width + j] = rec[i * sk + j].id;
         } else {
-            printf("[rknn] original-space AKNN: leaf=%" PRIu64 " n_trees=%" PRIu64 " ef=%" PRIu64 " metric=l2\n",
-                   leafA, ntA, efA);
+            printf("[rknn] original-space AKNN: leaf=%" PRIu64 " n_trees=%" PRIu64 " ef=%" PRIu64 " metric=%s\n",
+                   leafA, ntA, efA, metric.c_str());
             anqi_aknn_params ap{};
             ap.k = (uint32_t)width;
             ap.leaf = (uint32_t)leafA;
@@ -726,6 +734,9 @@ static int run(int argc, char** argv) {
             ap.nn_iters = (uint32_t)std::max(0, std::atoi(env_or("ANQI_NNITERS", "0").c_str()));
             ap.nn_sample = (uint32_t)std::min(std::max(0, std::atoi(env_or("ANQI_NNSAMPLE", "20").c_str())), 120);
             ap.precision = env_or("ANQI_B200_PRECISION", "bf16") == "fp32" ? 0u : 1u;
+            ap.metric = is_ip ? ANQI_METRIC_IP : ANQI_METRIC_L2;
+            if (is_ip && ap.nn_iters > 0)
+                die(2, "[rknn] ANQI_NNITERS > 0 is implemented for metric l2 only on this path");
             warm.resize(n * width);
             std::vector<float> wd(n * width);
             dev().check(anqi_aknn_build(dev().get(), base.x.data(), n, (uint32_t)d, &ap, warm.data(), wd.data(), nullptr),
@@ -740,8 +751,9 @@ static int run(int argc, char** argv) {
         printf("[rknn] RADIUS_MODE=%s:postfilter conceptual_radius_store=%.3fGB\n", radius_key.c_str(),
                verification_bytes() / 1e9);
         lifted.resize(n * dim);
-        dev().check(anqi_lift(dev().get(), base.x.data(), n, (uint32_t)d, radius.data(), lifted.data(), &Mstar2, &scale),
-                  "lift");
+        dev().check(anqi_lift_metric(dev().get(), base.x.data(), n, (uint32_t)d, radius.data(),
+                                     is_ip ? ANQI_METRIC_IP : ANQI_METRIC_L2, lifted.data(), &Mstar2, &scale),
+                    "lift");
         {
             const uint32_t hdr[2] = {(uint32_t)n, (uint32_t)dim};
             write_file_or_die(approxlift, {{hdr, 8}, {lifted.data(), lifted.size() * 4}}, 3, "[rknn]");
@@ -825,12 +837,14 @@ static int run(int argc, char** argv) {
     desc.tree_leaf_first = leaf_first.data();
     desc.scale = scale;
     desc.mstar2 = Mstar2;
+    desc.metric = is_ip ? ANQI_METRIC_IP : ANQI_METRIC_L2;
     dev().check(anqi_index_load(dev().get(), &desc), "index load");
     if (vmode == VMode::Compact)
         dev().check(anqi_verifier_load_bits(dev().get(), lrq.coeff.data(), lrq.codes.empty() ? nullptr : lrq.codes.data(),
                                             lrq.residual.empty() ? nullptr : lrq.residual.data(), n, lrq.nk, lrq.rankm,
                                             lrq.bits, lrq.mu.data(), lrq.basis.data(),
-                                            lrq.codebook.empty() ? nullptr : lrq.codebook.data(), lrq.code_size, 0),
+                                            lrq.codebook.empty() ? nullptr : lrq.codebook.data(), lrq.code_size,
+                                            is_ip ? 1 : 0),
                     "verifier load");
     else if (vmode == VMode::Analytic)
         dev().check(anqi_verifier_load_analytic(dev().get(), model.coeff.data(), n, (uint32_t)RANKM, model.train_kmax,

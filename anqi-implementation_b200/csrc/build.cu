@@ -42,6 +42,12 @@ static double ms_since(Clock::time_point t0) {
 
 enum GatherMode : int { kModeAknn = 0, kModeSelect = 1, kModeCommit = 2 };
 
+// Pair keys: L2 through the norms (index.h:172-176); the ip metric's distance
+// 1 - <a, b>, one sequential sum per pair and so one lane per pair
+// (distance.h:170-174); the ip ground truth's key -<a, b> in the lane order
+// (dataset_gt.cpp:224).
+enum KeyMode : uint32_t { kKeyL2 = 0, kKeyIpDist = 1, kKeyNegIp = 2 };
+
 struct GatherParams {
     const float* x;
     const float* norms;
@@ -76,6 +82,7 @@ struct GatherParams {
     uint32_t hash_cap, hash_shift;  // shared-memory visited table per warp (power of two, 0 = none)
     uint32_t* gtab;                 // per-slot L2-resident visited tables (all kEmpty between rows)
     uint32_t gcap, gshift;          // entries per slot (power of two, 0 = none)
+    uint32_t ip;  // AKNN mode only: keys are the ip metric's 1 - <a, b>
     uint32_t* next_row;
     const uint32_t* row_order;  // work item -> row (rows of one RP-tree leaf together), or null for identity
     unsigned long long* pool_total;
@@ -85,9 +92,16 @@ struct GatherParams {
 constexpr uint32_t kSortSmem = 1024;  // pool entries sorted in shared memory per warp
 
 // Distances of batch ids to row i: (n_i + n_j) - 2 ip(x_i, x_j).
+template <bool kIp>
 __device__ __forceinline__ void batch_d2(const GatherParams& p, uint64_t i, const uint32_t* ni, float* nd, uint32_t m,
                                          uint32_t gw, uint32_t gt) {
     const float* xi = p.x + i * p.stride;
+    if constexpr (kIp) {
+        for (uint32_t idx = threadIdx.x & 31u; idx < m; idx += 32)
+            nd[idx] = ip_dist_seq(xi, p.x + (uint64_t)ni[idx] * p.stride, p.dim);
+        __syncwarp();
+        return;
+    }
     const float ni_norm = p.norms[i];
     for (uint32_t r0 = 0; r0 < m; r0 += 8) {
         const uint32_t idx = r0 + gw;
@@ -204,6 +218,8 @@ __device__ __forceinline__ uint32_t gather_visit(const GatherParams& p, Visited&
     return m;
 }
 
+// kIp: the AKNN mode in the ip metric (a separate instance, so the L2 one is unchanged)
+template <bool kIp>
 __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -255,7 +271,7 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
                     ni[t] = pos < od ? p.O[i * p.M + pos] : p.rev_ids[r0 + (pos - od)];
                 }
                 __syncwarp();
-                batch_d2(p, i, ni, nd, m, gw, gt);
+                batch_d2<kIp>(p, i, ni, nd, m, gw, gt);
                 for (uint32_t t = lane; t < m; t += 32) {
                     if (np + t < p.pool_cap) {
                         pd[np + t] = nd[t];
@@ -376,7 +392,7 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
                     const uint32_t m = gather_visit(p, vis, nlog, a0 ? lst[32 * u + lane] : kEmpty,
                                                     a1 ? lst[32 * u + 32 + lane] : kEmpty, 0.f, 0.f, false, ni, nd, lane);
                     if (m == 0) continue;
-                    batch_d2(p, i, ni, nd, m, gw, gt);
+                    batch_d2<kIp>(p, i, ni, nd, m, gw, gt);
                     take(m);
                 }
                 __syncwarp();
@@ -618,7 +634,8 @@ __global__ void __launch_bounds__(256) leaf_topk_kernel(const float* __restrict_
                                                         const uint32_t* __restrict__ ids,
                                                         const LeafRef* __restrict__ leaves, uint32_t K,
                                                         uint32_t tile_rows, float* __restrict__ kd,
-                                                        uint32_t* __restrict__ ki, uint32_t* __restrict__ ksz) {
+                                                        uint32_t* __restrict__ ki, uint32_t* __restrict__ ksz,
+                                                        uint32_t mode) {
     extern __shared__ __align__(16) unsigned char sm[];
     const LeafRef lf = leaves[blockIdx.x];
     const uint32_t rb = blockIdx.y * kLeafRows;
@@ -672,14 +689,22 @@ __global__ void __launch_bounds__(256) leaf_topk_kernel(const float* __restrict_
             for (uint32_t b0 = 0; b0 < tr; b0 += 64) {
                 const uint32_t bm = min(64u, tr - b0);
                 // distances for the batch
-                for (uint32_t r0 = 0; r0 < bm; r0 += 8) {
-                    const uint32_t idx = r0 + gw;
-                    const bool ok = idx < bm;
-                    const uint32_t q = b0 + (ok ? idx : r0);
-                    const float ip = group_ip(rv + (size_t)r * stride, tv + (size_t)q * stride, dim, gt, kAll);
-                    if (ok && gt == 0) {
-                        wd[idx] = norm_d2(nr, norms[tid[q]], ip);
+                if (mode == kKeyIpDist) {
+                    for (uint32_t idx = lane; idx < bm; idx += 32) {
+                        const uint32_t q = b0 + idx;
+                        wd[idx] = ip_dist_seq(rv + (size_t)r * stride, tv + (size_t)q * stride, dim);
                         wi[idx] = tid[q];
+                    }
+                } else {
+                    for (uint32_t r0 = 0; r0 < bm; r0 += 8) {
+                        const uint32_t idx = r0 + gw;
+                        const bool ok = idx < bm;
+                        const uint32_t q = b0 + (ok ? idx : r0);
+                        const float ip = group_ip(rv + (size_t)r * stride, tv + (size_t)q * stride, dim, gt, kAll);
+                        if (ok && gt == 0) {
+                            wd[idx] = mode == kKeyNegIp ? -ip : norm_d2(nr, norms[tid[q]], ip);
+                            wi[idx] = tid[q];
+                        }
                     }
                 }
                 __syncwarp();
@@ -841,7 +866,7 @@ __global__ void init_lists_kernel(float* kd, uint32_t* ki, uint32_t* ksz, uint64
 // project's counter hash instead of mt19937; the id may be the row itself).
 __global__ void random_fill_kernel(const float* __restrict__ x, const float* __restrict__ norms, uint64_t n,
                                    uint32_t stride, uint32_t dim, uint64_t seed, uint32_t K, float* kd, uint32_t* ki,
-                                   uint32_t* ksz) {
+                                   uint32_t* ksz, uint32_t ip) {
     const uint32_t lane = threadIdx.x & 31u, gt = lane & 3u;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
@@ -852,8 +877,10 @@ __global__ void random_fill_kernel(const float* __restrict__ x, const float* __r
         uint32_t* id = ki + i * K;
         for (uint32_t t = 0; t < miss; t++) {
             const uint32_t r = (uint32_t)(hash64(hash64(seed + 0x51ED270Bull) ^ (i << 20) ^ t) % n);
-            const float ip = group_ip(x + i * stride, x + (uint64_t)r * stride, dim, gt, kAll);
-            const float v = norm_d2(norms[i], norms[r], ip);
+            // every lane forms the same key (the ip metric's is one sequential sum)
+            const float v = ip ? ip_dist_seq(x + i * stride, x + (uint64_t)r * stride, dim)
+                               : norm_d2(norms[i], norms[r], group_ip(x + i * stride, x + (uint64_t)r * stride, dim,
+                                                                     gt, kAll));
             bool dup = false;
             for (uint32_t s = lane; s < size; s += 32) dup |= id[s] == r;
             dup = __any_sync(kAll, dup);
@@ -958,9 +985,10 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     const size_t per_warp = gather_smem_words(p.ef, topk_cap, p.sort_words, hash_cap) * 4;
     const size_t smem = per_warp * warps_per_block;
     if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "explore range %u too large", p.ef);
-    ANQI_CUDA(c, cudaFuncSetAttribute(gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto* kern = p.ip ? gather_kernel<true> : gather_kernel<false>;
+    ANQI_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gather_kernel, 32 * warps_per_block, smem));
+    ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps_per_block, smem));
     if (per_sm < 1) return fail(c, ANQI_ERR_DEVICE, "gather kernel does not fit on an SM");
     uint32_t blocks = std::min<uint64_t>((uint64_t)per_sm * c->sm_count, (p.n + warps_per_block - 1) / warps_per_block);
     const uint32_t slots = blocks * warps_per_block;
@@ -1001,7 +1029,7 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
         c->l2_window = false;
     }
     ANQI_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-    gather_kernel<<<blocks, 32 * warps_per_block, smem, c->stream>>>(p);
+    kern<<<blocks, 32 * warps_per_block, smem, c->stream>>>(p);
     ANQI_CUDA(c, cudaGetLastError());
     ANQI_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     rc = check_device_error(c, "gather");  // synchronizes
@@ -1158,7 +1186,7 @@ static int run_select_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_
 // init_knn over leaves; lists kd/ki/ksz already initialised.
 static int run_leaf_topk(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
                          const uint32_t* d_ids, const std::vector<LeafRef>& leaves, uint32_t K, DevBuf& kd, DevBuf& ki,
-                         DevBuf& ksz) {
+                         DevBuf& ksz, uint32_t mode = kKeyL2) {
     if (leaves.empty()) return ANQI_OK;
     uint32_t maxcnt = 0;
     for (const LeafRef& l : leaves) maxcnt = std::max(maxcnt, l.cnt);
@@ -1167,6 +1195,7 @@ static int run_leaf_topk(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n,
     const size_t smem = ((size_t)kLeafRows * stride + (size_t)tile_rows * stride + 4 * (size_t)kLeafRows * K +
                          2 * nwarp * 64 + tile_rows + 2 * kLeafRows) * 4;
     if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "init_knn tile does not fit (dim %u, K %u)", dim, K);
+    if (mode > kKeyNegIp) return fail(c, ANQI_ERR_ARGS, "unknown key mode %u", mode);
     ANQI_CUDA(c, cudaFuncSetAttribute(leaf_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     TmpBuf dl(c);
     int rc = h2d(c, dl, leaves.data(), leaves.size() * sizeof(LeafRef));
@@ -1174,7 +1203,7 @@ static int run_leaf_topk(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n,
     dim3 grid((unsigned)leaves.size(), (maxcnt + kLeafRows - 1) / kLeafRows);
     leaf_topk_kernel<<<grid, 32 * nwarp, smem, c->stream>>>(dx.as<float>(), dn.as<float>(), n, stride, dim, d_ids,
                                                             dl.as<LeafRef>(), K, tile_rows, kd.as<float>(),
-                                                            ki.as<uint32_t>(), ksz.as<uint32_t>());
+                                                            ki.as<uint32_t>(), ksz.as<uint32_t>(), mode);
     ANQI_CUDA(c, cudaGetLastError());
     return sync(c);
 }
@@ -1400,8 +1429,16 @@ int anqi_graph_tree_copy(anqi_ctx* h, uint32_t* left, uint32_t* right, float* of
 
 int anqi_aknn_init(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint64_t* leaf_off,
                    const uint32_t* leaf_ids, uint64_t n_leaves, uint32_t K, uint32_t* ids, float* dists) {
-    if (!h || !x || !leaf_off || !leaf_ids || !ids || !dists || n == 0 || dim == 0 || K == 0 || K > 256)
+    return anqi_aknn_init_metric(h, x, n, dim, leaf_off, leaf_ids, n_leaves, K, ANQI_METRIC_L2, ids, dists);
+}
+
+int anqi_aknn_init_metric(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint64_t* leaf_off,
+                          const uint32_t* leaf_ids, uint64_t n_leaves, uint32_t K, uint32_t metric, uint32_t* ids,
+                          float* dists) {
+    if (!h || !x || !leaf_off || !leaf_ids || !ids || !dists || n == 0 || dim == 0 || K == 0 || K > 256 ||
+        metric > ANQI_METRIC_IP)
         return ANQI_ERR_ARGS;
+    const uint32_t mode = metric == ANQI_METRIC_IP ? kKeyIpDist : kKeyL2;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     const uint32_t xs = round_up(dim, 8);
@@ -1420,7 +1457,7 @@ int anqi_aknn_init(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const 
         if (l < n_leaves)
             for (uint64_t a = leaf_off[l]; a < leaf_off[l + 1] && !conflict; a++) conflict = seen[leaf_ids[a]];
         if (l == n_leaves || conflict) {
-            if ((rc = run_leaf_topk(c, dx, dn, n, xs, dim, dids.as<uint32_t>(), batch, K, kd, ki, ksz))) return rc;
+            if ((rc = run_leaf_topk(c, dx, dn, n, xs, dim, dids.as<uint32_t>(), batch, K, kd, ki, ksz, mode))) return rc;
             for (uint64_t r : batch_rows) seen[r] = 0;
             batch.clear();
             batch_rows.clear();
@@ -1438,7 +1475,14 @@ int anqi_aknn_init(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const 
 
 int anqi_aknn_gather(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids, const float* g_vals,
                      uint32_t K, uint32_t ef, uint32_t cap, uint32_t out_k, uint32_t* ids, float* dists) {
-    if (!h || !x || !g_ids || !g_vals || !ids || !dists || n == 0 || K == 0 || ef == 0 || out_k == 0 || out_k > 1024)
+    return anqi_aknn_gather_metric(h, x, n, dim, g_ids, g_vals, K, ef, cap, out_k, ANQI_METRIC_L2, ids, dists);
+}
+
+int anqi_aknn_gather_metric(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids,
+                            const float* g_vals, uint32_t K, uint32_t ef, uint32_t cap, uint32_t out_k, uint32_t metric,
+                            uint32_t* ids, float* dists) {
+    if (!h || !x || !g_ids || !g_vals || !ids || !dists || n == 0 || K == 0 || ef == 0 || out_k == 0 || out_k > 1024 ||
+        metric > ANQI_METRIC_IP)
         return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
@@ -1458,6 +1502,7 @@ int anqi_aknn_gather(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, cons
     p.ef = ef;
     p.cap = cap;
     p.mode = kModeAknn;
+    p.ip = metric == ANQI_METRIC_IP;
     p.out_k = out_k;
     p.out_ids = oi.as<uint32_t>();
     p.out_d = od.as<float>();
@@ -1469,11 +1514,13 @@ int anqi_aknn_gather(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, cons
 int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, const anqi_aknn_params* ap, uint32_t* ids,
                     float* dists, anqi_build_stats* st) {
     if (!h || !base || !ap || !ids || !dists || n == 0 || d == 0 || ap->k == 0 || ap->k > 256 || ap->trees == 0 ||
-        ap->leaf == 0 || ap->ef == 0)
+        ap->leaf == 0 || ap->ef == 0 || ap->metric > ANQI_METRIC_IP)
         return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     if (n <= ap->k) return fail(c, ANQI_ERR_FORMAT, "n must exceed K");
+    const bool ip = ap->metric == ANQI_METRIC_IP;
+    if (ip && ap->nn_iters > 0) return fail(c, ANQI_ERR_ARGS, "LocalJoin rounds are implemented for metric l2 only");
     const auto t0 = Clock::now();
     const uint32_t xs = round_up(d, 8);
     const uint32_t K = ap->k;
@@ -1483,7 +1530,7 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
     auto t = Clock::now();
     ForestOut f;
     const uint32_t cap_nodes = (uint32_t)std::min<uint64_t>(16 * n / ap->leaf + 1024, 4 * n + 8);
-    rc = build_forest(c, dx.as<float>(), n, d, xs, ap->trees, ap->leaf, 100, ap->seed, cap_nodes, f);
+    rc = build_forest(c, dx.as<float>(), n, d, xs, ap->trees, ap->leaf, 100, ap->seed, cap_nodes, f, ip);
     const double forest_ms = ms_since(t);
     t = Clock::now();
     if (!rc) {
@@ -1499,7 +1546,7 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
                 }
             }
         // the tensor-core tiles hold rows of up to 256 (padded) dimensions
-        if (ap->precision == 1 && round_up(d, 16u) <= 256) {
+        if (ap->precision == 1 && !ip && round_up(d, 16u) <= 256) {
             // BF16 tensor-core leaf tiles: candidates per tree, then the merge
             TcPrep tp;
             // candidate buffers (n x cap entries; GBs at 1M) are kept by the
@@ -1548,7 +1595,8 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
             tc_release(c, tp);
         } else {
             for (uint32_t tr = 0; tr < ap->trees && !rc; tr++)
-                rc = run_leaf_topk(c, dx, dn, n, xs, d, f.perm.as<uint32_t>(), tree_leaves[tr], K, kd, ki, ksz);
+                rc = run_leaf_topk(c, dx, dn, n, xs, d, f.perm.as<uint32_t>(), tree_leaves[tr], K, kd, ki, ksz,
+                                   ip ? kKeyIpDist : kKeyL2);
         }
     }
     // tree 0's leaf order groups the rows of one leaf: the gather runs them together
@@ -1561,7 +1609,7 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
     release(c, f.hyper);
     if (rc) return rc;
     random_fill_kernel<<<c->sm_count * 8, 128, 0, c->stream>>>(dx.as<float>(), dn.as<float>(), n, xs, d, ap->seed, K,
-                                                               kd.as<float>(), ki.as<uint32_t>(), ksz.as<uint32_t>());
+                                                               kd.as<float>(), ki.as<uint32_t>(), ksz.as<uint32_t>(), ip);
     ANQI_CUDA(c, cudaGetLastError());
     if ((rc = sync(c))) return rc;
     const double init_ms = ms_since(t);
@@ -1594,6 +1642,7 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
     p.ef = ap->ef;
     p.cap = std::max<uint32_t>(K, (ap->ef_alpha ? ap->ef_alpha : 8) * ap->ef);
     p.mode = kModeAknn;
+    p.ip = ip;
     p.out_k = K;
     p.out_ids = oi.as<uint32_t>();
     p.out_d = od.as<float>();
@@ -1628,7 +1677,12 @@ __global__ void iota_kernel(uint32_t* a, uint64_t n) {
 }
 
 int anqi_exact_topk(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, uint32_t K, uint32_t* ids, float* keys) {
-    if (!h || !base || !ids || !keys || d == 0 || K == 0 || K > 256) return ANQI_ERR_ARGS;
+    return anqi_exact_topk_metric(h, base, n, d, K, ANQI_METRIC_L2, ids, keys);
+}
+
+int anqi_exact_topk_metric(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, uint32_t K, uint32_t metric,
+                           uint32_t* ids, float* keys) {
+    if (!h || !base || !ids || !keys || d == 0 || K == 0 || K > 256 || metric > ANQI_METRIC_IP) return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     if (K >= n) return fail(c, ANQI_ERR_ARGS, "require K < base vector count");
@@ -1641,7 +1695,9 @@ int anqi_exact_topk(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, uint
     iota_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(dids.as<uint32_t>(), n);
     ANQI_CUDA(c, cudaGetLastError());
     std::vector<LeafRef> all{{0, (uint32_t)n, 0}};
-    if ((rc = run_leaf_topk(c, dx, dn, n, xs, d, dids.as<uint32_t>(), all, K, kd, ki, ksz))) return rc;
+    if ((rc = run_leaf_topk(c, dx, dn, n, xs, d, dids.as<uint32_t>(), all, K, kd, ki, ksz,
+                            metric == ANQI_METRIC_IP ? kKeyNegIp : kKeyL2)))
+        return rc;
     if ((rc = d2h(c, ids, ki, n * K * 4)) || (rc = d2h(c, keys, kd, n * K * 4))) return rc;
     return sync(c);
 }

@@ -36,12 +36,15 @@ __device__ __forceinline__ uint64_t node_key(uint64_t seed, uint32_t tree, uint3
     return hash64(hash64(seed ^ ((uint64_t)tree << 32)) ^ (uint64_t)node);
 }
 
-// One warp per splitting node: pivots, hyperplane, midpoint, offset.
+// One warp per splitting node: pivots, hyperplane, midpoint, offset.  The
+// angular form (the ip metric, rptrees.h:41-52) splits through the origin by
+// the normalized difference of the unit-scaled pivots: x0/|x0| - x1/|x1|,
+// divided by its norm; a norm below 1e-6 counts as 1.
 __global__ void forest_hyperplane_kernel(const float* __restrict__ x, uint32_t stride, uint32_t dim, uint64_t n,
                                          const uint32_t* __restrict__ perm, const SplitNode* __restrict__ nodes,
                                          uint32_t n_split, uint64_t seed, uint32_t cap_nodes,
                                          float* __restrict__ hyper, float* __restrict__ mid,
-                                         float* __restrict__ offset) {
+                                         float* __restrict__ offset, int angular) {
     const uint32_t lane = threadIdx.x & 31u, gt = lane & 3u;
     const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (w >= n_split) return;
@@ -55,6 +58,21 @@ __global__ void forest_hyperplane_kernel(const float* __restrict__ x, uint32_t s
     const float* x1 = x + (uint64_t)pt[r1] * stride;
     float* hp = hyper + ((uint64_t)nd.tree * cap_nodes + nd.local) * stride;
     float* md = mid + (uint64_t)w * stride;
+    if (angular) {
+        float n0 = __fsqrt_rn(group_ip(x0, x0, dim, gt, kAll));
+        float n1 = __fsqrt_rn(group_ip(x1, x1, dim, gt, kAll));
+        if (fabsf(n0) < kSplitEps) n0 = 1.0f;
+        if (fabsf(n1) < kSplitEps) n1 = 1.0f;
+        for (uint32_t j = lane; j < stride; j += 32)
+            hp[j] = j < dim ? __fsub_rn(__fdiv_rn(x0[j], n0), __fdiv_rn(x1[j], n1)) : 0.f;
+        __syncwarp();
+        float hn = __fsqrt_rn(group_ip(hp, hp, dim, gt, kAll));
+        if (fabsf(hn) < kSplitEps) hn = 1.0f;
+        __syncwarp();
+        for (uint32_t j = lane; j < dim; j += 32) hp[j] = __fdiv_rn(hp[j], hn);
+        if (lane == 0) offset[w] = 0.0f;
+        return;
+    }
     for (uint32_t j = lane; j < stride; j += 32) {
         const bool in = j < dim;
         hp[j] = in ? __fsub_rn(x0[j], x1[j]) : 0.f;
@@ -169,7 +187,7 @@ __global__ void iota_trees_kernel(uint32_t* perm, uint64_t n, uint32_t trees) {
 }
 
 int build_forest(Ctx* c, const float* d_x, uint64_t n, uint32_t dim, uint32_t stride, uint32_t trees,
-                 uint32_t leaf, uint32_t max_depth, uint64_t seed, uint32_t cap_nodes, ForestOut& out) {
+                 uint32_t leaf, uint32_t max_depth, uint64_t seed, uint32_t cap_nodes, ForestOut& out, int angular) {
     if (n == 0 || trees == 0 || leaf == 0 || cap_nodes < 1) return fail(c, ANQI_ERR_ARGS, "invalid forest arguments");
     if (n >= 0xFFFFFFFFull) return fail(c, ANQI_ERR_ARGS, "forest needs n < 2^32");
     out.trees = trees;
@@ -229,7 +247,7 @@ int build_forest(Ctx* c, const float* d_x, uint64_t n, uint32_t dim, uint32_t st
             return rc;
         forest_hyperplane_kernel<<<(ns + 3) / 4, 128, 0, c->stream>>>(
             d_x, stride, dim, n, out.perm.as<uint32_t>(), dnodes.as<SplitNode>(), ns, seed, cap_nodes,
-            out.hyper.as<float>(), dmid.as<float>(), doff.as<float>());
+            out.hyper.as<float>(), dmid.as<float>(), doff.as<float>(), angular);
         forest_sides_kernel<<<nc, 256, 0, c->stream>>>(d_x, stride, dim, n, out.perm.as<uint32_t>(),
                                                        dnodes.as<SplitNode>(), dchunks.as<Chunk>(), seed, cap_nodes,
                                                        out.hyper.as<float>(), doff.as<float>(), side.as<uint8_t>(),
@@ -310,8 +328,17 @@ extern "C" int anqi_rp_forest(anqi_ctx* h, const float* x, uint64_t n, uint32_t 
                               uint32_t leaf_size, uint32_t max_depth, uint64_t seed, uint32_t cap_nodes,
                               uint32_t* n_nodes, uint32_t* left, uint32_t* right, float* offset, float* hyperplane,
                               uint32_t* leaf_off, uint32_t* leaf_cnt, uint32_t* perm) {
+    return anqi_rp_forest_metric(h, x, n, dim, trees, leaf_size, max_depth, seed, cap_nodes, ANQI_METRIC_L2, n_nodes,
+                                 left, right, offset, hyperplane, leaf_off, leaf_cnt, perm);
+}
+
+extern "C" int anqi_rp_forest_metric(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, uint32_t trees,
+                                     uint32_t leaf_size, uint32_t max_depth, uint64_t seed, uint32_t cap_nodes,
+                                     uint32_t metric, uint32_t* n_nodes, uint32_t* left, uint32_t* right,
+                                     float* offset, float* hyperplane, uint32_t* leaf_off, uint32_t* leaf_cnt,
+                                     uint32_t* perm) {
     if (!h || !x || !n_nodes || !left || !right || !offset || !hyperplane || !leaf_off || !leaf_cnt || !perm ||
-        dim == 0)
+        dim == 0 || metric > ANQI_METRIC_IP)
         return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
@@ -320,7 +347,8 @@ extern "C" int anqi_rp_forest(anqi_ctx* h, const float* x, uint64_t n, uint32_t 
     int rc = upload_padded(c, dx, x, n, dim, stride);
     if (rc) return rc;
     ForestOut f;
-    rc = build_forest(c, dx.as<float>(), n, dim, stride, trees, leaf_size, max_depth, seed, cap_nodes, f);
+    rc = build_forest(c, dx.as<float>(), n, dim, stride, trees, leaf_size, max_depth, seed, cap_nodes, f,
+                      metric == ANQI_METRIC_IP);
     if (rc) {
         release(c, f.perm);
         release(c, f.hyper);

@@ -3,6 +3,7 @@
 // Reference: tools/dataset_gt.cpp:270-313 (--mode ground-truth): for every
 // query q, all base rows j with key = |q|^2 + |b_j|^2 - 2 <q, b_j> <= rk2[j],
 // sorted by (key, id); FP32 in the AVX lane order, so the CSR is bit-exact.
+// The ip metric's key is -<q, b_j> (dataset_gt.cpp:288).
 // Two passes over the same tiles: count hits per query, then write them at
 // scanned offsets and sort each query's segment.
 #include <algorithm>
@@ -20,7 +21,7 @@ __global__ void __launch_bounds__(256) rknn_gt_kernel(const float* __restrict__ 
                                                       uint32_t stride, uint32_t d, const float* __restrict__ rk2,
                                                       uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off,
                                                       uint32_t* __restrict__ fill, uint32_t* __restrict__ out_id,
-                                                      float* __restrict__ out_key) {
+                                                      float* __restrict__ out_key, uint32_t is_ip) {
     extern __shared__ __align__(16) unsigned char sm[];
     float* qv = reinterpret_cast<float*>(sm);            // kGtQ x stride
     float* tv = qv + (size_t)kGtQ * stride;              // kGtTile x stride
@@ -49,7 +50,7 @@ __global__ void __launch_bounds__(256) rknn_gt_kernel(const float* __restrict__ 
                 const bool ok = j < tr;
                 const uint32_t jj = ok ? j : b0;
                 const float ip = group_ip(qv + (size_t)r * stride, tv + (size_t)jj * stride, d, gt, kAll);
-                const float key = __fsub_rn(__fadd_rn(qn[r], bn[c0 + jj]), __fmul_rn(2.0f, ip));
+                const float key = is_ip ? -ip : __fsub_rn(__fadd_rn(qn[r], bn[c0 + jj]), __fmul_rn(2.0f, ip));
                 const bool hit = ok && gt == 0 && key <= rk2[c0 + jj];
                 if (hit) {
                     if (off) {
@@ -125,7 +126,15 @@ using namespace anqi;
 extern "C" int anqi_rknn_ground_truth(anqi_ctx* h, const float* base, uint64_t n, const float* query, uint64_t nq,
                                       uint32_t d, const float* rk2, uint32_t* off, uint32_t* ids, float* keys,
                                       uint64_t cap, uint64_t* total) {
-    if (!h || !base || !query || !rk2 || !off || n == 0 || nq == 0 || d == 0) return ANQI_ERR_ARGS;
+    return anqi_rknn_ground_truth_metric(h, base, n, query, nq, d, rk2, ANQI_METRIC_L2, off, ids, keys, cap, total);
+}
+
+extern "C" int anqi_rknn_ground_truth_metric(anqi_ctx* h, const float* base, uint64_t n, const float* query,
+                                             uint64_t nq, uint32_t d, const float* rk2, uint32_t metric, uint32_t* off,
+                                             uint32_t* ids, float* keys, uint64_t cap, uint64_t* total) {
+    if (!h || !base || !query || !rk2 || !off || n == 0 || nq == 0 || d == 0 || metric > ANQI_METRIC_IP)
+        return ANQI_ERR_ARGS;
+    const uint32_t is_ip = metric == ANQI_METRIC_IP;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     const uint32_t xs = round_up(d, 8);
@@ -144,7 +153,7 @@ extern "C" int anqi_rknn_ground_truth(anqi_ctx* h, const float* base, uint64_t n
     const unsigned blocks = (unsigned)((nq + kGtQ - 1) / kGtQ);
     rknn_gt_kernel<<<blocks, 256, smem, c->stream>>>(db.as<float>(), dbn.as<float>(), n, dq.as<float>(), nq, xs, d,
                                                      dr.as<float>(), dcnt.as<uint32_t>(), nullptr, nullptr, nullptr,
-                                                     nullptr);
+                                                     nullptr, is_ip);
     ANQI_CUDA(c, cudaGetLastError());
     if ((rc = device_scan(c, dcnt.as<uint32_t>(), doff.as<uint64_t>(), nq))) return rc;
     std::vector<uint64_t> hoff(nq + 1);
@@ -156,7 +165,7 @@ extern "C" int anqi_rknn_ground_truth(anqi_ctx* h, const float* base, uint64_t n
     if ((rc = ensure(c, did, tot * 4 + 4)) || (rc = ensure(c, dkey, tot * 4 + 4))) return rc;
     rknn_gt_kernel<<<blocks, 256, smem, c->stream>>>(db.as<float>(), dbn.as<float>(), n, dq.as<float>(), nq, xs, d,
                                                      dr.as<float>(), nullptr, doff.as<uint64_t>(), dfill.as<uint32_t>(),
-                                                     did.as<uint32_t>(), dkey.as<float>());
+                                                     did.as<uint32_t>(), dkey.as<float>(), is_ip);
     ANQI_CUDA(c, cudaGetLastError());
     uint64_t maxm = 0;
     for (uint64_t i = 0; i < nq; i++) maxm = std::max(maxm, hoff[i + 1] - hoff[i]);

@@ -40,6 +40,7 @@ struct QueryIndex {
     uint32_t bstride = 0, lstride = 0;  // padded row strides (floats, multiple of 8)
     uint32_t tree_nodes = 0, troot = 0;
     double scale = 0, mstar2 = 0;
+    uint32_t metric = 0;  // ANQI_METRIC_L2 / ANQI_METRIC_IP
     DevBuf base, lifted, onorm, deg, links;
     DevBuf tleft, tright, toffset, thyper, tleaf;
     // objects are held renumbered in breadth-first order of the graph:
@@ -73,6 +74,7 @@ struct Batch {
     DevBuf pred_off, cand_off;           // CSR offsets (device)
     DevBuf pred_csr, cand_csr;
     DevBuf entry, enode, order, leaf_cnt;  // entry object / leaf node per query, leaf-ordered work list
+    DevBuf qr2;                            // ip metric: per-query range radius (float, rounded down)
     uint64_t pred_cap = 0, cand_cap = 0;
     bool have_results = false;
     bool have_cands = false;
@@ -120,7 +122,8 @@ struct Ctx {
                 &ix.thyper, &ix.tleaf, &ix.perm, &vf.coeff, &vf.codes_t, &vf.mu, &vf.basis, &vf.codebook, &batch.q,
                 &batch.qL, &batch.qslot, &batch.npred, &batch.ncand, &batch.ndist, &batch.nexp, &batch.nflood,
                 &batch.pred_at, &batch.cand_at, &batch.pred_buf, &batch.cand_buf, &batch.pred_off,
-                &batch.cand_off, &batch.pred_csr, &batch.cand_csr, &err, &counters, &vis_bits, &vis_log,
+                &batch.cand_off, &batch.pred_csr, &batch.cand_csr, &batch.entry, &batch.enode, &batch.order,
+                &batch.leaf_cnt, &batch.qr2, &err, &counters, &vis_bits, &vis_log,
                 &cand_scratch, &thr_table, &gt_off, &gt_ids, &eval_rows, &eval_sums, &vis_gtab,
                 &init_cnt, &init_cid, &init_key, &g_bits, &g_vlog, &g_pd, &g_pi, &g_gtab};
     }
@@ -165,7 +168,7 @@ struct ForestOut {
     DevBuf perm, hyper;  // device; released by the caller
 };
 int build_forest(Ctx* c, const float* d_x, uint64_t n, uint32_t dim, uint32_t stride, uint32_t trees, uint32_t leaf,
-                 uint32_t max_depth, uint64_t seed, uint32_t cap_nodes, ForestOut& out);
+                 uint32_t max_depth, uint64_t seed, uint32_t cap_nodes, ForestOut& out, int angular = 0);
 // Exclusive scan of n u32 counts into n + 1 u64 offsets (device).
 int device_scan(Ctx* c, const uint32_t* d_in, uint64_t* d_out, uint64_t n);
 

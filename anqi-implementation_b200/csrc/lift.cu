@@ -1,7 +1,7 @@
 // The d+2 lift that turns "q inside o's r_K ball" into one global range test.
 //
-// Reference: src/rknn_query.cpp:2203-2235 (anyk_lift, L2, graph radius = the
-// AKNN rank-K cutoff of each object).  All arithmetic is double with explicit
+// Reference: src/rknn_query.cpp:2203-2235 (anyk_lift, graph radius = the
+// AKNN rank-K cutoff of each object; L2, or the ip metric's s^2 r coordinate).  All arithmetic is double with explicit
 // _rn operations (no contraction), matching the reference compiled with
 // -std=c++17.  The sum of squared norms is accumulated per row, then over rows
 // in index order -- the order of the reference's OpenMP reduction at one
@@ -35,7 +35,7 @@ __global__ void lift_scale_kernel(const double* __restrict__ rs, uint64_t n, dou
 
 __global__ void lift_rows_kernel(const float* __restrict__ base, uint64_t n, uint32_t d, const float* __restrict__ radius,
                                  const double* __restrict__ sc, float* __restrict__ lifted,
-                                 unsigned long long* __restrict__ maxbits) {
+                                 unsigned long long* __restrict__ maxbits, uint32_t ip) {
     const double s = sc[0], sc2 = sc[1];
     const uint32_t dout = d + 2;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -47,7 +47,9 @@ __global__ void lift_rows_kernel(const float* __restrict__ base, uint64_t n, uin
             h[j] = __double2float_rn(v);
             nr2 = __dadd_rn(nr2, __dmul_rn(v, v));
         }
-        const float hd = __double2float_rn(__dmul_rn(0.5, __dsub_rn(__dmul_rn((double)radius[i], sc2), nr2)));
+        // the ip metric's coordinate is s^2 r (rknn_query.cpp:2227)
+        const float hd = ip ? __double2float_rn(__dmul_rn((double)radius[i], sc2))
+                            : __double2float_rn(__dmul_rn(0.5, __dsub_rn(__dmul_rn((double)radius[i], sc2), nr2)));
         h[d] = hd;
         const double hn2 = __dadd_rn(nr2, __dmul_rn((double)hd, (double)hd));
         atomicMax(maxbits, (unsigned long long)__double_as_longlong(hn2));
@@ -77,7 +79,13 @@ extern "C" {
 
 int anqi_lift(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, const float* radius, float* lifted,
               double* mstar2, double* scale) {
-    if (!h || !base || !radius || !lifted || !mstar2 || !scale || n == 0 || d == 0) return ANQI_ERR_ARGS;
+    return anqi_lift_metric(h, base, n, d, radius, ANQI_METRIC_L2, lifted, mstar2, scale);
+}
+
+int anqi_lift_metric(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, const float* radius, uint32_t metric,
+                     float* lifted, double* mstar2, double* scale) {
+    if (!h || !base || !radius || !lifted || !mstar2 || !scale || n == 0 || d == 0 || metric > ANQI_METRIC_IP)
+        return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     TmpBuf db(c), dr(c), drs(c), dsc(c), dl(c), dmax(c);
@@ -90,7 +98,8 @@ int anqi_lift(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, const floa
     lift_rowsum_kernel<<<blocks, 256, 0, c->stream>>>(db.as<float>(), n, d, drs.as<double>());
     lift_scale_kernel<<<1, 32, 0, c->stream>>>(drs.as<double>(), n, dsc.as<double>());
     lift_rows_kernel<<<blocks, 256, 0, c->stream>>>(db.as<float>(), n, d, dr.as<float>(), dsc.as<double>(),
-                                                   dl.as<float>(), dmax.as<unsigned long long>());
+                                                   dl.as<float>(), dmax.as<unsigned long long>(),
+                                                   metric == ANQI_METRIC_IP);
     lift_pad_kernel<<<blocks, 256, 0, c->stream>>>(n, d, dmax.as<unsigned long long>(), dl.as<float>(),
                                                   dsc.as<double>() + 3);
     ANQI_CUDA(c, cudaGetLastError());

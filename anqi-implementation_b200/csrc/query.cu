@@ -44,8 +44,10 @@ struct SearchParams {
     uint64_t n;
     uint32_t dim, d, lstride, bstride, degree, troot;
     uint32_t stage_rows;  // rows per staging round: 8, 4 or 2 (long rows)
-    double scale, R2;
+    double scale, R2, mstar2;
     float R2f;  // the largest float <= R2 (float distances compare the same against either)
+    uint32_t ip;  // the ip metric: per-query R2 (qR2f) and postfilter key -<o, q>
+    float* qR2f;  // ip: per query, the largest float <= |s q|^2 + 1 + M*^2 (rknn_entry_kernel)
     const float* thr;  // slot-major thresholds
     const float* queries;
     const uint32_t* entry;  // entry object per query (rknn_entry_kernel)
@@ -247,11 +249,11 @@ __device__ __forceinline__ bool fresh_distances(const SearchParams& p, const flo
 // Appends fresh neighbours within R2 to the candidate / flood list (visit
 // order).  For a float x, (double)x <= R2 exactly when x <= R2f, the largest
 // float not above R2.
-__device__ __forceinline__ void append_in_range(const SearchParams& p, const float* nd, const uint32_t* ni,
+__device__ __forceinline__ void append_in_range(const SearchParams& p, float r2f, const float* nd, const uint32_t* ni,
                                                 uint32_t m, uint32_t* cl, uint32_t& ncand, bool& overflow,
                                                 uint32_t lane) {
-    const bool in0 = lane < m && nd[lane] <= p.R2f;
-    const bool in1 = lane + 32 < m && nd[lane + 32] <= p.R2f;
+    const bool in0 = lane < m && nd[lane] <= r2f;
+    const bool in1 = lane + 32 < m && nd[lane + 32] <= r2f;
     const unsigned b0 = __ballot_sync(kFull, in0), b1 = __ballot_sync(kFull, in1);
     const uint32_t c0 = __popc(b0), lt = lanemask_lt();
     const uint32_t pos0 = ncand + __popc(b0 & lt), pos1 = ncand + c0 + __popc(b1 & lt);
@@ -326,6 +328,7 @@ __global__ void __launch_bounds__(32 * kWpb, 32 / kWpb) rknn_search_kernel(Searc
         const uint32_t L = min(p.qL ? p.qL[qi] : p.L_all, p.L_max);
         const uint32_t tslot = p.qslot ? p.qslot[qi] : p.slot_all;
         const float* q = p.queries + (size_t)qi * p.bstride;
+        const float r2f = p.ip ? p.qR2f[qi] : p.R2f;
         // query lift, rknn_query.cpp:2724-2729 (in the rows' column order)
         for (uint32_t j = lane; j < ls; j += 32) {
             float v = 0.0f;
@@ -360,7 +363,7 @@ __global__ void __launch_bounds__(32 * kWpb, 32 / kWpb) rknn_search_kernel(Searc
         }
         uint32_t nlog = 0, nvis = 1, ncand = 0, nexp = 0, nfl = 0;
         bool overflow = false;
-        if (dep <= p.R2f) {
+        if (dep <= r2f) {
             if (lane == 0) cl[0] = ep;
             ncand = 1;
         }
@@ -430,7 +433,7 @@ __global__ void __launch_bounds__(32 * kWpb, 32 / kWpb) rknn_search_kernel(Searc
             uint32_t mk = 0;
             if (m != 0) {
                 if (!fresh_distances<kDim>(p, qhat, ni, nd, m, stage, bar, ph, lane)) return;
-                append_in_range(p, nd, ni, m, cl, ncand, overflow, lane);
+                append_in_range(p, r2f, nd, ni, m, cl, ncand, overflow, lane);
                 if (!flood) {
                     const bool full = size >= L;
                     mk = sort_fresh_kept<PermOrder, true>(nd, ni, m, full, full ? bd[L - 1] : 0.f,
@@ -508,7 +511,8 @@ __global__ void __launch_bounds__(32 * kWpb, 32 / kWpb) rknn_search_kernel(Searc
                 for (uint32_t i = lane; i < ncand; i += 32) p.cand_buf[cat + i] = p.perm[cl[i]];
             __syncwarp();
         }
-        // rknn_query.cpp:2555-2561: key = IP(o,o) + IP(q,q) - 2 IP(o,q) <= (double) thr[o]
+        // rknn_query.cpp:2555-2561: key = IP(o,o) + IP(q,q) - 2 IP(o,q) <= (double) thr[o];
+        // the ip metric's key is -IP(o,q)
         const float qn = group_ip(q, q, p.d, gt, kFull);
         const float* thr = p.thr + (size_t)tslot * p.n;
         uint32_t npred = 0;
@@ -528,7 +532,7 @@ __global__ void __launch_bounds__(32 * kWpb, 32 / kWpb) rknn_search_kernel(Searc
             const float ip = G == 4 ? group_ip(rr, q, p.d, pt, kFull)
                                     : (G == 8 ? group_ip_w<8>(rr, q, p.d, pt, kFull)
                                               : group_ip_w<16>(rr, q, p.d, pt, kFull));
-            const float key = __fsub_rn(__fadd_rn(p.onorm[o], qn), __fmul_rn(2.0f, ip));
+            const float key = p.ip ? -ip : __fsub_rn(__fadd_rn(p.onorm[o], qn), __fmul_rn(2.0f, ip));
             const bool pass = ok && key <= thr[o];  // (double) of both sides in the reference: same order
             const unsigned b = __ballot_sync(kFull, pass && pt == 0);
             __syncwarp();
@@ -603,6 +607,17 @@ __global__ void __launch_bounds__(128) rknn_entry_kernel(SearchParams p, uint32_
             if (ep == kEmpty || ep >= p.n) ep = 0;
             entry[qi] = ep;
             enode[qi] = v;
+            if (p.ip) {
+                // rknn_query.cpp:2724-2729: qn2s sums (q_j s)^2 in index order in
+                // double (multiply, then add); R2 = qn2s + 1 + M*^2
+                const float* q = p.queries + (size_t)qi * p.bstride;
+                double qn2s = 0.0;
+                for (uint32_t j = 0; j < p.d; j++) {
+                    const double t = __dmul_rn((double)q[j], p.scale);
+                    qn2s = __dadd_rn(qn2s, __dmul_rn(t, t));
+                }
+                p.qR2f[qi] = __double2float_rd(__dadd_rn(__dadd_rn(qn2s, 1.0), p.mstar2));
+            }
         }
         __syncwarp();
     }
@@ -871,6 +886,7 @@ int anqi_index_load(anqi_ctx* h, const anqi_index_desc* x) {
     cudaSetDevice(c->device);
     if (x->degree > 64) return fail(c, ANQI_ERR_ARGS, "graph degree %u > 64 is not supported", x->degree);
     if (x->n >= 0x7FFFFFFFull) return fail(c, ANQI_ERR_ARGS, "n must be < 2^31");
+    if (x->metric > ANQI_METRIC_IP) return fail(c, ANQI_ERR_ARGS, "unknown metric %u", x->metric);
     // index.h:1840-1861 validation: degrees and neighbour ids in range
     for (uint64_t i = 0; i < x->n; i++) {
         if (x->deg[i] > x->degree) return fail(c, ANQI_ERR_FORMAT, "invalid adjacency data: deg[%llu]", (unsigned long long)i);
@@ -893,6 +909,7 @@ int anqi_index_load(anqi_ctx* h, const anqi_index_desc* x) {
     ix.lstride = round_up(x->d + 2, 8);
     ix.tree_nodes = x->tree_nodes;
     ix.troot = x->tree_nodes - 1;
+    ix.metric = x->metric;
     ix.scale = x->scale;
     ix.mstar2 = x->mstar2;
     int rc;
@@ -1087,7 +1104,8 @@ static int prepare_entries(Ctx* c, bool* ordered) {
     int rc;
     const uint32_t nq = b.nq;
     if ((rc = ensure(c, b.entry, nq * 4ull)) || (rc = ensure(c, b.enode, nq * 4ull)) ||
-        (rc = ensure(c, b.order, nq * 4ull)) || (rc = ensure(c, b.leaf_cnt, 2 * (ix.tree_nodes + 1ull) * 4)))
+        (rc = ensure(c, b.order, nq * 4ull)) || (rc = ensure(c, b.leaf_cnt, 2 * (ix.tree_nodes + 1ull) * 4)) ||
+        (ix.metric == ANQI_METRIC_IP && (rc = ensure(c, b.qr2, nq * 4ull))))
         return rc;
     SearchParams p{};
     p.queries = b.q.as<float>();
@@ -1104,6 +1122,9 @@ static int prepare_entries(Ctx* c, bool* ordered) {
     p.thyper = ix.thyper.as<float>();
     p.tleaf = ix.tleaf.as<uint32_t>();
     p.troot = ix.troot;
+    p.ip = ix.metric == ANQI_METRIC_IP;
+    p.mstar2 = ix.mstar2;
+    p.qR2f = p.ip ? b.qr2.as<float>() : nullptr;
     // 8 queries per warp (one per 4-lane group) while their rows fit 48 KB per block
     const uint32_t qpw = 4ull * 8 * 2 * ix.lstride * 4 <= 48 * 1024 ? 8u : 1u;
     const size_t smem = 4ull * qpw * 2 * ix.lstride * 4;
@@ -1159,6 +1180,9 @@ static int enqueue_search(Ctx* c, const SearchCfg& cfg, int keep_candidates, boo
     p.R2 = ix.mstar2 + 1.0;  // rknn_query.cpp:2729, eps = 0
     p.R2f = (float)p.R2;
     if ((double)p.R2f > p.R2) p.R2f = std::nextafter(p.R2f, -INFINITY);
+    p.mstar2 = ix.mstar2;
+    p.ip = ix.metric == ANQI_METRIC_IP;
+    p.qR2f = p.ip ? b.qr2.as<float>() : nullptr;
     p.thr = c->thr_table.as<float>();
     p.queries = b.q.as<float>();
     p.entry = b.entry.as<uint32_t>();

@@ -154,7 +154,8 @@ __global__ void __launch_bounds__(32 * kWarps) noalloc_search_kernel(NoAllocPara
     uint32_t* vlog = bits + p.words;
     uint32_t* cl = vlog + kLogCap;
     VisitSlot vs{bits, vlog, kLogCap, p.words};
-    const double R2 = p.ix.mstar2 + 1.0;
+    const double R2_l2 = p.ix.mstar2 + 1.0;
+    const bool is_ip = p.ix.metric == ANQI_METRIC_IP;
     for (;;) {
         uint32_t qi = 0;
         if (lane == 0) qi = atomicAdd(work, 1u);
@@ -162,6 +163,16 @@ __global__ void __launch_bounds__(32 * kWarps) noalloc_search_kernel(NoAllocPara
         if (qi >= p.nq) break;
         const float* q = p.queries + (size_t)qi * bs;
         for (uint32_t j = lane; j < bs; j += 32) qraw[j] = j < p.ix.d ? q[j] : 0.0f;
+        // the ip metric's radius is per query: |s q|^2 (double, index order) + 1 + M*^2
+        double R2 = R2_l2;
+        if (is_ip) {
+            double qn2s = 0.0;
+            for (uint32_t j = 0; j < p.ix.d; j++) {
+                const double t = __dmul_rn((double)q[j], p.ix.scale);
+                qn2s = __dadd_rn(qn2s, __dmul_rn(t, t));
+            }
+            R2 = __dadd_rn(__dadd_rn(qn2s, 1.0), p.ix.mstar2);
+        }
         for (uint32_t j = lane; j < ls; j += 32) {
             float v = 0.0f;
             if (j < p.ix.d) v = __double2float_rn(__dmul_rn((double)q[j], p.ix.scale));
@@ -257,9 +268,9 @@ __global__ void __launch_bounds__(32 * kWarps) noalloc_search_kernel(NoAllocPara
             const bool ok = idx < ncand;
             const uint32_t o = cl[ok ? idx : r0];
             const float* orow = p.ix.base + (size_t)o * bs;
-            const float ip = group_ip(orow, qraw, p.ix.d, gt, kAll);
+            const float dot = group_ip(orow, qraw, p.ix.d, gt, kAll);
             const float on = group_ip(orow, orow, p.ix.d, gt, kAll);
-            const float key = __fsub_rn(__fadd_rn(on, qn), __fmul_rn(2.0f, ip));
+            const float key = is_ip ? -dot : __fsub_rn(__fadd_rn(on, qn), __fmul_rn(2.0f, dot));
             const bool pass = ok && (double)key <= (double)p.thr[o];
             const unsigned b = __ballot_sync(kAll, pass && gt == 0);
             if (pass && gt == 0) {
@@ -296,7 +307,7 @@ extern "C" int anqi_rknn_query_noalloc(const anqi_device_index* ix, const float*
                                        uint32_t* pred_ids, uint32_t* n_dist, void* stream) {
     if (!ix || !queries || !thresholds || !pred_count || (!pred_ids && max_pred) || nq == 0 || L == 0)
         return ANQI_ERR_ARGS;
-    if (L > kMaxL || ix->n == 0 || ix->n >= 0x7FFFFFFFull || ix->d == 0 || ix->degree == 0 || ix->degree > 64 ||
+    if (L > kMaxL || ix->metric > ANQI_METRIC_IP || ix->n == 0 || ix->n >= 0x7FFFFFFFull || ix->d == 0 || ix->degree == 0 || ix->degree > 64 ||
         ix->tree_nodes == 0 || !ix->base || !ix->lifted || !ix->deg || !ix->links || !ix->tree_left ||
         !ix->tree_right || !ix->tree_offset || !ix->tree_hyperplane || !ix->tree_leaf_first)
         return ANQI_ERR_ARGS;

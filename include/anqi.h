@@ -34,6 +34,15 @@ extern "C" {
 
 #define ANQI_EMPTY 0xFFFFFFFFu /* empty slot / no neighbour */
 
+/* Metrics (the reference's metric=l2|ip, include/distance.h:170-190).  Under
+ * ANQI_METRIC_IP the AKNN source ranks by 1 - <a, b> (a sequential sum, the
+ * reference's scalar ip distance), its forest splits angularly through the
+ * origin, the exact ground truth keys are -<a, b>, and the query radius and
+ * postfilter follow src/rknn_query.cpp:2227, 2555-2561, 2724-2731.  The
+ * lifted graph itself is always built in L2. */
+#define ANQI_METRIC_L2 0u
+#define ANQI_METRIC_IP 1u
+
 typedef struct anqi_ctx anqi_ctx;
 
 /* ---------------------------------------------------------------- context */
@@ -114,6 +123,10 @@ int anqi_analytic_rankm_materialize(anqi_ctx* ctx, const float* coeff, uint64_t 
  * graph-horizon radius (AKNN rank-K cutoff) -> lifted n x (d+2), M*^2, scale. */
 int anqi_lift(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d, const float* radius,
               float* lifted, double* mstar2, double* scale);
+/* Either metric: under ANQI_METRIC_IP the lift coordinate is s^2 * radius
+ * (src/rknn_query.cpp:2227) instead of (s^2 * radius - |s o|^2) / 2. */
+int anqi_lift_metric(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d, const float* radius,
+                     uint32_t metric, float* lifted, double* mstar2, double* scale);
 
 /* ------------------------------------------------------ random projection
  * RP trees (include/rptrees.h:28-84,127-186) in deterministic breadth-first
@@ -126,6 +139,12 @@ int anqi_rp_forest(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, uint
                    uint32_t leaf_size, uint32_t max_depth, uint64_t seed, uint32_t cap_nodes,
                    uint32_t* n_nodes, uint32_t* left, uint32_t* right, float* offset,
                    float* hyperplane, uint32_t* leaf_off, uint32_t* leaf_cnt, uint32_t* perm);
+/* The same with the metric's split: ANQI_METRIC_IP splits angularly
+ * (include/rptrees.h:41-52), hyperplane x0/|x0| - x1/|x1| normalized, offset 0. */
+int anqi_rp_forest_metric(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, uint32_t trees,
+                          uint32_t leaf_size, uint32_t max_depth, uint64_t seed, uint32_t cap_nodes, uint32_t metric,
+                          uint32_t* n_nodes, uint32_t* left, uint32_t* right, float* offset, float* hyperplane,
+                          uint32_t* leaf_off, uint32_t* leaf_cnt, uint32_t* perm);
 
 /* --------------------------------------------------------- AKNN source
  * nndindex::build_approx_knn (include/index.h:1300-1367) as driven by
@@ -144,6 +163,8 @@ typedef struct {
     uint32_t precision;  /* init_knn leaf distances: 0 = FP32 CUDA cores, 1 = BF16 tensor-core
                             tiles with FP32 recheck (identical output; d <= 256, larger d
                             runs on the CUDA cores) */
+    uint32_t metric;     /* ANQI_METRIC_L2 (0) or ANQI_METRIC_IP; the ip metric runs FP32
+                            init_knn on the CUDA cores and takes no LocalJoin (nn_iters = 0) */
 } anqi_aknn_params;
 
 typedef struct {
@@ -163,6 +184,13 @@ int anqi_aknn_init(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, cons
 int anqi_aknn_gather(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids,
                      const float* g_vals, uint32_t K, uint32_t ef, uint32_t cap, uint32_t out_k,
                      uint32_t* ids, float* dists);
+/* The two stages in either metric. */
+int anqi_aknn_init_metric(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint64_t* leaf_off,
+                          const uint32_t* leaf_ids, uint64_t n_leaves, uint32_t K, uint32_t metric, uint32_t* ids,
+                          float* dists);
+int anqi_aknn_gather_metric(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids,
+                            const float* g_vals, uint32_t K, uint32_t ef, uint32_t cap, uint32_t out_k,
+                            uint32_t metric, uint32_t* ids, float* dists);
 
 /* ----------------------------------------------------------- G48 graph
  * nndindex::build_index with a flat warm start (include/index.h:1071-1295):
@@ -234,6 +262,7 @@ typedef struct {
     const uint32_t* tree_leaf_first; /* indices[0] of each leaf, ANQI_EMPTY if empty */
     double scale;
     double mstar2;
+    uint32_t metric;            /* ANQI_METRIC_L2 or ANQI_METRIC_IP (the meta file's metric) */
 } anqi_index_desc;
 
 int anqi_index_load(anqi_ctx* ctx, const anqi_index_desc* desc);
@@ -365,6 +394,7 @@ typedef struct {
     const float* tree_hyperplane; /* tree_nodes x lifted_stride */
     const uint32_t* tree_leaf_first;
     double scale, mstar2;
+    uint32_t metric;              /* ANQI_METRIC_L2 or ANQI_METRIC_IP */
 } anqi_device_index;
 
 int anqi_rknn_query_noalloc(const anqi_device_index* ix, const float* queries, uint32_t nq,
@@ -409,6 +439,13 @@ int anqi_exact_topk(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d, ui
 int anqi_rknn_ground_truth(anqi_ctx* ctx, const float* base, uint64_t n, const float* query, uint64_t nq,
                            uint32_t d, const float* rk2, uint32_t* off, uint32_t* ids, float* keys,
                            uint64_t cap, uint64_t* total);
+/* The same in either metric: ANQI_METRIC_IP keys are -<a, b> in the same lane
+ * order (tools/dataset_gt.cpp:224, 288); rk2 may be negative. */
+int anqi_exact_topk_metric(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d, uint32_t K, uint32_t metric,
+                           uint32_t* ids, float* keys);
+int anqi_rknn_ground_truth_metric(anqi_ctx* ctx, const float* base, uint64_t n, const float* query, uint64_t nq,
+                                  uint32_t d, const float* rk2, uint32_t metric, uint32_t* off, uint32_t* ids,
+                                  float* keys, uint64_t cap, uint64_t* total);
 
 /* Precision form of the two entry points above: BF16 tcgen05 tiles with FP32
  * accumulation filter every pair by a derived bound on |key~ - key32|; the

@@ -205,11 +205,17 @@ def test_rknn_verifier_mode_files_are_validated(tmp_path):
     assert rc == 3 and "analytic Rank-M header mismatch" in err
 
 
-def test_rknn_ip_metric_is_named(tmp_path):
+def test_rknn_ip_metric_refusals(tmp_path):
+    """Under metric=ip the reference refuses the analytic verifier (an L2 power
+    law) and a non-zero slack on the compact verifier (signed thresholds):
+    rknn_query.cpp:1812-1816, 2417-2422."""
     pfx, env, _ = sample_prefix(tmp_path)
     Path(f"{pfx}_lifted.meta").write_text("0 8 100 ip 1.0\n")
-    rc, _, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10, env=env)
-    assert rc == 2 and "metric=ip" in err
+    rc, _, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10,
+                     env={**env, "ANQI_RADIUS_MODE": "analytic_rankm", "ANQI_CANDIDATE_ENVELOPE": "graph_horizon"})
+    assert rc == 2 and "does not support IP" in err
+    rc, _, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10, env={**env, "ANQI_RANKM_SLACK": "0.1"})
+    assert rc == 2 and "ANQI_RANKM_SLACK=0" in err
 
 
 REF_BIN = REPO / "oracle" / "_ref" / "rknn_query"

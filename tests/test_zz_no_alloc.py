@@ -29,7 +29,7 @@ class DeviceIndex(C.Structure):
         ("base_stride", C.c_uint32), ("lifted", C.c_void_p), ("lifted_stride", C.c_uint32), ("deg", C.c_void_p),
         ("links", C.c_void_p), ("tree_nodes", C.c_uint32), ("tree_left", C.c_void_p), ("tree_right", C.c_void_p),
         ("tree_offset", C.c_void_p), ("tree_hyperplane", C.c_void_p), ("tree_leaf_first", C.c_void_p),
-        ("scale", C.c_double), ("mstar2", C.c_double),
+        ("scale", C.c_double), ("mstar2", C.c_double), ("metric", C.c_uint32),
     ]
 
 
