@@ -177,3 +177,99 @@ def test_rknn_query_verifier_modes_match_reference(tmp_path, mode):
     assert rc == 0, err
     assert "[rknn] loaded cached index" in ours
     assert lines(ours) == lines(ref.stdout), (mode, lines(ours), lines(ref.stdout))
+
+
+def ip_prefix(tmp_path):
+    """The reference sample under metric=ip (tests/golden/sample_ip_d32.npz):
+    its prefix files, the reference's own .rec (keys d - 1), basis, codebook and
+    RkNN ground truth."""
+    z = dict(np.load(tc.GOLDEN / "sample_ip_d32.npz"))
+    pfx = tmp_path / "ipsample"
+    formats.write_fbin(f"{pfx}_base.bin", z["base"])
+    formats.write_fbin(f"{pfx}_query.bin", z["query"])
+    Path(f"{pfx}_lifted.meta").write_text("0 32 100 ip 1.0\n")
+    formats.write_rec(f"{pfx}_baseknn_aknn.rec", z["rec_ids"], z["rec_keys"])
+    formats.write_basis(f"{pfx}_radbasis_M8.bin", z["mu"], z["basis"])
+    formats.write_codebook(f"{pfx}_learned_rq_codebook_M8_u8.bin", z["codebook"])
+    for k in (10, 50, 100):
+        formats.write_rknn_csr(f"{pfx}_rknn_gt_k{k}.bin", z[f"gt_off_{k}"], z[f"gt_ids_{k}"], z[f"gt_keys_{k}"])
+    env = dict(tc.RUN_FINAL_ENV)
+    env["ANQI_PREBUILT_TOPK_REC"] = f"{pfx}_baseknn_aknn.rec"
+    env["ANQI_GRAPH_CACHE_DIR"] = str(tmp_path / "cache" / "graph")
+    env["ANQI_VERIFIER_CACHE_DIR"] = str(tmp_path / "cache" / "verifier")
+    return pfx, env, z
+
+
+def test_dataset_gt_cli_ip_bit_exact(tmp_path):
+    """--metric ip: thresholds and RkNN CSR with keys -<a, b>, the reference's files bit for bit."""
+    z = dict(np.load(tc.GOLDEN / "sample_ip_d32.npz"))
+    base, query = tmp_path / "b.bin", tmp_path / "q.bin"
+    formats.write_fbin(base, z["base"])
+    formats.write_fbin(query, z["query"])
+    thr = tmp_path / "thr"
+    rc, out, err = tc.run("dataset_gt", "--base", base, "--K", 100, "--rk_k", 100, "--metric", "ip",
+                          "--mode", "thresholds", "--out_prefix", thr)
+    assert rc == 0, err
+    raw = Path(f"{thr}_baseknn_gt.bin").read_bytes()
+    ids = np.frombuffer(raw[8:8 + 256 * 400], np.uint32).reshape(256, 100)
+    keys = np.frombuffer(raw[8 + 256 * 400:], np.float32).reshape(256, 100)
+    assert np.array_equal(ids, z["exact_ids"]) and np.array_equal(bits(keys), bits(z["exact_keys"]))
+    assert "metric ip" in Path(f"{thr}_threshold_build_time.meta").read_text()
+    for k in (10, 50, 100):
+        t = tmp_path / f"gt{k}"
+        rc, out, err = tc.run("dataset_gt", "--base", base, "--query", query, "--K", 100, "--rk_k", k,
+                              "--metric", "ip", "--mode", "ground-truth", "--threshold-table",
+                              f"{thr}_baseknn_gt.bin", "--out_prefix", t)
+        assert rc == 0, err
+        off, gids, gkeys = formats.read_rknn_csr(f"{t}_rknn_gt.bin")
+        assert np.array_equal(off, z[f"gt_off_{k}"]) and np.array_equal(gids, z[f"gt_ids_{k}"])
+        assert np.array_equal(bits(gkeys), bits(z[f"gt_keys_{k}"]))
+
+
+def test_build_aknn_source_cli_ip(tmp_path):
+    """metric=ip: .rec keys are d - 1 = -<a, b> (build_aknn_source.cpp:125), rows
+    ascending, self excluded, recall@100 against the exact -<a, b> table."""
+    z = dict(np.load(tc.GOLDEN / "sample_ip_d32.npz"))
+    base = tmp_path / "b.bin"
+    formats.write_fbin(base, z["base"])
+    pfx = tmp_path / "p"
+    rc, out, err = tc.run("build_aknn_source", base, pfx, 100, 64, 8, 64, 4, 10, "ip")
+    assert rc == 0, err
+    assert "metric=ip" in out
+    ids, keys = formats.read_rec(f"{pfx}_baseknn_aknn.rec", 256, 100)
+    n = 256
+    assert (ids < n).all() and (ids != np.arange(n)[:, None]).all()
+    assert (np.diff(keys, axis=1) >= 0).all() and (keys < 0).any()
+    x = z["base"].astype(np.float64)
+    # the keys are the negated inner products of the listed pairs (FP32, sequential sum)
+    assert np.allclose(keys, -np.einsum("id,ikd->ik", x, x[ids]), atol=1e-3)
+    hit = np.mean([len(set(ids[i]) & set(z["exact_ids"][i])) / 100 for i in range(n)])
+    assert hit > 0.95, hit
+    rc, _, err = tc.run("build_aknn_source", base, pfx, 100, 64, 8, 64, 4, 10, "ip", env={"ANQI_NNITERS": "2"})
+    assert rc == 2 and "ANQI_NNITERS" in err
+
+
+def test_rknn_query_cli_ip_matches_reference_lines(tmp_path):
+    """rknn_query on a metric=ip prefix: cold (graph built on the device from the
+    reference's warm start) within 0.02 recall of the reference's lines; on the
+    reference's own graph, the reference's result lines exactly."""
+    pfx, env, z = ip_prefix(tmp_path)
+    ref_lines = {(int(k), int(L)): list(v) for (k, L), v in zip(z["ref_lines_k_L"], z["ref_lines"])}
+    for k in (10, 50, 100):
+        rc, out, err = tc.run("rknn_query", "16,32,64,128", pfx, 48, 500, 64, 600, k, env=env)
+        assert rc == 0, err
+        assert "[rknn] metric=ip" in out
+        for L, v in lines(out).items():
+            r = ref_lines[k, L]
+            assert abs(v[0] - r[0]) < 0.02 and v[1] >= 0.99, (k, L, v, r)
+    gfiles = list(Path(env["ANQI_GRAPH_CACHE_DIR"]).glob("fd_metric_*"))
+    assert len(gfiles) == 1
+    gfiles[0].write_bytes(z["graph_file"].tobytes())
+    for k in (10, 50, 100):
+        rc, out, err = tc.run("rknn_query", "16,32,64,128", pfx, 48, 500, 64, 600, k, env=env)
+        assert rc == 0, err
+        assert "[rknn] loaded cached index" in out
+        got = lines(out)
+        assert sorted(got) == [16, 32, 64, 128]
+        for L, v in got.items():
+            assert v == ref_lines[k, L], (k, L, v, ref_lines[k, L])
