@@ -125,6 +125,9 @@ _SIGS = {
                                 C.c_uint32, C.c_uint32, _u32, _f32],
     "anqi_graph_build": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, C.c_uint32, C.POINTER(GraphParams), _u32, _u32,
                          C.POINTER(BuildStats)],
+    "anqi_graph_build_begin": [_vp, _f32, C.c_uint64, C.c_uint32, C.POINTER(GraphParams)],
+    "anqi_graph_build_warm_rows": [_vp, C.c_uint64, C.c_uint64, _u32, C.c_uint32],
+    "anqi_graph_build_finish": [_vp, _u32, _u32, C.POINTER(BuildStats)],
     "anqi_graph_tree_size": [_vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)],
     "anqi_graph_tree_copy": [_vp, _u32, _u32, _f32, _f32, _u32, _u32, _u32],
     "anqi_graph_warm_start": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, C.c_uint32, C.c_uint32, C.c_uint32, _u32,
@@ -160,6 +163,13 @@ _SIGS = {
                                    _vp, _vp, _vp, _vp],
     "anqi_lrq_objective_backward": [_vp, C.c_uint64, C.c_uint32, C.c_uint32, _vp, _vp, _vp, _vp, _vp,
                                     C.c_uint32, C.c_double, _vp, _vp, _vp, _vp],
+    "anqi_lrq_fit_stats": [_vp, _vp, C.c_uint64, C.c_uint32, _vp, _vp, C.c_uint64, _vp, _vp, _vp],
+    "anqi_lrq_fit_residual": [_vp, _vp, C.c_uint64, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp, _vp],
+    "anqi_lrq_fit_range": [_vp, C.c_uint64, C.c_uint32, _vp, _vp, C.c_uint32, _vp, _vp, _vp],
+    "anqi_lrq_fit_codebooks_scratch": [C.c_uint64, C.c_uint32],
+    "anqi_lrq_fit_codebooks": [_vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, _vp, C.c_uint64, _vp, _vp],
+    "anqi_lrq_fit_decode": [_vp, C.c_uint64, C.c_uint32, _vp, C.c_uint32, _vp, _vp, C.c_uint32,
+                            C.POINTER(C.c_uint32), _vp],
     "anqi_exact_topk_tc": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _vp, C.c_uint32, _u32, _f32],
     "anqi_rknn_ground_truth_tc": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32, _u32, _u32, _f32,
                                   C.c_uint64, C.POINTER(C.c_uint64)],
@@ -198,6 +208,7 @@ def load_library() -> C.CDLL:
     lib.anqi_ctx_destroy.restype = None
     lib.anqi_last_error.restype = C.c_char_p
     lib.anqi_device_bytes.restype = C.c_uint64
+    lib.anqi_lrq_fit_codebooks_scratch.restype = C.c_uint64
     _lib = lib
     return lib
 
@@ -232,6 +243,7 @@ class Context:
     def __init__(self, device: int = 0):
         self.lib = load_library()
         h = C.c_void_p()
+        self.device = device
         rc = self.lib.anqi_ctx_create(device, C.byref(h))
         if rc != ANQI_OK:
             raise AnqiError(rc, f"cannot create a context on CUDA device {device}")

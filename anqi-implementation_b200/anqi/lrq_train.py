@@ -176,6 +176,9 @@ def main(argv=None) -> int:
     ap.add_argument("--chunk", type=int, default=CHUNK)
     ap.add_argument("--codebook-workers", type=int,
                     default=int(os.environ.get("ANQI_CODEBOOK_WORKERS", os.environ.get("OMP_NUM_THREADS", "1"))))
+    ap.add_argument("--device", choices=("cpu", "gpu"), default="cpu",
+                    help="cpu: the NumPy fit (byte-identical files); gpu: anqi.lrq_fit's kernels (the same rounds, "
+                         "equal to rounding)")
     a = ap.parse_args(argv)
     for name in ("train_sample", "recursive_iters", "lloyd_iters", "chunk", "codebook_workers"):
         if getattr(a, name) < 1:
@@ -186,8 +189,13 @@ def main(argv=None) -> int:
     if n == 0:
         raise RuntimeError("invalid base header")
     _, keys = formats.read_rec(src, n, K_MAX, mmap=True)
-    mean, basis, cb = train(keys, n, a.train_sample, a.seed, a.recursive_iters, a.lloyd_iters, a.codebook_workers,
-                            a.chunk, log=lambda s: print(s, flush=True))
+    if a.device == "gpu":
+        from . import lrq_fit
+        mean, basis, cb = lrq_fit.train_gpu(keys, n, a.train_sample, a.seed, a.recursive_iters, a.lloyd_iters,
+                                            log=lambda s: print(s, flush=True))
+    else:
+        mean, basis, cb = train(keys, n, a.train_sample, a.seed, a.recursive_iters, a.lloyd_iters,
+                                a.codebook_workers, a.chunk, log=lambda s: print(s, flush=True))
     bp, cp = write_outputs(str(a.pfx), mean, basis, cb)
     elapsed = time.perf_counter() - started
     Path(f"{a.pfx}_verifier_train_time.meta").write_text(

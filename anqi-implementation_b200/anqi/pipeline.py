@@ -153,7 +153,11 @@ def graph_localjoin(ctx: Context, lifted: np.ndarray, ids, vals, precision="bf16
     return ids, vals, [int(u) for u in up[:done.value]], ms.value
 
 
-def build_index(ctx: Context, base: np.ndarray, aknn=None, graph=None, train_workers: int = 8, log=print) -> Index:
+def build_index(ctx: Context, base: np.ndarray, aknn=None, graph=None, train_workers: int = 8, log=print,
+                train: str = "gpu") -> Index:
+    """The whole index: AKNN source, LRQ fit (train "gpu": anqi.lrq_fit's
+    kernels; "numpy": the reference trainer's NumPy fit, byte-identical
+    files), LRQ encode, lift and the G48 graph."""
     aknn = aknn or {}
     graph = graph or {}
     t = {}
@@ -163,7 +167,11 @@ def build_index(ctx: Context, base: np.ndarray, aknn=None, graph=None, train_wor
     t["aknn_stats"] = st
     log(f"[anqi] AKNN source built in {t['aknn_build_s']:.2f}s {st}")
     t0 = time.perf_counter()
-    mu, basis, cb = lrq_train.train(keys, len(keys), workers=train_workers, log=lambda s: None)
+    if train == "gpu":
+        from . import lrq_fit
+        mu, basis, cb = lrq_fit.train_gpu(keys, len(keys), device=ctx.device, log=lambda s: None)
+    else:
+        mu, basis, cb = lrq_train.train(keys, len(keys), workers=train_workers, log=lambda s: None)
     mu, basis, cb = (np.asarray(a, np.float32) for a in (mu, basis, cb))
     t["lrq_train_s"] = time.perf_counter() - t0
     t0 = time.perf_counter()

@@ -22,6 +22,9 @@
 #include "cli_common.h"
 #include "graph_file.h"
 
+#include <fcntl.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <chrono>
 #include <iomanip>
@@ -171,6 +174,123 @@ static std::string graph_file_name(uint64_t M, uint64_t nn_k, uint64_t n, uint64
                       std::to_string(n) + "_dim_" + std::to_string(dim) + "_efa_" + std::to_string(8.0f) + "_pa_" + std::to_string(alpha) +
                       "_er_100_graphnnd_" + env_or("ANQI_GRAPHNND", "6") + "_gk_" + hash16(graph_key);
     return sanitize_tag(cfg);
+}
+
+// ANQI_BASE_U8BIN (rknn_query.cpp:55-123): a uint8 base, [u32 n][u32 d][n*d
+// u8], read in place of PREFIX_base.bin and widened to float (exact), so every
+// later stage sees the same values; the caches name the uint8 file.
+static std::string base_vector_source(const std::string& fbin_path) {
+    const char* u8 = std::getenv("ANQI_BASE_U8BIN");
+    return (u8 && *u8) ? std::string(u8) : fbin_path;
+}
+
+static Fbin load_base_or_die(const std::string& fbin_path) {
+    const char* u8 = std::getenv("ANQI_BASE_U8BIN");
+    if (!(u8 && *u8)) return load_fbin_or_die(fbin_path);
+    const std::string path = u8;
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    if (!f) die(3, "[rknn] cannot open uint8 base %s: %s", path.c_str(), std::strerror(errno));
+    const std::streamoff bytes = f.tellg();
+    f.seekg(0);
+    uint32_t shape[2] = {0, 0};
+    if (bytes < 8 || !f.read(reinterpret_cast<char*>(shape), 8))
+        die(3, "[rknn] cannot read uint8 base header %s", path.c_str());
+    const uint64_t values = (uint64_t)shape[0] * shape[1];
+    if (shape[0] == 0 || shape[1] == 0 || (uint64_t)bytes != 8 + values)
+        die(3, "[rknn] bad uint8 base %s: n=%u d=%u bytes=%lld expected=%llu", path.c_str(), shape[0], shape[1],
+            (long long)bytes, (unsigned long long)(8 + values));
+    std::vector<uint8_t> raw(values);
+    if (!f.read(reinterpret_cast<char*>(raw.data()), (std::streamsize)values))
+        die(3, "[rknn] cannot read uint8 base header %s", path.c_str());
+    Fbin out;
+    out.n = shape[0];
+    out.d = shape[1];
+    out.x.resize(values);
+    for (uint64_t i = 0; i < values; i++) out.x[i] = (float)raw[i];
+    printf("[rknn] loaded uint8 base directly as float: %s n=%u d=%u %.3fGB\n", path.c_str(), out.n, out.d,
+           values * 4.0 / 1e9);
+    return out;
+}
+
+// ANQI_COMPACT_PREBUILT_TOPK_IDS_INPLACE (rknn_query.cpp:988-1057): the
+// prebuilt {id, key} table becomes an n x width id table in place, in 64 MB
+// chunks, then is truncated; an id >= n exits 3.
+static void compact_topk_ids_in_place(const std::string& path, uint64_t n, uint64_t source_k, uint64_t width) {
+    validate_prebuilt_topk(path, n, source_k, width);
+    const int fd = ::open(path.c_str(), O_RDWR);
+    if (fd < 0) die(3, "[rknn] cannot open prebuilt top-k for compaction %s: %s", path.c_str(), std::strerror(errno));
+    const uint64_t rows_per_chunk = std::max<uint64_t>(1, (64ull << 20) / (source_k * sizeof(TopKRecord)));
+    std::vector<TopKRecord> rec(rows_per_chunk * source_k);
+    std::vector<uint32_t> ids(rows_per_chunk * width);
+    auto io = [&](bool write, void* buf, uint64_t bytes, uint64_t off) {
+        uint8_t* p = static_cast<uint8_t*>(buf);
+        while (bytes) {
+            const ssize_t got = write ? ::pwrite(fd, p, bytes, (off_t)off) : ::pread(fd, p, bytes, (off_t)off);
+            if (got < 0 && errno == EINTR) continue;
+            if (got <= 0)
+                die(3, write ? "[rknn] cannot write compact warm-start IDs %s offset=%llu: %s"
+                             : "[rknn] cannot read prebuilt top-k during compaction %s offset=%llu: %s",
+                    path.c_str(), (unsigned long long)off, got == 0 ? "unexpected EOF" : std::strerror(errno));
+            p += got;
+            bytes -= (uint64_t)got;
+            off += (uint64_t)got;
+        }
+    };
+    const uint64_t step = std::max<uint64_t>(1, n / 20);
+    uint64_t next = step;
+    for (uint64_t r0 = 0; r0 < n; r0 += rows_per_chunk) {
+        const uint64_t rows = std::min(rows_per_chunk, n - r0);
+        io(false, rec.data(), rows * source_k * sizeof(TopKRecord), r0 * source_k * sizeof(TopKRecord));
+        for (uint64_t r = 0; r < rows; r++)
+            for (uint64_t k = 0; k < width; k++) {
+                const uint32_t id = rec[r * source_k + k].id;
+                if (id >= n)
+                    die(3, "[rknn] invalid warm-start id at row=%llu k=%u", (unsigned long long)(r0 + r), (unsigned)k);
+                ids[r * width + k] = id;
+            }
+        // the rows written never pass the rows read: the ids table is smaller
+        io(true, ids.data(), rows * width * 4, r0 * width * 4);
+        if (r0 + rows >= next || r0 + rows == n) {
+            printf("[rknn] compact warm-start IDs: %.1f%%\n", 100.0 * (double)(r0 + rows) / (double)n);
+            next = r0 + rows + step;
+        }
+    }
+    if (::ftruncate(fd, (off_t)(n * width * 4)) != 0 || ::fsync(fd) != 0 || ::close(fd) != 0)
+        die(3, "[rknn] cannot finalize compact warm-start IDs %s: %s", path.c_str(), std::strerror(errno));
+    printf("[rknn] compacted regenerable prebuilt top-k to IDs in place: %s source_k=%" PRIu64 " width=%" PRIu64
+           " bytes=%.3fGB\n",
+           path.c_str(), source_k, width, n * width * 4 / 1e9);
+}
+
+// The streamed warm start (include/index.h:1127-1203): n rows of `stride`
+// records ({u32 id, f32 key}, or u32 ids when ids_only) read in 64 MB chunks
+// from a command's stdout or a file, each chunk handed to the device build;
+// the stream must hold exactly n rows.
+static void stream_warm_rows(anqi_ctx* ctx, FILE* in, bool is_command, uint64_t n, uint64_t stride, uint64_t width,
+                             bool ids_only) {
+    const uint64_t rec_bytes = ids_only ? 4 : sizeof(TopKRecord);
+    const uint64_t rows_per_chunk = std::max<uint64_t>(1, (64ull << 20) / (stride * rec_bytes));
+    std::vector<uint8_t> buf(rows_per_chunk * stride * rec_bytes);
+    std::vector<uint32_t> ids(rows_per_chunk * width);
+    bool ok = true;
+    for (uint64_t r0 = 0; r0 < n && ok; r0 += rows_per_chunk) {
+        const uint64_t rows = std::min(rows_per_chunk, n - r0);
+        if (std::fread(buf.data(), rec_bytes, rows * stride, in) != rows * stride) {
+            ok = false;
+            break;
+        }
+        for (uint64_t r = 0; r < rows; r++)
+            for (uint64_t k = 0; k < width; k++) {
+                uint32_t id;
+                std::memcpy(&id, buf.data() + (r * stride + k) * rec_bytes, 4);
+                ids[r * width + k] = id;
+            }
+        const int rc = anqi_graph_build_warm_rows(ctx, r0, rows, ids.data(), (uint32_t)width);
+        if (rc) die(rc, "[rknn] graph warm start failed: %s", anqi_last_error(ctx));
+    }
+    if (ok && std::fgetc(in) != EOF) ok = false;
+    const int status = is_command ? ::pclose(in) : std::fclose(in);
+    if (!ok || status != 0) die(3, "[rknn] streamed warm-start ended early, produced extra data, or failed");
 }
 
 // ------------------------------------------------------------- verifier
@@ -409,9 +529,7 @@ static int run(int argc, char** argv) {
     printf("[rknn] shared-index query: Kq=%" PRIu64 " NK=%" PRIu64 " graph_NK=%" PRIu64 " GT=%s\n", Kq, NK, GRAPH_NK,
            gt_p.c_str());
 
-    if (std::getenv("ANQI_BASE_U8BIN") && *std::getenv("ANQI_BASE_U8BIN"))
-        die(2, "[rknn] ANQI_BASE_U8BIN (uint8 base) is not implemented on the GPU path");
-    Fbin base = load_fbin_or_die(PFX + "_base.bin");
+    Fbin base = load_base_or_die(PFX + "_base.bin");
     Fbin query = load_fbin_or_die(PFX + "_query.bin");
     const uint64_t n = base.n, d = base.d, nq = query.n;
     if (d != d0 || query.d != d0)
@@ -523,9 +641,8 @@ static int run(int argc, char** argv) {
     if (env_flag("ANQI_RECHECK"))
         die(2, "[rknn] ANQI_RECHECK cannot be mixed with an independent postfilter verifier; select "
                "ANQI_RADIUS_MODE=exact_f32 for the exact component comparison");
-    for (const char* e : {"ANQI_VAMANA", "ANQI_EDGE_POLICY", "ANQI_REUSE_ORIG_KNN", "ANQI_PREBUILT_WARM_START_COMMAND"})
+    for (const char* e : {"ANQI_VAMANA", "ANQI_EDGE_POLICY", "ANQI_REUSE_ORIG_KNN"})
         if (std::getenv(e)) not_here(e);
-    if (env_flag("ANQI_COMPACT_PREBUILT_TOPK_IDS_INPLACE")) not_here("ANQI_COMPACT_PREBUILT_TOPK_IDS_INPLACE");
     if (env_or("ANQI_SEARCH_SCORE", "center") != "center") not_here("ANQI_SEARCH_SCORE=" + env_or("ANQI_SEARCH_SCORE", ""));
     if (std::getenv("ANQI_RCEPS") && std::atof(std::getenv("ANQI_RCEPS")) != 0.0) not_here("ANQI_RCEPS!=0");
     if (std::getenv("ANQI_RADIUS_RELAX") && std::atof(std::getenv("ANQI_RADIUS_RELAX")) != 0.0)
@@ -575,7 +692,7 @@ static int run(int argc, char** argv) {
     const std::string graph_radius_id =
         std::getenv("ANQI_GRAPH_RADIUS_ID")
             ? env_or("ANQI_GRAPH_RADIUS_ID", "aknn_k100_v1")
-            : file_stat_identity(graph_radius_source + "_base.bin") + "|" +
+            : file_stat_identity(base_vector_source(graph_radius_source + "_base.bin")) + "|" +
                   threshold_source_identity(graph_radius_source) + ":k" + std::to_string(GRAPH_NK) + ":v2";
     graph_key += "_graph_cutoff_k" + std::to_string(GRAPH_NK) + "_" + hash16(graph_radius_id);
     graph_key = sanitize_tag(graph_key);
@@ -714,8 +831,21 @@ static int run(int argc, char** argv) {
         std::vector<uint32_t> warm;
         const uint64_t width = 100;
         const std::string topk = prebuilt_topk_path();
-        if (!topk.empty()) {
-            const uint64_t sk = prebuilt_topk_width(width);
+        // where the graph's warm-start ids come from (rknn_query.cpp:2092-2131)
+        const char* stream_command = std::getenv("ANQI_PREBUILT_WARM_START_COMMAND");
+        const bool streamed_cmd = !topk.empty() && stream_command && *stream_command;
+        const bool compact_ids = !topk.empty() && env_flag("ANQI_COMPACT_PREBUILT_TOPK_IDS_INPLACE");
+        const uint64_t sk = topk.empty() ? width : prebuilt_topk_width(width);
+        if (compact_ids && streamed_cmd)
+            die(2, "[rknn] compact local warm-start IDs cannot be combined with ANQI_PREBUILT_WARM_START_COMMAND");
+        if (compact_ids || streamed_cmd) {
+            validate_prebuilt_topk(topk, n, sk, width);
+            printf(compact_ids ? "[rknn] deferred original KNN IDs to compact local graph warm-start (source_k=%" PRIu64
+                                 " width=%" PRIu64 ")\n"
+                               : "[rknn] deferred original KNN IDs to streamed graph warm-start (source_k=%" PRIu64
+                                 " width=%" PRIu64 ")\n",
+                   sk, width);
+        } else if (!topk.empty()) {
             validate_prebuilt_topk(topk, n, sk, width);
             const std::vector<TopKRecord> rec = read_prebuilt(topk, n, sk);
             warm.resize(n * width);
@@ -744,7 +874,7 @@ static int run(int argc, char** argv) {
         }
         source_prepare_s = since(t_src);
         printf("[rknn] original-space AKNN warm start ready: rows=%" PRIu64 " source=%s\n", n,
-               topk.empty() ? "internal" : "prebuilt-contiguous");
+               (compact_ids || streamed_cmd) ? "prebuilt-stream" : (topk.empty() ? "internal" : "prebuilt-contiguous"));
         const auto t_prep = Clock::now();
         ensure_lrq();
         const std::vector<float> radius = load_threshold_column(graph_radius_source, n, GRAPH_NK);
@@ -768,6 +898,15 @@ static int run(int argc, char** argv) {
         }
         printf("[rknn] BUILD lift M*^2=%.6g scale=%.4g (graph radius=aknn_k%" PRIu64 "; verifier=%s:postfilter)\n",
                Mstar2, scale, GRAPH_NK, radius_key.c_str());
+        // the prebuilt table's keys are read (verifier, radius): it can now be
+        // compacted to ids or released (rknn_query.cpp:2170-2186)
+        if (compact_ids) {
+            compact_topk_ids_in_place(topk, n, sk, width);
+        } else if (!topk.empty() && env_flag("ANQI_RELEASE_PREBUILT_TOPK_AFTER_PREP")) {
+            if (::unlink(topk.c_str()) != 0)
+                die(3, "[rknn] cannot release regenerable prebuilt top-k %s: %s", topk.c_str(), std::strerror(errno));
+            printf("[rknn] released regenerable prebuilt top-k after verifier/lift preparation: %s\n", topk.c_str());
+        }
         lift_verifier_prepare_s = since(t_prep);
 
         printf("[rknn] graph degree M=%" PRIu64 "\n", Marg);
@@ -789,9 +928,21 @@ static int run(int argc, char** argv) {
         deg.resize(n);
         links.resize(n * Marg);
         anqi_build_stats gs{};
-        dev().check(anqi_graph_build(dev().get(), lifted.data(), n, (uint32_t)dim, warm.data(), (uint32_t)width, &gp,
-                                   deg.data(), links.data(), &gs),
-                  "graph build");
+        if (compact_ids || streamed_cmd) {
+            dev().check(anqi_graph_build_begin(dev().get(), lifted.data(), n, (uint32_t)dim, &gp), "graph build");
+            FILE* in = streamed_cmd ? ::popen(stream_command, "r") : std::fopen(topk.c_str(), "rb");
+            if (!in) die(3, "[rknn] cannot start streamed warm-start %s", streamed_cmd ? "command" : topk.c_str());
+            stream_warm_rows(dev().get(), in, streamed_cmd, n, compact_ids ? width : sk, width, compact_ids);
+            if (compact_ids && ::unlink(topk.c_str()) != 0)
+                die(3, "[rknn] cannot release consumed streamed warm-start file %s", topk.c_str());
+            printf(compact_ids ? "[rknn] init: streamed compact KNN IDs warm-start (recompute lifted d2)\n"
+                               : "[rknn] init: streamed original KNN warm-start (recompute lifted d2)\n");
+            dev().check(anqi_graph_build_finish(dev().get(), deg.data(), links.data(), &gs), "graph build");
+        } else {
+            dev().check(anqi_graph_build(dev().get(), lifted.data(), n, (uint32_t)dim, warm.data(), (uint32_t)width,
+                                         &gp, deg.data(), links.data(), &gs),
+                        "graph build");
+        }
         uint32_t tn = 0;
         uint64_t tp = 0;
         dev().check(anqi_graph_tree_size(dev().get(), &tn, &tp), "entry tree size");

@@ -438,9 +438,11 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
 // ------------------------------------------------------- warm start
 
 // index.h:1210-1217: heap (cap K) of each row from its first `width` warm ids.
+// Rows [row0, row0 + rows) of n; cand holds their candidates, row by row.
 __global__ void warm_start_kernel(const float* __restrict__ x, const float* __restrict__ norms, uint64_t n,
-                                  uint32_t stride, uint32_t dim, const uint32_t* __restrict__ cand, uint32_t cstride,
-                                  uint32_t width, uint32_t K, uint32_t* __restrict__ hid, float* __restrict__ hval) {
+                                  uint64_t row0, uint64_t rows, uint32_t stride, uint32_t dim,
+                                  const uint32_t* __restrict__ cand, uint32_t cstride, uint32_t width, uint32_t K,
+                                  uint32_t* __restrict__ hid, float* __restrict__ hval) {
     extern __shared__ __align__(16) unsigned char sm[];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const size_t per_warp = (size_t)(2 * width + 2 * K) * 4;
@@ -449,8 +451,9 @@ __global__ void warm_start_kernel(const float* __restrict__ x, const float* __re
     uint32_t* hi = reinterpret_cast<uint32_t*>(cd + width);
     float* hv = reinterpret_cast<float*>(hi + K);
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
-        for (uint32_t t = lane; t < width; t += 32) cid[t] = cand[i * cstride + t];
+    for (uint64_t loc = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; loc < rows; loc += nw) {
+        const uint64_t i = row0 + loc;
+        for (uint32_t t = lane; t < width; t += 32) cid[t] = cand[loc * cstride + t];
         for (uint32_t t = lane; t < K; t += 32) {
             hi[t] = kEmpty;
             hv[t] = FLT_MAX;
@@ -1125,15 +1128,16 @@ static int run_localjoin(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n,
 
 static int run_warm_start(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
                           const uint32_t* d_cand, uint32_t cstride, uint32_t width, uint32_t K, DevBuf& hid,
-                          DevBuf& hval) {
+                          DevBuf& hval, uint64_t row0 = 0, uint64_t rows = ~0ull) {
     int rc;
+    if (rows == ~0ull) rows = n;
     if ((rc = ensure(c, hid, n * K * 4)) || (rc = ensure(c, hval, n * K * 4))) return rc;
     const int wpb = 4;
     const size_t smem = (size_t)(2 * width + 2 * K) * 4 * wpb;
     ANQI_CUDA(c, cudaFuncSetAttribute(warm_start_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    warm_start_kernel<<<c->sm_count * 8, 32 * wpb, smem, c->stream>>>(dx.as<float>(), dn.as<float>(), n, stride, dim,
-                                                                      d_cand, cstride, width, K, hid.as<uint32_t>(),
-                                                                      hval.as<float>());
+    warm_start_kernel<<<c->sm_count * 8, 32 * wpb, smem, c->stream>>>(dx.as<float>(), dn.as<float>(), n, row0, rows,
+                                                                      stride, dim, d_cand, cstride, width, K,
+                                                                      hid.as<uint32_t>(), hval.as<float>());
     ANQI_CUDA(c, cudaGetLastError());
     return sync(c);
 }
@@ -1318,28 +1322,39 @@ int anqi_graph_commit(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, con
     return sync(c);
 }
 
-int anqi_graph_build(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* warm_ids,
-                     uint32_t warm_stride, const anqi_graph_params* gp, uint32_t* deg, uint32_t* links,
-                     anqi_build_stats* st) {
-    if (!h || !x || !warm_ids || !gp || !deg || !links || n < 2 || dim == 0 || gp->degree == 0 || gp->degree > 64 ||
-        gp->nn_k == 0 || gp->nn_k > 256 || gp->warm_width > warm_stride || gp->leaf == 0)
+static void graph_build_reset(Ctx* c) {
+    GraphBuild& g = c->gb;
+    for (DevBuf* b : {&g.dx, &g.dn, &g.hid, &g.hv, &g.order}) release(c, *b);
+    g.seen.clear();
+    g.seen.shrink_to_fit();
+    g.active = false;
+    g.rows_done = 0;
+}
+
+int anqi_graph_build_begin(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const anqi_graph_params* gp) {
+    if (!h || !x || !gp || n < 2 || dim == 0 || gp->degree == 0 || gp->degree > 64 || gp->nn_k == 0 ||
+        gp->nn_k > 256 || gp->warm_width == 0 || gp->leaf == 0)
         return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
-    const auto t0 = Clock::now();
-    const uint32_t xs = round_up(dim, 8);
-    TmpBuf dx(c), dn(c), dw(c), hid(c), hv(c), dO(c), dOd(c), dl(c), dd(c);
+    graph_build_reset(c);
+    GraphBuild& g = c->gb;
+    g.n = n;
+    g.dim = dim;
+    g.xs = round_up(dim, 8);
+    g.gp = *gp;
     int rc;
-    if ((rc = upload_rows(c, dx, dn, x, n, dim, xs)) || (rc = h2d(c, dw, warm_ids, n * warm_stride * 4ull))) return rc;
+    if ((rc = upload_rows(c, g.dx, g.dn, x, n, dim, g.xs))) return rc;
     // entry tree: make_forest with one tree (index.h:1111-1120)
-    auto t = Clock::now();
+    const auto t = Clock::now();
     ForestOut f;
     const uint32_t cap_nodes = (uint32_t)std::min<uint64_t>(4 * n + 8, 0xFFFFFFF0ull);
-    rc = build_forest(c, dx.as<float>(), n, dim, xs, 1, gp->leaf, gp->max_depth ? gp->max_depth : 100, gp->seed,
+    rc = build_forest(c, g.dx.as<float>(), n, dim, g.xs, 1, gp->leaf, gp->max_depth ? gp->max_depth : 100, gp->seed,
                       cap_nodes, f);
     if (rc) {
         release(c, f.perm);
         release(c, f.hyper);
+        graph_build_reset(c);
         return rc;
     }
     c->t_nodes = f.n_nodes[0];
@@ -1351,56 +1366,115 @@ int anqi_graph_build(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, cons
     c->t_hyper.resize((size_t)c->t_nodes * dim);
     c->t_perm.resize(n);
     c->t_dim = dim;
-    cudaMemcpy2D(c->t_hyper.data(), dim * 4, f.hyper.p, xs * 4, dim * 4, c->t_nodes, cudaMemcpyDeviceToHost);
+    cudaMemcpy2D(c->t_hyper.data(), dim * 4, f.hyper.p, g.xs * 4, dim * 4, c->t_nodes, cudaMemcpyDeviceToHost);
     cudaMemcpy(c->t_perm.data(), f.perm.p, n * 4, cudaMemcpyDeviceToHost);
     for (uint32_t v = 0; v < c->t_nodes; v++)
         if (c->t_left[v] == kEmpty) std::memset(c->t_hyper.data() + (size_t)v * dim, 0, dim * 4);
     // the entry tree's leaf order groups nearby rows: the gathers run them together
-    TmpBuf order(c);
-    if ((rc = ensure(c, order, n * 4))) {
-        release(c, f.perm);
-        release(c, f.hyper);
-        return rc;
-    }
-    ANQI_CUDA(c, cudaMemcpyAsync(order.p, f.perm.p, n * 4, cudaMemcpyDeviceToDevice, c->stream));
+    rc = ensure(c, g.order, n * 4);
+    if (!rc && cudaMemcpyAsync(g.order.p, f.perm.p, n * 4, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+        rc = fail(c, ANQI_ERR_DEVICE, "row order copy failed");
     release(c, f.perm);
     release(c, f.hyper);
-    const double forest_ms = ms_since(t);
-    t = Clock::now();
-    if ((rc = run_warm_start(c, dx, dn, n, xs, dim, dw.as<uint32_t>(), warm_stride, gp->warm_width, gp->nn_k, hid, hv)))
+    if (!rc && ((rc = ensure(c, g.hid, n * gp->nn_k * 4ull)) || (rc = ensure(c, g.hv, n * gp->nn_k * 4ull))))
+        ;
+    if (rc) {
+        graph_build_reset(c);
         return rc;
-    const double init_ms = ms_since(t);
-    t = Clock::now();
+    }
+    g.forest_ms = ms_since(t);
+    g.warm_ms = 0;
+    g.seen.assign(n, 0);
+    g.active = true;
+    return ANQI_OK;
+}
+
+int anqi_graph_build_warm_rows(anqi_ctx* h, uint64_t row0, uint64_t rows, const uint32_t* ids, uint32_t stride) {
+    if (!h || !ids || rows == 0) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    GraphBuild& g = c->gb;
+    if (!g.active) return fail(c, ANQI_ERR_ARGS, "no graph build in progress (anqi_graph_build_begin)");
+    if (row0 >= g.n || rows > g.n - row0 || stride < g.gp.warm_width)
+        return fail(c, ANQI_ERR_ARGS, "warm-start rows [%llu, +%llu) or stride %u outside the build",
+                    (unsigned long long)row0, (unsigned long long)rows, stride);
+    for (uint64_t r = row0; r < row0 + rows; r++)
+        if (g.seen[r]) return fail(c, ANQI_ERR_ARGS, "warm-start row %llu delivered twice", (unsigned long long)r);
+    cudaSetDevice(c->device);
+    const auto t = Clock::now();
+    TmpBuf dw(c);
+    int rc;
+    if ((rc = h2d(c, dw, ids, rows * stride * 4ull)) ||
+        (rc = run_warm_start(c, g.dx, g.dn, g.n, g.xs, g.dim, dw.as<uint32_t>(), stride, g.gp.warm_width, g.gp.nn_k,
+                             g.hid, g.hv, row0, rows)))
+        return rc;
+    std::fill(g.seen.begin() + row0, g.seen.begin() + row0 + rows, 1);
+    g.rows_done += rows;
+    g.warm_ms += ms_since(t);
+    return ANQI_OK;
+}
+
+int anqi_graph_build_finish(anqi_ctx* h, uint32_t* deg, uint32_t* links, anqi_build_stats* st) {
+    if (!h || !deg || !links) return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    GraphBuild& g = c->gb;
+    if (!g.active) return fail(c, ANQI_ERR_ARGS, "no graph build in progress (anqi_graph_build_begin)");
+    if (g.rows_done != g.n) {
+        const uint64_t done = g.rows_done, n = g.n;
+        graph_build_reset(c);
+        return fail(c, ANQI_ERR_ARGS, "warm start covers %llu of %llu rows", (unsigned long long)done,
+                    (unsigned long long)n);
+    }
+    cudaSetDevice(c->device);
+    const auto t0 = Clock::now();
+    const anqi_graph_params& gp = g.gp;
+    const uint64_t n = g.n;
+    TmpBuf dO(c), dOd(c), dl(c), dd(c);
+    auto t = Clock::now();
     std::vector<uint64_t> up;
-    if ((rc = run_localjoin(c, dx, dn, n, xs, dim, hid, hv, gp->nn_k, gp->join_sample ? gp->join_sample : 20,
-                            gp->join_iters, up, gp->precision)))
-        return rc;
+    int rc = run_localjoin(c, g.dx, g.dn, n, g.xs, g.dim, g.hid, g.hv, gp.nn_k, gp.join_sample ? gp.join_sample : 20,
+                           gp.join_iters, up, gp.precision);
     const double join_ms = ms_since(t);
     t = Clock::now();
     uint64_t pool_total = 0;
     double gather_kernel_ms = 0;
-    const uint32_t cap = std::max<uint32_t>(gp->degree, gp->ef_alpha * gp->explore);
+    const uint32_t cap = std::max<uint32_t>(gp.degree, gp.ef_alpha * gp.explore);
     const char* ord_env = std::getenv("ANQI_B200_ORDER");
-    if ((rc = run_select_commit(c, dx, dn, n, xs, dim, hid, hv, gp->nn_k, gp->degree, gp->explore, cap, gp->alpha, dO,
-                                dOd, &dl, &dd, &pool_total,
-                                ord_env && ord_env[0] == '0' ? nullptr : order.as<uint32_t>(), &gather_kernel_ms)))
-        return rc;
+    if (!rc)
+        rc = run_select_commit(c, g.dx, g.dn, n, g.xs, g.dim, g.hid, g.hv, gp.nn_k, gp.degree, gp.explore, cap,
+                               gp.alpha, dO, dOd, &dl, &dd, &pool_total,
+                               ord_env && ord_env[0] == '0' ? nullptr : g.order.as<uint32_t>(), &gather_kernel_ms);
     const double gather_ms = ms_since(t);
-    if ((rc = d2h(c, links, dl, n * gp->degree * 4ull)) || (rc = d2h(c, deg, dd, n * 4)) || (rc = sync(c))) return rc;
-    if (st) {
-        st->forest_ms = forest_ms;
-        st->init_ms = init_ms;
+    if (!rc && !(rc = d2h(c, links, dl, n * gp.degree * 4ull)) && !(rc = d2h(c, deg, dd, n * 4))) rc = sync(c);
+    if (!rc && st) {
+        st->forest_ms = g.forest_ms;
+        st->init_ms = g.warm_ms;
         st->join_ms = join_ms;
         st->reverse_ms = 0;
         st->gather_ms = gather_ms;
         st->gather_kernel_ms = gather_kernel_ms;
-        st->total_ms = ms_since(t0);
+        st->total_ms = g.forest_ms + g.warm_ms + ms_since(t0);
         uint64_t tot = 0;
         for (uint64_t u : up) tot += u;
         st->join_updates = tot;
         st->pool_total = pool_total;
     }
-    return ANQI_OK;
+    graph_build_reset(c);
+    return rc;
+}
+
+int anqi_graph_build(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* warm_ids,
+                     uint32_t warm_stride, const anqi_graph_params* gp, uint32_t* deg, uint32_t* links,
+                     anqi_build_stats* st) {
+    if (!h || !x || !warm_ids || !gp || !deg || !links || n < 2 || dim == 0 || gp->degree == 0 || gp->degree > 64 ||
+        gp->nn_k == 0 || gp->nn_k > 256 || gp->warm_width > warm_stride || gp->leaf == 0)
+        return ANQI_ERR_ARGS;
+    int rc;
+    if ((rc = anqi_graph_build_begin(h, x, n, dim, gp))) return rc;
+    if ((rc = anqi_graph_build_warm_rows(h, 0, n, warm_ids, warm_stride))) {
+        graph_build_reset(&h->c);
+        return rc;
+    }
+    return anqi_graph_build_finish(h, deg, links, st);
 }
 
 int anqi_graph_tree_size(anqi_ctx* h, uint32_t* n_nodes, uint64_t* n_points) {

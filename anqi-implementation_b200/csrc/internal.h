@@ -81,6 +81,19 @@ struct Batch {
     bool ordered = false;  // work list ordered by entry leaf
 };
 
+// A G48 build in progress (anqi_graph_build_begin .. _finish): lifted rows,
+// norms, the warm-start heaps and the entry tree's row order stay on the
+// device between the calls that deliver warm-start rows.
+struct GraphBuild {
+    bool active = false;
+    uint64_t n = 0, rows_done = 0;
+    uint32_t dim = 0, xs = 0;
+    anqi_graph_params gp{};
+    DevBuf dx, dn, hid, hv, order;
+    std::vector<uint8_t> seen;  // rows delivered
+    double forest_ms = 0, warm_ms = 0;
+};
+
 struct Ctx {
     int device = 0;
     int sm_count = 0;
@@ -114,6 +127,7 @@ struct Ctx {
     uint32_t last_cfg_wpb = 4, last_cfg_post = 8;  // block shape and candidate tile
     cudaGraphExec_t qgraph = nullptr;
     DevBuf init_cnt, init_cid, init_key;  // tensor-core init_knn candidate buffers
+    GraphBuild gb;                        // staged G48 build
     DevBuf g_bits, g_vlog, g_pd, g_pi, g_gtab;  // gather kernel per-slot scratch
     std::vector<uint64_t> qgraph_key;
     uint64_t device_bytes = 0;
@@ -125,7 +139,8 @@ struct Ctx {
                 &batch.cand_off, &batch.pred_csr, &batch.cand_csr, &batch.entry, &batch.enode, &batch.order,
                 &batch.leaf_cnt, &batch.qr2, &err, &counters, &vis_bits, &vis_log,
                 &cand_scratch, &thr_table, &gt_off, &gt_ids, &eval_rows, &eval_sums, &vis_gtab,
-                &init_cnt, &init_cid, &init_key, &g_bits, &g_vlog, &g_pd, &g_pi, &g_gtab};
+                &init_cnt, &init_cid, &init_key, &g_bits, &g_vlog, &g_pd, &g_pi, &g_gtab, &gb.dx, &gb.dn,
+                &gb.hid, &gb.hv, &gb.order};
     }
     // Per-object thresholds for up to kThrSlots values of k: slot s holds
     // thr_k[s] (0 = unused) in thr_table[s * n .. (s+1) * n).

@@ -202,6 +202,26 @@ def build_workload(ctx, a, rank, log):
                           and np.array_equal(j16[1].view(np.uint32), j32[1].view(np.uint32)))}
     del wi, wv, j16, j32
     log(f"LocalJoin {ix.timings['localjoin']}")
+    # the LRQ fit in both forms on the same cutoff matrix: the index's (GPU
+    # kernels, anqi.lrq_fit) and the NumPy trainer's; codebooks compared per
+    # column range, thresholds per object at every k
+    from anqi import lrq_train
+    t0 = time.perf_counter()
+    fit_np = lrq_train.train(ix.aknn_keys, len(ix.aknn_keys), workers=os.cpu_count() or 8, log=lambda s: None)
+    t_np = time.perf_counter() - t0
+    mu_c, g_c, b_c = (np.asarray(v, np.float32) for v in fit_np)
+    coeff_c, codes_c = ctx.lrq_encode(ix.aknn_keys, mu_c, g_c, b_c)
+    span = (b_c[:, -1].astype(np.float64) - b_c[:, 0])[:, None]
+    agree = {}
+    for k in (10, 50, 100):
+        t_g = ctx.lrq_materialize(ix.coeff, ix.codes, ix.mu, ix.basis, ix.codebook, k)
+        t_c = ctx.lrq_materialize(coeff_c, codes_c, mu_c, g_c, b_c, k)
+        agree[k] = round(float(np.mean(np.isclose(t_g, t_c, rtol=1e-6, atol=1e-6))), 6)
+    ix.numpy_fit = (coeff_c, codes_c, mu_c, g_c, b_c)
+    ix.timings["lrq_fit"] = {"gpu_s": round(ix.timings["lrq_train_s"], 3), "numpy_s": round(t_np, 3),
+                             "codebook_max_rel": float(np.max(np.abs(ix.codebook.astype(np.float64) - b_c) / span)),
+                             "threshold_agree": agree}
+    log(f"LRQ fit {ix.timings['lrq_fit']}")
     log(f"AKNN fp32 build {ix.timings['aknn_build_fp32_s']:.2f}s identical={ix.timings['aknn_fp32_identical']}")
     ks = [int(k) for k in a.ks.split(",")]
     if a.no_gt or a.d > 256:
@@ -395,6 +415,20 @@ def run_ours(a, rank, world, local):
             e = ctx.query_evaluate(off, ids)
             per_k[k] = {"recall": round(e["recall"], 6), "precision": round(e["precision"], 6),
                         "candidate_recall": round(e["candidate_recall"], 6)}
+        # the same queries with the NumPy-fit verifier: the recall the fit costs or gains
+        coeff_c, codes_c, mu_c, g_c, b_c = ix.numpy_fit
+        ctx.verifier_load(coeff_c, codes_c, mu_c, g_c, b_c)
+        for j, k in enumerate(ks):
+            ctx.verifier_materialize(k)
+            ctx.query_upload(query, k, a.L)
+            ctx.query_run()
+            off, ids, _ = gt[k]
+            e = ctx.query_evaluate(off, ids)
+            ix.timings["lrq_fit"].setdefault("recall_numpy_fit", {})[k] = round(e["recall"], 6)
+            ix.timings["lrq_fit"].setdefault("recall_gpu_fit", {})[k] = per_k[k]["recall"]
+        ctx.verifier_load(ix.coeff, ix.codes, ix.mu, ix.basis, ix.codebook)
+        for k in ks:
+            ctx.verifier_materialize(k)
     # ---- the reference's beam-width sweep, one launch of nq queries per (k, L):
     # recall / precision and QPS with the device evaluation inside the timing,
     # as the reference's query loop has it
@@ -513,6 +547,7 @@ def run_ours(a, rank, world, local):
         "batched_form": batched,
         "build_s": {k: round(v, 3) for k, v in ix.timings.items() if isinstance(v, float)},
         "localjoin": ix.timings["localjoin"],
+        "lrq_fit": ix.timings.get("lrq_fit"),
         "fp64_error": fp64_error,
         "aknn_build": {"bf16_tensor_init_s": round(ix.timings["aknn_build_warm_s"], 3),
                        "fp32_init_s": round(ix.timings["aknn_build_fp32_s"], 3),

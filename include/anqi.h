@@ -221,6 +221,19 @@ typedef struct {
 int anqi_graph_build(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* warm_ids,
                      uint32_t warm_stride, const anqi_graph_params* p, uint32_t* deg, uint32_t* links,
                      anqi_build_stats* st);
+/* The same build with the warm start delivered in row chunks, so the host
+ * holds one chunk of ids at a time (the reference's streamed warm start,
+ * include/index.h:1127-1203, fed by ANQI_PREBUILT_WARM_START_COMMAND or the
+ * compacted id file, src/rknn_query.cpp:988-1057).  begin: lifted rows to the
+ * device and the entry tree; warm_rows: rows [row0, row0 + rows) of the ids,
+ * `stride` per row (the first p->warm_width used), each row exactly once, in
+ * any order; finish: LocalJoin, gather + prune, commit, outputs as
+ * anqi_graph_build.  A new begin discards a build in progress; finish fails
+ * (ANQI_ERR_ARGS) unless every row was delivered.  anqi_graph_build is begin
+ * + one warm_rows over all rows + finish. */
+int anqi_graph_build_begin(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const anqi_graph_params* p);
+int anqi_graph_build_warm_rows(anqi_ctx* ctx, uint64_t row0, uint64_t rows, const uint32_t* ids, uint32_t stride);
+int anqi_graph_build_finish(anqi_ctx* ctx, uint32_t* deg, uint32_t* links, anqi_build_stats* st);
 /* Entry tree of the last anqi_graph_build, breadth-first arrays (see anqi_rp_forest). */
 int anqi_graph_tree_size(anqi_ctx* ctx, uint32_t* n_nodes, uint64_t* n_points);
 int anqi_graph_tree_copy(anqi_ctx* ctx, uint32_t* left, uint32_t* right, float* offset, float* hyperplane,
@@ -420,6 +433,38 @@ int anqi_lrq_objective_forward(const double* T, uint64_t n, uint32_t nk, uint32_
 int anqi_lrq_objective_backward(const double* T, uint64_t n, uint32_t nk, uint32_t m, const double* mu,
                                 const double* G, const double* r, const double* c, const uint8_t* a, uint32_t cs,
                                 double scale, double* g_mu, double* g_G, double* g_B, void* stream);
+
+/* ------------------------------------------- LRQ fit on the device
+ * The trainer's rounds (tools/train_final_m8_u8.py:81-258) as FP64 kernels; a
+ * host driver keeps the nk x nk eigen-decomposition.  DEVICE pointers, the
+ * caller's stream, nothing allocated; scratch sizes are checked
+ * (ANQI_ERR_CAPACITY).  keys: cutoff rows (rows x nk, f32, row-major); ids:
+ * the rows used (NULL = the first m).  nk <= 128, rank <= 16, cs <= 256.
+ * Results agree with the NumPy fit to rounding (sums run in other orders),
+ * not bit for bit.
+ * stats: mean (nk) and covariance (nk x nk, divided by m) of keys[ids] - sub,
+ *   sub nk x m column-major or NULL (fit_basis, :81-89); scratch
+ *   ceil(m / 1024) * nk * nk doubles.
+ * residual: res = T - (mu + ((T - mu) G^T) G), nk x m column-major
+ *   (reconstruct, :90-93); *status |= 1 on a non-finite value.
+ * range: lohi[2k], lohi[2k+1] = min, max over all n rows of column k of
+ *   the residual (:159-174).
+ * codebooks: per column, the sorted residuals' 1-D Lloyd (quantile
+ *   centres, prefix-sum cell means, monotone repair, stop below 1e-12;
+ *   :97-144); scratch anqi_lrq_fit_codebooks_scratch(m, nk) doubles.
+ * decode: dec = nearest centre (lower on ties; :146-156), nk x m; partial
+ *   receives *n_partial per-block sums of (dec - res)^2. */
+int anqi_lrq_fit_stats(const float* keys, const uint32_t* ids, uint64_t m, uint32_t nk, const double* sub,
+                       double* scratch, uint64_t scratch_doubles, double* mean, double* cov, void* stream);
+int anqi_lrq_fit_residual(const float* keys, const uint32_t* ids, uint64_t m, uint32_t nk, const double* mu,
+                          const double* basis, uint32_t rank, double* res, uint32_t* status, void* stream);
+int anqi_lrq_fit_range(const float* keys, uint64_t n, uint32_t nk, const double* mu, const double* basis,
+                       uint32_t rank, double* lohi, uint32_t* status, void* stream);
+uint64_t anqi_lrq_fit_codebooks_scratch(uint64_t m, uint32_t nk);
+int anqi_lrq_fit_codebooks(const double* res, uint64_t m, uint32_t nk, uint32_t cs, uint32_t iters, double* scratch,
+                           uint64_t scratch_doubles, double* codebooks, void* stream);
+int anqi_lrq_fit_decode(const double* res, uint64_t m, uint32_t nk, const double* codebooks, uint32_t cs, double* dec,
+                        double* partial, uint32_t partial_cap, uint32_t* n_partial, void* stream);
 
 /* ------------------------------------------ BF16 tensor-core tiles
  * out[i, j] = <bf16(a_i), bf16(b_j)> accumulated in FP32 on the tcgen05 tensor

@@ -246,3 +246,26 @@ def test_rknn_finds_and_validates_the_reference_caches(tmp_path):
     assert degree and degree[0] in out
     if rc != 0:  # no device here: everything up to the device stage ran
         assert rc == 7 and "no usable CUDA device" in err
+
+
+def test_rknn_u8_base_validation(tmp_path):
+    """ANQI_BASE_U8BIN (rknn_query.cpp:55-107): a missing or mis-sized uint8
+    base exits 3 with the reference's messages, before any device work."""
+    pfx, env, _ = sample_prefix(tmp_path)
+    rc, _, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10,
+                     env={**env, "ANQI_BASE_U8BIN": str(tmp_path / "missing.u8bin")})
+    assert rc == 3 and "cannot open uint8 base" in err
+    bad = tmp_path / "bad.u8bin"
+    bad.write_bytes(np.array([256, 8], np.uint32).tobytes() + bytes(256 * 8 - 1))
+    rc, _, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10, env={**env, "ANQI_BASE_U8BIN": str(bad)})
+    assert rc == 3 and "bad uint8 base" in err
+
+
+def test_rknn_streamed_warm_start_options(tmp_path):
+    """The streamed warm start takes one source: a command or the compacted
+    id file, not both (rknn_query.cpp:2106-2111)."""
+    pfx, env, _ = sample_prefix(tmp_path)
+    rc, _, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10,
+                     env={**env, "ANQI_PREBUILT_WARM_START_COMMAND": "cat /dev/null",
+                          "ANQI_COMPACT_PREBUILT_TOPK_IDS_INPLACE": "1"})
+    assert rc == 2 and "cannot be combined" in err

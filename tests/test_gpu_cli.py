@@ -273,3 +273,70 @@ def test_rknn_query_cli_ip_matches_reference_lines(tmp_path):
         assert sorted(got) == [16, 32, 64, 128]
         for L, v in got.items():
             assert v == ref_lines[k, L], (k, L, v, ref_lines[k, L])
+
+
+def test_rknn_query_u8_base_equals_float_base(tmp_path):
+    """ANQI_BASE_U8BIN: an integer-valued base given as uint8 gives the result
+    lines of the same base given as float32 (the values widen exactly), with
+    the uint8 file named in the cache identity."""
+    from anqi import pipeline
+    from anqi._lib import Context
+    base, query = pipeline.mixture(3000, 16, 200, centers=20, sigma=20.0, seed=5)
+    with Context(0) as ctx:
+        ix = pipeline.build_index(ctx, base, aknn=dict(k=100, leaf=200, trees=8, ef=200), log=lambda *a: None)
+        _, keys = pipeline.exact_thresholds(ctx, base, 100)
+        gt = {k: pipeline.rknn_ground_truth(ctx, base, query, keys[:, k - 1]) for k in (10, 50, 100)}
+    pfx = tmp_path / "mix"
+    pipeline.write_prefix(str(pfx), base, query, ix, gt)
+    u8 = tmp_path / "mix_base.u8bin"
+    u8.write_bytes(np.array(base.shape, np.uint32).tobytes() + base.astype(np.uint8).tobytes())
+    assert np.array_equal(base.astype(np.uint8).astype(np.float32), base)
+    outs = []
+    for name, extra in (("f32", {}), ("u8", {"ANQI_BASE_U8BIN": str(u8)})):
+        env = dict(tc.RUN_FINAL_ENV, ANQI_PREBUILT_TOPK_REC=f"{pfx}_baseknn_aknn.rec",
+                   ANQI_GRAPH_CACHE_DIR=str(tmp_path / name / "graph"),
+                   ANQI_VERIFIER_CACHE_DIR=str(tmp_path / name / "verifier"), **extra)
+        rc, out, err = tc.run("rknn_query", "16,64", pfx, 48, 500, 64, 600, 10, env=env)
+        assert rc == 0, err
+        assert ("loaded uint8 base directly as float" in out) == (name == "u8")
+        outs.append(lines(out))
+    assert outs[0] == outs[1] and sorted(outs[0]) == [16, 64]
+
+
+@pytest.mark.parametrize("mode", ["command", "compact", "release"])
+def test_rknn_query_streamed_warm_start(tmp_path, mode):
+    """The streamed G48 warm start (index.h:1127-1203) gives the graph and the
+    result lines of the in-memory one: from a command's stdout
+    (ANQI_PREBUILT_WARM_START_COMMAND), from the table compacted to ids in
+    place and then removed (ANQI_COMPACT_PREBUILT_TOPK_IDS_INPLACE), or with
+    the table released after preparation (ANQI_RELEASE_PREBUILT_TOPK_AFTER_PREP)."""
+    import shutil
+    pfx, env, z = tc.sample_prefix(tmp_path, 32)
+    rc, ref_out, err = tc.run("rknn_query", "16,32,64", pfx, 48, 500, 64, 600, 50, env=env)
+    assert rc == 0, err
+    rec = Path(f"{pfx}_baseknn_aknn.rec")
+    copy = tmp_path / "warm.rec"
+    shutil.copy(rec, copy)
+    env2 = dict(env, ANQI_GRAPH_CACHE_DIR=str(tmp_path / "g2"), ANQI_VERIFIER_CACHE_DIR=str(tmp_path / "v2"))
+    if mode == "command":
+        env2["ANQI_PREBUILT_WARM_START_COMMAND"] = f"cat {copy}"
+    elif mode == "compact":
+        env2["ANQI_COMPACT_PREBUILT_TOPK_IDS_INPLACE"] = "1"
+        env2["ANQI_PREBUILT_TOPK_REC"] = str(copy)
+    else:
+        env2["ANQI_RELEASE_PREBUILT_TOPK_AFTER_PREP"] = "1"
+        env2["ANQI_PREBUILT_TOPK_REC"] = str(copy)
+    rc, out, err = tc.run("rknn_query", "16,32,64", pfx, 48, 500, 64, 600, 50, env=env2)
+    assert rc == 0, err
+    assert lines(out) == lines(ref_out)
+    g1 = list(Path(env["ANQI_GRAPH_CACHE_DIR"]).glob("fd_metric_*"))
+    g2 = list((tmp_path / "g2").glob("fd_metric_*"))
+    assert len(g1) == 1 and len(g2) == 1
+    # the same adjacency and entry tree: all but the build-time field
+    # ([u64 n, dim, M][f32 seconds], then the rows and the tree)
+    a, b = g1[0].read_bytes(), g2[0].read_bytes()
+    assert len(a) == len(b) and a[:24] == b[:24] and a[28:] == b[28:]
+    if mode == "command":
+        assert "source=prebuilt-stream" in out and copy.exists()
+    else:
+        assert not copy.exists()
