@@ -204,7 +204,7 @@ def exact_thresholds(ctx: Context, base: np.ndarray, K: int = 100, method: str =
     -<a, b> (FP32 CUDA cores)."""
     base = np.ascontiguousarray(base, np.float32)
     n, d = base.shape
-    if method == "tc" and d <= 208 and metric == "l2":
+    if method == "tc" and d <= 1024 and metric == "l2":
         return ctx.exact_topk_tc(base, K, hints)
     ids = np.empty((n, K), np.uint32)
     keys = np.empty((n, K), np.float32)
@@ -215,7 +215,7 @@ def exact_thresholds(ctx: Context, base: np.ndarray, K: int = 100, method: str =
 def rknn_ground_truth(ctx: Context, base: np.ndarray, query: np.ndarray, rk2: np.ndarray, method: str = "fp32",
                       metric: str = "l2"):
     """Exact RkNN CSR (dataset_gt --mode ground-truth); method "tc" as above."""
-    if method == "tc" and base.shape[1] <= 208 and metric == "l2":
+    if method == "tc" and base.shape[1] <= 1024 and metric == "l2":
         return ctx.rknn_ground_truth_tc(base, query, rk2)
     base = np.ascontiguousarray(base, np.float32)
     query = np.ascontiguousarray(query, np.float32)

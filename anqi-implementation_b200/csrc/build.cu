@@ -1619,8 +1619,9 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
                     maxcnt = std::max(maxcnt, f.leaf_cnt[g]);
                 }
             }
-        // the tensor-core tiles hold rows of up to 256 (padded) dimensions
-        if (ap->precision == 1 && !ip && round_up(d, 16u) <= 256) {
+        // the tensor-core tiles: query tile resident up to 256 (padded)
+        // dimensions, K-chunked up to 1024
+        if (ap->precision == 1 && !ip && tc_padded_dim(d) != 0) {
             // BF16 tensor-core leaf tiles: candidates per tree, then the merge
             TcPrep tp;
             // candidate buffers (n x cap entries; GBs at 1M) are kept by the

@@ -209,6 +209,9 @@ struct TcPrep {
     float bnorm = 0, berr = 0, bn = 0;  // maxima of |x|, |x - bf16(x)|, the FP32 norm
     int all_exact = 0;                  // every row exact-integer
 };
+// Padded row length of the tensor path for dimension d: resident query tiles
+// up to 256, the wide (K-chunked) form up to 1024; 0 above.
+uint32_t tc_padded_dim(uint32_t d);
 int tc_prep(Ctx* c, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs, uint32_t d, TcPrep& tp);
 void tc_release(Ctx* c, TcPrep& tp);
 // LocalJoin precision form: for each source u's samples (samp, scnt; S <= 32)

@@ -87,15 +87,16 @@ __device__ __forceinline__ void cp_async_wait_all_() {
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Issues the dp/16 MMA steps of one 128 x 128 tile.
+// Issues the dp/16 MMA steps of one 128 x 128 tile (K = dp elements staged
+// at a and b); the first step accumulates onto TMEM when `accumulate`.
 __device__ __forceinline__ void issue_tile_mma(uint32_t tmem_d, const unsigned char* a, const unsigned char* b,
-                                               uint32_t dp) {
+                                               uint32_t dp, bool accumulate = false) {
     constexpr uint32_t idesc = tc::idesc_bf16_f32(kTile, kTile);
     const uint32_t sa = tc::smem_u32(a), sb = tc::smem_u32(b);
     for (uint32_t s = 0; s < dp / 16; s++) {
         const uint64_t ad = tc::smem_desc(sa + 2 * s * kTile * 16, kTile * 16, 128);
         const uint64_t bd = tc::smem_desc(sb + 2 * s * kTile * 16, kTile * 16, 128);
-        tc::mma_bf16(tmem_d, ad, bd, idesc, s > 0 ? 1u : 0u);
+        tc::mma_bf16(tmem_d, ad, bd, idesc, (s > 0 || accumulate) ? 1u : 0u);
     }
 }
 
@@ -194,6 +195,13 @@ struct FilterParams {
 
 constexpr uint32_t kStages = 2;  // base-tile ring; two CTAs fit an SM (shared memory, TMEM)
 constexpr uint32_t kFilterThreads = 256;
+// Wide form (rows too long to keep the query tile resident, dp > kMaxDp): per
+// base tile, the query and base rows pass through a ring of K chunks
+// (kWideK elements of 128 rows each, both operands) and the MMAs of the
+// chunks accumulate in TMEM.
+constexpr uint32_t kWideK = 64;
+constexpr uint32_t kWideStages = 4;
+constexpr uint32_t kWideMaxDp = 1024;
 
 // The reference's FP32 key |q|^2 + |x|^2 - 2 <q, x> (dataset_gt.cpp:225, 294)
 // with <q, x> in the 16-lane AVX-512 order of include/distance.h:89-116,
@@ -225,16 +233,20 @@ __device__ __forceinline__ float ref_key(const float* __restrict__ q, const floa
     return __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, ip));
 }
 
-__global__ void __launch_bounds__(kFilterThreads, 2) tc_filter_kernel(FilterParams p) {
+template <bool kWide>
+__global__ void __launch_bounds__(kFilterThreads, kWide ? 1 : 2) tc_filter_kernel(FilterParams p) {
     extern __shared__ __align__(128) unsigned char sm[];
-    const uint32_t tile_bytes = kTile * p.dp * 2;
+    // resident form: the query tile, then kStages base tiles; wide form:
+    // kWideStages query chunks, then kWideStages base chunks
+    const uint32_t tile_bytes = kTile * (kWide ? kWideK : p.dp) * 2;
     unsigned char* sa = sm;
-    unsigned char* sb = sm + tile_bytes;                                         // kStages tiles
-    float* col = reinterpret_cast<float*>(sb + (size_t)kStages * tile_bytes);   // kStages x 4 x 128
+    unsigned char* sb = sm + (size_t)(kWide ? kWideStages : 1) * tile_bytes;
+    float* col = reinterpret_cast<float*>(sb + (size_t)(kWide ? kWideStages : kStages) * tile_bytes);  // kStages x 4 x 128
     uint8_t* colint = reinterpret_cast<uint8_t*>(col + kStages * 4 * kTile);    // kStages x 128
     uint64_t* rowid = reinterpret_cast<uint64_t*>(colint + kStages * kTile);    // 128 (aligned: 2*... bytes)
     uint32_t* colid = reinterpret_cast<uint32_t*>(rowid + kTile);                // kStages x 128 (leaf mode)
     __shared__ uint64_t bar[2];
+    __shared__ uint64_t cbar[kWideStages];  // wide form: chunk slot free again
     __shared__ uint32_t tslot;
     __shared__ int s_abort;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -262,13 +274,14 @@ __global__ void __launch_bounds__(kFilterThreads, 2) tc_filter_kernel(FilterPara
     if (threadIdx.x == 0) {
         tc::mbar_init(&bar[0], 1);
         tc::mbar_init(&bar[1], 1);
+        for (uint32_t k = 0; k < kWideStages; k++) tc::mbar_init(&cbar[k], 1);
         tc::fence_mbar_init();
         s_abort = 0;
     }
     __syncthreads();
 
-    // A: the query tile (gathered rows)
-    const uint32_t chunks = p.dp / 8;
+    // A: the query tile (gathered rows), resident form only
+    const uint32_t chunks = kWide ? 0u : p.dp / 8;
     for (uint32_t t = threadIdx.x; t < kTile * chunks; t += blockDim.x) {
         const uint32_t rr = t % kTile, c = t / kTile;
         const uint64_t row = rowid[rr];
@@ -281,7 +294,7 @@ __global__ void __launch_bounds__(kFilterThreads, 2) tc_filter_kernel(FilterPara
         const uint32_t st = t % kStages;
         const uint64_t j0 = js + (uint64_t)t * kTile;
         unsigned char* dst = sb + (size_t)st * tile_bytes;
-        for (uint32_t i = threadIdx.x; i < kTile * chunks; i += blockDim.x) {
+        for (uint32_t i = threadIdx.x; i < kTile * chunks; i += blockDim.x) {  // (no operand in the wide form)
             const uint32_t rr = i % kTile, c = i / kTile;
             const uint64_t pos = j0 + rr;
             const bool ok = pos < je;
@@ -301,9 +314,11 @@ __global__ void __launch_bounds__(kFilterThreads, 2) tc_filter_kernel(FilterPara
             colint[st * kTile + threadIdx.x] = ok ? p.xint[j] : 0;
         }
     };
-    if (T > 0) prefetch(0);
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    if (T > 1) prefetch(1);
+    if (!kWide) {
+        if (T > 0) prefetch(0);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        if (T > 1) prefetch(1);
+    }
 
     // per-row constants of the error bound
     const uint64_t my_row = rowid[r];
@@ -327,6 +342,71 @@ __global__ void __launch_bounds__(kFilterThreads, 2) tc_filter_kernel(FilterPara
     // |x|, |x - bf16(x)| and norm; exact rows against all-exact columns: 0)
     const float epsmax = (qexact && p.all_exact) ? 0.f : fmaf(ca, p.bx_norm, fmaf(cb, p.bx_err, fmaf(cc, p.bx_n, cd)));
 
+    // the filter of tile e's 128 x 128 block (TMEM buffer e & 1, column data
+    // in stage e % kStages): each thread its row, each warp half the columns
+    auto epilogue = [&](uint32_t e, uint32_t tmem) {
+        const uint32_t st = e % kStages;
+        const float* cs = col + (size_t)st * 4 * kTile;
+        const uint64_t j0 = js + (uint64_t)e * kTile;
+        for (uint32_t c0 = half * 64; c0 < half * 64 + 64; c0 += 32) {
+            float v[32];
+            tc::tmem_ld32(tmem + (((warp & 3u) * 32u) << 16) + (e & 1u) * kTile + c0, v);
+            if (!row_ok) continue;
+            // columns that survive the row's eps bound, without branches:
+            // 4 norms (and thresholds) per shared load
+            const bool rowthr = p.thr_row || leaf;
+            uint32_t keep = 0;
+#pragma unroll
+            for (uint32_t k = 0; k < 32; k += 4) {
+                const float4 xn4 = *reinterpret_cast<const float4*>(cs + c0 + k);
+                const float4 th4 = rowthr ? make_float4(thr_r, thr_r, thr_r, thr_r)
+                                          : *reinterpret_cast<const float4*>(cs + 3 * kTile + c0 + k);
+                const float xa[4] = {xn4.x, xn4.y, xn4.z, xn4.w}, ta[4] = {th4.x, th4.y, th4.z, th4.w};
+#pragma unroll
+                for (uint32_t q = 0; q < 4; q++) {
+                    const float approx = __fsub_rn(__fadd_rn(qn, xa[q]), __fmul_rn(2.0f, v[k + q]));
+                    keep |= (approx - epsmax <= ta[q] ? 1u : 0u) << (k + q);
+                }
+            }
+            for (; keep; keep &= keep - 1) {
+                const uint32_t k = __ffs(keep) - 1;
+                const uint32_t cj = c0 + k;
+                const uint64_t j = leaf ? (uint64_t)colid[st * kTile + cj] : j0 + cj;
+                const float xn = cs[cj];
+                float vk = 0.f;
+#pragma unroll
+                for (uint32_t q = 0; q < 32; q++)
+                    if (q == k) vk = v[q];
+                const float approx = __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, vk));
+                const float thr = rowthr ? thr_r : cs[3 * kTile + cj];
+                const bool exact = qexact && colint[st * kTile + cj];
+                const float eps =
+                    exact ? 0.f : fmaf(ca, cs[kTile + cj], fmaf(cb, cs[2 * kTile + cj], fmaf(cc, xn, cd)));
+                if (!(approx - eps <= thr)) continue;
+                if (p.exclude_self && j == my_row) continue;
+                if (leaf) {
+                    // the merge recomputes flagged keys in FP32 and keeps <= its K-th;
+                    // slots are indexed by the row's position in the batch of leaves
+                    const uint64_t cs0 = lt.off + (uint64_t)lt.rb * kTile + r - p.pos_base;
+                    const uint32_t pos = atomicAdd(p.cnt + cs0, 1u);
+                    if (pos < p.cap) {
+                        p.out_id[cs0 * p.cap + pos] = (uint32_t)j | (exact ? 0u : kRecheck);
+                        p.out_key[cs0 * p.cap + pos] = approx;
+                    }
+                    continue;
+                }
+                const float key = exact ? approx : ref_key(qrow, p.x32 + j * p.xs, p.d, qn, xn);
+                if (!(key <= thr)) continue;
+                const uint32_t pos = atomicAdd(p.cnt + my_row, 1u);
+                if (pos < p.cap) {
+                    p.out_id[my_row * p.cap + pos] = (uint32_t)j;
+                    p.out_key[my_row * p.cap + pos] = key;
+                }
+            }
+        }
+    };
+
+    if constexpr (!kWide) {
     for (uint32_t t = 0; t <= T; t++) {
         // tile t (prefetched one iteration ahead) and the query tile resident
         // and visible to the tensor cores; TMEM buffer t & 1 free (its last
@@ -351,67 +431,7 @@ __global__ void __launch_bounds__(kFilterThreads, 2) tc_filter_kernel(FilterPara
             atomicExch(p.err, 8u);
         }
         tc::fence_after_sync();
-        if (ok) {
-            const uint32_t st = e % kStages;
-            const float* cs = col + (size_t)st * 4 * kTile;
-            const uint64_t j0 = js + (uint64_t)e * kTile;
-            for (uint32_t c0 = half * 64; c0 < half * 64 + 64; c0 += 32) {
-                float v[32];
-                tc::tmem_ld32(tmem + (((warp & 3u) * 32u) << 16) + (e & 1u) * kTile + c0, v);
-                if (!row_ok) continue;
-                // columns that survive the row's eps bound, without branches:
-                // 4 norms (and thresholds) per shared load
-                const bool rowthr = p.thr_row || leaf;
-                uint32_t keep = 0;
-#pragma unroll
-                for (uint32_t k = 0; k < 32; k += 4) {
-                    const float4 xn4 = *reinterpret_cast<const float4*>(cs + c0 + k);
-                    const float4 th4 = rowthr ? make_float4(thr_r, thr_r, thr_r, thr_r)
-                                              : *reinterpret_cast<const float4*>(cs + 3 * kTile + c0 + k);
-                    const float xa[4] = {xn4.x, xn4.y, xn4.z, xn4.w}, ta[4] = {th4.x, th4.y, th4.z, th4.w};
-#pragma unroll
-                    for (uint32_t q = 0; q < 4; q++) {
-                        const float approx = __fsub_rn(__fadd_rn(qn, xa[q]), __fmul_rn(2.0f, v[k + q]));
-                        keep |= (approx - epsmax <= ta[q] ? 1u : 0u) << (k + q);
-                    }
-                }
-                for (; keep; keep &= keep - 1) {
-                    const uint32_t k = __ffs(keep) - 1;
-                    const uint32_t cj = c0 + k;
-                    const uint64_t j = leaf ? (uint64_t)colid[st * kTile + cj] : j0 + cj;
-                    const float xn = cs[cj];
-                    float vk = 0.f;
-#pragma unroll
-                    for (uint32_t q = 0; q < 32; q++)
-                        if (q == k) vk = v[q];
-                    const float approx = __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, vk));
-                    const float thr = rowthr ? thr_r : cs[3 * kTile + cj];
-                    const bool exact = qexact && colint[st * kTile + cj];
-                    const float eps =
-                        exact ? 0.f : fmaf(ca, cs[kTile + cj], fmaf(cb, cs[2 * kTile + cj], fmaf(cc, xn, cd)));
-                    if (!(approx - eps <= thr)) continue;
-                    if (p.exclude_self && j == my_row) continue;
-                    if (leaf) {
-                        // the merge recomputes flagged keys in FP32 and keeps <= its K-th;
-                        // slots are indexed by the row's position in the batch of leaves
-                        const uint64_t cs0 = lt.off + (uint64_t)lt.rb * kTile + r - p.pos_base;
-                        const uint32_t pos = atomicAdd(p.cnt + cs0, 1u);
-                        if (pos < p.cap) {
-                            p.out_id[cs0 * p.cap + pos] = (uint32_t)j | (exact ? 0u : kRecheck);
-                            p.out_key[cs0 * p.cap + pos] = approx;
-                        }
-                        continue;
-                    }
-                    const float key = exact ? approx : ref_key(qrow, p.x32 + j * p.xs, p.d, qn, xn);
-                    if (!(key <= thr)) continue;
-                    const uint32_t pos = atomicAdd(p.cnt + my_row, 1u);
-                    if (pos < p.cap) {
-                        p.out_id[my_row * p.cap + pos] = (uint32_t)j;
-                        p.out_key[my_row * p.cap + pos] = key;
-                    }
-                }
-            }
-        }
+        if (ok) epilogue(e, tmem);
         // stage (t + 1) % 2 held tile e: its MMA finished (waited above); once
         // every warp has left its epilogue the stage is refilled
         if (t + 1 < T) {
@@ -419,6 +439,75 @@ __global__ void __launch_bounds__(kFilterThreads, 2) tc_filter_kernel(FilterPara
             prefetch(t + 1);
         }
         tc::fence_before_sync();
+    }
+    } else {
+        // per base tile t: its nc K chunks through the ring (slot it % kWideStages,
+        // free again when the MMAs of chunk it - kWideStages are done), one MMA
+        // batch per chunk into TMEM buffer t & 1; then the epilogue of tile t - 1
+        // while the tensor cores finish tile t
+        const uint32_t nc = p.dp / kWideK;
+        uint32_t it = 0;
+        bool stop = false;
+        for (uint32_t t = 0; t <= T && !stop; t++) {
+            const uint32_t tmem = tslot;
+            if (t < T) {
+                const uint64_t j0 = js + (uint64_t)t * kTile;
+                for (uint32_t c = 0; c < nc; c++, it++) {
+                    const uint32_t slot = it % kWideStages;
+                    if (it >= kWideStages &&
+                        !tc::mbar_wait(&cbar[slot], ((it / kWideStages) - 1u) & 1u, kWaitPolls)) {
+                        s_abort = 1;
+                        atomicExch(p.err, 8u);
+                    }
+                    unsigned char* da = sa + (size_t)slot * tile_bytes;
+                    unsigned char* db = sb + (size_t)slot * tile_bytes;
+                    constexpr uint32_t kGroups = kWideK / 8;  // 16-byte groups of a chunk row
+                    for (uint32_t i = threadIdx.x; i < kTile * kGroups; i += blockDim.x) {
+                        const uint32_t rr = i % kTile, q = i / kTile;
+                        const uint64_t row = rowid[rr];
+                        const bool oka = row != ~0ull;
+                        tc::cp_async16_zfill(da + (size_t)q * kTile * 16 + rr * 16,
+                                             p.qb + (oka ? row : 0) * p.dp + c * kWideK + 8 * q, oka ? 16u : 0u);
+                        const uint64_t pos = j0 + rr;
+                        const bool okb = pos < je;
+                        const uint64_t brow = okb ? (leaf ? (uint64_t)mem[pos] : pos) : 0;
+                        tc::cp_async16_zfill(db + (size_t)q * kTile * 16 + rr * 16,
+                                             p.xb + brow * p.dp + c * kWideK + 8 * q, okb ? 16u : 0u);
+                    }
+                    if (c == 0) {
+                        // column data of tile t: stage t % kStages was last read by
+                        // the epilogue of tile t - 2, which every thread has left
+                        if (t >= 2) __syncthreads();
+                        prefetch(t);
+                    }
+                    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+                    tc::fence_async_smem();
+                    tc::fence_before_sync();
+                    __syncthreads();
+                    tc::fence_after_sync();
+                    if (s_abort) {  // uniform: read after the barrier
+                        stop = true;
+                        break;
+                    }
+                    if (threadIdx.x == 0) {
+                        issue_tile_mma(tmem + (t & 1u) * kTile, da, db, kWideK, c > 0);
+                        tc::mma_commit(&cbar[slot]);
+                        if (c + 1 == nc) tc::mma_commit(&bar[t & 1u]);
+                    }
+                }
+                if (stop) break;
+            }
+            if (t == 0) continue;
+            const uint32_t e = t - 1;
+            const bool ok = tc::mbar_wait(&bar[e & 1u], (e >> 1) & 1u, kWaitPolls);
+            if (!ok) {
+                s_abort = 1;
+                atomicExch(p.err, 8u);
+            }
+            tc::fence_after_sync();
+            if (ok) epilogue(e, tmem);
+            tc::fence_before_sync();
+        }
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     tc::fence_before_sync();
@@ -550,14 +639,34 @@ __global__ void take_first_k_kernel(const uint64_t* __restrict__ off, uint64_t n
 }
 
 size_t filter_smem(uint32_t dp) {
-    return (size_t)(1 + kStages) * kTile * dp * 2 + (size_t)kStages * 4 * kTile * 4 + kStages * kTile + kTile * 8 +
-           (size_t)kStages * kTile * 4;
+    const size_t operands = dp > kMaxDp ? (size_t)2 * kWideStages * kTile * kWideK * 2 : (size_t)(1 + kStages) * kTile * dp * 2;
+    return operands + (size_t)kStages * 4 * kTile * 4 + kStages * kTile + kTile * 8 + (size_t)kStages * kTile * 4;
+}
+
+// The padded dimension of the tensor path for d: a multiple of 16 with the
+// query tile resident (up to kMaxDp), else a multiple of kWideK for the wide
+// form (up to kWideMaxDp); 0 when d is too large.
+uint32_t tc_dp(uint32_t d) {
+    const uint32_t dp = round_up(d, 16u);
+    if (dp <= kMaxDp && filter_smem(dp) <= 227 * 1024) return dp;
+    const uint32_t dw = round_up(d, kWideK);
+    return dw <= kWideMaxDp ? dw : 0u;
+}
+
+// The filter kernel for p.dp (resident or wide form) with its shared memory.
+int filter_kernel_for(Ctx* c, uint32_t dp, void (**kern)(FilterParams), size_t* smem) {
+    *kern = dp > kMaxDp ? tc_filter_kernel<true> : tc_filter_kernel<false>;
+    *smem = filter_smem(dp);
+    ANQI_CUDA(c, cudaFuncSetAttribute(*kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+    return ANQI_OK;
 }
 
 int launch_filter(Ctx* c, FilterParams p, uint64_t nrows) {
     if (nrows == 0) return ANQI_OK;
-    const size_t smem = filter_smem(p.dp);
-    ANQI_CUDA(c, cudaFuncSetAttribute(tc_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    void (*kern)(FilterParams) = nullptr;
+    size_t smem = 0;
+    int rc = filter_kernel_for(c, p.dp, &kern, &smem);
+    if (rc) return rc;
     const uint64_t gx = (nrows + kTile - 1) / kTile;
     const uint64_t tiles = (p.n + kTile - 1) / kTile;
     uint64_t gy = std::max<uint64_t>(1, ((uint64_t)2 * c->sm_count + gx - 1) / gx);
@@ -565,7 +674,7 @@ int launch_filter(Ctx* c, FilterParams p, uint64_t nrows) {
     p.split_len = (tiles + gy - 1) / gy * kTile;
     p.nrows = nrows;
     dim3 grid((unsigned)gx, (unsigned)gy);
-    tc_filter_kernel<<<grid, kFilterThreads, smem, c->stream>>>(p);
+    kern<<<grid, kFilterThreads, smem, c->stream>>>(p);
     ANQI_CUDA(c, cudaGetLastError());
     return ANQI_OK;
 }
@@ -645,9 +754,11 @@ int filter_to_csr(Ctx* c, FilterParams p, uint64_t nq, uint32_t cap, std::vector
 
 }  // namespace
 
+uint32_t tc_padded_dim(uint32_t d) { return tc_dp(d); }
+
 int tc_prep(Ctx* c, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs, uint32_t d, TcPrep& tp) {
-    tp.dp = round_up(d, 16u);
-    if (filter_smem(tp.dp) > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "dimension %u too large for the tensor path", d);
+    tp.dp = tc_dp(d);
+    if (tp.dp == 0) return fail(c, ANQI_ERR_ARGS, "dimension %u too large for the tensor path", d);
     int rc = tc_prepare_rows(c, d_x, n, xs, d, tp.dp, tp.bf, tp.nrm, tp.err, tp.xint);
     if (rc) return rc;
     return tc_row_bounds(c, d_norms, tp.nrm.as<float>(), tp.err.as<float>(), tp.xint.as<uint8_t>(), n, &tp.bnorm,
@@ -838,9 +949,10 @@ int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* 
     p.all_exact = tp.all_exact;
     p.nrows = tiles.size() * kTile;
     p.split_len = 0;
-    const size_t smem = filter_smem(p.dp);
-    ANQI_CUDA(c, cudaFuncSetAttribute(tc_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    tc_filter_kernel<<<(unsigned)tiles.size(), kFilterThreads, smem, c->stream>>>(p);
+    void (*kern)(FilterParams) = nullptr;
+    size_t smem = 0;
+    if ((rc = filter_kernel_for(c, p.dp, &kern, &smem))) return rc;
+    kern<<<(unsigned)tiles.size(), kFilterThreads, smem, c->stream>>>(p);
     ANQI_CUDA(c, cudaGetLastError());
     return check_device_error(c, "tensor-core init_knn filter");
 }
@@ -907,8 +1019,8 @@ int anqi_rknn_ground_truth_tc(anqi_ctx* h, const float* base, uint64_t n, const 
     if (!h || !base || !query || !rk2 || !off || n == 0 || nq == 0 || d == 0) return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
-    const uint32_t dp = round_up(d, 16u), xs = round_up(d, 8u);
-    if (filter_smem(dp) > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "dimension %u too large for the tensor path", d);
+    const uint32_t dp = tc_dp(d), xs = round_up(d, 8u);
+    if (dp == 0) return fail(c, ANQI_ERR_ARGS, "dimension %u too large for the tensor path", d);
     TcRows X(c), Q(c);
     TmpBuf dr(c), doff(c), did(c), dkey(c);
     int rc;
@@ -939,8 +1051,8 @@ int anqi_exact_topk_tc(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, u
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     if (K >= n) return fail(c, ANQI_ERR_ARGS, "require K < base vector count");
-    const uint32_t dp = round_up(d, 16u), xs = round_up(d, 8u);
-    if (filter_smem(dp) > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "dimension %u too large for the tensor path", d);
+    const uint32_t dp = tc_dp(d), xs = round_up(d, 8u);
+    if (dp == 0) return fail(c, ANQI_ERR_ARGS, "dimension %u too large for the tensor path", d);
     // hints: the caller's (e.g. AKNN lists) or an AKNN build here
     std::vector<uint32_t> own;
     if (!hints) {

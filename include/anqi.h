@@ -161,8 +161,8 @@ typedef struct {
     uint32_t nn_iters;   /* ANQI_NNITERS, default 0 */
     uint32_t nn_sample;  /* ANQI_NNSAMPLE, default 20 */
     uint32_t precision;  /* init_knn leaf distances: 0 = FP32 CUDA cores, 1 = BF16 tensor-core
-                            tiles with FP32 recheck (identical output; d <= 256, larger d
-                            runs on the CUDA cores) */
+                            tiles with FP32 recheck (identical output; d <= 1024, rows
+                            above 256 dimensions in K chunks; larger d runs on the CUDA cores) */
     uint32_t metric;     /* ANQI_METRIC_L2 (0) or ANQI_METRIC_IP; the ip metric runs FP32
                             init_knn on the CUDA cores and takes no LocalJoin (nn_iters = 0) */
 } anqi_aknn_params;
@@ -495,7 +495,9 @@ int anqi_rknn_ground_truth_metric(anqi_ctx* ctx, const float* base, uint64_t n, 
 /* Precision form of the two entry points above: BF16 tcgen05 tiles with FP32
  * accumulation filter every pair by a derived bound on |key~ - key32|; the
  * pairs within it are recomputed in the reference's FP32 order.  Outputs equal
- * anqi_exact_topk / anqi_rknn_ground_truth bit for bit.  d <= 208.
+ * anqi_exact_topk / anqi_rknn_ground_truth bit for bit.  d <= 1024: up to 256
+ * (padded to 16) the query tile stays in shared memory; above, both operands
+ * pass through a ring of 64-wide K chunks accumulating in TMEM.
  * anqi_exact_topk_tc bounds each row's K-th key by the largest FP32 key to K
  * distinct other rows: hints (n x hint_k ids, e.g. the AKNN lists, hint_k >= K)
  * or, when hints is NULL, an AKNN build run here. */

@@ -95,3 +95,35 @@ def test_rknn_gt_tc_reference_sample(ctx, sample):
         off, ids, keys = ctx.rknn_ground_truth_tc(sample["base"], sample["query"], sample["exact_keys"][:, k - 1])
         assert np.array_equal(off, sample[f"gt_off_{k}"]) and np.array_equal(ids, sample[f"gt_ids_{k}"])
         assert np.array_equal(bits(keys), bits(sample[f"gt_keys_{k}"]))
+
+
+def unit_gaussian(n, d, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(n, d))
+    return (x / np.linalg.norm(x, axis=1, keepdims=True)).astype(np.float32)
+
+
+@pytest.mark.parametrize("d", [300, 960])
+def test_wide_tensor_path_equals_fp32(ctx, d):
+    """Rows above 256 dimensions: both operands stream through the K-chunk
+    ring (64 elements per chunk, MMAs accumulating in TMEM).  Exact top-K,
+    RkNN CSR and the AKNN build with the tensor-core init_knn equal the FP32
+    path bit for bit (L2-normalised N(0,1) rows, the batching form's second
+    shape, and an integer mixture)."""
+    from anqi import pipeline
+    base = unit_gaussian(3000, d, d) if d == 960 else mixture(3000, d, 7, True)
+    base[11] = base[3]
+    query = unit_gaussian(300, d, d + 1) if d == 960 else mixture(300, d, 8, True)
+    ids32, keys32 = pipeline.exact_thresholds(ctx, base, 100)
+    ids, keys = ctx.exact_topk_tc(base, 100, hints=ids32)
+    assert np.array_equal(ids, ids32) and np.array_equal(bits(keys), bits(keys32))
+    ids2, keys2 = ctx.exact_topk_tc(base, 100)
+    assert np.array_equal(ids2, ids32) and np.array_equal(bits(keys2), bits(keys32))
+    for k in (10, 100):
+        off, gid, gkey = pipeline.rknn_ground_truth(ctx, base, query, keys32[:, k - 1])
+        off2, gid2, gkey2 = ctx.rknn_ground_truth_tc(base, query, keys32[:, k - 1])
+        assert np.array_equal(off, off2) and np.array_equal(gid, gid2) and np.array_equal(bits(gkey), bits(gkey2))
+        assert off[-1] > 0
+    a_ids, a_keys, _ = pipeline.aknn_build(ctx, base, k=50, leaf=300, trees=8, ef=150, precision="bf16")
+    f_ids, f_keys, _ = pipeline.aknn_build(ctx, base, k=50, leaf=300, trees=8, ef=150, precision="fp32")
+    assert np.array_equal(a_ids, f_ids) and np.array_equal(bits(a_keys), bits(f_keys))
