@@ -48,8 +48,8 @@ def mixture_queries(nq: int, d: int = 128, centers: int = 1000, sigma: float = 2
 
 def gaussian(n: int, d: int, nq: int, seed: int = 20260819, normalize: bool = False):
     rng = np.random.default_rng(seed)
-    b = rng.normal(0.0, 1.0, size=(n, d)).astype(np.float32)
-    q = rng.normal(0.0, 1.0, size=(nq, d)).astype(np.float32)
+    b = rng.standard_normal((n, d), dtype=np.float32)
+    q = rng.standard_normal((nq, d), dtype=np.float32)
     if normalize:
         b /= np.linalg.norm(b, axis=1, keepdims=True)
         q /= np.linalg.norm(q, axis=1, keepdims=True)

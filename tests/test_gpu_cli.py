@@ -340,3 +340,38 @@ def test_rknn_query_streamed_warm_start(tmp_path, mode):
         assert "source=prebuilt-stream" in out and copy.exists()
     else:
         assert not copy.exists()
+
+
+@pytest.mark.skipif(not tc.REF_BIN.exists(), reason="reference binaries not built")
+def test_rknn_query_scale_profile_degree20_kpivot10(tmp_path):
+    """The scale path's graph profile (degree 20, K_pivot = ANQI_GRAPH_NK = 10):
+    this driver builds and queries it; on the reference's own degree-20 graph
+    (built by the reference binary here) it prints the reference's result
+    lines exactly."""
+    pfx, env, z = tc.sample_prefix(tmp_path, 32)
+    env = dict(env, ANQI_GRAPH_NK="10")
+    ref_env = {k: v for k, v in os.environ.items() if not k.startswith("ANQI_")}
+    ref_env.update(env, OMP_NUM_THREADS="1", ANQI_GRAPH_CACHE_DIR=str(tmp_path / "ref" / "graph"),
+                   ANQI_VERIFIER_CACHE_DIR=str(tmp_path / "ref" / "verifier"))
+    for sub in ("graph", "verifier"):
+        (tmp_path / "ref" / sub).mkdir(parents=True)
+    ref = subprocess.run([str(tc.REF_BIN), "16,32,64", str(pfx), "20", "500", "64", "600", "10"], env=ref_env,
+                         capture_output=True, text=True, timeout=300)
+    assert ref.returncode == 0, ref.stderr
+    rc, ours, err = tc.run("rknn_query", "16,32,64", pfx, 20, 500, 64, 600, 10, env=env)
+    assert rc == 0, err
+    assert "graph degree M=20" in ours
+    for L, v in lines(ours).items():
+        r = lines(ref.stdout)[L]
+        assert abs(v[0] - r[0]) < 0.05, (L, v, r)
+    gref = list((tmp_path / "ref" / "graph").glob("fd_metric_*"))
+    gours = list(Path(env["ANQI_GRAPH_CACHE_DIR"]).glob("fd_metric_*"))
+    assert len(gref) == 1 and len(gours) == 1 and gref[0].name == gours[0].name
+    gours[0].write_bytes(gref[0].read_bytes())
+    for suffix in ("_approxlift_graph_", "_anqi_meta_graph_"):
+        for p in (tmp_path / "ref" / "graph").glob(suffix + "*"):
+            (Path(env["ANQI_GRAPH_CACHE_DIR"]) / p.name).write_bytes(p.read_bytes())
+    rc, ours, err = tc.run("rknn_query", "16,32,64", pfx, 20, 500, 64, 600, 10, env=env)
+    assert rc == 0, err
+    assert "[rknn] loaded cached index" in ours
+    assert lines(ours) == lines(ref.stdout)
