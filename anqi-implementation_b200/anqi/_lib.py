@@ -75,7 +75,7 @@ class GraphParams(C.Structure):
     _fields_ = [("degree", C.c_uint32), ("nn_k", C.c_uint32), ("explore", C.c_uint32), ("ef_alpha", C.c_uint32),
                 ("join_iters", C.c_uint32), ("join_sample", C.c_uint32), ("leaf", C.c_uint32),
                 ("max_depth", C.c_uint32), ("seed", C.c_uint64), ("alpha", C.c_float), ("warm_width", C.c_uint32),
-                ("precision", C.c_uint32)]
+                ("precision", C.c_uint32), ("vamana_passes", C.c_uint32), ("vamana_L", C.c_uint32)]
 
 
 class BuildStats(C.Structure):
@@ -139,6 +139,8 @@ _SIGS = {
     "anqi_graph_select": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _f32, C.c_uint32, C.c_uint32, C.c_uint32,
                           C.c_uint32, C.c_float, _u32, _u32],
     "anqi_graph_commit": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _u32, C.c_uint32, C.c_float, _u32, _u32],
+    "anqi_graph_vamana_select": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _u32, C.c_uint32, _u32, C.c_uint32, _u32,
+                                 C.c_uint32, C.c_float, _u32, _u32],
     "anqi_index_load": [_vp, C.POINTER(IndexDesc)],
     "anqi_verifier_load": [_vp, _f32, _u8, C.c_uint64, C.c_uint32, C.c_uint32, _f32, _f32, _f32, C.c_uint32],
     "anqi_verifier_load_bits": [_vp, _f32, _vp, _vp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, _f32, _f32,

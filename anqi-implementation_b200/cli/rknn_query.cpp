@@ -162,7 +162,17 @@ static std::string threshold_source_identity(const std::string& pfx) {
 static std::string graph_cache_key(uint64_t M, uint64_t leaf, uint64_t nt, uint64_t ef) {
     std::string k = "M" + std::to_string(M) + "_leaf" + std::to_string(leaf) + "_nt" + std::to_string(nt) + "_ef" +
                     std::to_string(ef) + "_geomanyk_lift_rankm0_specific0_alpha" + env_or("ANQI_ALPHA", "1.2") +
-                    "_liftnnk" + env_or("ANQI_LIFTNNK", "50") + "_graphnnd" + env_or("ANQI_GRAPHNND", "6") + "_vam0";
+                    "_liftnnk" + env_or("ANQI_LIFTNNK", "50") + "_graphnnd" + env_or("ANQI_GRAPHNND", "6");
+    if (std::getenv("ANQI_VAMANA")) {
+        const std::string style = env_or("ANQI_VAMANA_STYLE", "global");
+        k += "_vam1_style" + style + "_L" + env_or("ANQI_VAMANA_L", "128") + "_P" + env_or("ANQI_VAMANA_PASS", "2") +
+             "_bf" + env_or("ANQI_VAMANA_BATCH_FRAC", "0.02") + "_mb" + env_or("ANQI_VAMANA_MAX_BATCH", "1000000") +
+             "_bb" + env_or("ANQI_VAMANA_BATCH_BASE", "2") + "_ea" + env_or("ANQI_VAMANA_EARLY_ALPHA", "1.0") +
+             "_eao" + env_or("ANQI_VAMANA_EARLY_ALPHA_ONE", "1") + "_entry" + env_or("ANQI_VAMANA_ENTRY", "0");
+        if (style == "batch") k += "_implcsr1";
+    } else {
+        k += "_vam0";
+    }
     return sanitize_tag(k);
 }
 
@@ -641,8 +651,17 @@ static int run(int argc, char** argv) {
     if (env_flag("ANQI_RECHECK"))
         die(2, "[rknn] ANQI_RECHECK cannot be mixed with an independent postfilter verifier; select "
                "ANQI_RADIUS_MODE=exact_f32 for the exact component comparison");
-    for (const char* e : {"ANQI_VAMANA", "ANQI_EDGE_POLICY", "ANQI_REUSE_ORIG_KNN"})
+    for (const char* e : {"ANQI_EDGE_POLICY", "ANQI_REUSE_ORIG_KNN"})
         if (std::getenv(e)) not_here(e);
+    // the global Vamana refine (index.h:1262-1285); the batched variant is not built here
+    uint32_t vamana_passes = 0, vamana_L = 128;
+    if (std::getenv("ANQI_VAMANA")) {
+        const std::string style = env_or("ANQI_VAMANA_STYLE", "global");
+        if (style != "global" && style != "old") not_here("ANQI_VAMANA_STYLE=" + style);
+        vamana_passes = (uint32_t)std::max(0, std::atoi(env_or("ANQI_VAMANA_PASS", "2").c_str()));
+        vamana_L = (uint32_t)std::max(1, std::atoi(env_or("ANQI_VAMANA_L", "128").c_str()));
+        if (vamana_L > 1024) die(2, "[rknn] ANQI_VAMANA_L=%u exceeds the device beam limit 1024", vamana_L);
+    }
     if (env_or("ANQI_SEARCH_SCORE", "center") != "center") not_here("ANQI_SEARCH_SCORE=" + env_or("ANQI_SEARCH_SCORE", ""));
     if (std::getenv("ANQI_RCEPS") && std::atof(std::getenv("ANQI_RCEPS")) != 0.0) not_here("ANQI_RCEPS!=0");
     if (std::getenv("ANQI_RADIUS_RELAX") && std::atof(std::getenv("ANQI_RADIUS_RELAX")) != 0.0)
@@ -925,6 +944,8 @@ static int run(int argc, char** argv) {
         gp.alpha = alpha;
         gp.warm_width = (uint32_t)width;
         gp.precision = env_or("ANQI_B200_PRECISION", "bf16") == "fp32" ? 0u : 1u;
+        gp.vamana_passes = vamana_passes;
+        gp.vamana_L = vamana_L;
         deg.resize(n);
         links.resize(n * Marg);
         anqi_build_stats gs{};

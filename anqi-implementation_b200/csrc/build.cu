@@ -40,7 +40,11 @@ static double ms_since(Clock::time_point t0) {
 
 // ------------------------------------------------------------ gather
 
-enum GatherMode : int { kModeAknn = 0, kModeSelect = 1, kModeCommit = 2 };
+// kModeVamana: one pass of the global Vamana refine (index.h:856-875,
+// 1262-1285): the beam runs over the current graph from the row's entry,
+// without a pool cap, then the row's g0 list joins the pool, which is pruned
+// as in select mode.
+enum GatherMode : int { kModeAknn = 0, kModeSelect = 1, kModeCommit = 2, kModeVamana = 3 };
 
 // Pair keys: L2 through the norms (index.h:172-176); the ip metric's distance
 // 1 - <a, b>, one sequential sum per pair and so one lane per pair
@@ -83,6 +87,11 @@ struct GatherParams {
     uint32_t* gtab;                 // per-slot L2-resident visited tables (all kEmpty between rows)
     uint32_t gcap, gshift;          // entries per slot (power of two, 0 = none)
     uint32_t ip;  // AKNN mode only: keys are the ip metric's 1 - <a, b>
+    // Vamana mode: the current graph (links n x cur_M, degrees) and each row's entry
+    const uint32_t* cur_links;
+    const uint32_t* cur_deg;
+    uint32_t cur_M;
+    const uint32_t* entry;
     uint32_t* next_row;
     const uint32_t* row_order;  // work item -> row (rows of one RP-tree leaf together), or null for identity
     unsigned long long* pool_total;
@@ -303,7 +312,7 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
         uint64_t npool = 0;
         // one visited batch: pool (select mode), beam and top-K list
         auto take = [&](uint32_t m) {
-            if (p.mode == kModeSelect) {
+            if (p.mode == kModeSelect || p.mode == kModeVamana) {
                 for (uint32_t t = lane; t < m; t += 32)
                     if (npool + t < p.pool_cap) {
                         pd[npool + t] = nd[t];
@@ -321,8 +330,16 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
             }
             lo = min(lo, beam_insert(bd, bi, size, p.ef, nd, ni, m, lane));
         };
-        // seeds: the row's own list with its stored distances
-        for (uint32_t c0 = 0; c0 < p.K; c0 += 64) {
+        // seeds: the row's entry (Vamana), or the row's own list with its stored distances
+        if (p.mode == kModeVamana) {
+            const uint32_t ep = p.entry[i] < p.n ? p.entry[i] : 0u;
+            const uint32_t m = gather_visit(p, vis, nlog, lane == 0 ? ep : kEmpty, kEmpty, 0.f, 0.f, false, ni, nd, lane);
+            if (m) {
+                batch_d2<kIp>(p, i, ni, nd, m, gw, gt);
+                take(m);
+            }
+        }
+        for (uint32_t c0 = 0; p.mode != kModeVamana && c0 < p.K; c0 += 64) {
             const uint32_t m0 = min(64u, p.K - c0);
             uint32_t id0 = kEmpty, id1 = kEmpty;
             float v0 = 0.f, v1 = 0.f;
@@ -355,8 +372,9 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
             if (lane == 0) bi[cur] = node | kExpanded;
             __syncwarp();
             lo = cur + 1;
-            const uint64_t r0 = p.rev_off[node], r1 = p.rev_off[node + 1];
-            const uint32_t tot = p.K + (uint32_t)(r1 - r0);
+            const bool vam = p.mode == kModeVamana;
+            const uint64_t r0 = vam ? 0 : p.rev_off[node], r1 = vam ? 0 : p.rev_off[node + 1];
+            const uint32_t tot = vam ? min(p.cur_deg[node], p.cur_M) : p.K + (uint32_t)(r1 - r0);
             // list slots in chunks of 64 (slot c0 + lane, c0 + lane + 32); the
             // ids of four chunks are loaded together, one memory round trip
             for (uint32_t c0 = 0; c0 < tot; c0 += 256) {
@@ -364,8 +382,9 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
 #pragma unroll
                 for (uint32_t u = 0; u < 8; u++) {
                     const uint32_t pa = c0 + lane + 32 * u;
-                    ids[u] = pa < tot ? (pa < p.K ? p.g_ids[(uint64_t)node * p.K + pa] : p.rev_ids[r0 + (pa - p.K)])
-                                      : kEmpty;
+                    ids[u] = pa >= tot ? kEmpty
+                             : vam      ? p.cur_links[(uint64_t)node * p.cur_M + pa]
+                             : (pa < p.K ? p.g_ids[(uint64_t)node * p.K + pa] : p.rev_ids[r0 + (pa - p.K)]);
                 }
 #pragma unroll
                 for (uint32_t u = 0; u < 8; u++) lst[32 * u + lane] = ids[u];
@@ -398,6 +417,26 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
                 __syncwarp();
             }
             if (npool >= p.cap) break;
+        }
+        if (p.mode == kModeVamana) {
+            // append_aknn_edges (index.h:767-770): the row's g0 list, fresh distances
+            for (uint32_t c0 = 0; c0 < p.K; c0 += 32) {
+                const uint32_t t = c0 + lane;
+                const uint32_t j = t < p.K ? p.g_ids[i * p.K + t] : kEmpty;
+                const bool ok = j < p.n && j != (uint32_t)i;
+                const unsigned b = __ballot_sync(kAll, ok);
+                if (ok) ni[__popc(b & lane_lt_mask())] = j;
+                __syncwarp();
+                const uint32_t m = __popc(b);
+                if (m == 0) continue;
+                batch_d2<kIp>(p, i, ni, nd, m, gw, gt);
+                if (lane < m && npool + lane < p.pool_cap) {
+                    pd[npool + lane] = nd[lane];
+                    pi[npool + lane] = ni[lane];
+                }
+                npool += m;
+                __syncwarp();
+            }
         }
         if (lane == 0) atomicAdd(p.pool_total, (unsigned long long)npool);
 
@@ -432,6 +471,50 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
         vis_release(vis, vs, nlog, lane);
         for (uint32_t t = lane; t < p.hash_cap; t += 32) tab[t] = kEmpty;
         __syncwarp();
+    }
+}
+
+// ------------------------------------------------------- Vamana entries
+
+// The entry of each row for the Vamana refine (rptrees.h:108-123): the RP-tree
+// descent of the row's own vector, |margin| <= 1e-6 to the left (the
+// reference draws a random side there), and the first point of the leaf
+// reached, 0 for an empty leaf or a child outside the tree.  One 4-lane group
+// per row, the reference's lane order.
+__global__ void __launch_bounds__(128) tree_entry_kernel(const float* __restrict__ x, uint64_t n, uint32_t stride,
+                                                         uint32_t dim, const uint32_t* __restrict__ left,
+                                                         const uint32_t* __restrict__ right,
+                                                         const float* __restrict__ offset,
+                                                         const float* __restrict__ hyper,
+                                                         const uint32_t* __restrict__ leaf_first, uint32_t n_nodes,
+                                                         uint32_t* __restrict__ entry) {
+    const uint32_t lane = threadIdx.x & 31u, gt = lane & 3u, gw = lane >> 2;
+    const uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t r0 = w * 8; r0 < n; r0 += nw * 8) {
+        const uint64_t i = r0 + gw;
+        const bool ok = i < n;
+        uint32_t v = 0;
+        bool done = !ok, bad = false;
+        for (uint32_t depth = 0; depth < 4096; depth++) {
+            if (!done && left[v] == kEmpty) done = true;
+            if (__all_sync(kAll, done)) break;
+            const float ip = group_ip(hyper + (size_t)(done ? 0u : v) * stride, x + (ok ? i : 0) * stride, dim, gt,
+                                      kAll);
+            if (!done) {
+                const float m = __fsub_rn(ip, offset[v]);
+                const uint32_t nx = m > kSplitEps ? right[v] : left[v];
+                if (nx >= n_nodes) {
+                    bad = done = true;
+                } else {
+                    v = nx;
+                }
+            }
+        }
+        if (ok && gt == 0) {
+            const uint32_t ep = bad ? 0u : leaf_first[v];
+            entry[i] = ep < n ? ep : 0u;
+        }
     }
 }
 
@@ -998,6 +1081,7 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     const uint32_t words = (uint32_t)((p.n + 31) / 32);
     uint64_t need = (uint64_t)p.cap + p.K + max_rev + 64;
     if (p.mode == kModeCommit) need = p.M + max_rev + 64;
+    if (p.mode == kModeVamana) need = (uint64_t)p.ef * 128 + p.K + 64;  // every visit of an uncapped beam
     const uint32_t pool_cap = p.mode == kModeAknn ? 1u : (uint32_t)std::min<uint64_t>(1ull << 30, 1ull << (64 - __builtin_clzll(need)));
     // per-slot scratch, kept by the context between builds (the first build
     // maps it; later ones reuse it)
@@ -1142,6 +1226,10 @@ static int run_warm_start(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n
     return sync(c);
 }
 
+static int run_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
+                      DevBuf& O, DevBuf& Odeg, uint32_t M, float alpha, DevBuf& links_buf, DevBuf& deg_buf,
+                      const uint32_t* row_order, double* kernel_ms);
+
 static int run_select_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
                              const DevBuf& hid, const DevBuf& hval, uint32_t K, uint32_t M, uint32_t ef, uint32_t cap,
                              float alpha, DevBuf& O, DevBuf& Odeg, DevBuf* links, DevBuf* deg, uint64_t* pool_total,
@@ -1167,6 +1255,17 @@ static int run_select_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_
     p.row_order = row_order;
     if ((rc = run_gather(c, p, mr, pool_total, kernel_ms))) return rc;
     if (!links) return ANQI_OK;
+    return run_commit(c, dx, dn, n, stride, dim, O, Odeg, M, alpha, *links, *deg, row_order, kernel_ms);
+}
+
+// commit_edges (index.h:907-930): reverse lists of O, then per row O_i + R_i
+// pruned to the final adjacency.
+static int run_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
+                      DevBuf& O, DevBuf& Odeg, uint32_t M, float alpha, DevBuf& links_buf, DevBuf& deg_buf,
+                      const uint32_t* row_order, double* kernel_ms) {
+    int rc;
+    DevBuf* links = &links_buf;
+    DevBuf* deg = &deg_buf;
     TmpBuf roff2(c), rev2(c);
     if ((rc = build_reverse(c, O.as<uint32_t>(), n, M, roff2, rev2))) return rc;
     const uint64_t mr2 = max_reverse(c, roff2, n);
@@ -1185,6 +1284,55 @@ static int run_select_commit(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_
     q.deg = deg->as<uint32_t>();
     q.row_order = row_order;
     return run_gather(c, q, mr2, nullptr, kernel_ms);
+}
+
+// One pass of the global Vamana refine over the current graph (dl, dd: n x M,
+// degrees), rows' entries given: the Vamana-mode gather (beam of width Lb
+// over the graph + the row's g0 list, pruned) -> O, then commit_edges -> dl, dd.
+static int run_vamana_pass(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
+                           const DevBuf& hid, uint32_t K, const uint32_t* d_entry, uint32_t Lb, uint32_t M,
+                           float alpha, DevBuf& dl, DevBuf& dd, DevBuf& O, DevBuf& Odeg, const uint32_t* row_order,
+                           uint64_t* pool_total, double* kernel_ms, bool commit = true) {
+    int rc;
+    if ((rc = ensure(c, O, n * M * 4)) || (rc = ensure(c, Odeg, n * 4))) return rc;
+    GatherParams p = base_params(dx, dn, n, stride, dim);
+    p.g_ids = hid.as<uint32_t>();
+    p.K = K;
+    p.ef = Lb;
+    p.cap = 0xFFFFFFFFu;
+    p.mode = kModeVamana;
+    p.M = M;
+    p.alpha = alpha;
+    p.O = O.as<uint32_t>();
+    p.O_deg = Odeg.as<uint32_t>();
+    p.cur_links = dl.as<uint32_t>();
+    p.cur_deg = dd.as<uint32_t>();
+    p.cur_M = M;
+    p.entry = d_entry;
+    p.row_order = row_order;
+    if ((rc = run_gather(c, p, 0, pool_total, kernel_ms))) return rc;
+    if (!commit) return ANQI_OK;
+    return run_commit(c, dx, dn, n, stride, dim, O, Odeg, M, alpha, dl, dd, row_order, kernel_ms);
+}
+
+// Entries of every row from the context's entry tree (the last graph build's).
+static int vamana_entries(Ctx* c, const DevBuf& dx, uint64_t n, uint32_t stride, uint32_t dim, DevBuf& ent) {
+    const uint32_t nn = c->t_nodes;
+    if (nn == 0 || c->t_dim != dim) return fail(c, ANQI_ERR_ARGS, "no entry tree for the Vamana refine");
+    std::vector<uint32_t> lf(nn, kEmpty);
+    for (uint32_t v = 0; v < nn; v++)
+        if (c->t_left[v] == kEmpty && c->t_leaf_cnt[v] > 0) lf[v] = c->t_perm[c->t_leaf_off[v]];
+    TmpBuf tl(c), tr(c), to(c), th(c), tf(c);
+    int rc;
+    if ((rc = h2d(c, tl, c->t_left.data(), nn * 4)) || (rc = h2d(c, tr, c->t_right.data(), nn * 4)) ||
+        (rc = h2d(c, to, c->t_offset.data(), nn * 4)) || (rc = upload_padded(c, th, c->t_hyper.data(), nn, dim, stride)) ||
+        (rc = h2d(c, tf, lf.data(), nn * 4)) || (rc = ensure(c, ent, n * 4)))
+        return rc;
+    tree_entry_kernel<<<c->sm_count * 8, 128, 0, c->stream>>>(dx.as<float>(), n, stride, dim, tl.as<uint32_t>(),
+                                                              tr.as<uint32_t>(), to.as<float>(), th.as<float>(),
+                                                              tf.as<uint32_t>(), nn, ent.as<uint32_t>());
+    ANQI_CUDA(c, cudaGetLastError());
+    return sync(c);
 }
 
 // init_knn over leaves; lists kd/ki/ksz already initialised.
@@ -1322,6 +1470,33 @@ int anqi_graph_commit(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, con
     return sync(c);
 }
 
+int anqi_graph_vamana_select(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* links,
+                             const uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, const uint32_t* entry,
+                             uint32_t Lb, float alpha, uint32_t* O, uint32_t* O_deg) {
+    if (!h || !x || !links || !deg || !g0 || !entry || !O || !O_deg || n == 0 || dim == 0 || M == 0 || M > 64 ||
+        K == 0 || Lb == 0 || Lb > 1024)
+        return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    for (uint64_t i = 0; i < n; i++) {
+        if (deg[i] > M || entry[i] >= n) return fail(c, ANQI_ERR_FORMAT, "invalid graph row or entry %llu", (unsigned long long)i);
+        for (uint32_t j = 0; j < deg[i]; j++)
+            if (links[i * M + j] >= n) return fail(c, ANQI_ERR_FORMAT, "invalid neighbor id in graph row %llu", (unsigned long long)i);
+    }
+    const uint32_t xs = round_up(dim, 8);
+    TmpBuf dx(c), dn(c), dl(c), dd(c), dg(c), de(c), dO(c), dOd(c);
+    int rc;
+    if ((rc = upload_rows(c, dx, dn, x, n, dim, xs)) || (rc = h2d(c, dl, links, n * M * 4ull)) ||
+        (rc = h2d(c, dd, deg, n * 4)) || (rc = h2d(c, dg, g0, n * K * 4ull)) || (rc = h2d(c, de, entry, n * 4)))
+        return rc;
+    uint64_t pool_total = 0;
+    if ((rc = run_vamana_pass(c, dx, dn, n, xs, dim, dg, K, de.as<uint32_t>(), Lb, M, alpha, dl, dd, dO, dOd, nullptr,
+                              &pool_total, nullptr, false)))
+        return rc;
+    if ((rc = d2h(c, O, dO, n * M * 4ull)) || (rc = d2h(c, O_deg, dOd, n * 4))) return rc;
+    return sync(c);
+}
+
 static void graph_build_reset(Ctx* c) {
     GraphBuild& g = c->gb;
     for (DevBuf* b : {&g.dx, &g.dn, &g.hid, &g.hv, &g.order}) release(c, *b);
@@ -1443,6 +1618,17 @@ int anqi_graph_build_finish(anqi_ctx* h, uint32_t* deg, uint32_t* links, anqi_bu
         rc = run_select_commit(c, g.dx, g.dn, n, g.xs, g.dim, g.hid, g.hv, gp.nn_k, gp.degree, gp.explore, cap,
                                gp.alpha, dO, dOd, &dl, &dd, &pool_total,
                                ord_env && ord_env[0] == '0' ? nullptr : g.order.as<uint32_t>(), &gather_kernel_ms);
+    // optional global Vamana refine (index.h:1262-1285): every row's entry
+    // from the entry tree, then `vamana_passes` passes over the graph
+    if (!rc && gp.vamana_passes > 0) {
+        TmpBuf ent(c);
+        rc = vamana_entries(c, g.dx, n, g.xs, g.dim, ent);
+        for (uint32_t pass = 0; pass < gp.vamana_passes && !rc; pass++)
+            rc = run_vamana_pass(c, g.dx, g.dn, n, g.xs, g.dim, g.hid, gp.nn_k, ent.as<uint32_t>(),
+                                 gp.vamana_L ? gp.vamana_L : 128, gp.degree, gp.alpha, dl, dd, dO, dOd,
+                                 ord_env && ord_env[0] == '0' ? nullptr : g.order.as<uint32_t>(), &pool_total,
+                                 nullptr);
+    }
     const double gather_ms = ms_since(t);
     if (!rc && !(rc = d2h(c, links, dl, n * gp.degree * 4ull)) && !(rc = d2h(c, deg, dd, n * 4))) rc = sync(c);
     if (!rc && st) {

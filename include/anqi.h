@@ -216,6 +216,9 @@ typedef struct {
                               filter each round's pairs against the round-start heap tops and
                               only kept pairs are recomputed in FP32 (identical heaps; needs
                               join_sample <= 32 and dim <= 256, else FP32) */
+    uint32_t vamana_passes;  /* ANQI_VAMANA (ANQI_VAMANA_PASS, 2): global Vamana refine passes after
+                                the commit (include/index.h:1262-1285); 0 = none */
+    uint32_t vamana_L;       /* ANQI_VAMANA_L: the refine's beam width (128; 0 = 128) */
 } anqi_graph_params;
 
 int anqi_graph_build(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* warm_ids,
@@ -254,6 +257,16 @@ int anqi_graph_select(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, c
                       uint32_t* O, uint32_t* O_deg);
 int anqi_graph_commit(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* O,
                       const uint32_t* O_deg, uint32_t M, float alpha, uint32_t* links, uint32_t* deg);
+/* One pass of the global Vamana refine (include/index.h:856-875,
+ * 1262-1285), select half: for every row i, a beam of width Lb over the graph
+ * (links n x M, deg) from entry[i] collects every visited node, the row's g0
+ * list (n x K, ANQI_EMPTY skipped) joins with fresh distances, and the pool is
+ * pruned as anqi_graph_select does -> O, O_deg (then anqi_graph_commit).
+ * anqi_graph_params.vamana_passes runs whole passes inside anqi_graph_build,
+ * the entries from the build's entry tree (ties at the margin to the left). */
+int anqi_graph_vamana_select(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* links,
+                             const uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, const uint32_t* entry,
+                             uint32_t Lb, float alpha, uint32_t* O, uint32_t* O_deg);
 
 /* ------------------------------------------------------- query index
  * A device-resident copy of what rknn_query holds after index load

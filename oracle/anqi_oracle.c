@@ -646,6 +646,67 @@ void ao_graph_select(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t 
     free(pi);
 }
 
+/* One pass of the global Vamana refine (index.h:856-875 greedy_collect,
+ * 767-770 append_aknn_edges, 1262-1285): for every row i, a beam of width Lb
+ * over the current graph (links n x M, deg) from entry[i] collects every
+ * visited node but i with its distance, the row's g0 list (n x K, ANQI_EMPTY
+ * skipped) follows with fresh distances, and the pool is pruned as
+ * prune_pool_to_ids -> O (n x M, ANQI_EMPTY padded), O_deg. */
+void ao_vamana_select(const float* x, const float* norms, uint32_t dim, uint64_t n, const uint32_t* links,
+                      const uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, const uint32_t* entry,
+                      uint32_t Lb, float alpha, uint32_t* O, uint32_t* O_deg) {
+    uint8_t* vis = (uint8_t*)malloc(n);
+    uint64_t cap = 1024;
+    float* pd = (float*)malloc(sizeof(float) * cap);
+    uint32_t* pi = (uint32_t*)malloc(sizeof(uint32_t) * cap);
+    for (uint64_t i = 0; i < n; i++) {
+        memset(vis, 0, n);
+        uint64_t np = 0;
+#define AO_VPUSH(ID, D)                                              \
+    do {                                                             \
+        if (np == cap) {                                             \
+            cap *= 2;                                                \
+            pd = (float*)realloc(pd, sizeof(float) * cap);           \
+            pi = (uint32_t*)realloc(pi, sizeof(uint32_t) * cap);     \
+        }                                                            \
+        pd[np] = (D);                                                \
+        pi[np] = (ID);                                               \
+        np++;                                                        \
+    } while (0)
+        queue_t beam;
+        q_init(&beam, Lb);
+        uint32_t ep = entry[i] < n ? entry[i] : 0;
+        vis[ep] = 1;
+        float d0 = ao_d2(x + i * dim, x + (uint64_t)ep * dim, norms[i], norms[ep], dim);
+        q_insert(&beam, d0, ep);
+        if (ep != (uint32_t)i) AO_VPUSH(ep, d0);
+        while (beam.cur < beam.size) {
+            uint32_t cur = q_pop(&beam);
+            for (uint32_t j = 0; j < deg[cur]; j++) {
+                uint32_t nb = links[(uint64_t)cur * M + j];
+                if (nb >= n || vis[nb]) continue;
+                vis[nb] = 1;
+                float d = ao_d2(x + i * dim, x + (uint64_t)nb * dim, norms[i], norms[nb], dim);
+                q_insert(&beam, d, nb);
+                if (nb != (uint32_t)i) AO_VPUSH(nb, d);
+            }
+        }
+        for (uint32_t k = 0; k < K; k++) {
+            uint32_t j = g0[i * K + k];
+            if (j == AO_EMPTY || j >= n || j == (uint32_t)i) continue;
+            AO_VPUSH(j, ao_d2(x + i * dim, x + (uint64_t)j * dim, norms[i], norms[j], dim));
+        }
+#undef AO_VPUSH
+        free(beam.data);
+        uint32_t* row = O + i * M;
+        for (uint32_t j = 0; j < M; j++) row[j] = AO_EMPTY;
+        O_deg[i] = ao_prune(x, norms, dim, n, i, pd, pi, np, M, alpha, row);
+    }
+    free(vis);
+    free(pd);
+    free(pi);
+}
+
 /* commit_edges, index.h:907-930 */
 void ao_graph_commit(const float* x, const float* norms, uint32_t dim, uint64_t n,
                      const uint32_t* O, const uint32_t* O_deg, uint32_t M, float alpha,

@@ -119,6 +119,11 @@ uint32_t ao_prune(const float* x, const float* norms, uint32_t dim, uint64_t n, 
 /* gather + prune for all rows -> O (n x M, UINT32_MAX padded) */
 void ao_graph_select(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t M, float alpha,
                      uint32_t* O, uint32_t* O_deg);
+/* one pass of the global Vamana refine over the current graph (links, deg):
+ * greedy beam from entry[i] + the row's g0 list -> prune -> O, O_deg */
+void ao_vamana_select(const float* x, const float* norms, uint32_t dim, uint64_t n, const uint32_t* links,
+                      const uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, const uint32_t* entry,
+                      uint32_t Lb, float alpha, uint32_t* O, uint32_t* O_deg);
 /* commit_edges: final adjacency (n x M) from O */
 void ao_graph_commit(const float* x, const float* norms, uint32_t dim, uint64_t n,
                      const uint32_t* O, const uint32_t* O_deg, uint32_t M, float alpha,

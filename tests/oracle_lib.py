@@ -57,6 +57,8 @@ def _load() -> C.CDLL:
         "ao_reverse": (None, [u32p, C.c_uint64, C.c_uint32, u64p, u32p]),
         "ao_init_knn": (None, [f32p, f32p, C.c_uint32, C.c_uint64, C.c_uint32, u64p, u32p, C.c_uint64, u32p, f32p]),
         "ao_graph_commit": (None, [f32p, f32p, C.c_uint32, C.c_uint64, u32p, u32p, C.c_uint32, C.c_float, u32p, u32p]),
+        "ao_vamana_select": (None, [f32p, f32p, C.c_uint32, C.c_uint64, u32p, u32p, C.c_uint32, u32p, C.c_uint32,
+                                    u32p, C.c_uint32, C.c_float, u32p, u32p]),
         "ao_exact_topk": (None, [f32p, C.c_uint64, C.c_uint32, C.c_uint32, u32p, f32p]),
         "ao_rknn_gt": (C.c_int64, [f32p, C.c_uint64, f32p, C.c_uint64, C.c_uint32, f32p, u32p, u32p, f32p, C.c_uint64]),
         "ao_hash64": (C.c_uint64, [C.c_uint64]),
@@ -248,6 +250,17 @@ def graph_select(x, nrm, ids, vals, M=48, ef=100, cap=800, alpha=1.2):
     O = np.empty((n, M), np.uint32)
     Od = np.empty(n, np.uint32)
     LIB.ao_graph_select(C.byref(g), ef, cap, M, alpha, O, Od)
+    return O, Od
+
+
+def vamana_select(x, nrm, links, deg, g0, entry, Lb=128, alpha=1.2):
+    x = np.ascontiguousarray(x, np.float32)
+    n, M = links.shape
+    O = np.empty((n, M), np.uint32)
+    Od = np.empty(n, np.uint32)
+    LIB.ao_vamana_select(x, nrm, x.shape[1], n, np.ascontiguousarray(links, np.uint32),
+                         np.ascontiguousarray(deg, np.uint32), M, np.ascontiguousarray(g0, np.uint32), g0.shape[1],
+                         np.ascontiguousarray(entry, np.uint32), Lb, alpha, O, Od)
     return O, Od
 
 

@@ -172,13 +172,14 @@ def test_rknn_bad_inputs_exit_3(tmp_path):
     ("ANQI_GRAPH_GEOMETRY", "original"), ("ANQI_GRAPH_GEOMETRY", "bogus"), ("ANQI_RADIUS_MODE", "knots"),
     ("ANQI_RADIUS_MODE", "rankm_resid_u8_floor"), ("ANQI_RADIUS_MODE", "analytic_rankm"),
     ("ANQI_VERIFIER_PLACEMENT", "integrated"), ("ANQI_VERIFIER_PLACEMENT", "x"), ("ANQI_RECHECK", "1"),
-    ("ANQI_SPECIFIC", "1"), ("ANQI_VAMANA", "1"), ("ANQI_EDGE_POLICY", "lsg_rng"),
+    ("ANQI_SPECIFIC", "1"), ("ANQI_VAMANA_STYLE", "batch"), ("ANQI_EDGE_POLICY", "lsg_rng"),
     ("ANQI_RQ_OBJECTIVE", "predicate_boundary"), ("ANQI_CANDIDATE_ENVELOPE", "verifier"),
     ("ANQI_RANKM_SLACK", "-1"), ("ANQI_RADIUS_RELAX", "0.1"),
 ])
 def test_rknn_configurations_outside_the_path_exit_2(tmp_path, var, val):
     pfx, env, _ = sample_prefix(tmp_path)
-    rc, out, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10, env={**env, var: val})
+    extra = {"ANQI_VAMANA": "1"} if var == "ANQI_VAMANA_STYLE" else {}
+    rc, out, err = run("rknn_query", "16", pfx, 48, 500, 64, 600, 10, env={**env, **extra, var: val})
     assert rc == 2, (out, err)
 
 

@@ -237,6 +237,56 @@ def test_localjoin_and_select_random_vs_oracle(ctx):
         assert np.array_equal(L1[i, :D1[i]], L2[i, :D2[i]]), i
 
 
+def test_vamana_pass_vs_oracle(ctx):
+    """One global Vamana pass (index.h:856-875, 1262-1285): per row a beam of
+    width 64 over the current graph from a given entry, plus the row's g0
+    list, pruned -> O; then commit.  Bit-exact against the oracle."""
+    x = clustered(3000, 18, 41)
+    n = len(x)
+    nrm = ol.norms(x)
+    rng = np.random.default_rng(8)
+    cand = rng.integers(0, n, size=(n, 100)).astype(np.uint32)
+    gi, gv = ol.warm_start(x, nrm, cand, 100, 50)
+    gi, gv, _ = ol.localjoin(x, nrm, gi, gv)
+    O, Od = ol.graph_select(x, nrm, gi, gv, M=24)
+    links, deg = ol.graph_commit(x, nrm, O, Od)
+    entry = rng.integers(0, n, size=n).astype(np.uint32)
+    for Lb in (16, 64):
+        Og = np.empty((n, 24), np.uint32)
+        Odg = np.empty(n, np.uint32)
+        ctx._check(ctx.lib.anqi_graph_vamana_select(ctx.h, f32(x), n, x.shape[1], u32(links), u32(deg), 24, u32(gi),
+                                                    gi.shape[1], entry, Lb, 1.2, Og, Odg), "vamana_select")
+        Oo, Odo = ol.vamana_select(x, nrm, links, deg, gi, entry, Lb)
+        assert np.array_equal(Odg, Odo), Lb
+        for i in range(n):
+            assert np.array_equal(Og[i, :Odg[i]], Oo[i, :Odo[i]]), (Lb, i)
+    L1, D1 = commit(ctx, x, Og, Odg)
+    L2, D2 = ol.graph_commit(x, nrm, Oo, Odo)
+    assert np.array_equal(D1, D2)
+
+
+def test_graph_build_with_vamana_passes(ctx, sample):
+    """anqi_graph_build with two global Vamana passes on the reference sample:
+    a valid degree-capped graph (ids in range, no self edge, no duplicate),
+    changed by the passes."""
+    x = sample["lifted"]
+    n, dim = x.shape
+    out = {}
+    for passes in (0, 2):
+        gp = GraphParams(48, 50, 100, 8, 6, 20, 100, 100, 10, 1.2, 100, 0, passes, 64)
+        deg = np.empty(n, np.uint32)
+        links = np.empty((n, 48), np.uint32)
+        st = BuildStats()
+        ctx._check(ctx.lib.anqi_graph_build(ctx.h, f32(x), n, dim, u32(sample["rec_ids"]), 100, C.byref(gp), deg,
+                                            links, C.byref(st)), "graph_build")
+        assert (deg <= 48).all() and (deg > 0).all()
+        for i in range(n):
+            row = links[i, :deg[i]]
+            assert (row < n).all() and (row != i).all() and len(set(row.tolist())) == deg[i]
+        out[passes] = (links.copy(), deg.copy())
+    assert not np.array_equal(out[0][0], out[2][0])
+
+
 def test_aknn_gather_beam_path_vs_oracle(ctx):
     # ef >= K + 1 -> the beam holds the answer
     x = clustered(4000, 24, 41)

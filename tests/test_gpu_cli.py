@@ -375,3 +375,36 @@ def test_rknn_query_scale_profile_degree20_kpivot10(tmp_path):
     assert rc == 0, err
     assert "[rknn] loaded cached index" in ours
     assert lines(ours) == lines(ref.stdout)
+
+
+@pytest.mark.skipif(not tc.REF_BIN.exists(), reason="reference binaries not built")
+def test_rknn_query_vamana_global(tmp_path):
+    """ANQI_VAMANA=1 (global style, 2 passes of L = 128): the graph cache is
+    named as the reference names it, recall is within 0.05 of the reference's
+    own Vamana-refined build, and on the reference's refined graph the result
+    lines are the reference's."""
+    pfx, env, z = tc.sample_prefix(tmp_path, 32)
+    env = dict(env, ANQI_VAMANA="1")
+    ref_env = {k: v for k, v in os.environ.items() if not k.startswith("ANQI_")}
+    ref_env.update(env, OMP_NUM_THREADS="1", ANQI_GRAPH_CACHE_DIR=str(tmp_path / "ref" / "graph"),
+                   ANQI_VERIFIER_CACHE_DIR=str(tmp_path / "ref" / "verifier"))
+    for sub in ("graph", "verifier"):
+        (tmp_path / "ref" / sub).mkdir(parents=True)
+    ref = subprocess.run([str(tc.REF_BIN), "16,32,64", str(pfx), "48", "500", "64", "600", "10"], env=ref_env,
+                         capture_output=True, text=True, timeout=300)
+    assert ref.returncode == 0, ref.stderr
+    rc, ours, err = tc.run("rknn_query", "16,32,64", pfx, 48, 500, 64, 600, 10, env=env)
+    assert rc == 0, err
+    rl = lines(ref.stdout)
+    for L, v in lines(ours).items():
+        assert abs(v[0] - rl[L][0]) < 0.05, (L, v, rl[L])
+    gref = list((tmp_path / "ref" / "graph").glob("fd_metric_*"))
+    gours = list(Path(env["ANQI_GRAPH_CACHE_DIR"]).glob("fd_metric_*"))
+    assert len(gref) == 1 and len(gours) == 1 and gref[0].name == gours[0].name
+    gours[0].write_bytes(gref[0].read_bytes())
+    for suffix in ("_approxlift_graph_", "_anqi_meta_graph_"):
+        for p in (tmp_path / "ref" / "graph").glob(suffix + "*"):
+            (Path(env["ANQI_GRAPH_CACHE_DIR"]) / p.name).write_bytes(p.read_bytes())
+    rc, ours, err = tc.run("rknn_query", "16,32,64", pfx, 48, 500, 64, 600, 10, env=env)
+    assert rc == 0, err
+    assert lines(ours) == lines(ref.stdout)
