@@ -191,6 +191,9 @@ __device__ __forceinline__ bool visit_id(Visited& vis, uint32_t* win, uint32_t w
     if (w < kWinBits) {
         logged = false;
         const uint32_t bit = 1u << (w & 31u);
+        // most links are visited already: a plain read answers them, and only
+        // a first visit takes the atomic (which settles lanes racing on a word)
+        if (win[w >> 5] & bit) return false;
         return (atomicOr(win + (w >> 5), bit) & bit) == 0u;
     }
     logged = true;

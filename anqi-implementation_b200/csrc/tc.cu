@@ -712,7 +712,10 @@ int filter_to_csr(Ctx* c, FilterParams p, uint64_t nq, uint32_t cap, std::vector
     if (!over.empty()) {
         const uint64_t no = over.size();
         // rerun outputs are indexed by row id, so they take nq x cap2 entries
-        if (nq * (uint64_t)cap2 * 4 > (8ull << 30))
+        // (ids and keys: 8 bytes per entry) within most of the free device memory
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 8ull << 30;
+        if (nq * (uint64_t)cap2 * 8 > free_b / 10 * 7)
             return fail(c, ANQI_ERR_CAPACITY, "%zu rows need up to %u candidates each", over.size(), cap2);
         if ((rc = h2d(c, orow, over.data(), no * 4)) || (rc = ensure(c, ocnt, nq * 4)) ||
             (rc = ensure(c, oid2, nq * (uint64_t)cap2 * 4)) || (rc = ensure(c, okey2, nq * (uint64_t)cap2 * 4)))
