@@ -86,7 +86,8 @@ struct GatherParams {
     uint32_t hash_cap, hash_shift;  // shared-memory visited table per warp (power of two, 0 = none)
     uint32_t* gtab;                 // per-slot L2-resident visited tables (all kEmpty between rows)
     uint32_t gcap, gshift;          // entries per slot (power of two, 0 = none)
-    uint32_t ip;  // AKNN mode only: keys are the ip metric's 1 - <a, b>
+    uint32_t ip;    // AKNN mode only: keys are the ip metric's 1 - <a, b>
+    uint32_t cols;  // AKNN mode, d = 128: rows stored in chunk column order (group_ip_cols)
     // Vamana mode: the current graph (links n x cur_M, degrees) and each row's entry
     const uint32_t* cur_links;
     const uint32_t* cur_deg;
@@ -116,7 +117,8 @@ __device__ __forceinline__ void batch_d2(const GatherParams& p, uint64_t i, cons
         const uint32_t idx = r0 + gw;
         const bool ok = idx < m;
         const uint32_t j = ni[ok ? idx : r0];
-        const float ip = group_ip(xi, p.x + (uint64_t)j * p.stride, p.dim, gt, kAll);
+        const float ip = p.cols ? group_ip_cols<128>(xi, p.x + (uint64_t)j * p.stride, gt, kAll)
+                                : group_ip(xi, p.x + (uint64_t)j * p.stride, p.dim, gt, kAll);
         if (ok && gt == 0) nd[idx] = norm_d2(ni_norm, p.norms[j], ip);
     }
     __syncwarp();
@@ -1895,6 +1897,15 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
     t = Clock::now();
     if ((rc = ensure(c, oi, n * K * 4)) || (rc = ensure(c, od, n * K * 4))) return rc;
     GatherParams p = base_params(dx, dn, n, xs, d);
+    // d = 128: the gather reads its rows in chunk column order (two shuffles
+    // per distance instead of the lane tree's nine; the same bits)
+    TmpBuf dxc(c);
+    if (d == 128 && !ip) {
+        if ((rc = ensure(c, dxc, n * xs * 4ull))) return rc;
+        if ((rc = chunk_cols(c, dx.as<float>(), dxc.as<float>(), n, xs, 128))) return rc;
+        p.x = dxc.as<float>();
+        p.cols = 1;
+    }
     p.g_ids = gid.as<uint32_t>();
     p.g_vals = gval.as<float>();
     p.K = K;

@@ -232,6 +232,31 @@ __host__ __device__ __forceinline__ uint32_t chunk_col_pos(uint32_t j, uint32_t 
     return j < full ? (j & ~15u) | ((j & 3u) << 2) | ((j >> 2) & 3u) : j;
 }
 
+// Inner product (distance.h:89-116) of two rows in chunk column order,
+// dimension kDim (a multiple of 16) known at compile time: thread gt holds
+// AVX lanes gt, gt + 4, gt + 8, gt + 12 of every chunk, folds lane i + 8 onto
+// i and i + 4 onto i in registers and finishes the reference's tree with two
+// shuffles.  The accumulators and the tree are group_ip's, so the bits are
+// the same; the result is valid in all 4 threads.
+template <uint32_t kDim>
+__device__ __forceinline__ float group_ip_cols(const float* __restrict__ a, const float* __restrict__ b, uint32_t gt,
+                                               unsigned mask) {
+    static_assert(kDim % 16 == 0, "whole chunks only");
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;  // AVX lanes gt, gt + 4, gt + 8, gt + 12
+#pragma unroll
+    for (uint32_t c = 0; c < kDim / 16; c++) {
+        const float4 x = *reinterpret_cast<const float4*>(a + 16 * c + 4 * gt);
+        const float4 y = *reinterpret_cast<const float4*>(b + 16 * c + 4 * gt);
+        c0 = __fmaf_rn(x.x, y.x, c0);
+        c1 = __fmaf_rn(x.y, y.y, c1);
+        c2 = __fmaf_rn(x.z, y.z, c2);
+        c3 = __fmaf_rn(x.w, y.w, c3);
+    }
+    const float t6 = __fadd_rn(__fadd_rn(c3, c1), __fadd_rn(c2, c0));
+    const float t8 = __fadd_rn(__shfl_xor_sync(mask, t6, 2, 4), t6);
+    return __fadd_rn(__shfl_xor_sync(mask, t8, 1, 4), t8);
+}
+
 // Squared L2 (distance.h:58-86) of two rows in chunk column order, dimension
 // kDim known at compile time with a tail of at most 4 elements.  The lane
 // accumulators, the fold tree and the tail are those of group_l2sqr, so the

@@ -229,6 +229,12 @@ __global__ void chunk_cols_kernel(const float* __restrict__ src, float* __restri
     }
 }
 
+int chunk_cols(Ctx* c, const float* src, float* dst, uint64_t n, uint32_t stride, uint32_t full) {
+    chunk_cols_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(src, dst, n, stride, full);
+    ANQI_CUDA(c, cudaGetLastError());
+    return ANQI_OK;
+}
+
 // three-phase exclusive scan: block sums, one-block scan of the sums, apply
 constexpr uint32_t kScanBlock = 1024;
 

@@ -172,6 +172,9 @@ inline uint32_t round_up(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
 
 // Pad rows of a host matrix into a device buffer with stride (floats), zero fill.
 int upload_padded(Ctx* c, DevBuf& b, const float* src, uint64_t n, uint32_t d, uint32_t stride);
+// Device rows (n x stride) with each of the first `full` columns' 16-float
+// chunks stored in chunk column order (common.cuh chunk_col_pos), on the stream.
+int chunk_cols(Ctx* c, const float* src, float* dst, uint64_t n, uint32_t stride, uint32_t full);
 
 // A built random-projection forest (breadth-first node numbering per tree; tree
 // t's nodes at [t * cap_nodes, ...), its permutation at [t * n, ...)).

@@ -454,3 +454,29 @@ def test_localjoin_tensor_tiles_identical(ctx, kind):
     assert a[2] == b[2], (a[2], b[2])
     assert np.array_equal(a[0], b[0]) and np.array_equal(bits(a[1]), bits(b[1]))
     assert sum(a[2]) > 0
+
+
+def test_aknn_build_d128_vs_oracle_stages(ctx):
+    """A whole AKNN build at d = 128, where the gather reads its rows in chunk
+    column order (group_ip_cols), equals the oracle's forest -> init_knn ->
+    gather on the same seed, bit for bit (every row has K leaf-mates, so no
+    random fill)."""
+    from anqi import pipeline
+    x = clustered(3000, 128, 77)
+    n = len(x)
+    K, leaf, trees, ef = 20, 100, 4, 40
+    for precision in ("bf16", "fp32"):
+        ids, keys, _ = pipeline.aknn_build(ctx, x, k=K, leaf=leaf, trees=trees, ef=ef, precision=precision)
+        nrm = ol.norms(x)
+        leaf_off, leaves = [0], []
+        for t in range(trees):
+            o = ol.rp_tree(x, leaf, 100, 10, t)
+            for v in np.flatnonzero(o["left"] == EMPTY):
+                a, c = int(o["leaf_off"][v]), int(o["leaf_cnt"][v])
+                leaves.extend(o["perm"][a:a + c].tolist())
+                leaf_off.append(len(leaves))
+        ii, iv = ol.init_knn(x, nrm, np.array(leaf_off, np.uint64), np.array(leaves, np.uint32), K)
+        assert not np.any(ii == EMPTY)
+        ref_i, ref_d = ol.aknn_rows(x, nrm, ii, iv, K=K, ef=ef)
+        assert np.array_equal(ids, ref_i), precision
+        assert np.array_equal(bits(keys), bits(np.maximum(ref_d, np.float32(0.0)))), precision
