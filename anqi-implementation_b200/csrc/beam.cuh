@@ -191,9 +191,6 @@ __device__ __forceinline__ bool visit_id(Visited& vis, uint32_t* win, uint32_t w
     if (w < kWinBits) {
         logged = false;
         const uint32_t bit = 1u << (w & 31u);
-        // most links are visited already: a plain read answers them, and only
-        // a first visit takes the atomic (which settles lanes racing on a word)
-        if (win[w >> 5] & bit) return false;
         return (atomicOr(win + (w >> 5), bit) & bit) == 0u;
     }
     logged = true;
@@ -268,18 +265,6 @@ __device__ __forceinline__ uint32_t sort_fresh_kept(float* nd, uint32_t* ni, uin
 // it), beam entry j at j + (fresh entries before it); entries before cn, the
 // rank of the best kept fresh entry, do not move.  Returns cn (size when no
 // fresh entry enters).  Warp-collective; nd/ni are reordered.
-// The number of fresh entries that rank before old beam entry j, for mk <= 32
-// fresh entries whose ranks in the old beam are held one per lane (lane r <
-// mk: fresh entry r has `rank` beam entries before it): fresh r precedes beam
-// entry j exactly when its rank is <= j ((dist, id) is a total order and no id
-// is in both).  A count over shuffled ranks in registers; every lane takes
-// part, with its own j.
-__device__ __forceinline__ uint32_t fresh_before(uint32_t rank, uint32_t mk, uint32_t j) {
-    uint32_t s = 0;
-    for (uint32_t r = 0; r < mk; r++) s += __shfl_sync(kAll, rank, r) <= j ? 1u : 0u;
-    return s;
-}
-
 template <class Ord = IdOrder>
 __device__ __forceinline__ uint32_t beam_insert(float* bd, uint32_t* bi, uint32_t& size, uint32_t cap, float* nd,
                                                 uint32_t* ni, uint32_t m, uint32_t lane, Ord ord = Ord()) {
@@ -298,11 +283,10 @@ __device__ __forceinline__ uint32_t beam_insert(float* bd, uint32_t* bi, uint32_
         const bool mv = lane < hi - cn;
         float dv = 0.f;
         uint32_t iv = 0, pos = ns;
-        const uint32_t sh = mk <= 32 ? fresh_before(r0, mk, j) : 0u;
         if (mv) {
             dv = bd[j];
             iv = bi[j];
-            pos = j + (mk <= 32 ? sh : lower_rank(nd, ni, mk, dv, iv, ord));
+            pos = j + lower_rank(nd, ni, mk, dv, iv, ord);
         }
         __syncwarp();
         if (pos < ns) {

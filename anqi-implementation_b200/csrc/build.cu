@@ -229,9 +229,10 @@ __device__ __forceinline__ uint32_t gather_visit(const GatherParams& p, Visited&
     return m;
 }
 
-// kIp: the AKNN mode in the ip metric (a separate instance, so the L2 one is unchanged)
-template <bool kIp>
-__global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
+// kIp: the AKNN mode in the ip metric; kVam: the Vamana mode (separate
+// instances, so the L2 build modes keep their registers and occupancy)
+template <bool kIp, bool kVam = false>
+__global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
     const uint32_t topk_cap = (p.mode == kModeAknn && p.ef < p.out_k + 1) ? p.out_k + 1 : 0;
@@ -314,7 +315,7 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
         uint64_t npool = 0;
         // one visited batch: pool (select mode), beam and top-K list
         auto take = [&](uint32_t m) {
-            if (p.mode == kModeSelect || p.mode == kModeVamana) {
+            if (p.mode == kModeSelect || kVam) {
                 for (uint32_t t = lane; t < m; t += 32)
                     if (npool + t < p.pool_cap) {
                         pd[npool + t] = nd[t];
@@ -333,7 +334,7 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
             lo = min(lo, beam_insert(bd, bi, size, p.ef, nd, ni, m, lane));
         };
         // seeds: the row's entry (Vamana), or the row's own list with its stored distances
-        if (p.mode == kModeVamana) {
+        if constexpr (kVam) {
             const uint32_t ep = p.entry[i] < p.n ? p.entry[i] : 0u;
             const uint32_t m = gather_visit(p, vis, nlog, lane == 0 ? ep : kEmpty, kEmpty, 0.f, 0.f, false, ni, nd, lane);
             if (m) {
@@ -341,7 +342,7 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
                 take(m);
             }
         }
-        for (uint32_t c0 = 0; p.mode != kModeVamana && c0 < p.K; c0 += 64) {
+        for (uint32_t c0 = 0; !kVam && c0 < p.K; c0 += 64) {
             const uint32_t m0 = min(64u, p.K - c0);
             uint32_t id0 = kEmpty, id1 = kEmpty;
             float v0 = 0.f, v1 = 0.f;
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
             if (lane == 0) bi[cur] = node | kExpanded;
             __syncwarp();
             lo = cur + 1;
-            const bool vam = p.mode == kModeVamana;
+            constexpr bool vam = kVam;
             const uint64_t r0 = vam ? 0 : p.rev_off[node], r1 = vam ? 0 : p.rev_off[node + 1];
             const uint32_t tot = vam ? min(p.cur_deg[node], p.cur_M) : p.K + (uint32_t)(r1 - r0);
             // list slots in chunks of 64 (slot c0 + lane, c0 + lane + 32); the
@@ -420,7 +421,7 @@ __global__ void __launch_bounds__(128) gather_kernel(GatherParams p) {
             }
             if (npool >= p.cap) break;
         }
-        if (p.mode == kModeVamana) {
+        if constexpr (kVam) {
             // append_aknn_edges (index.h:767-770): the row's g0 list, fresh distances
             for (uint32_t c0 = 0; c0 < p.K; c0 += 32) {
                 const uint32_t t = c0 + lane;
@@ -1073,7 +1074,9 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     const size_t per_warp = gather_smem_words(p.ef, topk_cap, p.sort_words, hash_cap) * 4;
     const size_t smem = per_warp * warps_per_block;
     if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "explore range %u too large", p.ef);
-    auto* kern = p.ip ? gather_kernel<true> : gather_kernel<false>;
+    auto* kern = p.mode == kModeVamana ? gather_kernel<false, true>
+                 : p.ip                  ? gather_kernel<true>
+                                         : gather_kernel<false>;
     ANQI_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps_per_block, smem));

@@ -14,18 +14,18 @@
 namespace anqi {
 
 constexpr uint32_t kGtQ = 16;     // queries per CTA
-constexpr uint32_t kGtTile = 64;  // base rows per tile
+constexpr uint32_t kGtTile = 64;  // base rows per tile (fewer for long rows, to fit shared memory)
 
 __global__ void __launch_bounds__(256) rknn_gt_kernel(const float* __restrict__ base, const float* __restrict__ bn,
                                                       uint64_t n, const float* __restrict__ q, uint64_t nq,
                                                       uint32_t stride, uint32_t d, const float* __restrict__ rk2,
                                                       uint32_t* __restrict__ cnt, const uint64_t* __restrict__ off,
                                                       uint32_t* __restrict__ fill, uint32_t* __restrict__ out_id,
-                                                      float* __restrict__ out_key, uint32_t is_ip) {
+                                                      float* __restrict__ out_key, uint32_t is_ip, uint32_t tile) {
     extern __shared__ __align__(16) unsigned char sm[];
     float* qv = reinterpret_cast<float*>(sm);            // kGtQ x stride
-    float* tv = qv + (size_t)kGtQ * stride;              // kGtTile x stride
-    float* qn = tv + (size_t)kGtTile * stride;           // kGtQ
+    float* tv = qv + (size_t)kGtQ * stride;              // tile x stride
+    float* qn = tv + (size_t)tile * stride;              // kGtQ
     const uint64_t q0 = (uint64_t)blockIdx.x * kGtQ;
     const uint32_t nqb = (uint32_t)min_u64(kGtQ, nq - q0);
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
@@ -37,8 +37,8 @@ __global__ void __launch_bounds__(256) rknn_gt_kernel(const float* __restrict__ 
         if (lane == 0) qn[r] = v;
     }
     __syncthreads();
-    for (uint64_t c0 = 0; c0 < n; c0 += kGtTile) {
-        const uint32_t tr = (uint32_t)min_u64(kGtTile, n - c0);
+    for (uint64_t c0 = 0; c0 < n; c0 += tile) {
+        const uint32_t tr = (uint32_t)min_u64(tile, n - c0);
         for (uint32_t t = threadIdx.x; t < tr * (stride / 4); t += blockDim.x)
             reinterpret_cast<float4*>(tv)[t] = reinterpret_cast<const float4*>(base + c0 * stride)[t];
         __syncthreads();
@@ -147,13 +147,16 @@ extern "C" int anqi_rknn_ground_truth_metric(anqi_ctx* h, const float* base, uin
     if ((rc = compute_norms_device(c, db.as<float>(), n, d, xs, dbn.as<float>()))) return rc;
     ANQI_CUDA(c, cudaMemsetAsync(dcnt.p, 0, nq * 4, c->stream));
     ANQI_CUDA(c, cudaMemsetAsync(dfill.p, 0, nq * 4, c->stream));
-    const size_t smem = ((size_t)(kGtQ + kGtTile) * xs + kGtQ) * 4;
+    // base rows per tile: 64, or fewer (a multiple of 8) when rows are long
+    uint32_t tile = kGtTile;
+    while (tile > 8 && ((size_t)(kGtQ + tile) * xs + kGtQ) * 4 > 227 * 1024) tile -= 8;
+    const size_t smem = ((size_t)(kGtQ + tile) * xs + kGtQ) * 4;
     if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "dimension %u too large for the ground-truth kernel", d);
     ANQI_CUDA(c, cudaFuncSetAttribute(rknn_gt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const unsigned blocks = (unsigned)((nq + kGtQ - 1) / kGtQ);
     rknn_gt_kernel<<<blocks, 256, smem, c->stream>>>(db.as<float>(), dbn.as<float>(), n, dq.as<float>(), nq, xs, d,
                                                      dr.as<float>(), dcnt.as<uint32_t>(), nullptr, nullptr, nullptr,
-                                                     nullptr, is_ip);
+                                                     nullptr, is_ip, tile);
     ANQI_CUDA(c, cudaGetLastError());
     if ((rc = device_scan(c, dcnt.as<uint32_t>(), doff.as<uint64_t>(), nq))) return rc;
     std::vector<uint64_t> hoff(nq + 1);
@@ -165,7 +168,7 @@ extern "C" int anqi_rknn_ground_truth_metric(anqi_ctx* h, const float* base, uin
     if ((rc = ensure(c, did, tot * 4 + 4)) || (rc = ensure(c, dkey, tot * 4 + 4))) return rc;
     rknn_gt_kernel<<<blocks, 256, smem, c->stream>>>(db.as<float>(), dbn.as<float>(), n, dq.as<float>(), nq, xs, d,
                                                      dr.as<float>(), nullptr, doff.as<uint64_t>(), dfill.as<uint32_t>(),
-                                                     did.as<uint32_t>(), dkey.as<float>(), is_ip);
+                                                     did.as<uint32_t>(), dkey.as<float>(), is_ip, tile);
     ANQI_CUDA(c, cudaGetLastError());
     uint64_t maxm = 0;
     for (uint64_t i = 0; i < nq; i++) maxm = std::max(maxm, hoff[i + 1] - hoff[i]);

@@ -472,13 +472,10 @@ __global__ void __launch_bounds__(32 * kWpb, 32 / kWpb) rknn_search_kernel(Searc
                 const bool mv = lane < hi - cn;
                 float dv = 0.f;
                 uint32_t iv = 0, pos = ns;
-                // fresh entries before beam entry j: a count over the ranks in
-                // registers (few fresh entries), else a search of the batch
-                const uint32_t sh = mk <= 32 ? fresh_before(r0, mk, j) : 0u;
                 if (mv) {
                     dv = bd[j];
                     iv = bi[j];
-                    pos = j + (mk <= 32 ? sh : lower_rank(nd, ni, mk, dv, iv, ord));
+                    pos = j + lower_rank(nd, ni, mk, dv, iv, ord);
                 }
                 __syncwarp();
                 if (pos < ns) {

@@ -191,6 +191,10 @@ struct FilterParams {
     float bx_norm, bx_err, bx_n;
     int all_exact;
     uint64_t pos_base;  // leaf mode: candidate slot = member position - pos_base (the batch's first)
+    // top-K mode: pairs that need the FP32 recheck are written with their
+    // approximate key and kRecheck in the id, for recheck_rows_kernel (a
+    // 4-thread group per pair instead of one thread here)
+    int defer_recheck;
 };
 
 constexpr uint32_t kStages = 2;  // base-tile ring; two CTAs fit an SM (shared memory, TMEM)
@@ -395,11 +399,12 @@ __global__ void __launch_bounds__(kFilterThreads, kWide ? 1 : 2) tc_filter_kerne
                     }
                     continue;
                 }
-                const float key = exact ? approx : ref_key(qrow, p.x32 + j * p.xs, p.d, qn, xn);
-                if (!(key <= thr)) continue;
+                const bool later = p.defer_recheck && !exact;
+                const float key = (exact || later) ? approx : ref_key(qrow, p.x32 + j * p.xs, p.d, qn, xn);
+                if (!later && !(key <= thr)) continue;
                 const uint32_t pos = atomicAdd(p.cnt + my_row, 1u);
                 if (pos < p.cap) {
-                    p.out_id[my_row * p.cap + pos] = (uint32_t)j;
+                    p.out_id[my_row * p.cap + pos] = (uint32_t)j | (later ? kRecheck : 0u);
                     p.out_key[my_row * p.cap + pos] = key;
                 }
             }
@@ -618,6 +623,37 @@ __global__ void compact_rows_kernel(const uint32_t* __restrict__ cnt, uint32_t c
         for (uint32_t k = lane; k < m; k += 32) {
             out_id[off[i] + k] = in_id[i * cap + k];
             out_key[off[i] + k] = in_key[i * cap + k];
+        }
+    }
+}
+
+// The deferred FP32 recheck of a CSR of (id, key) rows: every entry flagged
+// kRecheck gets the reference's FP32 key (ref_key's arithmetic, by a 4-thread
+// group in the lane order), the flag cleared.  One warp per row, 8 entries at
+// a time.  Keys above the row's bound stay: they sort after the K it keeps.
+__global__ void __launch_bounds__(256) recheck_rows_kernel(const uint64_t* __restrict__ off, uint64_t nrows,
+                                                           const uint32_t* __restrict__ rows, uint32_t* __restrict__ ids,
+                                                           float* __restrict__ keys, const float* __restrict__ x32,
+                                                           const float* __restrict__ xn, uint32_t xs, uint32_t d) {
+    const uint32_t lane = threadIdx.x & 31u, gt = lane & 3u, gw = lane >> 2;
+    const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = w0; i < nrows; i += nw) {
+        const uint64_t q = rows ? rows[i] : i;
+        const uint64_t o0 = off[i], o1 = off[i + 1];
+        for (uint64_t e0 = o0; e0 < o1; e0 += 8) {
+            const uint64_t e = e0 + gw;
+            const bool ok = e < o1;
+            const uint32_t raw = ok ? ids[e] : 0u;
+            const bool flagged = ok && (raw & kRecheck);
+            if (!__any_sync(0xFFFFFFFFu, flagged)) continue;
+            const uint32_t j = raw & ~kRecheck;
+            const float ip = group_ip(x32 + q * xs, x32 + (uint64_t)(flagged ? j : (uint32_t)q) * xs, d, gt,
+                                      0xFFFFFFFFu);
+            if (flagged && gt == 0) {
+                keys[e] = __fsub_rn(__fadd_rn(xn[q], xn[j]), __fmul_rn(2.0f, ip));
+                ids[e] = j;
+            }
         }
     }
 }
@@ -1091,8 +1127,19 @@ int anqi_exact_topk_tc(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, u
         return rc;
     p.thr_row = tau.as<float>();
     p.exclude_self = 1;
+    p.defer_recheck = 1;
     std::vector<uint64_t> hoff;
     if ((rc = filter_to_csr(c, p, n, K + 156, hoff, doff, did, dkey))) return rc;
+    // the deferred FP32 rechecks, then each row again in (key, id) order
+    recheck_rows_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(doff.as<uint64_t>(), n, nullptr, did.as<uint32_t>(),
+                                                                dkey.as<float>(), X.f32.as<float>(), X.rn.as<float>(),
+                                                                xs, d);
+    ANQI_CUDA(c, cudaGetLastError());
+    {
+        uint64_t maxm = 0;
+        for (uint64_t i = 0; i < n; i++) maxm = std::max<uint64_t>(maxm, hoff[i + 1] - hoff[i]);
+        if ((rc = sort_csr_segments(c, doff.as<uint64_t>(), n, did.as<uint32_t>(), dkey.as<float>(), maxm))) return rc;
+    }
     if ((rc = ensure(c, ko, n * K * 4)) || (rc = ensure(c, kk, n * K * 4))) return rc;
     ANQI_CUDA(c, cudaMemsetAsync(c->err.p, 0, 4, c->stream));
     const uint64_t tk = n * K;

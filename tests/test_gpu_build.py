@@ -265,21 +265,22 @@ def test_vamana_pass_vs_oracle(ctx):
     assert np.array_equal(D1, D2)
 
 
-def test_graph_build_with_vamana_passes(ctx, sample):
-    """anqi_graph_build with two global Vamana passes on the reference sample:
+def test_graph_build_with_vamana_passes(ctx):
+    """anqi_graph_build with two global Vamana passes (beam 64) on 4,000 rows:
     a valid degree-capped graph (ids in range, no self edge, no duplicate),
     changed by the passes."""
-    x = sample["lifted"]
+    x = clustered(4000, 24, 12)
     n, dim = x.shape
+    warm = np.random.default_rng(3).integers(0, n, size=(n, 100)).astype(np.uint32)
     out = {}
     for passes in (0, 2):
-        gp = GraphParams(48, 50, 100, 8, 6, 20, 100, 100, 10, 1.2, 100, 0, passes, 64)
+        gp = GraphParams(24, 50, 100, 8, 6, 20, 100, 100, 10, 1.2, 100, 0, passes, 64)
         deg = np.empty(n, np.uint32)
-        links = np.empty((n, 48), np.uint32)
+        links = np.empty((n, 24), np.uint32)
         st = BuildStats()
-        ctx._check(ctx.lib.anqi_graph_build(ctx.h, f32(x), n, dim, u32(sample["rec_ids"]), 100, C.byref(gp), deg,
-                                            links, C.byref(st)), "graph_build")
-        assert (deg <= 48).all() and (deg > 0).all()
+        ctx._check(ctx.lib.anqi_graph_build(ctx.h, f32(x), n, dim, warm, 100, C.byref(gp), deg, links, C.byref(st)),
+                   "graph_build")
+        assert (deg <= 24).all() and (deg > 0).all()
         for i in range(n):
             row = links[i, :deg[i]]
             assert (row < n).all() and (row != i).all() and len(set(row.tolist())) == deg[i]

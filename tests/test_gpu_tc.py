@@ -111,9 +111,9 @@ def test_wide_tensor_path_equals_fp32(ctx, d):
     path bit for bit (L2-normalised N(0,1) rows, the batching form's second
     shape, and an integer mixture)."""
     from anqi import pipeline
-    base = unit_gaussian(3000, d, d) if d == 960 else mixture(3000, d, 7, True)
+    both = unit_gaussian(3300, d, d) if d == 960 else mixture(3300, d, 7, True)  # queries from the same law
+    base, query = both[:3000].copy(), both[3000:]
     base[11] = base[3]
-    query = unit_gaussian(300, d, d + 1) if d == 960 else mixture(300, d, 8, True)
     ids32, keys32 = pipeline.exact_thresholds(ctx, base, 100)
     ids, keys = ctx.exact_topk_tc(base, 100, hints=ids32)
     assert np.array_equal(ids, ids32) and np.array_equal(bits(keys), bits(keys32))
