@@ -10,9 +10,11 @@
 // verifier (compact LRQ forms, rank-M only, float32 residuals, exact_f32,
 // analytic rank-M): the same argv, environment, prefix files, caches (file
 // names and identity keys, so a cache written by either program is found by
-// the other), stdout result lines and exit codes.  Configurations outside that
-// path (rank-M or original geometry, integrated verifier, Vamana, edge
-// policies, fixed-k lift, recheck) exit 2 with a message naming the setting.
+// the other), stdout result lines and exit codes.  The global Vamana refine
+// (ANQI_VAMANA, styles global and old) runs on the device too.  Configurations
+// outside that path (rank-M or original geometry, integrated verifier, the
+// batched Vamana style, edge policies, fixed-k lift, recheck) exit 2 with a
+// message naming the setting.
 //
 // Differences of mechanism, not of result: the graph build, lift, LRQ
 // encode/materialize, search, postfilter and evaluation run on the device;
