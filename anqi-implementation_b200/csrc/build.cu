@@ -95,6 +95,10 @@ struct GatherParams {
     const uint32_t* entry;
     uint32_t* next_row;
     const uint32_t* row_order;  // work item -> row (rows of one RP-tree leaf together), or null for identity
+    // AKNN mode with rows renumbered for locality (gather_kernel<.., .., true>):
+    // row number -> original id.  Lists, rows and norms are given in the new
+    // numbering; (dist, id) ties and the output use the original ids.
+    const uint32_t* perm;
     unsigned long long* pool_total;
     uint32_t* err;
 };
@@ -195,48 +199,60 @@ __host__ __device__ __forceinline__ size_t gather_smem_pre(uint32_t ef, uint32_t
 }
 
 __host__ __device__ __forceinline__ size_t gather_smem_words(uint32_t ef, uint32_t topk_cap, uint32_t sort_words,
-                                                             uint32_t hash_cap) {
-    return gather_smem_pre(ef, topk_cap, sort_words) + hash_cap + 256;
+                                                             uint32_t hash_cap, uint32_t win_words = 0) {
+    return gather_smem_pre(ef, topk_cap, sort_words) + hash_cap + 256 + win_words;
 }
 
 // Visits one chunk of up to 64 list ids (slots lane and lane + 32): ids seen
 // for the first time go to ni (with their seed distances v0/v1 in nd when
-// `vals`) in slot order and are logged.  Returns their count.
+// `vals`) in slot order, and the visits that went to the visited tables are
+// logged.  kWin: ids in [wbase, wbase + kWinBits) are visited in the warp's
+// window bitmap `win` instead (not logged).  Returns the count of first visits.
+template <bool kWin = false>
 __device__ __forceinline__ uint32_t gather_visit(const GatherParams& p, Visited& vis, uint32_t& nlog, uint32_t id0,
                                                  uint32_t id1, float v0, float v1, bool vals, uint32_t* ni, float* nd,
-                                                 uint32_t lane) {
+                                                 uint32_t lane, uint32_t* win = nullptr, uint32_t wbase = 0) {
     vis_room(vis, nlog, 64, lane, p.err);
     uint32_t r0 = 0, r1 = 0;
-    const bool f0 = id0 < p.n && vis_first(vis, id0, r0, p.err);
-    const bool f1 = id1 < p.n && vis_first(vis, id1, r1, p.err);
+    bool f0 = false, f1 = false, g0 = true, g1 = true;  // g: a table visit (logged)
+    if constexpr (kWin) {
+        if (id0 < p.n) f0 = visit_id(vis, win, wbase, id0, r0, g0, p.err);
+        if (id1 < p.n) f1 = visit_id(vis, win, wbase, id1, r1, g1, p.err);
+    } else {
+        f0 = id0 < p.n && vis_first(vis, id0, r0, p.err);
+        f1 = id1 < p.n && vis_first(vis, id1, r1, p.err);
+    }
     const unsigned b0 = __ballot_sync(kAll, f0), b1 = __ballot_sync(kAll, f1);
     const uint32_t cnt0 = __popc(b0), lt = lane_lt_mask();
     const uint32_t q0 = __popc(b0 & lt), q1 = cnt0 + __popc(b1 & lt);
+    const unsigned h0 = kWin ? __ballot_sync(kAll, f0 && g0) : b0, h1 = kWin ? __ballot_sync(kAll, f1 && g1) : b1;
+    const uint32_t l0 = __popc(h0 & lt), l1 = __popc(h0) + __popc(h1 & lt);
     const bool logs = vis.level != 0;
     if (f0) {
         ni[q0] = id0;
         if (vals) nd[q0] = v0;
-        if (logs && nlog + q0 < p.log_cap) vis.vlog[nlog + q0] = r0;
+        if (logs && g0 && nlog + l0 < p.log_cap) vis.vlog[nlog + l0] = r0;
     }
     if (f1) {
         ni[q1] = id1;
         if (vals) nd[q1] = v1;
-        if (logs && nlog + q1 < p.log_cap) vis.vlog[nlog + q1] = r1;
+        if (logs && g1 && nlog + l1 < p.log_cap) vis.vlog[nlog + l1] = r1;
     }
-    const uint32_t m = cnt0 + __popc(b1);
-    nlog += m;
+    nlog += __popc(h0) + __popc(h1);
     __syncwarp();
-    return m;
+    return cnt0 + __popc(b1);
 }
 
-// kIp: the AKNN mode in the ip metric; kVam: the Vamana mode (separate
-// instances, so the L2 build modes keep their registers and occupancy)
-template <bool kIp, bool kVam = false>
+// kIp: the AKNN mode in the ip metric; kVam: the Vamana mode; kRen: the AKNN
+// mode over rows renumbered for locality (p.perm), whose visits near the row
+// go to a per-warp window bitmap (separate instances, so each mode keeps its
+// registers and occupancy)
+template <bool kIp, bool kVam = false, bool kRen = false>
 __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
     const uint32_t topk_cap = (p.mode == kModeAknn && p.ef < p.out_k + 1) ? p.out_k + 1 : 0;
-    const size_t per_warp = gather_smem_words(p.ef, topk_cap, p.sort_words, p.hash_cap) * 4;
+    const size_t per_warp = gather_smem_words(p.ef, topk_cap, p.sort_words, p.hash_cap, kRen ? kWinWords : 0) * 4;
     unsigned char* my = g_build_smem + wib * per_warp;
     float* bd = reinterpret_cast<float*>(my);  // the beam (queue cap ef), sorted, expanded flag in the id's top bit
     uint32_t* bi = reinterpret_cast<uint32_t*>(bd + p.ef);
@@ -251,6 +267,12 @@ __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams 
     uint32_t* sm_i = reinterpret_cast<uint32_t*>(sm_d + p.sort_words / 2);
     uint32_t* tab = reinterpret_cast<uint32_t*>(my) + gather_smem_pre(p.ef, topk_cap, p.sort_words);
     uint32_t* lst = tab + p.hash_cap;  // 256 list ids of the expansion being visited
+    uint32_t* win = lst + 256;         // kRen: the window bitmap (kWinWords)
+    // (dist, id) order of the beam and the top-K list: through the original ids when renumbered
+    const auto ord = [&]() {
+        if constexpr (kRen) return PermOrder{p.perm};
+        else return IdOrder{};
+    }();
     uint32_t* bits = p.vis_bits + (size_t)slot * p.vis_words;
     uint32_t* vlog = p.vis_log + (size_t)slot * p.log_cap;
     float* pd = p.pool_d + (size_t)slot * p.pool_cap;
@@ -313,6 +335,15 @@ __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams 
         uint32_t size = 0, tsize = 0, nlog = 0;
         uint32_t lo = 0;  // beam entries before lo are expanded
         uint64_t npool = 0;
+        // kRen: the window of row numbers around the row
+        uint32_t wbase = 0;
+        if constexpr (kRen) {
+            wbase = i > kWinBits / 2 ? (uint32_t)i - kWinBits / 2 : 0u;
+            if (p.n <= kWinBits) wbase = 0;
+            else if ((uint64_t)wbase > p.n - kWinBits) wbase = (uint32_t)(p.n - kWinBits);
+            for (uint32_t t = lane; t < kWinWords; t += 32) win[t] = 0u;
+            __syncwarp();
+        }
         // one visited batch: pool (select mode), beam and top-K list
         auto take = [&](uint32_t m) {
             if (p.mode == kModeSelect || kVam) {
@@ -329,9 +360,9 @@ __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams 
                     ni2[t] = ni[t];
                 }
                 __syncwarp();
-                beam_insert(td, ti, tsize, topk_cap, nd2, ni2, m, lane);
+                beam_insert(td, ti, tsize, topk_cap, nd2, ni2, m, lane, ord);
             }
-            lo = min(lo, beam_insert(bd, bi, size, p.ef, nd, ni, m, lane));
+            lo = min(lo, beam_insert(bd, bi, size, p.ef, nd, ni, m, lane, ord));
         };
         // seeds: the row's entry (Vamana), or the row's own list with its stored distances
         if constexpr (kVam) {
@@ -354,7 +385,7 @@ __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams 
                 id1 = p.g_ids[i * p.K + c0 + lane + 32];
                 v1 = p.g_vals[i * p.K + c0 + lane + 32];
             }
-            const uint32_t m = gather_visit(p, vis, nlog, id0, id1, v0, v1, true, ni, nd, lane);
+            const uint32_t m = gather_visit<kRen>(p, vis, nlog, id0, id1, v0, v1, true, ni, nd, lane, win, wbase);
             if (m) take(m);
         }
         // expansions: the closest unexpanded entry, its forward then reverse list
@@ -401,18 +432,26 @@ __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams 
                 for (uint32_t h = 0; h < 8; h += 4) {
                     uint4 q[4];
 #pragma unroll
-                    for (uint32_t k = 0; k < 4; k++)
-                        q[k] = ids[h + k] < p.n ? probe_visited(vis, ids[h + k]) : make_uint4(0, 0, 0, 0);
+                    for (uint32_t k = 0; k < 4; k++) {
+                        const uint32_t id = ids[h + k], w = id - wbase;
+                        if (kRen && w < kWinBits) q[k] = make_uint4(win[w >> 5], 0, 0, 0);
+                        else q[k] = id < p.n ? probe_visited(vis, id) : make_uint4(0, 0, 0, 0);
+                    }
 #pragma unroll
-                    for (uint32_t k = 0; k < 4; k++)
-                        if (ids[h + k] < p.n && !probe_found(vis, q[k], ids[h + k])) maybe |= 1u << (h + k);
+                    for (uint32_t k = 0; k < 4; k++) {
+                        const uint32_t id = ids[h + k], w = id - wbase;
+                        const bool found = (kRen && w < kWinBits) ? ((q[k].x >> (w & 31u)) & 1u) != 0u
+                                                                 : probe_found(vis, q[k], id);
+                        if (id < p.n && !found) maybe |= 1u << (h + k);
+                    }
                 }
                 __syncwarp();
                 for (uint32_t u = 0; u < 8 && c0 + 32 * u < tot; u += 2) {
                     const bool a0 = (maybe >> u) & 1u, a1 = (maybe >> (u + 1)) & 1u;
                     if (!__any_sync(kAll, a0 || a1)) continue;
-                    const uint32_t m = gather_visit(p, vis, nlog, a0 ? lst[32 * u + lane] : kEmpty,
-                                                    a1 ? lst[32 * u + 32 + lane] : kEmpty, 0.f, 0.f, false, ni, nd, lane);
+                    const uint32_t m = gather_visit<kRen>(p, vis, nlog, a0 ? lst[32 * u + lane] : kEmpty,
+                                                          a1 ? lst[32 * u + 32 + lane] : kEmpty, 0.f, 0.f, false, ni,
+                                                          nd, lane, win, wbase);
                     if (m == 0) continue;
                     batch_d2<kIp>(p, i, ni, nd, m, gw, gt);
                     take(m);
@@ -453,11 +492,14 @@ __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams 
             for (uint32_t t = lane; t < min(ls, p.out_k + 1); t += 32)
                 if ((li[t] & kIdMask) == (uint32_t)i) self_pos = t;
             for (int o = 16; o > 0; o >>= 1) self_pos = min(self_pos, __shfl_xor_sync(kAll, self_pos, o));
+            // kRen: the row's original id and its neighbours' original ids
+            const uint64_t orow = kRen ? (uint64_t)p.perm[i] : i;
             for (uint32_t t = lane; t < p.out_k; t += 32) {
                 const uint32_t src = (self_pos != kEmpty && t >= self_pos) ? t + 1 : t;
                 const bool ok = src < ls;
-                p.out_ids[i * p.out_k + t] = ok ? (li[src] & kIdMask) : kEmpty;
-                p.out_d[i * p.out_k + t] = ok ? ld[src] : FLT_MAX;
+                const uint32_t id = ok ? (li[src] & kIdMask) : kEmpty;
+                p.out_ids[orow * p.out_k + t] = (kRen && ok) ? p.perm[id] : id;
+                p.out_d[orow * p.out_k + t] = ok ? ld[src] : FLT_MAX;
             }
         } else {
             // prune_pool_to_ids: sort_unique_candidates + rng_extend (index.h:772-829)
@@ -709,6 +751,77 @@ __global__ void fill_reverse_kernel(const uint32_t* __restrict__ ids, uint64_t n
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n * K; t += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t v = ids[t];
         if (v < n) rev[off[v] + atomicAdd(fill + v, 1u)] = (uint32_t)(t / K);
+    }
+}
+
+// ------------------------------------------------------------ locality numbering
+// The AKNN gather's visited tests and row reads stay local when rows that
+// visit one another carry nearby numbers.  Rows are numbered component by
+// component of the list graph (min-label propagation over the lists, both
+// directions), in tree 0's leaf order inside a component.  The numbering
+// changes no result: the gather breaks (dist, id) ties and writes its output
+// through the original ids.
+
+__device__ __forceinline__ uint32_t ld_cg_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.global.cg.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// One propagation round, a warp per row: the smallest label of the row and its
+// list goes to all of them; *changed is set when any label fell.
+__global__ void label_prop_kernel(const uint32_t* __restrict__ ids, uint64_t n, uint32_t K, uint32_t* lab,
+                                  uint32_t* changed) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+        uint32_t m = ld_cg_u32(lab + i);
+        for (uint32_t j = lane; j < K; j += 32) {
+            const uint32_t v = ids[i * K + j];
+            if (v < n) m = min(m, ld_cg_u32(lab + v));
+        }
+        for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(kAll, m, o));
+        bool fell = false;
+        if (lane == 0 && atomicMin(lab + i, m) > m) fell = true;
+        for (uint32_t j = lane; j < K; j += 32) {
+            const uint32_t v = ids[i * K + j];
+            if (v < n && ld_cg_u32(lab + v) > m && atomicMin(lab + v, m) > m) fell = true;
+        }
+        if (__any_sync(kAll, fell) && lane == 0) atomicOr(changed, 1u);
+    }
+}
+
+// lab[i] = lab[lab[i]]: every label is the number of a row of the same
+// component, so one jump follows a chain of propagated labels.
+__global__ void label_jump_kernel(uint32_t* lab, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t l = ld_cg_u32(lab + i);
+        const uint32_t l2 = ld_cg_u32(lab + l);
+        if (l2 < l) atomicMin(lab + i, l2);
+    }
+}
+
+__global__ void label_init_kernel(uint32_t* lab, uint64_t n) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        lab[i] = (uint32_t)i;
+}
+
+__global__ void inverse_perm_kernel(const uint32_t* __restrict__ perm, uint64_t n, uint32_t* __restrict__ inv) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        inv[perm[i]] = (uint32_t)i;
+}
+
+// Lists in the new numbering: row k is original row perm[k], its ids mapped by
+// inv (empty slots stay empty), its values as they are.
+__global__ void renumber_lists_kernel(const uint32_t* __restrict__ ids, const float* __restrict__ vals,
+                                      const uint32_t* __restrict__ perm, const uint32_t* __restrict__ inv, uint64_t n,
+                                      uint32_t K, uint32_t* __restrict__ ids2, float* __restrict__ vals2) {
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n * K; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = t / K;
+        const uint64_t src = (uint64_t)perm[k] * K + (t - k * K);
+        const uint32_t v = ids[src];
+        ids2[t] = v < n ? inv[v] : kEmpty;
+        vals2[t] = vals[src];
     }
 }
 
@@ -1038,6 +1151,49 @@ static int build_reverse(Ctx* c, const uint32_t* d_ids, uint64_t n, uint32_t K, 
     return sync(c);
 }
 
+// The locality numbering of the gather (label propagation on the device, a
+// counting sort by label in tree-0 order on the host): perm (new -> original)
+// and inv (original -> new).  order: tree 0's permutation.
+static int locality_order(Ctx* c, const uint32_t* d_ids, uint64_t n, uint32_t K, const uint32_t* d_order, DevBuf& perm,
+                          DevBuf& inv) {
+    TmpBuf lab(c), flag(c);
+    int rc;
+    if ((rc = ensure(c, lab, n * 4)) || (rc = ensure(c, flag, 4)) || (rc = ensure(c, perm, n * 4)) ||
+        (rc = ensure(c, inv, n * 4)))
+        return rc;
+    const int blocks = c->sm_count * 8;
+    label_init_kernel<<<blocks, 256, 0, c->stream>>>(lab.as<uint32_t>(), n);
+    ANQI_CUDA(c, cudaGetLastError());
+    // rounds until no label falls (bounded; a cut-off round count only
+    // weakens the locality, never a result)
+    for (int round = 0; round < 64; round++) {
+        ANQI_CUDA(c, cudaMemsetAsync(flag.p, 0, 4, c->stream));
+        label_prop_kernel<<<blocks, 256, 0, c->stream>>>(d_ids, n, K, lab.as<uint32_t>(), flag.as<uint32_t>());
+        label_jump_kernel<<<blocks, 256, 0, c->stream>>>(lab.as<uint32_t>(), n);
+        ANQI_CUDA(c, cudaGetLastError());
+        uint32_t changed = 0;
+        if ((rc = d2h(c, &changed, flag, 4)) || (rc = sync(c))) return rc;
+        if (!changed) break;
+    }
+    std::vector<uint32_t> hl(n), ho(n), start(n + 1, 0), out(n);
+    ANQI_CUDA(c, cudaMemcpyAsync(ho.data(), d_order, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    if ((rc = d2h(c, hl.data(), lab, n * 4)) || (rc = sync(c))) return rc;
+    for (uint64_t i = 0; i < n; i++) {
+        if (hl[i] >= n) return fail(c, ANQI_ERR_DEVICE, "locality numbering: label out of range");
+        start[hl[i] + 1]++;
+    }
+    for (uint64_t l = 0; l < n; l++) start[l + 1] += start[l];
+    for (uint64_t k = 0; k < n; k++) {
+        const uint32_t o = ho[k];
+        if (o >= n) return fail(c, ANQI_ERR_DEVICE, "locality numbering: bad tree order");
+        out[start[hl[o]]++] = o;
+    }
+    if ((rc = h2d(c, perm, out.data(), n * 4))) return rc;
+    inverse_perm_kernel<<<blocks, 256, 0, c->stream>>>(perm.as<uint32_t>(), n, inv.as<uint32_t>());
+    ANQI_CUDA(c, cudaGetLastError());
+    return ANQI_OK;
+}
+
 static uint64_t max_reverse(Ctx* c, const DevBuf& off, uint64_t n) {
     std::vector<uint64_t> h(n + 1);
     cudaMemcpy(h.data(), off.p, (n + 1) * 8, cudaMemcpyDeviceToHost);
@@ -1071,11 +1227,14 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     p.hash_shift = hash_cap ? 32u - (uint32_t)__builtin_ctz(hash_cap) : 0u;
     p.gcap = gcap;
     p.gshift = gcap ? 32u - (uint32_t)__builtin_ctz(gcap) : 0u;
-    const size_t per_warp = gather_smem_words(p.ef, topk_cap, p.sort_words, hash_cap) * 4;
+    const bool ren = p.mode == kModeAknn && p.perm && !p.ip;
+    if (p.perm && !ren) return fail(c, ANQI_ERR_ARGS, "renumbered rows are an AKNN-mode (l2) option");
+    const size_t per_warp = gather_smem_words(p.ef, topk_cap, p.sort_words, hash_cap, ren ? kWinWords : 0) * 4;
     const size_t smem = per_warp * warps_per_block;
     if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "explore range %u too large", p.ef);
     auto* kern = p.mode == kModeVamana ? gather_kernel<false, true>
                  : p.ip                  ? gather_kernel<true>
+                 : ren                   ? gather_kernel<false, false, true>
                                          : gather_kernel<false>;
     ANQI_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -1895,22 +2054,49 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
     t = Clock::now();
     const DevBuf& gid = ap->nn_iters > 0 ? static_cast<const DevBuf&>(hi) : static_cast<const DevBuf&>(ki);
     const DevBuf& gval = ap->nn_iters > 0 ? static_cast<const DevBuf&>(hv) : static_cast<const DevBuf&>(kd);
-    if ((rc = build_reverse(c, gid.as<uint32_t>(), n, K, roff, rev))) return rc;
+    GatherParams p = base_params(dx, dn, n, xs, d);
+    // l2: the gather runs over rows renumbered for locality (lists, rows and
+    // norms permuted; ANQI_B200_GATHER_RENUMBER=0 keeps the original numbering)
+    const char* ren_env = std::getenv("ANQI_B200_GATHER_RENUMBER");
+    const bool ren = !ip && !(ren_env && ren_env[0] == '0');
+    TmpBuf dxc(c), rperm(c), rinv(c), rids(c), rvals(c), rnorm(c);
+    if (ren) {
+        if ((rc = locality_order(c, gid.as<uint32_t>(), n, K, order.as<uint32_t>(), rperm, rinv)) ||
+            (rc = ensure(c, rids, n * K * 4)) || (rc = ensure(c, rvals, n * K * 4)) || (rc = ensure(c, rnorm, n * 4)) ||
+            (rc = ensure(c, dxc, n * xs * 4ull)))
+            return rc;
+        const int blocks = c->sm_count * 8;
+        renumber_lists_kernel<<<blocks, 256, 0, c->stream>>>(gid.as<uint32_t>(), gval.as<float>(), rperm.as<uint32_t>(),
+                                                            rinv.as<uint32_t>(), n, K, rids.as<uint32_t>(),
+                                                            rvals.as<float>());
+        // d = 128: rows in chunk column order (two shuffles per distance
+        // instead of the lane tree's nine; the same bits)
+        permute_rows_kernel<<<blocks, 256, 0, c->stream>>>(dx.as<float>(), dxc.as<float>(), rperm.as<uint32_t>(), n, xs,
+                                                           d == 128 ? 128u : 0u);
+        permute_vals_kernel<<<blocks, 256, 0, c->stream>>>(dn.as<float>(), rnorm.as<float>(), rperm.as<uint32_t>(), n);
+        ANQI_CUDA(c, cudaGetLastError());
+        if ((rc = build_reverse(c, rids.as<uint32_t>(), n, K, roff, rev))) return rc;
+        p.x = dxc.as<float>();
+        p.norms = rnorm.as<float>();
+        p.cols = d == 128 ? 1 : 0;
+        p.g_ids = rids.as<uint32_t>();
+        p.g_vals = rvals.as<float>();
+        p.perm = rperm.as<uint32_t>();
+    } else {
+        if ((rc = build_reverse(c, gid.as<uint32_t>(), n, K, roff, rev))) return rc;
+        // d = 128: the gather reads its rows in chunk column order
+        if (d == 128 && !ip) {
+            if ((rc = ensure(c, dxc, n * xs * 4ull))) return rc;
+            if ((rc = chunk_cols(c, dx.as<float>(), dxc.as<float>(), n, xs, 128))) return rc;
+            p.x = dxc.as<float>();
+            p.cols = 1;
+        }
+        p.g_ids = gid.as<uint32_t>();
+        p.g_vals = gval.as<float>();
+    }
     const double reverse_ms = ms_since(t);
     t = Clock::now();
     if ((rc = ensure(c, oi, n * K * 4)) || (rc = ensure(c, od, n * K * 4))) return rc;
-    GatherParams p = base_params(dx, dn, n, xs, d);
-    // d = 128: the gather reads its rows in chunk column order (two shuffles
-    // per distance instead of the lane tree's nine; the same bits)
-    TmpBuf dxc(c);
-    if (d == 128 && !ip) {
-        if ((rc = ensure(c, dxc, n * xs * 4ull))) return rc;
-        if ((rc = chunk_cols(c, dx.as<float>(), dxc.as<float>(), n, xs, 128))) return rc;
-        p.x = dxc.as<float>();
-        p.cols = 1;
-    }
-    p.g_ids = gid.as<uint32_t>();
-    p.g_vals = gval.as<float>();
     p.K = K;
     p.rev_off = roff.as<uint64_t>();
     p.rev_ids = rev.as<uint32_t>();
@@ -1921,8 +2107,10 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
     p.out_k = K;
     p.out_ids = oi.as<uint32_t>();
     p.out_d = od.as<float>();
-    p.row_order = std::getenv("ANQI_B200_ORDER") && std::getenv("ANQI_B200_ORDER")[0] == '0' ? nullptr
-                                                                                            : order.as<uint32_t>();
+    // rows of one RP-tree leaf run together (the renumbered rows are in that order already)
+    p.row_order = ren || (std::getenv("ANQI_B200_ORDER") && std::getenv("ANQI_B200_ORDER")[0] == '0')
+                      ? nullptr
+                      : order.as<uint32_t>();
     uint64_t pool_total = 0;
     double gather_kernel_ms = 0;
     if ((rc = run_gather(c, p, max_reverse(c, roff, n), &pool_total, &gather_kernel_ms))) return rc;

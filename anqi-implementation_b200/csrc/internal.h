@@ -175,6 +175,13 @@ int upload_padded(Ctx* c, DevBuf& b, const float* src, uint64_t n, uint32_t d, u
 // Device rows (n x stride) with each of the first `full` columns' 16-float
 // chunks stored in chunk column order (common.cuh chunk_col_pos), on the stream.
 int chunk_cols(Ctx* c, const float* src, float* dst, uint64_t n, uint32_t stride, uint32_t full);
+// dst row i = src row perm[i] (cols_full != 0: in chunk column order over the
+// first cols_full columns); dst[i] = src[perm[i]] for one value per row.
+__global__ void permute_rows_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                                    const uint32_t* __restrict__ perm, uint64_t n, uint32_t stride,
+                                    uint32_t cols_full);
+__global__ void permute_vals_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                                    const uint32_t* __restrict__ perm, uint64_t n);
 
 // A built random-projection forest (breadth-first node numbering per tree; tree
 // t's nodes at [t * cap_nodes, ...), its permutation at [t * n, ...)).

@@ -417,6 +417,30 @@ def test_aknn_build_tensor_init_identical(ctx, kind, monkeypatch):
 
 
 
+@pytest.mark.parametrize("kind", ["integer128", "float40", "duplicates", "islands"])
+def test_aknn_gather_renumbered_identical(ctx, kind, monkeypatch):
+    """The AKNN gather over rows renumbered for locality (components of the
+    list graph, tree-0 order inside; the per-warp window bitmap) gives the
+    original numbering's lists bit for bit: ties at equal distances (integer
+    rows, duplicate rows) break on the original ids."""
+    from anqi import pipeline
+    if kind == "integer128":
+        x, _ = pipeline.mixture(20000, 128, 1, centers=50, seed=7)
+    elif kind == "float40":
+        x = clustered(12000, 40, 11, nc=60)
+    elif kind == "duplicates":
+        x = clustered(6000, 24, 4, nc=30)
+        x = np.concatenate([x, x[:3000], x[:500]])
+    else:  # well-separated clusters of about 90 rows (K = 50): the list graph falls into components
+        x, _ = pipeline.mixture(9000, 128, 1, centers=100, sigma=2.0, seed=3)
+    got = []
+    for ren in ("1", "0"):
+        monkeypatch.setenv("ANQI_B200_GATHER_RENUMBER", ren)
+        got.append(_aknn(ctx, x, 1))
+    assert np.array_equal(got[0][0], got[1][0])
+    assert np.array_equal(bits(got[0][1]), bits(got[1][1]))
+
+
 def localjoin_precision(ctx, x, ids, vals, precision, sample=20, rounds=6):
     x = f32(x)
     ids = u32(ids).copy()
