@@ -89,8 +89,12 @@ def aknn_build(ctx: Context, base: np.ndarray, k=100, leaf=500, trees=64, ef=600
     dist = np.empty((n, k), np.float32)
     st = BuildStats()
     ctx._check(ctx.lib.anqi_aknn_build(ctx.h, base, n, d, C.byref(p), ids, dist, C.byref(st)), "aknn_build")
-    keys = dist - np.float32(1.0) if metric == "ip" else np.maximum(dist, np.float32(0.0))
-    return ids, keys, st.as_dict()
+    # the record keys in place (a second n x k array costs a pass over memory)
+    if metric == "ip":
+        np.subtract(dist, np.float32(1.0), out=dist)
+    else:
+        np.maximum(dist, np.float32(0.0), out=dist)
+    return ids, dist, st.as_dict()
 
 
 def graph_build(ctx: Context, lifted: np.ndarray, warm_ids: np.ndarray, degree=48, nn_k=50, explore=100,

@@ -1993,6 +1993,15 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
                 if (!rc && msmem > 48 * 1024)
                     rc = cu(cudaFuncSetAttribute(leaf_merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem),
                             "cudaFuncSetAttribute");
+                // every tree's batches planned on the host first, their tiles
+                // uploaded once: the filter and merge launches then follow
+                // each other on the stream without a host round trip
+                struct BatchPlan {
+                    uint64_t base, nslots;
+                    size_t t0, nt;
+                };
+                std::vector<LeafTile> tiles;
+                std::vector<BatchPlan> plan;
                 for (uint32_t tr = 0; tr < ap->trees && !rc; tr++) {
                     // leaves in permutation order, in batches of contiguous positions
                     std::vector<LeafRef>& lv = tree_leaves[tr];
@@ -2002,20 +2011,27 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
                         size_t l1 = l0;
                         while (l1 < lv.size() && lv[l1].off + lv[l1].cnt - base <= brows) l1++;
                         const std::vector<LeafRef> batch(lv.begin() + l0, lv.begin() + l1);
-                        const uint64_t nslots = lv[l1 - 1].off + lv[l1 - 1].cnt - base;
-                        rc = tc_leaf_candidates(c, tp, dx.as<float>(), dn.as<float>(), n, xs, d, f.perm.as<uint32_t>(),
-                                                batch, kd.as<float>(), ksz.as<uint32_t>(), K, ccnt.as<uint32_t>(), cap,
-                                                cid.as<uint32_t>(), ckey.as<float>(), base);
-                        if (rc) break;
-                        leaf_merge_kernel<<<c->sm_count * 8, 32 * wpb, msmem, c->stream>>>(
-                            dx.as<float>(), dn.as<float>(), n, xs, d, f.perm.as<uint32_t>(), base, nslots,
-                            ccnt.as<uint32_t>(), cap, cid.as<uint32_t>(), ckey.as<float>(), K, kd.as<float>(),
-                            ki.as<uint32_t>(), ksz.as<uint32_t>(), c->err.as<uint32_t>());
-                        rc = cu(cudaGetLastError(), "leaf_merge_kernel");
+                        const size_t t0 = tiles.size();
+                        rc = tc_leaf_tiles(c, batch, cap, tiles);
+                        plan.push_back({base, lv[l1 - 1].off + lv[l1 - 1].cnt - base, t0, tiles.size() - t0});
                         l0 = l1;
                     }
                 }
-                if (!rc) rc = check_device_error(c, "init_knn merge");
+                TmpBuf dtiles(c);
+                if (!rc) rc = h2d(c, dtiles, tiles.data(), std::max<size_t>(1, tiles.size()) * sizeof(LeafTile));
+                for (size_t b = 0; b < plan.size() && !rc; b++) {
+                    const BatchPlan& bp = plan[b];
+                    rc = tc_leaf_filter(c, tp, dx.as<float>(), dn.as<float>(), n, xs, d, f.perm.as<uint32_t>(),
+                                        dtiles.as<LeafTile>() + bp.t0, bp.nt, kd.as<float>(), ksz.as<uint32_t>(), K,
+                                        ccnt.as<uint32_t>(), cap, cid.as<uint32_t>(), ckey.as<float>(), bp.base);
+                    if (rc) break;
+                    leaf_merge_kernel<<<c->sm_count * 8, 32 * wpb, msmem, c->stream>>>(
+                        dx.as<float>(), dn.as<float>(), n, xs, d, f.perm.as<uint32_t>(), bp.base, bp.nslots,
+                        ccnt.as<uint32_t>(), cap, cid.as<uint32_t>(), ckey.as<float>(), K, kd.as<float>(),
+                        ki.as<uint32_t>(), ksz.as<uint32_t>(), c->err.as<uint32_t>());
+                    rc = cu(cudaGetLastError(), "leaf_merge_kernel");
+                }
+                if (!rc) rc = check_device_error(c, "tensor-core init_knn");
             }
             tc_release(c, tp);
         } else {

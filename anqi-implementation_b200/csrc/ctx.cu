@@ -2,6 +2,7 @@
 // Context lifetime, device memory, error reporting, and small shared kernels.
 #include <cstdarg>
 #include <cstdio>
+#include <thread>
 
 #include "common.cuh"
 #include "internal.h"
@@ -50,17 +51,113 @@ void release(Ctx* c, DevBuf& b) {
     b.bytes = 0;
 }
 
-int h2d(Ctx* c, DevBuf& b, const void* src, size_t bytes) {
-    int rc = ensure(c, b, bytes);
-    if (rc) return rc;
-    if (bytes) ANQI_CUDA(c, cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, c->stream));
+// Large copies between pageable host memory and the device go through the
+// context's pinned staging slots: host threads copy one chunk into (or out of)
+// a slot while the copy engine moves another, instead of the driver staging
+// pageable memory through one thread.  Pinned or registered host memory and
+// small copies go direct.
+constexpr size_t kStageChunk = (size_t)32 << 20;
+constexpr size_t kStageMin = (size_t)48 << 20;
+
+static void par_memcpy(void* dst, const void* src, size_t bytes) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const unsigned T = std::max(1u, std::min(8u, hw / 2));
+    const size_t part = ((bytes + T - 1) / T + 4095) & ~(size_t)4095;
+    if (T == 1 || bytes < ((size_t)4 << 20)) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < T && (size_t)t * part < bytes; t++) {
+        const size_t o = (size_t)t * part, len = std::min(part, bytes - o);
+        th.emplace_back([=] { std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, len); });
+    }
+    std::memcpy(dst, src, std::min(part, bytes));
+    for (std::thread& x : th) x.join();
+}
+
+static bool staged(Ctx* c, const void* host, size_t bytes) {
+    if (bytes < kStageMin) return false;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (a.type != cudaMemoryTypeUnregistered) return false;
+    if (!c->stage[0]) {
+        for (int s = 0; s < Ctx::kStageSlots; s++) {
+            if (cudaHostAlloc(&c->stage[s], kStageChunk, cudaHostAllocDefault) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->stage_ev[s], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                for (int t = 0; t <= s; t++) {
+                    if (c->stage[t]) cudaFreeHost(c->stage[t]);
+                    if (c->stage_ev[t]) cudaEventDestroy(c->stage_ev[t]);
+                    c->stage[t] = nullptr;
+                    c->stage_ev[t] = nullptr;
+                }
+                return false;
+            }
+        }
+    }
+    return true;
+}
+
+int h2d_raw(Ctx* c, void* dst, const void* src, size_t bytes) {
+    if (!bytes) return ANQI_OK;
+    if (!staged(c, src, bytes)) {
+        ANQI_CUDA(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+        return ANQI_OK;
+    }
+    size_t k = 0;
+    for (size_t o = 0; o < bytes; o += kStageChunk, k++) {
+        const int s = (int)(k % Ctx::kStageSlots);
+        const size_t len = std::min(kStageChunk, bytes - o);
+        ANQI_CUDA(c, cudaEventSynchronize(c->stage_ev[s]));  // the slot's previous copy has left it
+        par_memcpy(c->stage[s], static_cast<const char*>(src) + o, len);
+        ANQI_CUDA(c, cudaMemcpyAsync(static_cast<char*>(dst) + o, c->stage[s], len, cudaMemcpyHostToDevice, c->stream));
+        ANQI_CUDA(c, cudaEventRecord(c->stage_ev[s], c->stream));
+    }
     return ANQI_OK;
 }
 
-int d2h(Ctx* c, void* dst, const DevBuf& b, size_t bytes) {
-    if (bytes) ANQI_CUDA(c, cudaMemcpyAsync(dst, b.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+// Staged copies return with the data in dst; direct ones are ordered on the
+// stream (the caller synchronizes before reading).
+int d2h_raw(Ctx* c, void* dst, const void* src, size_t bytes) {
+    if (!bytes) return ANQI_OK;
+    if (!staged(c, dst, bytes)) {
+        ANQI_CUDA(c, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+        return ANQI_OK;
+    }
+    const size_t nch = (bytes + kStageChunk - 1) / kStageChunk;
+    auto issue = [&](size_t k) -> int {
+        const int s = (int)(k % Ctx::kStageSlots);
+        const size_t o = k * kStageChunk, len = std::min(kStageChunk, bytes - o);
+        ANQI_CUDA(c, cudaEventSynchronize(c->stage_ev[s]));
+        ANQI_CUDA(c, cudaMemcpyAsync(c->stage[s], static_cast<const char*>(src) + o, len, cudaMemcpyDeviceToHost,
+                                     c->stream));
+        ANQI_CUDA(c, cudaEventRecord(c->stage_ev[s], c->stream));
+        return ANQI_OK;
+    };
+    int rc;
+    for (size_t k = 0; k < nch && k < (size_t)Ctx::kStageSlots; k++)
+        if ((rc = issue(k))) return rc;
+    for (size_t k = 0; k < nch; k++) {
+        const int s = (int)(k % Ctx::kStageSlots);
+        const size_t o = k * kStageChunk, len = std::min(kStageChunk, bytes - o);
+        ANQI_CUDA(c, cudaEventSynchronize(c->stage_ev[s]));
+        par_memcpy(static_cast<char*>(dst) + o, c->stage[s], len);
+        if (k + Ctx::kStageSlots < nch && (rc = issue(k + Ctx::kStageSlots))) return rc;
+    }
     return ANQI_OK;
 }
+
+int h2d(Ctx* c, DevBuf& b, const void* src, size_t bytes) {
+    int rc = ensure(c, b, bytes);
+    if (rc) return rc;
+    return h2d_raw(c, b.p, src, bytes);
+}
+
+int d2h(Ctx* c, void* dst, const DevBuf& b, size_t bytes) { return d2h_raw(c, dst, b.p, bytes); }
 
 int sync(Ctx* c) {
     ANQI_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -134,14 +231,11 @@ __global__ void pad_rows_kernel(const float* __restrict__ src, float* __restrict
 int upload_padded(Ctx* c, DevBuf& b, const float* src, uint64_t n, uint32_t d, uint32_t stride) {
     int rc = ensure(c, b, (size_t)n * stride * 4 + 64);
     if (rc) return rc;
-    if (stride == d) {
-        ANQI_CUDA(c, cudaMemcpyAsync(b.p, src, (size_t)n * d * 4, cudaMemcpyHostToDevice, c->stream));
-        return ANQI_OK;
-    }
+    if (stride == d) return h2d_raw(c, b.p, src, (size_t)n * d * 4);
     TmpBuf tmp(c);
     rc = ensure(c, tmp, (size_t)n * d * 4);
     if (rc) return rc;
-    ANQI_CUDA(c, cudaMemcpyAsync(tmp.p, src, (size_t)n * d * 4, cudaMemcpyHostToDevice, c->stream));
+    if ((rc = h2d_raw(c, tmp.p, src, (size_t)n * d * 4))) return rc;
     pad_rows_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(tmp.as<float>(), b.as<float>(), n, d, stride);
     ANQI_CUDA(c, cudaGetLastError());
     ANQI_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -380,6 +474,10 @@ void anqi_ctx_destroy(anqi_ctx* h) {
     if (c->ev3) cudaEventDestroy(c->ev3);
     if (c->tev0) cudaEventDestroy(c->tev0);
     if (c->tev1) cudaEventDestroy(c->tev1);
+    for (int s = 0; s < Ctx::kStageSlots; s++) {
+        if (c->stage[s]) cudaFreeHost(c->stage[s]);
+        if (c->stage_ev[s]) cudaEventDestroy(c->stage_ev[s]);
+    }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete h;
 }

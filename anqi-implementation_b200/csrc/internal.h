@@ -129,6 +129,10 @@ struct Ctx {
     DevBuf init_cnt, init_cid, init_key;  // tensor-core init_knn candidate buffers
     GraphBuild gb;                        // staged G48 build
     DevBuf g_bits, g_vlog, g_pd, g_pi, g_gtab;  // gather kernel per-slot scratch
+    // pinned staging slots for large copies to and from pageable host memory
+    static constexpr int kStageSlots = 3;
+    void* stage[kStageSlots] = {};
+    cudaEvent_t stage_ev[kStageSlots] = {};
     std::vector<uint64_t> qgraph_key;
     uint64_t device_bytes = 0;
     std::vector<DevBuf*> member_bufs() {
@@ -163,6 +167,11 @@ struct TmpBuf : DevBuf {
     TmpBuf& operator=(const TmpBuf&) = delete;
 };
 int h2d(Ctx* c, DevBuf& b, const void* src, size_t bytes);
+// Host <-> device copies of raw ranges on the context's stream (large
+// pageable ranges through pinned staging slots; d2h_raw then returns with the
+// data in place).
+int h2d_raw(Ctx* c, void* dst, const void* src, size_t bytes);
+int d2h_raw(Ctx* c, void* dst, const void* src, size_t bytes);
 int d2h(Ctx* c, void* dst, const DevBuf& b, size_t bytes);
 int sync(Ctx* c);
 // Reads the device error word, maps it to a status (and clears it).
@@ -238,6 +247,15 @@ int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* 
                        uint32_t d, const uint32_t* d_members, const std::vector<LeafRef>& leaves,
                        const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
                        uint32_t* out_id, float* out_key, uint64_t pos_base);
+// The same in two steps, so that many batches launch without a host round
+// trip: the 128-row tiles of a batch's leaves (appended to tiles; a leaf
+// longer than cap + 1 is an argument error), then the filter over ntiles
+// tiles already on the device (errors are left in the device error word).
+int tc_leaf_tiles(Ctx* c, const std::vector<LeafRef>& leaves, uint32_t cap, std::vector<LeafTile>& tiles);
+int tc_leaf_filter(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs,
+                   uint32_t d, const uint32_t* d_members, const LeafTile* d_tiles, size_t ntiles,
+                   const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
+                   uint32_t* out_id, float* out_key, uint64_t pos_base);
 
 // L2 persisting window over [p, p + bytes) for kernels on the context's stream.
 void set_l2_window(Ctx* c, const void* p, size_t bytes);

@@ -946,19 +946,19 @@ int tc_join_filter(Ctx* c, const TcPrep& tp, const float* d_norms, uint64_t n, c
     return ANQI_OK;
 }
 
-int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs,
-                       uint32_t d, const uint32_t* d_members, const std::vector<LeafRef>& leaves,
-                       const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
-                       uint32_t* out_id, float* out_key, uint64_t pos_base) {
-    std::vector<LeafTile> tiles;
+int tc_leaf_tiles(Ctx* c, const std::vector<LeafRef>& leaves, uint32_t cap, std::vector<LeafTile>& tiles) {
     for (const LeafRef& l : leaves) {
         if (l.cnt > cap + 1) return fail(c, ANQI_ERR_ARGS, "leaf of %u rows exceeds the candidate capacity", l.cnt);
         for (uint32_t rb = 0; rb * kTile < l.cnt; rb++) tiles.push_back({l.off, l.cnt, rb});
     }
-    if (tiles.empty()) return ANQI_OK;
-    TmpBuf dt(c);
-    int rc;
-    if ((rc = h2d(c, dt, tiles.data(), tiles.size() * sizeof(LeafTile)))) return rc;
+    return ANQI_OK;
+}
+
+int tc_leaf_filter(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs,
+                   uint32_t d, const uint32_t* d_members, const LeafTile* d_tiles, size_t ntiles,
+                   const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
+                   uint32_t* out_id, float* out_key, uint64_t pos_base) {
+    if (ntiles == 0) return ANQI_OK;
     FilterParams p{};
     p.qb = p.xb = tp.bf.as<__nv_bfloat16>();
     p.q32 = p.x32 = d_x;
@@ -976,7 +976,7 @@ int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* 
     p.out_id = out_id;
     p.out_key = out_key;
     p.err = c->err.as<uint32_t>();
-    p.leaf_tiles = dt.as<LeafTile>();
+    p.leaf_tiles = d_tiles;
     p.members = d_members;
     p.list_kd = list_kd;
     p.list_sz = list_sz;
@@ -986,13 +986,30 @@ int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* 
     p.bx_err = tp.berr;
     p.bx_n = tp.bn;
     p.all_exact = tp.all_exact;
-    p.nrows = tiles.size() * kTile;
+    p.nrows = ntiles * kTile;
     p.split_len = 0;
     void (*kern)(FilterParams) = nullptr;
     size_t smem = 0;
+    int rc;
     if ((rc = filter_kernel_for(c, p.dp, &kern, &smem))) return rc;
-    kern<<<(unsigned)tiles.size(), kFilterThreads, smem, c->stream>>>(p);
+    kern<<<(unsigned)ntiles, kFilterThreads, smem, c->stream>>>(p);
     ANQI_CUDA(c, cudaGetLastError());
+    return ANQI_OK;
+}
+
+int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs,
+                       uint32_t d, const uint32_t* d_members, const std::vector<LeafRef>& leaves,
+                       const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
+                       uint32_t* out_id, float* out_key, uint64_t pos_base) {
+    std::vector<LeafTile> tiles;
+    int rc;
+    if ((rc = tc_leaf_tiles(c, leaves, cap, tiles))) return rc;
+    if (tiles.empty()) return ANQI_OK;
+    TmpBuf dt(c);
+    if ((rc = h2d(c, dt, tiles.data(), tiles.size() * sizeof(LeafTile)))) return rc;
+    if ((rc = tc_leaf_filter(c, tp, d_x, d_norms, n, xs, d, d_members, dt.as<LeafTile>(), tiles.size(), list_kd,
+                             list_sz, K, cnt, cap, out_id, out_key, pos_base)))
+        return rc;
     return check_device_error(c, "tensor-core init_knn filter");
 }
 
