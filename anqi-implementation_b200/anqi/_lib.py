@@ -75,7 +75,31 @@ class GraphParams(C.Structure):
     _fields_ = [("degree", C.c_uint32), ("nn_k", C.c_uint32), ("explore", C.c_uint32), ("ef_alpha", C.c_uint32),
                 ("join_iters", C.c_uint32), ("join_sample", C.c_uint32), ("leaf", C.c_uint32),
                 ("max_depth", C.c_uint32), ("seed", C.c_uint64), ("alpha", C.c_float), ("warm_width", C.c_uint32),
-                ("precision", C.c_uint32), ("vamana_passes", C.c_uint32), ("vamana_L", C.c_uint32)]
+                ("precision", C.c_uint32), ("vamana_passes", C.c_uint32), ("vamana_L", C.c_uint32),
+                ("edge", C.c_void_p)]
+
+
+class EdgePolicyC(C.Structure):
+    """anqi_edge_policy (include/anqi.h)."""
+    _fields_ = [("flags", C.c_uint32), ("nks", C.c_uint32), ("ks", C.c_uint32 * 8), ("nk", C.c_uint32),
+                ("budget", C.c_uint32), ("occlude_all", C.c_uint32), ("auto_candidates", C.c_uint32),
+                ("auto_max_swaps", C.c_uint32), ("lam", C.c_double), ("scale2", C.c_double),
+                ("lsg_alpha", C.c_double), ("resid", C.c_void_p), ("mu", C.c_void_p)]
+
+
+def edge_policy_c(pol):
+    """anqi_edge_policy of an anqi.edge_policy.EdgePolicy, or None for the
+    default prune; the returned struct keeps its tables alive."""
+    if pol is None or not pol.active:
+        return None
+    resid = np.ascontiguousarray(pol.resid, np.float32) if pol.resid is not None else None
+    mu = np.ascontiguousarray(pol.mu, np.float32) if pol.mu is not None else None
+    ks = (C.c_uint32 * 8)(*(list(pol.ks) + [0] * (8 - len(pol.ks))))
+    s = EdgePolicyC(pol.flags, len(pol.ks), ks, pol.nk, pol.budget, int(pol.occlude_all), pol.auto_candidates,
+                    pol.auto_max_swaps, pol.lam, pol.scale2, pol.lsg_alpha,
+                    resid.ctypes.data if resid is not None else None, mu.ctypes.data if mu is not None else None)
+    s._keep = (resid, mu)
+    return s
 
 
 class BuildStats(C.Structure):
@@ -139,6 +163,10 @@ _SIGS = {
     "anqi_graph_select": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _f32, C.c_uint32, C.c_uint32, C.c_uint32,
                           C.c_uint32, C.c_float, _u32, _u32],
     "anqi_graph_commit": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _u32, C.c_uint32, C.c_float, _u32, _u32],
+    "anqi_graph_select_policy": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _f32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                 C.c_uint32, C.c_float, _vp, _u32, _u32],
+    "anqi_graph_commit_policy": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _u32, C.c_uint32, C.c_float, _vp, _u32,
+                                 _u32],
     "anqi_graph_vamana_select": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _u32, C.c_uint32, _u32, C.c_uint32, _u32,
                                  C.c_uint32, C.c_float, _u32, _u32],
     "anqi_index_load": [_vp, C.POINTER(IndexDesc)],

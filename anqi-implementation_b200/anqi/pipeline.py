@@ -15,7 +15,7 @@ from pathlib import Path
 import numpy as np
 
 from . import formats, lrq_train
-from ._lib import METRICS, AknnParams, BuildStats, Context, GraphParams
+from ._lib import edge_policy_c, METRICS, AknnParams, BuildStats, Context, GraphParams
 
 EMPTY = 0xFFFFFFFF
 
@@ -99,15 +99,20 @@ def aknn_build(ctx: Context, base: np.ndarray, k=100, leaf=500, trees=64, ef=600
 
 def graph_build(ctx: Context, lifted: np.ndarray, warm_ids: np.ndarray, degree=48, nn_k=50, explore=100,
                 ef_alpha=8, join_iters=6, join_sample=20, leaf=100, seed=10, alpha=1.2, warm_width=100,
-                precision="bf16"):
+                precision="bf16", vamana_passes=0, vamana_L=128, edge=None):
     """build_index with the flat AKNN warm start; returns deg, links, post-order tree, stats.
     precision "bf16": LocalJoin pairs filtered on BF16 tensor-core tiles, kept
-    pairs recomputed in FP32 (identical graph); "fp32": CUDA cores only."""
+    pairs recomputed in FP32 (identical graph); "fp32": CUDA cores only.
+    vamana_passes: global Vamana refine passes; edge: an anqi.edge_policy
+    EdgePolicy for the prunes (None: the default prune)."""
     lifted = np.ascontiguousarray(lifted, np.float32)
     warm_ids = np.ascontiguousarray(warm_ids, np.uint32)
     n, dim = lifted.shape
     gp = GraphParams(degree, nn_k, explore, ef_alpha, join_iters, join_sample, leaf, 100, seed, alpha, warm_width,
-                     {"fp32": 0, "bf16": 1}[precision])
+                     {"fp32": 0, "bf16": 1}[precision], vamana_passes, vamana_L)
+    edge_c = edge_policy_c(edge)
+    if edge_c is not None:
+        gp.edge = C.addressof(edge_c)
     deg = np.empty(n, np.uint32)
     links = np.empty((n, degree), np.uint32)
     st = BuildStats()

@@ -11,10 +11,11 @@
 // analytic rank-M): the same argv, environment, prefix files, caches (file
 // names and identity keys, so a cache written by either program is found by
 // the other), stdout result lines and exit codes.  The global Vamana refine
-// (ANQI_VAMANA, styles global and old) runs on the device too.  Configurations
+// (ANQI_VAMANA, styles global and old) and the edge policies of the prune
+// (ANQI_EDGE_POLICY and its options) run on the device too.  Configurations
 // outside that path (rank-M or original geometry, integrated verifier, the
-// batched Vamana style, edge policies, fixed-k lift, recheck) exit 2 with a
-// message naming the setting.
+// batched Vamana style, fixed-k lift, recheck) exit 2 with a message naming
+// the setting.
 //
 // Differences of mechanism, not of result: the graph build, lift, LRQ
 // encode/materialize, search, postfilter and evaluation run on the device;
@@ -165,6 +166,14 @@ static std::string graph_cache_key(uint64_t M, uint64_t leaf, uint64_t nt, uint6
     std::string k = "M" + std::to_string(M) + "_leaf" + std::to_string(leaf) + "_nt" + std::to_string(nt) + "_ef" +
                     std::to_string(ef) + "_geomanyk_lift_rankm0_specific0_alpha" + env_or("ANQI_ALPHA", "1.2") +
                     "_liftnnk" + env_or("ANQI_LIFTNNK", "50") + "_graphnnd" + env_or("ANQI_GRAPHNND", "6");
+    // rknn_query.cpp:314-324
+    if (std::getenv("ANQI_EDGE_POLICY")) {
+        k += "_edge" + env_or("ANQI_EDGE_POLICY", "none") + "_eks" + env_or("ANQI_EDGE_KS", "10,50,100") + "_enk" +
+             env_or("ANQI_EDGE_NK", "100") + "_erb" + env_or("ANQI_EDGE_RESID_BUDGET", "16") + "_erl" +
+             env_or("ANQI_EDGE_RESID_LAMBDA", "1.0") + "_ebo" + env_or("ANQI_EDGE_BALL_OCCLUSION", "all");
+        if (std::getenv("ANQI_EDGE_RESID_FILE"))
+            k += "_erf" + hash16(file_fingerprint(env_or("ANQI_EDGE_RESID_FILE", "")));
+    }
     if (std::getenv("ANQI_VAMANA")) {
         const std::string style = env_or("ANQI_VAMANA_STYLE", "global");
         k += "_vam1_style" + style + "_L" + env_or("ANQI_VAMANA_L", "128") + "_P" + env_or("ANQI_VAMANA_PASS", "2") +
@@ -178,6 +187,122 @@ static std::string graph_cache_key(uint64_t M, uint64_t leaf, uint64_t nt, uint6
     return sanitize_tag(k);
 }
 
+// ANQI_EDGE_POLICY and its options, resolved for the device prune as
+// configure_edge_residual_cover (include/index.h:305-440) configures the
+// reference's: the same defaults, atoi / atof parsing, filters and exit-2
+// errors.  folder: the graph's folder prefix (its lift meta and default
+// residual table).  Resolved only when the graph is built, as there.
+struct EdgePolicyHost {
+    anqi_edge_policy p{};
+    std::vector<float> resid, mu;
+};
+
+static std::vector<int> parse_int_list(const std::string& s) {
+    std::vector<int> out;
+    std::stringstream ss(s);
+    std::string tok;
+    while (std::getline(ss, tok, ',')) {
+        if (tok.empty()) continue;
+        const int v = std::atoi(tok.c_str());
+        if (v > 0) out.push_back(v);
+    }
+    return out;
+}
+
+static bool read_table(const std::string& path, size_t floats, std::vector<float>& out, long long& got) {
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    got = -1;
+    if (!f) return false;
+    got = (long long)f.tellg();
+    if (got != (long long)(floats * 4)) return true;
+    f.seekg(0);
+    out.resize(floats);
+    f.read(reinterpret_cast<char*>(out.data()), (std::streamsize)(floats * 4));
+    if (!f) got = -2;
+    return true;
+}
+
+static void resolve_edge_policy(EdgePolicyHost& e, uint64_t n, uint32_t M, const std::string& folder) {
+    const char* pol_c = std::getenv("ANQI_EDGE_POLICY");
+    if (!pol_c || !*pol_c) return;
+    const std::string pol = pol_c;
+    anqi_edge_policy& p = e.p;
+    auto envd = [](const char* k, double d) { const char* v = std::getenv(k); return v ? std::atof(v) : d; };
+    auto envi = [](const char* k, int d) { const char* v = std::getenv(k); return v ? std::atoi(v) : d; };
+    if (pol == "lsg_rng" || pol == "lsg_bubble_hybrid") {
+        p.lsg_alpha = envd("ANQI_LSG_ALPHA", 1.0);
+        if (!std::isfinite(p.lsg_alpha) || p.lsg_alpha < 0.0)
+            die(2, "[edge-policy] invalid ANQI_LSG_ALPHA=%.17g", p.lsg_alpha);
+        const char* mp = std::getenv("ANQI_LSG_MU_FILE");
+        const std::string mu_path = mp ? mp : "";
+        if (mu_path.empty()) die(2, "[edge-policy] lsg_rng requires ANQI_LSG_MU_FILE");
+        long long got = 0;
+        if (!read_table(mu_path, n, e.mu, got)) die(2, "[edge-policy] lsg_rng cannot open mu table %s", mu_path.c_str());
+        if (got != (long long)(n * 4))
+            die(2, "[edge-policy] lsg mu size mismatch %s: expected %zu bytes, got %lld", mu_path.c_str(),
+                (size_t)(n * 4), got);
+        for (uint64_t i = 0; i < n; i++)
+            if (!std::isfinite((double)e.mu[i]) || e.mu[i] <= 0.0f)
+                die(2, "[edge-policy] invalid lsg mu[%zu]=%.9g", (size_t)i, (double)e.mu[i]);
+        p.flags |= ANQI_EDGE_LSG;
+        fprintf(stderr, "[edge-policy] %s lsg enabled alpha=%.6g mu=%s\n", pol.c_str(), p.lsg_alpha, mu_path.c_str());
+        if (pol == "lsg_rng") return;
+    }
+    static const char* kResidual[] = {"residual_cover", "ball_rng", "ball_hybrid", "ball_multik", "bubble_rng",
+                                      "bubble_hybrid", "bubble_multik", "bubble_auto", "bubble_auto_full",
+                                      "lsg_bubble_hybrid"};
+    bool needs = false;
+    for (const char* r : kResidual) needs = needs || pol == r;
+    if (!needs) return;
+    int nk = envi("ANQI_EDGE_NK", 100);
+    if (nk == 0) nk = 100;
+    if (nk < 0) die(2, "[edge-policy] invalid ANQI_EDGE_NK=%d", nk);
+    p.nk = (uint32_t)nk;
+    p.budget = (uint32_t)std::min<long long>(std::max(0, envi("ANQI_EDGE_RESID_BUDGET", 16)), M);
+    p.auto_candidates = (uint32_t)std::max(1, envi("ANQI_EDGE_AUTO_CANDIDATES", (int)M));
+    p.auto_max_swaps = (uint32_t)std::max(1, envi("ANQI_EDGE_AUTO_MAX_SWAPS", (int)M));
+    p.lambda = envd("ANQI_EDGE_RESID_LAMBDA", 1.0);
+    p.scale2 = 1.0;
+    const char* ks_c = std::getenv("ANQI_EDGE_KS");
+    std::vector<int> ks;
+    for (int k : parse_int_list(ks_c ? ks_c : "10,50,100"))
+        if (k >= 1 && k <= nk) ks.push_back(k);
+    if (ks.empty()) return;
+    if (ks.size() > 8) die(2, "[edge-policy] at most 8 values in ANQI_EDGE_KS are supported here");
+    p.nks = (uint32_t)ks.size();
+    for (size_t t = 0; t < ks.size(); t++) p.ks[t] = (uint32_t)ks[t];
+    const bool autop = pol == "bubble_auto" || pol == "bubble_auto_full";
+    if (p.budget == 0 && pol != "ball_rng" && !autop) return;
+    {
+        std::ifstream mf(folder + "_anqi_meta.txt");
+        double mstar = 0.0, sc = 1.0;
+        if (mf >> mstar >> sc) p.scale2 = sc * sc;
+    }
+    const char* rf = std::getenv("ANQI_EDGE_RESID_FILE");
+    const std::string resid_path = rf ? rf : folder + "_anqi_rankm_residual.bin";
+    long long got = 0;
+    if (!read_table(resid_path, n * (size_t)nk, e.resid, got))
+        die(2, "[edge-policy] residual_cover requested but missing %s", resid_path.c_str());
+    if (got == -2) die(2, "[edge-policy] bad residual table %s", resid_path.c_str());
+    if (got != (long long)(n * (size_t)nk * 4))
+        die(2, "[edge-policy] residual table stride/size mismatch %s: expected %zu bytes (n=%zu edge_nk=%d), got %lld "
+               "bytes; set ANQI_EDGE_NK to the table stride",
+            resid_path.c_str(), (size_t)(n * (size_t)nk * 4), (size_t)n, nk, got);
+    if (pol == "residual_cover") {
+        p.flags |= ANQI_EDGE_COVER;
+    } else {
+        p.flags |= ANQI_EDGE_BALL;
+        if (pol == "ball_rng" || pol == "bubble_rng") p.flags |= ANQI_EDGE_PURE;
+        const char* oc = std::getenv("ANQI_EDGE_BALL_OCCLUSION");
+        p.occlude_all = std::string(oc ? oc : "all") != "any";
+    }
+    if (autop) p.flags |= ANQI_EDGE_AUTO | (pol == "bubble_auto_full" ? ANQI_EDGE_AUTO_FULL : 0u);
+    p.resid = e.resid.data();
+    p.mu = e.mu.empty() ? nullptr : e.mu.data();
+    fprintf(stderr, "[edge-policy] %s enabled budget=%u lambda=%.4g scale2=%.6g nk=%d\n", pol.c_str(), p.budget,
+            p.lambda, p.scale2, nk);
+}
+
 // nndindex::generate_config (include/index.h:1703-1769) with ANQI_GRAPH_CACHE_KEY set;
 // ef_alpha and prune_alpha are floats there, printed by std::to_string.
 static std::string graph_file_name(uint64_t M, uint64_t nn_k, uint64_t n, uint64_t dim, float alpha,
@@ -185,6 +310,24 @@ static std::string graph_file_name(uint64_t M, uint64_t nn_k, uint64_t n, uint64
     std::string cfg = "fd_metric_l2_M_" + std::to_string(M) + "_nnk_" + std::to_string(nn_k) + "_ntrees_64_n_" +
                       std::to_string(n) + "_dim_" + std::to_string(dim) + "_efa_" + std::to_string(8.0f) + "_pa_" + std::to_string(alpha) +
                       "_er_100_graphnnd_" + env_or("ANQI_GRAPHNND", "6") + "_gk_" + hash16(graph_key);
+    // the edge policy's part of the name (index.h:1741-1764)
+    if (std::getenv("ANQI_EDGE_POLICY")) {
+        const std::string pol = env_or("ANQI_EDGE_POLICY", "none");
+        cfg += "_edge_" + pol;
+        if (pol == "lsg_rng" || pol == "lsg_bubble_hybrid") {
+            std::string mu_key = env_or("ANQI_LSG_CACHE_KEY", "");
+            if (mu_key.empty()) mu_key = env_or("ANQI_LSG_MU_FILE", "");
+            cfg += "_lsa_" + env_or("ANQI_LSG_ALPHA", "1.0") + "_lsgmu_" + hash16(mu_key);
+        }
+        if (pol != "lsg_rng") {
+            cfg += "_eks_" + env_or("ANQI_EDGE_KS", "10,50,100") + "_enk_" + env_or("ANQI_EDGE_NK", "100") + "_erb_" +
+                   env_or("ANQI_EDGE_RESID_BUDGET", "16") + "_erl_" + env_or("ANQI_EDGE_RESID_LAMBDA", "1.0") + "_ebo_" +
+                   env_or("ANQI_EDGE_BALL_OCCLUSION", "all");
+            if (pol == "bubble_auto" || pol == "bubble_auto_full")
+                cfg += "_eac_" + env_or("ANQI_EDGE_AUTO_CANDIDATES", "M") + "_eas_" +
+                       env_or("ANQI_EDGE_AUTO_MAX_SWAPS", "M");
+        }
+    }
     return sanitize_tag(cfg);
 }
 
@@ -653,8 +796,7 @@ static int run(int argc, char** argv) {
     if (env_flag("ANQI_RECHECK"))
         die(2, "[rknn] ANQI_RECHECK cannot be mixed with an independent postfilter verifier; select "
                "ANQI_RADIUS_MODE=exact_f32 for the exact component comparison");
-    for (const char* e : {"ANQI_EDGE_POLICY", "ANQI_REUSE_ORIG_KNN"})
-        if (std::getenv(e)) not_here(e);
+    if (std::getenv("ANQI_REUSE_ORIG_KNN")) not_here("ANQI_REUSE_ORIG_KNN");
     // the global Vamana refine (index.h:1262-1285); the batched variant is not built here
     uint32_t vamana_passes = 0, vamana_L = 128;
     if (std::getenv("ANQI_VAMANA")) {
@@ -948,6 +1090,11 @@ static int run(int argc, char** argv) {
         gp.precision = env_or("ANQI_B200_PRECISION", "bf16") == "fp32" ? 0u : 1u;
         gp.vamana_passes = vamana_passes;
         gp.vamana_L = vamana_L;
+        // the edge policy of the prunes (the graph folder of the postfilter
+        // placement is the graph cache directory, rknn_query.cpp:1947)
+        EdgePolicyHost edge;
+        resolve_edge_policy(edge, n, (uint32_t)Marg, graph_cache_dir);
+        if (edge.p.flags) gp.edge = &edge.p;
         deg.resize(n);
         links.resize(n * Marg);
         anqi_build_stats gs{};

@@ -99,6 +99,14 @@ struct GatherParams {
     // row number -> original id.  Lists, rows and norms are given in the new
     // numbering; (dist, id) ties and the output use the original ids.
     const uint32_t* perm;
+    // edge-policy prunes: the rows [row_base, row_base + row_count) of the work
+    // list (row_count 0: all), each writing its pool (pool_cap entries apart)
+    // and its size to the dump buffers instead of pruning it
+    uint64_t row_base;
+    uint32_t row_count;
+    float* dump_d;
+    uint32_t* dump_i;
+    uint32_t* dump_n;
     unsigned long long* pool_total;
     uint32_t* err;
 };
@@ -243,11 +251,24 @@ __device__ __forceinline__ uint32_t gather_visit(const GatherParams& p, Visited&
     return cnt0 + __popc(b1);
 }
 
+// A row's pool (np entries) to dump entry t of the chunk, for the policy prune.
+__device__ __forceinline__ void dump_pool(const GatherParams& p, uint32_t t, const float* pd, const uint32_t* pi,
+                                          uint32_t np, uint32_t lane) {
+    float* dd = p.dump_d + (uint64_t)t * p.pool_cap;
+    uint32_t* di = p.dump_i + (uint64_t)t * p.pool_cap;
+    for (uint32_t e = lane; e < np; e += 32) {
+        dd[e] = pd[e];
+        di[e] = pi[e];
+    }
+    if (lane == 0) p.dump_n[t] = np;
+    __syncwarp();
+}
+
 // kIp: the AKNN mode in the ip metric; kVam: the Vamana mode; kRen: the AKNN
 // mode over rows renumbered for locality (p.perm), whose visits near the row
 // go to a per-warp window bitmap (separate instances, so each mode keeps its
 // registers and occupancy)
-template <bool kIp, bool kVam = false, bool kRen = false>
+template <bool kIp, bool kVam = false, bool kRen = false, bool kDump = false>
 __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -285,8 +306,9 @@ __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams 
         uint32_t row = 0;
         if (lane == 0) row = atomicAdd(p.next_row, 1u);
         row = __shfl_sync(kAll, row, 0);
-        if (row >= p.n) break;
-        const uint64_t i = p.row_order ? p.row_order[row] : row;
+        if (row >= (kDump ? (uint64_t)p.row_count : p.n)) break;
+        const uint64_t i = kDump ? (p.row_order ? p.row_order[p.row_base + row] : p.row_base + row)
+                                 : (p.row_order ? p.row_order[row] : row);
         if (i >= p.n) {
             if (lane == 0) set_error(p.err, kDevBadId);
             continue;
@@ -318,6 +340,10 @@ __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams 
             if (np > p.pool_cap) {
                 if (lane == 0) set_error(p.err, kDevPoolOverflow);
                 np = p.pool_cap;
+            }
+            if constexpr (kDump) {
+                dump_pool(p, row, pd, pi, np, lane);
+                continue;
             }
             const float* sd;
             const uint32_t* si;
@@ -505,12 +531,16 @@ __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams 
             // prune_pool_to_ids: sort_unique_candidates + rng_extend (index.h:772-829)
             uint32_t np = (uint32_t)(npool < (uint64_t)p.pool_cap ? npool : (uint64_t)p.pool_cap);
             if (npool > p.pool_cap && lane == 0) set_error(p.err, kDevPoolOverflow);
-            const float* sd;
-            const uint32_t* si;
-            sort_pool(pd, pi, np, sm_d, sm_i, p.pool_cap, &sd, &si);
-            const uint32_t nsel = rng_prune(p, i, sd, si, np, sel, gw, gt);
-            for (uint32_t t = lane; t < p.M; t += 32) p.O[i * p.M + t] = t < nsel ? sel[t] : kEmpty;
-            if (lane == 0) p.O_deg[i] = nsel;
+            if constexpr (kDump) {
+                dump_pool(p, row, pd, pi, np, lane);
+            } else {
+                const float* sd;
+                const uint32_t* si;
+                sort_pool(pd, pi, np, sm_d, sm_i, p.pool_cap, &sd, &si);
+                const uint32_t nsel = rng_prune(p, i, sd, si, np, sel, gw, gt);
+                for (uint32_t t = lane; t < p.M; t += 32) p.O[i * p.M + t] = t < nsel ? sel[t] : kEmpty;
+                if (lane == 0) p.O_deg[i] = nsel;
+            }
         }
         __syncwarp();
         vis_release(vis, vs, nlog, lane);
@@ -1232,9 +1262,12 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     const size_t per_warp = gather_smem_words(p.ef, topk_cap, p.sort_words, hash_cap, ren ? kWinWords : 0) * 4;
     const size_t smem = per_warp * warps_per_block;
     if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "explore range %u too large", p.ef);
-    auto* kern = p.mode == kModeVamana ? gather_kernel<false, true>
+    const bool policy = c->edge.active && (p.mode == kModeSelect || p.mode == kModeCommit || p.mode == kModeVamana);
+    if (policy && p.ip) return fail(c, ANQI_ERR_ARGS, "edge policies are an l2 graph option");
+    auto* kern = p.mode == kModeVamana ? (policy ? gather_kernel<false, true, false, true> : gather_kernel<false, true>)
                  : p.ip                  ? gather_kernel<true>
                  : ren                   ? gather_kernel<false, false, true>
+                 : policy                ? gather_kernel<false, false, false, true>
                                          : gather_kernel<false>;
     ANQI_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -1280,8 +1313,33 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
         c->l2_window = false;
     }
     ANQI_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-    kern<<<blocks, 32 * warps_per_block, smem, c->stream>>>(p);
-    ANQI_CUDA(c, cudaGetLastError());
+    if (!policy) {
+        kern<<<blocks, 32 * warps_per_block, smem, c->stream>>>(p);
+        ANQI_CUDA(c, cudaGetLastError());
+    } else {
+        // pools dumped a chunk of rows at a time (about 1 GB), each chunk
+        // pruned under the edge policy into O (select, Vamana) or the links (commit)
+        uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(p.n, (1ull << 30) / (pool_cap * 8ull)));
+        if (const char* e = std::getenv("ANQI_B200_POLICY_CHUNK_ROWS")) chunk = std::max<uint64_t>(1, std::strtoull(e, nullptr, 10));
+        if ((rc = ensure(c, c->pol_dump_d, chunk * pool_cap * 4)) || (rc = ensure(c, c->pol_dump_i, chunk * pool_cap * 4)) ||
+            (rc = ensure(c, c->pol_dump_n, chunk * 4)))
+            return rc;
+        p.dump_d = c->pol_dump_d.as<float>();
+        p.dump_i = c->pol_dump_i.as<uint32_t>();
+        p.dump_n = c->pol_dump_n.as<uint32_t>();
+        uint32_t* out = p.mode == kModeCommit ? p.links : p.O;
+        uint32_t* out_deg = p.mode == kModeCommit ? p.deg : p.O_deg;
+        for (uint64_t r0 = 0; r0 < p.n; r0 += chunk) {
+            p.row_base = r0;
+            p.row_count = (uint32_t)std::min<uint64_t>(chunk, p.n - r0);
+            ANQI_CUDA(c, cudaMemsetAsync(p.next_row, 0, 4, c->stream));
+            kern<<<blocks, 32 * warps_per_block, smem, c->stream>>>(p);
+            ANQI_CUDA(c, cudaGetLastError());
+            if ((rc = run_policy_prune(c, p.x, p.norms, p.n, p.stride, p.dim, p.M, p.alpha, p.dump_d, p.dump_i,
+                                       p.dump_n, pool_cap, p.row_order, r0, p.row_count, out, out_deg)))
+                return rc;
+        }
+    }
     ANQI_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     rc = check_device_error(c, "gather");  // synchronizes
     if (gcap) clear_l2_window(c);
@@ -1587,15 +1645,29 @@ int anqi_graph_localjoin_precision(anqi_ctx* h, const float* x, uint64_t n, uint
     return sync(c);
 }
 
+// Clears the context's edge policy when the entry point that set it returns.
+struct PolicyScope {
+    Ctx* c;
+    ~PolicyScope() { clear_edge_policy(c); }
+};
+
 int anqi_graph_select(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids,
                       const float* g_vals, uint32_t K, uint32_t M, uint32_t ef, uint32_t cap, float alpha, uint32_t* O,
                       uint32_t* O_deg) {
+    return anqi_graph_select_policy(h, x, n, dim, g_ids, g_vals, K, M, ef, cap, alpha, nullptr, O, O_deg);
+}
+
+int anqi_graph_select_policy(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids,
+                             const float* g_vals, uint32_t K, uint32_t M, uint32_t ef, uint32_t cap, float alpha,
+                             const anqi_edge_policy* edge, uint32_t* O, uint32_t* O_deg) {
     if (!h || !x || !g_ids || !g_vals || !O || !O_deg || n == 0 || M == 0 || M > 64 || ef == 0) return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     const uint32_t xs = round_up(dim, 8);
     TmpBuf dx(c), dn(c), hid(c), hv(c), dO(c), dOd(c);
+    PolicyScope scope{c};
     int rc;
+    if ((rc = set_edge_policy(c, edge, n))) return rc;
     if ((rc = upload_rows(c, dx, dn, x, n, dim, xs)) || (rc = h2d(c, hid, g_ids, n * K * 4)) ||
         (rc = h2d(c, hv, g_vals, n * K * 4)) ||
         (rc = run_select_commit(c, dx, dn, n, xs, dim, hid, hv, K, M, ef, cap, alpha, dO, dOd, nullptr, nullptr,
@@ -1607,12 +1679,20 @@ int anqi_graph_select(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, con
 
 int anqi_graph_commit(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* O, const uint32_t* O_deg,
                       uint32_t M, float alpha, uint32_t* links, uint32_t* deg) {
+    return anqi_graph_commit_policy(h, x, n, dim, O, O_deg, M, alpha, nullptr, links, deg);
+}
+
+int anqi_graph_commit_policy(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* O,
+                             const uint32_t* O_deg, uint32_t M, float alpha, const anqi_edge_policy* edge,
+                             uint32_t* links, uint32_t* deg) {
     if (!h || !x || !O || !O_deg || !links || !deg || n == 0 || M == 0 || M > 64) return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     const uint32_t xs = round_up(dim, 8);
     TmpBuf dx(c), dn(c), dO(c), dOd(c), roff(c), rev(c), dl(c), dd(c);
+    PolicyScope scope{c};
     int rc;
+    if ((rc = set_edge_policy(c, edge, n))) return rc;
     if ((rc = upload_rows(c, dx, dn, x, n, dim, xs)) || (rc = h2d(c, dO, O, n * M * 4)) ||
         (rc = h2d(c, dOd, O_deg, n * 4)) || (rc = build_reverse(c, dO.as<uint32_t>(), n, M, roff, rev)) ||
         (rc = ensure(c, dl, n * M * 4)) || (rc = ensure(c, dd, n * 4)))
@@ -1668,6 +1748,11 @@ static void graph_build_reset(Ctx* c) {
     g.seen.shrink_to_fit();
     g.active = false;
     g.rows_done = 0;
+    g.has_edge = false;
+    g.edge_resid.clear();
+    g.edge_resid.shrink_to_fit();
+    g.edge_mu.clear();
+    g.edge_mu.shrink_to_fit();
 }
 
 int anqi_graph_build_begin(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const anqi_graph_params* gp) {
@@ -1682,6 +1767,20 @@ int anqi_graph_build_begin(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim
     g.dim = dim;
     g.xs = round_up(dim, 8);
     g.gp = *gp;
+    g.gp.edge = nullptr;
+    g.has_edge = gp->edge && gp->edge->flags != 0;
+    if (g.has_edge) {
+        // the policy and its tables, kept for the prunes of _finish
+        const anqi_edge_policy& e = *gp->edge;
+        if (e.nks > 8 || ((e.flags & (ANQI_EDGE_COVER | ANQI_EDGE_BALL | ANQI_EDGE_AUTO)) && (!e.resid || !e.nk)) ||
+            ((e.flags & ANQI_EDGE_LSG) && !e.mu))
+            return fail(c, ANQI_ERR_ARGS, "invalid edge policy");
+        g.edge = e;
+        g.edge_resid.assign(e.resid ? e.resid : nullptr, e.resid ? e.resid + n * (uint64_t)e.nk : nullptr);
+        g.edge_mu.assign(e.mu ? e.mu : nullptr, e.mu ? e.mu + n : nullptr);
+        g.edge.resid = g.edge_resid.empty() ? nullptr : g.edge_resid.data();
+        g.edge.mu = g.edge_mu.empty() ? nullptr : g.edge_mu.data();
+    }
     int rc;
     if ((rc = upload_rows(c, g.dx, g.dn, x, n, dim, g.xs))) return rc;
     // entry tree: make_forest with one tree (index.h:1111-1120)
@@ -1778,6 +1877,8 @@ int anqi_graph_build_finish(anqi_ctx* h, uint32_t* deg, uint32_t* links, anqi_bu
     double gather_kernel_ms = 0;
     const uint32_t cap = std::max<uint32_t>(gp.degree, gp.ef_alpha * gp.explore);
     const char* ord_env = std::getenv("ANQI_B200_ORDER");
+    PolicyScope scope{c};
+    if (!rc && g.has_edge) rc = set_edge_policy(c, &g.edge, n);
     if (!rc)
         rc = run_select_commit(c, g.dx, g.dn, n, g.xs, g.dim, g.hid, g.hv, gp.nn_k, gp.degree, gp.explore, cap,
                                gp.alpha, dO, dOd, &dl, &dd, &pool_total,

@@ -92,6 +92,25 @@ struct GraphBuild {
     DevBuf dx, dn, hid, hv, order;
     std::vector<uint8_t> seen;  // rows delivered
     double forest_ms = 0, warm_ms = 0;
+    // the edge policy of anqi_graph_params.edge, copied at begin
+    bool has_edge = false;
+    anqi_edge_policy edge{};
+    std::vector<float> edge_resid, edge_mu;
+};
+
+// The edge policy of the current graph build (anqi_edge_policy on the
+// device): the prune of select, commit and Vamana passes runs in
+// policy_prune_kernel while active.
+struct DevPolicyView {
+    uint32_t flags, nks, ks[8], nk, budget, occ_all, auto_cand, auto_swaps;
+    double lambda, scale2, lsg_alpha;
+    const float* resid;
+    const float* mu;
+};
+struct DevPolicy {
+    bool active = false;
+    DevPolicyView view{};
+    DevBuf resid, mu;
 };
 
 struct Ctx {
@@ -129,6 +148,8 @@ struct Ctx {
     DevBuf init_cnt, init_cid, init_key;  // tensor-core init_knn candidate buffers
     GraphBuild gb;                        // staged G48 build
     DevBuf g_bits, g_vlog, g_pd, g_pi, g_gtab;  // gather kernel per-slot scratch
+    DevPolicy edge;                              // edge policy of the build in progress
+    DevBuf pol_scratch, pol_dump_d, pol_dump_i, pol_dump_n;  // policy prune scratch and pool dumps
     // pinned staging slots for large copies to and from pageable host memory
     static constexpr int kStageSlots = 3;
     void* stage[kStageSlots] = {};
@@ -144,6 +165,7 @@ struct Ctx {
                 &batch.leaf_cnt, &batch.qr2, &err, &counters, &vis_bits, &vis_log,
                 &cand_scratch, &thr_table, &gt_off, &gt_ids, &eval_rows, &eval_sums, &vis_gtab,
                 &init_cnt, &init_cid, &init_key, &g_bits, &g_vlog, &g_pd, &g_pi, &g_gtab, &gb.dx, &gb.dn,
+                &edge.resid, &edge.mu, &pol_scratch, &pol_dump_d, &pol_dump_i, &pol_dump_n,
                 &gb.hid, &gb.hv, &gb.order};
     }
     // Per-object thresholds for up to kThrSlots values of k: slot s holds
@@ -256,6 +278,18 @@ int tc_leaf_filter(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_no
                    uint32_t d, const uint32_t* d_members, const LeafTile* d_tiles, size_t ntiles,
                    const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
                    uint32_t* out_id, float* out_key, uint64_t pos_base);
+
+// Edge policy of the next select / commit / Vamana prunes (nullptr or flags 0:
+// the default prune; tables copied to the device), and its release.
+int set_edge_policy(Ctx* c, const anqi_edge_policy* pol, uint64_t n);
+void clear_edge_policy(Ctx* c);
+// Prunes the pools of nrows rows (row of entry t: rows[row_base + t], or
+// row_base + t; pool t at pool_d / pool_i [t * pool_cap], pool_n[t] entries)
+// under the active edge policy into out (n x M) / out_deg.
+int run_policy_prune(Ctx* c, const float* x, const float* norms, uint64_t n, uint32_t stride, uint32_t dim, uint32_t M,
+                     float alpha, const float* pool_d, const uint32_t* pool_i, const uint32_t* pool_n,
+                     uint32_t pool_cap, const uint32_t* rows, uint64_t row_base, uint32_t nrows, uint32_t* out,
+                     uint32_t* out_deg);
 
 // L2 persisting window over [p, p + bytes) for kernels on the context's stream.
 void set_l2_window(Ctx* c, const void* p, size_t bytes);

@@ -192,6 +192,40 @@ int anqi_aknn_gather_metric(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t 
                             const float* g_vals, uint32_t K, uint32_t ef, uint32_t cap, uint32_t out_k,
                             uint32_t metric, uint32_t* ids, float* dists);
 
+/* ----------------------------------------------------------- edge policies
+ * The prune of the G48 build under ANQI_EDGE_POLICY (prune_pool_to_ids,
+ * include/index.h:772-829, as configure_edge_residual_cover leaves it,
+ * :305-440), resolved to flags:
+ *   ANQI_EDGE_COVER      residual_cover: RNG to M - budget, residual-cover edges, RNG to M
+ *   ANQI_EDGE_BALL       ball occlusion over the pool ordered by d - lambda max_k radj
+ *   ANQI_EDGE_PURE       with BALL: ball RNG first (ball_rng, bubble_rng), else RNG to M - budget first
+ *   ANQI_EDGE_LSG        the LSG metric d2 / (mu_a mu_b)^lsg_alpha (lsg_rng; with BALL lsg_bubble_hybrid)
+ *   ANQI_EDGE_AUTO       RNG, then the verification-constrained bubble optimizer (bubble_auto)
+ *   ANQI_EDGE_AUTO_FULL  with AUTO: every pool entry an alternative and a target (bubble_auto_full)
+ * radj(id, k) = scale2 * resid[id * nk + k - 1]; flags 0 is the default prune.
+ * The tables are host arrays, copied for the build. */
+#define ANQI_EDGE_COVER 1u
+#define ANQI_EDGE_BALL 2u
+#define ANQI_EDGE_PURE 4u
+#define ANQI_EDGE_LSG 8u
+#define ANQI_EDGE_AUTO 16u
+#define ANQI_EDGE_AUTO_FULL 32u
+typedef struct {
+    uint32_t flags;
+    uint32_t nks;              /* ANQI_EDGE_KS values kept (1 <= k <= nk), at most 8 */
+    uint32_t ks[8];
+    uint32_t nk;               /* ANQI_EDGE_NK: the residual table's stride (100) */
+    uint32_t budget;           /* min(ANQI_EDGE_RESID_BUDGET, M) (16) */
+    uint32_t occlude_all;      /* ANQI_EDGE_BALL_OCCLUSION != "any" */
+    uint32_t auto_candidates;  /* ANQI_EDGE_AUTO_CANDIDATES (M) */
+    uint32_t auto_max_swaps;   /* ANQI_EDGE_AUTO_MAX_SWAPS (M) */
+    double lambda;             /* ANQI_EDGE_RESID_LAMBDA (1) */
+    double scale2;             /* the lift scale squared from <graph folder>_anqi_meta.txt, else 1 */
+    double lsg_alpha;          /* ANQI_LSG_ALPHA (1) */
+    const float* resid;        /* n x nk (COVER, BALL, AUTO) */
+    const float* mu;           /* n, positive (LSG) */
+} anqi_edge_policy;
+
 /* ----------------------------------------------------------- G48 graph
  * nndindex::build_index with a flat warm start (include/index.h:1071-1295):
  * entry RP tree (1 tree, leaf p->leaf) -> warm-start heaps (cap nn_k) from the
@@ -219,6 +253,7 @@ typedef struct {
     uint32_t vamana_passes;  /* ANQI_VAMANA (ANQI_VAMANA_PASS, 2): global Vamana refine passes after
                                 the commit (include/index.h:1262-1285); 0 = none */
     uint32_t vamana_L;       /* ANQI_VAMANA_L: the refine's beam width (128; 0 = 128) */
+    const anqi_edge_policy* edge;  /* the prune's edge policy (select, commit, Vamana); NULL = default */
 } anqi_graph_params;
 
 int anqi_graph_build(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* warm_ids,
@@ -257,6 +292,13 @@ int anqi_graph_select(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, c
                       uint32_t* O, uint32_t* O_deg);
 int anqi_graph_commit(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* O,
                       const uint32_t* O_deg, uint32_t M, float alpha, uint32_t* links, uint32_t* deg);
+/* The select and commit stages under an edge policy (NULL: as above). */
+int anqi_graph_select_policy(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* g_ids,
+                             const float* g_vals, uint32_t K, uint32_t M, uint32_t ef, uint32_t cap, float alpha,
+                             const anqi_edge_policy* edge, uint32_t* O, uint32_t* O_deg);
+int anqi_graph_commit_policy(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* O,
+                             const uint32_t* O_deg, uint32_t M, float alpha, const anqi_edge_policy* edge,
+                             uint32_t* links, uint32_t* deg);
 /* One pass of the global Vamana refine (include/index.h:856-875,
  * 1262-1285), select half: for every row i, a beam of width Lb over the graph
  * (links n x M, deg) from entry[i] collects every visited node, the row's g0

@@ -12,6 +12,7 @@
 #include "anqi_oracle.h"
 
 #include <float.h>
+#include <limits.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -584,9 +585,342 @@ void ao_aknn_rows(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t K,
 
 /* sort_unique_candidates (index.h:225-248) + rng_extend (index.h:267-281) as
  * prune_pool_to_ids runs them with the default edge policy (index.h:823-828). */
-uint32_t ao_prune(const float* x, const float* norms, uint32_t dim, uint64_t n, uint64_t i,
-                  float* pool_d, uint32_t* pool_id, uint64_t pool_n, uint32_t M, float alpha,
-                  uint32_t* out) {
+/* ---- edge policies, include/index.h:283-829 ----
+ * One prune's state: the pool sorted by (dist, id) without duplicates or the
+ * base (sort_unique_candidates, :225-247), and the selected ids. */
+typedef struct {
+    const float* x;
+    const float* norms;
+    uint32_t dim;
+    uint64_t base;
+    float alpha;
+    uint32_t M;
+    const ao_edge_policy* pol;
+    const pair_t* cand;
+    uint64_t nc;
+    uint32_t* ids;
+    uint32_t nids;
+} ao_prune_state;
+
+typedef struct {
+    double key;
+    uint32_t id;
+} dpair_t;
+
+static int cmp_dkey_id(const void* a, const void* b) {
+    const dpair_t* x = (const dpair_t*)a;
+    const dpair_t* y = (const dpair_t*)b;
+    if (x->key < y->key) return -1;
+    if (x->key > y->key) return 1;
+    return (x->id > y->id) - (x->id < y->id);
+}
+
+static float ps_d2(const ao_prune_state* st, uint32_t a, uint32_t b) {
+    return ao_d2(st->x + (uint64_t)a * st->dim, st->x + (uint64_t)b * st->dim, st->norms[a], st->norms[b], st->dim);
+}
+
+static int ps_has(const ao_prune_state* st, uint32_t id) {
+    for (uint32_t s = 0; s < st->nids; s++)
+        if (st->ids[s] == id) return 1;
+    return 0;
+}
+
+/* edge_radj, :292-294 */
+static double ps_radj(const ao_prune_state* st, uint32_t id, uint32_t k) {
+    return st->pol->scale2 * (double)st->pol->resid[(uint64_t)id * st->pol->nk + (k - 1)];
+}
+
+/* edge_sort_radj, :296-303 */
+static double ps_sort_radj(const ao_prune_state* st, uint32_t id) {
+    const ao_edge_policy* p = st->pol;
+    if (!p || !(p->flags & AO_EDGE_BALL) || p->nks == 0) return 0.0;
+    double best = -INFINITY;
+    for (uint32_t t = 0; t < p->nks; t++) {
+        const double r = ps_radj(st, id, p->ks[t]);
+        best = best > r ? best : r;
+    }
+    return isfinite(best) ? best : 0.0;
+}
+
+/* rng_extend, :264-278 */
+static void ps_rng_extend(ao_prune_state* st, uint32_t cap) {
+    for (uint64_t q = 0; q < st->nc; q++) {
+        if (st->nids >= cap) break;
+        const uint32_t cid = st->cand[q].id;
+        if (ps_has(st, cid)) continue;
+        int occluded = 0;
+        for (uint32_t s = 0; s < st->nids && !occluded; s++)
+            if (st->alpha * ps_d2(st, st->ids[s], cid) < st->cand[q].d) occluded = 1;
+        if (!occluded) st->ids[st->nids++] = cid;
+    }
+}
+
+/* ball_occludes_distance, :478-495 */
+static int ps_ball_occludes(const ao_prune_state* st, uint32_t sid, float dbase_cid, float dsc) {
+    const ao_edge_policy* p = st->pol;
+    if (!(p->flags & AO_EDGE_BALL) || p->nks == 0) return 0;
+    int any = 0, all = 1;
+    for (uint32_t t = 0; t < p->nks; t++) {
+        const uint32_t k = p->ks[t];
+        const double lhs = (double)st->alpha * (double)dsc - p->lambda * ps_radj(st, sid, k);
+        const double rhs = (double)dbase_cid - p->lambda * ps_radj(st, (uint32_t)st->base, k);
+        const int occ = lhs < rhs;
+        any = any || occ;
+        all = all && occ;
+        if (!p->occlude_all && any) return 1;
+        if (p->occlude_all && !all) return 0;
+    }
+    return p->occlude_all ? all : any;
+}
+
+/* ball_sort_candidates, :501-510: the pool by (dist - lambda * sort_radj, id) */
+static dpair_t* ps_ball_order(const ao_prune_state* st) {
+    dpair_t* o = (dpair_t*)malloc(sizeof(dpair_t) * (st->nc + 1));
+    for (uint64_t q = 0; q < st->nc; q++) {
+        o[q].id = st->cand[q].id;
+        o[q].key = (st->pol->flags & AO_EDGE_BALL)
+                       ? (double)st->cand[q].d - st->pol->lambda * ps_sort_radj(st, st->cand[q].id)
+                       : (double)st->cand[q].d;
+    }
+    if (st->pol->flags & AO_EDGE_BALL) qsort(o, (size_t)st->nc, sizeof(dpair_t), cmp_dkey_id);
+    return o;
+}
+
+static float ps_cand_d(const ao_prune_state* st, uint32_t id) {
+    for (uint64_t q = 0; q < st->nc; q++)
+        if (st->cand[q].id == id) return st->cand[q].d;
+    return 0.0f;
+}
+
+/* rng_extend_ball, :512-527 (the occlusion compares the raw distance of the
+ * candidate, its pool entry, whatever the order) */
+static void ps_rng_extend_ball(ao_prune_state* st, const dpair_t* order, uint32_t cap) {
+    for (uint64_t q = 0; q < st->nc; q++) {
+        if (st->nids >= cap) break;
+        const uint32_t cid = order[q].id;
+        if (ps_has(st, cid)) continue;
+        const float d2c = ps_cand_d(st, cid);
+        int occluded = 0;
+        for (uint32_t s = 0; s < st->nids && !occluded; s++)
+            if (ps_ball_occludes(st, st->ids[s], d2c, ps_d2(st, st->ids[s], cid))) occluded = 1;
+        if (!occluded) st->ids[st->nids++] = cid;
+    }
+}
+
+/* lsg_distance2, :719-725 */
+static double ps_lsg_d2(const ao_prune_state* st, uint32_t a, uint32_t b, double raw) {
+    const ao_edge_policy* p = st->pol;
+    if (!(p->flags & AO_EDGE_LSG) || p->lsg_alpha == 0.0) return raw;
+    const double mu_product = (double)p->mu[a] * (double)p->mu[b];
+    const double denom = pow(mu_product, p->lsg_alpha);
+    if (!isfinite(denom) || denom <= 0.0) return raw;
+    return raw / denom;
+}
+
+/* lsg_sort_candidates, :727-737 */
+static dpair_t* ps_lsg_order(const ao_prune_state* st) {
+    dpair_t* o = (dpair_t*)malloc(sizeof(dpair_t) * (st->nc + 1));
+    for (uint64_t q = 0; q < st->nc; q++) {
+        o[q].id = st->cand[q].id;
+        o[q].key = ps_lsg_d2(st, (uint32_t)st->base, st->cand[q].id, (double)st->cand[q].d);
+    }
+    qsort(o, (size_t)st->nc, sizeof(dpair_t), cmp_dkey_id);
+    return o;
+}
+
+/* rng_extend_lsg, :739-754 */
+static void ps_rng_extend_lsg(ao_prune_state* st, const dpair_t* order, uint32_t cap) {
+    for (uint64_t q = 0; q < st->nc; q++) {
+        if (st->nids >= cap) break;
+        const uint32_t cid = order[q].id;
+        if (ps_has(st, cid)) continue;
+        int occluded = 0;
+        for (uint32_t s = 0; s < st->nids && !occluded; s++) {
+            const double dsc = ps_lsg_d2(st, st->ids[s], cid, (double)ps_d2(st, st->ids[s], cid));
+            if ((double)st->alpha * dsc < order[q].key) occluded = 1;
+        }
+        if (!occluded) st->ids[st->nids++] = cid;
+    }
+}
+
+/* add_residual_cover_edges, :441-476 */
+static void ps_residual_cover(ao_prune_state* st) {
+    const ao_edge_policy* p = st->pol;
+    if (!(p->flags & AO_EDGE_COVER) || st->nids >= st->M) return;
+    uint32_t total = p->budget < st->M - st->nids ? p->budget : st->M - st->nids;
+    if (total == 0 || p->nks == 0) return;
+    uint32_t per_k = (total + p->nks - 1) / p->nks;
+    if (per_k < 1) per_k = 1;
+    uint32_t added_total = 0;
+    dpair_t* scored = (dpair_t*)malloc(sizeof(dpair_t) * (st->nc + 1));
+    for (uint32_t t = 0; t < p->nks; t++) {
+        if (added_total >= total || st->nids >= st->M) break;
+        const uint32_t k = p->ks[t];
+        uint64_t m = 0;
+        for (uint64_t q = 0; q < st->nc; q++) {
+            const uint32_t cid = st->cand[q].id;
+            if (cid == (uint32_t)st->base || ps_has(st, cid)) continue;
+            const double residual = (double)p->resid[(uint64_t)cid * p->nk + (k - 1)];
+            const double risk = residual > 0.0 ? residual : 0.0;
+            if (risk <= 0.0) continue;
+            scored[m].key = (double)st->cand[q].d - p->lambda * p->scale2 * risk;
+            scored[m].id = cid;
+            m++;
+        }
+        qsort(scored, (size_t)m, sizeof(dpair_t), cmp_dkey_id);
+        uint32_t added_k = 0;
+        for (uint64_t q = 0; q < m; q++) {
+            if (st->nids >= st->M || added_total >= total || added_k >= per_k) break;
+            if (ps_has(st, scored[q].id)) continue;
+            st->ids[st->nids++] = scored[q].id;
+            added_k++;
+            added_total++;
+        }
+    }
+    free(scored);
+}
+
+/* optimize_verification_constrained_bubble, :531-717 */
+static void ps_bubble(ao_prune_state* st) {
+    const ao_edge_policy* p = st->pol;
+    if (!(p->flags & AO_EDGE_AUTO) || st->nids == 0 || st->nc == 0) return;
+    dpair_t* order = ps_ball_order(st);
+    const uint64_t ucap = st->nids + st->nc;
+    uint32_t* universe = (uint32_t*)malloc(sizeof(uint32_t) * ucap);
+    uint64_t nu = 0;
+    for (uint32_t s = 0; s < st->nids; s++) universe[nu++] = st->ids[s];
+    const uint64_t limit = (p->flags & AO_EDGE_AUTO_FULL) ? st->nc : p->auto_candidates;
+    uint64_t alternatives = 0;
+    for (uint64_t q = 0; q < st->nc; q++) {
+        int dup = 0;
+        for (uint64_t u = 0; u < nu && !dup; u++) dup = universe[u] == order[q].id;
+        if (dup) continue;
+        universe[nu++] = order[q].id;
+        if (++alternatives >= limit) break;
+    }
+    free(order);
+    if (alternatives == 0) {
+        free(universe);
+        return;
+    }
+    pair_t* targets = (pair_t*)malloc(sizeof(pair_t) * (st->nc + 1));
+    uint64_t T = 0;
+    if (p->flags & AO_EDGE_AUTO_FULL) {
+        for (uint64_t q = 0; q < st->nc; q++) targets[T++] = st->cand[q];
+    } else {
+        for (uint64_t u = 0; u < nu; u++)
+            for (uint64_t q = 0; q < st->nc; q++)
+                if (st->cand[q].id == universe[u]) {
+                    targets[T++] = st->cand[q];
+                    break;
+                }
+        qsort(targets, (size_t)T, sizeof(pair_t), cmp_dist_id);
+    }
+    const uint64_t words = (T + 63) / 64;
+    uint64_t* verify = (uint64_t*)calloc(nu * words + 1, sizeof(uint64_t));
+    uint64_t* route = (uint64_t*)calloc(nu * words + 1, sizeof(uint64_t));
+    double* power = (double*)malloc(sizeof(double) * (nu + 1));
+    for (uint64_t u = 0; u < nu; u++) {
+        const uint32_t id = universe[u];
+        const float dbase_u = ps_cand_d(st, id);
+        power[u] = (double)dbase_u - p->lambda * ps_sort_radj(st, id);
+        for (uint64_t ti = 0; ti < T; ti++) {
+            const uint32_t target = targets[ti].id;
+            float dsc = 0.0f;
+            if (id != target) dsc = ps_d2(st, id, target);
+            const uint64_t bit = 1ull << (ti & 63u);
+            if (id == target || st->alpha * dsc < targets[ti].d) verify[u * words + (ti >> 6)] |= bit;
+            if (ps_ball_occludes(st, id, targets[ti].d, dsc)) route[u * words + (ti >> 6)] |= bit;
+        }
+    }
+    uint64_t* selected = (uint64_t*)malloc(sizeof(uint64_t) * (st->nids + 1));
+    uint8_t* is_sel = (uint8_t*)calloc(nu + 1, 1);
+    uint64_t nsel = 0;
+    for (uint32_t s = 0; s < st->nids; s++)
+        for (uint64_t u = 0; u < nu; u++)
+            if (universe[u] == st->ids[s]) {
+                selected[nsel++] = u;
+                is_sel[u] = 1;
+                break;
+            }
+    if (nsel > 0) {
+        int32_t* vcount = (int32_t*)calloc(T + 1, sizeof(int32_t));
+        int32_t* rcount = (int32_t*)calloc(T + 1, sizeof(int32_t));
+        uint8_t* required = (uint8_t*)calloc(T + 1, 1);
+#define AO_SIG(u, delta)                                                         \
+    for (uint64_t ti = 0; ti < T; ti++) {                                        \
+        const uint64_t bit = 1ull << (ti & 63u);                                 \
+        if (verify[(u) * words + (ti >> 6)] & bit) vcount[ti] += (delta);        \
+        if (route[(u) * words + (ti >> 6)] & bit) rcount[ti] += (delta);         \
+    }
+        for (uint64_t s = 0; s < nsel; s++) AO_SIG(selected[s], 1);
+        for (uint64_t ti = 0; ti < T; ti++) required[ti] = vcount[ti] > 0;
+        uint64_t swaps = 0;
+        const uint64_t max_swaps = p->auto_max_swaps < alternatives ? p->auto_max_swaps : alternatives;
+        while (swaps < max_swaps) {
+            long best_gain = LONG_MIN;
+            double best_power = -INFINITY;
+            uint64_t best_q = UINT64_MAX, best_slot = UINT64_MAX;
+            for (uint64_t q = 0; q < nu; q++) {
+                if (is_sel[q]) continue;
+                long newly = 0;
+                for (uint64_t ti = 0; ti < T; ti++)
+                    if (rcount[ti] == 0 && (route[q * words + (ti >> 6)] >> (ti & 63u) & 1u)) newly++;
+                for (uint64_t slot = 0; slot < nsel; slot++) {
+                    const uint64_t old = selected[slot];
+                    int feasible = 1;
+                    long lost = 0;
+                    for (uint64_t ti = 0; ti < T; ti++) {
+                        const int ov = (verify[old * words + (ti >> 6)] >> (ti & 63u)) & 1u;
+                        const int qv = (verify[q * words + (ti >> 6)] >> (ti & 63u)) & 1u;
+                        if (required[ti] && ov && vcount[ti] == 1 && !qv) {
+                            feasible = 0;
+                            break;
+                        }
+                        const int orr = (route[old * words + (ti >> 6)] >> (ti & 63u)) & 1u;
+                        const int qr = (route[q * words + (ti >> 6)] >> (ti & 63u)) & 1u;
+                        if (orr && rcount[ti] == 1 && !qr) lost++;
+                    }
+                    if (!feasible) continue;
+                    const long gain = newly - lost;
+                    const double pg = power[old] - power[q];
+                    if (gain > best_gain || (gain == best_gain && pg > best_power)) {
+                        best_gain = gain;
+                        best_power = pg;
+                        best_q = q;
+                        best_slot = slot;
+                    }
+                }
+            }
+            if (best_q == UINT64_MAX || best_gain < 0 || (best_gain == 0 && best_power <= 1e-12)) break;
+            const uint64_t old = selected[best_slot];
+            AO_SIG(old, -1);
+            AO_SIG(best_q, 1);
+            is_sel[old] = 0;
+            is_sel[best_q] = 1;
+            selected[best_slot] = best_q;
+            swaps++;
+        }
+#undef AO_SIG
+        for (uint64_t s = 0; s < nsel; s++) st->ids[s] = universe[selected[s]];
+        free(vcount);
+        free(rcount);
+        free(required);
+    }
+    free(selected);
+    free(is_sel);
+    free(verify);
+    free(route);
+    free(power);
+    free(targets);
+    free(universe);
+}
+
+/* prune_pool_to_ids, :772-829 */
+uint32_t ao_prune_policy(const float* x, const float* norms, uint32_t dim, uint64_t n, uint64_t i,
+                         const float* pool_d, const uint32_t* pool_id, uint64_t pool_n, uint32_t M, float alpha,
+                         const ao_edge_policy* pol, uint32_t* out) {
+    /* sort_unique_candidates, :225-247 */
     pair_t* c = (pair_t*)malloc(sizeof(pair_t) * (pool_n + 1));
     uint64_t m = 0;
     for (uint64_t p = 0; p < pool_n; p++) {
@@ -612,27 +946,60 @@ uint32_t ao_prune(const float* x, const float* norms, uint32_t dim, uint64_t n, 
         r = e;
     }
     qsort(c, (size_t)w, sizeof(pair_t), cmp_dist_id);
-    uint32_t sel = 0;
-    for (uint64_t p = 0; p < w; p++) {
-        if (sel >= M) break;
-        uint32_t cid = c[p].id;
-        int occluded = 0;
-        for (uint32_t s = 0; s < sel; s++) {
-            float dsc = ao_d2(x + (uint64_t)out[s] * dim, x + (uint64_t)cid * dim, norms[out[s]], norms[cid], dim);
-            if (alpha * dsc < c[p].d) {
-                occluded = 1;
-                break;
-            }
+    /* the selection may hold up to M ids and, transiently, no more */
+    ao_prune_state st = {x, norms, dim, i, alpha, M, pol, c, w, out, 0};
+    const uint32_t f = pol ? pol->flags : 0u;
+    if (f & AO_EDGE_AUTO) {
+        ps_rng_extend(&st, M);
+        ps_bubble(&st);
+    } else if ((f & AO_EDGE_LSG) && (f & AO_EDGE_BALL) && pol->lsg_alpha != 0.0) {
+        dpair_t* lo = ps_lsg_order(&st);
+        uint32_t lsg_cap = M - (pol->budget < M ? pol->budget : M);
+        if (lsg_cap == 0) lsg_cap = M;
+        ps_rng_extend_lsg(&st, lo, lsg_cap);
+        dpair_t* bo = ps_ball_order(&st);
+        ps_rng_extend_ball(&st, bo, M);
+        ps_rng_extend_lsg(&st, lo, M);
+        free(lo);
+        free(bo);
+    } else if ((f & AO_EDGE_LSG) && pol->lsg_alpha != 0.0) {
+        dpair_t* lo = ps_lsg_order(&st);
+        ps_rng_extend_lsg(&st, lo, M);
+        free(lo);
+    } else if (f & AO_EDGE_BALL) {
+        dpair_t* bo = ps_ball_order(&st);
+        if (f & AO_EDGE_PURE) {
+            ps_rng_extend_ball(&st, bo, M);
+            ps_rng_extend(&st, M);
+        } else {
+            uint32_t center_cap = M - (pol->budget < M ? pol->budget : M);
+            if (center_cap == 0) center_cap = M;
+            ps_rng_extend(&st, center_cap);
+            ps_rng_extend_ball(&st, bo, M);
+            ps_rng_extend(&st, M);
         }
-        if (!occluded) out[sel++] = cid;
+        free(bo);
+    } else {
+        const uint32_t cover = (f & AO_EDGE_COVER) ? (pol->budget < M ? pol->budget : M) : 0u;
+        uint32_t normal_cap = M - cover;
+        if (normal_cap == 0) normal_cap = M;
+        ps_rng_extend(&st, normal_cap);
+        if (f & AO_EDGE_COVER) ps_residual_cover(&st);
+        ps_rng_extend(&st, M);
     }
     free(c);
-    return sel;
+    return st.nids;
+}
+
+uint32_t ao_prune(const float* x, const float* norms, uint32_t dim, uint64_t n, uint64_t i,
+                  float* pool_d, uint32_t* pool_id, uint64_t pool_n, uint32_t M, float alpha,
+                  uint32_t* out) {
+    return ao_prune_policy(x, norms, dim, n, i, pool_d, pool_id, pool_n, M, alpha, NULL, out);
 }
 
 /* build_index gather + prune loop, index.h:1248-1257 */
-void ao_graph_select(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t M, float alpha,
-                     uint32_t* O, uint32_t* O_deg) {
+void ao_graph_select_policy(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t M, float alpha,
+                            const ao_edge_policy* pol, uint32_t* O, uint32_t* O_deg) {
     uint64_t pool_cap = (uint64_t)cap + (uint64_t)g->K + (g->rev_off[g->n] - g->rev_off[0]) + 1;
     float* pd = (float*)malloc(sizeof(float) * pool_cap);
     uint32_t* pi = (uint32_t*)malloc(sizeof(uint32_t) * pool_cap);
@@ -640,10 +1007,15 @@ void ao_graph_select(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t 
         int64_t np = ao_gather(g, i, ef, cap, pd, pi, pool_cap);
         uint32_t* row = O + i * M;
         for (uint32_t j = 0; j < M; j++) row[j] = AO_EMPTY;
-        O_deg[i] = ao_prune(g->x, g->norms, g->dim, g->n, i, pd, pi, (uint64_t)np, M, alpha, row);
+        O_deg[i] = ao_prune_policy(g->x, g->norms, g->dim, g->n, i, pd, pi, (uint64_t)np, M, alpha, pol, row);
     }
     free(pd);
     free(pi);
+}
+
+void ao_graph_select(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t M, float alpha,
+                     uint32_t* O, uint32_t* O_deg) {
+    ao_graph_select_policy(g, ef, cap, M, alpha, NULL, O, O_deg);
 }
 
 /* One pass of the global Vamana refine (index.h:856-875 greedy_collect,
@@ -708,9 +1080,9 @@ void ao_vamana_select(const float* x, const float* norms, uint32_t dim, uint64_t
 }
 
 /* commit_edges, index.h:907-930 */
-void ao_graph_commit(const float* x, const float* norms, uint32_t dim, uint64_t n,
-                     const uint32_t* O, const uint32_t* O_deg, uint32_t M, float alpha,
-                     uint32_t* links, uint32_t* deg) {
+void ao_graph_commit_policy(const float* x, const float* norms, uint32_t dim, uint64_t n, const uint32_t* O,
+                            const uint32_t* O_deg, uint32_t M, float alpha, const ao_edge_policy* pol,
+                            uint32_t* links, uint32_t* deg) {
     uint64_t* roff = (uint64_t*)calloc(n + 1, sizeof(uint64_t));
     for (uint64_t i = 0; i < n; i++)
         for (uint32_t j = 0; j < O_deg[i]; j++) roff[O[i * M + j] + 1]++;
@@ -743,13 +1115,19 @@ void ao_graph_commit(const float* x, const float* norms, uint32_t dim, uint64_t 
         }
         uint32_t* row = links + i * M;
         for (uint32_t j = 0; j < M; j++) row[j] = AO_EMPTY;
-        deg[i] = ao_prune(x, norms, dim, n, i, pd, pi, c, M, alpha, row);
+        deg[i] = ao_prune_policy(x, norms, dim, n, i, pd, pi, c, M, alpha, pol, row);
     }
     free(pd);
     free(pi);
     free(roff);
     free(rids);
     free(fill);
+}
+
+void ao_graph_commit(const float* x, const float* norms, uint32_t dim, uint64_t n,
+                     const uint32_t* O, const uint32_t* O_deg, uint32_t M, float alpha,
+                     uint32_t* links, uint32_t* deg) {
+    ao_graph_commit_policy(x, norms, dim, n, O, O_deg, M, alpha, NULL, links, deg);
 }
 
 /* -------------------------------------------------------------- heaps */

@@ -112,6 +112,38 @@ int64_t ao_gather(const ao_knn_graph* g, uint64_t i, uint32_t ef, uint32_t cap,
 /* build_approx_knn tail: gather, sort, first K ids != i (index.h:1347-1366). */
 void ao_aknn_rows(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t K,
                   uint32_t* out_ids, float* out_d);
+/* ---- edge policies of the graph prune (include/index.h:283-829) ----
+ * The configuration configure_edge_residual_cover (:305-440) leaves, as
+ * flags: residual cover, ball occlusion (pure or hybrid), LSG ordering, and
+ * the verification-constrained bubble optimizer (lazy or full). */
+#define AO_EDGE_COVER 1u
+#define AO_EDGE_BALL 2u
+#define AO_EDGE_PURE 4u
+#define AO_EDGE_LSG 8u
+#define AO_EDGE_AUTO 16u
+#define AO_EDGE_AUTO_FULL 32u
+typedef struct {
+    uint32_t flags;
+    uint32_t nks;
+    uint32_t ks[8];         /* the residual columns' k values, 1 <= k <= nk, in order */
+    uint32_t nk;            /* residual table stride */
+    uint32_t budget;        /* min(ANQI_EDGE_RESID_BUDGET, M) */
+    uint32_t occlude_all;   /* ball occlusion over all k (else any) */
+    uint32_t auto_candidates, auto_max_swaps;
+    double lambda, scale2, lsg_alpha;
+    const float* resid;     /* n x nk */
+    const float* mu;        /* n (LSG) */
+} ao_edge_policy;
+/* prune_pool_to_ids (index.h:772-829) under pol (NULL: the default policy);
+ * returns the degree. */
+uint32_t ao_prune_policy(const float* x, const float* norms, uint32_t dim, uint64_t n, uint64_t i,
+                         const float* pool_d, const uint32_t* pool_id, uint64_t pool_n, uint32_t M, float alpha,
+                         const ao_edge_policy* pol, uint32_t* out);
+void ao_graph_select_policy(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t M, float alpha,
+                            const ao_edge_policy* pol, uint32_t* O, uint32_t* O_deg);
+void ao_graph_commit_policy(const float* x, const float* norms, uint32_t dim, uint64_t n, const uint32_t* O,
+                            const uint32_t* O_deg, uint32_t M, float alpha, const ao_edge_policy* pol,
+                            uint32_t* links, uint32_t* deg);
 /* prune_pool_to_ids with the default edge policy; returns the degree. */
 uint32_t ao_prune(const float* x, const float* norms, uint32_t dim, uint64_t n, uint64_t i,
                   float* pool_d, uint32_t* pool_id, uint64_t pool_n, uint32_t M, float alpha,

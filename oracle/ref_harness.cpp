@@ -243,6 +243,9 @@ int cmd_graph(int argc, char** argv) {
     read_fbin(lifted, n, dim);
     Parms par = lifted_parms(n, dim, nnk, M, out + "_scratch/");
     nndindex index(lifted, par);
+    // the edge policy of the prune from ANQI_EDGE_* / ANQI_LSG_* (none when
+    // unset), as build_index configures it before its stages
+    index.configure_edge_residual_cover();
     // Warm-start IDs: the interleaved {u32 id, f32 key} top-100 records.
     std::vector<uint32_t> ids(n * 100);
     {

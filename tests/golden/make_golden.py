@@ -14,6 +14,10 @@ Fixtures:
   sample_ip_d32.npz  the d = 32 sample under the ip metric (every stage, as sample_d32.npz)
   lrq_forms.npz   CompactLrqVerifier in every form (bits 0/2/4/8/16/32, three policies,
                   signed IP keys) and the analytic Rank-M model, on the d = 32 sample
+  edge_policies.npz  the G48 select and commit stages (gather_candidates +
+                  prune_pool_to_ids, commit_edges) under every edge policy of
+                  include/index.h:283-829, on the d = 32 sample's lifted rows, with a
+                  seeded residual table and LSG mu table
 
 Usage: python tests/golden/make_golden.py --ref REFERENCE_TREE
        (or set ANQI_REFERENCE to the reference source tree)
@@ -338,12 +342,91 @@ def lrq_forms_fixture(sample: Path, out: Path) -> None:
         shutil.rmtree(work, ignore_errors=True)
 
 
+# (name, environment): ANQI_EDGE_POLICY and its options (include/index.h:305-440)
+EDGE_POLICIES = [
+    ("residual_cover", {"ANQI_EDGE_POLICY": "residual_cover"}),
+    ("residual_cover_scaled", {"ANQI_EDGE_POLICY": "residual_cover", "ANQI_EDGE_RESID_LAMBDA": "0.5",
+                               "_scale": "1.7"}),
+    ("residual_cover_ks", {"ANQI_EDGE_POLICY": "residual_cover", "ANQI_EDGE_KS": "0,5,200,7",
+                           "ANQI_EDGE_RESID_BUDGET": "9"}),
+    ("ball_rng", {"ANQI_EDGE_POLICY": "ball_rng"}),
+    ("ball_rng_any", {"ANQI_EDGE_POLICY": "ball_rng", "ANQI_EDGE_BALL_OCCLUSION": "any", "_scale": "0.8"}),
+    ("ball_rng_budget0", {"ANQI_EDGE_POLICY": "ball_rng", "ANQI_EDGE_RESID_BUDGET": "0"}),
+    ("bubble_rng", {"ANQI_EDGE_POLICY": "bubble_rng", "ANQI_EDGE_RESID_LAMBDA": "2.0"}),
+    ("ball_hybrid", {"ANQI_EDGE_POLICY": "ball_hybrid"}),
+    ("ball_hybrid_budget0", {"ANQI_EDGE_POLICY": "ball_hybrid", "ANQI_EDGE_RESID_BUDGET": "0"}),
+    ("ball_multik", {"ANQI_EDGE_POLICY": "ball_multik", "ANQI_EDGE_KS": "10,50,100"}),
+    ("bubble_hybrid", {"ANQI_EDGE_POLICY": "bubble_hybrid", "ANQI_EDGE_KS": "10,50",
+                       "ANQI_EDGE_RESID_BUDGET": "24"}),
+    ("bubble_multik", {"ANQI_EDGE_POLICY": "bubble_multik", "ANQI_EDGE_BALL_OCCLUSION": "any"}),
+    ("lsg_rng", {"ANQI_EDGE_POLICY": "lsg_rng"}),
+    ("lsg_rng_half", {"ANQI_EDGE_POLICY": "lsg_rng", "ANQI_LSG_ALPHA": "0.5"}),
+    ("lsg_rng_zero", {"ANQI_EDGE_POLICY": "lsg_rng", "ANQI_LSG_ALPHA": "0"}),
+    ("lsg_bubble_hybrid", {"ANQI_EDGE_POLICY": "lsg_bubble_hybrid"}),
+    ("bubble_auto", {"ANQI_EDGE_POLICY": "bubble_auto"}),
+    ("bubble_auto_small", {"ANQI_EDGE_POLICY": "bubble_auto", "ANQI_EDGE_AUTO_CANDIDATES": "8",
+                           "ANQI_EDGE_AUTO_MAX_SWAPS": "3", "ANQI_EDGE_BALL_OCCLUSION": "any"}),
+    ("bubble_auto_full", {"ANQI_EDGE_POLICY": "bubble_auto_full", "ANQI_EDGE_KS": "10,100"}),
+    ("unknown", {"ANQI_EDGE_POLICY": "no_such_policy"}),
+]
+
+
+def edge_policy_fixture(sample: Path, out: Path) -> None:
+    """The reference's select (gather_candidates + prune_pool_to_ids) and
+    commit_edges under every edge policy, driven by oracle/ref_harness graph
+    on the d = 32 sample's lifted rows and AKNN records.  The residual table
+    (n x 100) and the LSG mu table are seeded draws scaled to the sample's
+    lifted distances; "_scale" writes the lift meta file the policy reads its
+    scale from (otherwise absent: scale^2 = 1)."""
+    z = dict(np.load(sample))
+    lifted, rec_ids, rec_keys = z["lifted"], z["rec_ids"], z["rec_keys"]
+    n = lifted.shape[0]
+    rng = np.random.default_rng(31)
+    med = float(np.median(z["g_join_vals"][z["g_join_vals"] < np.float32(3e38)]))
+    resid = rng.normal(0.0, 0.3 * med, size=(n, 100)).astype(np.float32)
+    mu = np.exp(rng.normal(0.0, 0.35, size=n)).astype(np.float32)
+    data = {"resid": resid, "mu": mu, "names": np.array([p[0] for p in EDGE_POLICIES])}
+    work = Path(tempfile.mkdtemp(prefix="anqi_golden_edge_"))
+    try:
+        lf = work / "lifted.bin"
+        write_fbin(lf, lifted)
+        rec = np.empty((n, 100, 2), np.uint32)
+        rec[:, :, 0] = rec_ids
+        rec[:, :, 1] = rec_keys.view(np.uint32)
+        rf = work / "warm.rec"
+        rec.tofile(rf)
+        resid_f = work / "resid.bin"
+        resid.tofile(resid_f)
+        mu_f = work / "mu.bin"
+        mu.tofile(mu_f)
+        for name, env in EDGE_POLICIES:
+            h = work / name
+            (work / f"{name}_scratch").mkdir()
+            env = dict(env)
+            scale = env.pop("_scale", None)
+            if scale is not None:
+                (work / f"{name}_scratch" / "_anqi_meta.txt").write_text(f"1.5 {scale}\n")
+            env.setdefault("ANQI_EDGE_RESID_FILE", str(resid_f))
+            env.setdefault("ANQI_LSG_MU_FILE", str(mu_f))
+            run([REFBIN / "ref_harness", "graph", lf, rf, 50, 48, h], env=env)
+            for stage in ("O", "adj"):
+                off, ids = read_csr64(Path(f"{h}_{stage}.bin"))
+                data[f"{name}_{stage}_off"] = off
+                data[f"{name}_{stage}"] = ids
+            data[f"{name}_env"] = np.array([f"{k}={v}" for k, v in sorted(env.items())
+                                            if k not in ("ANQI_EDGE_RESID_FILE", "ANQI_LSG_MU_FILE")])
+            data[f"{name}_scale"] = np.float64(float(scale) if scale is not None else 1.0)
+        np.savez_compressed(out, **data)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     env = os.environ.get("ANQI_REFERENCE")
     ap.add_argument("--ref", type=Path, default=Path(env) if env else None,
                     help="reference source tree (default: $ANQI_REFERENCE)")
-    ap.add_argument("--only", choices=("lrq_forms", "sample_ip"), help="regenerate one fixture")
+    ap.add_argument("--only", choices=("lrq_forms", "sample_ip", "edge_policies"), help="regenerate one fixture")
     args = ap.parse_args()
     if args.ref is None or not (args.ref / "include" / "index.h").exists():
         raise SystemExit("give the reference source tree with --ref or ANQI_REFERENCE")
@@ -355,11 +438,15 @@ def main() -> int:
     if args.only == "sample_ip":
         sample_fixture(args.ref, 32, HERE / "sample_ip_d32.npz", metric="ip")
         return 0
+    if args.only == "edge_policies":
+        edge_policy_fixture(HERE / "sample_d32.npz", HERE / "edge_policies.npz")
+        return 0
     dist_fixture(HERE / "dist.npz")
     sample_fixture(args.ref, 8, HERE / "sample_d8.npz")
     sample_fixture(args.ref, 32, HERE / "sample_d32.npz")
     lrq_forms_fixture(HERE / "sample_d32.npz", HERE / "lrq_forms.npz")
     sample_fixture(args.ref, 32, HERE / "sample_ip_d32.npz", metric="ip")
+    edge_policy_fixture(HERE / "sample_d32.npz", HERE / "edge_policies.npz")
     for p in sorted(HERE.glob("*.npz")):
         print(f"{p.name}: {p.stat().st_size} bytes")
     return 0

@@ -105,6 +105,12 @@ LIB.ao_gather.restype = C.c_int64
 LIB.ao_gather.argtypes = [C.POINTER(AoKnnGraph), C.c_uint64, C.c_uint32, C.c_uint32, f32p, u32p, C.c_uint64]
 LIB.ao_aknn_rows.restype = None
 LIB.ao_aknn_rows.argtypes = [C.POINTER(AoKnnGraph), C.c_uint32, C.c_uint32, C.c_uint32, u32p, f32p]
+LIB.ao_graph_select_policy.restype = None
+LIB.ao_graph_select_policy.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, u32p,
+                                       u32p]
+LIB.ao_graph_commit_policy.restype = None
+LIB.ao_graph_commit_policy.argtypes = [f32p, f32p, C.c_uint32, C.c_uint64, u32p, u32p, C.c_uint32, C.c_float,
+                                       C.c_void_p, u32p, u32p]
 LIB.ao_graph_select.restype = None
 LIB.ao_graph_select.argtypes = [C.POINTER(AoKnnGraph), C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, u32p, u32p]
 LIB.ao_rp_tree.restype = C.c_int64
@@ -262,6 +268,54 @@ def vamana_select(x, nrm, links, deg, g0, entry, Lb=128, alpha=1.2):
                          np.ascontiguousarray(deg, np.uint32), M, np.ascontiguousarray(g0, np.uint32), g0.shape[1],
                          np.ascontiguousarray(entry, np.uint32), Lb, alpha, O, Od)
     return O, Od
+
+
+class AoEdgePolicy(C.Structure):
+    _fields_ = [
+        ("flags", C.c_uint32), ("nks", C.c_uint32), ("ks", C.c_uint32 * 8), ("nk", C.c_uint32),
+        ("budget", C.c_uint32), ("occlude_all", C.c_uint32), ("auto_candidates", C.c_uint32),
+        ("auto_max_swaps", C.c_uint32), ("lam", C.c_double), ("scale2", C.c_double), ("lsg_alpha", C.c_double),
+        ("resid", C.c_void_p), ("mu", C.c_void_p),
+    ]
+
+
+def edge_policy(pol):
+    """ao_edge_policy of an anqi.edge_policy.EdgePolicy (None: the default prune)."""
+    if pol is None or not pol.active:
+        return None
+    resid = np.ascontiguousarray(pol.resid, np.float32) if pol.resid is not None else np.zeros(1, np.float32)
+    mu = np.ascontiguousarray(pol.mu, np.float32) if pol.mu is not None else np.zeros(1, np.float32)
+    ks = (C.c_uint32 * 8)(*(list(pol.ks) + [0] * (8 - len(pol.ks))))
+    s = AoEdgePolicy(pol.flags, len(pol.ks), ks, pol.nk, pol.budget, int(pol.occlude_all), pol.auto_candidates,
+                     pol.auto_max_swaps, pol.lam, pol.scale2, pol.lsg_alpha, _p(resid), _p(mu))
+    s._keep = (resid, mu)
+    return s
+
+
+def graph_select_policy(x, nrm, ids, vals, pol, M=48, ef=100, cap=800, alpha=1.2):
+    x = np.ascontiguousarray(x, np.float32)
+    ids = np.ascontiguousarray(ids, np.uint32)
+    vals = np.ascontiguousarray(vals, np.float32)
+    off, rev = reverse(ids)
+    rev = rev if rev.size else np.zeros(1, np.uint32)
+    g = knn_graph(x, nrm, ids, vals, off, rev)
+    n = x.shape[0]
+    O = np.empty((n, M), np.uint32)
+    Od = np.empty(n, np.uint32)
+    ep = edge_policy(pol)
+    LIB.ao_graph_select_policy(C.byref(g), ef, cap, M, alpha, C.byref(ep) if ep is not None else None, O, Od)
+    return O, Od
+
+
+def graph_commit_policy(x, nrm, O, Od, pol, alpha=1.2):
+    n, M = O.shape
+    links = np.empty((n, M), np.uint32)
+    deg = np.empty(n, np.uint32)
+    ep = edge_policy(pol)
+    LIB.ao_graph_commit_policy(x, nrm, x.shape[1], n, np.ascontiguousarray(O, np.uint32),
+                               np.ascontiguousarray(Od, np.uint32), M, alpha,
+                               C.byref(ep) if ep is not None else None, links, deg)
+    return links, deg
 
 
 def graph_commit(x, nrm, O, Od, alpha=1.2):

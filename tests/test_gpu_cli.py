@@ -408,3 +408,56 @@ def test_rknn_query_vamana_global(tmp_path):
     rc, ours, err = tc.run("rknn_query", "16,32,64", pfx, 48, 500, 64, 600, 10, env=env)
     assert rc == 0, err
     assert lines(ours) == lines(ref.stdout)
+
+
+@pytest.mark.skipif(not tc.REF_BIN.exists(), reason="reference binaries not built")
+@pytest.mark.parametrize("policy", ["ball_rng", "residual_cover", "lsg_bubble_hybrid", "bubble_auto"])
+def test_rknn_query_edge_policy(tmp_path, policy):
+    """ANQI_EDGE_POLICY with a residual table (ANQI_EDGE_RESID_FILE) and an LSG
+    mu table: the graph cache is named as the reference names it (the _edge
+    key), the build's recall is within 0.05 of the reference's own build under
+    the policy, and on the reference's graph the result lines are the
+    reference's."""
+    pfx, env, z = tc.sample_prefix(tmp_path, 32)
+    n = z["base"].shape[0]
+    rng = np.random.default_rng(4)
+    rf = tmp_path / "resid.bin"
+    mf = tmp_path / "mu.bin"
+    rng.normal(0.0, 2.0, size=(n, 100)).astype(np.float32).tofile(rf)
+    np.exp(rng.normal(0.0, 0.3, size=n)).astype(np.float32).tofile(mf)
+    env = dict(env, ANQI_EDGE_POLICY=policy, ANQI_EDGE_RESID_FILE=str(rf), ANQI_LSG_MU_FILE=str(mf))
+    ref_env = {k: v for k, v in os.environ.items() if not k.startswith("ANQI_")}
+    ref_env.update(env, OMP_NUM_THREADS="1", ANQI_GRAPH_CACHE_DIR=str(tmp_path / "ref" / "graph"),
+                   ANQI_VERIFIER_CACHE_DIR=str(tmp_path / "ref" / "verifier"))
+    for sub in ("graph", "verifier"):
+        (tmp_path / "ref" / sub).mkdir(parents=True)
+    ref = subprocess.run([str(tc.REF_BIN), "16,32,64", str(pfx), "48", "500", "64", "600", "10"], env=ref_env,
+                         capture_output=True, text=True, timeout=300)
+    assert ref.returncode == 0, ref.stderr
+    rc, ours, err = tc.run("rknn_query", "16,32,64", pfx, 48, 500, 64, 600, 10, env=env)
+    assert rc == 0, err
+    assert "[edge-policy]" in err
+    rl = lines(ref.stdout)
+    for L, v in lines(ours).items():
+        assert abs(v[0] - rl[L][0]) < 0.05, (L, v, rl[L])
+    gref = list((tmp_path / "ref" / "graph").glob("fd_metric_*"))
+    gours = list(Path(env["ANQI_GRAPH_CACHE_DIR"]).glob("fd_metric_*"))
+    assert len(gref) == 1 and len(gours) == 1 and gref[0].name == gours[0].name
+    gours[0].write_bytes(gref[0].read_bytes())
+    for suffix in ("_approxlift_graph_", "_anqi_meta_graph_"):
+        for p in (tmp_path / "ref" / "graph").glob(suffix + "*"):
+            (Path(env["ANQI_GRAPH_CACHE_DIR"]) / p.name).write_bytes(p.read_bytes())
+    rc, ours, err = tc.run("rknn_query", "16,32,64", pfx, 48, 500, 64, 600, 10, env=env)
+    assert rc == 0, err
+    assert lines(ours) == lines(ref.stdout)
+
+
+def test_rknn_query_edge_policy_errors(tmp_path):
+    """The reference's exit-2 errors of the policy configuration, at graph
+    build time: LSG without its mu table, a missing residual table."""
+    pfx, env, _ = tc.sample_prefix(tmp_path, 32)
+    rc, _, err = tc.run("rknn_query", "16", pfx, 48, 500, 64, 600, 10, env=dict(env, ANQI_EDGE_POLICY="lsg_rng"))
+    assert rc == 2 and "requires ANQI_LSG_MU_FILE" in err
+    rc, _, err = tc.run("rknn_query", "16", pfx, 48, 500, 64, 600, 10,
+                        env=dict(env, ANQI_EDGE_POLICY="ball_rng", ANQI_EDGE_RESID_FILE=str(tmp_path / "none.bin")))
+    assert rc == 2 and "residual_cover requested but missing" in err
