@@ -1024,59 +1024,203 @@ void ao_graph_select(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t 
  * visited node but i with its distance, the row's g0 list (n x K, ANQI_EMPTY
  * skipped) follows with fresh distances, and the pool is pruned as
  * prune_pool_to_ids -> O (n x M, ANQI_EMPTY padded), O_deg. */
+/* A Vamana pool of row i (appended to pd/pi, grown as needed): the visits of
+ * a beam of width Lb over the current graph (links, deg) from ep but i
+ * (greedy_collect / greedy_collect_from_entry, index.h:856-903), the row's g0
+ * list (append_aknn_edges, :767-770) and, when cur, the row's current links
+ * (append_current_edges, :759-765), each with a fresh distance. */
+typedef struct {
+    float* d;
+    uint32_t* id;
+    uint64_t n, cap;
+} ao_pool;
+
+static void pool_push(ao_pool* p, uint32_t id, float d) {
+    if (p->n == p->cap) {
+        p->cap = p->cap ? 2 * p->cap : 1024;
+        p->d = (float*)realloc(p->d, sizeof(float) * p->cap);
+        p->id = (uint32_t*)realloc(p->id, sizeof(uint32_t) * p->cap);
+    }
+    p->d[p->n] = d;
+    p->id[p->n] = id;
+    p->n++;
+}
+
+static void vamana_pool(const float* x, const float* norms, uint32_t dim, uint64_t n, const uint32_t* links,
+                        const uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, uint64_t i, uint32_t ep,
+                        uint32_t Lb, int cur_edges, uint8_t* vis, ao_pool* pool) {
+    memset(vis, 0, n);
+    pool->n = 0;
+    queue_t beam;
+    q_init(&beam, Lb);
+    if (ep >= n) ep = 0;
+    vis[ep] = 1;
+    float d0 = ao_d2(x + i * dim, x + (uint64_t)ep * dim, norms[i], norms[ep], dim);
+    q_insert(&beam, d0, ep);
+    if (ep != (uint32_t)i) pool_push(pool, ep, d0);
+    while (beam.cur < beam.size) {
+        uint32_t cur = q_pop(&beam);
+        for (uint32_t j = 0; j < deg[cur]; j++) {
+            uint32_t nb = links[(uint64_t)cur * M + j];
+            if (nb >= n || vis[nb]) continue;
+            vis[nb] = 1;
+            float d = ao_d2(x + i * dim, x + (uint64_t)nb * dim, norms[i], norms[nb], dim);
+            q_insert(&beam, d, nb);
+            if (nb != (uint32_t)i) pool_push(pool, nb, d);
+        }
+    }
+    free(beam.data);
+    for (uint32_t k = 0; k < K; k++) {
+        uint32_t j = g0[i * K + k];
+        if (j == AO_EMPTY || j >= n || j == (uint32_t)i) continue;
+        pool_push(pool, j, ao_d2(x + i * dim, x + (uint64_t)j * dim, norms[i], norms[j], dim));
+    }
+    if (cur_edges)
+        for (uint32_t k = 0; k < deg[i]; k++) {
+            uint32_t j = links[i * M + k];
+            if (j == AO_EMPTY || j >= n || j == (uint32_t)i) continue;
+            pool_push(pool, j, ao_d2(x + i * dim, x + (uint64_t)j * dim, norms[i], norms[j], dim));
+        }
+}
+
+void ao_vamana_select_policy(const float* x, const float* norms, uint32_t dim, uint64_t n, const uint32_t* links,
+                             const uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, const uint32_t* entry,
+                             uint32_t Lb, float alpha, const ao_edge_policy* pol, uint32_t* O, uint32_t* O_deg) {
+    uint8_t* vis = (uint8_t*)malloc(n);
+    ao_pool pool = {0};
+    for (uint64_t i = 0; i < n; i++) {
+        vamana_pool(x, norms, dim, n, links, deg, M, g0, K, i, entry[i], Lb, 0, vis, &pool);
+        uint32_t* row = O + i * M;
+        for (uint32_t j = 0; j < M; j++) row[j] = AO_EMPTY;
+        O_deg[i] = ao_prune_policy(x, norms, dim, n, i, pool.d, pool.id, pool.n, M, alpha, pol, row);
+    }
+    free(vis);
+    free(pool.d);
+    free(pool.id);
+}
+
 void ao_vamana_select(const float* x, const float* norms, uint32_t dim, uint64_t n, const uint32_t* links,
                       const uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, const uint32_t* entry,
                       uint32_t Lb, float alpha, uint32_t* O, uint32_t* O_deg) {
+    ao_vamana_select_policy(x, norms, dim, n, links, deg, M, g0, K, entry, Lb, alpha, NULL, O, O_deg);
+}
+
+/* vamana_batch_refine, index.h:936-1065: per pass, the order shuffled
+ * (ao_vamana_batch_order) and cut into batches of 1, b-1, b^2-b, ... rows up
+ * to max_batch, then max_batch rows; a batch's rows each prune a pool from
+ * the graph as it was at the batch's start (beam from the single entry, g0,
+ * current links) and take the result as their links; then every row that a
+ * batch row now links to prunes its current links plus those batch rows. */
+void ao_vamana_batch_refine(const float* x, const float* norms, uint32_t dim, uint64_t n, uint32_t* links,
+                            uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, uint32_t entry, uint32_t Lb,
+                            int passes, float final_alpha, float early_alpha, int early_one, double max_frac,
+                            uint64_t max_batch_cap, double batch_base, uint64_t seed, const ao_edge_policy* pol) {
+    if (n == 0 || passes <= 0) return;
+    if (max_frac <= 0.0) max_frac = 0.02;
+    double mb = max_frac * (double)n;
+    uint64_t max_batch = (uint64_t)(mb > 1.0 ? mb : 1.0);
+    if (max_batch > max_batch_cap) max_batch = max_batch_cap;
+    if (max_batch == 0) max_batch = n;
+    if (batch_base <= 1.0) batch_base = 2.0;
+    uint32_t* order = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    for (uint64_t i = 0; i < n; i++) order[i] = (uint32_t)i;
     uint8_t* vis = (uint8_t*)malloc(n);
-    uint64_t cap = 1024;
-    float* pd = (float*)malloc(sizeof(float) * cap);
-    uint32_t* pi = (uint32_t*)malloc(sizeof(uint32_t) * cap);
-    for (uint64_t i = 0; i < n; i++) {
-        memset(vis, 0, n);
-        uint64_t np = 0;
-#define AO_VPUSH(ID, D)                                              \
-    do {                                                             \
-        if (np == cap) {                                             \
-            cap *= 2;                                                \
-            pd = (float*)realloc(pd, sizeof(float) * cap);           \
-            pi = (uint32_t*)realloc(pi, sizeof(uint32_t) * cap);     \
-        }                                                            \
-        pd[np] = (D);                                                \
-        pi[np] = (ID);                                               \
-        np++;                                                        \
-    } while (0)
-        queue_t beam;
-        q_init(&beam, Lb);
-        uint32_t ep = entry[i] < n ? entry[i] : 0;
-        vis[ep] = 1;
-        float d0 = ao_d2(x + i * dim, x + (uint64_t)ep * dim, norms[i], norms[ep], dim);
-        q_insert(&beam, d0, ep);
-        if (ep != (uint32_t)i) AO_VPUSH(ep, d0);
-        while (beam.cur < beam.size) {
-            uint32_t cur = q_pop(&beam);
-            for (uint32_t j = 0; j < deg[cur]; j++) {
-                uint32_t nb = links[(uint64_t)cur * M + j];
-                if (nb >= n || vis[nb]) continue;
-                vis[nb] = 1;
-                float d = ao_d2(x + i * dim, x + (uint64_t)nb * dim, norms[i], norms[nb], dim);
-                q_insert(&beam, d, nb);
-                if (nb != (uint32_t)i) AO_VPUSH(nb, d);
+    uint32_t* out = NULL;
+    uint32_t* out_deg = NULL;
+    uint32_t* rcount = (uint32_t*)calloc(n, sizeof(uint32_t));
+    uint64_t* roff = (uint64_t*)calloc(n + 1, sizeof(uint64_t));
+    uint32_t* rfill = (uint32_t*)calloc(n, sizeof(uint32_t));
+    uint32_t* touched = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* rsrc = NULL;
+    uint32_t ids[64];
+    ao_pool pool = {0};
+    for (int pass = 0; pass < passes; pass++) {
+        const float alpha = (early_one && pass + 1 < passes) ? early_alpha : final_alpha;
+        ao_vamana_batch_order(order, n, seed, pass);
+        uint64_t count = 0, inc = 0;
+        while (count < n) {
+            uint64_t floor_ = count, ceiling;
+            const double p0 = pow(batch_base, (double)inc);
+            if (p0 <= (double)max_batch) {
+                floor_ = (uint64_t)p0 - 1;
+                const double p1 = pow(batch_base, (double)(inc + 1));
+                ceiling = (uint64_t)p1 - 1;
+                if (ceiling > n) ceiling = n;
+                count = ceiling;
+            } else {
+                ceiling = count + max_batch < n ? count + max_batch : n;
+                count = ceiling;
+            }
+            inc++;
+            if (ceiling <= floor_ || floor_ >= n) continue;
+            const uint64_t bsz = ceiling - floor_;
+            out = (uint32_t*)realloc(out, sizeof(uint32_t) * bsz * M);
+            out_deg = (uint32_t*)realloc(out_deg, sizeof(uint32_t) * bsz);
+            for (uint64_t b = 0; b < bsz; b++) {
+                const uint32_t node = order[floor_ + b];
+                vamana_pool(x, norms, dim, n, links, deg, M, g0, K, node, entry, Lb, 1, vis, &pool);
+                out_deg[b] = ao_prune_policy(x, norms, dim, n, node, pool.d, pool.id, pool.n, M, alpha, pol,
+                                             out + b * M);
+            }
+            for (uint64_t b = 0; b < bsz; b++) {
+                const uint32_t node = order[floor_ + b];
+                for (uint32_t j = 0; j < M; j++) links[(uint64_t)node * M + j] = j < out_deg[b] ? out[b * M + j] : AO_EMPTY;
+                deg[node] = out_deg[b];
+            }
+            uint64_t nt = 0, tot = 0;
+            for (uint64_t b = 0; b < bsz; b++)
+                for (uint32_t j = 0; j < out_deg[b]; j++) {
+                    const uint32_t dst = out[b * M + j];
+                    if (dst >= n) continue;
+                    if (rcount[dst]++ == 0) touched[nt++] = dst;
+                    tot++;
+                }
+            rsrc = (uint32_t*)realloc(rsrc, sizeof(uint32_t) * (tot + 1));
+            uint64_t acc = 0;
+            for (uint64_t t = 0; t < nt; t++) {
+                roff[touched[t]] = acc;
+                acc += rcount[touched[t]];
+            }
+            for (uint64_t b = 0; b < bsz; b++)
+                for (uint32_t j = 0; j < out_deg[b]; j++) {
+                    const uint32_t dst = out[b * M + j];
+                    if (dst >= n) continue;
+                    rsrc[roff[dst] + rfill[dst]++] = order[floor_ + b];
+                }
+            for (uint64_t t = 0; t < nt; t++) {
+                const uint32_t dst = touched[t];
+                pool.n = 0;
+                for (uint32_t k = 0; k < deg[dst]; k++) {
+                    const uint32_t j = links[(uint64_t)dst * M + k];
+                    if (j == AO_EMPTY || j >= n || j == dst) continue;
+                    pool_push(&pool, j, ao_d2(x + (uint64_t)dst * dim, x + (uint64_t)j * dim, norms[dst], norms[j], dim));
+                }
+                for (uint32_t r = 0; r < rcount[dst]; r++) {
+                    const uint32_t src = rsrc[roff[dst] + r];
+                    if (src == dst || src >= n) continue;
+                    pool_push(&pool, src, ao_d2(x + (uint64_t)dst * dim, x + (uint64_t)src * dim, norms[dst], norms[src], dim));
+                }
+                const uint32_t nd = ao_prune_policy(x, norms, dim, n, dst, pool.d, pool.id, pool.n, M, alpha, pol, ids);
+                for (uint32_t j = 0; j < M; j++) links[(uint64_t)dst * M + j] = j < nd ? ids[j] : AO_EMPTY;
+                deg[dst] = nd;
+            }
+            for (uint64_t t = 0; t < nt; t++) {
+                rcount[touched[t]] = 0;
+                rfill[touched[t]] = 0;
             }
         }
-        for (uint32_t k = 0; k < K; k++) {
-            uint32_t j = g0[i * K + k];
-            if (j == AO_EMPTY || j >= n || j == (uint32_t)i) continue;
-            AO_VPUSH(j, ao_d2(x + i * dim, x + (uint64_t)j * dim, norms[i], norms[j], dim));
-        }
-#undef AO_VPUSH
-        free(beam.data);
-        uint32_t* row = O + i * M;
-        for (uint32_t j = 0; j < M; j++) row[j] = AO_EMPTY;
-        O_deg[i] = ao_prune(x, norms, dim, n, i, pd, pi, np, M, alpha, row);
     }
+    free(order);
     free(vis);
-    free(pd);
-    free(pi);
+    free(out);
+    free(out_deg);
+    free(rcount);
+    free(roff);
+    free(rfill);
+    free(touched);
+    free(rsrc);
+    free(pool.d);
+    free(pool.id);
 }
 
 /* commit_edges, index.h:907-930 */
@@ -1500,4 +1644,73 @@ int64_t ao_rknn_gt_metric(const float* base, uint64_t n, const float* query, uin
     free(bn);
     free(hits);
     return over ? -1 : (int64_t)total;
+}
+
+/* ---- the batched Vamana style's insertion order ---- */
+void ao_mt64_seed(ao_mt64* g, uint64_t seed) {
+    g->mt[0] = seed;
+    for (uint32_t i = 1; i < 312; i++) g->mt[i] = 6364136223846793005ull * (g->mt[i - 1] ^ (g->mt[i - 1] >> 62)) + i;
+    g->idx = 312;
+}
+
+uint64_t ao_mt64_next(ao_mt64* g) {
+    if (g->idx >= 312) {
+        for (uint32_t i = 0; i < 312; i++) {
+            const uint64_t y = (g->mt[i] & 0xFFFFFFFF80000000ull) | (g->mt[(i + 1) % 312] & 0x7FFFFFFFull);
+            g->mt[i] = g->mt[(i + 156) % 312] ^ (y >> 1) ^ ((y & 1ull) ? 0xB5026F5AA96619E9ull : 0ull);
+        }
+        g->idx = 0;
+    }
+    uint64_t x = g->mt[g->idx++];
+    x ^= (x >> 29) & 0x5555555555555555ull;
+    x ^= (x << 17) & 0x71D67FFFEDA60000ull;
+    x ^= (x << 37) & 0xFFF7EEE000000000ull;
+    x ^= x >> 43;
+    return x;
+}
+
+/* a uniform draw in [0, range) from full 64-bit outputs: the high half of
+ * the 128-bit product, rejecting low halves below 2^64 mod range */
+static uint64_t ao_bounded(ao_mt64* g, uint64_t range) {
+    unsigned __int128 prod = (unsigned __int128)ao_mt64_next(g) * range;
+    uint64_t low = (uint64_t)prod;
+    if (low < range) {
+        const uint64_t threshold = (0ull - range) % range;
+        while (low < threshold) {
+            prod = (unsigned __int128)ao_mt64_next(g) * range;
+            low = (uint64_t)prod;
+        }
+    }
+    return (uint64_t)(prod >> 64);
+}
+
+void ao_shuffle_u32(uint32_t* a, uint64_t n, ao_mt64* g) {
+    if (n < 2) return;
+    uint64_t i = 1;
+    if (n % 2 == 0) {
+        const uint64_t j = ao_bounded(g, 2);
+        const uint32_t t = a[i];
+        a[i] = a[j];
+        a[j] = t;
+        i++;
+    }
+    while (i < n) {
+        const uint64_t b0 = i + 1, b1 = i + 2;
+        const uint64_t x = ao_bounded(g, b0 * b1);
+        const uint64_t p0 = x / b1, p1 = x % b1;
+        uint32_t t = a[i];
+        a[i] = a[p0];
+        a[p0] = t;
+        i++;
+        t = a[i];
+        a[i] = a[p1];
+        a[p1] = t;
+        i++;
+    }
+}
+
+void ao_vamana_batch_order(uint32_t* order, uint64_t n, uint64_t seed, int pass) {
+    ao_mt64 g;
+    ao_mt64_seed(&g, seed + 0x9e3779b97f4a7c15ull * (uint64_t)(pass + 1));
+    ao_shuffle_u32(order, n, &g);
 }

@@ -144,6 +144,23 @@ void ao_graph_select_policy(const ao_knn_graph* g, uint32_t ef, uint32_t cap, ui
 void ao_graph_commit_policy(const float* x, const float* norms, uint32_t dim, uint64_t n, const uint32_t* O,
                             const uint32_t* O_deg, uint32_t M, float alpha, const ao_edge_policy* pol,
                             uint32_t* links, uint32_t* deg);
+/* ---- the batched Vamana style's insertion order ----
+ * std::mt19937_64 (the 64-bit Mersenne Twister of Matsumoto and Nishimura,
+ * seeded from one value) and std::shuffle as GCC's library performs it on a
+ * vector of 32-bit ids: Fisher-Yates from the front, positions drawn two at a
+ * time from one bounded draw (Brackett-Rozinsky and Lemire's batched ranged
+ * integers), each bounded draw by Lemire's multiply-and-reject.  Checked
+ * against the compiler's own std::shuffle (tests/test_vamana_batch.py). */
+typedef struct {
+    uint64_t mt[312];
+    uint32_t idx;
+} ao_mt64;
+void ao_mt64_seed(ao_mt64* g, uint64_t seed);
+uint64_t ao_mt64_next(ao_mt64* g);
+void ao_shuffle_u32(uint32_t* a, uint64_t n, ao_mt64* g);
+/* index.h:936-1065: pass p's order, shuffled from the previous pass's */
+void ao_vamana_batch_order(uint32_t* order, uint64_t n, uint64_t seed, int pass);
+
 /* prune_pool_to_ids with the default edge policy; returns the degree. */
 uint32_t ao_prune(const float* x, const float* norms, uint32_t dim, uint64_t n, uint64_t i,
                   float* pool_d, uint32_t* pool_id, uint64_t pool_n, uint32_t M, float alpha,
@@ -156,6 +173,15 @@ void ao_graph_select(const ao_knn_graph* g, uint32_t ef, uint32_t cap, uint32_t 
 void ao_vamana_select(const float* x, const float* norms, uint32_t dim, uint64_t n, const uint32_t* links,
                       const uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, const uint32_t* entry,
                       uint32_t Lb, float alpha, uint32_t* O, uint32_t* O_deg);
+void ao_vamana_select_policy(const float* x, const float* norms, uint32_t dim, uint64_t n, const uint32_t* links,
+                             const uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, const uint32_t* entry,
+                             uint32_t Lb, float alpha, const ao_edge_policy* pol, uint32_t* O, uint32_t* O_deg);
+/* vamana_batch_refine (index.h:936-1065) on links / deg (n x M) in place,
+ * from the single entry, with the prunes under pol (NULL: default) */
+void ao_vamana_batch_refine(const float* x, const float* norms, uint32_t dim, uint64_t n, uint32_t* links,
+                            uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, uint32_t entry, uint32_t Lb,
+                            int passes, float final_alpha, float early_alpha, int early_one, double max_frac,
+                            uint64_t max_batch_cap, double batch_base, uint64_t seed, const ao_edge_policy* pol);
 /* commit_edges: final adjacency (n x M) from O */
 void ao_graph_commit(const float* x, const float* norms, uint32_t dim, uint64_t n,
                      const uint32_t* O, const uint32_t* O_deg, uint32_t M, float alpha,

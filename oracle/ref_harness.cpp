@@ -294,6 +294,33 @@ int cmd_graph(int argc, char** argv) {
     std::vector<std::vector<uint32_t>> adj(n);
     for (size_t i = 0; i < n; i++) adj[i].assign(index.lnk(i), index.lnk(i) + index.deg(i));
     dump_csr(adj, out + "_adj.bin");
+    // the Vamana refine of build_index (index.h:1262-1285) when ANQI_VAMANA is
+    // set: global passes from the RP-tree entries, or the batched style
+    if (std::getenv("ANQI_VAMANA")) {
+        const char* lv = std::getenv("ANQI_VAMANA_L");
+        const char* pv = std::getenv("ANQI_VAMANA_PASS");
+        const size_t Lb = lv ? (size_t)std::atoi(lv) : 128;
+        const int passes = pv ? std::atoi(pv) : 2;
+        const char* sv = std::getenv("ANQI_VAMANA_STYLE");
+        const std::string style = sv ? sv : "global";
+        if (style == "global" || style == "old") {
+            for (int pass = 0; pass < passes; pass++) {
+                for (size_t i = 0; i < n; i++) {
+                    std::vector<std::pair<float, uint32_t>> pool;
+                    index.greedy_collect(i, pool, Lb);
+                    index.append_aknn_edges(i, g0, pool);
+                    std::vector<uint32_t> ids;
+                    index.prune_pool_to_ids(i, pool, ids);
+                    O[i].assign(ids.begin(), ids.end());
+                }
+                index.commit_edges(O);
+            }
+        } else {
+            index.vamana_batch_refine(g0, rec, Lb, passes);
+        }
+        for (size_t i = 0; i < n; i++) adj[i].assign(index.lnk(i), index.lnk(i) + index.deg(i));
+        dump_csr(adj, out + "_vam_adj.bin");
+    }
     index.construction_time = 0.0f;
     // save_index writes into folder_path + generate_config(); mirror that layout explicitly.
     {

@@ -14,6 +14,9 @@ Fixtures:
   sample_ip_d32.npz  the d = 32 sample under the ip metric (every stage, as sample_d32.npz)
   lrq_forms.npz   CompactLrqVerifier in every form (bits 0/2/4/8/16/32, three policies,
                   signed IP keys) and the analytic Rank-M model, on the d = 32 sample
+  vamana.npz      the Vamana refine of build_index (global passes, the batched style
+                  with its options, each with and without an edge policy) after the
+                  G48 commit, on the d = 32 sample's lifted rows
   edge_policies.npz  the G48 select and commit stages (gather_candidates +
                   prune_pool_to_ids, commit_edges) under every edge policy of
                   include/index.h:283-829, on the d = 32 sample's lifted rows, with a
@@ -421,12 +424,63 @@ def edge_policy_fixture(sample: Path, out: Path) -> None:
         shutil.rmtree(work, ignore_errors=True)
 
 
+# (name, environment) of the Vamana refine (include/index.h:936-1065, 1262-1285)
+VAMANA_CONFIGS = [
+    ("global", {"ANQI_VAMANA": "1", "ANQI_VAMANA_L": "32", "ANQI_VAMANA_PASS": "2"}),
+    ("batch", {"ANQI_VAMANA": "1", "ANQI_VAMANA_STYLE": "batch", "ANQI_VAMANA_L": "32", "ANQI_VAMANA_PASS": "2"}),
+    ("batch_opts", {"ANQI_VAMANA": "1", "ANQI_VAMANA_STYLE": "batch", "ANQI_VAMANA_L": "24", "ANQI_VAMANA_PASS": "3",
+                    "ANQI_VAMANA_BATCH_FRAC": "0.1", "ANQI_VAMANA_BATCH_BASE": "3", "ANQI_VAMANA_MAX_BATCH": "20",
+                    "ANQI_VAMANA_ENTRY": "17", "ANQI_VAMANA_EARLY_ALPHA": "1.1", "ANQI_VAMANA_EARLY_ALPHA_ONE": "1"}),
+    ("batch_one_alpha", {"ANQI_VAMANA": "1", "ANQI_VAMANA_STYLE": "batch", "ANQI_VAMANA_L": "40",
+                         "ANQI_VAMANA_PASS": "1", "ANQI_VAMANA_EARLY_ALPHA_ONE": "0", "ANQI_VAMANA_BATCH_BASE": "1.5"}),
+    ("batch_ball", {"ANQI_VAMANA": "1", "ANQI_VAMANA_STYLE": "batch", "ANQI_VAMANA_L": "32", "ANQI_VAMANA_PASS": "2",
+                    "ANQI_EDGE_POLICY": "ball_rng"}),
+    ("global_cover", {"ANQI_VAMANA": "1", "ANQI_VAMANA_L": "32", "ANQI_VAMANA_PASS": "1",
+                      "ANQI_EDGE_POLICY": "residual_cover"}),
+]
+
+
+def vamana_fixture(sample: Path, edge: Path, out: Path) -> None:
+    """The reference's build_index Vamana refine after the G48 commit, driven
+    by oracle/ref_harness graph with ANQI_VAMANA set, on the d = 32 sample
+    (the edge policies' residual table where a policy is set)."""
+    z = dict(np.load(sample))
+    e = dict(np.load(edge))
+    lifted, rec_ids, rec_keys = z["lifted"], z["rec_ids"], z["rec_keys"]
+    n = lifted.shape[0]
+    data = {"names": np.array([c[0] for c in VAMANA_CONFIGS])}
+    work = Path(tempfile.mkdtemp(prefix="anqi_golden_vam_"))
+    try:
+        lf = work / "lifted.bin"
+        write_fbin(lf, lifted)
+        rec = np.empty((n, 100, 2), np.uint32)
+        rec[:, :, 0] = rec_ids
+        rec[:, :, 1] = rec_keys.view(np.uint32)
+        rf = work / "warm.rec"
+        rec.tofile(rf)
+        resid_f = work / "resid.bin"
+        e["resid"].tofile(resid_f)
+        for name, env in VAMANA_CONFIGS:
+            h = work / name
+            (work / f"{name}_scratch").mkdir()
+            env = dict(env, ANQI_EDGE_RESID_FILE=str(resid_f))
+            run([REFBIN / "ref_harness", "graph", lf, rf, 50, 48, h], env=env)
+            off, ids = read_csr64(Path(f"{h}_vam_adj.bin"))
+            data[f"{name}_off"] = off
+            data[f"{name}_adj"] = ids
+            data[f"{name}_env"] = np.array([f"{k}={v}" for k, v in sorted(env.items()) if k != "ANQI_EDGE_RESID_FILE"])
+        np.savez_compressed(out, **data)
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     env = os.environ.get("ANQI_REFERENCE")
     ap.add_argument("--ref", type=Path, default=Path(env) if env else None,
                     help="reference source tree (default: $ANQI_REFERENCE)")
-    ap.add_argument("--only", choices=("lrq_forms", "sample_ip", "edge_policies"), help="regenerate one fixture")
+    ap.add_argument("--only", choices=("lrq_forms", "sample_ip", "edge_policies", "vamana"),
+                    help="regenerate one fixture")
     args = ap.parse_args()
     if args.ref is None or not (args.ref / "include" / "index.h").exists():
         raise SystemExit("give the reference source tree with --ref or ANQI_REFERENCE")
@@ -441,12 +495,16 @@ def main() -> int:
     if args.only == "edge_policies":
         edge_policy_fixture(HERE / "sample_d32.npz", HERE / "edge_policies.npz")
         return 0
+    if args.only == "vamana":
+        vamana_fixture(HERE / "sample_d32.npz", HERE / "edge_policies.npz", HERE / "vamana.npz")
+        return 0
     dist_fixture(HERE / "dist.npz")
     sample_fixture(args.ref, 8, HERE / "sample_d8.npz")
     sample_fixture(args.ref, 32, HERE / "sample_d32.npz")
     lrq_forms_fixture(HERE / "sample_d32.npz", HERE / "lrq_forms.npz")
     sample_fixture(args.ref, 32, HERE / "sample_ip_d32.npz", metric="ip")
     edge_policy_fixture(HERE / "sample_d32.npz", HERE / "edge_policies.npz")
+    vamana_fixture(HERE / "sample_d32.npz", HERE / "edge_policies.npz", HERE / "vamana.npz")
     for p in sorted(HERE.glob("*.npz")):
         print(f"{p.name}: {p.stat().st_size} bytes")
     return 0

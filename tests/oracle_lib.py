@@ -111,6 +111,15 @@ LIB.ao_graph_select_policy.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_u
 LIB.ao_graph_commit_policy.restype = None
 LIB.ao_graph_commit_policy.argtypes = [f32p, f32p, C.c_uint32, C.c_uint64, u32p, u32p, C.c_uint32, C.c_float,
                                        C.c_void_p, u32p, u32p]
+LIB.ao_vamana_select_policy.restype = None
+LIB.ao_vamana_select_policy.argtypes = [f32p, f32p, C.c_uint32, C.c_uint64, u32p, u32p, C.c_uint32, u32p, C.c_uint32,
+                                        u32p, C.c_uint32, C.c_float, C.c_void_p, u32p, u32p]
+LIB.ao_vamana_batch_refine.restype = None
+LIB.ao_vamana_batch_refine.argtypes = [f32p, f32p, C.c_uint32, C.c_uint64, u32p, u32p, C.c_uint32, u32p, C.c_uint32,
+                                       C.c_uint32, C.c_uint32, C.c_int, C.c_float, C.c_float, C.c_int, C.c_double,
+                                       C.c_uint64, C.c_double, C.c_uint64, C.c_void_p]
+LIB.ao_vamana_batch_order.restype = None
+LIB.ao_vamana_batch_order.argtypes = [u32p, C.c_uint64, C.c_uint64, C.c_int]
 LIB.ao_graph_select.restype = None
 LIB.ao_graph_select.argtypes = [C.POINTER(AoKnnGraph), C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, u32p, u32p]
 LIB.ao_rp_tree.restype = C.c_int64
@@ -316,6 +325,40 @@ def graph_commit_policy(x, nrm, O, Od, pol, alpha=1.2):
                                np.ascontiguousarray(Od, np.uint32), M, alpha,
                                C.byref(ep) if ep is not None else None, links, deg)
     return links, deg
+
+
+def vamana_select_policy(x, nrm, links, deg, g0, entry, pol, Lb=128, alpha=1.2):
+    x = np.ascontiguousarray(x, np.float32)
+    n, M = links.shape
+    O = np.empty((n, M), np.uint32)
+    Od = np.empty(n, np.uint32)
+    ep = edge_policy(pol)
+    LIB.ao_vamana_select_policy(x, nrm, x.shape[1], n, np.ascontiguousarray(links, np.uint32),
+                                np.ascontiguousarray(deg, np.uint32), M, np.ascontiguousarray(g0, np.uint32),
+                                g0.shape[1], np.ascontiguousarray(entry, np.uint32), Lb, alpha,
+                                C.byref(ep) if ep is not None else None, O, Od)
+    return O, Od
+
+
+def vamana_batch_refine(x, nrm, links, deg, g0, vp, pol=None, alpha=1.2, seed=10):
+    """vamana_batch_refine on copies of links / deg; vp: anqi.vamana.VamanaParams."""
+    x = np.ascontiguousarray(x, np.float32)
+    links = np.ascontiguousarray(links, np.uint32).copy()
+    deg = np.ascontiguousarray(deg, np.uint32).copy()
+    n, M = links.shape
+    ep = edge_policy(pol)
+    LIB.ao_vamana_batch_refine(x, nrm, x.shape[1], n, links, deg, M, np.ascontiguousarray(g0, np.uint32), g0.shape[1],
+                               vp.entry, vp.L, vp.passes, alpha, vp.early_alpha, int(vp.early_alpha_one),
+                               vp.batch_frac, vp.max_batch, vp.batch_base, seed,
+                               C.byref(ep) if ep is not None else None)
+    return links, deg
+
+
+def vamana_batch_order(n, seed, passes):
+    o = np.arange(n, dtype=np.uint32)
+    for p in range(passes):
+        LIB.ao_vamana_batch_order(o, n, seed, p)
+    return o
 
 
 def graph_commit(x, nrm, O, Od, alpha=1.2):
