@@ -76,7 +76,10 @@ class GraphParams(C.Structure):
                 ("join_iters", C.c_uint32), ("join_sample", C.c_uint32), ("leaf", C.c_uint32),
                 ("max_depth", C.c_uint32), ("seed", C.c_uint64), ("alpha", C.c_float), ("warm_width", C.c_uint32),
                 ("precision", C.c_uint32), ("vamana_passes", C.c_uint32), ("vamana_L", C.c_uint32),
-                ("edge", C.c_void_p)]
+                ("edge", C.c_void_p), ("vamana_batch", C.c_uint32), ("vamana_entry", C.c_uint32),
+                ("vamana_batch_frac", C.c_double), ("vamana_max_batch", C.c_uint64),
+                ("vamana_batch_base", C.c_double), ("vamana_early_alpha", C.c_float),
+                ("vamana_early_alpha_one", C.c_uint32)]
 
 
 class EdgePolicyC(C.Structure):
@@ -167,6 +170,7 @@ _SIGS = {
                                  C.c_uint32, C.c_float, _vp, _u32, _u32],
     "anqi_graph_commit_policy": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _u32, C.c_uint32, C.c_float, _vp, _u32,
                                  _u32],
+    "anqi_graph_vamana_batch_refine": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _u32, _u32, C.c_uint32, _vp],
     "anqi_graph_vamana_select": [_vp, _f32, C.c_uint64, C.c_uint32, _u32, _u32, C.c_uint32, _u32, C.c_uint32, _u32,
                                  C.c_uint32, C.c_float, _u32, _u32],
     "anqi_index_load": [_vp, C.POINTER(IndexDesc)],

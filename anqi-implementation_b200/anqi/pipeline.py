@@ -97,9 +97,23 @@ def aknn_build(ctx: Context, base: np.ndarray, k=100, leaf=500, trees=64, ef=600
     return ids, dist, st.as_dict()
 
 
+def vamana_params(gp: GraphParams, vp) -> GraphParams:
+    """anqi_graph_params' Vamana fields from an anqi.vamana.VamanaParams."""
+    gp.vamana_passes = max(0, vp.passes)
+    gp.vamana_L = vp.L
+    gp.vamana_batch = int(vp.style not in ("global", "old"))
+    gp.vamana_entry = vp.entry
+    gp.vamana_batch_frac = vp.batch_frac
+    gp.vamana_max_batch = vp.max_batch % 2**64
+    gp.vamana_batch_base = vp.batch_base
+    gp.vamana_early_alpha = vp.early_alpha
+    gp.vamana_early_alpha_one = int(vp.early_alpha_one)
+    return gp
+
+
 def graph_build(ctx: Context, lifted: np.ndarray, warm_ids: np.ndarray, degree=48, nn_k=50, explore=100,
                 ef_alpha=8, join_iters=6, join_sample=20, leaf=100, seed=10, alpha=1.2, warm_width=100,
-                precision="bf16", vamana_passes=0, vamana_L=128, edge=None):
+                precision="bf16", vamana_passes=0, vamana_L=128, edge=None, vamana=None):
     """build_index with the flat AKNN warm start; returns deg, links, post-order tree, stats.
     precision "bf16": LocalJoin pairs filtered on BF16 tensor-core tiles, kept
     pairs recomputed in FP32 (identical graph); "fp32": CUDA cores only.
@@ -113,6 +127,8 @@ def graph_build(ctx: Context, lifted: np.ndarray, warm_ids: np.ndarray, degree=4
     edge_c = edge_policy_c(edge)
     if edge_c is not None:
         gp.edge = C.addressof(edge_c)
+    if vamana is not None:  # an anqi.vamana.VamanaParams (its passes and width win)
+        vamana_params(gp, vamana)
     deg = np.empty(n, np.uint32)
     links = np.empty((n, degree), np.uint32)
     st = BuildStats()

@@ -10,12 +10,11 @@
 // verifier (compact LRQ forms, rank-M only, float32 residuals, exact_f32,
 // analytic rank-M): the same argv, environment, prefix files, caches (file
 // names and identity keys, so a cache written by either program is found by
-// the other), stdout result lines and exit codes.  The global Vamana refine
-// (ANQI_VAMANA, styles global and old) and the edge policies of the prune
-// (ANQI_EDGE_POLICY and its options) run on the device too.  Configurations
-// outside that path (rank-M or original geometry, integrated verifier, the
-// batched Vamana style, fixed-k lift, recheck) exit 2 with a message naming
-// the setting.
+// the other), stdout result lines and exit codes.  The Vamana refine
+// (ANQI_VAMANA, the global passes and the batched style) and the edge policies
+// of the prune (ANQI_EDGE_POLICY and its options) run on the device too.
+// Configurations outside that path (rank-M or original geometry, integrated
+// verifier, fixed-k lift, recheck) exit 2 with a message naming the setting.
 //
 // Differences of mechanism, not of result: the graph build, lift, LRQ
 // encode/materialize, search, postfilter and evaluation run on the device;
@@ -797,11 +796,13 @@ static int run(int argc, char** argv) {
         die(2, "[rknn] ANQI_RECHECK cannot be mixed with an independent postfilter verifier; select "
                "ANQI_RADIUS_MODE=exact_f32 for the exact component comparison");
     if (std::getenv("ANQI_REUSE_ORIG_KNN")) not_here("ANQI_REUSE_ORIG_KNN");
-    // the global Vamana refine (index.h:1262-1285); the batched variant is not built here
+    // the Vamana refine (index.h:1262-1285): global passes, or the batched style (:936-1065)
     uint32_t vamana_passes = 0, vamana_L = 128;
+    bool vamana_batch = false;
     if (std::getenv("ANQI_VAMANA")) {
-        const std::string style = env_or("ANQI_VAMANA_STYLE", "global");
-        if (style != "global" && style != "old") not_here("ANQI_VAMANA_STYLE=" + style);
+        const char* sv = std::getenv("ANQI_VAMANA_STYLE");
+        const std::string style = sv ? sv : "global";
+        vamana_batch = style != "global" && style != "old";
         vamana_passes = (uint32_t)std::max(0, std::atoi(env_or("ANQI_VAMANA_PASS", "2").c_str()));
         vamana_L = (uint32_t)std::max(1, std::atoi(env_or("ANQI_VAMANA_L", "128").c_str()));
         if (vamana_L > 1024) die(2, "[rknn] ANQI_VAMANA_L=%u exceeds the device beam limit 1024", vamana_L);
@@ -1090,6 +1091,50 @@ static int run(int argc, char** argv) {
         gp.precision = env_or("ANQI_B200_PRECISION", "bf16") == "fp32" ? 0u : 1u;
         gp.vamana_passes = vamana_passes;
         gp.vamana_L = vamana_L;
+        if (vamana_batch) {
+            // vamana_batch_refine's settings (index.h:939-951) and entry (choose_vamana_entry, :190-222)
+            auto envd = [](const char* k, double d) { const char* v = std::getenv(k); return v ? std::atof(v) : d; };
+            auto envi = [](const char* k, int d) { const char* v = std::getenv(k); return v ? std::atoi(v) : d; };
+            gp.vamana_batch = 1;
+            gp.vamana_batch_frac = envd("ANQI_VAMANA_BATCH_FRAC", 0.02);
+            gp.vamana_max_batch = (uint64_t)(int64_t)envi("ANQI_VAMANA_MAX_BATCH", 1000000);
+            gp.vamana_batch_base = envd("ANQI_VAMANA_BATCH_BASE", 2.0);
+            const char* ea = std::getenv("ANQI_VAMANA_EARLY_ALPHA");
+            gp.vamana_early_alpha = ea ? (float)std::atof(ea) : 1.0f;
+            gp.vamana_early_alpha_one = envi("ANQI_VAMANA_EARLY_ALPHA_ONE", 1) != 0;
+            const char* ev = std::getenv("ANQI_VAMANA_ENTRY");
+            uint32_t entry = 0;
+            if (ev && *ev) {
+                const std::string es(ev);
+                if (es == "medoid" || es == "centroid") {
+                    size_t sample = (size_t)envi("ANQI_VAMANA_ENTRY_SAMPLE", (int)std::min<uint64_t>(n, 100000));
+                    sample = std::max<size_t>(1, std::min<size_t>(sample, n));
+                    std::vector<double> mean(dim, 0.0);
+                    const size_t step = std::max<size_t>(1, n / sample);
+                    for (size_t t = 0; t < sample; t++)
+                        for (size_t j = 0; j < dim; j++) mean[j] += (double)lifted[((t * step) % n) * dim + j];
+                    for (size_t j = 0; j < dim; j++) mean[j] /= (double)sample;
+                    double bestd = std::numeric_limits<double>::infinity();
+                    for (size_t t = 0; t < sample; t++) {
+                        const size_t id = (t * step) % n;
+                        double dd = 0.0;
+                        for (size_t j = 0; j < dim; j++) {
+                            const double z = (double)lifted[id * dim + j] - mean[j];
+                            dd += z * z;
+                        }
+                        if (dd < bestd) {
+                            bestd = dd;
+                            entry = (uint32_t)id;
+                        }
+                    }
+                } else {
+                    char* endp = nullptr;
+                    const unsigned long long id = std::strtoull(ev, &endp, 10);
+                    if (endp != ev && n > 0) entry = (uint32_t)(id % n);
+                }
+            }
+            gp.vamana_entry = entry;
+        }
         // the edge policy of the prunes (the graph folder of the postfilter
         // placement is the graph cache directory, rknn_query.cpp:1947)
         EdgePolicyHost edge;

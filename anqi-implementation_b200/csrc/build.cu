@@ -104,6 +104,9 @@ struct GatherParams {
     // and its size to the dump buffers instead of pruning it
     uint64_t row_base;
     uint32_t row_count;
+    // Vamana mode: also append the row's current links (the batched style,
+    // append_current_edges, index.h:759-765)
+    uint32_t cur_append;
     float* dump_d;
     uint32_t* dump_i;
     uint32_t* dump_n;
@@ -268,7 +271,7 @@ __device__ __forceinline__ void dump_pool(const GatherParams& p, uint32_t t, con
 // mode over rows renumbered for locality (p.perm), whose visits near the row
 // go to a per-warp window bitmap (separate instances, so each mode keeps its
 // registers and occupancy)
-template <bool kIp, bool kVam = false, bool kRen = false, bool kDump = false>
+template <bool kIp, bool kVam = false, bool kRen = false, bool kDump = false, bool kRows = kDump>
 __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams p) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     const uint32_t slot = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -306,8 +309,8 @@ __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams 
         uint32_t row = 0;
         if (lane == 0) row = atomicAdd(p.next_row, 1u);
         row = __shfl_sync(kAll, row, 0);
-        if (row >= (kDump ? (uint64_t)p.row_count : p.n)) break;
-        const uint64_t i = kDump ? (p.row_order ? p.row_order[p.row_base + row] : p.row_base + row)
+        if (row >= (kRows ? (uint64_t)p.row_count : p.n)) break;
+        const uint64_t i = kRows ? (p.row_order ? p.row_order[p.row_base + row] : p.row_base + row)
                                  : (p.row_order ? p.row_order[row] : row);
         if (i >= p.n) {
             if (lane == 0) set_error(p.err, kDevBadId);
@@ -491,6 +494,25 @@ __global__ void __launch_bounds__(128, kVam ? 5 : 7) gather_kernel(GatherParams 
             for (uint32_t c0 = 0; c0 < p.K; c0 += 32) {
                 const uint32_t t = c0 + lane;
                 const uint32_t j = t < p.K ? p.g_ids[i * p.K + t] : kEmpty;
+                const bool ok = j < p.n && j != (uint32_t)i;
+                const unsigned b = __ballot_sync(kAll, ok);
+                if (ok) ni[__popc(b & lane_lt_mask())] = j;
+                __syncwarp();
+                const uint32_t m = __popc(b);
+                if (m == 0) continue;
+                batch_d2<kIp>(p, i, ni, nd, m, gw, gt);
+                if (lane < m && npool + lane < p.pool_cap) {
+                    pd[npool + lane] = nd[lane];
+                    pi[npool + lane] = ni[lane];
+                }
+                npool += m;
+                __syncwarp();
+            }
+            // append_current_edges (index.h:759-765): the row's links at the batch's start
+            const uint32_t cdeg = p.cur_append ? min(p.cur_deg[i], p.cur_M) : 0u;
+            for (uint32_t c0 = 0; c0 < cdeg; c0 += 32) {
+                const uint32_t t = c0 + lane;
+                const uint32_t j = t < cdeg ? p.cur_links[i * p.cur_M + t] : kEmpty;
                 const bool ok = j < p.n && j != (uint32_t)i;
                 const unsigned b = __ballot_sync(kAll, ok);
                 if (ok) ni[__popc(b & lane_lt_mask())] = j;
@@ -1264,21 +1286,29 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
     if (smem > 227 * 1024) return fail(c, ANQI_ERR_ARGS, "explore range %u too large", p.ef);
     const bool policy = c->edge.active && (p.mode == kModeSelect || p.mode == kModeCommit || p.mode == kModeVamana);
     if (policy && p.ip) return fail(c, ANQI_ERR_ARGS, "edge policies are an l2 graph option");
-    auto* kern = p.mode == kModeVamana ? (policy ? gather_kernel<false, true, false, true> : gather_kernel<false, true>)
+    // a subset of the work list: rows [row_base, row_base + row_count) of it
+    const bool sub = p.row_count != 0;
+    if (sub && (p.ip || ren)) return fail(c, ANQI_ERR_ARGS, "row subsets are a select / commit / Vamana option");
+    const uint64_t rb0 = sub ? p.row_base : 0, rc0 = sub ? p.row_count : p.n;
+    auto* kern = p.mode == kModeVamana ? (policy ? gather_kernel<false, true, false, true>
+                                                 : (sub ? gather_kernel<false, true, false, false, true>
+                                                        : gather_kernel<false, true>))
                  : p.ip                  ? gather_kernel<true>
                  : ren                   ? gather_kernel<false, false, true>
                  : policy                ? gather_kernel<false, false, false, true>
+                 : sub                   ? gather_kernel<false, false, false, false, true>
                                          : gather_kernel<false>;
     ANQI_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     ANQI_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps_per_block, smem));
     if (per_sm < 1) return fail(c, ANQI_ERR_DEVICE, "gather kernel does not fit on an SM");
-    uint32_t blocks = std::min<uint64_t>((uint64_t)per_sm * c->sm_count, (p.n + warps_per_block - 1) / warps_per_block);
+    uint32_t blocks = std::min<uint64_t>((uint64_t)per_sm * c->sm_count, (rc0 + warps_per_block - 1) / warps_per_block);
     const uint32_t slots = blocks * warps_per_block;
     const uint32_t words = (uint32_t)((p.n + 31) / 32);
     uint64_t need = (uint64_t)p.cap + p.K + max_rev + 64;
     if (p.mode == kModeCommit) need = p.M + max_rev + 64;
-    if (p.mode == kModeVamana) need = (uint64_t)p.ef * 128 + p.K + 64;  // every visit of an uncapped beam
+    if (p.mode == kModeVamana)  // every visit of an uncapped beam, g0, the current links
+        need = (uint64_t)p.ef * 128 + p.K + (p.cur_append ? p.cur_M : 0) + 64;
     const uint32_t pool_cap = p.mode == kModeAknn ? 1u : (uint32_t)std::min<uint64_t>(1ull << 30, 1ull << (64 - __builtin_clzll(need)));
     // per-slot scratch, kept by the context between builds (the first build
     // maps it; later ones reuse it)
@@ -1329,9 +1359,9 @@ static int run_gather(Ctx* c, GatherParams p, uint64_t max_rev, uint64_t* pool_t
         p.dump_n = c->pol_dump_n.as<uint32_t>();
         uint32_t* out = p.mode == kModeCommit ? p.links : p.O;
         uint32_t* out_deg = p.mode == kModeCommit ? p.deg : p.O_deg;
-        for (uint64_t r0 = 0; r0 < p.n; r0 += chunk) {
+        for (uint64_t r0 = rb0; r0 < rb0 + rc0; r0 += chunk) {
             p.row_base = r0;
-            p.row_count = (uint32_t)std::min<uint64_t>(chunk, p.n - r0);
+            p.row_count = (uint32_t)std::min<uint64_t>(chunk, rb0 + rc0 - r0);
             ANQI_CUDA(c, cudaMemsetAsync(p.next_row, 0, 4, c->stream));
             kern<<<blocks, 32 * warps_per_block, smem, c->stream>>>(p);
             ANQI_CUDA(c, cudaGetLastError());
@@ -1538,6 +1568,232 @@ static int run_vamana_pass(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t 
 }
 
 // Entries of every row from the context's entry tree (the last graph build's).
+// ------------------------------------------------- the batched Vamana style
+// index.h:936-1065.  The insertion order is the reference's: std::mt19937_64
+// seeded from one value (the 64-bit Mersenne Twister of Matsumoto and
+// Nishimura) and std::shuffle as GCC's library performs it on 32-bit ids --
+// Fisher-Yates from the front, two positions per bounded draw
+// (Brackett-Rozinsky and Lemire's batched ranged integers), each bounded draw
+// by Lemire's multiply-and-reject -- restated here.
+struct Mt64 {
+    uint64_t mt[312];
+    uint32_t idx = 312;
+    explicit Mt64(uint64_t seed) {
+        mt[0] = seed;
+        for (uint32_t i = 1; i < 312; i++) mt[i] = 6364136223846793005ull * (mt[i - 1] ^ (mt[i - 1] >> 62)) + i;
+    }
+    uint64_t next() {
+        if (idx >= 312) {
+            for (uint32_t i = 0; i < 312; i++) {
+                const uint64_t y = (mt[i] & 0xFFFFFFFF80000000ull) | (mt[(i + 1) % 312] & 0x7FFFFFFFull);
+                mt[i] = mt[(i + 156) % 312] ^ (y >> 1) ^ ((y & 1ull) ? 0xB5026F5AA96619E9ull : 0ull);
+            }
+            idx = 0;
+        }
+        uint64_t x = mt[idx++];
+        x ^= (x >> 29) & 0x5555555555555555ull;
+        x ^= (x << 17) & 0x71D67FFFEDA60000ull;
+        x ^= (x << 37) & 0xFFF7EEE000000000ull;
+        return x ^ (x >> 43);
+    }
+    uint64_t below(uint64_t range) {  // uniform in [0, range)
+        unsigned __int128 prod = (unsigned __int128)next() * range;
+        uint64_t low = (uint64_t)prod;
+        if (low < range) {
+            const uint64_t threshold = (0ull - range) % range;
+            while (low < threshold) {
+                prod = (unsigned __int128)next() * range;
+                low = (uint64_t)prod;
+            }
+        }
+        return (uint64_t)(prod >> 64);
+    }
+};
+
+static void shuffle_ids(std::vector<uint32_t>& a, Mt64& g) {
+    const uint64_t n = a.size();
+    if (n < 2) return;
+    uint64_t i = 1;
+    if (n % 2 == 0) std::swap(a[i++], a[g.below(2)]);
+    while (i < n) {
+        const uint64_t b1 = i + 2, x = g.below((i + 1) * b1);
+        std::swap(a[i++], a[x / b1]);
+        std::swap(a[i++], a[x % b1]);
+    }
+}
+
+// The batch's rows take their new links (write_ids for every batch row).
+__global__ void batch_write_kernel(const uint32_t* __restrict__ order, uint64_t floor_, uint32_t bsz,
+                                   const uint32_t* __restrict__ O, const uint32_t* __restrict__ Od, uint32_t M,
+                                   uint32_t* __restrict__ links, uint32_t* __restrict__ deg) {
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (uint64_t)bsz * M;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t node = order[floor_ + t / M];
+        const uint32_t j = (uint32_t)(t % M);
+        links[node * M + j] = O[node * M + j];
+        if (j == 0) deg[node] = Od[node];
+    }
+}
+
+// Reverse edges of the batch: counts per target, the targets touched (listed
+// once each, in any order), the largest count; then the sources per target.
+__global__ void batch_count_kernel(const uint32_t* __restrict__ order, uint64_t floor_, uint32_t bsz,
+                                   const uint32_t* __restrict__ O, const uint32_t* __restrict__ Od, uint32_t M,
+                                   uint64_t n, uint32_t* __restrict__ cnt, uint32_t* __restrict__ touched,
+                                   uint32_t* __restrict__ nt_max) {
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (uint64_t)bsz * M;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t node = order[floor_ + t / M];
+        const uint32_t j = (uint32_t)(t % M);
+        if (j >= Od[node]) continue;
+        const uint32_t dst = O[node * M + j];
+        if (dst >= n) continue;
+        const uint32_t old = atomicAdd(cnt + dst, 1u);
+        if (old == 0) touched[atomicAdd(nt_max, 1u)] = dst;
+        atomicMax(nt_max + 1, old + 1);
+    }
+}
+
+__global__ void batch_fill_kernel(const uint32_t* __restrict__ order, uint64_t floor_, uint32_t bsz,
+                                  const uint32_t* __restrict__ O, const uint32_t* __restrict__ Od, uint32_t M,
+                                  uint64_t n, const uint64_t* __restrict__ off, uint32_t* __restrict__ fill,
+                                  uint32_t* __restrict__ rev) {
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (uint64_t)bsz * M;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t node = order[floor_ + t / M];
+        const uint32_t j = (uint32_t)(t % M);
+        if (j >= Od[node]) continue;
+        const uint32_t dst = O[node * M + j];
+        if (dst >= n) continue;
+        rev[off[dst] + atomicAdd(fill + dst, 1u)] = (uint32_t)node;
+    }
+}
+
+__global__ void fill_u32_kernel(uint32_t* a, uint64_t n, uint32_t v) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        a[i] = v;
+}
+
+// vamana_batch_refine on the device graph (dl, dd: n x M, degrees), g0 = the
+// build's heaps (n x K).
+static int run_vamana_batch(Ctx* c, const DevBuf& dx, const DevBuf& dn, uint64_t n, uint32_t stride, uint32_t dim,
+                            const DevBuf& hid, uint32_t K, const anqi_graph_params& gp, DevBuf& dl, DevBuf& dd,
+                            uint64_t* pool_total) {
+    const int passes = (int)gp.vamana_passes;
+    const uint32_t M = gp.degree, Lb = gp.vamana_L ? gp.vamana_L : 128;
+    if (n == 0 || passes <= 0) return ANQI_OK;
+    double frac = gp.vamana_batch_frac;
+    if (frac <= 0.0) frac = 0.02;
+    const double mb = frac * (double)n;
+    uint64_t max_batch = std::min<uint64_t>((uint64_t)std::max(1.0, mb), gp.vamana_max_batch);
+    if (max_batch == 0) max_batch = n;
+    double base = gp.vamana_batch_base;
+    if (base <= 1.0) base = 2.0;
+    // the batches of a pass: [floor, ceiling) of the order
+    std::vector<std::pair<uint64_t, uint64_t>> batches;
+    uint64_t largest = 1;
+    for (uint64_t count = 0, inc = 0; count < n;) {
+        uint64_t floor_ = count, ceiling;
+        const double p0 = std::pow(base, (double)inc);
+        if (p0 <= (double)max_batch) {
+            floor_ = (uint64_t)p0 - 1;
+            ceiling = std::min<uint64_t>((uint64_t)std::pow(base, (double)(inc + 1)) - 1, n);
+        } else {
+            ceiling = std::min<uint64_t>(count + max_batch, n);
+        }
+        count = ceiling;
+        inc++;
+        if (ceiling <= floor_ || floor_ >= n) continue;
+        batches.push_back({floor_, ceiling});
+        largest = std::max(largest, ceiling - floor_);
+    }
+    if (largest * M > 0xFFFFFFFFull) return fail(c, ANQI_ERR_ARGS, "Vamana batch of %llu rows too large",
+                                                (unsigned long long)largest);
+    TmpBuf dord(c), dent(c), dO(c), dOd(c), cnt(c), fill(c), roff(c), rev(c), touched(c), ntm(c);
+    int rc;
+    const uint64_t tcap = std::min<uint64_t>(n, largest * M);
+    if ((rc = ensure(c, dord, n * 4)) || (rc = ensure(c, dent, n * 4)) || (rc = ensure(c, dO, n * M * 4ull)) ||
+        (rc = ensure(c, dOd, n * 4)) || (rc = ensure(c, cnt, n * 4)) || (rc = ensure(c, fill, n * 4)) ||
+        (rc = ensure(c, roff, (n + 1) * 8)) || (rc = ensure(c, rev, largest * M * 4ull + 4)) ||
+        (rc = ensure(c, touched, tcap * 4 + 4)) || (rc = ensure(c, ntm, 8)))
+        return rc;
+    const int blocks = c->sm_count * 8;
+    fill_u32_kernel<<<blocks, 256, 0, c->stream>>>(dent.as<uint32_t>(), n, gp.vamana_entry < n ? gp.vamana_entry : 0u);
+    ANQI_CUDA(c, cudaMemsetAsync(cnt.p, 0, n * 4, c->stream));
+    ANQI_CUDA(c, cudaMemsetAsync(fill.p, 0, n * 4, c->stream));
+    std::vector<uint32_t> order(n);
+    for (uint64_t i = 0; i < n; i++) order[i] = (uint32_t)i;
+    for (int pass = 0; pass < passes; pass++) {
+        const float alpha = (gp.vamana_early_alpha_one && pass + 1 < passes) ? gp.vamana_early_alpha : gp.alpha;
+        Mt64 g(gp.seed + 0x9e3779b97f4a7c15ull * (uint64_t)(pass + 1));
+        shuffle_ids(order, g);
+        if ((rc = h2d(c, dord, order.data(), n * 4))) return rc;
+        for (const auto& bt : batches) {
+            const uint64_t floor_ = bt.first;
+            const uint32_t bsz = (uint32_t)(bt.second - bt.first);
+            // the batch's rows: beam from the entry + g0 + current links, pruned -> O
+            GatherParams p = base_params(dx, dn, n, stride, dim);
+            p.g_ids = hid.as<uint32_t>();
+            p.K = K;
+            p.ef = Lb;
+            p.cap = 0xFFFFFFFFu;
+            p.mode = kModeVamana;
+            p.M = M;
+            p.alpha = alpha;
+            p.O = dO.as<uint32_t>();
+            p.O_deg = dOd.as<uint32_t>();
+            p.cur_links = dl.as<uint32_t>();
+            p.cur_deg = dd.as<uint32_t>();
+            p.cur_M = M;
+            p.cur_append = 1;
+            p.entry = dent.as<uint32_t>();
+            p.row_order = dord.as<uint32_t>();
+            p.row_base = floor_;
+            p.row_count = bsz;
+            if ((rc = run_gather(c, p, 0, pool_total))) return rc;
+            batch_write_kernel<<<blocks, 256, 0, c->stream>>>(dord.as<uint32_t>(), floor_, bsz, dO.as<uint32_t>(),
+                                                            dOd.as<uint32_t>(), M, dl.as<uint32_t>(),
+                                                            dd.as<uint32_t>());
+            // every row the batch now links to: its links + those batch rows, pruned in place
+            ANQI_CUDA(c, cudaMemsetAsync(ntm.p, 0, 8, c->stream));
+            batch_count_kernel<<<blocks, 256, 0, c->stream>>>(dord.as<uint32_t>(), floor_, bsz, dO.as<uint32_t>(),
+                                                            dOd.as<uint32_t>(), M, n, cnt.as<uint32_t>(),
+                                                            touched.as<uint32_t>(), ntm.as<uint32_t>());
+            ANQI_CUDA(c, cudaGetLastError());
+            if ((rc = device_scan(c, cnt.as<uint32_t>(), roff.as<uint64_t>(), n))) return rc;
+            batch_fill_kernel<<<blocks, 256, 0, c->stream>>>(dord.as<uint32_t>(), floor_, bsz, dO.as<uint32_t>(),
+                                                           dOd.as<uint32_t>(), M, n, roff.as<uint64_t>(),
+                                                           fill.as<uint32_t>(), rev.as<uint32_t>());
+            ANQI_CUDA(c, cudaGetLastError());
+            uint32_t nt[2] = {0, 0};
+            if ((rc = d2h(c, nt, ntm, 8)) || (rc = sync(c))) return rc;
+            if (nt[0] > 0) {
+                GatherParams q = base_params(dx, dn, n, stride, dim);
+                q.mode = kModeCommit;
+                q.K = 1;
+                q.ef = 4;
+                q.M = M;
+                q.alpha = alpha;
+                q.O = dl.as<uint32_t>();
+                q.O_deg = dd.as<uint32_t>();
+                q.rev_off = roff.as<uint64_t>();
+                q.rev_ids = rev.as<uint32_t>();
+                q.links = dl.as<uint32_t>();
+                q.deg = dd.as<uint32_t>();
+                q.row_order = touched.as<uint32_t>();
+                q.row_base = 0;
+                q.row_count = nt[0];
+                if ((rc = run_gather(c, q, nt[1], nullptr))) return rc;
+            }
+            // counts and fill cursors back to zero for the next batch
+            fill_u32_kernel<<<blocks, 256, 0, c->stream>>>(cnt.as<uint32_t>(), n, 0u);
+            fill_u32_kernel<<<blocks, 256, 0, c->stream>>>(fill.as<uint32_t>(), n, 0u);
+            ANQI_CUDA(c, cudaGetLastError());
+        }
+    }
+    return sync(c);
+}
+
 static int vamana_entries(Ctx* c, const DevBuf& dx, uint64_t n, uint32_t stride, uint32_t dim, DevBuf& ent) {
     const uint32_t nn = c->t_nodes;
     if (nn == 0 || c->t_dim != dim) return fail(c, ANQI_ERR_ARGS, "no entry tree for the Vamana refine");
@@ -1714,6 +1970,25 @@ int anqi_graph_commit_policy(anqi_ctx* h, const float* x, uint64_t n, uint32_t d
     return sync(c);
 }
 
+int anqi_graph_vamana_batch_refine(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, uint32_t* links,
+                                   uint32_t* deg, const uint32_t* g0, uint32_t K, const anqi_graph_params* gp) {
+    if (!h || !x || !links || !deg || !g0 || !gp || n == 0 || dim == 0 || K == 0 || gp->degree == 0 ||
+        gp->degree > 64 || (gp->vamana_L ? gp->vamana_L : 128) > 1024)
+        return ANQI_ERR_ARGS;
+    Ctx* c = &h->c;
+    cudaSetDevice(c->device);
+    const uint32_t xs = round_up(dim, 8), M = gp->degree;
+    TmpBuf dx(c), dn(c), dl(c), dd(c), dg(c);
+    PolicyScope scope{c};
+    int rc;
+    if ((rc = set_edge_policy(c, gp->edge, n)) || (rc = upload_rows(c, dx, dn, x, n, dim, xs)) ||
+        (rc = h2d(c, dl, links, n * M * 4ull)) || (rc = h2d(c, dd, deg, n * 4)) || (rc = h2d(c, dg, g0, n * K * 4ull)))
+        return rc;
+    if ((rc = run_vamana_batch(c, dx, dn, n, xs, dim, dg, K, *gp, dl, dd, nullptr))) return rc;
+    if ((rc = d2h(c, links, dl, n * M * 4ull)) || (rc = d2h(c, deg, dd, n * 4))) return rc;
+    return sync(c);
+}
+
 int anqi_graph_vamana_select(anqi_ctx* h, const float* x, uint64_t n, uint32_t dim, const uint32_t* links,
                              const uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, const uint32_t* entry,
                              uint32_t Lb, float alpha, uint32_t* O, uint32_t* O_deg) {
@@ -1885,7 +2160,9 @@ int anqi_graph_build_finish(anqi_ctx* h, uint32_t* deg, uint32_t* links, anqi_bu
                                ord_env && ord_env[0] == '0' ? nullptr : g.order.as<uint32_t>(), &gather_kernel_ms);
     // optional global Vamana refine (index.h:1262-1285): every row's entry
     // from the entry tree, then `vamana_passes` passes over the graph
-    if (!rc && gp.vamana_passes > 0) {
+    if (!rc && gp.vamana_passes > 0 && gp.vamana_batch)
+        rc = run_vamana_batch(c, g.dx, g.dn, n, g.xs, g.dim, g.hid, gp.nn_k, gp, dl, dd, &pool_total);
+    else if (!rc && gp.vamana_passes > 0) {
         TmpBuf ent(c);
         rc = vamana_entries(c, g.dx, n, g.xs, g.dim, ent);
         for (uint32_t pass = 0; pass < gp.vamana_passes && !rc; pass++)

@@ -254,6 +254,14 @@ typedef struct {
                                 the commit (include/index.h:1262-1285); 0 = none */
     uint32_t vamana_L;       /* ANQI_VAMANA_L: the refine's beam width (128; 0 = 128) */
     const anqi_edge_policy* edge;  /* the prune's edge policy (select, commit, Vamana); NULL = default */
+    /* ANQI_VAMANA_STYLE=batch (include/index.h:936-1065) in place of the global passes: */
+    uint32_t vamana_batch;         /* 1: the batched style */
+    uint32_t vamana_entry;         /* ANQI_VAMANA_ENTRY resolved to a row (0; "medoid" resolved by the caller) */
+    double vamana_batch_frac;      /* ANQI_VAMANA_BATCH_FRAC (0.02) */
+    uint64_t vamana_max_batch;     /* ANQI_VAMANA_MAX_BATCH (1000000) */
+    double vamana_batch_base;      /* ANQI_VAMANA_BATCH_BASE (2) */
+    float vamana_early_alpha;      /* ANQI_VAMANA_EARLY_ALPHA (1): alpha of every pass but the last ... */
+    uint32_t vamana_early_alpha_one;  /* ... when ANQI_VAMANA_EARLY_ALPHA_ONE (1) is non-zero */
 } anqi_graph_params;
 
 int anqi_graph_build(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* warm_ids,
@@ -306,6 +314,17 @@ int anqi_graph_commit_policy(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t
  * pruned as anqi_graph_select does -> O, O_deg (then anqi_graph_commit).
  * anqi_graph_params.vamana_passes runs whole passes inside anqi_graph_build,
  * the entries from the build's entry tree (ties at the margin to the left). */
+/* The batched Vamana refine (include/index.h:936-1065) on a graph (links
+ * n x M, deg; refined in place): per pass the rows in a shuffled order
+ * (std::mt19937_64 from seed + 0x9e3779b97f4a7c15 (pass + 1), std::shuffle's
+ * order restated), cut into batches of growing size; each batch's rows prune
+ * a beam from the single entry over the graph as it was at the batch's start,
+ * their g0 list (n x K) and current links, take the result as their links,
+ * and every row they now link to prunes its links plus those rows.  Uses
+ * p->degree (M), alpha, seed, edge, vamana_L, vamana_passes and the
+ * vamana_batch* / vamana_entry / vamana_early_alpha* fields. */
+int anqi_graph_vamana_batch_refine(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, uint32_t* links,
+                                   uint32_t* deg, const uint32_t* g0, uint32_t K, const anqi_graph_params* p);
 int anqi_graph_vamana_select(anqi_ctx* ctx, const float* x, uint64_t n, uint32_t dim, const uint32_t* links,
                              const uint32_t* deg, uint32_t M, const uint32_t* g0, uint32_t K, const uint32_t* entry,
                              uint32_t Lb, float alpha, uint32_t* O, uint32_t* O_deg);

@@ -172,7 +172,7 @@ def test_rknn_bad_inputs_exit_3(tmp_path):
     ("ANQI_GRAPH_GEOMETRY", "original"), ("ANQI_GRAPH_GEOMETRY", "bogus"), ("ANQI_RADIUS_MODE", "knots"),
     ("ANQI_RADIUS_MODE", "rankm_resid_u8_floor"), ("ANQI_RADIUS_MODE", "analytic_rankm"),
     ("ANQI_VERIFIER_PLACEMENT", "integrated"), ("ANQI_VERIFIER_PLACEMENT", "x"), ("ANQI_RECHECK", "1"),
-    ("ANQI_SPECIFIC", "1"), ("ANQI_VAMANA_STYLE", "batch"),
+    ("ANQI_SPECIFIC", "1"),
     ("ANQI_RQ_OBJECTIVE", "predicate_boundary"), ("ANQI_CANDIDATE_ENVELOPE", "verifier"),
     ("ANQI_RANKM_SLACK", "-1"), ("ANQI_RADIUS_RELAX", "0.1"),
 ])

@@ -378,13 +378,14 @@ def test_rknn_query_scale_profile_degree20_kpivot10(tmp_path):
 
 
 @pytest.mark.skipif(not tc.REF_BIN.exists(), reason="reference binaries not built")
-def test_rknn_query_vamana_global(tmp_path):
-    """ANQI_VAMANA=1 (global style, 2 passes of L = 128): the graph cache is
-    named as the reference names it, recall is within 0.05 of the reference's
-    own Vamana-refined build, and on the reference's refined graph the result
-    lines are the reference's."""
+@pytest.mark.parametrize("style", ["global", "batch"])
+def test_rknn_query_vamana(tmp_path, style):
+    """ANQI_VAMANA=1 (the global passes, or the batched style; 2 passes of
+    L = 128): the graph cache is named as the reference names it, recall is
+    within 0.05 of the reference's own Vamana-refined build, and on the
+    reference's refined graph the result lines are the reference's."""
     pfx, env, z = tc.sample_prefix(tmp_path, 32)
-    env = dict(env, ANQI_VAMANA="1")
+    env = dict(env, ANQI_VAMANA="1", ANQI_VAMANA_STYLE=style)
     ref_env = {k: v for k, v in os.environ.items() if not k.startswith("ANQI_")}
     ref_env.update(env, OMP_NUM_THREADS="1", ANQI_GRAPH_CACHE_DIR=str(tmp_path / "ref" / "graph"),
                    ANQI_VERIFIER_CACHE_DIR=str(tmp_path / "ref" / "verifier"))
