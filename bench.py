@@ -88,6 +88,9 @@ def parse():
                     help="queries of the batching form (per-query k and L, CUDA graph); 0 skips it")
     ap.add_argument("--batch", type=int, default=10_000)
     ap.add_argument("--batched-reps", type=int, default=2, help="timed passes over the batching-form queries")
+    ap.add_argument("--graph-options", type=int, default=200_000,
+                    help="rows of the mixture on which the graph options (both Vamana styles, an edge "
+                         "policy) are built and queried beside the default graph; 0 skips it")
     ap.add_argument("--shape960", type=int, default=1_000_000,
                     help="rows of the batching form's second shape (L2-normalised N(0,1), d = 960) run after the "
                          "main line, with QPS and recall; 0 skips it")
@@ -384,6 +387,65 @@ def run_plain(a, dev, ix, query, ks, steps, warmup):
             "visited_table": [0, 4096], "shape": {"warps_per_block": 4, "candidate_tile": 8}}
 
 
+def run_graph_options(ctx, a):
+    """The G48 build's options on an n-row mixture index: the default graph,
+    the global Vamana refine, the batched Vamana refine and the ball_rng edge
+    policy (its residual table: each object's decoded LRQ residual at k = 10,
+    50, 100, the table the reference's integrated verifier writes).  Per
+    graph: device build seconds, then recall / precision and QPS of one
+    launch over the queries at k = 10, 50, 100 (L = 128), against the exact
+    RkNN."""
+    import dataclasses
+    from anqi import pipeline, vamana, edge_policy
+    n, nq = a.graph_options, 2000
+    base, query = pipeline.mixture(n, a.d, nq, seed=20260819)
+    ix = pipeline.build_index(ctx, base, log=lambda *m: None)
+    ks = [10, 50, 100]
+    _, ex = pipeline.exact_thresholds(ctx, base, 100, method="tc", hints=ix.aknn_ids)
+    gt = {k: pipeline.rknn_ground_truth(ctx, base, query, ex[:, k - 1], method="tc") for k in ks}
+    # the residual table of the policy: materialized threshold minus the rank-M reconstruction
+    recon = ix.mu[None, :].astype(np.float64) + ix.coeff.astype(np.float64) @ ix.basis.astype(np.float64)
+    resid = np.zeros((n, 100), np.float32)
+    for k in ks:
+        resid[:, k - 1] = (ctx.lrq_materialize(ix.coeff, ix.codes, ix.mu, ix.basis, ix.codebook, k)
+                           - recon[:, k - 1]).astype(np.float32)
+    pol = edge_policy.EdgePolicy("ball_rng", flags=edge_policy.BALL | edge_policy.PURE, ks=ks, nk=100, budget=16,
+                                 occlude_all=True, auto_candidates=48, auto_max_swaps=48, lam=1.0,
+                                 scale2=float(ix.scale) ** 2, resid=resid)
+    variants = {
+        "default": {},
+        "vamana_global": {"vamana": vamana.from_env({"ANQI_VAMANA": "1"})},
+        "vamana_batch": {"vamana": vamana.from_env({"ANQI_VAMANA": "1", "ANQI_VAMANA_STYLE": "batch"}, ix.lifted)},
+        "edge_ball_rng": {"edge": pol},
+    }
+    out = {"n": n, "nq": nq, "L": a.L}
+    qb = np.ascontiguousarray(np.tile(query, (len(ks), 1)))
+    kb = np.repeat(np.array(ks, np.uint32), nq)
+    for name, kw in variants.items():
+        t0 = time.perf_counter()
+        deg, links, tree, st = pipeline.graph_build(ctx, ix.lifted, ix.aknn_ids, **kw)
+        build_s = time.perf_counter() - t0
+        gix = dataclasses.replace(ix, deg=deg, links=links, tree=tree)
+        pipeline.load_index(ctx, gix, ks)
+        res = {"graph_build_s": round(build_s, 3), "graph_library_ms": round(st["total_ms"], 1),
+               "mean_degree": round(float(deg.mean()), 2), "per_k": {}}
+        for k in ks:
+            ctx.query_upload(query, k, a.L)
+            ctx.query_run()
+            e = ctx.query_evaluate(gt[k][0], gt[k][1])
+            res["per_k"][k] = {"recall": round(e["recall"], 6), "precision": round(e["precision"], 6)}
+        ctx.query_upload(qb, kb, np.full(len(kb), a.L, np.uint32))
+        for _ in range(3):
+            ctx.query_run_graph()
+        ctx.timer_start()
+        for _ in range(10):
+            ctx.query_run_graph()
+        ms = ctx.timer_stop()
+        res["qps"] = round(10 * len(kb) / (ms / 1e3), 1)
+        out[name] = res
+    return out
+
+
 def run_shape960(ctx, a, steps, warmup):
     """The batching form's second shape: n x 960 L2-normalised N(0,1) rows and
     10,000 queries, the whole index built here (AKNN source with the K-chunked
@@ -644,6 +706,12 @@ def run_ours(a, rank, world, local):
         finally:
             if not a.keep:
                 shutil.rmtree(tmp, ignore_errors=True)
+    if a.graph_options and world == 1 and a.data == "mixture":
+        # after the main line's measurements: another index replaces it
+        try:
+            line["graph_options"] = run_graph_options(ctx, a)
+        except Exception as e:  # reported, not fatal: the main line stands
+            line["graph_options"] = {"error": f"{type(e).__name__}: {e}"}
     if a.shape960 and world == 1 and a.d == 128:
         # after the main line's measurements: the second shape replaces the index
         try:
