@@ -310,10 +310,8 @@ int build_forest(Ctx* c, const float* d_x, uint64_t n, uint32_t dim, uint32_t st
             next.push_back({sn.tree, L, sn.start, nl[s], split_depth[s] + 1});
             next.push_back({sn.tree, R, sn.start + nl[s], sn.count - nl[s], split_depth[s] + 1});
         }
-        // keep breadth-first order per tree: sort by (tree, local)
-        std::stable_sort(next.begin(), next.end(), [](const Active& a, const Active& b) {
-            return a.tree < b.tree || (a.tree == b.tree && a.local < b.local);
-        });
+        // `next` is already in (tree, local) order, breadth-first per tree: the
+        // splits come in that order and each takes the next two numbers of its tree
         active.swap(next);
     }
     for (uint32_t t = 0; t < trees; t++) out.n_nodes[t] = next_local[t];
