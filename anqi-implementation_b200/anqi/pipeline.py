@@ -80,7 +80,7 @@ def aknn_build(ctx: Context, base: np.ndarray, k=100, leaf=500, trees=64, ef=600
     """build_aknn_source: returns ids (n x k) and the record keys: max(0, d) for
     l2, d - 1 = -<a, b> for ip (build_aknn_source.cpp:125-126).
     precision "bf16": init_knn leaf distances on BF16 tensor-core tiles with FP32
-    recheck; "fp32": CUDA cores.  Both give identical output (ip runs FP32)."""
+    recheck (both metrics); "fp32": CUDA cores.  Both give identical output."""
     base = np.ascontiguousarray(base, np.float32)
     n, d = base.shape
     p = AknnParams(k, leaf, trees, ef, 8, seed, nn_iters, nn_sample, {"fp32": 0, "bf16": 1}[precision],

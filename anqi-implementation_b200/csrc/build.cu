@@ -1008,8 +1008,9 @@ __global__ void __launch_bounds__(256) leaf_topk_kernel(const float* __restrict_
 }
 
 // Merges one tree's tensor-core init_knn candidates (tc_leaf_candidates) into
-// every row's list: flagged keys are recomputed in FP32 in the AVX lane order
-// (the leaf_topk_kernel arithmetic), candidates that cannot enter are dropped,
+// every row's list: flagged keys are recomputed in FP32 in the leaf_topk_kernel
+// arithmetic (mode kKeyL2: the AVX lane order; kKeyIpDist: 1 - <a, b> summed
+// in sequence), candidates that cannot enter are dropped,
 // the rest sorted and merged with duplicates of list entries removed.  The
 // list stays the K smallest unique (key, id) of all candidates seen, whatever
 // their order.  Resets cnt.  One warp per row.
@@ -1020,7 +1021,8 @@ __global__ void __launch_bounds__(128) leaf_merge_kernel(const float* __restrict
                                                          const uint32_t* __restrict__ cid,
                                                          const float* __restrict__ ckey, uint32_t K,
                                                          float* __restrict__ kd, uint32_t* __restrict__ ki,
-                                                         uint32_t* __restrict__ ksz, uint32_t* __restrict__ err) {
+                                                         uint32_t* __restrict__ ksz, uint32_t* __restrict__ err,
+                                                         uint32_t mode) {
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5, gt = lane & 3u, gw = lane >> 2;
     float* ld = reinterpret_cast<float*>(g_build_smem) + (size_t)wib * (4 * K + 128);
     uint32_t* li = reinterpret_cast<uint32_t*>(ld + 2 * K);
@@ -1055,7 +1057,12 @@ __global__ void __launch_bounds__(128) leaf_merge_kernel(const float* __restrict
                 flag |= (id & kRecheck) != 0;
             }
             __syncwarp();
-            if (__any_sync(kAll, flag)) {
+            if (__any_sync(kAll, flag) && mode == kKeyIpDist) {
+                // the ip distance in the sequential order of leaf_topk_kernel
+                for (uint32_t t = lane; t < bm; t += 32)
+                    if (cid[sl * cap + c0 + t] & kRecheck) wd[t] = ip_dist_seq(xi, x + (uint64_t)wi[t] * stride, dim);
+                __syncwarp();
+            } else if (__any_sync(kAll, flag)) {
                 for (uint32_t r0 = 0; r0 < bm; r0 += 8) {
                     const uint32_t idx = r0 + gw;
                     const bool ok = idx < bm;
@@ -2349,7 +2356,7 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
             }
         // the tensor-core tiles: query tile resident up to 256 (padded)
         // dimensions, K-chunked up to 1024
-        if (ap->precision == 1 && !ip && tc_padded_dim(d) != 0) {
+        if (ap->precision == 1 && tc_padded_dim(d) != 0) {
             // BF16 tensor-core leaf tiles: candidates per tree, then the merge
             TcPrep tp;
             // candidate buffers (n x cap entries; GBs at 1M) are kept by the
@@ -2401,12 +2408,13 @@ int anqi_aknn_build(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, cons
                     const BatchPlan& bp = plan[b];
                     rc = tc_leaf_filter(c, tp, dx.as<float>(), dn.as<float>(), n, xs, d, f.perm.as<uint32_t>(),
                                         dtiles.as<LeafTile>() + bp.t0, bp.nt, kd.as<float>(), ksz.as<uint32_t>(), K,
-                                        ccnt.as<uint32_t>(), cap, cid.as<uint32_t>(), ckey.as<float>(), bp.base);
+                                        ccnt.as<uint32_t>(), cap, cid.as<uint32_t>(), ckey.as<float>(), bp.base,
+                                        ip ? kKeyIpDist : kKeyL2);
                     if (rc) break;
                     leaf_merge_kernel<<<c->sm_count * 8, 32 * wpb, msmem, c->stream>>>(
                         dx.as<float>(), dn.as<float>(), n, xs, d, f.perm.as<uint32_t>(), bp.base, bp.nslots,
                         ccnt.as<uint32_t>(), cap, cid.as<uint32_t>(), ckey.as<float>(), K, kd.as<float>(),
-                        ki.as<uint32_t>(), ksz.as<uint32_t>(), c->err.as<uint32_t>());
+                        ki.as<uint32_t>(), ksz.as<uint32_t>(), c->err.as<uint32_t>(), ip ? kKeyIpDist : kKeyL2);
                     rc = cu(cudaGetLastError(), "leaf_merge_kernel");
                 }
                 if (!rc) rc = check_device_error(c, "tensor-core init_knn");

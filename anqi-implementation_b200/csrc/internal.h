@@ -273,11 +273,12 @@ int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* 
 // trip: the 128-row tiles of a batch's leaves (appended to tiles; a leaf
 // longer than cap + 1 is an argument error), then the filter over ntiles
 // tiles already on the device (errors are left in the device error word).
+// key_mode 0: the l2 key; 1: the ip metric's 1 - <a, b>.
 int tc_leaf_tiles(Ctx* c, const std::vector<LeafRef>& leaves, uint32_t cap, std::vector<LeafTile>& tiles);
 int tc_leaf_filter(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs,
                    uint32_t d, const uint32_t* d_members, const LeafTile* d_tiles, size_t ntiles,
                    const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
-                   uint32_t* out_id, float* out_key, uint64_t pos_base);
+                   uint32_t* out_id, float* out_key, uint64_t pos_base, uint32_t key_mode);
 
 // Edge policy of the next select / commit / Vamana prunes (nullptr or flags 0:
 // the default prune; tables copied to the device), and its release.

@@ -14,7 +14,10 @@
 //   eps = 2 (|dq| |x| + |q| |dx| + |dq| |dx|)      bf16 rounding of the rows
 //       + 4 g (|q~| |x~| + |q| |x|)                 FP32 accumulation, g = 2 d 2^-24
 //       + 4 u (|q|^2 + |x|^2 + 2 |q| |x|)           the key's own roundings, u = 2^-24
-// (|dq| = |q - bf16(q)|).  Candidates are recomputed in the reference's FP32
+// (|dq| = |q - bf16(q)|).  The ip metric's keys (1 - <q, x> for the AKNN
+// source, -<q, x> for the ground truth) hold the product once: half the
+// first two terms, and 4 u (1 + |q| |x|) for the rounding of the key.
+// Candidates are recomputed in the reference's FP32
 // order, so accept decisions and keys equal the FP32 path.  When both rows
 // hold integers of magnitude <= 256 and d <= 128, bf16 and every partial
 // sum are exact and key~ == key32: eps = 0 and no recheck is needed.
@@ -195,6 +198,9 @@ struct FilterParams {
     // approximate key and kRecheck in the id, for recheck_rows_kernel (a
     // 4-thread group per pair instead of one thread here)
     int defer_recheck;
+    // the key: 0 = |q|^2 + |x|^2 - 2 <q, x> (l2), 1 = 1 - <q, x> (the ip
+    // metric's AKNN distance), 2 = -<q, x> (the ip metric's ground-truth key)
+    uint32_t key_mode;
 };
 
 constexpr uint32_t kStages = 2;  // base-tile ring; two CTAs fit an SM (shared memory, TMEM)
@@ -337,10 +343,19 @@ __global__ void __launch_bounds__(kFilterThreads, kWide ? 1 : 2) tc_filter_kerne
                                                 : __int_as_float(0x7f800000);
     const float u = 5.9604645e-8f;        // 2^-24
     const float g = 2.0f * p.dp * u;
-    const float ca = 2.f * qer + 4.f * g * (qnm + qer) + 4.f * g * qnm + 8.f * u * qnm;
-    const float cb = 2.f * qnm + 2.f * qer + 4.f * g * (qnm + qer);
-    const float cc = 4.f * u;
-    const float cd = 4.f * u * qn;
+    // ip keys carry <q, x> once instead of twice: half the product terms; the
+    // rounding of 1 - <q, x> (or none for -<q, x>) is below 4 u (1 + |q| |x|)
+    const bool l2k = p.key_mode == 0;
+    const float kh = l2k ? 1.f : 0.5f;
+    const float ca = kh * (2.f * qer + 4.f * g * (qnm + qer) + 4.f * g * qnm + 8.f * u * qnm);
+    const float cb = kh * (2.f * qnm + 2.f * qer + 4.f * g * (qnm + qer));
+    const float cc = l2k ? 4.f * u : 0.f;
+    const float cd = l2k ? 4.f * u * qn : 4.f * u;
+    // key~ from the accumulator, in the FP32 steps of the reference's key
+    auto approx_key = [&](float xnc, float acc) {
+        return l2k ? __fsub_rn(__fadd_rn(qn, xnc), __fmul_rn(2.0f, acc))
+                   : (p.key_mode == 1 ? __fsub_rn(1.0f, acc) : -acc);
+    };
     const float* qrow = p.q32 + (row_ok ? my_row : 0) * p.xs;
     // eps <= epsmax for every column of this row (eps grows with the column's
     // |x|, |x - bf16(x)| and norm; exact rows against all-exact columns: 0)
@@ -368,7 +383,7 @@ __global__ void __launch_bounds__(kFilterThreads, kWide ? 1 : 2) tc_filter_kerne
                 const float xa[4] = {xn4.x, xn4.y, xn4.z, xn4.w}, ta[4] = {th4.x, th4.y, th4.z, th4.w};
 #pragma unroll
                 for (uint32_t q = 0; q < 4; q++) {
-                    const float approx = __fsub_rn(__fadd_rn(qn, xa[q]), __fmul_rn(2.0f, v[k + q]));
+                    const float approx = approx_key(xa[q], v[k + q]);
                     keep |= (approx - epsmax <= ta[q] ? 1u : 0u) << (k + q);
                 }
             }
@@ -381,7 +396,7 @@ __global__ void __launch_bounds__(kFilterThreads, kWide ? 1 : 2) tc_filter_kerne
 #pragma unroll
                 for (uint32_t q = 0; q < 32; q++)
                     if (q == k) vk = v[q];
-                const float approx = __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, vk));
+                const float approx = approx_key(xn, vk);
                 const float thr = rowthr ? thr_r : cs[3 * kTile + cj];
                 const bool exact = qexact && colint[st * kTile + cj];
                 const float eps =
@@ -957,8 +972,9 @@ int tc_leaf_tiles(Ctx* c, const std::vector<LeafRef>& leaves, uint32_t cap, std:
 int tc_leaf_filter(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_norms, uint64_t n, uint32_t xs,
                    uint32_t d, const uint32_t* d_members, const LeafTile* d_tiles, size_t ntiles,
                    const float* list_kd, const uint32_t* list_sz, uint32_t K, uint32_t* cnt, uint32_t cap,
-                   uint32_t* out_id, float* out_key, uint64_t pos_base) {
+                   uint32_t* out_id, float* out_key, uint64_t pos_base, uint32_t key_mode) {
     if (ntiles == 0) return ANQI_OK;
+    if (key_mode > 1) return fail(c, ANQI_ERR_ARGS, "leaf tiles take the l2 or ip distance, not mode %u", key_mode);
     FilterParams p{};
     p.qb = p.xb = tp.bf.as<__nv_bfloat16>();
     p.q32 = p.x32 = d_x;
@@ -982,6 +998,7 @@ int tc_leaf_filter(Ctx* c, const TcPrep& tp, const float* d_x, const float* d_no
     p.list_sz = list_sz;
     p.list_k = K;
     p.pos_base = pos_base;
+    p.key_mode = key_mode;
     p.bx_norm = tp.bnorm;
     p.bx_err = tp.berr;
     p.bx_n = tp.bn;
@@ -1008,7 +1025,7 @@ int tc_leaf_candidates(Ctx* c, const TcPrep& tp, const float* d_x, const float* 
     TmpBuf dt(c);
     if ((rc = h2d(c, dt, tiles.data(), tiles.size() * sizeof(LeafTile)))) return rc;
     if ((rc = tc_leaf_filter(c, tp, d_x, d_norms, n, xs, d, d_members, dt.as<LeafTile>(), tiles.size(), list_kd,
-                             list_sz, K, cnt, cap, out_id, out_key, pos_base)))
+                             list_sz, K, cnt, cap, out_id, out_key, pos_base, 0)))
         return rc;
     return check_device_error(c, "tensor-core init_knn filter");
 }

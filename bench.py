@@ -91,6 +91,9 @@ def parse():
     ap.add_argument("--graph-options", type=int, default=200_000,
                     help="rows of the mixture on which the graph options (both Vamana styles, an edge "
                          "policy) are built and queried beside the default graph; 0 skips it")
+    ap.add_argument("--ip-metric", type=int, default=200_000,
+                    help="rows of an L2-normalised N(0,1) index built and queried under the ip metric "
+                         "(AKNN source, LRQ, lift, graph, exact ground truth); 0 skips it")
     ap.add_argument("--shape960", type=int, default=1_000_000,
                     help="rows of the batching form's second shape (L2-normalised N(0,1), d = 960) run after the "
                          "main line, with QPS and recall; 0 skips it")
@@ -446,6 +449,69 @@ def run_graph_options(ctx, a):
     return out
 
 
+def run_ip_metric(ctx, a):
+    """The ip metric on an n-row L2-normalised N(0,1) index (d = a.d): the
+    AKNN source under ip (angular forest, record keys -<a, b>), the LRQ fit on
+    those signed keys (u8, floor), the ip lift (s^2 r), the G48 graph, the
+    exact ip ground truth (keys -<a, b>, FP32 CUDA cores), then recall /
+    precision per k and the QPS of one CUDA-graph replay over the queries at
+    every k (L = a.L).  The same stages as build_aknn_source / lrq_train /
+    dataset_gt / rknn_query with metric ip."""
+    from anqi import pipeline, lrq_fit
+    n, nq, ks = a.ip_metric, 2000, [10, 50, 100]
+    base, query = pipeline.gaussian(n, a.d, nq, seed=20260819, normalize=True)
+    t = {}
+    t0 = time.perf_counter()
+    ids, keys, st = pipeline.aknn_build(ctx, base, metric="ip")
+    t["aknn_build"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    mu, basis, cb = (np.asarray(v, np.float32) for v in
+                     lrq_fit.train_gpu(keys, len(keys), device=ctx.device, log=lambda s: None))
+    t["lrq_train"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    coeff, codes, _ = ctx.lrq_encode_bits(keys, mu, basis, cb, 8)
+    lifted, m2, sc = ctx.lift(base, keys[:, -1], metric="ip")
+    t["encode_lift"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    deg, links, tree, _ = pipeline.graph_build(ctx, lifted, ids)
+    t["graph"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ex_ids, ex = pipeline.exact_thresholds(ctx, base, 100, metric="ip")
+    t["exact_thresholds"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    gt = {k: pipeline.rknn_ground_truth(ctx, base, query, ex[:, k - 1], metric="ip") for k in ks}
+    t["rknn_ground_truth"] = time.perf_counter() - t0
+    # the AKNN lists against the exact top-100 on every 100th row
+    rows = range(0, n, 100)
+    aknn_recall = float(np.mean([len(np.intersect1d(ids[i], ex_ids[i])) for i in rows])) / 100.0
+    del ex_ids
+    ctx.index_load(base, lifted, deg, links, tree, sc, m2, metric="ip")
+    ctx.verifier_load_bits(coeff, codes, None, keys.shape[1], mu, basis, cb, 8, signed_keys=True)
+    for k in ks:
+        ctx.verifier_materialize(k)
+    per_k = {}
+    for k in ks:
+        ctx.query_upload(query, k, a.L)
+        ctx.query_run()
+        e = ctx.query_evaluate(gt[k][0], gt[k][1])
+        per_k[k] = {"recall": round(e["recall"], 6), "precision": round(e["precision"], 6),
+                    "mean_gt": round(float(np.diff(gt[k][0]).mean()), 3)}
+    qb = np.ascontiguousarray(np.tile(query, (len(ks), 1)))
+    kb = np.repeat(np.array(ks, np.uint32), nq)
+    ctx.query_upload(qb, kb, np.full(len(kb), a.L, np.uint32))
+    for _ in range(3):
+        ctx.query_run_graph()
+    ctx.timer_start()
+    for _ in range(10):
+        ctx.query_run_graph()
+    ms = ctx.timer_stop()
+    return {"n": n, "d": a.d, "nq": nq, "L": a.L, "data": "L2-normalised N(0,1) rows, metric ip",
+            "seconds": {k: round(v, 3) for k, v in t.items()},
+            "aknn_init_ms": round(st["init_ms"], 1), "aknn_gather_kernel_ms": round(st["gather_kernel_ms"], 1),
+            "aknn_recall_at_100": round(aknn_recall, 5), "mean_degree": round(float(deg.mean()), 2),
+            "per_k": per_k, "qps": round(10 * len(kb) / (ms / 1e3), 1)}
+
+
 def run_shape960(ctx, a, steps, warmup):
     """The batching form's second shape: n x 960 L2-normalised N(0,1) rows and
     10,000 queries, the whole index built here (AKNN source with the K-chunked
@@ -712,6 +778,12 @@ def run_ours(a, rank, world, local):
             line["graph_options"] = run_graph_options(ctx, a)
         except Exception as e:  # reported, not fatal: the main line stands
             line["graph_options"] = {"error": f"{type(e).__name__}: {e}"}
+    if a.ip_metric and world == 1:
+        # after the main line's measurements: another index replaces it
+        try:
+            line["ip_metric"] = run_ip_metric(ctx, a)
+        except Exception as e:  # reported, not fatal: the main line stands
+            line["ip_metric"] = {"error": f"{type(e).__name__}: {e}"}
     if a.shape960 and world == 1 and a.d == 128:
         # after the main line's measurements: the second shape replaces the index
         try:

@@ -174,6 +174,28 @@ def test_ip_aknn_build_vs_oracle_stages(ctx):
     assert np.array_equal(bits(keys), bits(ref_d - np.float32(1.0)))
 
 
+@pytest.mark.parametrize("data", ["normalized", "integers", "wide"])
+def test_ip_aknn_build_tensor_init_equals_fp32(ctx, data):
+    """init_knn under ip on BF16 tcgen05 tiles (key~ = 1 - <q~, x~>, eps bound,
+    FP32 recheck in the sequential order) gives the FP32 path's lists and keys:
+    L2-normalised rows (every pair near the bound rechecked), integer rows (the
+    exact path, no recheck) and rows wider than the resident tile (K chunks)."""
+    rng = np.random.default_rng(17)
+    if data == "normalized":
+        x = rng.normal(size=(6000, 96))
+        x /= np.linalg.norm(x, axis=1, keepdims=True)
+    elif data == "integers":
+        x = rng.integers(-6, 7, size=(6000, 64))
+    else:
+        x = rng.normal(size=(2500, 300))
+    x = x.astype(np.float32)
+    kw = dict(k=50, leaf=200, trees=6, ef=100, metric="ip")
+    i16, k16, st = pipeline.aknn_build(ctx, x, precision="bf16", **kw)
+    i32, k32, _ = pipeline.aknn_build(ctx, x, precision="fp32", **kw)
+    assert np.array_equal(i16, i32)
+    assert np.array_equal(bits(k16), bits(k32))
+
+
 def test_ip_rejects_localjoin_rounds(ctx):
     x = np.random.default_rng(1).normal(size=(500, 8)).astype(np.float32)
     p = AknnParams(10, 50, 2, 20, 8, 10, 2, 20, 0, IP)
