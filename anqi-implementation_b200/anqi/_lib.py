@@ -205,8 +205,12 @@ _SIGS = {
     "anqi_lrq_fit_decode": [_vp, C.c_uint64, C.c_uint32, _vp, C.c_uint32, _vp, _vp, C.c_uint32,
                             C.POINTER(C.c_uint32), _vp],
     "anqi_exact_topk_tc": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _vp, C.c_uint32, _u32, _f32],
+    "anqi_exact_topk_tc_metric": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _vp, C.c_uint32, C.c_uint32, _u32,
+                                  _f32],
     "anqi_rknn_ground_truth_tc": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32, _u32, _u32, _f32,
                                   C.c_uint64, C.POINTER(C.c_uint64)],
+    "anqi_rknn_ground_truth_tc_metric": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32, C.c_uint32, _u32,
+                                         _u32, _f32, C.c_uint64, C.POINTER(C.c_uint64)],
     "anqi_bf16_gram": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32],
     "anqi_exact_topk": [_vp, _f32, C.c_uint64, C.c_uint32, C.c_uint32, _u32, _f32],
     "anqi_rknn_ground_truth": [_vp, _f32, C.c_uint64, _f32, C.c_uint64, C.c_uint32, _f32, _u32, _u32, _f32,
@@ -560,19 +564,19 @@ class Context:
         self._check(self.lib.anqi_query_evaluate_sums(self.h, C.byref(e)), "query_evaluate_sums")
         return {k: getattr(e, k) for k, _ in EvalSums._fields_}
 
-    def exact_topk_tc(self, base: np.ndarray, K: int, hints: np.ndarray | None = None):
-        """Exact top-K (ids, keys) on the BF16 tensor path; equals anqi_exact_topk."""
+    def exact_topk_tc(self, base: np.ndarray, K: int, hints: np.ndarray | None = None, metric: str = "l2"):
+        """Exact top-K (ids, keys) on the BF16 tensor path; equals anqi_exact_topk_metric."""
         base = _c(base, np.float32)
         n, d = base.shape
         ids = np.empty((n, K), np.uint32)
         keys = np.empty((n, K), np.float32)
         h = None if hints is None else _c(hints, np.uint32)
-        self._check(self.lib.anqi_exact_topk_tc(self.h, base, n, d, K, _ptr(h), 0 if h is None else h.shape[1], ids,
-                                                keys), "exact_topk_tc")
+        self._check(self.lib.anqi_exact_topk_tc_metric(self.h, base, n, d, K, _ptr(h), 0 if h is None else h.shape[1],
+                                                       METRICS[metric], ids, keys), "exact_topk_tc")
         return ids, keys
 
-    def rknn_ground_truth_tc(self, base: np.ndarray, query: np.ndarray, rk2: np.ndarray):
-        """Reverse-kNN CSR (off, ids, keys) on the BF16 tensor path; equals anqi_rknn_ground_truth."""
+    def rknn_ground_truth_tc(self, base: np.ndarray, query: np.ndarray, rk2: np.ndarray, metric: str = "l2"):
+        """Reverse-kNN CSR (off, ids, keys) on the BF16 tensor path; equals anqi_rknn_ground_truth_metric."""
         base = _c(base, np.float32)
         query = _c(query, np.float32)
         rk2 = _c(rk2, np.float32)
@@ -584,8 +588,8 @@ class Context:
         while True:
             ids = np.empty(cap, np.uint32)
             keys = np.empty(cap, np.float32)
-            rc = self.lib.anqi_rknn_ground_truth_tc(self.h, base, n, query, nq, d, rk2, off, ids, keys, cap,
-                                                    C.byref(tot))
+            rc = self.lib.anqi_rknn_ground_truth_tc_metric(self.h, base, n, query, nq, d, rk2, METRICS[metric], off,
+                                                           ids, keys, cap, C.byref(tot))
             if rc == ANQI_ERR_CAPACITY and tot.value > cap:
                 cap = int(tot.value)
                 continue

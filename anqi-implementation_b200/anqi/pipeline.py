@@ -226,11 +226,11 @@ def exact_thresholds(ctx: Context, base: np.ndarray, K: int = 100, method: str =
     """Exact top-K (dataset_gt --mode thresholds).  method "tc": BF16 tensor-core
     tiles with FP32 recheck (bit-identical output); hints = AKNN lists bound each
     row's K-th key (an AKNN build runs when they are absent).  metric "ip": keys
-    -<a, b> (FP32 CUDA cores)."""
+    -<a, b>."""
     base = np.ascontiguousarray(base, np.float32)
     n, d = base.shape
-    if method == "tc" and d <= 1024 and metric == "l2":
-        return ctx.exact_topk_tc(base, K, hints)
+    if method == "tc" and d <= 1024:
+        return ctx.exact_topk_tc(base, K, hints, metric)
     ids = np.empty((n, K), np.uint32)
     keys = np.empty((n, K), np.float32)
     ctx._check(ctx.lib.anqi_exact_topk_metric(ctx.h, base, n, d, K, METRICS[metric], ids, keys), "exact_topk")
@@ -240,8 +240,8 @@ def exact_thresholds(ctx: Context, base: np.ndarray, K: int = 100, method: str =
 def rknn_ground_truth(ctx: Context, base: np.ndarray, query: np.ndarray, rk2: np.ndarray, method: str = "fp32",
                       metric: str = "l2"):
     """Exact RkNN CSR (dataset_gt --mode ground-truth); method "tc" as above."""
-    if method == "tc" and base.shape[1] <= 1024 and metric == "l2":
-        return ctx.rknn_ground_truth_tc(base, query, rk2)
+    if method == "tc" and base.shape[1] <= 1024:
+        return ctx.rknn_ground_truth_tc(base, query, rk2, metric)
     base = np.ascontiguousarray(base, np.float32)
     query = np.ascontiguousarray(query, np.float32)
     n, d = base.shape

@@ -213,11 +213,11 @@ constexpr uint32_t kWideK = 64;
 constexpr uint32_t kWideStages = 4;
 constexpr uint32_t kWideMaxDp = 1024;
 
-// The reference's FP32 key |q|^2 + |x|^2 - 2 <q, x> (dataset_gt.cpp:225, 294)
-// with <q, x> in the 16-lane AVX-512 order of include/distance.h:89-116,
-// computed by one thread.
+// The reference's FP32 key |q|^2 + |x|^2 - 2 <q, x> (dataset_gt.cpp:225, 294;
+// mode 2, the ip metric: -<q, x>, dataset_gt.cpp:288) with <q, x> in the
+// 16-lane AVX-512 order of include/distance.h:89-116, computed by one thread.
 __device__ __forceinline__ float ref_key(const float* __restrict__ q, const float* __restrict__ x, uint32_t d,
-                                         float qn, float xn) {
+                                         float qn, float xn, uint32_t mode = 0) {
     const uint32_t d16 = d & ~15u;
     float acc[16];
 #pragma unroll
@@ -240,6 +240,7 @@ __device__ __forceinline__ float ref_key(const float* __restrict__ q, const floa
         for (int l = 0; l < 16; l++) p[l] = (d16 + l < d) ? __fmul_rn(q[d16 + l], x[d16 + l]) : 0.f;
         ip = __fadd_rn(ip, fold(p));
     }
+    if (mode == 2) return -ip;
     return __fsub_rn(__fadd_rn(qn, xn), __fmul_rn(2.0f, ip));
 }
 
@@ -354,7 +355,7 @@ __global__ void __launch_bounds__(kFilterThreads, kWide ? 1 : 2) tc_filter_kerne
     // key~ from the accumulator, in the FP32 steps of the reference's key
     auto approx_key = [&](float xnc, float acc) {
         return l2k ? __fsub_rn(__fadd_rn(qn, xnc), __fmul_rn(2.0f, acc))
-                   : (p.key_mode == 1 ? __fsub_rn(1.0f, acc) : -acc);
+                   : (p.key_mode == 1 ? __fsub_rn(1.0f, acc) : -__fadd_rn(acc, 0.0f));  // +0 as the reference's
     };
     const float* qrow = p.q32 + (row_ok ? my_row : 0) * p.xs;
     // eps <= epsmax for every column of this row (eps grows with the column's
@@ -415,7 +416,7 @@ __global__ void __launch_bounds__(kFilterThreads, kWide ? 1 : 2) tc_filter_kerne
                     continue;
                 }
                 const bool later = p.defer_recheck && !exact;
-                const float key = (exact || later) ? approx : ref_key(qrow, p.x32 + j * p.xs, p.d, qn, xn);
+                const float key = (exact || later) ? approx : ref_key(qrow, p.x32 + j * p.xs, p.d, qn, xn, p.key_mode);
                 if (!later && !(key <= thr)) continue;
                 const uint32_t pos = atomicAdd(p.cnt + my_row, 1u);
                 if (pos < p.cap) {
@@ -539,7 +540,7 @@ __global__ void __launch_bounds__(kFilterThreads, kWide ? 1 : 2) tc_filter_kerne
 // to K distinct other rows (the hints, e.g. the AKNN lists).  Warp per row.
 __global__ void hint_bound_kernel(const float* __restrict__ x, const float* __restrict__ xn, uint64_t n,
                                   uint32_t xs, uint32_t d, const uint32_t* __restrict__ hints, uint32_t hk,
-                                  uint32_t K, float* __restrict__ tau) {
+                                  uint32_t K, float* __restrict__ tau, uint32_t mode) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -552,7 +553,7 @@ __global__ void hint_bound_kernel(const float* __restrict__ x, const float* __re
                 bad = true;
                 continue;
             }
-            mx = fmaxf(mx, ref_key(x + i * xs, x + (uint64_t)j * xs, d, xn[i], xn[j]));
+            mx = fmaxf(mx, ref_key(x + i * xs, x + (uint64_t)j * xs, d, xn[i], xn[j], mode));
         }
         for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
         bad = __any_sync(0xFFFFFFFFu, bad);
@@ -649,7 +650,8 @@ __global__ void compact_rows_kernel(const uint32_t* __restrict__ cnt, uint32_t c
 __global__ void __launch_bounds__(256) recheck_rows_kernel(const uint64_t* __restrict__ off, uint64_t nrows,
                                                            const uint32_t* __restrict__ rows, uint32_t* __restrict__ ids,
                                                            float* __restrict__ keys, const float* __restrict__ x32,
-                                                           const float* __restrict__ xn, uint32_t xs, uint32_t d) {
+                                                           const float* __restrict__ xn, uint32_t xs, uint32_t d,
+                                                           uint32_t mode) {
     const uint32_t lane = threadIdx.x & 31u, gt = lane & 3u, gw = lane >> 2;
     const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -666,7 +668,7 @@ __global__ void __launch_bounds__(256) recheck_rows_kernel(const uint64_t* __res
             const float ip = group_ip(x32 + q * xs, x32 + (uint64_t)(flagged ? j : (uint32_t)q) * xs, d, gt,
                                       0xFFFFFFFFu);
             if (flagged && gt == 0) {
-                keys[e] = __fsub_rn(__fadd_rn(xn[q], xn[j]), __fmul_rn(2.0f, ip));
+                keys[e] = mode == 2 ? -ip : __fsub_rn(__fadd_rn(xn[q], xn[j]), __fmul_rn(2.0f, ip));
                 ids[e] = j;
             }
         }
@@ -1089,7 +1091,15 @@ int anqi_bf16_gram(anqi_ctx* h, const float* a, uint64_t na, const float* b, uin
 int anqi_rknn_ground_truth_tc(anqi_ctx* h, const float* base, uint64_t n, const float* query, uint64_t nq,
                               uint32_t d, const float* rk2, uint32_t* off, uint32_t* ids, float* keys, uint64_t cap,
                               uint64_t* total) {
-    if (!h || !base || !query || !rk2 || !off || n == 0 || nq == 0 || d == 0) return ANQI_ERR_ARGS;
+    return anqi_rknn_ground_truth_tc_metric(h, base, n, query, nq, d, rk2, ANQI_METRIC_L2, off, ids, keys, cap,
+                                            total);
+}
+
+int anqi_rknn_ground_truth_tc_metric(anqi_ctx* h, const float* base, uint64_t n, const float* query, uint64_t nq,
+                                     uint32_t d, const float* rk2, uint32_t metric, uint32_t* off, uint32_t* ids,
+                                     float* keys, uint64_t cap, uint64_t* total) {
+    if (!h || !base || !query || !rk2 || !off || n == 0 || nq == 0 || d == 0 || metric > ANQI_METRIC_IP)
+        return ANQI_ERR_ARGS;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     const uint32_t dp = tc_dp(d), xs = round_up(d, 8u);
@@ -1104,6 +1114,7 @@ int anqi_rknn_ground_truth_tc(anqi_ctx* h, const float* base, uint64_t n, const 
                             &p.bx_norm, &p.bx_err, &p.bx_n, &p.all_exact)))
         return rc;
     p.thr_col = dr.as<float>();
+    p.key_mode = metric == ANQI_METRIC_IP ? 2u : 0u;
     std::vector<uint64_t> hoff;
     if ((rc = filter_to_csr(c, p, nq, 256, hoff, doff, did, dkey))) return rc;
     const uint64_t tot = hoff[nq];
@@ -1120,7 +1131,13 @@ int anqi_rknn_ground_truth_tc(anqi_ctx* h, const float* base, uint64_t n, const 
 
 int anqi_exact_topk_tc(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, uint32_t K, const uint32_t* hints,
                        uint32_t hint_k, uint32_t* ids, float* keys) {
-    if (!h || !base || !ids || !keys || d == 0 || K == 0 || K > 256) return ANQI_ERR_ARGS;
+    return anqi_exact_topk_tc_metric(h, base, n, d, K, hints, hint_k, ANQI_METRIC_L2, ids, keys);
+}
+
+int anqi_exact_topk_tc_metric(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, uint32_t K,
+                              const uint32_t* hints, uint32_t hint_k, uint32_t metric, uint32_t* ids, float* keys) {
+    if (!h || !base || !ids || !keys || d == 0 || K == 0 || K > 256 || metric > ANQI_METRIC_IP) return ANQI_ERR_ARGS;
+    const uint32_t mode = metric == ANQI_METRIC_IP ? 2u : 0u;
     Ctx* c = &h->c;
     cudaSetDevice(c->device);
     if (K >= n) return fail(c, ANQI_ERR_ARGS, "require K < base vector count");
@@ -1138,6 +1155,7 @@ int anqi_exact_topk_tc(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, u
         ap.seed = 10;
         ap.nn_sample = 20;
         ap.precision = 1;
+        ap.metric = metric;
         if (ap.k >= n) ap.k = (uint32_t)n - 1;
         own.resize(n * ap.k);
         std::vector<float> od(n * ap.k);
@@ -1153,7 +1171,7 @@ int anqi_exact_topk_tc(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, u
     if ((rc = X.load(c, base, n, d, xs, dp)) || (rc = h2d(c, dh, hints, n * hint_k * 4)) || (rc = ensure(c, tau, n * 4)))
         return rc;
     hint_bound_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(X.f32.as<float>(), X.rn.as<float>(), n, xs, d,
-                                                              dh.as<uint32_t>(), hint_k, K, tau.as<float>());
+                                                              dh.as<uint32_t>(), hint_k, K, tau.as<float>(), mode);
     ANQI_CUDA(c, cudaGetLastError());
     FilterParams p = make_params(X, X, n, xs, d, dp);
     if ((rc = tc_row_bounds(c, X.rn.as<float>(), X.nrm.as<float>(), X.err.as<float>(), X.xint.as<uint8_t>(), n,
@@ -1162,12 +1180,13 @@ int anqi_exact_topk_tc(anqi_ctx* h, const float* base, uint64_t n, uint32_t d, u
     p.thr_row = tau.as<float>();
     p.exclude_self = 1;
     p.defer_recheck = 1;
+    p.key_mode = mode;
     std::vector<uint64_t> hoff;
     if ((rc = filter_to_csr(c, p, n, K + 156, hoff, doff, did, dkey))) return rc;
     // the deferred FP32 rechecks, then each row again in (key, id) order
     recheck_rows_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(doff.as<uint64_t>(), n, nullptr, did.as<uint32_t>(),
                                                                 dkey.as<float>(), X.f32.as<float>(), X.rn.as<float>(),
-                                                                xs, d);
+                                                                xs, d, mode);
     ANQI_CUDA(c, cudaGetLastError());
     {
         uint64_t maxm = 0;

@@ -475,12 +475,24 @@ def run_ip_metric(ctx, a):
     t0 = time.perf_counter()
     deg, links, tree, _ = pipeline.graph_build(ctx, lifted, ids)
     t["graph"] = time.perf_counter() - t0
+    # the exact ground truth on the BF16 tensor path (the AKNN lists bound each
+    # row's 100th key) and on FP32 CUDA cores: identical outputs
     t0 = time.perf_counter()
-    ex_ids, ex = pipeline.exact_thresholds(ctx, base, 100, metric="ip")
+    ex_ids, ex = pipeline.exact_thresholds(ctx, base, 100, method="tc", hints=ids, metric="ip")
     t["exact_thresholds"] = time.perf_counter() - t0
     t0 = time.perf_counter()
-    gt = {k: pipeline.rknn_ground_truth(ctx, base, query, ex[:, k - 1], metric="ip") for k in ks}
+    gt = {k: pipeline.rknn_ground_truth(ctx, base, query, ex[:, k - 1], method="tc", metric="ip") for k in ks}
     t["rknn_ground_truth"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    f_ids, f_keys = pipeline.exact_thresholds(ctx, base, 100, metric="ip")
+    t["exact_thresholds_fp32"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    f_gt = {k: pipeline.rknn_ground_truth(ctx, base, query, f_keys[:, k - 1], metric="ip") for k in ks}
+    t["rknn_ground_truth_fp32"] = time.perf_counter() - t0
+    gt_identical = bool(np.array_equal(f_ids, ex_ids) and np.array_equal(f_keys.view(np.uint32), ex.view(np.uint32))
+                        and all(np.array_equal(f_gt[k][0], gt[k][0]) and np.array_equal(f_gt[k][1], gt[k][1])
+                                for k in ks))
+    del f_ids, f_keys, f_gt
     # the AKNN lists against the exact top-100 on every 100th row
     rows = range(0, n, 100)
     aknn_recall = float(np.mean([len(np.intersect1d(ids[i], ex_ids[i])) for i in rows])) / 100.0
@@ -508,7 +520,7 @@ def run_ip_metric(ctx, a):
     return {"n": n, "d": a.d, "nq": nq, "L": a.L, "data": "L2-normalised N(0,1) rows, metric ip",
             "seconds": {k: round(v, 3) for k, v in t.items()},
             "aknn_init_ms": round(st["init_ms"], 1), "aknn_gather_kernel_ms": round(st["gather_kernel_ms"], 1),
-            "aknn_recall_at_100": round(aknn_recall, 5), "mean_degree": round(float(deg.mean()), 2),
+            "exact_gt_tc_equals_fp32": gt_identical, "aknn_recall_at_100": round(aknn_recall, 5), "mean_degree": round(float(deg.mean()), 2),
             "per_k": per_k, "qps": round(10 * len(kb) / (ms / 1e3), 1)}
 
 

@@ -580,6 +580,14 @@ int anqi_exact_topk_tc(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d,
 int anqi_rknn_ground_truth_tc(anqi_ctx* ctx, const float* base, uint64_t n, const float* query, uint64_t nq,
                               uint32_t d, const float* rk2, uint32_t* off, uint32_t* ids, float* keys,
                               uint64_t cap, uint64_t* total);
+/* The same under either metric (ANQI_METRIC_L2 or ANQI_METRIC_IP: key -<a, b>,
+ * as anqi_exact_topk_metric / anqi_rknn_ground_truth_metric, which they equal
+ * bit for bit).  Without hints the AKNN build runs under the same metric. */
+int anqi_exact_topk_tc_metric(anqi_ctx* ctx, const float* base, uint64_t n, uint32_t d, uint32_t K,
+                              const uint32_t* hints, uint32_t hint_k, uint32_t metric, uint32_t* ids, float* keys);
+int anqi_rknn_ground_truth_tc_metric(anqi_ctx* ctx, const float* base, uint64_t n, const float* query, uint64_t nq,
+                                     uint32_t d, const float* rk2, uint32_t metric, uint32_t* off, uint32_t* ids,
+                                     float* keys, uint64_t cap, uint64_t* total);
 
 #ifdef __cplusplus
 }

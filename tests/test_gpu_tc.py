@@ -127,3 +127,35 @@ def test_wide_tensor_path_equals_fp32(ctx, d):
     a_ids, a_keys, _ = pipeline.aknn_build(ctx, base, k=50, leaf=300, trees=8, ef=150, precision="bf16")
     f_ids, f_keys, _ = pipeline.aknn_build(ctx, base, k=50, leaf=300, trees=8, ef=150, precision="fp32")
     assert np.array_equal(a_ids, f_ids) and np.array_equal(bits(a_keys), bits(f_keys))
+
+
+@pytest.mark.parametrize("data,d", [("normalized", 96), ("integers", 64), ("sparse_integers", 40), ("wide", 300)])
+def test_ip_tensor_ground_truth_equals_fp32(ctx, data, d):
+    """The ip metric on the tensor path (key -<a, b>: half the product terms of
+    the l2 bound, FP32 recheck in the lane order): exact top-K, with the AKNN
+    lists as hints and without, and the RkNN CSR equal the FP32 path bit for
+    bit.  Sparse integer rows make exactly-zero products of either sign."""
+    from anqi import pipeline
+    rng = np.random.default_rng(d)
+    n, nq, K = 3000, 300, 50
+    if data == "normalized" or data == "wide":
+        x = rng.normal(size=(n + nq, d))
+        x /= np.linalg.norm(x, axis=1, keepdims=True)
+    elif data == "integers":
+        x = rng.integers(-8, 9, size=(n + nq, d))
+    else:
+        x = rng.integers(-2, 3, size=(n + nq, d)) * (rng.random((n + nq, d)) < 0.1)
+    x = x.astype(np.float32)
+    base, query = x[:n], x[n:]
+    fi, fk = pipeline.exact_thresholds(ctx, base, K, metric="ip")
+    hints, _, _ = pipeline.aknn_build(ctx, base, k=K, leaf=200, trees=6, ef=100, metric="ip")
+    for h in (hints, None):
+        ti, tk = pipeline.exact_thresholds(ctx, base, K, method="tc", hints=h, metric="ip")
+        assert np.array_equal(ti, fi)
+        assert np.array_equal(tk.view(np.uint32), fk.view(np.uint32))
+    for k in (1, 10, K):
+        fo, fid, fkey = pipeline.rknn_ground_truth(ctx, base, query, fk[:, k - 1], metric="ip")
+        to, tid, tkey = pipeline.rknn_ground_truth(ctx, base, query, fk[:, k - 1], method="tc", metric="ip")
+        assert np.array_equal(fo, to)
+        assert np.array_equal(fid, tid)
+        assert np.array_equal(fkey.view(np.uint32), tkey.view(np.uint32))
