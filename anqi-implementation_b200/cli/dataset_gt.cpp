@@ -119,12 +119,19 @@ static int run(int argc, char** argv) {
 
     std::vector<float> rk2(n);
     double threshold_build_s = 0.0;
+    // From 20,000 rows the BF16 tensor-core tiles with FP32 recheck (outputs
+    // equal to the FP32 CUDA-core path bit for bit); ANQI_B200_GT_TENSOR=0
+    // keeps the FP32 path.
+    const char* tenv = std::getenv("ANQI_B200_GT_TENSOR");
+    const bool tensor = D <= 1024 && n >= 20000 && !(tenv && std::strcmp(tenv, "0") == 0);
     if (build_thresholds) {
         std::vector<uint32_t> ids(n * K);
         std::vector<float> keys(n * K);
         const auto t1 = std::chrono::steady_clock::now();
-        dev().check(anqi_exact_topk_metric(dev().get(), base.x.data(), n, (uint32_t)D, (uint32_t)K, metric_code,
-                                           ids.data(), keys.data()),
+        dev().check(tensor ? anqi_exact_topk_tc_metric(dev().get(), base.x.data(), n, (uint32_t)D, (uint32_t)K, nullptr,
+                                                       0, metric_code, ids.data(), keys.data())
+                           : anqi_exact_topk_metric(dev().get(), base.x.data(), n, (uint32_t)D, (uint32_t)K,
+                                                    metric_code, ids.data(), keys.data()),
                     "exact top-K");
         std::cout << "[dgt] base-to-base top-K done in "
                   << std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count() << "s\n";
@@ -169,9 +176,13 @@ static int run(int argc, char** argv) {
         for (int attempt = 0; attempt < 2; attempt++) {
             ids.resize(cap);
             keys.resize(cap);
-            const int rc = anqi_rknn_ground_truth_metric(dev().get(), base.x.data(), n, query.x.data(), nq,
-                                                         (uint32_t)D, rk2.data(), metric_code, off.data(), ids.data(),
-                                                         keys.data(), cap, &total);
+            const int rc =
+                tensor ? anqi_rknn_ground_truth_tc_metric(dev().get(), base.x.data(), n, query.x.data(), nq, (uint32_t)D,
+                                                          rk2.data(), metric_code, off.data(), ids.data(), keys.data(),
+                                                          cap, &total)
+                       : anqi_rknn_ground_truth_metric(dev().get(), base.x.data(), n, query.x.data(), nq, (uint32_t)D,
+                                                       rk2.data(), metric_code, off.data(), ids.data(), keys.data(), cap,
+                                                       &total);
             if (rc == ANQI_ERR_CAPACITY && attempt == 0) {
                 cap = total;
                 continue;

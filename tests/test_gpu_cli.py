@@ -226,6 +226,34 @@ def test_dataset_gt_cli_ip_bit_exact(tmp_path):
         assert np.array_equal(bits(gkeys), bits(z[f"gt_keys_{k}"]))
 
 
+@pytest.mark.parametrize("metric", ["l2", "ip"])
+def test_dataset_gt_cli_tensor_path_equals_fp32(tmp_path, metric):
+    """From 20,000 rows dataset_gt runs the BF16 tensor path (its own AKNN
+    lists bound the thresholds); its files equal the FP32 path's
+    (ANQI_B200_GT_TENSOR=0) byte for byte."""
+    rng = np.random.default_rng(3)
+    x = rng.normal(size=(20500, 48))
+    if metric == "ip":
+        x /= np.linalg.norm(x, axis=1, keepdims=True)
+    base, query = tmp_path / "b.bin", tmp_path / "q.bin"
+    formats.write_fbin(base, x[:20000].astype(np.float32))
+    formats.write_fbin(query, x[20000:].astype(np.float32))
+    files = {}
+    for mode, env in (("tensor", {}), ("fp32", {"ANQI_B200_GT_TENSOR": "0"})):
+        thr = tmp_path / f"thr_{mode}"
+        rc, out, err = tc.run("dataset_gt", "--base", base, "--K", 100, "--rk_k", 50, "--metric", metric,
+                              "--mode", "thresholds", "--out_prefix", thr, env=env)
+        assert rc == 0, err
+        t = tmp_path / f"gt_{mode}"
+        rc, out, err = tc.run("dataset_gt", "--base", base, "--query", query, "--K", 100, "--rk_k", 50,
+                              "--metric", metric, "--mode", "ground-truth", "--threshold-table",
+                              f"{thr}_baseknn_gt.bin", "--out_prefix", t, env=env)
+        assert rc == 0, err
+        files[mode] = (Path(f"{thr}_baseknn_gt.bin").read_bytes(), Path(f"{t}_rknn_gt.bin").read_bytes())
+    assert files["tensor"][0] == files["fp32"][0]
+    assert files["tensor"][1] == files["fp32"][1]
+
+
 def test_build_aknn_source_cli_ip(tmp_path):
     """metric=ip: .rec keys are d - 1 = -<a, b> (build_aknn_source.cpp:125), rows
     ascending, self excluded, recall@100 against the exact -<a, b> table."""
