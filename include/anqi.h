@@ -163,8 +163,8 @@ typedef struct {
     uint32_t precision;  /* init_knn leaf distances: 0 = FP32 CUDA cores, 1 = BF16 tensor-core
                             tiles with FP32 recheck (identical output; d <= 1024, rows
                             above 256 dimensions in K chunks; larger d runs on the CUDA cores) */
-    uint32_t metric;     /* ANQI_METRIC_L2 (0) or ANQI_METRIC_IP; the ip metric runs FP32
-                            init_knn on the CUDA cores and takes no LocalJoin (nn_iters = 0) */
+    uint32_t metric;     /* ANQI_METRIC_L2 (0) or ANQI_METRIC_IP (key 1 - <a, b>, either
+                            precision); the ip metric takes no LocalJoin (nn_iters = 0) */
 } anqi_aknn_params;
 
 typedef struct {
